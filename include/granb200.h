@@ -1,0 +1,144 @@
+/*
+ * granb200.h -- C ABI of the B200 granular hot-path engine (libgranb200.so).
+ *
+ * One context = one LIGGGHTS "run" state on one GPU: particles (owned +
+ * periodic ghost images), the granular half neighbor list with contact
+ * history, wall fixes and the Velocity-Verlet sphere integrator.  The whole
+ * time step stays on the device; the host only uploads the initial state and
+ * downloads state on request.
+ *
+ * The entry points replace the following reference interfaces
+ * (LIGGGHTS-PUBLIC 3.8.0, paths relative to the project root):
+ *   gb2_create / gb2_set_materials  <- pair_style gran ... settings and the
+ *       material matrices of MODEL_PARAMS::createYeff/Geff/BetaEff/
+ *       CoeffFrict/CoeffRollFrict (src/pair_gran_proxy.cpp:63,
+ *       src/global_properties.cpp:411-560)
+ *   gb2_upload_atoms               <- read_data Atoms/Velocities into
+ *       Atom::x,v,omega,radius,rmass,type,tag (src/atom_vec_sphere.cpp:1055)
+ *   gb2_add_gravity                <- FixGravity (src/fix_gravity.cpp:301)
+ *   gb2_add_wall_plane             <- FixWallGran primitive {x,y,z}plane
+ *       (src/fix_wall_gran.cpp:1024)
+ *   gb2_add_wall_mesh              <- FixMeshSurface + FixWallGran mesh
+ *       (src/fix_mesh.cpp:343, src/fix_wall_gran.cpp:845)
+ *   gb2_setup                      <- Verlet::setup (src/verlet.cpp:134)
+ *   gb2_run                        <- Verlet::run (src/verlet.cpp:264): per
+ *       step FixNVESphere::initial_integrate, Neighbor::decide, the rebuild
+ *       (FixContactHistory::pre_exchange, Domain::pbc, Atom::sort,
+ *       Comm::borders, Neighbor::granular_bin_no_newton) or
+ *       Comm::forward_comm, PairGran::compute, post_force fixes and
+ *       FixNVESphere::final_integrate
+ *   gb2_download_atoms             <- lammps_gather_atoms (src/library.cpp)
+ *   gb2_download_pairs             <- NeighList firstneigh/firstdouble of the
+ *       granular history list (src/neigh_gran.cpp:485)
+ *   gb2_download_wall_history      <- fix wall/gran property/atom history
+ *   gb2_download_mesh_contacts     <- FixContactHistoryMesh partner_/
+ *       contacthistory_ (src/fix_contact_history_mesh.cpp)
+ *
+ * Every call returns 0 on success or a negative GB2_ERR_* code; the message
+ * is available from gb2_last_error.  The ABI is single-host-thread per
+ * context; different contexts are independent.
+ */
+#ifndef GRANB200_H
+#define GRANB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB2_OK               0
+#define GB2_ERR_ARG         -1   /* bad argument / unsupported keyword      */
+#define GB2_ERR_CUDA        -2   /* CUDA runtime error                      */
+#define GB2_ERR_CAPACITY    -3   /* capacity could not be grown             */
+#define GB2_ERR_LOST        -4   /* atom left a non-periodic box            */
+#define GB2_ERR_STATE       -5   /* call out of order (e.g. run before setup) */
+#define GB2_ERR_UNSUPPORTED -6   /* option outside the accelerated path     */
+
+#define GB2_PREC_FP64   0        /* IEEE FP64 throughout, FMA contraction off */
+#define GB2_PREC_SPLIT  1        /* FP32 contact arithmetic on FP64-differenced
+                                    positions, FP64 integration              */
+
+typedef struct gb2_ctx gb2_ctx;
+
+typedef struct {
+    int ntypes;                  /* atom types 1..ntypes                    */
+    double dt;                   /* timestep                                */
+    double skin;                 /* neighbor <skin> bin                     */
+    double boxlo[3], boxhi[3];   /* orthogonal box                          */
+    int periodic[3];             /* boundary p (1) or f (0) per dimension   */
+    int neigh_every;             /* neigh_modify every  (default 1)         */
+    int neigh_delay;             /* neigh_modify delay  (0 recommended)     */
+    int neigh_check;             /* neigh_modify check yes/no               */
+    int sort_freq;               /* atom_modify sort <freq> (default 1000)  */
+    double sort_binsize;         /* atom_modify sort ... <binsize> (0: auto)*/
+    int rolling_cdt;             /* pair_style gran ... rolling_friction cdt*/
+    int tangential_damping;      /* model option tangential_damping on/off  */
+    int precision;               /* GB2_PREC_FP64 or GB2_PREC_SPLIT          */
+    int device;                  /* CUDA device ordinal                     */
+} gb2_params;
+
+typedef struct {
+    long ntimestep;              /* update->ntimestep                       */
+    int nlocal, nghost;
+    int nbuilds;                 /* neighbor list builds so far             */
+    long npairs;                 /* half-list pairs at the last build       */
+    long ntouch;                 /* pairs with a set contact flag           */
+    int maxneigh, maxpartner;    /* current per-atom capacities             */
+    double time_pair, time_neigh, time_other;   /* device ms, cumulative    */
+    long kernel_launches;        /* kernels launched by gb2_run so far      */
+} gb2_stats;
+
+/* context lifecycle */
+int gb2_create(const gb2_params *p, gb2_ctx **out);
+int gb2_destroy(gb2_ctx *ctx);
+
+/* fix property/global youngsModulus/poissonsRatio (per type, ntypes values)
+   and coefficientRestitution/coefficientFriction/coefficientRollingFriction
+   (per type pair, row-major ntypes x ntypes; rollfriction may be NULL when
+   rolling friction is off). */
+int gb2_set_materials(gb2_ctx *ctx, const double *youngs, const double *poisson,
+                      const double *restitution, const double *friction,
+                      const double *rollfriction);
+
+/* owned atoms, host arrays: x,v,omega [n][3], radius,rmass [n], type,tag [n] */
+int gb2_upload_atoms(gb2_ctx *ctx, int n, const double *x, const double *v,
+                     const double *omega, const double *radius, const double *rmass,
+                     const int *type, const int *tag);
+
+/* post_force fixes, applied in the order they are added */
+int gb2_add_gravity(gb2_ctx *ctx, double magnitude, const double dir[3]);
+int gb2_add_wall_plane(gb2_ctx *ctx, int dim, double pos, int wall_type, int rolling_cdt);
+/* ntri triangles as read from an STL file, nodes[ntri][3][3]; curvature <= 0
+   selects the default 1 - 1e-5.  Returns the fix index (>= 0) or an error. */
+int gb2_add_wall_mesh(gb2_ctx *ctx, int ntri, const double *nodes, int wall_type,
+                      double curvature, int rolling_cdt);
+
+/* Verlet::setup and Verlet::run(nsteps) */
+int gb2_setup(gb2_ctx *ctx);
+int gb2_run(gb2_ctx *ctx, int nsteps);
+/* block until all device work of this context has finished */
+int gb2_sync(gb2_ctx *ctx);
+
+/* downloads (current owned-atom order; any pointer may be NULL) */
+int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, double *omega,
+                       double *f, double *torque, int *tag);
+/* half-list pairs (tag_i, tag_j, contact flag, shear history[3]); returns
+   the pair count in *n, writes at most cap entries */
+int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
+/* per-atom shear history of primitive-wall fix ifix, [nlocal][3] */
+int gb2_download_wall_history(gb2_ctx *ctx, int ifix, int cap, double *hist);
+/* occupied mesh-contact slots of mesh fix ifix: (atom tag, triangle id, shear[3]) */
+int gb2_download_mesh_contacts(gb2_ctx *ctx, int ifix, int cap, int *n, int *tag, int *tri, double *hist);
+/* mesh topology after load: per triangle edge/corner active flags and obtuse index */
+int gb2_mesh_topology(gb2_ctx *ctx, int ifix, int cap, int *ntri, unsigned char *edge_active,
+                      unsigned char *corner_active, int *obtuse);
+
+int gb2_get_stats(gb2_ctx *ctx, gb2_stats *st);
+/* copies the last error message (NUL-terminated) into buf */
+int gb2_last_error(gb2_ctx *ctx, char *buf, int len);
+/* library version string, e.g. "granb200 0.1 sm_100a" */
+const char *gb2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

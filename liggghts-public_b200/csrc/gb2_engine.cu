@@ -1,0 +1,1223 @@
+// gb2_engine.cu -- libgranb200: host orchestration of the device-resident
+// granular time step and the C ABI declared in include/granb200.h.
+//
+// Step structure (Verlet::run, src/verlet.cpp:264-388, one GPU):
+//   initial_integrate (+ displacement check)  -> one kernel
+//   Neighbor::decide                           -> host reads one flag
+//   rebuild (pre_exchange partners, pbc, sort, borders, bins, half list,
+//            reverse list)  or  forward_comm   -> kernels + CUB
+//   pre_force (wall neighbour lists, mesh history re-paging, rebuild only)
+//   pair pass A (reverse entries) + pass B (own entries, post_force fixes,
+//   final_integrate)                           -> two kernels
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/granb200.h"
+#include "gb2_internal.h"
+#include "gb2_kernels.cuh"
+
+using namespace gb2;
+
+namespace {
+
+constexpr int kBlock = 128;
+
+inline int nblk(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+// device buffer with explicit growth
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t m)   // discards contents
+    {
+        if (m <= n && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
+        if (e == cudaSuccess) n = m;
+        return e;
+    }
+    cudaError_t grow_keep(size_t m, size_t keep, cudaStream_t s)   // keeps the first `keep` elements
+    {
+        if (m <= n && p) return cudaSuccess;
+        T *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(m, 1) * sizeof(T));
+        if (e != cudaSuccess) return e;
+        if (p && keep) cudaMemcpyAsync(q, p, std::min(keep, n) * sizeof(T), cudaMemcpyDeviceToDevice, s);
+        cudaStreamSynchronize(s);
+        release();
+        p = q;
+        n = m;
+        return cudaSuccess;
+    }
+    void swap(DBuf &o)
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
+};
+
+struct MeshFix {
+    MeshTopo topo;
+    DBuf<TriGeom> tri;
+    DBuf<int> cnn_start, cnn_list, bin_tri_start, bin_tri_list;
+    int maxt = 8;
+    DBuf<int> tcnt, tlist, snp, spartner;
+    DBuf<double> shist;
+    DBuf<int> snp2, spartner2;   // re-paging target
+    DBuf<double> shist2;
+    bool bins_valid = false;
+    double nl_skin = 0, distmax = 0;
+};
+
+struct HostFix {
+    int kind = FIX_NONE;
+    double acc[3] = {0, 0, 0};
+    int dim = 2;
+    double pos = 0;
+    int wtype = 1;
+    int rolling = 0;
+    DBuf<uint8_t> inlist;
+    DBuf<double> whist;
+    MeshFix *mesh = nullptr;
+};
+
+}  // namespace
+
+struct gb2_ctx {
+    gb2_params P{};
+    std::string err;
+    cudaStream_t st = nullptr;
+    bool have_mat = false, have_atoms = false, setup_done = false, computeflag = false;
+    MatPair hmat[(kMaxTypes + 1) * (kMaxTypes + 1)];
+    DBuf<MatPair> dmat;
+
+    int nlocal = 0, nghost = 0, nmax = 0, cap = 0;
+    std::vector<double> h_radius;
+    std::vector<int> h_type;
+    DBuf<dbl4> pos, vel, omg, vel2, omg2, f, tq, fpart, tpart, xhold;
+    DBuf<int> type, tag;
+    int maxn = 16, maxr = 16, maxp = 16;
+    DBuf<int> nnum, nbr, flag, rnum, rev, pnum, ptag;
+    DBuf<double> hist, phist;
+    DBuf<int> gsrc;
+    DBuf<dbl4> gshift;
+    // bins
+    double bboxlo[3], bboxhi[3], bininv[3], binsize[3];
+    int nbin[3], mbinlo[3], mbin[3], mbins = 0;
+    std::vector<int> h_stencil;
+    DBuf<int> stencil, bin_start, bin_atoms, counts, vals, vals2, sel, nsel;
+    DBuf<unsigned> keys, keys2;
+    DBuf<uint8_t> bflags;
+    DBuf<char> cubtmp;
+    DBuf<int> dstatus, ddflag;
+    int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel
+    // neighbor
+    double cutneighmax = 0, triggersq = 0;
+    int ago = 0, nbuilds = 0;
+    long ntimestep = 0, nextsort = 0;
+    int snb[3] = {1, 1, 1};
+    double sinv[3] = {0, 0, 0}, slo[3] = {0, 0, 0};
+    // fixes
+    int nfix = 0;
+    HostFix fix[kMaxFix];
+    // stats
+    long npairs_last = 0;
+    long launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int set_err(gb2_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                                  \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) return set_err(c, GB2_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                                              __FILE__, __LINE__);                                                \
+    } while (0)
+
+#define CKL()                                                                                                     \
+    do {                                                                                                          \
+        c->launches++;                                                                                            \
+        cudaError_t e_ = cudaGetLastError();                                                                      \
+        if (e_ != cudaSuccess)                                                                                    \
+            return set_err(c, GB2_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__,       \
+                           __LINE__);                                                                             \
+    } while (0)
+
+Dev make_dev(gb2_ctx *c)
+{
+    Dev D;
+    std::memset(&D, 0, sizeof D);
+    D.nlocal = c->nlocal;
+    D.nghost = c->nghost;
+    D.nmax = c->nmax;
+    D.cap = c->cap;
+    D.pos = c->pos.p;
+    D.vel = c->vel.p;
+    D.omg = c->omg.p;
+    D.vel_out = c->vel2.p;
+    D.omg_out = c->omg2.p;
+    D.type = c->type.p;
+    D.tag = c->tag.p;
+    D.f = c->f.p;
+    D.tq = c->tq.p;
+    D.fpart = c->fpart.p;
+    D.tpart = c->tpart.p;
+    D.xhold = c->xhold.p;
+    D.maxn = c->maxn;
+    D.nnum = c->nnum.p;
+    D.nbr = c->nbr.p;
+    D.flag = c->flag.p;
+    D.hist = c->hist.p;
+    D.maxr = c->maxr;
+    D.rnum = c->rnum.p;
+    D.rev = c->rev.p;
+    D.maxp = c->maxp;
+    D.pnum = c->pnum.p;
+    D.ptag = c->ptag.p;
+    D.phist = c->phist.p;
+    D.gsrc = c->gsrc.p;
+    D.gshift = c->gshift.p;
+    for (int d = 0; d < 3; d++) {
+        D.bboxlo[d] = c->bboxlo[d];
+        D.bboxhi[d] = c->bboxhi[d];
+        D.bininv[d] = c->bininv[d];
+        D.binsize[d] = c->binsize[d];
+        D.nbin[d] = c->nbin[d];
+        D.mbinlo[d] = c->mbinlo[d];
+        D.mbin[d] = c->mbin[d];
+    }
+    D.mbins = c->mbins;
+    D.nstencil = (int)c->h_stencil.size();
+    D.stencil = c->stencil.p;
+    D.bin_start = c->bin_start.p;
+    D.bin_atoms = c->bin_atoms.p;
+    D.mat = c->dmat.p;
+    D.ntypes = c->P.ntypes;
+    D.dt = c->P.dt;
+    D.skin = c->P.skin;
+    D.cutneighmax = c->cutneighmax;
+    D.triggersq = c->triggersq;
+    D.rolling = c->P.rolling_cdt;
+    D.tdamp = c->P.tangential_damping;
+    D.nfix = c->nfix;
+    for (int k = 0; k < c->nfix; k++) {
+        const HostFix &H = c->fix[k];
+        FixDev &F = D.fix[k];
+        F.kind = H.kind;
+        for (int q = 0; q < 3; q++) F.acc[q] = H.acc[q];
+        F.dim = H.dim;
+        F.pos = H.pos;
+        F.wtype = H.wtype;
+        F.rolling = H.rolling;
+        F.inlist = H.inlist.p;
+        F.whist = H.whist.p;
+        if (H.mesh) {
+            MeshFix &M = *H.mesh;
+            MeshDev &m = F.mesh;
+            m.ntri = (int)M.topo.tri.size();
+            m.tri = M.tri.p;
+            m.cnn_start = M.cnn_start.p;
+            m.cnn_list = M.cnn_list.p;
+            m.bin_tri_start = M.bin_tri_start.p;
+            m.bin_tri_list = M.bin_tri_list.p;
+            m.nl_skin = M.nl_skin;
+            m.wtype = H.wtype;
+            m.rolling = H.rolling;
+            m.maxt = M.maxt;
+            m.tcnt = M.tcnt.p;
+            m.tlist = M.tlist.p;
+            m.snp = M.snp.p;
+            m.spartner = M.spartner.p;
+            m.shist = M.shist.p;
+        }
+    }
+    D.status = c->dstatus.p;
+    D.dflag = c->ddflag.p;
+    return D;
+}
+
+int read_status(gb2_ctx *c, int *st)
+{
+    CK(cudaMemcpyAsync(&c->h_pinned[0], c->dstatus.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *st = c->h_pinned[0];
+    return 0;
+}
+
+int clear_status(gb2_ctx *c)
+{
+    CK(cudaMemsetAsync(c->dstatus.p, 0, sizeof(int), c->st));
+    return 0;
+}
+
+int cub_tmp(gb2_ctx *c, size_t bytes)
+{
+    if (bytes > c->cubtmp.n) CK(c->cubtmp.alloc(bytes + bytes / 4 + 1024));
+    return 0;
+}
+
+// ---------------------------------------------------------------- capacity
+
+int ensure_nmax(gb2_ctx *c, int need)
+{
+    if (need <= c->nmax) return 0;
+    const int nm = std::max(need + need / 4, c->nmax + 1024);
+    const size_t keep = (size_t)(c->nlocal + c->nghost);
+    CK(c->pos.grow_keep(nm, keep, c->st));
+    CK(c->vel.grow_keep(nm, keep, c->st));
+    CK(c->omg.grow_keep(nm, keep, c->st));
+    CK(c->vel2.grow_keep(nm, 0, c->st));
+    CK(c->omg2.grow_keep(nm, 0, c->st));
+    CK(c->type.grow_keep(nm, keep, c->st));
+    CK(c->tag.grow_keep(nm, keep, c->st));
+    CK(c->gsrc.grow_keep(nm, (size_t)c->nghost, c->st));
+    CK(c->gshift.grow_keep(nm, (size_t)c->nghost, c->st));
+    c->nmax = nm;
+    return 0;
+}
+
+// ---------------------------------------------------------------- neighbor
+
+void neighbor_init(gb2_ctx *c)
+{
+    // Neighbor::init cutoffs (src/neighbor.cpp:292-332) with
+    // PairGran::init_one (src/pair_gran.cpp:623): cut = maxrad_i + maxrad_j
+    const int nt = c->P.ntypes;
+    std::vector<double> maxrad(nt + 1, 0.0);
+    for (int i = 0; i < c->nlocal; i++) maxrad[c->h_type[i]] = std::max(maxrad[c->h_type[i]], c->h_radius[i]);
+    c->triggersq = 0.25 * c->P.skin * c->P.skin;
+    c->cutneighmax = 0.0;
+    for (int i = 1; i <= nt; i++)
+        for (int j = 1; j <= nt; j++) {
+            const double cut = (maxrad[i] + maxrad[j]) * 1.0;
+            const double cutoff = std::sqrt(cut * cut);
+            const double c2 = cutoff + (cutoff > 0.0 ? c->P.skin : 0.0);
+            c->cutneighmax = std::max(c->cutneighmax, c2);
+        }
+}
+
+int setup_bins(gb2_ctx *c)
+{
+    // Neighbor::setup_bins (src/neighbor.cpp:1642-1808), orthogonal box, one proc
+    const double SMALL = 1.0e-6;
+    const double cutghost = c->cutneighmax;
+    double bbox[3], bsublo[3], bsubhi[3];
+    for (int d = 0; d < 3; d++) {
+        c->bboxlo[d] = c->P.boxlo[d];
+        c->bboxhi[d] = c->P.boxhi[d];
+        bsublo[d] = c->P.boxlo[d] - cutghost;
+        bsubhi[d] = c->P.boxhi[d] + cutghost;
+        bbox[d] = c->bboxhi[d] - c->bboxlo[d];
+    }
+    double binsize_optimal = 0.5 * c->cutneighmax;
+    if (binsize_optimal == 0.0) binsize_optimal = bbox[0];
+    const double binsizeinv = 1.0 / binsize_optimal;
+    for (int d = 0; d < 3; d++) {
+        c->nbin[d] = static_cast<int>(bbox[d] * binsizeinv);
+        if (c->nbin[d] == 0) c->nbin[d] = 1;
+        c->binsize[d] = bbox[d] / c->nbin[d];
+        c->bininv[d] = 1.0 / c->binsize[d];
+        if (binsize_optimal * c->bininv[d] > 100)
+            return set_err(c, GB2_ERR_ARG, "Cannot use neighbor bins - box size << cutoff");
+    }
+    for (int d = 0; d < 3; d++) {
+        double coord = bsublo[d] - SMALL * bbox[d];
+        int lo = static_cast<int>((coord - c->bboxlo[d]) * c->bininv[d]);
+        if (coord < c->bboxlo[d]) lo = lo - 1;
+        coord = bsubhi[d] + SMALL * bbox[d];
+        int hi = static_cast<int>((coord - c->bboxlo[d]) * c->bininv[d]);
+        lo -= 1;
+        hi += 1;
+        c->mbinlo[d] = lo;
+        c->mbin[d] = hi - lo + 1;
+    }
+    const long mb = (long)c->mbin[0] * c->mbin[1] * c->mbin[2];
+    if (mb > (1l << 30)) return set_err(c, GB2_ERR_CAPACITY, "Too many neighbor bins");
+    c->mbins = (int)mb;
+    int s[3];
+    for (int d = 0; d < 3; d++) {
+        s[d] = static_cast<int>(c->cutneighmax * c->bininv[d]);
+        if (s[d] * c->binsize[d] < c->cutneighmax) s[d]++;
+    }
+    const double cutsq = c->cutneighmax * c->cutneighmax;
+    auto bin_distance = [&](int i, int j, int k) {
+        double dx, dy, dz;
+        if (i > 0) dx = (i - 1) * c->binsize[0];
+        else if (i == 0) dx = 0.0;
+        else dx = (i + 1) * c->binsize[0];
+        if (j > 0) dy = (j - 1) * c->binsize[1];
+        else if (j == 0) dy = 0.0;
+        else dy = (j + 1) * c->binsize[1];
+        if (k > 0) dz = (k - 1) * c->binsize[2];
+        else if (k == 0) dz = 0.0;
+        else dz = (k + 1) * c->binsize[2];
+        return dx * dx + dy * dy + dz * dz;
+    };
+    c->h_stencil.clear();
+    for (int k = -s[2]; k <= s[2]; k++)
+        for (int j = -s[1]; j <= s[1]; j++)
+            for (int i = -s[0]; i <= s[0]; i++)
+                if (bin_distance(i, j, k) < cutsq) c->h_stencil.push_back(k * c->mbin[1] * c->mbin[0] + j * c->mbin[0] + i);
+    CK(c->stencil.alloc(c->h_stencil.size()));
+    CK(cudaMemcpyAsync(c->stencil.p, c->h_stencil.data(), c->h_stencil.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       c->st));
+    CK(c->bin_start.alloc((size_t)c->mbins + 1));
+    CK(c->counts.alloc((size_t)c->mbins + 1));
+    for (int k = 0; k < c->nfix; k++)
+        if (c->fix[k].mesh) c->fix[k].mesh->bins_valid = false;
+    return 0;
+}
+
+int coord2bin3_host(const gb2_ctx *c, const double *x, int *idx)
+{
+    for (int d = 0; d < 3; d++) {
+        int v;
+        if (x[d] >= c->bboxhi[d])
+            v = static_cast<int>((x[d] - c->bboxhi[d]) * c->bininv[d]) + c->nbin[d];
+        else if (x[d] >= c->bboxlo[d]) {
+            v = static_cast<int>((x[d] - c->bboxlo[d]) * c->bininv[d]);
+            v = std::min(v, c->nbin[d] - 1);
+        } else
+            v = static_cast<int>((x[d] - c->bboxlo[d]) * c->bininv[d]) - 1;
+        idx[d] = v - c->mbinlo[d];
+    }
+    return idx[2] * c->mbin[1] * c->mbin[0] + idx[1] * c->mbin[0] + idx[0];
+}
+
+// FixNeighlistMesh::generate_bin_list (src/fix_neighlist_mesh.cpp:456) for a
+// static mesh, inverted into bin -> ascending triangle list
+int mesh_bins(gb2_ctx *c, MeshFix &M)
+{
+    const double skin = 0.5 * c->P.skin;
+    const double rmax = 0.5 * (c->cutneighmax - c->P.skin);
+    const double distmax = c->cutneighmax - rmax + skin / (70. * M_PI);
+    M.nl_skin = skin;
+    M.distmax = distmax;
+    const double dx = c->binsize[0] / 2.0, dy = c->binsize[1] / 2.0, dz = c->binsize[2] / 2.0;
+    const double maxdiag = std::sqrt(dx * dx + dy * dy + dz * dz);
+    const int n = (int)M.topo.tri.size();
+    std::vector<int> cnt((size_t)c->mbins + 1, 0);
+    std::vector<std::pair<int, int>> entries;   // (bin, tri)
+    for (int t = 0; t < n; t++) {
+        const TriGeom &T = M.topo.tri[t];
+        double blo[3], bhi[3];
+        for (int d = 0; d < 3; d++) {
+            blo[d] = 1e300;
+            bhi[d] = -1e300;
+        }
+        for (int k = 0; k < 3; k++)
+            for (int d = 0; d < 3; d++) {
+                blo[d] = std::min(blo[d], T.node[k][d]);
+                bhi[d] = std::max(bhi[d], T.node[k][d]);
+            }
+        for (int d = 0; d < 3; d++) {   // BoundingBox::shrinkToSubbox
+            if (blo[d] < c->P.boxlo[d]) blo[d] = c->P.boxlo[d];
+            if (bhi[d] > c->P.boxhi[d]) bhi[d] = c->P.boxhi[d];
+        }
+        double tmin[3] = {blo[0] - distmax, blo[1] - distmax, blo[2] - distmax};
+        double tmax[3] = {bhi[0] + distmax, bhi[1] + distmax, bhi[2] + distmax};
+        int lo[3], hi[3];
+        coord2bin3_host(c, tmin, lo);
+        coord2bin3_host(c, tmax, hi);
+        for (int ix = lo[0]; ix <= hi[0]; ix++)
+            for (int iy = lo[1]; iy <= hi[1]; iy++)
+                for (int iz = lo[2]; iz <= hi[2]; iz++) {
+                    const int b = iz * c->mbin[1] * c->mbin[0] + iy * c->mbin[0] + ix;
+                    if (b < 0 || b >= c->mbins) continue;
+                    double center[3];
+                    center[0] = (c->mbinlo[0] + ix + 0.5) * c->binsize[0] + c->bboxlo[0];
+                    center[1] = (c->mbinlo[1] + iy + 0.5) * c->binsize[1] + c->bboxlo[1];
+                    center[2] = (c->mbinlo[2] + iz + 0.5) * c->binsize[2] + c->bboxlo[2];
+                    if (tri_neighbuild_host(T, maxdiag, center, distmax + skin)) {
+                        entries.emplace_back(b, t);
+                        cnt[b]++;
+                    }
+                }
+    }
+    std::vector<int> start((size_t)c->mbins + 1, 0);
+    for (int b = 0; b < c->mbins; b++) start[b + 1] = start[b] + cnt[b];
+    std::vector<int> list(entries.size());
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (auto &e : entries) list[fill[e.first]++] = e.second;   // triangles visited in ascending order
+    CK(M.bin_tri_start.alloc(start.size()));
+    CK(M.bin_tri_list.alloc(std::max<size_t>(list.size(), 1)));
+    CK(cudaMemcpyAsync(M.bin_tri_start.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    if (!list.empty())
+        CK(cudaMemcpyAsync(M.bin_tri_list.p, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    M.bins_valid = true;
+    return 0;
+}
+
+// ---------------------------------------------------------------- rebuild parts
+
+int do_partners(gb2_ctx *c)
+{
+    for (int attempt = 0; attempt < 8; attempt++) {
+        if (clear_status(c)) return GB2_ERR_CUDA;
+        Dev D = make_dev(c);
+        k_partners<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D);
+        CKL();
+        int st;
+        if (read_status(c, &st)) return GB2_ERR_CUDA;
+        if (!(st & ST_PARTNER_OVERFLOW)) return 0;
+        c->maxp *= 2;
+        CK(c->ptag.alloc((size_t)c->maxp * c->cap));
+        CK(c->phist.alloc((size_t)3 * c->maxp * c->cap));
+    }
+    return set_err(c, GB2_ERR_CAPACITY, "contact history partner capacity could not be grown");
+}
+
+int do_atom_sort(gb2_ctx *c)
+{
+    // Atom::sort (src/atom.cpp:1309): stable order by spatial sort bin
+    c->nextsort = (c->ntimestep / c->P.sort_freq) * c->P.sort_freq + c->P.sort_freq;
+    if ((long)c->snb[0] * c->snb[1] * c->snb[2] == 1) return 0;
+    const int n = c->nlocal;
+    Dev D = make_dev(c);
+    CK(c->keys.alloc(std::max(c->nmax, 1)));
+    CK(c->keys2.alloc(std::max(c->nmax, 1)));
+    CK(c->vals.alloc(std::max(c->nmax, 1)));
+    CK(c->vals2.alloc(std::max(c->nmax, 1)));
+    k_sort_keys<<<nblk(n), kBlock, 0, c->st>>>(D, c->slo[0], c->slo[1], c->slo[2], c->sinv[0], c->sinv[1], c->sinv[2],
+                                                c->snb[0], c->snb[1], c->snb[2], c->keys.p, c->vals.p);
+    CKL();
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, c->keys.p, c->keys2.p, c->vals.p, c->vals2.p, n, 0, 32, c->st);
+    if (cub_tmp(c, bytes)) return GB2_ERR_CUDA;
+    bytes = c->cubtmp.n;
+    CK(cub::DeviceRadixSort::SortPairs(c->cubtmp.p, bytes, c->keys.p, c->keys2.p, c->vals.p, c->vals2.p, n, 0, 32,
+                                       c->st));
+    const int *perm = c->vals2.p;
+    // every per-atom array moves with its atom
+    {
+        DBuf<dbl4> tmp;
+        CK(tmp.alloc(c->nmax));
+        DBuf<dbl4> *arrs[] = {&c->pos, &c->vel, &c->omg};
+        for (auto *a : arrs) {
+            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a->p, tmp.p, perm, n);
+            CKL();
+            CK(cudaMemcpyAsync(a->p, tmp.p, sizeof(dbl4) * n, cudaMemcpyDeviceToDevice, c->st));
+        }
+        DBuf<int> itmp;
+        CK(itmp.alloc(std::max(c->nmax, c->cap * std::max(c->maxp, 1))));
+        DBuf<int> *iarrs[] = {&c->type, &c->tag, &c->pnum};
+        for (auto *a : iarrs) {
+            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a->p, itmp.p, perm, n);
+            CKL();
+            CK(cudaMemcpyAsync(a->p, itmp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, c->st));
+        }
+        auto gather_slots_i = [&](DBuf<int> &a, int nslot) -> int {
+            if (nslot <= 0) return 0;
+            DBuf<int> t2;
+            CK(t2.alloc((size_t)nslot * c->cap));
+            dim3 g(nblk(n), nslot);
+            k_gather_slots<<<g, kBlock, 0, c->st>>>(a.p, t2.p, perm, n, c->cap, nslot);
+            CKL();
+            a.swap(t2);
+            CK(cudaStreamSynchronize(c->st));
+            return 0;
+        };
+        auto gather_slots_d = [&](DBuf<double> &a, int nslot) -> int {
+            if (nslot <= 0) return 0;
+            DBuf<double> t2;
+            CK(t2.alloc((size_t)nslot * c->cap));
+            dim3 g(nblk(n), nslot);
+            k_gather_slots<<<g, kBlock, 0, c->st>>>(a.p, t2.p, perm, n, c->cap, nslot);
+            CKL();
+            a.swap(t2);
+            CK(cudaStreamSynchronize(c->st));
+            return 0;
+        };
+        if (gather_slots_i(c->ptag, c->maxp)) return GB2_ERR_CUDA;
+        if (gather_slots_d(c->phist, 3 * c->maxp)) return GB2_ERR_CUDA;
+        for (int k = 0; k < c->nfix; k++) {
+            HostFix &H = c->fix[k];
+            if (H.kind == FIX_WALL_PLANE)
+                if (gather_slots_d(H.whist, 3)) return GB2_ERR_CUDA;
+            if (H.mesh) {
+                MeshFix &M = *H.mesh;
+                if (gather_slots_i(M.tcnt, 1)) return GB2_ERR_CUDA;
+                if (gather_slots_i(M.snp, 1)) return GB2_ERR_CUDA;
+                if (gather_slots_i(M.spartner, M.maxt)) return GB2_ERR_CUDA;
+                if (gather_slots_d(M.shist, 3 * M.maxt)) return GB2_ERR_CUDA;
+            }
+        }
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return 0;
+}
+
+int do_borders(gb2_ctx *c)
+{
+    // Comm::borders (src/comm.cpp:1028) with the granular slab widths of
+    // Comm::setup (src/comm.cpp:670-695), one proc, periodic dims only
+    c->nghost = 0;
+    const double cg = c->cutneighmax / 2. + c->P.skin / 2.;
+    for (int dim = 0; dim < 3; dim++) {
+        if (!c->P.periodic[dim]) continue;
+        const int nlast = c->nlocal + c->nghost;   // both swaps of a dim scan the same range
+        for (int ineed = 0; ineed < 2; ineed++) {
+            const bool low = (ineed % 2 == 0);
+            const double prd = c->P.boxhi[dim] - c->P.boxlo[dim];
+            const double bound = low ? c->P.boxlo[dim] + cg : c->P.boxhi[dim] - cg;
+            const double shift = low ? 1 * prd : -1 * prd;
+            CK(c->bflags.alloc(std::max(nlast, 1)));
+            CK(c->sel.alloc(std::max(nlast, 1)));
+            CK(c->nsel.alloc(1));
+            Dev D = make_dev(c);
+            k_border_flags<<<nblk(nlast), kBlock, 0, c->st>>>(D, nlast, dim, low ? 1 : 0, bound, c->bflags.p);
+            CKL();
+            size_t bytes = 0;
+            thrust::counting_iterator<int> it(0);
+            cub::DeviceSelect::Flagged(nullptr, bytes, it, c->bflags.p, c->sel.p, c->nsel.p, nlast, c->st);
+            if (cub_tmp(c, bytes)) return GB2_ERR_CUDA;
+            bytes = c->cubtmp.n;
+            CK(cub::DeviceSelect::Flagged(c->cubtmp.p, bytes, it, c->bflags.p, c->sel.p, c->nsel.p, nlast, c->st));
+            CK(cudaMemcpyAsync(&c->h_pinned[2], c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            const int ns = c->h_pinned[2];
+            const int first = c->nlocal + c->nghost;
+            if (ensure_nmax(c, first + ns)) return GB2_ERR_CUDA;
+            D = make_dev(c);
+            if (ns > 0) {
+                k_border_fill<<<nblk(ns), kBlock, 0, c->st>>>(D, c->sel.p, ns, first, dim, shift);
+                CKL();
+            }
+            c->nghost += ns;
+        }
+    }
+    return 0;
+}
+
+int do_build(gb2_ctx *c)
+{
+    const int nall = c->nlocal + c->nghost;
+    CK(c->keys.alloc(std::max(c->nmax, 1)));
+    CK(c->keys2.alloc(std::max(c->nmax, 1)));
+    CK(c->vals.alloc(std::max(c->nmax, 1)));
+    CK(c->bin_atoms.alloc(std::max(c->nmax, 1)));
+    CK(cudaMemsetAsync(c->counts.p, 0, sizeof(int) * ((size_t)c->mbins + 1), c->st));
+    if (clear_status(c)) return GB2_ERR_CUDA;
+    Dev D = make_dev(c);
+    k_bin_keys<<<nblk(nall), kBlock, 0, c->st>>>(D, nall, c->keys.p, c->vals.p, c->counts.p);
+    CKL();
+    size_t bytes = 0, b2 = 0;
+    int endbit = 1;
+    while ((1l << endbit) < (long)c->mbins + 1) endbit++;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, c->keys.p, c->keys2.p, c->vals.p, c->bin_atoms.p, nall, 0, endbit,
+                                    c->st);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, c->counts.p, c->bin_start.p, c->mbins + 1, c->st);
+    if (cub_tmp(c, std::max(bytes, b2))) return GB2_ERR_CUDA;
+    bytes = c->cubtmp.n;
+    CK(cub::DeviceRadixSort::SortPairs(c->cubtmp.p, bytes, c->keys.p, c->keys2.p, c->vals.p, c->bin_atoms.p, nall, 0,
+                                       endbit, c->st));
+    bytes = c->cubtmp.n;
+    CK(cub::DeviceScan::ExclusiveSum(c->cubtmp.p, bytes, c->counts.p, c->bin_start.p, c->mbins + 1, c->st));
+    for (int attempt = 0; attempt < 8; attempt++) {
+        if (clear_status(c)) return GB2_ERR_CUDA;
+        D = make_dev(c);
+        k_build_list<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D);
+        CKL();
+        int st;
+        if (read_status(c, &st)) return GB2_ERR_CUDA;
+        if (st & ST_LOST_ATOM) return set_err(c, GB2_ERR_LOST, "an atom is outside the binned domain");
+        if (!(st & ST_NEIGH_OVERFLOW)) break;
+        c->maxn *= 2;
+        CK(c->nbr.alloc((size_t)c->maxn * c->cap));
+        CK(c->flag.alloc((size_t)c->maxn * c->cap));
+        CK(c->hist.alloc((size_t)3 * c->maxn * c->cap));
+        if (attempt == 7) return set_err(c, GB2_ERR_CAPACITY, "neighbor list capacity could not be grown");
+    }
+    for (int attempt = 0; attempt < 8; attempt++) {
+        if (clear_status(c)) return GB2_ERR_CUDA;
+        CK(cudaMemsetAsync(c->rnum.p, 0, sizeof(int) * c->cap, c->st));
+        D = make_dev(c);
+        k_rev_fill<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D);
+        CKL();
+        int st;
+        if (read_status(c, &st)) return GB2_ERR_CUDA;
+        if (!(st & ST_REV_OVERFLOW)) break;
+        c->maxr *= 2;
+        CK(c->rev.alloc((size_t)c->maxr * c->cap));
+        if (attempt == 7) return set_err(c, GB2_ERR_CAPACITY, "reverse list capacity could not be grown");
+    }
+    D = make_dev(c);
+    k_rev_sort<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D);
+    CKL();
+    c->ago = 0;
+    c->nbuilds++;
+    return 0;
+}
+
+int do_pre_force(gb2_ctx *c)
+{
+    // FixWallGran::pre_force, FixNeighlistMesh::pre_force,
+    // FixContactHistoryMesh::pre_force (rebuild steps only)
+    for (int k = 0; k < c->nfix; k++) {
+        HostFix &H = c->fix[k];
+        if (H.kind == FIX_WALL_PLANE) {
+            Dev D = make_dev(c);
+            k_plane_neighlist<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, k);
+            CKL();
+        } else if (H.kind == FIX_WALL_MESH) {
+            MeshFix &M = *H.mesh;
+            if (!M.bins_valid)
+                if (mesh_bins(c, M)) return GB2_ERR_CUDA;
+            // candidates into fresh buffers (old slots are still needed)
+            const int old_maxt = M.maxt;
+            DBuf<int> old_tcnt;
+            old_tcnt.swap(M.tcnt);
+            CK(M.tcnt.alloc(c->cap));
+            for (int attempt = 0; attempt < 8; attempt++) {
+                CK(M.tlist.alloc((size_t)M.maxt * c->cap));
+                if (clear_status(c)) return GB2_ERR_CUDA;
+                Dev D = make_dev(c);
+                k_mesh_candidates<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, k);
+                CKL();
+                int st;
+                if (read_status(c, &st)) return GB2_ERR_CUDA;
+                if (!(st & ST_MESHSLOT_OVERFLOW)) break;
+                M.maxt *= 2;
+                if (M.maxt > 64) return set_err(c, GB2_ERR_CAPACITY, "more than 64 candidate triangles per atom");
+                M.tlist.release();
+            }
+            // re-page history into buffers sized for the new capacity
+            CK(M.snp2.alloc(c->cap));
+            CK(M.spartner2.alloc((size_t)M.maxt * c->cap));
+            CK(M.shist2.alloc((size_t)3 * M.maxt * c->cap));
+            M.snp.swap(M.snp2);
+            M.spartner.swap(M.spartner2);
+            M.shist.swap(M.shist2);
+            if (clear_status(c)) return GB2_ERR_CUDA;
+            Dev D = make_dev(c);
+            // old slots now live in *2 buffers
+            k_mesh_repage<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, k, M.snp2.p, M.spartner2.p, M.shist2.p, old_maxt);
+            CKL();
+            int st;
+            if (read_status(c, &st)) return GB2_ERR_CUDA;
+            if (st & ST_MESH_INTERNAL) return set_err(c, GB2_ERR_STATE, "mesh contact history inconsistent");
+            (void)old_tcnt;
+        }
+    }
+    return 0;
+}
+
+int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
+{
+    if (pre_exchange)
+        if (do_partners(c)) return GB2_ERR_CUDA;
+    Dev D = make_dev(c);
+    for (int k = 0; k < c->nfix; k++)
+        if (c->fix[k].kind == FIX_WALL_MESH) {
+            k_mesh_sort_contacts<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, k);
+            CKL();
+        }
+    if (clear_status(c)) return GB2_ERR_CUDA;
+    k_pbc<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, c->P.boxlo[0], c->P.boxlo[1], c->P.boxlo[2], c->P.boxhi[0],
+                                                  c->P.boxhi[1], c->P.boxhi[2], c->P.periodic[0], c->P.periodic[1],
+                                                  c->P.periodic[2]);
+    CKL();
+    int st;
+    if (read_status(c, &st)) return GB2_ERR_CUDA;
+    if (st & ST_LOST_ATOM) return set_err(c, GB2_ERR_LOST, "atom left the non-periodic box (lost atoms unsupported)");
+    if (sort_now)
+        if (do_atom_sort(c)) return GB2_ERR_CUDA;
+    if (do_borders(c)) return GB2_ERR_CUDA;
+    if (do_build(c)) return c->err.empty() ? GB2_ERR_CUDA : GB2_ERR_CAPACITY;
+    if (do_pre_force(c)) return GB2_ERR_CUDA;
+    return 0;
+}
+
+int do_force(gb2_ctx *c, int shearupdate, int integrate)
+{
+    Dev D = make_dev(c);
+    if (c->P.rolling_cdt)
+        k_pair_reverse<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
+    else
+        k_pair_reverse<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
+    CKL();
+    if (c->P.rolling_cdt)
+        k_pair_main<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
+    else
+        k_pair_main<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
+    CKL();
+    if (integrate) {
+        c->vel.swap(c->vel2);
+        c->omg.swap(c->omg2);
+    }
+    return 0;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+const char *gb2_version(void) { return "granb200 0.1 sm_100a"; }
+
+int gb2_create(const gb2_params *p, gb2_ctx **out)
+{
+    if (!p || !out) return GB2_ERR_ARG;
+    *out = nullptr;
+    if (p->ntypes < 1 || p->ntypes > kMaxTypes) return GB2_ERR_ARG;
+    if (p->dt <= 0 || p->skin < 0) return GB2_ERR_ARG;
+    if (p->precision != GB2_PREC_FP64) return GB2_ERR_UNSUPPORTED;
+    gb2_ctx *c = new gb2_ctx();
+    c->P = *p;
+    if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) {
+        delete c;
+        return GB2_ERR_CUDA;
+    }
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&c->h_pinned, 4 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
+        c->ddflag.alloc(1) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
+        cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return GB2_ERR_CUDA;
+    }
+    *out = c;
+    return 0;
+}
+
+int gb2_destroy(gb2_ctx *c)
+{
+    if (!c) return 0;
+    cudaStreamSynchronize(c->st);
+    for (int k = 0; k < c->nfix; k++) delete c->fix[k].mesh;
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    cudaStream_t st = c->st;
+    delete c;
+    if (st) cudaStreamDestroy(st);
+    return 0;
+}
+
+int gb2_set_materials(gb2_ctx *c, const double *youngs, const double *poisson, const double *restitution,
+                      const double *friction, const double *rollfriction)
+{
+    if (!c || !youngs || !poisson || !restitution || !friction) return GB2_ERR_ARG;
+    const int nt = c->P.ntypes;
+    std::memset(c->hmat, 0, sizeof c->hmat);
+    for (int i = 1; i <= nt; i++)
+        for (int j = 1; j <= nt; j++) {
+            const double Yi = youngs[i - 1], Yj = youngs[j - 1];
+            const double vi = poisson[i - 1], vj = poisson[j - 1];
+            if (vi < 0. || vi > 0.5 || vj < 0. || vj > 0.5)
+                return set_err(c, GB2_ERR_ARG, "0 <= poissonsRatio <= 0.5 required");
+            const double cor = restitution[(i - 1) * nt + (j - 1)];
+            if (cor <= 0.05 || cor > 1) return set_err(c, GB2_ERR_ARG, "0.05 < coefficientRestitution <= 1 required");
+            MatPair &m = c->hmat[i * (kMaxTypes + 1) + j];
+            // src/global_properties.cpp:432, :461, :508, :540
+            m.Yeff = 1. / ((1. - std::pow(vi, 2.)) / Yi + (1. - std::pow(vj, 2.)) / Yj);
+            m.Geff = 1. / (2. * (2. - vi) * (1. + vi) / Yi + 2. * (2. - vj) * (1. + vj) / Yj);
+            const double lg = std::log(cor);
+            m.betaeff = lg / std::sqrt(std::pow(lg, 2.) + std::pow(M_PI, 2.));
+            m.mu = friction[(i - 1) * nt + (j - 1)];
+            m.mur = rollfriction ? rollfriction[(i - 1) * nt + (j - 1)] : 0.0;
+        }
+    if (c->dmat.alloc((kMaxTypes + 1) * (kMaxTypes + 1))) return set_err(c, GB2_ERR_CUDA, "alloc");
+    CK(cudaMemcpyAsync(c->dmat.p, c->hmat, sizeof c->hmat, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->have_mat = true;
+    return 0;
+}
+
+int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const double *omega, const double *radius,
+                     const double *rmass, const int *type, const int *tag)
+{
+    if (!c || n <= 0 || !x || !v || !omega || !radius || !rmass || !type || !tag) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "atoms must be uploaded before setup");
+    for (int i = 0; i < n; i++) {
+        if (type[i] < 1 || type[i] > c->P.ntypes) return set_err(c, GB2_ERR_ARG, "atom type out of range");
+        if (!(radius[i] > 0.0)) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
+        if (!(rmass[i] > 0.0)) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
+        for (int d = 0; d < 3; d++)
+            if (!std::isfinite(x[3 * i + d]) || !std::isfinite(v[3 * i + d]) || !std::isfinite(omega[3 * i + d]))
+                return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", i);
+    }
+    c->nlocal = n;
+    c->cap = (n + 31) / 32 * 32;
+    c->nmax = 0;
+    c->nghost = 0;
+    if (ensure_nmax(c, n + n / 4 + 1024)) return GB2_ERR_CUDA;
+    std::vector<dbl4> hp(n), hv(n), hw(n);
+    c->h_radius.assign(radius, radius + n);
+    c->h_type.assign(type, type + n);
+    for (int i = 0; i < n; i++) {
+        hp[i] = {x[3 * i], x[3 * i + 1], x[3 * i + 2], radius[i]};
+        hv[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2], rmass[i]};
+        hw[i] = {omega[3 * i], omega[3 * i + 1], omega[3 * i + 2], 0.0};
+    }
+    CK(cudaMemcpyAsync(c->pos.p, hp.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->vel.p, hv.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->omg.p, hw.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->type.p, type, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->tag.p, tag, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    const size_t cap = c->cap;
+    CK(c->f.alloc(cap));
+    CK(c->tq.alloc(cap));
+    CK(c->fpart.alloc(cap));
+    CK(c->tpart.alloc(cap));
+    CK(c->xhold.alloc(cap));
+    CK(c->nnum.alloc(cap));
+    CK(c->rnum.alloc(cap));
+    CK(c->pnum.alloc(cap));
+    CK(c->nbr.alloc((size_t)c->maxn * cap));
+    CK(c->flag.alloc((size_t)c->maxn * cap));
+    CK(c->hist.alloc((size_t)3 * c->maxn * cap));
+    CK(c->rev.alloc((size_t)c->maxr * cap));
+    CK(c->ptag.alloc((size_t)c->maxp * cap));
+    CK(c->phist.alloc((size_t)3 * c->maxp * cap));
+    CK(cudaMemsetAsync(c->f.p, 0, sizeof(dbl4) * cap, c->st));
+    CK(cudaMemsetAsync(c->tq.p, 0, sizeof(dbl4) * cap, c->st));
+    CK(cudaMemsetAsync(c->nnum.p, 0, sizeof(int) * cap, c->st));
+    CK(cudaMemsetAsync(c->rnum.p, 0, sizeof(int) * cap, c->st));
+    CK(cudaMemsetAsync(c->pnum.p, 0, sizeof(int) * cap, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->have_atoms = true;
+    return 0;
+}
+
+static int add_fix_common(gb2_ctx *c)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (c->nfix >= kMaxFix) return set_err(c, GB2_ERR_CAPACITY, "too many fixes");
+    if (!c->have_atoms) return set_err(c, GB2_ERR_STATE, "upload atoms before adding fixes");
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fixes must be added before setup");
+    return 0;
+}
+
+int gb2_add_gravity(gb2_ctx *c, double magnitude, const double dir[3])
+{
+    int rc = add_fix_common(c);
+    if (rc) return rc;
+    // FixGravity::set_acceleration, style vector (src/fix_gravity.cpp:376-397)
+    const double length = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    if (length == 0.) return set_err(c, GB2_ERR_ARG, "Gravity direction vector = 0");
+    HostFix &H = c->fix[c->nfix];
+    H.kind = FIX_GRAVITY;
+    H.acc[0] = magnitude * (dir[0] / length);
+    H.acc[1] = magnitude * (dir[1] / length);
+    H.acc[2] = magnitude * (dir[2] / length);
+    return c->nfix++;
+}
+
+int gb2_add_wall_plane(gb2_ctx *c, int dim, double pos, int wall_type, int rolling_cdt)
+{
+    int rc = add_fix_common(c);
+    if (rc) return rc;
+    if (dim < 0 || dim > 2) return set_err(c, GB2_ERR_ARG, "plane dimension must be 0, 1 or 2");
+    if (wall_type < 1 || wall_type > c->P.ntypes) return set_err(c, GB2_ERR_ARG, "wall type out of range");
+    HostFix &H = c->fix[c->nfix];
+    H.kind = FIX_WALL_PLANE;
+    H.dim = dim;
+    H.pos = pos;
+    H.wtype = wall_type;
+    H.rolling = rolling_cdt;
+    CK(H.inlist.alloc(c->cap));
+    CK(H.whist.alloc((size_t)3 * c->cap));
+    CK(cudaMemsetAsync(H.inlist.p, 0, c->cap, c->st));
+    CK(cudaMemsetAsync(H.whist.p, 0, sizeof(double) * 3 * c->cap, c->st));
+    return c->nfix++;
+}
+
+int gb2_add_wall_mesh(gb2_ctx *c, int ntri, const double *nodes, int wall_type, double curvature, int rolling_cdt)
+{
+    int rc = add_fix_common(c);
+    if (rc) return rc;
+    if (ntri <= 0 || !nodes) return set_err(c, GB2_ERR_ARG, "empty mesh");
+    if (wall_type < 1 || wall_type > c->P.ntypes) return set_err(c, GB2_ERR_ARG, "wall type out of range");
+    for (long q = 0; q < 9l * ntri; q++)
+        if (!std::isfinite(nodes[q])) return set_err(c, GB2_ERR_ARG, "non-finite mesh node");
+    MeshFix *M = new MeshFix();
+    const double curv = curvature > 0 ? curvature : 1. - 0.00001;
+    if (!build_mesh_topology(nodes, ntri, curv, 1e-8, M->topo, c->err)) {
+        delete M;
+        return GB2_ERR_ARG;
+    }
+    const int n = (int)M->topo.tri.size();
+    for (int t = 0; t < n; t++)
+        for (int k = 0; k < 3; k++)
+            for (int d = 0; d < 3; d++)
+                if (M->topo.tri[t].node[k][d] < c->P.boxlo[d] || M->topo.tri[t].node[k][d] >= c->P.boxhi[d]) {
+                    delete M;
+                    return set_err(c, GB2_ERR_UNSUPPORTED, "mesh nodes must lie inside the simulation box");
+                }
+    if (M->tri.alloc(n) || M->cnn_start.alloc(n + 1) || M->cnn_list.alloc(std::max<size_t>(M->topo.cnn_list.size(), 1))) {
+        delete M;
+        return set_err(c, GB2_ERR_CUDA, "mesh alloc");
+    }
+    cudaMemcpyAsync(M->tri.p, M->topo.tri.data(), sizeof(TriGeom) * n, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(M->cnn_start.p, M->topo.cnn_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->st);
+    if (!M->topo.cnn_list.empty())
+        cudaMemcpyAsync(M->cnn_list.p, M->topo.cnn_list.data(), sizeof(int) * M->topo.cnn_list.size(),
+                        cudaMemcpyHostToDevice, c->st);
+    const size_t cap = c->cap;
+    if (M->tcnt.alloc(cap) || M->snp.alloc(cap) || M->spartner.alloc((size_t)M->maxt * cap) ||
+        M->shist.alloc((size_t)3 * M->maxt * cap) || M->tlist.alloc((size_t)M->maxt * cap)) {
+        delete M;
+        return set_err(c, GB2_ERR_CUDA, "mesh alloc");
+    }
+    cudaMemsetAsync(M->tcnt.p, 0, sizeof(int) * cap, c->st);
+    cudaMemsetAsync(M->snp.p, 0, sizeof(int) * cap, c->st);
+    cudaMemsetAsync(M->spartner.p, 0xff, sizeof(int) * M->maxt * cap, c->st);
+    cudaMemsetAsync(M->shist.p, 0, sizeof(double) * 3 * M->maxt * cap, c->st);
+    CK(cudaStreamSynchronize(c->st));
+    HostFix &H = c->fix[c->nfix];
+    H.kind = FIX_WALL_MESH;
+    H.wtype = wall_type;
+    H.rolling = rolling_cdt;
+    H.mesh = M;
+    return c->nfix++;
+}
+
+int gb2_setup(gb2_ctx *c)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->have_mat || !c->have_atoms) return set_err(c, GB2_ERR_STATE, "materials and atoms are required before setup");
+    c->err.clear();
+    neighbor_init(c);
+    if (c->P.sort_freq > 0) {
+        // Atom::setup_sort_bins (src/atom.cpp:1405)
+        const double binsize = c->P.sort_binsize > 0.0 ? c->P.sort_binsize : 0.5 * c->cutneighmax;
+        const double bininv = 1.0 / binsize;
+        for (int d = 0; d < 3; d++) {
+            c->slo[d] = c->P.boxlo[d];
+            c->snb[d] = static_cast<int>((c->P.boxhi[d] - c->P.boxlo[d]) * bininv);
+            if (c->snb[d] == 0) c->snb[d] = 1;
+            c->sinv[d] = c->snb[d] / (c->P.boxhi[d] - c->P.boxlo[d]);
+        }
+    }
+    if (setup_bins(c)) return GB2_ERR_ARG;
+    // Verlet::setup: setup_pre_exchange, pbc, exchange, sort (always), borders,
+    // neighbor build, setup_pre_force, pair (shearupdate 0), fix setup
+    int rc = do_rebuild(c, c->computeflag, c->P.sort_freq > 0);
+    if (rc) return rc;
+    if (do_force(c, 0, 0)) return GB2_ERR_CUDA;
+    CK(cudaStreamSynchronize(c->st));
+    c->setup_done = true;
+    c->computeflag = true;
+    return 0;
+}
+
+int gb2_run(gb2_ctx *c, int nsteps)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "gb2_setup must precede gb2_run");
+    for (int step = 0; step < nsteps; step++) {
+        c->ntimestep++;
+        c->ago++;
+        const bool decide = c->ago >= c->P.neigh_delay && c->ago % c->P.neigh_every == 0;
+        const bool check = decide && c->P.neigh_check;
+        if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
+        Dev D = make_dev(c);
+        k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
+        CKL();
+        bool rebuild = decide && !c->P.neigh_check;
+        if (check) {
+            CK(cudaMemcpyAsync(&c->h_pinned[1], c->ddflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            rebuild = c->h_pinned[1] != 0;
+        }
+        if (rebuild) {
+            const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
+            int rc = do_rebuild(c, true, sort_now);
+            if (rc) return rc;
+        } else if (c->nghost > 0) {
+            k_forward_comm<<<nblk(c->nghost), kBlock, 0, c->st>>>(D);
+            CKL();
+        }
+        if (do_force(c, 1, 1)) return GB2_ERR_CUDA;
+    }
+    int st;
+    if (read_status(c, &st)) return GB2_ERR_CUDA;
+    if (st & ST_MESH_INTERNAL) return set_err(c, GB2_ERR_STATE, "mesh contact history inconsistent");
+    return 0;
+}
+
+int gb2_sync(gb2_ctx *c)
+{
+    if (!c) return GB2_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int gb2_download_atoms(gb2_ctx *c, int cap, int *n, double *x, double *v, double *omega, double *f, double *torque,
+                       int *tag)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (n) *n = c->nlocal;
+    const int m = std::min(cap, c->nlocal);
+    if (m <= 0) return 0;
+    std::vector<dbl4> b(m);
+    auto get4 = [&](const DBuf<dbl4> &src, double *dst) -> int {
+        if (!dst) return 0;
+        CK(cudaMemcpyAsync(b.data(), src.p, sizeof(dbl4) * m, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (int i = 0; i < m; i++) {
+            dst[3 * i] = b[i].x;
+            dst[3 * i + 1] = b[i].y;
+            dst[3 * i + 2] = b[i].z;
+        }
+        return 0;
+    };
+    if (get4(c->pos, x) || get4(c->vel, v) || get4(c->omg, omega) || get4(c->f, f) || get4(c->tq, torque))
+        return GB2_ERR_CUDA;
+    if (tag) {
+        CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return 0;
+}
+
+int gb2_download_pairs(gb2_ctx *c, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no neighbor list before setup");
+    const size_t cp = c->cap;
+    const int nl = c->nlocal;
+    std::vector<int> nnum(nl), nbr((size_t)c->maxn * cp), fl((size_t)c->maxn * cp), tg(c->nlocal + c->nghost);
+    std::vector<double> h((size_t)3 * c->maxn * cp);
+    CK(cudaMemcpyAsync(nnum.data(), c->nnum.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(nbr.data(), c->nbr.p, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(fl.data(), c->flag.p, sizeof(int) * fl.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(h.data(), c->hist.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(tg.data(), c->tag.p, sizeof(int) * tg.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int k = 0;
+    for (int i = 0; i < nl; i++)
+        for (int s = 0; s < nnum[i]; s++) {
+            const size_t e = (size_t)s * cp + i;
+            if (k < cap) {
+                if (tag_i) tag_i[k] = tg[i];
+                if (tag_j) tag_j[k] = tg[nbr[e]];
+                if (flag) flag[k] = fl[e];
+                if (hist)
+                    for (int q = 0; q < 3; q++) hist[3 * k + q] = h[(size_t)(3 * s + q) * cp + i];
+            }
+            k++;
+        }
+    if (n) *n = k;
+    c->npairs_last = k;
+    return 0;
+}
+
+int gb2_download_wall_history(gb2_ctx *c, int ifix, int cap, double *hist)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_PLANE) return GB2_ERR_ARG;
+    const int m = std::min(cap, c->nlocal);
+    std::vector<double> h((size_t)3 * c->cap);
+    CK(cudaMemcpyAsync(h.data(), c->fix[ifix].whist.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < m; i++)
+        for (int q = 0; q < 3; q++) hist[3 * i + q] = h[(size_t)q * c->cap + i];
+    return 0;
+}
+
+int gb2_download_mesh_contacts(gb2_ctx *c, int ifix, int cap, int *n, int *tag, int *tri, double *hist)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH) return GB2_ERR_ARG;
+    MeshFix &M = *c->fix[ifix].mesh;
+    const size_t cp = c->cap;
+    const int nl = c->nlocal;
+    std::vector<int> tc(nl), sp((size_t)M.maxt * cp), tg(nl);
+    std::vector<double> h((size_t)3 * M.maxt * cp);
+    CK(cudaMemcpyAsync(tc.data(), M.tcnt.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(sp.data(), M.spartner.p, sizeof(int) * sp.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(h.data(), M.shist.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(tg.data(), c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int k = 0;
+    for (int i = 0; i < nl; i++)
+        for (int s = 0; s < tc[i]; s++) {
+            const int t = sp[(size_t)s * cp + i];
+            if (t < 0) continue;
+            if (k < cap) {
+                if (tag) tag[k] = tg[i];
+                if (tri) tri[k] = t;
+                if (hist)
+                    for (int q = 0; q < 3; q++) hist[3 * k + q] = h[(size_t)(3 * s + q) * cp + i];
+            }
+            k++;
+        }
+    if (n) *n = k;
+    return 0;
+}
+
+int gb2_mesh_topology(gb2_ctx *c, int ifix, int cap, int *ntri, unsigned char *edge_active,
+                      unsigned char *corner_active, int *obtuse)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH) return GB2_ERR_ARG;
+    const MeshTopo &T = c->fix[ifix].mesh->topo;
+    const int n = (int)T.tri.size();
+    if (ntri) *ntri = n;
+    for (int t = 0; t < std::min(n, cap); t++) {
+        for (int k = 0; k < 3; k++) {
+            if (edge_active) edge_active[3 * t + k] = (T.tri[t].active >> k) & 1;
+            if (corner_active) corner_active[3 * t + k] = (T.tri[t].active >> (3 + k)) & 1;
+        }
+        if (obtuse) obtuse[t] = T.tri[t].obtuse;
+    }
+    return 0;
+}
+
+int gb2_get_stats(gb2_ctx *c, gb2_stats *s)
+{
+    if (!c || !s) return GB2_ERR_ARG;
+    std::memset(s, 0, sizeof *s);
+    s->ntimestep = c->ntimestep;
+    s->nlocal = c->nlocal;
+    s->nghost = c->nghost;
+    s->nbuilds = c->nbuilds;
+    s->npairs = c->npairs_last;
+    s->maxneigh = c->maxn;
+    s->maxpartner = c->maxp;
+    s->kernel_launches = c->launches;
+    return 0;
+}
+
+int gb2_last_error(gb2_ctx *c, char *buf, int len)
+{
+    if (!c || !buf || len <= 0) return GB2_ERR_ARG;
+    std::snprintf(buf, len, "%s", c->err.c_str());
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+// gb2_internal.h -- device data layout and kernel interfaces of libgranb200.
+//
+// Layout in HBM (capacities in parentheses):
+//   per atom (nmax = owned + ghost images), 32-byte records so one sector
+//   serves a neighbour gather:
+//     pos  {x, y, z, radius}      vel {vx, vy, vz, rmass}
+//     omg  {wx, wy, wz, -}        type, tag (int32)
+//   per owned atom:
+//     f, tq {., ., ., -}          force / torque of the last step
+//     fpart, tpart                reverse-entry partial sums (pair pass A)
+//     xhold {x, y, z, -}          positions at the last neighbour build
+//   half neighbour list, slot-major so a warp reads consecutive atoms
+//   (capacity maxn slots per owned atom, stride `cap`):
+//     nnum[i], nbr[s*cap+i] (j index), flag[s*cap+i] (contact flag bits),
+//     hist[(3s+c)*cap+i] (shear history, FP64)
+//   reverse list (entries where the atom is the j side, ascending owner):
+//     rnum[k], rev[s*cap+k] = half-list slot e = s'*cap + i'
+//   contact-history partners (FixContactHistory::partner_, keyed by tag):
+//     pnum[i], ptag[s*cap+i], phist[(3s+c)*cap+i]
+//   ghosts: gsrc[g] (owned source atom), gshift[g] {dx, dy, dz, -}
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "gb2_contact.cuh"
+
+namespace gb2 {
+
+struct __align__(32) dbl4 {
+    double x, y, z, w;
+};
+
+constexpr int kMaxTypes = 8;      // material table is [kMaxTypes+1]^2
+constexpr int kMaxFix = 16;
+constexpr int kNeighMax = 5;      // TriMesh = SurfaceMesh<3,5>
+
+// status bits written by device code
+enum : int {
+    ST_NEIGH_OVERFLOW = 1 << 0,
+    ST_PARTNER_OVERFLOW = 1 << 1,
+    ST_MESHSLOT_OVERFLOW = 1 << 2,
+    ST_LOST_ATOM = 1 << 3,
+    ST_REV_OVERFLOW = 1 << 4,
+    ST_MESH_INTERNAL = 1 << 5,
+};
+
+enum FixKind : int { FIX_NONE = 0, FIX_GRAVITY = 1, FIX_WALL_PLANE = 2, FIX_WALL_MESH = 3 };
+
+// one triangle, as the narrow phase reads it (all FP64)
+struct TriGeom {
+    double node[3][3];
+    double edgevec[3][3];
+    double edgelen[3];
+    double edgenorm[3][3];
+    double surfnorm[3];
+    double center[3];
+    double rbound;
+    int obtuse;            // obtuse-angle node or -1
+    int active;            // bits 0-2 edge active, bits 3-5 corner active
+};
+
+struct MeshDev {
+    int ntri;
+    const TriGeom *tri;
+    // coplanar node-neighbour relation (areCoplanarNodeNeighs), CSR sorted
+    const int *cnn_start;
+    const int *cnn_list;
+    // bin -> triangles whose precomputed bin list contains the bin (ascending)
+    const int *bin_tri_start;
+    const int *bin_tri_list;
+    double nl_skin;        // FixNeighlistMesh skin (0.5 * neighbor skin, static mesh)
+    int wtype;
+    int rolling;
+    // per owned atom: candidate triangles (ascending) and contact slots
+    int maxt;              // slot capacity per atom
+    int *tcnt;             // fix_nneighs
+    int *tlist;            // [s*cap + i]
+    int *snp;              // npartner
+    int *spartner;         // [s*cap + i] triangle id or -1
+    double *shist;         // [(3s+c)*cap + i]
+};
+
+struct FixDev {
+    int kind;
+    double acc[3];         // gravity
+    int dim;               // plane
+    double pos;
+    int wtype;
+    int rolling;
+    uint8_t *inlist;       // primitive-wall neighbour flag per owned atom
+    double *whist;         // [c*cap + i]
+    MeshDev mesh;
+};
+
+// everything a step kernel needs, passed by value
+struct Dev {
+    int nlocal, nghost, nmax, cap;   // cap: stride of slot-major arrays (>= nlocal)
+    dbl4 *pos, *vel, *omg;
+    dbl4 *vel_out, *omg_out;   // final_integrate target (double buffer: pass B reads vel/omg of neighbours)
+    int *type, *tag;
+    dbl4 *f, *tq, *fpart, *tpart, *xhold;
+    // half list
+    int maxn;
+    int *nnum, *nbr, *flag;
+    double *hist;
+    // reverse list
+    int maxr;
+    int *rnum, *rev;
+    // partners
+    int maxp;
+    int *pnum, *ptag;
+    double *phist;
+    // ghosts
+    int *gsrc;
+    dbl4 *gshift;
+    // bins
+    double bboxlo[3], bboxhi[3], bininv[3], binsize[3];
+    int nbin[3], mbinlo[3], mbin[3], mbins;
+    int nstencil;
+    const int *stencil;
+    const int *bin_start;    // [mbins+1]
+    const int *bin_atoms;    // atoms sorted by bin, ascending index within a bin
+    // materials [(kMaxTypes+1)^2]
+    const MatPair *mat;
+    int ntypes;
+    // physics
+    double dt, skin, cutneighmax, triggersq;
+    int rolling, tdamp;
+    // fixes
+    int nfix;
+    FixDev fix[kMaxFix];
+    int *status;
+    int *dflag;              // displacement trigger
+};
+
+// host-side mesh topology (gb2_mesh.cpp)
+struct MeshTopo {
+    std::vector<TriGeom> tri;
+    std::vector<int> cnn_start, cnn_list;       // coplanar node neighbours, CSR
+    std::vector<std::vector<int>> edge_neigh;   // elements sharing an edge
+};
+bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, double precision, MeshTopo &out,
+                         std::string &err);
+bool tri_neighbuild_host(const TriGeom &T, double rSphere, const double *c, double treshold);
+
+}  // namespace gb2

@@ -1,0 +1,175 @@
+"""Seeded synthetic workloads for the granular hot path.
+
+The reference publishes no benchmark inputs, so these generators stand in for
+them with the shapes, sizes and value distributions the benchmark
+configurations name:
+
+* ``sphere_pour``  -- monodisperse Hertz/history pour on a flat floor with
+  periodic x/y (20,000 spheres, r = 1 mm, 40 x 40 x 200 mm box).
+* ``hopper``       -- polydisperse spheres (lognormal radius, median 1 mm,
+  sigma 0.25, clipped to 0.5-2 mm) with Hertz/history + rolling friction cdt
+  in a procedurally triangulated conical hopper (60 deg half-angle, 30 mm
+  outlet) discharging onto a flat catch floor.
+
+A scenario is a plain dict (box, materials, atoms, ordered fix list) that the
+engine wrapper and the tests both consume.  Units are SI throughout.
+"""
+import math
+
+import numpy as np
+
+
+def _materials(ntypes, E, nu, e, mu, mur=0.0):
+    return {
+        "ntypes": ntypes,
+        "youngs": np.full(ntypes, E),
+        "poisson": np.full(ntypes, nu),
+        "restitution": np.full((ntypes, ntypes), e),
+        "friction": np.full((ntypes, ntypes), mu),
+        "rollfriction": np.full((ntypes, ntypes), mur),
+    }
+
+
+def _atoms(pos, radius, density, vel, seed_omega=None):
+    n = len(radius)
+    rmass = 4.0 * math.pi / 3.0 * radius ** 3 * density
+    return {
+        "x": np.ascontiguousarray(pos, dtype=np.float64),
+        "v": np.ascontiguousarray(vel, dtype=np.float64),
+        "omega": np.zeros((n, 3)) if seed_omega is None else seed_omega,
+        "radius": np.ascontiguousarray(radius, dtype=np.float64),
+        "rmass": np.ascontiguousarray(rmass, dtype=np.float64),
+        "type": np.ones(n, dtype=np.int32),
+        "tag": np.arange(1, n + 1, dtype=np.int32),
+    }
+
+
+def sphere_pour(n=20000, seed=12345, dt=1e-5, skin=0.5e-3, jitter=0.2e-3, vmax=0.1,
+                box=(0.04, 0.04, 0.2), spacing=(2.5e-3, 2.5e-3, 2.4e-3), omega_max=0.0):
+    """Monodisperse pour: jittered lattice (16 x 16 per layer at 2.5 mm, layers
+    2.4 mm apart), uniform +-vmax velocities, flat z=0 floor, gravity -z."""
+    rng = np.random.default_rng(seed)
+    r = 1e-3
+    nx = int(round(box[0] / spacing[0]))
+    ny = int(round(box[1] / spacing[1]))
+    per_layer = nx * ny
+    nlayers = (n + per_layer - 1) // per_layer
+    ii = np.arange(nlayers * per_layer)[:n]
+    ix = ii % nx
+    iy = (ii // nx) % ny
+    iz = ii // per_layer
+    pos = np.stack([(ix + 0.5) * spacing[0], (iy + 0.5) * spacing[1], 1.5e-3 + iz * spacing[2]], axis=1)
+    pos = pos + rng.uniform(-jitter, jitter, size=pos.shape)
+    vel = rng.uniform(-vmax, vmax, size=(n, 3))
+    om = rng.uniform(-omega_max, omega_max, size=(n, 3)) if omega_max > 0 else None
+    if pos[:, 2].max() + r >= box[2]:
+        raise ValueError("lattice does not fit the box")
+    sc = {
+        "name": "sphere_pour",
+        "dt": dt, "skin": skin,
+        "boxlo": [0.0, 0.0, 0.0], "boxhi": list(box), "periodic": [1, 1, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": 1000, "sortbinsize": 0.0,
+        "rolling_cdt": 0, "tangential_damping": 1,
+        "atoms": _atoms(pos, np.full(n, r), 2500.0, vel, om),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_plane", "dim": 2, "pos": 0.0, "wall_type": 1, "rolling_cdt": 0},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5))
+    return sc
+
+
+def cone_mesh(n_theta=128, n_z=32, r_out=0.015, half_angle_deg=60.0, height=0.17, z0=0.0):
+    """Triangulated cone frustum (a hopper), ``2 * n_theta * n_z`` triangles.
+
+    Rings are evenly spaced in z; every quad between two rings and two
+    generators is planar and is split along one diagonal.  Returned as an
+    (ntri, 3, 3) node array in STL facet order."""
+    t = math.tan(math.radians(half_angle_deg))
+    th = np.linspace(0.0, 2.0 * math.pi, n_theta + 1)[:-1]
+    zs = z0 + np.linspace(0.0, height, n_z + 1)
+    rs = r_out + (zs - z0) * t
+    tris = []
+    for l in range(n_z):
+        for k in range(n_theta):
+            k2 = (k + 1) % n_theta
+            p00 = (rs[l] * math.cos(th[k]), rs[l] * math.sin(th[k]), zs[l])
+            p01 = (rs[l] * math.cos(th[k2]), rs[l] * math.sin(th[k2]), zs[l])
+            p10 = (rs[l + 1] * math.cos(th[k]), rs[l + 1] * math.sin(th[k]), zs[l + 1])
+            p11 = (rs[l + 1] * math.cos(th[k2]), rs[l + 1] * math.sin(th[k2]), zs[l + 1])
+            tris.append((p00, p01, p11))
+            tris.append((p00, p11, p10))
+    return np.asarray(tris, dtype=np.float64)
+
+
+def hopper(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z=32, half_angle_deg=60.0,
+           r_out=0.015, gap=0.05, vmax=0.0, floor_drop=0.08):
+    """Polydisperse hopper discharge (Hertz/history + rolling friction cdt).
+
+    Radii: lognormal, median 1 mm, sigma 0.25, clipped to [0.5, 2] mm.  The
+    particles are sorted by radius (largest first) and stacked bottom-up in
+    simple-cubic layers whose spacing is (2 + gap) x the largest radius in the
+    layer, clipped to the cone interior, so the fill starts dense with small
+    gaps and no overlaps.  A flat floor ``floor_drop`` below the outlet
+    catches the discharge so no atom leaves the box."""
+    rng = np.random.default_rng(seed)
+    rad = np.exp(rng.normal(math.log(1e-3), 0.25, size=n))
+    rad = np.clip(rad, 0.5e-3, 2e-3)
+    rad = np.sort(rad)[::-1].copy()
+    t = math.tan(math.radians(half_angle_deg))
+    pos = np.zeros((n, 3))
+    placed = 0
+    z = 2.1e-3
+    while placed < n:
+        rmax = rad[placed]
+        s = (2.0 + gap) * rmax
+        zc = z + rmax
+        # usable radius: cone wall distance >= radius (wall normal inclined)
+        rcone = r_out + zc * t
+        rin = rcone - rmax / math.cos(math.radians(half_angle_deg)) - 0.2e-3
+        if rin <= 0:
+            z += s
+            continue
+        m = int(rin // s)
+        g = np.arange(-m, m + 1) * s
+        gx, gy = np.meshgrid(g, g, indexing="ij")
+        ok = gx ** 2 + gy ** 2 <= rin ** 2
+        pts = np.stack([gx[ok], gy[ok]], axis=1)
+        take = min(len(pts), n - placed)
+        sl = slice(placed, placed + take)
+        pos[sl, 0] = pts[:take, 0]
+        pos[sl, 1] = pts[:take, 1]
+        pos[sl, 2] = zc
+        placed += take
+        z = zc + rmax + gap * rmax
+    height = pos[:, 2].max() + 0.01
+    nodes = cone_mesh(n_theta, n_z, r_out, half_angle_deg, height)
+    rtop = r_out + height * t
+    lo = [-(rtop + 0.01), -(rtop + 0.01), -floor_drop - 0.01]
+    hi = [rtop + 0.01, rtop + 0.01, height + 0.02]
+    vel = rng.uniform(-vmax, vmax, size=(n, 3)) if vmax > 0 else np.zeros((n, 3))
+    sc = {
+        "name": "hopper",
+        "dt": dt, "skin": skin,
+        "boxlo": lo, "boxhi": hi, "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": 1000, "sortbinsize": 0.0,
+        "rolling_cdt": 1, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2500.0, vel),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_mesh", "nodes": nodes, "wall_type": 1, "curvature": 0.0, "rolling_cdt": 1},
+            {"kind": "wall_plane", "dim": 2, "pos": -floor_drop, "wall_type": 1, "rolling_cdt": 1},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5, 0.1))
+    return sc
+
+
+def subset(sc, n):
+    """First ``n`` atoms of a scenario (same box, fixes and materials)."""
+    out = dict(sc)
+    out["atoms"] = {k: np.ascontiguousarray(v[:n]) for k, v in sc["atoms"].items()}
+    return out

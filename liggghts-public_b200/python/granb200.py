@@ -1,0 +1,258 @@
+"""ctypes front end of libgranb200 (the C ABI in include/granb200.h).
+
+``Engine(scenario)`` builds one device-resident simulation from a scenario
+dict (see gb2_scenarios) and mirrors the reference's run sequence:
+``setup()`` is Verlet::setup, ``run(n)`` is Verlet::run(n).  There is no CPU
+fallback: constructing an Engine without the built library, or without a
+CUDA device, raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libgranb200.so")
+_LIB = None
+
+D = ctypes.POINTER(ctypes.c_double)
+I = ctypes.POINTER(ctypes.c_int)
+U8 = ctypes.POINTER(ctypes.c_ubyte)
+
+PREC_FP64 = 0
+PREC_SPLIT = 1
+
+EXPORTS = (
+    "gb2_create", "gb2_destroy", "gb2_set_materials", "gb2_upload_atoms", "gb2_add_gravity",
+    "gb2_add_wall_plane", "gb2_add_wall_mesh", "gb2_setup", "gb2_run", "gb2_sync", "gb2_download_atoms",
+    "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
+    "gb2_get_stats", "gb2_last_error", "gb2_version",
+)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("ntypes", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("skin", ctypes.c_double),
+        ("boxlo", ctypes.c_double * 3),
+        ("boxhi", ctypes.c_double * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("neigh_every", ctypes.c_int),
+        ("neigh_delay", ctypes.c_int),
+        ("neigh_check", ctypes.c_int),
+        ("sort_freq", ctypes.c_int),
+        ("sort_binsize", ctypes.c_double),
+        ("rolling_cdt", ctypes.c_int),
+        ("tangential_damping", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("ntimestep", ctypes.c_long),
+        ("nlocal", ctypes.c_int),
+        ("nghost", ctypes.c_int),
+        ("nbuilds", ctypes.c_int),
+        ("npairs", ctypes.c_long),
+        ("ntouch", ctypes.c_long),
+        ("maxneigh", ctypes.c_int),
+        ("maxpartner", ctypes.c_int),
+        ("time_pair", ctypes.c_double),
+        ("time_neigh", ctypes.c_double),
+        ("time_other", ctypes.c_double),
+        ("kernel_launches", ctypes.c_long),
+    ]
+
+
+def lib(path=LIB_PATH):
+    """Load the in-tree shared library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise RuntimeError("libgranb200.so not built: run __graft_entry__.build() (%s)" % path)
+        L = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        L.gb2_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+        L.gb2_destroy.argtypes = [vp]
+        L.gb2_set_materials.argtypes = [vp, D, D, D, D, D]
+        L.gb2_upload_atoms.argtypes = [vp, ctypes.c_int, D, D, D, D, D, I, I]
+        L.gb2_add_gravity.argtypes = [vp, ctypes.c_double, D]
+        L.gb2_add_wall_plane.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.gb2_add_wall_mesh.argtypes = [vp, ctypes.c_int, D, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.gb2_setup.argtypes = [vp]
+        L.gb2_run.argtypes = [vp, ctypes.c_int]
+        L.gb2_sync.argtypes = [vp]
+        L.gb2_download_atoms.argtypes = [vp, ctypes.c_int, I, D, D, D, D, D, I]
+        L.gb2_download_pairs.argtypes = [vp, ctypes.c_int, I, I, I, I, D]
+        L.gb2_download_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
+        L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
+        L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
+        L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.gb2_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.gb2_version.restype = ctypes.c_char_p
+        _LIB = L
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(I)
+
+
+class GB2Error(RuntimeError):
+    pass
+
+
+class Engine:
+    """One device-resident granular simulation (one gb2_ctx)."""
+
+    def __init__(self, sc, precision=PREC_FP64, device=0):
+        L = lib()
+        self.L = L
+        p = Params()
+        p.ntypes = sc["ntypes"]
+        p.dt = sc["dt"]
+        p.skin = sc["skin"]
+        for d in range(3):
+            p.boxlo[d] = sc["boxlo"][d]
+            p.boxhi[d] = sc["boxhi"][d]
+            p.periodic[d] = int(sc["periodic"][d])
+        p.neigh_every = sc.get("every", 1)
+        p.neigh_delay = sc.get("delay", 0)
+        p.neigh_check = sc.get("check", 1)
+        p.sort_freq = sc.get("sortfreq", 1000)
+        p.sort_binsize = sc.get("sortbinsize", 0.0)
+        p.rolling_cdt = int(sc.get("rolling_cdt", 0))
+        p.tangential_damping = int(sc.get("tangential_damping", 1))
+        p.precision = precision
+        p.device = device
+        self.h = ctypes.c_void_p()
+        rc = L.gb2_create(ctypes.byref(p), ctypes.byref(self.h))
+        if rc != 0:
+            raise GB2Error("gb2_create failed (%d): no CUDA device or unsupported option" % rc)
+        keep = []
+
+        def arr(x, dt=np.float64):
+            a = np.ascontiguousarray(np.asarray(x, dtype=dt).ravel())
+            keep.append(a)
+            return a
+
+        self._check(L.gb2_set_materials(self.h, _dp(arr(sc["youngs"])), _dp(arr(sc["poisson"])),
+                                        _dp(arr(sc["restitution"])), _dp(arr(sc["friction"])),
+                                        _dp(arr(sc["rollfriction"]))))
+        a = sc["atoms"]
+        n = len(a["tag"])
+        self._check(L.gb2_upload_atoms(self.h, n, _dp(arr(a["x"])), _dp(arr(a["v"])), _dp(arr(a["omega"])),
+                                       _dp(arr(a["radius"])), _dp(arr(a["rmass"])), _ip(arr(a["type"], np.int32)),
+                                       _ip(arr(a["tag"], np.int32))))
+        self.fix_ids = []
+        self.ntri = {}
+        for fx in sc["fixes"]:
+            kind = fx["kind"]
+            if kind == "gravity":
+                k = L.gb2_add_gravity(self.h, fx["magnitude"], _dp(arr(fx["vector"])))
+            elif kind == "wall_plane":
+                k = L.gb2_add_wall_plane(self.h, fx["dim"], fx["pos"], fx["wall_type"], int(fx.get("rolling_cdt", 0)))
+            elif kind == "wall_mesh":
+                nodes = arr(fx["nodes"])
+                k = L.gb2_add_wall_mesh(self.h, len(nodes) // 9, _dp(nodes), fx["wall_type"], fx.get("curvature", 0.0),
+                                        int(fx.get("rolling_cdt", 0)))
+                if k >= 0:
+                    self.ntri[len(self.fix_ids)] = len(nodes) // 9
+            elif kind == "nve_sphere":
+                k = None
+            else:
+                raise ValueError("unsupported fix kind " + kind)
+            if k is not None and k < 0:
+                self._check(k)
+            self.fix_ids.append(k)
+        self.n = n
+
+    def _err(self):
+        buf = ctypes.create_string_buffer(512)
+        self.L.gb2_last_error(self.h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise GB2Error("granb200 error %d: %s" % (rc, self._err()))
+
+    def close(self):
+        if self.h:
+            self.L.gb2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self):
+        self._check(self.L.gb2_setup(self.h))
+
+    def run(self, n):
+        self._check(self.L.gb2_run(self.h, n))
+
+    def sync(self):
+        self._check(self.L.gb2_sync(self.h))
+
+    def stats(self):
+        s = Stats()
+        self._check(self.L.gb2_get_stats(self.h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def atoms(self):
+        n = self.n
+        out = {k: np.zeros((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
+        tag = np.zeros(n, dtype=np.int32)
+        cnt = ctypes.c_int()
+        self._check(self.L.gb2_download_atoms(self.h, n, ctypes.byref(cnt), _dp(out["x"]), _dp(out["v"]),
+                                              _dp(out["omega"]), _dp(out["f"]), _dp(out["torque"]), _ip(tag)))
+        out["tag"] = tag
+        return out
+
+    def pairs(self):
+        cnt = ctypes.c_int()
+        self._check(self.L.gb2_download_pairs(self.h, 0, ctypes.byref(cnt), None, None, None, None))
+        n = cnt.value
+        ti = np.zeros(n, dtype=np.int32)
+        tj = np.zeros(n, dtype=np.int32)
+        fl = np.zeros(n, dtype=np.int32)
+        hi = np.zeros((n, 3))
+        self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
+        return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def wall_hist(self, ifix):
+        h = np.zeros((self.n, 3))
+        self._check(self.L.gb2_download_wall_history(self.h, self.fix_ids[ifix], self.n, _dp(h)))
+        return h
+
+    def mesh_contacts(self, ifix):
+        k = self.fix_ids[ifix]
+        cnt = ctypes.c_int()
+        self._check(self.L.gb2_download_mesh_contacts(self.h, k, 0, ctypes.byref(cnt), None, None, None))
+        n = cnt.value
+        tag = np.zeros(n, dtype=np.int32)
+        tri = np.zeros(n, dtype=np.int32)
+        h = np.zeros((n, 3))
+        self._check(self.L.gb2_download_mesh_contacts(self.h, k, n, ctypes.byref(cnt), _ip(tag), _ip(tri), _dp(h)))
+        return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_topology(self, ifix):
+        k = self.fix_ids[ifix]
+        nmax = self.ntri[ifix]
+        ea = np.zeros(3 * nmax, dtype=np.uint8)
+        ca = np.zeros(3 * nmax, dtype=np.uint8)
+        ob = np.zeros(nmax, dtype=np.int32)
+        nt = ctypes.c_int()
+        self._check(self.L.gb2_mesh_topology(self.h, k, nmax, ctypes.byref(nt), ea.ctypes.data_as(U8),
+                                             ca.ctypes.data_as(U8), _ip(ob)))
+        n = nt.value
+        return ea[:3 * n].reshape(n, 3), ca[:3 * n].reshape(n, 3), ob[:n]

@@ -1,0 +1,1794 @@
+/*
+ * gran_oracle.c -- CPU oracle (TEST INFRASTRUCTURE ONLY, see gran_oracle.h).
+ *
+ * A single-threaded C restatement of the LIGGGHTS-PUBLIC granular time step.
+ * Every function cites the reference file:line it follows; the arithmetic is
+ * written in the same operation order so that IEEE results coincide.
+ * Parity status: unpinned against reference binaries (the reference needs
+ * generated style headers to compile); pinned against analytic cases.
+ */
+#include "gran_oracle.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define BIG 1.0e20
+#define SMALL 1.0e-6            /* src/neighbor.cpp:58 */
+#define CUT2BIN_RATIO 100
+#define SMALL_TRIMESH 1.e-10    /* src/tri_mesh_I.h:48 */
+#define LARGE_TRIMESH 1000000   /* src/tri_mesh_I.h:50 */
+#define EPSILON_PRECISION 1e-8  /* src/multi_node_mesh.h:59 */
+#define NEIGH_MAX 5             /* TriMesh = SurfaceMesh<3,5> */
+#define CONTACT_NORMAL_MODEL 1  /* src/contact_model_constants.h:64 */
+#define CONTACT_TANGENTIAL_MODEL 4
+#define MAXFIX 16
+#define NO_OBTUSE_ANGLE -1
+
+/* ------------------------------------------------------------------ */
+/* small vector helpers, same operation order as src/vector_liggghts.h  */
+
+static inline double dot3(const double *a, const double *b) { return a[0]*b[0]+a[1]*b[1]+a[2]*b[2]; }
+static inline double mag3(const double *v) { return sqrt(v[0]*v[0]+v[1]*v[1]+v[2]*v[2]); }
+static inline void sub3(const double *a, const double *b, double *r) { r[0]=a[0]-b[0]; r[1]=a[1]-b[1]; r[2]=a[2]-b[2]; }
+static inline void cross3(const double *a, const double *b, double *r)
+{ r[0]=a[1]*b[2]-a[2]*b[1]; r[1]=a[2]*b[0]-a[0]*b[2]; r[2]=a[0]*b[1]-a[1]*b[0]; }
+static inline void sdiv3(double *v, double s) { const double sinv = 1./s; v[0]=sinv*v[0]; v[1]=sinv*v[1]; v[2]=sinv*v[2]; }
+static inline int comp_double(double a, double b, double prec)   /* src/math_extra_liggghts.h:536 */
+{
+    if (a == b) return 1;
+    if (b == 0) return a < prec && a > -prec;
+    double x = (a-b);
+    return x < prec && x > -prec;
+}
+
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    int dim; double pos; int wtype; int rolling;
+    int rebuild;            /* rebuildPrimitiveNeighlist_ */
+    int *list; int nlist, caplist;
+    double *hist;           /* property/atom history, 3 per atom */
+} wall_plane;
+
+typedef struct {
+    int ntri;
+    double (*node)[3][3];
+    double (*center)[3];
+    double *rbound;
+    double (*edgevec)[3][3];
+    double (*edgelen)[3];
+    double (*edgenorm)[3][3];
+    double (*surfnorm)[3];
+    int *obtuse;
+    unsigned char (*edge_active)[3];
+    unsigned char (*corner_active)[3];
+    int *nneigh; int (*neighfaces)[NEIGH_MAX];
+    double curvature, precision;
+    int wtype, rolling;
+    /* FixNeighlistMesh */
+    int **tri_list; int *tri_n; int *tri_cap;
+    int **tri_bins; int *tri_nbins;
+    double nl_skin, nl_distmax;
+    long last_bin_update;
+    int build_neighlist_nl;   /* FixNeighlistMesh::buildNeighList */
+    /* FixContactHistoryMesh, per atom */
+    int build_neighlist_ch;   /* FixContactHistoryMesh::build_neighlist_ */
+    int *nneighs; int *npartner; int **partner; double **chist;
+    unsigned char **keep; unsigned char **isect;
+} wall_mesh;
+
+typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; } fixrec;
+
+struct orc_sim {
+    orc_params p;
+    int ntypes;
+    double **Yeff, **Geff, **betaeff, **mu, **mur;
+    /* atoms */
+    int nlocal, nghost, nmax;
+    double *x, *v, *omega, *f, *torque, *radius, *rmass;
+    int *type, *tag;
+    /* ghosts: source index and swap shift */
+    int *gsrc; double *gshift;   /* per ghost: 3 shifts */
+    int nswap; int swapfirst[8], swapnum[8];
+    /* domain */
+    double boxlo[3], boxhi[3], prd[3];
+    /* neighbor */
+    double cutneighmax, cutneighmaxsq, triggersq, cutghost;
+    double *maxrad;
+    double bboxlo[3], bboxhi[3];
+    int nbinx, nbiny, nbinz, mbinx, mbiny, mbinz, mbinxlo, mbinylo, mbinzlo, mbins;
+    double binsizex, binsizey, binsizez, bininvx, bininvy, bininvz;
+    int *binhead, *bins; int nstencil; int *stencil;
+    int ago; long ntimestep; int nbuilds;
+    double *xhold;
+    /* half list */
+    int *nstart, *nnum; int *nbr, *flag; double *hist; int npairs, cappairs;
+    /* FixContactHistory partner arrays */
+    int *npartner; int **partner; double **phist; int computeflag;
+    /* sort */
+    long nextsort; int snbinx, snbiny, snbinz; double sbboxlo[3], sbininvx, sbininvy, sbininvz;
+    /* fixes */
+    int nfix; fixrec fix[MAXFIX]; int has_nve;
+    int setupflag;
+    char err[256];
+};
+
+static void fail(orc_sim *s, const char *fmt, ...)
+{
+    va_list ap; va_start(ap, fmt); vsnprintf(s->err, sizeof s->err, fmt, ap); va_end(ap);
+}
+
+static void *xrealloc(void *p, size_t n) { void *q = realloc(p, n ? n : 1); if (!q) { fprintf(stderr, "oracle: out of memory\n"); abort(); } return q; }
+static double **matrix(int n) { double **m = malloc(sizeof(double*)*n); double *d = calloc((size_t)n*n, sizeof(double)); for (int i = 0; i < n; i++) m[i] = d + (size_t)i*n; return m; }
+static void free_matrix(double **m) { if (m) { free(m[0]); free(m); } }
+
+/* ------------------------------------------------------------------ */
+/* material matrices: src/global_properties.cpp:411-560                */
+
+static void setup_materials(orc_sim *s)
+{
+    const int nt = s->ntypes;
+    s->Yeff = matrix(nt+1); s->Geff = matrix(nt+1); s->betaeff = matrix(nt+1);
+    s->mu = matrix(nt+1); s->mur = matrix(nt+1);
+    const orc_params *p = &s->p;
+    for (int i = 1; i <= nt; i++)
+        for (int j = 1; j <= nt; j++) {
+            const double Yi = p->youngs[i-1], Yj = p->youngs[j-1];
+            const double vi = p->poisson[i-1], vj = p->poisson[j-1];
+            s->Yeff[i][j] = 1./((1.-pow(vi,2.))/Yi+(1.-pow(vj,2.))/Yj);          /* :432 */
+            s->Geff[i][j] = 1./(2.*(2.-vi)*(1.+vi)/Yi+2.*(2.-vj)*(1.+vj)/Yj);   /* :461 */
+            const double lg = log(p->restitution[(i-1)*nt+(j-1)]);              /* :508 */
+            s->betaeff[i][j] = lg / sqrt(pow(lg,2.)+pow(M_PI,2.));               /* :540 */
+            s->mu[i][j] = p->friction[(i-1)*nt+(j-1)];
+            s->mur[i][j] = p->rollfriction ? p->rollfriction[(i-1)*nt+(j-1)] : 0.0;
+        }
+}
+
+/* ------------------------------------------------------------------ */
+/* the contact-model chain surface->normal->tangential->rolling
+   src/contact_models.h:228-238, for sphere pairs and walls             */
+
+typedef struct {
+    int is_wall;
+    double radi, radj, radsum, r, rinv, rsq, deltan;
+    double delta[3], en[3];
+    const double *v_i, *v_j, *omega_i, *omega_j;
+    double meff, mi, mj;
+    int itype, jtype;
+    int *contact_flags; double *contact_history;
+    int computeflag, shearupdate;
+    /* filled by the models */
+    double vn, wr1, wr2, wr3, vtr1, vtr2, vtr3, cri, crj, Fn, kn, kt, gamman, gammat;
+} sidata_t;
+
+typedef struct { double F[3], T[3]; } force_t;
+
+/* src/surface_model_default.h:150-204 */
+static void surface_default(sidata_t *sd)
+{
+    const double enx = sd->en[0], eny = sd->en[1], enz = sd->en[2];
+    const double vr1 = sd->v_i[0] - sd->v_j[0];
+    const double vr2 = sd->v_i[1] - sd->v_j[1];
+    const double vr3 = sd->v_i[2] - sd->v_j[2];
+    const double vn = vr1 * enx + vr2 * eny + vr3 * enz;
+    const double vn1 = vn * enx, vn2 = vn * eny, vn3 = vn * enz;
+    const double vt1 = vr1 - vn1, vt2 = vr2 - vn2, vt3 = vr3 - vn3;
+    const double deltan = sd->radsum - sd->r;
+    const double dx = sd->delta[0], dy = sd->delta[1], dz = sd->delta[2];
+    const double rinv = sd->rinv;
+    double wr1, wr2, wr3;
+    if (sd->is_wall) {
+        const double cr = sd->radi - 0.5*sd->deltan;
+        wr1 = cr * sd->omega_i[0] * rinv;
+        wr2 = cr * sd->omega_i[1] * rinv;
+        wr3 = cr * sd->omega_i[2] * rinv;
+        sd->cri = cr;
+    } else {
+        const double cri = sd->radi - 0.5 * deltan;
+        const double crj = sd->radj - 0.5 * deltan;
+        wr1 = (cri * sd->omega_i[0] + crj * sd->omega_j[0]) * rinv;
+        wr2 = (cri * sd->omega_i[1] + crj * sd->omega_j[1]) * rinv;
+        wr3 = (cri * sd->omega_i[2] + crj * sd->omega_j[2]) * rinv;
+        sd->cri = cri; sd->crj = crj;
+    }
+    sd->vtr1 = vt1 - (dz * wr2 - dy * wr3);
+    sd->vtr2 = vt2 - (dx * wr3 - dz * wr1);
+    sd->vtr3 = vt3 - (dy * wr1 - dx * wr2);
+    sd->vn = vn; sd->deltan = deltan;
+    sd->wr1 = wr1; sd->wr2 = wr2; sd->wr3 = wr3;
+}
+
+/* src/normal_model_hertz.h:202-393 (energy/heating/bond options off) */
+static void normal_hertz(orc_sim *s, sidata_t *sd, force_t *fi, force_t *fj)
+{
+    if (sd->contact_flags) *sd->contact_flags |= CONTACT_NORMAL_MODEL;
+    const int it = sd->itype, jt = sd->jtype;
+    const double radi = sd->radi, radj = sd->radj;
+    const double reff = sd->is_wall ? radi : (radi*radj/(radi+radj));
+    const double meff = sd->meff;
+    const double sqrtval = sqrt(reff*sd->deltan);
+    const double deltan = sd->deltan;
+    const double Sn = 2.*s->Yeff[it][jt]*sqrtval;
+    const double St = 8.*s->Geff[it][jt]*sqrtval;
+    double kn = 4./3.*s->Yeff[it][jt]*sqrtval;
+    double kt = St;
+    const double sqrtFiveOverSix = 0.91287092917527685576161630466800355658790782499663875;
+    const double gamman = -2.*sqrtFiveOverSix*s->betaeff[it][jt]*sqrt(Sn*meff);
+    const double gammat = s->p.tangential_damping ? -2.*sqrtFiveOverSix*s->betaeff[it][jt]*sqrt(St*meff) : 0.0;
+    kn /= 1.0;  /* force->nktv2p = 1 in si */
+    kt /= 1.0;
+    const double Fn_damping = -gamman*sd->vn;
+    const double Fn_contact = kn*deltan;
+    const double Fn = Fn_damping + Fn_contact;
+    sd->Fn = Fn; sd->kn = kn; sd->kt = kt; sd->gamman = gamman; sd->gammat = gammat;
+    if (sd->is_wall) {
+        const double Fn_ = Fn * 1.0;   /* area_ratio */
+        fi->F[0] += Fn_ * sd->en[0];
+        fi->F[1] += Fn_ * sd->en[1];
+        fi->F[2] += Fn_ * sd->en[2];
+    } else {
+        fi->F[0] += sd->Fn * sd->en[0];
+        fi->F[1] += sd->Fn * sd->en[1];
+        fi->F[2] += sd->Fn * sd->en[2];
+        fj->F[0] += -fi->F[0];
+        fj->F[1] += -fi->F[1];
+        fj->F[2] += -fi->F[2];
+    }
+}
+
+/* src/tangential_model_history.h:130-339 */
+static void tangential_history(orc_sim *s, sidata_t *sd, force_t *fi, force_t *fj)
+{
+    const double enx = sd->en[0], eny = sd->en[1], enz = sd->en[2];
+    if (sd->contact_flags) *sd->contact_flags |= CONTACT_TANGENTIAL_MODEL;
+    double *const shear = sd->contact_history;
+    const int update_history = sd->computeflag && sd->shearupdate;
+    if (update_history) {
+        const double dt = s->p.dt;
+        shear[0] += sd->vtr1 * dt;
+        shear[1] += sd->vtr2 * dt;
+        shear[2] += sd->vtr3 * dt;
+        double rsht = shear[0]*enx + shear[1]*eny + shear[2]*enz;
+        shear[0] -= rsht * enx;
+        shear[1] -= rsht * eny;
+        shear[2] -= rsht * enz;
+    }
+    const double shrmag = sqrt(shear[0]*shear[0] + shear[1]*shear[1] + shear[2]*shear[2]);
+    const double kt = sd->kt;
+    const double xmu = s->mu[sd->itype][sd->jtype];
+    double Ft1 = -(kt * shear[0]);
+    double Ft2 = -(kt * shear[1]);
+    double Ft3 = -(kt * shear[2]);
+    const double Ft_shear = kt * shrmag;
+    const double Ft_friction = xmu * fabs(sd->Fn);
+    if (Ft_shear > Ft_friction) {
+        if (shrmag != 0.0) {
+            const double ratio = Ft_friction / Ft_shear;
+            Ft1 *= ratio; Ft2 *= ratio; Ft3 *= ratio;
+            if (update_history) {
+                shear[0] = -Ft1/kt;
+                shear[1] = -Ft2/kt;
+                shear[2] = -Ft3/kt;
+            }
+        } else Ft1 = Ft2 = Ft3 = 0.0;
+    } else {
+        const double gammat = sd->gammat;
+        Ft1 -= (gammat*sd->vtr1);
+        Ft2 -= (gammat*sd->vtr2);
+        Ft3 -= (gammat*sd->vtr3);
+    }
+    const double tor1 = eny * Ft3 - enz * Ft2;
+    const double tor2 = enz * Ft1 - enx * Ft3;
+    const double tor3 = enx * Ft2 - eny * Ft1;
+    double torque_i[3], torque_j[3] = {0, 0, 0};
+    torque_i[0] = -sd->cri * tor1;
+    torque_i[1] = -sd->cri * tor2;
+    torque_i[2] = -sd->cri * tor3;
+    if (!sd->is_wall) {
+        torque_j[0] = -sd->crj * tor1;
+        torque_j[1] = -sd->crj * tor2;
+        torque_j[2] = -sd->crj * tor3;
+    }
+    if (sd->is_wall) {
+        const double area_ratio = 1.0;
+        fi->F[0] += Ft1 * area_ratio; fi->F[1] += Ft2 * area_ratio; fi->F[2] += Ft3 * area_ratio;
+        fi->T[0] += torque_i[0] * area_ratio; fi->T[1] += torque_i[1] * area_ratio; fi->T[2] += torque_i[2] * area_ratio;
+    } else {
+        fi->F[0] += Ft1; fi->F[1] += Ft2; fi->F[2] += Ft3;
+        fj->F[0] += -Ft1; fj->F[1] += -Ft2; fj->F[2] += -Ft3;
+        fi->T[0] += torque_i[0]; fi->T[1] += torque_i[1]; fi->T[2] += torque_i[2];
+        fj->T[0] += torque_j[0]; fj->T[1] += torque_j[1]; fj->T[2] += torque_j[2];
+    }
+}
+
+/* src/rolling_model_cdt.h:89-159 (torsionTorque off) */
+static void rolling_cdt(orc_sim *s, sidata_t *sd, force_t *fi, force_t *fj)
+{
+    const double rmu = s->mur[sd->itype][sd->jtype];
+    double r_torque[3] = {0., 0., 0.}, wr_roll[3];
+    const double radi = sd->radi, radj = sd->radj;
+    const double reff = sd->is_wall ? radi : (radi*radj/(radi+radj));
+    if (sd->is_wall) {
+        const double wr1 = sd->wr1, wr2 = sd->wr2, wr3 = sd->wr3;
+        const double wrmag = sqrt(wr1*wr1+wr2*wr2+wr3*wr3);
+        if (wrmag > 0.) {
+            const double kn = sd->kn;
+            const double enx = sd->en[0], eny = sd->en[1], enz = sd->en[2];
+            const double Fn = sd->deltan*kn;
+            r_torque[0] = rmu*Fn*wr1/wrmag*reff;
+            r_torque[1] = rmu*Fn*wr2/wrmag*reff;
+            r_torque[2] = rmu*Fn*wr3/wrmag*reff;
+            double d = r_torque[0]*enx+ r_torque[1]*eny + r_torque[2]*enz;
+            double rn[3] = {enx * d, eny * d, enz * d};
+            r_torque[0] = r_torque[0]-rn[0]; r_torque[1] = r_torque[1]-rn[1]; r_torque[2] = r_torque[2]-rn[2];
+        }
+    } else {
+        sub3(sd->omega_i, sd->omega_j, wr_roll);
+        const double wr_rollmag = mag3(wr_roll);
+        if (wr_rollmag > 0.) {
+            const double enx = sd->en[0], eny = sd->en[1], enz = sd->en[2];
+            const double sc = rmu*sd->kn*sd->deltan*reff/wr_rollmag;
+            r_torque[0] = sc*wr_roll[0]; r_torque[1] = sc*wr_roll[1]; r_torque[2] = sc*wr_roll[2];
+            const double d = r_torque[0]*enx + r_torque[1]*eny + r_torque[2]*enz;
+            double rn[3] = {enx * d, eny * d, enz * d};
+            r_torque[0] = r_torque[0]-rn[0]; r_torque[1] = r_torque[1]-rn[1]; r_torque[2] = r_torque[2]-rn[2];
+        }
+    }
+    fi->T[0] -= r_torque[0]; fi->T[1] -= r_torque[1]; fi->T[2] -= r_torque[2];
+    fj->T[0] += r_torque[0]; fj->T[1] += r_torque[1]; fj->T[2] += r_torque[2];
+}
+
+static void contact_chain(orc_sim *s, sidata_t *sd, force_t *fi, force_t *fj, int rolling)
+{
+    surface_default(sd);
+    normal_hertz(s, sd, fi, fj);
+    tangential_history(s, sd, fi, fj);
+    if (rolling) rolling_cdt(s, sd, fi, fj);
+}
+
+/* ------------------------------------------------------------------ */
+/* atoms                                                                */
+
+static void grow_atoms(orc_sim *s, int nmax)
+{
+    if (nmax <= s->nmax) return;
+    int old = s->nmax;
+    s->nmax = nmax;
+    s->x = xrealloc(s->x, sizeof(double)*3*nmax);
+    s->v = xrealloc(s->v, sizeof(double)*3*nmax);
+    s->omega = xrealloc(s->omega, sizeof(double)*3*nmax);
+    s->f = xrealloc(s->f, sizeof(double)*3*nmax);
+    s->torque = xrealloc(s->torque, sizeof(double)*3*nmax);
+    s->radius = xrealloc(s->radius, sizeof(double)*nmax);
+    s->rmass = xrealloc(s->rmass, sizeof(double)*nmax);
+    s->type = xrealloc(s->type, sizeof(int)*nmax);
+    s->tag = xrealloc(s->tag, sizeof(int)*nmax);
+    s->bins = xrealloc(s->bins, sizeof(int)*nmax);
+    (void)old;
+}
+
+/* grow every per-atom array (atoms and per-atom fix data) to nmax */
+static void grow_all(orc_sim *s, int nmax)
+{
+    int old = s->nmax;
+    if (nmax <= old) return;
+    grow_atoms(s, nmax);
+    s->npartner = xrealloc(s->npartner, sizeof(int)*s->nmax);
+    s->partner = xrealloc(s->partner, sizeof(int*)*s->nmax);
+    s->phist = xrealloc(s->phist, sizeof(double*)*s->nmax);
+    s->xhold = xrealloc(s->xhold, sizeof(double)*3*s->nmax);
+    for (int i = old; i < s->nmax; i++) { s->npartner[i] = 0; s->partner[i] = NULL; s->phist[i] = NULL; }
+    for (int k = 0; k < s->nfix; k++) {
+        if (s->fix[k].wp) { s->fix[k].wp->hist = xrealloc(s->fix[k].wp->hist, sizeof(double)*3*s->nmax); memset(s->fix[k].wp->hist + 3*old, 0, sizeof(double)*3*(s->nmax-old)); }
+        if (s->fix[k].wm) {
+            wall_mesh *m = s->fix[k].wm;
+            m->nneighs = xrealloc(m->nneighs, sizeof(int)*s->nmax);
+            m->npartner = xrealloc(m->npartner, sizeof(int)*s->nmax);
+            m->partner = xrealloc(m->partner, sizeof(int*)*s->nmax);
+            m->chist = xrealloc(m->chist, sizeof(double*)*s->nmax);
+            m->keep = xrealloc(m->keep, sizeof(unsigned char*)*s->nmax);
+            m->isect = xrealloc(m->isect, sizeof(unsigned char*)*s->nmax);
+            for (int i = old; i < s->nmax; i++) { m->nneighs[i] = 0; m->npartner[i] = 0; m->partner[i] = NULL; m->chist[i] = NULL; m->keep[i] = NULL; m->isect[i] = NULL; }
+        }
+    }
+}
+
+orc_sim *orc_create(const orc_params *p, int n, const double *x, const double *v, const double *omega,
+                    const double *radius, const double *rmass, const int *type, const int *tag)
+{
+    orc_sim *s = calloc(1, sizeof(orc_sim));
+    s->p = *p;
+    s->ntypes = p->ntypes;
+    setup_materials(s);
+    grow_atoms(s, n > 16 ? 2*n : 32);
+    s->nlocal = n;
+    memcpy(s->x, x, sizeof(double)*3*n);
+    memcpy(s->v, v, sizeof(double)*3*n);
+    memcpy(s->omega, omega, sizeof(double)*3*n);
+    memcpy(s->radius, radius, sizeof(double)*n);
+    memcpy(s->rmass, rmass, sizeof(double)*n);
+    memcpy(s->type, type, sizeof(int)*n);
+    memcpy(s->tag, tag, sizeof(int)*n);
+    memset(s->f, 0, sizeof(double)*3*n);
+    memset(s->torque, 0, sizeof(double)*3*n);
+    for (int d = 0; d < 3; d++) { s->boxlo[d] = p->boxlo[d]; s->boxhi[d] = p->boxhi[d]; s->prd[d] = p->boxhi[d]-p->boxlo[d]; }
+    s->npartner = calloc(s->nmax, sizeof(int));
+    s->partner = calloc(s->nmax, sizeof(int*));
+    s->phist = calloc(s->nmax, sizeof(double*));
+    s->xhold = calloc((size_t)3*s->nmax, sizeof(double));
+    return s;
+}
+
+void orc_destroy(orc_sim *s)
+{
+    if (!s) return;
+    free(s->x); free(s->v); free(s->omega); free(s->f); free(s->torque); free(s->radius); free(s->rmass);
+    free(s->type); free(s->tag); free(s->bins); free(s->binhead); free(s->stencil); free(s->xhold);
+    free(s->gsrc); free(s->gshift); free(s->maxrad);
+    free(s->nstart); free(s->nnum); free(s->nbr); free(s->flag); free(s->hist);
+    for (int i = 0; i < s->nmax; i++) { if (s->partner) free(s->partner[i]); if (s->phist) free(s->phist[i]); }
+    free(s->npartner); free(s->partner); free(s->phist);
+    for (int k = 0; k < s->nfix; k++) {
+        if (s->fix[k].wp) { free(s->fix[k].wp->list); free(s->fix[k].wp->hist); free(s->fix[k].wp); }
+        if (s->fix[k].wm) {
+            wall_mesh *m = s->fix[k].wm;
+            for (int t = 0; t < m->ntri; t++) { if (m->tri_list) free(m->tri_list[t]); if (m->tri_bins) free(m->tri_bins[t]); }
+            free(m->tri_list); free(m->tri_n); free(m->tri_cap); free(m->tri_bins); free(m->tri_nbins);
+            for (int i = 0; i < s->nmax; i++) {
+                if (m->partner) free(m->partner[i]);
+                if (m->chist) free(m->chist[i]);
+                if (m->keep) free(m->keep[i]);
+                if (m->isect) free(m->isect[i]);
+            }
+            free(m->nneighs); free(m->npartner); free(m->partner); free(m->chist); free(m->keep); free(m->isect);
+            free(m->node); free(m->center); free(m->rbound); free(m->edgevec); free(m->edgelen); free(m->edgenorm);
+            free(m->surfnorm); free(m->obtuse); free(m->edge_active); free(m->corner_active); free(m->nneigh); free(m->neighfaces);
+            free(m);
+        }
+    }
+    free_matrix(s->Yeff); free_matrix(s->Geff); free_matrix(s->betaeff); free_matrix(s->mu); free_matrix(s->mur);
+    free(s);
+}
+
+const char *orc_error(orc_sim *s) { return s->err; }
+int orc_nlocal(orc_sim *s) { return s->nlocal; }
+int orc_nghost(orc_sim *s) { return s->nghost; }
+long orc_ntimestep(orc_sim *s) { return s->ntimestep; }
+int orc_nbuilds(orc_sim *s) { return s->nbuilds; }
+
+/* ------------------------------------------------------------------ */
+/* fixes                                                                */
+
+int orc_add_gravity(orc_sim *s, double mag, double dx, double dy, double dz)
+{
+    /* src/fix_gravity.cpp:376-397 (style vector, 3d) */
+    fixrec *fr = &s->fix[s->nfix++];
+    fr->kind = ORC_FIX_GRAVITY;
+    double length = sqrt(dx*dx + dy*dy + dz*dz);
+    double xg = dx/length, yg = dy/length, zg = dz/length;
+    fr->xacc = mag*xg; fr->yacc = mag*yg; fr->zacc = mag*zg;
+    return s->nfix-1;
+}
+
+int orc_add_wall_plane(orc_sim *s, int dim, double pos, int wall_type, int rolling_cdt)
+{
+    fixrec *fr = &s->fix[s->nfix++];
+    fr->kind = ORC_FIX_WALL_PLANE;
+    wall_plane *w = calloc(1, sizeof(wall_plane));
+    w->dim = dim; w->pos = pos; w->wtype = wall_type; w->rolling = rolling_cdt;
+    w->hist = calloc((size_t)3*s->nmax, sizeof(double));
+    fr->wp = w;
+    return s->nfix-1;
+}
+
+/* forward decl */
+static void mesh_build_topology(orc_sim *s, wall_mesh *m);
+
+int orc_add_wall_mesh(orc_sim *s, int ntri, const double *nodes, int wall_type, double curvature, int rolling_cdt)
+{
+    fixrec *fr = &s->fix[s->nfix++];
+    fr->kind = ORC_FIX_WALL_MESH;
+    wall_mesh *m = calloc(1, sizeof(wall_mesh));
+    m->wtype = wall_type; m->rolling = rolling_cdt;
+    m->curvature = curvature > 0 ? curvature : 1.-0.00001;   /* src/surface_mesh_I.h:58 */
+    m->precision = EPSILON_PRECISION;
+    m->node = malloc(sizeof(double)*9*(ntri > 0 ? ntri : 1));
+    m->center = malloc(sizeof(double)*3*(ntri > 0 ? ntri : 1));
+    m->rbound = malloc(sizeof(double)*(ntri > 0 ? ntri : 1));
+    /* MultiNodeMesh::addElement src/multi_node_mesh_I.h:139-190 */
+    int n = 0;
+    for (int t = 0; t < ntri; t++) {
+        double nd[3][3];
+        memcpy(nd, nodes + 9*t, sizeof nd);
+        int eq = 0;
+        for (int a = 0; a < 3 && !eq; a++)
+            for (int b = a+1; b < 3 && !eq; b++) {
+                int all = 1;
+                for (int c = 0; c < 3; c++) if (!comp_double(nd[a][c], nd[b][c], m->precision)) all = 0;
+                if (all) eq = 1;
+            }
+        if (eq) continue;
+        memcpy(m->node[n], nd, sizeof nd);
+        double avg[3] = {0., 0., 0.};
+        for (int i = 0; i < 3; i++) { avg[0] = nd[i][0]+avg[0]; avg[1] = nd[i][1]+avg[1]; avg[2] = nd[i][2]+avg[2]; }
+        sdiv3(avg, 3.0);
+        memcpy(m->center[n], avg, sizeof avg);
+        double rb = 0.;
+        for (int i = 0; i < 3; i++) { double vec[3]; sub3(m->center[n], nd[i], vec); double mg = mag3(vec); rb = rb > mg ? rb : mg; }
+        m->rbound[n] = rb;
+        n++;
+    }
+    m->ntri = n;
+    mesh_build_topology(s, m);
+    m->tri_list = calloc(n > 0 ? n : 1, sizeof(int*));
+    m->tri_n = calloc(n > 0 ? n : 1, sizeof(int));
+    m->tri_cap = calloc(n > 0 ? n : 1, sizeof(int));
+    m->tri_bins = calloc(n > 0 ? n : 1, sizeof(int*));
+    m->tri_nbins = calloc(n > 0 ? n : 1, sizeof(int));
+    m->last_bin_update = -1;
+    m->nl_skin = -1; m->nl_distmax = -1;
+    m->nneighs = calloc(s->nmax, sizeof(int));
+    m->npartner = calloc(s->nmax, sizeof(int));
+    m->partner = calloc(s->nmax, sizeof(int*));
+    m->chist = calloc(s->nmax, sizeof(double*));
+    m->keep = calloc(s->nmax, sizeof(unsigned char*));
+    m->isect = calloc(s->nmax, sizeof(unsigned char*));
+    fr->wm = m;
+    return s->nfix-1;
+}
+
+/* ------------------------------------------------------------------ */
+/* mesh topology: src/surface_mesh_I.h:282-446 (element properties),
+   :453-555 buildNeighbours, :1035-1152 edges/corners                   */
+
+static int mesh_nodes_equal(wall_mesh *m, const double *a, const double *b)
+{
+    for (int i = 0; i < 3; i++) if (!comp_double(a[i], b[i], m->precision)) return 0;
+    return 1;
+}
+
+static int mesh_n_shared(wall_mesh *m, int a, int b)   /* src/multi_node_mesh_I.h:328 */
+{
+    double dist[3]; sub3(m->center[a], m->center[b], dist);
+    double radsum = m->rbound[a] + m->rbound[b];
+    if (dot3(dist, dist) > radsum*radsum) return 0;
+    int ns = 0;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) if (mesh_nodes_equal(m, m->node[a][i], m->node[b][j])) ns++;
+    return ns;
+}
+
+static int mesh_share_edge(wall_mesh *m, int a, int b, int *ie, int *je)  /* src/surface_mesh_I.h:1003 */
+{
+    double dist[3]; sub3(m->center[a], m->center[b], dist);
+    double radsum = m->rbound[a] + m->rbound[b];
+    if (dot3(dist, dist) > radsum*radsum) return 0;
+    int i1 = -1, j1 = -1, i2 = -1, j2 = -1, ns = 0;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++)
+        if (mesh_nodes_equal(m, m->node[a][i], m->node[b][j])) {
+            if (ns == 0) { i1 = i; j1 = j; }
+            else if (ns == 1) { i2 = i; j2 = j; goto found; }
+            ns++;
+        }
+    return 0;
+found:
+    *ie = (2 == i1+i2) ? 2 : (i1 < i2 ? i1 : i2);
+    *je = (2 == j1+j2) ? 2 : (j1 < j2 ? j1 : j2);
+    return 1;
+}
+
+static void mesh_build_topology(orc_sim *s, wall_mesh *m)
+{
+    const int n = m->ntri;
+    (void)s;
+    m->edgevec = malloc(sizeof(double)*9*(n?n:1)); m->edgelen = malloc(sizeof(double)*3*(n?n:1));
+    m->edgenorm = malloc(sizeof(double)*9*(n?n:1)); m->surfnorm = malloc(sizeof(double)*3*(n?n:1));
+    m->obtuse = malloc(sizeof(int)*(n?n:1));
+    m->edge_active = malloc(3*(n?n:1)); m->corner_active = malloc(3*(n?n:1));
+    m->nneigh = calloc(n?n:1, sizeof(int)); m->neighfaces = malloc(sizeof(int)*NEIGH_MAX*(n?n:1));
+    for (int t = 0; t < n; t++) {
+        /* calcEdgeVecLen :363 */
+        for (int i = 0; i < 3; i++) {
+            sub3(m->node[t][(i+1)%3], m->node[t][i], m->edgevec[t][i]);
+            m->edgelen[t][i] = mag3(m->edgevec[t][i]);
+            sdiv3(m->edgevec[t][i], m->edgelen[t][i]);
+        }
+        /* calcSurfaceNorm :375 (degenerate fallbacks omitted: duplicates removed) */
+        double *sn = m->surfnorm[t];
+        cross3(m->edgevec[t][0], m->edgevec[t][1], sn);
+        if (mag3(sn) < 1e-15) cross3(m->edgevec[t][1], m->edgevec[t][2], sn);
+        if (mag3(sn) < 1e-15) cross3(m->edgevec[t][2], m->edgevec[t][0], sn);
+        sdiv3(sn, mag3(sn));
+        /* calcEdgeNormals :417 */
+        for (int i = 0; i < 3; i++) {
+            cross3(m->edgevec[t][i], sn, m->edgenorm[t][i]);
+            if (mag3(m->edgenorm[t][i]) < 1e-15) memcpy(m->edgenorm[t][i], m->edgevec[t][(i+1)%3], sizeof(double)*3);
+            else sdiv3(m->edgenorm[t][i], mag3(m->edgenorm[t][i]));
+        }
+        /* calcObtuseAngleIndex :433, called for iNode = 0,1,2 -- each call
+           overwrites the element's index, so the last call decides */
+        m->obtuse[t] = NO_OBTUSE_ANGLE;
+        for (int i = 0; i < 3; i++) {
+            double d = dot3(m->edgevec[t][i], m->edgevec[t][(i+2)%3]);
+            m->obtuse[t] = (d > 0.) ? i : NO_OBTUSE_ANGLE;
+        }
+        for (int i = 0; i < 3; i++) { m->edge_active[t][i] = 1; m->corner_active[t][i] = 1; }
+        for (int i = 0; i < NEIGH_MAX; i++) m->neighfaces[t][i] = -1;
+    }
+    /* buildNeighbours: every pair sharing an edge (the bounding-sphere
+       overlap search of :505-524 finds every such pair); element ids are
+       the element indices (src/tracking_mesh_I.h:91) */
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++) {
+            int ie, je;
+            if (!mesh_share_edge(m, i, j, &ie, &je)) continue;
+            /* areCoplanar :844 */
+            int coplanar = fabs(dot3(m->surfnorm[i], m->surfnorm[j])) >= m->curvature;
+            /* handleSharedEdge :1035 (neighflag true) */
+            if (m->nneigh[i] < NEIGH_MAX) m->neighfaces[i][m->nneigh[i]] = j;
+            if (m->nneigh[j] < NEIGH_MAX) m->neighfaces[j][m->nneigh[j]] = i;
+            m->nneigh[i]++; m->nneigh[j]++;
+            int overlap = 0;
+            if (coplanar) {   /* coplanarNeighsOverlap :935 */
+                double pRef[3], edgeN[3], vecI[3], vecJ[3];
+                memcpy(pRef, m->node[i][ie], sizeof pRef);
+                memcpy(edgeN, m->edgenorm[i][ie], sizeof edgeN);
+                sub3(m->node[i][(ie+2)%3], pRef, vecI);
+                sub3(m->node[j][(je+2)%3], pRef, vecJ);
+                double d1 = dot3(vecI, edgeN), d2 = dot3(vecJ, edgeN);
+                overlap = d1*d2 > 0.;
+            }
+            if (!coplanar || overlap) {
+                if (i < j) { m->edge_active[i][ie] = 0; m->edge_active[j][je] = 1; }
+                else { m->edge_active[i][ie] = 1; m->edge_active[j][je] = 0; }
+            } else { m->edge_active[i][ie] = 0; m->edge_active[j][je] = 0; }
+        }
+    /* handleCorner :1109 with checkNodeRecursive :1159 (depth-first over
+       edge neighbours that contain the node) */
+    int *visited = malloc(sizeof(int)*(n?n:1)), *hasnode = malloc(sizeof(int)*(n?n:1));
+    int *stack = malloc(sizeof(int)*(n?n:1)*(NEIGH_MAX+1));
+    double (*edgelist)[3] = malloc(sizeof(double)*3*2*(n?n:1));
+    double (*endpt)[3] = malloc(sizeof(double)*3*2*(n?n:1));
+    unsigned char *vis = calloc(n?n:1, 1);
+    for (int t = 0; t < n; t++)
+        for (int inode = 0; inode < 3; inode++) {
+            double nc[3]; memcpy(nc, m->node[t][inode], sizeof nc);
+            int nvis = 0, nhas = 0, anyActive = 0, ne = 0;
+            /* recursion order does not change the sets collected */
+            int sp = 0; stack[sp++] = t;
+            while (sp > 0) {
+                int e = stack[--sp];
+                if (vis[e]) continue;
+                vis[e] = 1; visited[nvis++] = e;
+                int in = -1;
+                for (int q = 0; q < 3; q++)
+                    if (comp_double(m->node[e][q][0], nc[0], m->precision) && comp_double(m->node[e][q][1], nc[1], m->precision) &&
+                        comp_double(m->node[e][q][2], nc[2], m->precision)) { in = q; break; }
+                if (in < 0) continue;
+                hasnode[nhas++] = e;
+                memcpy(edgelist[ne], m->edgevec[e][in], sizeof(double)*3);
+                memcpy(endpt[ne], m->node[e][(in+1)%3], sizeof(double)*3); ne++;
+                memcpy(edgelist[ne], m->edgevec[e][(in+2)%3], sizeof(double)*3);
+                memcpy(endpt[ne], m->node[e][(in+2)%3], sizeof(double)*3); ne++;
+                if (m->edge_active[e][in]) anyActive = 1;
+                else if (m->edge_active[e][(in+2)%3]) anyActive = 1;
+                int nn = m->nneigh[e] < NEIGH_MAX ? m->nneigh[e] : NEIGH_MAX;
+                for (int k = nn-1; k >= 0; k--) { int nb = m->neighfaces[e][k]; if (nb >= 0 && !vis[nb]) stack[sp++] = nb; }
+            }
+            for (int q = 0; q < nvis; q++) vis[visited[q]] = 0;
+            int maxId = -1;
+            for (int q = 0; q < nhas; q++) maxId = maxId > hasnode[q] ? maxId : hasnode[q];
+            int colinear = 0;
+            for (int a = 0; a < ne; a++)
+                for (int b = a+1; b < ne; b++)
+                    if (fabs(dot3(edgelist[a], edgelist[b])) > m->curvature && !mesh_nodes_equal(m, endpt[a], endpt[b])) colinear = 1;
+            if (colinear || !anyActive) m->corner_active[t][inode] = 0;
+            else if (t == maxId) m->corner_active[t][inode] = 1;
+            else m->corner_active[t][inode] = 0;
+        }
+    free(visited); free(hasnode); free(stack); free(edgelist); free(endpt); free(vis);
+}
+
+/* areCoplanarNodeNeighs src/surface_mesh_I.h:892 */
+static int mesh_coplanar_node_neighs(wall_mesh *m, int a, int b)
+{
+    int areNeighs = 0;
+    int nn = m->nneigh[a] < NEIGH_MAX ? m->nneigh[a] : NEIGH_MAX;
+    for (int i = 0; i < nn; i++) if (m->neighfaces[a][i] == b) areNeighs = 1;
+    int found = 0;
+    if (!areNeighs) if (mesh_n_shared(m, a, b) != 0) found = 1;
+    if (!areNeighs && !found) return 0;
+    double d = dot3(m->surfnorm[a], m->surfnorm[b]);
+    return fabs(d) > m->curvature;
+}
+
+int orc_get_mesh_topology(orc_sim *s, int ifix, unsigned char *edge_active, unsigned char *corner_active, int *obtuse)
+{
+    wall_mesh *m = s->fix[ifix].wm;
+    if (!m) return -1;
+    for (int t = 0; t < m->ntri; t++) {
+        for (int i = 0; i < 3; i++) {
+            if (edge_active) edge_active[3*t+i] = m->edge_active[t][i];
+            if (corner_active) corner_active[3*t+i] = m->corner_active[t][i];
+        }
+        if (obtuse) obtuse[t] = m->obtuse[t];
+    }
+    return m->ntri;
+}
+
+/* ------------------------------------------------------------------ */
+/* neighbor: cutoffs src/neighbor.cpp:292-332, src/pair_gran.cpp:623;
+   bins src/neighbor.cpp:1642-1808; stencil src/neigh_stencil.cpp:116  */
+
+static void neighbor_init(orc_sim *s)
+{
+    const int nt = s->ntypes;
+    free(s->maxrad);
+    s->maxrad = calloc(nt+1, sizeof(double));
+    for (int i = 0; i < s->nlocal; i++)
+        if (s->radius[i] > s->maxrad[s->type[i]]) s->maxrad[s->type[i]] = s->radius[i];
+    s->triggersq = 0.25*s->p.skin*s->p.skin;
+    s->cutneighmax = 0.0;
+    for (int i = 1; i <= nt; i++)
+        for (int j = 1; j <= nt; j++) {
+            double cut = (s->maxrad[i]+s->maxrad[j]) * 1.0;   /* init_one * contactDistanceFactor */
+            double cutsq = cut*cut;
+            double cutoff = sqrt(cutsq);
+            double delta = cutoff > 0.0 ? s->p.skin : 0.0;
+            double c = cutoff + delta;
+            if (c > s->cutneighmax) s->cutneighmax = c;
+        }
+    s->cutneighmaxsq = s->cutneighmax * s->cutneighmax;
+    s->cutghost = s->cutneighmax;   /* src/comm.cpp:456, cutghostuser = 0 */
+}
+
+static double bin_distance(orc_sim *s, int i, int j, int k)
+{
+    double delx, dely, delz;
+    if (i > 0) delx = (i-1)*s->binsizex; else if (i == 0) delx = 0.0; else delx = (i+1)*s->binsizex;
+    if (j > 0) dely = (j-1)*s->binsizey; else if (j == 0) dely = 0.0; else dely = (j+1)*s->binsizey;
+    if (k > 0) delz = (k-1)*s->binsizez; else if (k == 0) delz = 0.0; else delz = (k+1)*s->binsizez;
+    return (delx*delx + dely*dely + delz*delz);
+}
+
+static void setup_bins(orc_sim *s)
+{
+    double bbox[3], bsubboxlo[3], bsubboxhi[3];
+    for (int d = 0; d < 3; d++) {
+        s->bboxlo[d] = s->boxlo[d]; s->bboxhi[d] = s->boxhi[d];
+        bsubboxlo[d] = s->boxlo[d] - s->cutghost;
+        bsubboxhi[d] = s->boxhi[d] + s->cutghost;
+        bbox[d] = s->bboxhi[d] - s->bboxlo[d];
+    }
+    double binsize_optimal = 0.5*s->cutneighmax;
+    if (binsize_optimal == 0.0) binsize_optimal = bbox[0];
+    double binsizeinv = 1.0/binsize_optimal;
+    s->nbinx = (int)(bbox[0]*binsizeinv);
+    s->nbiny = (int)(bbox[1]*binsizeinv);
+    s->nbinz = (int)(bbox[2]*binsizeinv);
+    if (s->nbinx == 0) s->nbinx = 1;
+    if (s->nbiny == 0) s->nbiny = 1;
+    if (s->nbinz == 0) s->nbinz = 1;
+    s->binsizex = bbox[0]/s->nbinx; s->binsizey = bbox[1]/s->nbiny; s->binsizez = bbox[2]/s->nbinz;
+    s->bininvx = 1.0 / s->binsizex; s->bininvy = 1.0 / s->binsizey; s->bininvz = 1.0 / s->binsizez;
+    int mbinxhi, mbinyhi, mbinzhi;
+    double coord;
+    coord = bsubboxlo[0] - SMALL*bbox[0];
+    s->mbinxlo = (int)((coord-s->bboxlo[0])*s->bininvx);
+    if (coord < s->bboxlo[0]) s->mbinxlo = s->mbinxlo - 1;
+    coord = bsubboxhi[0] + SMALL*bbox[0];
+    mbinxhi = (int)((coord-s->bboxlo[0])*s->bininvx);
+    coord = bsubboxlo[1] - SMALL*bbox[1];
+    s->mbinylo = (int)((coord-s->bboxlo[1])*s->bininvy);
+    if (coord < s->bboxlo[1]) s->mbinylo = s->mbinylo - 1;
+    coord = bsubboxhi[1] + SMALL*bbox[1];
+    mbinyhi = (int)((coord-s->bboxlo[1])*s->bininvy);
+    coord = bsubboxlo[2] - SMALL*bbox[2];
+    s->mbinzlo = (int)((coord-s->bboxlo[2])*s->bininvz);
+    if (coord < s->bboxlo[2]) s->mbinzlo = s->mbinzlo - 1;
+    coord = bsubboxhi[2] + SMALL*bbox[2];
+    mbinzhi = (int)((coord-s->bboxlo[2])*s->bininvz);
+    s->mbinxlo -= 1; mbinxhi += 1; s->mbinx = mbinxhi - s->mbinxlo + 1;
+    s->mbinylo -= 1; mbinyhi += 1; s->mbiny = mbinyhi - s->mbinylo + 1;
+    s->mbinzlo -= 1; mbinzhi += 1; s->mbinz = mbinzhi - s->mbinzlo + 1;
+    s->mbins = s->mbinx*s->mbiny*s->mbinz;
+    s->binhead = xrealloc(s->binhead, sizeof(int)*s->mbins);
+    int sx = (int)(s->cutneighmax*s->bininvx); if (sx*s->binsizex < s->cutneighmax) sx++;
+    int sy = (int)(s->cutneighmax*s->bininvy); if (sy*s->binsizey < s->cutneighmax) sy++;
+    int sz = (int)(s->cutneighmax*s->bininvz); if (sz*s->binsizez < s->cutneighmax) sz++;
+    int smax = (2*sx+1)*(2*sy+1)*(2*sz+1);
+    s->stencil = xrealloc(s->stencil, sizeof(int)*smax);
+    s->nstencil = 0;
+    for (int k = -sz; k <= sz; k++)
+        for (int j = -sy; j <= sy; j++)
+            for (int i = -sx; i <= sx; i++)
+                if (bin_distance(s, i, j, k) < s->cutneighmaxsq)
+                    s->stencil[s->nstencil++] = k*s->mbiny*s->mbinx + j*s->mbinx + i;
+}
+
+/* src/neighbor.cpp:2112 (index triple relative to mbin*lo) */
+static int coord2bin3(orc_sim *s, const double *x, int *ix, int *iy, int *iz)
+{
+    if (x[0] >= s->bboxhi[0]) *ix = (int)((x[0]-s->bboxhi[0])*s->bininvx) + s->nbinx;
+    else if (x[0] >= s->bboxlo[0]) { *ix = (int)((x[0]-s->bboxlo[0])*s->bininvx); if (*ix > s->nbinx-1) *ix = s->nbinx-1; }
+    else *ix = (int)((x[0]-s->bboxlo[0])*s->bininvx) - 1;
+    if (x[1] >= s->bboxhi[1]) *iy = (int)((x[1]-s->bboxhi[1])*s->bininvy) + s->nbiny;
+    else if (x[1] >= s->bboxlo[1]) { *iy = (int)((x[1]-s->bboxlo[1])*s->bininvy); if (*iy > s->nbiny-1) *iy = s->nbiny-1; }
+    else *iy = (int)((x[1]-s->bboxlo[1])*s->bininvy) - 1;
+    if (x[2] >= s->bboxhi[2]) *iz = (int)((x[2]-s->bboxhi[2])*s->bininvz) + s->nbinz;
+    else if (x[2] >= s->bboxlo[2]) { *iz = (int)((x[2]-s->bboxlo[2])*s->bininvz); if (*iz > s->nbinz-1) *iz = s->nbinz-1; }
+    else *iz = (int)((x[2]-s->bboxlo[2])*s->bininvz) - 1;
+    *ix -= s->mbinxlo; *iy -= s->mbinylo; *iz -= s->mbinzlo;
+    return (*iz)*s->mbiny*s->mbinx + (*iy)*s->mbinx + (*ix);
+}
+
+static int coord2bin(orc_sim *s, const double *x)   /* src/neighbor.cpp:2077 */
+{
+    int ix, iy, iz;
+    return coord2bin3(s, x, &ix, &iy, &iz);
+}
+
+static void bin_atoms(orc_sim *s)   /* src/neighbor.cpp:2027 */
+{
+    for (int i = 0; i < s->mbins; i++) s->binhead[i] = -1;
+    int nall = s->nlocal + s->nghost;
+    for (int i = nall-1; i >= 0; i--) {
+        int ibin = coord2bin(s, &s->x[3*i]);
+        s->bins[i] = s->binhead[ibin];
+        s->binhead[ibin] = i;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* domain / comm                                                        */
+
+static void domain_pbc(orc_sim *s)   /* src/domain.cpp:530 */
+{
+    for (int i = 0; i < s->nlocal; i++)
+        for (int d = 0; d < 3; d++) {
+            if (!s->p.periodic[d]) continue;
+            double *xc = &s->x[3*i+d];
+            if (*xc < s->boxlo[d]) *xc += s->prd[d];
+            if (*xc >= s->boxhi[d]) { *xc -= s->prd[d]; if (*xc < s->boxlo[d]) *xc = s->boxlo[d]; }
+        }
+}
+
+static int comm_exchange_check(orc_sim *s)   /* src/comm.cpp:901, one proc */
+{
+    for (int i = 0; i < s->nlocal; i++)
+        for (int d = 0; d < 3; d++)
+            if (s->x[3*i+d] < s->boxlo[d] || s->x[3*i+d] >= s->boxhi[d]) {
+                fail(s, "atom tag %d left the box in dim %d (lost atoms are not supported)", s->tag[i], d);
+                return -1;
+            }
+    return 0;
+}
+
+/* Comm::borders src/comm.cpp:1028 with Comm::decide src/comm_I.h:66 and
+   the swap slabs of Comm::setup src/comm.cpp:655-712 (one proc) */
+static void comm_borders(orc_sim *s)
+{
+    s->nghost = 0;
+    s->nswap = 0;
+    const double c = s->cutghost / 2. + s->p.skin/2.;
+    int nlast = 0;
+    for (int dim = 0; dim < 3; dim++) {
+        if (!s->p.periodic[dim]) continue;   /* maxneed = 0 for a non-periodic dim with one proc */
+        nlast = 0;
+        int nfirst = 0;
+        for (int ineed = 0; ineed < 2; ineed++) {
+            double lo, hi, shift;
+            if (ineed % 2 == 0) { lo = -BIG; hi = s->boxlo[dim] + c; shift = 1*s->prd[dim]; }
+            else { lo = s->boxhi[dim] - c; hi = BIG; shift = -1*s->prd[dim]; }
+            if (ineed % 2 == 0) { nfirst = nlast; nlast = s->nlocal + s->nghost; }
+            (void)nfirst;
+            int first = s->nlocal + s->nghost;
+            int nsend = 0;
+            for (int i = 0; i < nlast; i++) {
+                double xd = s->x[3*i+dim];
+                int send = (ineed % 2 == 0) ? (xd >= lo && xd <= (hi + s->radius[i]))
+                                            : (xd >= (lo - s->radius[i]) && xd <= hi);
+                if (!send) continue;
+                int g = first + nsend;
+                if (g >= s->nmax) grow_all(s, 2*s->nmax);
+                s->gsrc = xrealloc(s->gsrc, sizeof(int)*(g - s->nlocal + 1));
+                s->gshift = xrealloc(s->gshift, sizeof(double)*3*(g - s->nlocal + 1));
+                int gi = g - s->nlocal;
+                s->gsrc[gi] = i;
+                double sh[3] = {0.0, 0.0, 0.0}; sh[dim] = shift;
+                /* dx = pbc[0]*xprd etc: only the swap dimension is nonzero */
+                for (int d = 0; d < 3; d++) { s->gshift[3*gi+d] = (d == dim) ? shift : 0*s->prd[d]; s->x[3*g+d] = s->x[3*i+d] + s->gshift[3*gi+d]; }
+                (void)sh;
+                s->v[3*g] = s->v[3*i]; s->v[3*g+1] = s->v[3*i+1]; s->v[3*g+2] = s->v[3*i+2];
+                s->omega[3*g] = s->omega[3*i]; s->omega[3*g+1] = s->omega[3*i+1]; s->omega[3*g+2] = s->omega[3*i+2];
+                s->radius[g] = s->radius[i]; s->rmass[g] = s->rmass[i]; s->type[g] = s->type[i]; s->tag[g] = s->tag[i];
+                nsend++;
+            }
+            s->swapfirst[s->nswap] = first; s->swapnum[s->nswap] = nsend; s->nswap++;
+            s->nghost += nsend;
+        }
+    }
+}
+
+static void comm_forward(orc_sim *s)   /* src/comm.cpp:773 with pack_comm_vel */
+{
+    for (int gi = 0; gi < s->nghost; gi++) {
+        int g = s->nlocal + gi, i = s->gsrc[gi];
+        for (int d = 0; d < 3; d++) s->x[3*g+d] = s->x[3*i+d] + s->gshift[3*gi+d];
+        for (int d = 0; d < 3; d++) { s->v[3*g+d] = s->v[3*i+d]; s->omega[3*g+d] = s->omega[3*i+d]; }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* atom sort src/atom.cpp:1309-1398, bins :1405-1480                    */
+
+static void setup_sort_bins(orc_sim *s)
+{
+    double binsize = s->p.sortbinsize > 0.0 ? s->p.sortbinsize : 0.5 * s->cutneighmax;
+    double bininv = 1.0/binsize;
+    for (int d = 0; d < 3; d++) s->sbboxlo[d] = s->boxlo[d];
+    s->snbinx = (int)((s->boxhi[0]-s->boxlo[0]) * bininv);
+    s->snbiny = (int)((s->boxhi[1]-s->boxlo[1]) * bininv);
+    s->snbinz = (int)((s->boxhi[2]-s->boxlo[2]) * bininv);
+    if (s->snbinx == 0) s->snbinx = 1;
+    if (s->snbiny == 0) s->snbiny = 1;
+    if (s->snbinz == 0) s->snbinz = 1;
+    s->sbininvx = s->snbinx / (s->boxhi[0]-s->boxlo[0]);
+    s->sbininvy = s->snbiny / (s->boxhi[1]-s->boxlo[1]);
+    s->sbininvz = s->snbinz / (s->boxhi[2]-s->boxlo[2]);
+}
+
+#define PERMUTE(arr, type, width) do { type *tmp_ = malloc(sizeof(type)*(width)*(size_t)(n>0?n:1)); \
+    for (int q_ = 0; q_ < n; q_++) memcpy(tmp_ + (size_t)(width)*q_, (arr) + (size_t)(width)*perm[q_], sizeof(type)*(width)); \
+    memcpy((arr), tmp_, sizeof(type)*(width)*(size_t)n); free(tmp_); } while (0)
+
+static void atom_sort(orc_sim *s)
+{
+    s->nextsort = (s->ntimestep/s->p.sortfreq)*s->p.sortfreq + s->p.sortfreq;
+    int nbins = s->snbinx*s->snbiny*s->snbinz;
+    if (nbins == 1) return;
+    const int n = s->nlocal;
+    int *binhead = malloc(sizeof(int)*nbins), *next = malloc(sizeof(int)*(n>0?n:1)), *perm = malloc(sizeof(int)*(n>0?n:1));
+    for (int i = 0; i < nbins; i++) binhead[i] = -1;
+    for (int i = n-1; i >= 0; i--) {
+        int ix = (int)((s->x[3*i]-s->sbboxlo[0])*s->sbininvx);
+        int iy = (int)((s->x[3*i+1]-s->sbboxlo[1])*s->sbininvy);
+        int iz = (int)((s->x[3*i+2]-s->sbboxlo[2])*s->sbininvz);
+        if (ix < 0) ix = 0; if (iy < 0) iy = 0; if (iz < 0) iz = 0;
+        if (ix > s->snbinx-1) ix = s->snbinx-1; if (iy > s->snbiny-1) iy = s->snbiny-1; if (iz > s->snbinz-1) iz = s->snbinz-1;
+        int ibin = iz*s->snbiny*s->snbinx + iy*s->snbinx + ix;
+        next[i] = binhead[ibin]; binhead[ibin] = i;
+    }
+    int k = 0;
+    for (int m = 0; m < nbins; m++) for (int i = binhead[m]; i >= 0; i = next[i]) perm[k++] = i;
+    /* perm[new] = old; every per-atom array moves with its atom */
+    PERMUTE(s->x, double, 3); PERMUTE(s->v, double, 3); PERMUTE(s->omega, double, 3);
+    PERMUTE(s->f, double, 3); PERMUTE(s->torque, double, 3);
+    PERMUTE(s->radius, double, 1); PERMUTE(s->rmass, double, 1);
+    PERMUTE(s->type, int, 1); PERMUTE(s->tag, int, 1);
+    PERMUTE(s->npartner, int, 1); PERMUTE(s->partner, int*, 1); PERMUTE(s->phist, double*, 1);
+    for (int q = 0; q < s->nfix; q++) {
+        if (s->fix[q].wp) PERMUTE(s->fix[q].wp->hist, double, 3);
+        if (s->fix[q].wm) {
+            wall_mesh *m = s->fix[q].wm;
+            PERMUTE(m->nneighs, int, 1); PERMUTE(m->npartner, int, 1); PERMUTE(m->partner, int*, 1);
+            PERMUTE(m->chist, double*, 1); PERMUTE(m->keep, unsigned char*, 1); PERMUTE(m->isect, unsigned char*, 1);
+        }
+    }
+    free(binhead); free(next); free(perm);
+}
+
+/* ------------------------------------------------------------------ */
+/* FixContactHistory::pre_exchange src/fix_contact_history.cpp:305-425 */
+
+static void history_pre_exchange(orc_sim *s)
+{
+    s->computeflag = 0;
+    const int nl = s->nlocal;
+    for (int i = 0; i < nl; i++) { free(s->partner[i]); free(s->phist[i]); s->partner[i] = NULL; s->phist[i] = NULL; s->npartner[i] = 0; }
+    int inum = s->npairs > 0 || nl > 0 ? nl : 0;
+    int nlocal_neigh = inum;  /* ilist[inum-1]+1 */
+    int *cnt = calloc(nl > 0 ? nl : 1, sizeof(int));
+    for (int i = 0; i < nl; i++)
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            int e = s->nstart[i] + jj;
+            if (s->flag[e]) { cnt[i]++; int j = s->nbr[e]; if (j < nlocal_neigh) cnt[j]++; }
+        }
+    for (int i = 0; i < nl; i++) {
+        s->partner[i] = malloc(sizeof(int)*(cnt[i] > 0 ? cnt[i] : 1));
+        s->phist[i] = malloc(sizeof(double)*3*(cnt[i] > 0 ? cnt[i] : 1));
+    }
+    for (int i = 0; i < nl; i++)
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            int e = s->nstart[i] + jj;
+            if (!s->flag[e]) continue;
+            double *h = &s->hist[3*e];
+            int j = s->nbr[e];
+            int m = s->npartner[i];
+            s->partner[i][m] = s->tag[j];
+            for (int d = 0; d < 3; d++) s->phist[i][3*m+d] = h[d];
+            s->npartner[i]++;
+            if (j < nlocal_neigh) {
+                m = s->npartner[j];
+                s->partner[j][m] = s->tag[i];
+                for (int d = 0; d < 3; d++) s->phist[j][3*m+d] = -h[d];   /* newtonflag = 1 for shear */
+                s->npartner[j]++;
+            }
+        }
+    free(cnt);
+}
+
+/* ------------------------------------------------------------------ */
+/* Neighbor::granular_bin_no_newton src/neigh_gran.cpp:485-639         */
+
+static void neighbor_build(orc_sim *s)
+{
+    s->ago = 0;
+    s->nbuilds++;
+    for (int i = 0; i < 3*s->nlocal; i++) s->xhold[i] = s->x[i];
+    bin_atoms(s);
+    const int nl = s->nlocal;
+    s->nstart = xrealloc(s->nstart, sizeof(int)*(nl > 0 ? nl : 1));
+    s->nnum = xrealloc(s->nnum, sizeof(int)*(nl > 0 ? nl : 1));
+    s->npairs = 0;
+    const double skin = s->p.skin;
+    for (int i = 0; i < nl; i++) {
+        s->nstart[i] = s->npairs;
+        int n = 0;
+        const double xtmp = s->x[3*i], ytmp = s->x[3*i+1], ztmp = s->x[3*i+2];
+        const double radi = s->radius[i];
+        int ibin = coord2bin(s, &s->x[3*i]);
+        for (int k = 0; k < s->nstencil; k++)
+            for (int j = s->binhead[ibin+s->stencil[k]]; j >= 0; j = s->bins[j]) {
+                if (j <= i) continue;
+                double delx = xtmp - s->x[3*j], dely = ytmp - s->x[3*j+1], delz = ztmp - s->x[3*j+2];
+                double rsq = delx*delx + dely*dely + delz*delz;
+                double radsum = (radi + s->radius[j]) * 1.0;
+                double cutsq = (radsum+skin) * (radsum+skin);
+                if (rsq <= cutsq) {
+                    if (s->npairs >= s->cappairs) {
+                        s->cappairs = s->cappairs ? 2*s->cappairs : 1024;
+                        s->nbr = xrealloc(s->nbr, sizeof(int)*s->cappairs);
+                        s->flag = xrealloc(s->flag, sizeof(int)*s->cappairs);
+                        s->hist = xrealloc(s->hist, sizeof(double)*3*s->cappairs);
+                    }
+                    int e = s->npairs++;
+                    s->nbr[e] = j;
+                    int m = 0;
+                    if (rsq < radsum*radsum) {
+                        for (m = 0; m < s->npartner[i]; m++) if (s->partner[i][m] == s->tag[j]) break;
+                        if (m < s->npartner[i]) {
+                            s->flag[e] = 1;
+                            for (int d = 0; d < 3; d++) s->hist[3*e+d] = s->phist[i][3*m+d];
+                        } else {
+                            s->flag[e] = 0;
+                            for (int d = 0; d < 3; d++) s->hist[3*e+d] = 0.0;
+                        }
+                    } else {
+                        s->flag[e] = 0;
+                        for (int d = 0; d < 3; d++) s->hist[3*e+d] = 0.0;
+                    }
+                    n++;
+                }
+            }
+        s->nnum[i] = n;
+    }
+}
+
+/* Neighbor::decide / check_distance src/neighbor.cpp:1357-1460 */
+static int neighbor_decide(orc_sim *s)
+{
+    s->ago++;
+    if (s->ago >= s->p.delay && s->ago % s->p.every == 0) {
+        if (!s->p.check) return 1;
+        const double deltasq = s->triggersq;
+        int flag = 0;
+        for (int i = 0; i < s->nlocal; i++) {
+            double delx = s->x[3*i] - s->xhold[3*i];
+            double dely = s->x[3*i+1] - s->xhold[3*i+1];
+            double delz = s->x[3*i+2] - s->xhold[3*i+2];
+            double rsq = delx*delx + dely*dely + delz*delz;
+            if (rsq > deltasq) flag = 1;
+        }
+        return flag;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* pair compute src/pair_gran_base.h:187-430                            */
+
+static void pair_compute(orc_sim *s, int shearupdate)
+{
+    s->computeflag = 1;
+    for (int i = 0; i < s->nlocal; i++) {
+        const double xtmp = s->x[3*i], ytmp = s->x[3*i+1], ztmp = s->x[3*i+2];
+        const double radi = s->radius[i];
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            const int e = s->nstart[i] + jj;
+            const int j = s->nbr[e];
+            const double delx = xtmp - s->x[3*j], dely = ytmp - s->x[3*j+1], delz = ztmp - s->x[3*j+2];
+            const double rsq = delx * delx + dely * dely + delz * delz;
+            const double radj = s->radius[j];
+            const double radsum = radi + radj;
+            if (!(rsq < radsum * radsum)) continue;   /* surfacesClose unreachable with cdf = 1 */
+            sidata_t sd; memset(&sd, 0, sizeof sd);
+            force_t fi, fj; memset(&fi, 0, sizeof fi); memset(&fj, 0, sizeof fj);
+            sd.is_wall = 0;
+            sd.radi = radi; sd.radj = radj; sd.radsum = radsum; sd.rsq = rsq;
+            sd.delta[0] = delx; sd.delta[1] = dely; sd.delta[2] = delz;
+            sd.contact_flags = &s->flag[e];
+            sd.contact_history = &s->hist[3*e];
+            sd.v_i = &s->v[3*i]; sd.v_j = &s->v[3*j];
+            sd.itype = s->type[i]; sd.jtype = s->type[j];
+            sd.computeflag = 1; sd.shearupdate = shearupdate;
+            const double r = sqrt(rsq);
+            const double rinv = 1.0 / r;
+            const double mi = s->rmass[i], mj = s->rmass[j];
+            const double meff = mi * mj / (mi + mj);
+            sd.r = r; sd.rinv = rinv; sd.meff = meff; sd.mi = mi; sd.mj = mj;
+            sd.en[0] = delx * rinv; sd.en[1] = dely * rinv; sd.en[2] = delz * rinv;
+            sd.omega_i = &s->omega[3*i]; sd.omega_j = &s->omega[3*j];
+            contact_chain(s, &sd, &fi, &fj, s->p.rolling_cdt);
+            for (int c = 0; c < 3; c++) { s->f[3*i+c] += 1.0*fi.F[c]; s->torque[3*i+c] += 1.0*fi.T[c]; }
+            if (j < s->nlocal)
+                for (int c = 0; c < 3; c++) { s->f[3*j+c] += 1.0*fj.F[c]; s->torque[3*j+c] += 1.0*fj.T[c]; }
+        }
+    }
+}
+
+void orc_pair_force(const orc_params *p, const double xi[3], const double xj[3], const double vi[3], const double vj[3],
+                    const double wi[3], const double wj[3], double ri, double rj, double mi, double mj, int ti, int tj,
+                    double shear[3], int shearupdate, double fi_out[3], double ti_out[3], double fj_out[3], double tj_out[3])
+{
+    orc_sim tmp; memset(&tmp, 0, sizeof tmp);
+    tmp.p = *p; tmp.ntypes = p->ntypes; setup_materials(&tmp);
+    sidata_t sd; memset(&sd, 0, sizeof sd);
+    force_t fi, fj; memset(&fi, 0, sizeof fi); memset(&fj, 0, sizeof fj);
+    const double delx = xi[0]-xj[0], dely = xi[1]-xj[1], delz = xi[2]-xj[2];
+    const double rsq = delx*delx + dely*dely + delz*delz;
+    int flagv = 0;
+    if (rsq < (ri+rj)*(ri+rj)) {
+        sd.radi = ri; sd.radj = rj; sd.radsum = ri+rj; sd.rsq = rsq;
+        sd.delta[0] = delx; sd.delta[1] = dely; sd.delta[2] = delz;
+        sd.contact_flags = &flagv; sd.contact_history = shear;
+        sd.v_i = vi; sd.v_j = vj; sd.itype = ti; sd.jtype = tj; sd.computeflag = 1; sd.shearupdate = shearupdate;
+        const double r = sqrt(rsq), rinv = 1.0/r;
+        sd.r = r; sd.rinv = rinv; sd.meff = mi*mj/(mi+mj); sd.mi = mi; sd.mj = mj;
+        sd.en[0] = delx*rinv; sd.en[1] = dely*rinv; sd.en[2] = delz*rinv;
+        sd.omega_i = wi; sd.omega_j = wj;
+        contact_chain(&tmp, &sd, &fi, &fj, p->rolling_cdt);
+    }
+    for (int c = 0; c < 3; c++) { fi_out[c] = fi.F[c]; ti_out[c] = fi.T[c]; fj_out[c] = fj.F[c]; tj_out[c] = fj.T[c]; }
+    free_matrix(tmp.Yeff); free_matrix(tmp.Geff); free_matrix(tmp.betaeff); free_matrix(tmp.mu); free_matrix(tmp.mur);
+}
+
+/* ------------------------------------------------------------------ */
+/* walls: Walls::Granular::compute_force src/fix_wall_gran_base.h:148  */
+
+static void wall_compute_force(orc_sim *s, int ip, sidata_t *sd, const double *vwall, int wtype, int rolling, int shearupdate)
+{
+    force_t fi, fj; memset(&fi, 0, sizeof fi); memset(&fj, 0, sizeof fj);
+    sd->v_i = &s->v[3*ip]; sd->v_j = vwall; sd->omega_i = &s->omega[3*ip];
+    sd->r = sd->radi - sd->deltan;
+    sd->rsq = sd->r*sd->r;
+    const double rinv = 1.0/sd->r;
+    sd->rinv = rinv;
+    sd->contact_flags = NULL;
+    sd->itype = s->type[ip];
+    sd->meff = s->rmass[ip]; sd->mi = s->rmass[ip];
+    sd->computeflag = 1; sd->shearupdate = shearupdate;
+    sd->jtype = wtype;
+    sd->en[0] = sd->delta[0] * rinv; sd->en[1] = sd->delta[1] * rinv; sd->en[2] = sd->delta[2] * rinv;
+    sd->radsum = sd->radi;
+    contact_chain(s, sd, &fi, &fj, rolling);
+    for (int c = 0; c < 3; c++) { s->f[3*ip+c] += fi.F[c]; s->torque[3*ip+c] += fi.T[c]; }
+}
+
+/* FixWallGran::pre_force (primitive neighlist) src/fix_wall_gran.cpp:708,
+   PrimitiveWall::buildNeighList src/primitive_wall.h:129,
+   Plane::resolveNeighlist src/primitive_wall_definitions.h:145 */
+static void wall_plane_pre_force(orc_sim *s, wall_plane *w)
+{
+    if (!w->rebuild) return;
+    w->rebuild = 0;
+    w->nlist = 0;
+    for (int i = 0; i < s->nlocal; i++) {
+        double dMax = s->radius[i] + s->p.skin;
+        double dist = s->x[3*i+w->dim] - w->pos;
+        double absdist = (dist > 0.0) ? dist : -dist;
+        if (absdist <= dMax) {
+            if (w->nlist >= w->caplist) { w->caplist = w->caplist ? 2*w->caplist : 256; w->list = xrealloc(w->list, sizeof(int)*w->caplist); }
+            w->list[w->nlist++] = i;
+        }
+    }
+}
+
+/* FixWallGran::post_force_primitive src/fix_wall_gran.cpp:1024-1148 */
+static void wall_plane_post_force(orc_sim *s, wall_plane *w, int shearupdate)
+{
+    const double vwall[3] = {0., 0., 0.};
+    for (int ic = 0; ic < w->nlist; ic++) {
+        int ip = w->list[ic];
+        sidata_t sd; memset(&sd, 0, sizeof sd);
+        sd.is_wall = 1;
+        sd.radi = s->radius[ip];
+        /* Plane<dim>::resolveContact src/primitive_wall_definitions.h:133 */
+        double delta[3] = {0., 0., 0.}, deltan;
+        const double *pos = &s->x[3*ip];
+        delta[w->dim] = w->pos - pos[w->dim];
+        if (pos[w->dim] > w->pos) deltan = pos[w->dim] - w->pos - sd.radi;
+        else deltan = w->pos - pos[w->dim] - sd.radi;
+        if (deltan > s->cutneighmax) continue;
+        double *hist = &w->hist[3*ip];
+        if (deltan <= 0 || deltan < 0.0*s->radius[ip]) {
+            sd.contact_history = hist;
+            sd.deltan = -deltan;
+            sd.delta[0] = -delta[0]; sd.delta[1] = -delta[1]; sd.delta[2] = -delta[2];
+            wall_compute_force(s, ip, &sd, vwall, w->wtype, w->rolling, shearupdate);
+        } else {
+            hist[0] = hist[1] = hist[2] = 0.0;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* mesh neighbor list: FixNeighlistMesh src/fix_neighlist_mesh.cpp:230-503,
+   TriMesh::resolveTriSphereNeighbuild src/tri_mesh_I.h:255-283          */
+
+static double dist_to_plane(const double *p, const double *pPlane, const double *nPlane)
+{
+    double v[3]; sub3(p, pPlane, v); return dot3(nPlane, v);
+}
+
+static int tri_sphere_neighbuild(wall_mesh *m, int t, double rSphere, const double *cSphere, double treshold)
+{
+    double maxDist = rSphere + treshold;
+    double dNorm = fabs(dist_to_plane(cSphere, m->center[t], m->surfnorm[t]));
+    if (dNorm > maxDist) return 0;
+    double dParaMax = maxDist*maxDist;
+    for (int i = 0; i < 3; i++) {
+        double d = dist_to_plane(cSphere, m->node[t][i], m->edgenorm[t][i]);
+        if (d > 0 && d*d > dParaMax) return 0;
+    }
+    return 1;
+}
+
+static void mesh_bin_bounds(orc_sim *s, wall_mesh *m, int t, int *lo, int *hi)
+{
+    /* getElementBoundingBoxOnSubdomain + getBinBoundariesFromBoundingBox */
+    double blo[3], bhi[3];
+    for (int d = 0; d < 3; d++) { blo[d] = BIG; bhi[d] = -BIG; }
+    for (int i = 0; i < 3; i++)
+        for (int d = 0; d < 3; d++) {
+            if (m->node[t][i][d] < blo[d]) blo[d] = m->node[t][i][d];
+            if (m->node[t][i][d] > bhi[d]) bhi[d] = m->node[t][i][d];
+        }
+    for (int d = 0; d < 3; d++) {   /* shrinkToSubbox */
+        if (blo[d] < s->boxlo[d]) blo[d] = s->boxlo[d];
+        if (bhi[d] > s->boxhi[d]) bhi[d] = s->boxhi[d];
+    }
+    double delta = m->nl_distmax;
+    double tmin[3] = {blo[0]-delta, blo[1]-delta, blo[2]-delta};
+    double tmax[3] = {bhi[0]+delta, bhi[1]+delta, bhi[2]+delta};
+    coord2bin3(s, tmin, &lo[0], &lo[1], &lo[2]);
+    coord2bin3(s, tmax, &hi[0], &hi[1], &hi[2]);
+}
+
+static void mesh_neighlist_pre_force(orc_sim *s, wall_mesh *m)
+{
+    if (!m->build_neighlist_nl) return;
+    m->build_neighlist_nl = 0;
+    for (int i = 0; i < s->nlocal + s->nghost; i++) m->nneighs[i] = 0;
+    /* static mesh, non-changing domain */
+    double prev_skin = m->nl_skin, prev_distmax = m->nl_distmax;
+    double rmax = 0.5*(s->cutneighmax - s->p.skin);
+    m->nl_skin = 0.5*s->p.skin;
+    m->nl_distmax = s->cutneighmax - rmax + m->nl_skin/(70.*M_PI);
+    if (m->nl_skin != prev_skin || m->nl_distmax != prev_distmax || m->last_bin_update < 0) {
+        /* generate_bin_list :456 */
+        double dx = s->binsizex / 2.0, dy = s->binsizey / 2.0, dz = s->binsizez / 2.0;
+        double maxdiag = sqrt(dx * dx + dy * dy + dz * dz);
+        for (int t = 0; t < m->ntri; t++) {
+            int lo[3], hi[3];
+            mesh_bin_bounds(s, m, t, lo, hi);
+            m->tri_nbins[t] = 0;
+            int cap = 0; free(m->tri_bins[t]); m->tri_bins[t] = NULL;
+            for (int ix = lo[0]; ix <= hi[0]; ix++)
+                for (int iy = lo[1]; iy <= hi[1]; iy++)
+                    for (int iz = lo[2]; iz <= hi[2]; iz++) {
+                        int iBin = iz*s->mbiny*s->mbinx + iy*s->mbinx + ix;
+                        if (iBin < 0 || iBin >= s->mbins) continue;
+                        double center[3];
+                        center[0] = (s->mbinxlo + ix + 0.5) * s->binsizex + s->bboxlo[0];
+                        center[1] = (s->mbinylo + iy + 0.5) * s->binsizey + s->bboxlo[1];
+                        center[2] = (s->mbinzlo + iz + 0.5) * s->binsizez + s->bboxlo[2];
+                        if (tri_sphere_neighbuild(m, t, maxdiag, center, m->nl_distmax + m->nl_skin)) {
+                            if (m->tri_nbins[t] >= cap) { cap = cap ? 2*cap : 16; m->tri_bins[t] = xrealloc(m->tri_bins[t], sizeof(int)*cap); }
+                            m->tri_bins[t][m->tri_nbins[t]++] = iBin;
+                        }
+                    }
+        }
+        m->last_bin_update = s->ntimestep;
+    }
+    for (int t = 0; t < m->ntri; t++) {
+        m->tri_n[t] = 0;
+        if (!s->nlocal) continue;
+        for (int b = 0; b < m->tri_nbins[t]; b++) {
+            int iBin = m->tri_bins[t][b];
+            for (int ia = s->binhead[iBin]; ia != -1; ia = s->bins[ia]) {
+                /* (iAtom > nlocal) && !periodic ghost: every ghost here is periodic */
+                if (tri_sphere_neighbuild(m, t, s->radius[ia]*1.0, &s->x[3*ia], m->nl_skin)) {
+                    if (m->tri_n[t] >= m->tri_cap[t]) { m->tri_cap[t] = m->tri_cap[t] ? 2*m->tri_cap[t] : 8; m->tri_list[t] = xrealloc(m->tri_list[t], sizeof(int)*m->tri_cap[t]); }
+                    m->tri_list[t][m->tri_n[t]++] = ia;
+                    m->nneighs[ia]++;
+                }
+            }
+        }
+    }
+}
+
+/* FixContactHistoryMesh::sort_contacts src/fix_contact_history_mesh.cpp:375 */
+static void mesh_swap(wall_mesh *m, int i, int a, int b, int keepswap)
+{
+    int t = m->partner[i][a]; m->partner[i][a] = m->partner[i][b]; m->partner[i][b] = t;
+    double h[3]; memcpy(h, &m->chist[i][3*a], sizeof h);
+    memcpy(&m->chist[i][3*a], &m->chist[i][3*b], sizeof h);
+    memcpy(&m->chist[i][3*b], h, sizeof h);
+    if (keepswap) {
+        unsigned char k = m->keep[i][a]; m->keep[i][a] = m->keep[i][b]; m->keep[i][b] = k;
+        k = m->isect[i][a]; m->isect[i][a] = m->isect[i][b]; m->isect[i][b] = k;
+    }
+}
+
+static void mesh_sort_contacts(orc_sim *s, wall_mesh *m)
+{
+    for (int i = 0; i < s->nlocal; i++) {
+        int nn = m->nneighs[i];
+        if (0 == nn) continue;
+        int fe, lf;
+        do {
+            fe = lf = -1;
+            for (int j = 0; j < nn; j++) {
+                if (-1 == fe && -1 == m->partner[i][j]) fe = j;
+                if (m->partner[i][j] >= 0) lf = j;
+            }
+            if (fe > -1 && lf > -1 && fe < lf) mesh_swap(m, i, fe, lf, 1);
+        } while (fe > -1 && lf > -1 && fe < lf);
+    }
+}
+
+static int tri_contains_atom(wall_mesh *m, int t, int i)   /* FixNeighlistMesh::contactInList */
+{
+    for (int k = 0; k < m->tri_n[t]; k++) if (m->tri_list[t][k] == i) return 1;
+    return 0;
+}
+
+/* FixContactHistoryMesh::pre_force src/fix_contact_history_mesh.cpp:315-373
+   with cleanUpContactJumps :466 */
+static void mesh_history_pre_force(orc_sim *s, wall_mesh *m)
+{
+    if (!m->build_neighlist_ch) return;
+    m->build_neighlist_ch = 0;
+    const int nl = s->nlocal;
+    for (int i = 0; i < nl; i++) {
+        int ip = 0;
+        while (ip < m->npartner[i]) {
+            int tri = m->partner[i][ip];
+            if (tri < 0) { fail(s, "mesh history internal error"); return; }
+            if (!tri_contains_atom(m, tri, i)) {
+                m->partner[i][ip] = -1;
+                m->chist[i][3*ip] = m->chist[i][3*ip+1] = m->chist[i][3*ip+2] = 0.0;
+                mesh_swap(m, i, ip, m->npartner[i]-1, 0);
+                m->npartner[i]--;
+            } else ip++;
+        }
+    }
+    for (int i = 0; i < nl; i++) {
+        int nn = m->nneighs[i];
+        int *np = malloc(sizeof(int)*(nn > 0 ? nn : 1));
+        double *nh = calloc((size_t)3*(nn > 0 ? nn : 1), sizeof(double));
+        for (int k = 0; k < nn; k++) np[k] = -1;
+        if (m->npartner[i] > nn) { fail(s, "mesh history internal error (npartner > nneighs)"); free(np); free(nh); return; }
+        for (int k = 0; k < m->npartner[i]; k++) {
+            np[k] = m->partner[i][k];
+            memcpy(&nh[3*k], &m->chist[i][3*k], sizeof(double)*3);
+        }
+        free(m->partner[i]); free(m->chist[i]);
+        m->partner[i] = np; m->chist[i] = nh;
+        free(m->keep[i]); free(m->isect[i]);
+        m->keep[i] = calloc(nn > 0 ? nn : 1, 1);
+        m->isect[i] = calloc(nn > 0 ? nn : 1, 1);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* triangle-sphere narrow phase src/tri_mesh_I.h:65-251                 */
+
+static double calc_dist(const double *cs, const double *cp, double *delta)
+{
+    sub3(cp, cs, delta);
+    double d2 = (cs[0]-cp[0]) * (cs[0]-cp[0]) + (cs[1]-cp[1]) * (cs[1]-cp[1]) + (cs[2]-cp[2]) * (cs[2]-cp[2]);
+    return sqrt(d2);
+}
+
+static double resolve_edge(wall_mesh *m, int t, int iEdge, const double *p, double *delta, double *bary)
+{
+    int ip = (iEdge+1)%3, ipp = (iEdge+2)%3;
+    double nodeToP[3], d;
+    double (*n)[3] = m->node[t];
+    sub3(p, n[iEdge], nodeToP);
+    double distFromNode = dot3(nodeToP, m->edgevec[t][iEdge]);
+    if (distFromNode < -SMALL_TRIMESH) {
+        if (!m->corner_active[t][iEdge]) return LARGE_TRIMESH;
+        d = calc_dist(p, n[iEdge], delta);
+        bary[iEdge] = 1.; bary[ip] = 0.; bary[ipp] = 0.;
+    } else if (distFromNode > m->edgelen[t][iEdge] + SMALL_TRIMESH) {
+        if (!m->corner_active[t][ip]) return LARGE_TRIMESH;
+        d = calc_dist(p, n[ip], delta);
+        bary[iEdge] = 0.; bary[ip] = 1.; bary[ipp] = 0.;
+    } else {
+        double cp[3];
+        if (!m->edge_active[t][iEdge]) return LARGE_TRIMESH;
+        cp[0] = n[iEdge][0]+distFromNode*m->edgevec[t][iEdge][0];
+        cp[1] = n[iEdge][1]+distFromNode*m->edgevec[t][iEdge][1];
+        cp[2] = n[iEdge][2]+distFromNode*m->edgevec[t][iEdge][2];
+        d = calc_dist(p, cp, delta);
+        bary[ipp] = 0.;
+        bary[iEdge] = 1. - distFromNode/m->edgelen[t][iEdge];
+        bary[ip] = 1. - bary[iEdge];
+    }
+    return d;
+}
+
+static double resolve_corner(wall_mesh *m, int t, int iNode, int obtuse, const double *p, double *delta, double *bary)
+{
+    int ip = (iNode+1)%3, ipp = (iNode+2)%3;
+    const double *n = m->node[t][iNode];
+    if (obtuse) {
+        double (*edge)[3] = m->edgevec[t];
+        double nodeToP[3], cp[3];
+        sub3(p, n, nodeToP);
+        double distFromNode = dot3(nodeToP, edge[ipp]);
+        if (distFromNode < SMALL_TRIMESH) {
+            if (distFromNode > -m->edgelen[t][ipp]) {
+                if (!m->edge_active[t][ipp]) return LARGE_TRIMESH;
+                cp[0] = n[0]+distFromNode*edge[ipp][0]; cp[1] = n[1]+distFromNode*edge[ipp][1]; cp[2] = n[2]+distFromNode*edge[ipp][2];
+                bary[ip] = 0.;
+                bary[iNode] = 1. + distFromNode/m->edgelen[t][ipp];
+                bary[ipp] = 1. - bary[iNode];
+                return calc_dist(p, cp, delta);
+            } else {
+                if (!m->corner_active[t][ipp]) return LARGE_TRIMESH;
+                bary[ipp] = 1.; bary[iNode] = bary[ip] = 0.;
+                return calc_dist(p, m->node[t][ipp], delta);
+            }
+        }
+        distFromNode = dot3(nodeToP, edge[iNode]);
+        if (distFromNode > -SMALL_TRIMESH) {
+            if (distFromNode < m->edgelen[t][iNode]) {
+                if (!m->edge_active[t][iNode]) return LARGE_TRIMESH;
+                cp[0] = n[0]+distFromNode*edge[iNode][0]; cp[1] = n[1]+distFromNode*edge[iNode][1]; cp[2] = n[2]+distFromNode*edge[iNode][2];
+                bary[ipp] = 0.;
+                bary[iNode] = 1. - distFromNode/m->edgelen[t][iNode];
+                bary[ip] = 1. - bary[iNode];
+                return calc_dist(p, cp, delta);
+            } else {
+                if (!m->corner_active[t][ip]) return LARGE_TRIMESH;
+                bary[ip] = 1.; bary[iNode] = bary[ipp] = 0.;
+                return calc_dist(p, m->node[t][ip], delta);
+            }
+        }
+    }
+    if (!m->corner_active[t][iNode]) return LARGE_TRIMESH;
+    bary[iNode] = 1.; bary[ip] = bary[ipp] = 0.;
+    return calc_dist(p, m->node[t][iNode], delta);
+}
+
+static double resolve_tri_sphere(wall_mesh *m, int t, double rSphere, const double *cs, double *delta, double *bary, int *barySign)
+{
+    int obt = m->obtuse[t];
+    bary[0] = bary[1] = bary[2] = 0.;
+    double n0ToC[3];
+    sub3(cs, m->node[t][0], n0ToC);
+    /* calcBaryTriCoords src/math_extra_liggghts.h:559 */
+    double a = dot3(n0ToC, m->edgevec[t][0]);
+    double b = dot3(n0ToC, m->edgevec[t][2]);
+    double c = dot3(m->edgevec[t][0], m->edgevec[t][2]);
+    double oneMinCSqr = 1 - c*c;
+    bary[1] = (a - b*c)/(m->edgelen[t][0] * oneMinCSqr);
+    bary[2] = (a*c - b)/(m->edgelen[t][2] * oneMinCSqr);
+    bary[0] = 1. - bary[1] - bary[2];
+    double invlen = 1./(2.*m->rbound[t]);
+    double prec = m->precision;
+    *barySign = (bary[0] > -prec*invlen) + 2*(bary[1] > -prec*invlen) + 4*(bary[2] > -prec*invlen);
+    double d = 0.;
+    switch (*barySign) {
+    case 1: d = resolve_corner(m, t, 0, obt == 0, cs, delta, bary); break;
+    case 2: d = resolve_corner(m, t, 1, obt == 1, cs, delta, bary); break;
+    case 3: d = resolve_edge(m, t, 0, cs, delta, bary); break;
+    case 4: d = resolve_corner(m, t, 2, obt == 2, cs, delta, bary); break;
+    case 5: d = resolve_edge(m, t, 2, cs, delta, bary); break;
+    case 6: d = resolve_edge(m, t, 1, cs, delta, bary); break;
+    case 7: {
+        const double *sn = m->surfnorm[t];
+        double dNorm = dot3(sn, n0ToC);
+        double tmp[3] = {dNorm*sn[0], dNorm*sn[1], dNorm*sn[2]};
+        double csPlane[3]; sub3(cs, tmp, csPlane);
+        d = calc_dist(cs, csPlane, delta);
+        break;
+    }
+    default: d = 1.; break;
+    }
+    return d - rSphere;
+}
+
+/* ------------------------------------------------------------------ */
+/* FixWallGran::post_force_mesh src/fix_wall_gran.cpp:845-1018 with
+   FixContactHistoryMesh::handleContact src/fix_contact_history_mesh_I.h:51-216 */
+
+static int mesh_handle_contact(orc_sim *s, wall_mesh *m, int iP, int idTri, double **history, int intersect, int faceflag)
+{
+    const int nn = m->nneighs[iP];
+    for (int i = 0; i < nn; i++)
+        if (m->partner[iP][i] == idTri) {
+            *history = &m->chist[iP][3*i];
+            m->keep[iP][i] = 1; m->isect[iP][i] = (unsigned char)intersect;
+            return 1;
+        }
+    if (faceflag) {   /* coplanarContactAlready */
+        for (int i = 0; i < nn; i++) {
+            int idp = m->partner[iP][i];
+            if (idp >= 0 && idp != idTri && mesh_coplanar_node_neighs(m, idp, idTri))
+                if (m->keep[iP][i]) return 0;
+        }
+    }
+    /* addNewTriContactToExistingParticle */
+    int ic = -1;
+    if (m->npartner[iP] >= nn) { fail(s, "mesh history: npartner >= nneighs"); return 0; }
+    for (int k = 0; k < nn; k++) if (-1 == m->partner[iP][k]) { ic = k; break; }
+    if (ic < 0) { fail(s, "mesh history: no free slot"); return 0; }
+    m->partner[iP][ic] = idTri; m->keep[iP][ic] = 1; m->isect[iP][ic] = (unsigned char)intersect;
+    *history = &m->chist[iP][3*ic];
+    (*history)[0] = (*history)[1] = (*history)[2] = 0.0;
+    m->npartner[iP]++;
+    if (faceflag) {   /* checkCoplanarContactHistory */
+        for (int i = 0; i < nn; i++) {
+            int tri = m->partner[iP][i];
+            if (tri >= 0 && tri != idTri && mesh_coplanar_node_neighs(m, tri, idTri))
+                memcpy(*history, &m->chist[iP][3*i], sizeof(double)*3);
+        }
+    }
+    return 1;
+}
+
+static void mesh_post_force(orc_sim *s, wall_mesh *m, int shearupdate)
+{
+    const int nl = s->nlocal;
+    /* markAllContacts */
+    for (int i = 0; i < nl; i++) memset(m->keep[i], 0, m->nneighs[i] > 0 ? m->nneighs[i] : 0);
+    const double vwall[3] = {0., 0., 0.};
+    for (int t = 0; t < m->ntri; t++) {
+        for (int ic = 0; ic < m->tri_n[t]; ic++) {
+            const int ip = m->tri_list[t][ic];
+            if (ip >= nl) continue;
+            double delta[3], bary[3]; int barysign = -1;
+            sidata_t sd; memset(&sd, 0, sizeof sd);
+            sd.is_wall = 1;
+            sd.radi = s->radius[ip];
+            double deltan = resolve_tri_sphere(m, t, sd.radi, &s->x[3*ip], delta, bary, &barysign);
+            if (deltan > s->cutneighmax) continue;
+            int intersectflag = (deltan <= 0);
+            if (deltan <= 0 || (deltan < 0.0*s->radius[ip])) {
+                double *hist = NULL;
+                if (!mesh_handle_contact(s, m, ip, t, &hist, intersectflag, 7 == barysign)) continue;
+                sd.deltan = -deltan;
+                sd.delta[0] = -delta[0]; sd.delta[1] = -delta[1]; sd.delta[2] = -delta[2];
+                sd.contact_history = hist;
+                wall_compute_force(s, ip, &sd, vwall, m->wtype, m->rolling, shearupdate);
+            }
+        }
+    }
+    /* cleanUpContacts :437 */
+    for (int i = 0; i < nl; i++)
+        for (int j = 0; j < m->nneighs[i]; j++)
+            if (!m->keep[i][j]) {
+                if (m->partner[i][j] > -1) m->npartner[i]--;
+                m->partner[i][j] = -1;
+                m->isect[i][j] = 0;
+                m->chist[i][3*j] = m->chist[i][3*j+1] = m->chist[i][3*j+2] = 0.0;
+            }
+}
+
+/* ------------------------------------------------------------------ */
+/* integrate src/fix_nve_sphere.cpp:138-246                             */
+
+static void nve_initial(orc_sim *s)
+{
+    const double dtv = s->p.dt, dtf = 0.5 * s->p.dt * 1.0;
+    const double dtfrotate = dtf / 0.4;
+    for (int i = 0; i < s->nlocal; i++) {
+        double dtfm = dtf / (s->rmass[i]*1.0);
+        s->v[3*i] += dtfm * s->f[3*i]; s->v[3*i+1] += dtfm * s->f[3*i+1]; s->v[3*i+2] += dtfm * s->f[3*i+2];
+        s->x[3*i] += dtv * s->v[3*i]; s->x[3*i+1] += dtv * s->v[3*i+1]; s->x[3*i+2] += dtv * s->v[3*i+2];
+        double dtirotate = dtfrotate / (s->radius[i]*s->radius[i]*s->rmass[i]);
+        s->omega[3*i] += dtirotate * s->torque[3*i]; s->omega[3*i+1] += dtirotate * s->torque[3*i+1]; s->omega[3*i+2] += dtirotate * s->torque[3*i+2];
+    }
+}
+
+static void nve_final(orc_sim *s)
+{
+    const double dtf = 0.5 * s->p.dt * 1.0;
+    const double dtfrotate = dtf / 0.4;
+    for (int i = 0; i < s->nlocal; i++) {
+        double dtfm = dtf / (s->rmass[i]*1.0);
+        s->v[3*i] += dtfm * s->f[3*i]; s->v[3*i+1] += dtfm * s->f[3*i+1]; s->v[3*i+2] += dtfm * s->f[3*i+2];
+        double dtirotate = dtfrotate / (s->radius[i]*s->radius[i]*s->rmass[i]);
+        s->omega[3*i] += dtirotate * s->torque[3*i]; s->omega[3*i+1] += dtirotate * s->torque[3*i+1]; s->omega[3*i+2] += dtirotate * s->torque[3*i+2];
+    }
+}
+
+static void gravity_post_force(orc_sim *s, fixrec *fr)   /* src/fix_gravity.cpp:301-337 */
+{
+    for (int i = 0; i < s->nlocal; i++) {
+        double massone = s->rmass[i] * 1.;
+        s->f[3*i] += massone*fr->xacc; s->f[3*i+1] += massone*fr->yacc; s->f[3*i+2] += massone*fr->zacc;
+    }
+}
+
+static void force_clear(orc_sim *s)
+{
+    int nall = s->nlocal + s->nghost;
+    memset(s->f, 0, sizeof(double)*3*nall);
+    memset(s->torque, 0, sizeof(double)*3*nall);
+}
+
+static void post_force_all(orc_sim *s, int shearupdate)
+{
+    for (int k = 0; k < s->nfix; k++) {
+        fixrec *fr = &s->fix[k];
+        if (fr->kind == ORC_FIX_GRAVITY) gravity_post_force(s, fr);
+        else if (fr->kind == ORC_FIX_WALL_PLANE) wall_plane_post_force(s, fr->wp, shearupdate);
+        else if (fr->kind == ORC_FIX_WALL_MESH) mesh_post_force(s, fr->wm, shearupdate);
+    }
+}
+
+static void pre_force_all(orc_sim *s)
+{
+    for (int k = 0; k < s->nfix; k++) {
+        fixrec *fr = &s->fix[k];
+        if (fr->kind == ORC_FIX_WALL_PLANE) wall_plane_pre_force(s, fr->wp);
+        else if (fr->kind == ORC_FIX_WALL_MESH) { mesh_neighlist_pre_force(s, fr->wm); mesh_history_pre_force(s, fr->wm); }
+    }
+}
+
+static void pre_neighbor_all(orc_sim *s)
+{
+    for (int k = 0; k < s->nfix; k++) {
+        fixrec *fr = &s->fix[k];
+        if (fr->kind == ORC_FIX_WALL_PLANE) fr->wp->rebuild = 1;
+        else if (fr->kind == ORC_FIX_WALL_MESH) { fr->wm->build_neighlist_nl = 1; fr->wm->build_neighlist_ch = 1; }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Verlet::setup src/verlet.cpp:134-197                                 */
+
+int orc_setup(orc_sim *s)
+{
+    s->setupflag = 1;
+    grow_all(s, 4*s->nlocal + 64);
+    for (int i = 0; i < s->nlocal; i++)
+        if (s->radius[i] == 0.0) { fail(s, "Fix nve/sphere requires extended particles"); return -1; }
+    neighbor_init(s);
+    if (s->p.sortfreq > 0) setup_sort_bins(s);
+    /* setup_pre_exchange: FixContactHistory only if computeflag; mesh sort */
+    if (s->computeflag) history_pre_exchange(s);
+    for (int k = 0; k < s->nfix; k++) if (s->fix[k].wm) mesh_sort_contacts(s, s->fix[k].wm);
+    domain_pbc(s);
+    setup_bins(s);
+    if (comm_exchange_check(s)) return -1;
+    if (s->p.sortfreq > 0) atom_sort(s);
+    comm_borders(s);
+    pre_neighbor_all(s);
+    neighbor_build(s);
+    force_clear(s);
+    pre_force_all(s);
+    pair_compute(s, 0);
+    post_force_all(s, 0);
+    s->setupflag = 0;
+    return s->err[0] ? -1 : 0;
+}
+
+/* Verlet::run src/verlet.cpp:264-388 */
+int orc_run(orc_sim *s, int nsteps)
+{
+    for (int step = 0; step < nsteps; step++) {
+        s->ntimestep++;
+        nve_initial(s);
+        int nflag = neighbor_decide(s);
+        if (nflag == 0) comm_forward(s);
+        else {
+            history_pre_exchange(s);
+            for (int k = 0; k < s->nfix; k++) if (s->fix[k].wm) mesh_sort_contacts(s, s->fix[k].wm);
+            domain_pbc(s);
+            if (comm_exchange_check(s)) return -1;
+            if (s->p.sortfreq > 0 && s->ntimestep >= s->nextsort) atom_sort(s);
+            comm_borders(s);
+            pre_neighbor_all(s);
+            neighbor_build(s);
+        }
+        force_clear(s);
+        pre_force_all(s);
+        pair_compute(s, 1);
+        post_force_all(s, 1);
+        nve_final(s);
+        if (s->err[0]) return -1;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* accessors                                                            */
+
+void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega, double *f, double *torque, int *tag)
+{
+    int n = s->nlocal;
+    if (x) memcpy(x, s->x, sizeof(double)*3*n);
+    if (v) memcpy(v, s->v, sizeof(double)*3*n);
+    if (omega) memcpy(omega, s->omega, sizeof(double)*3*n);
+    if (f) memcpy(f, s->f, sizeof(double)*3*n);
+    if (torque) memcpy(torque, s->torque, sizeof(double)*3*n);
+    if (tag) memcpy(tag, s->tag, sizeof(int)*n);
+}
+
+int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist)
+{
+    int k = 0;
+    for (int i = 0; i < s->nlocal; i++)
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            int e = s->nstart[i] + jj;
+            if (k < cap) {
+                if (tag_i) tag_i[k] = s->tag[i];
+                if (tag_j) tag_j[k] = s->tag[s->nbr[e]];
+                if (flag) flag[k] = s->flag[e];
+                if (hist) memcpy(&hist[3*k], &s->hist[3*e], sizeof(double)*3);
+            }
+            k++;
+        }
+    return k;
+}
+
+int orc_get_wall_hist(orc_sim *s, int ifix, double *hist)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wp) return -1;
+    memcpy(hist, s->fix[ifix].wp->hist, sizeof(double)*3*s->nlocal);
+    return s->nlocal;
+}
+
+int orc_get_mesh_contacts(orc_sim *s, int ifix, int cap, int *tag, int *tri, double *hist)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    int k = 0;
+    for (int i = 0; i < s->nlocal; i++)
+        for (int j = 0; j < m->nneighs[i]; j++) {
+            if (!m->partner[i] || m->partner[i][j] < 0) continue;
+            if (k < cap) {
+                if (tag) tag[k] = s->tag[i];
+                if (tri) tri[k] = m->partner[i][j];
+                if (hist) memcpy(&hist[3*k], &m->chist[i][3*j], sizeof(double)*3);
+            }
+            k++;
+        }
+    return k;
+}
+
+int orc_get_mesh_nneighs(orc_sim *s, int ifix, int *nneighs)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    memcpy(nneighs, s->fix[ifix].wm->nneighs, sizeof(int)*s->nlocal);
+    return s->nlocal;
+}

@@ -1,0 +1,233 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use this
+module, and only as the checker.  The oracle restates the reference algorithm
+(LIGGGHTS-PUBLIC 3.8.0); see gran_oracle.h for its parity status.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+D = ctypes.POINTER(ctypes.c_double)
+I = ctypes.POINTER(ctypes.c_int)
+U8 = ctypes.POINTER(ctypes.c_ubyte)
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("ntypes", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("skin", ctypes.c_double),
+        ("boxlo", ctypes.c_double * 3),
+        ("boxhi", ctypes.c_double * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("every", ctypes.c_int),
+        ("delay", ctypes.c_int),
+        ("check", ctypes.c_int),
+        ("sortfreq", ctypes.c_int),
+        ("sortbinsize", ctypes.c_double),
+        ("rolling_cdt", ctypes.c_int),
+        ("tangential_damping", ctypes.c_int),
+        ("youngs", D),
+        ("poisson", D),
+        ("restitution", D),
+        ("friction", D),
+        ("rollfriction", D),
+    ]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int, D, D, D, D, D, I, I]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_add_gravity.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 4
+        L.orc_add_wall_plane.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_add_wall_mesh.argtypes = [ctypes.c_void_p, ctypes.c_int, D, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.orc_setup.argtypes = [ctypes.c_void_p]
+        L.orc_run.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        for fn in ("orc_nlocal", "orc_nghost", "orc_nbuilds"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.orc_ntimestep.restype = ctypes.c_long
+        L.orc_ntimestep.argtypes = [ctypes.c_void_p]
+        L.orc_get_atoms.argtypes = [ctypes.c_void_p, D, D, D, D, D, I]
+        L.orc_get_pairs.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, I, D]
+        L.orc_get_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
+        L.orc_get_mesh_contacts.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
+        L.orc_get_mesh_topology.argtypes = [ctypes.c_void_p, ctypes.c_int, U8, U8, I]
+        L.orc_get_mesh_nneighs.argtypes = [ctypes.c_void_p, ctypes.c_int, I]
+        L.orc_error.restype = ctypes.c_char_p
+        L.orc_error.argtypes = [ctypes.c_void_p]
+        L.orc_pair_force.argtypes = [ctypes.POINTER(OrcParams), D, D, D, D, D, D, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, D, ctypes.c_int,
+                                     D, D, D, D]
+        _LIB = L
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(I)
+
+
+def make_params(sc):
+    """OrcParams from a scenario dict (see the package's scenarios module)."""
+    keep = []
+    p = OrcParams()
+    p.ntypes = sc["ntypes"]
+    p.dt = sc["dt"]
+    p.skin = sc["skin"]
+    for d in range(3):
+        p.boxlo[d] = sc["boxlo"][d]
+        p.boxhi[d] = sc["boxhi"][d]
+        p.periodic[d] = int(sc["periodic"][d])
+    p.every, p.delay, p.check = sc.get("every", 1), sc.get("delay", 0), sc.get("check", 1)
+    p.sortfreq = sc.get("sortfreq", 1000)
+    p.sortbinsize = sc.get("sortbinsize", 0.0)
+    p.rolling_cdt = int(sc.get("rolling_cdt", 0))
+    p.tangential_damping = int(sc.get("tangential_damping", 1))
+    for name in ("youngs", "poisson", "restitution", "friction", "rollfriction"):
+        arr = np.ascontiguousarray(np.asarray(sc[name], dtype=np.float64).ravel())
+        keep.append(arr)
+        setattr(p, name, _dp(arr))
+    return p, keep
+
+
+class Oracle:
+    """One oracle simulation built from a scenario dict."""
+
+    def __init__(self, sc):
+        L = lib()
+        self.L = L
+        self.p, self._keep = make_params(sc)
+        a = sc["atoms"]
+        self._arrs = {k: np.ascontiguousarray(a[k], dtype=np.float64) for k in ("x", "v", "omega", "radius", "rmass")}
+        self._type = np.ascontiguousarray(a["type"], dtype=np.int32)
+        self._tag = np.ascontiguousarray(a["tag"], dtype=np.int32)
+        n = len(self._tag)
+        self.h = L.orc_create(ctypes.byref(self.p), n, _dp(self._arrs["x"]), _dp(self._arrs["v"]),
+                              _dp(self._arrs["omega"]), _dp(self._arrs["radius"]), _dp(self._arrs["rmass"]),
+                              _ip(self._type), _ip(self._tag))
+        self.fix_ids = []
+        for fx in sc["fixes"]:
+            kind = fx["kind"]
+            if kind == "gravity":
+                d = fx["vector"]
+                k = L.orc_add_gravity(self.h, fx["magnitude"], d[0], d[1], d[2])
+            elif kind == "wall_plane":
+                k = L.orc_add_wall_plane(self.h, fx["dim"], fx["pos"], fx["wall_type"], int(fx.get("rolling_cdt", 0)))
+            elif kind == "wall_mesh":
+                nodes = np.ascontiguousarray(fx["nodes"], dtype=np.float64)
+                self._keep.append(nodes)
+                k = L.orc_add_wall_mesh(self.h, nodes.shape[0], _dp(nodes), fx["wall_type"],
+                                        fx.get("curvature", 0.0), int(fx.get("rolling_cdt", 0)))
+            elif kind == "nve_sphere":
+                k = None   # the oracle always integrates with fix nve/sphere
+            else:
+                raise ValueError(kind)
+            self.fix_ids.append(k)
+
+    def close(self):
+        if self.h:
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError("oracle: " + self.L.orc_error(self.h).decode())
+
+    def setup(self):
+        self._check(self.L.orc_setup(self.h))
+
+    def run(self, n):
+        self._check(self.L.orc_run(self.h, n))
+
+    @property
+    def nlocal(self):
+        return self.L.orc_nlocal(self.h)
+
+    @property
+    def nbuilds(self):
+        return self.L.orc_nbuilds(self.h)
+
+    def atoms(self):
+        n = self.nlocal
+        out = {k: np.zeros((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
+        tag = np.zeros(n, dtype=np.int32)
+        self.L.orc_get_atoms(self.h, _dp(out["x"]), _dp(out["v"]), _dp(out["omega"]), _dp(out["f"]),
+                             _dp(out["torque"]), _ip(tag))
+        out["tag"] = tag
+        return out
+
+    def pairs(self):
+        n = self.L.orc_get_pairs(self.h, 0, None, None, None, None)
+        ti = np.zeros(n, dtype=np.int32)
+        tj = np.zeros(n, dtype=np.int32)
+        fl = np.zeros(n, dtype=np.int32)
+        hi = np.zeros((n, 3))
+        self.L.orc_get_pairs(self.h, n, _ip(ti), _ip(tj), _ip(fl), _dp(hi))
+        return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def wall_hist(self, ifix):
+        n = self.nlocal
+        h = np.zeros((n, 3))
+        self.L.orc_get_wall_hist(self.h, self.fix_ids[ifix], _dp(h))
+        return h
+
+    def mesh_contacts(self, ifix):
+        k = self.fix_ids[ifix]
+        n = self.L.orc_get_mesh_contacts(self.h, k, 0, None, None, None)
+        tag = np.zeros(n, dtype=np.int32)
+        tri = np.zeros(n, dtype=np.int32)
+        h = np.zeros((n, 3))
+        self.L.orc_get_mesh_contacts(self.h, k, n, _ip(tag), _ip(tri), _dp(h))
+        return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_topology(self, ifix, ntri_max):
+        k = self.fix_ids[ifix]
+        ea = np.zeros(3 * ntri_max, dtype=np.uint8)
+        ca = np.zeros(3 * ntri_max, dtype=np.uint8)
+        ob = np.zeros(ntri_max, dtype=np.int32)
+        n = self.L.orc_get_mesh_topology(self.h, k, ea.ctypes.data_as(U8), ca.ctypes.data_as(U8), _ip(ob))
+        return ea[:3 * n].reshape(n, 3), ca[:3 * n].reshape(n, 3), ob[:n]
+
+    def mesh_nneighs(self, ifix):
+        n = self.nlocal
+        out = np.zeros(n, dtype=np.int32)
+        self.L.orc_get_mesh_nneighs(self.h, self.fix_ids[ifix], _ip(out))
+        return out
+
+
+def pair_force(sc, xi, xj, vi, vj, wi, wj, ri, rj, mi, mj, ti=1, tj=1, shear=None, shearupdate=1):
+    """Single-pair force through the oracle's contact chain (for known-answer tests)."""
+    L = lib()
+    p, keep = make_params(sc)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xi, xj, vi, vj, wi, wj)]
+    sh = np.zeros(3) if shear is None else np.ascontiguousarray(shear, dtype=np.float64)
+    outs = [np.zeros(3) for _ in range(4)]
+    L.orc_pair_force(ctypes.byref(p), *[_dp(a) for a in arrs], ri, rj, mi, mj, ti, tj, _dp(sh), shearupdate,
+                     *[_dp(o) for o in outs])
+    return outs[0], outs[1], outs[2], outs[3], sh
