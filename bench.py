@@ -1,0 +1,355 @@
+"""Benchmark of the granular hot path: particle-steps/s on the 1M-sphere
+Hertz/history + rolling-friction hopper with a triangulated mesh wall.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload hopper|pour] [--n N] [--settle S]
+
+Own arm: the workload is generated (seeded), uploaded, set up and settled for
+S steps, then W warm-up steps run untimed and K steps are timed with CUDA
+events on the engine's stream, bracketed by a barrier and device syncs.
+``value`` = particles x K / device time (whole job, summed over ranks).
+Multi-GPU: every rank runs an independent replica (different seed) -- the
+domain-decomposed multi-GPU path is not built, see DESIGN.md.
+
+Reference arm (--impl reference): the CPU oracle (a restatement of the
+reference's own CPU algorithm) on rank 0, on the host cores, timed on a
+bounded number of steps of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "liggghts-public_b200", "python"))
+
+METRIC = "particle-steps/s @1M spheres Hertz/history+mesh, 1 B200 vs plain FP64 GPU & host-CPU ref"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--workload", default="hopper", choices=["hopper", "pour"])
+    ap.add_argument("--n", type=int, default=0, help="particle count (default: 1M hopper, 20k pour)")
+    ap.add_argument("--settle", type=int, default=200, help="untimed settling steps before warm-up")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(args, seed_offset=0):
+    import gb2_scenarios as S
+    if args.workload == "hopper":
+        n = args.n or 1_000_000
+        sc = S.hopper(n=n, seed=2024 + seed_offset, gap=0.01, vmax=0.05)
+        ntri = len(sc["fixes"][1]["nodes"])
+        desc = ("hopper-%d: %d polydisperse spheres (lognormal r, median 1 mm, sigma 0.25, clip 0.5-2 mm), "
+                "Hertz/history + rolling cdt, conical mesh hopper %d triangles (60 deg, 30 mm outlet), "
+                "plane catch floor, dt 5e-6" % (n, n, ntri))
+        return sc, desc, {"n_particles": n, "triangles": ntri}
+    n = args.n or 20000
+    sc = S.sphere_pour(n=n, seed=12345 + seed_offset)
+    desc = "sphere-pour-%d: monodisperse r=1 mm, Hertz/history, periodic x/y, plane floor, dt 1e-5" % n
+    return sc, desc, {"n_particles": n, "triangles": 0}
+
+
+# --------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.p = None
+        self.out = None
+        try:
+            self.out = open(os.devnull if False else "/tmp/gb2_clocks_%d.csv" % os.getpid(), "w")
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                       "-i", str(device), "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.out.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.out.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.out.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- roofline
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(kernel, n, cen, nfix_plane, nfix_mesh):
+    """Algorithmic HBM bytes per launch (model in DESIGN.md): owned-atom
+    records, list indices and shear history that must cross HBM once;
+    neighbour-state gathers are served from L2 and not counted."""
+    avg = lambda k: 0.5 * (cen[0][k] + cen[1][k])
+    if kernel == "k_pair_main":
+        per_atom = 92 + 48 + 4 + 48 + 48 + nfix_plane * 1 + nfix_mesh * 4
+        b = n * per_atom + avg("nlist") * 4 + avg("ntouch") * 52
+        b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
+        return b
+    if kernel == "k_pair_reverse":
+        return n * (92 + 4 + 48) + avg("nrev") * 4 + avg("ntouch") * 24
+    raise ValueError(kernel)
+
+
+def load_traffic(kernel, workload):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            d = json.load(fh)
+        e = d.get(workload, {}).get(kernel)
+        return e
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------- CPU oracle
+
+def run_oracle_sample(sc, target_s, max_steps):
+    """Time the oracle (single thread) on sc: setup + 2 warm-up steps untimed,
+    then steps until ~target_s of CPU time (at most max_steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    o = oracle.Oracle(sc)
+    o.setup()
+    o.run(2)
+    t0 = time.perf_counter()
+    o.run(1)
+    one = time.perf_counter() - t0
+    k = int(max(1, min(max_steps, target_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    o.run(k)
+    dt = time.perf_counter() - t0 + one
+    n = len(sc["atoms"]["tag"])
+    return n * (k + 1) / dt, k + 1
+
+
+# --------------------------------------------------------------- arms
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return ws, rank, local, dist
+    return 1, 0, 0, None
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def allmax(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reference_arm(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc, desc, extra = make_workload(args)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    o = oracle.Oracle(sc)
+    o.setup()
+    settle = min(args.settle, 200)
+    o.run(settle)
+    w = min(args.warmup, 3)
+    o.run(w)
+    n = len(sc["atoms"]["tag"])
+    t0 = time.perf_counter()
+    o.run(1)
+    one = time.perf_counter() - t0
+    k = int(max(1, min(args.steps, 30.0 / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    o.run(k)
+    dt = time.perf_counter() - t0
+    val = n * k / dt
+    sample = "%s; oracle port (1 thread) after %d settle + %d warm-up steps, %d timed steps" % (desc, settle, w, k)
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": k, "warmup": w,
+        "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": dict({"workload": desc, "settle_steps": settle}, **extra),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def own_arm(args):
+    ws, rank, local, dist = dist_init()
+    import granb200
+    sc, desc, extra = make_workload(args, seed_offset=rank)
+    n = len(sc["atoms"]["tag"])
+    eng = granb200.Engine(sc, device=local)
+    eng.setup()
+    eng.run(args.settle)
+    eng.run(max(args.warmup, 3))
+    eng.sync()
+    cen0 = eng.census()
+    st0 = eng.stats()
+    clocks = ClockSampler(local)
+    barrier(dist)
+    eng.sync()
+    eng.set_profiling(True)
+    eng.timer_start()
+    eng.run(args.steps)
+    ms = eng.timer_stop()
+    eng.sync()
+    barrier(dist)
+    clk = clocks.stop()
+    st1 = eng.stats()
+    eng.set_profiling(False)
+    cen1 = eng.census()
+    ms_max = allmax(dist, ms)
+    value = n * args.steps * ws / (ms_max * 1e-3)
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+
+    # per-kernel device time and the roofline of the dominant kernel
+    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_reverse", "t_pair_main", "t_forward", "t_rebuild")}
+    npm = st1["n_pair_main"] - st0["n_pair_main"]
+    nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] == "wall_plane")
+    nfix_mesh = sum(1 for f in sc["fixes"] if f["kind"] == "wall_mesh")
+    dom = "k_pair_main" if kt["t_pair_main"] >= kt["t_pair_reverse"] else "k_pair_reverse"
+    dom_ms = kt["t_pair_main" if dom == "k_pair_main" else "t_pair_reverse"] / max(npm, 1)
+    ab = algorithmic_bytes(dom, n, (cen0, cen1), nfix_plane, nfix_mesh)
+    peak, peak_kind = peaks()
+    achieved = ab / (dom_ms * 1e-3) / 1e9
+    traffic = load_traffic(dom, args.workload)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": traffic["bytes_per_launch"] if traffic else None,
+            "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": dict({"workload": desc, "settle_steps": args.settle, "precision": "fp64 (bit-exact to the oracle)",
+                        "l2": "inputs larger than L2 (per-step working set > 126 MB at 1M particles)",
+                        "parallelism": "replicas x%d" % ws if ws > 1 else "single GPU"}, **extra),
+        "roofline": roof,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "kernel_ms_per_step": {k: v / args.steps for k, v in kt.items()},
+        "census": {k: 0.5 * (cen0[k] + cen1[k]) for k in cen0},
+        "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
+    }
+
+    # end to end through the C ABI: host arrays in, setup, run, host arrays out
+    if not args.no_e2e:
+        a = eng.atoms()
+        sc2 = dict(sc)
+        order = np.argsort(a["tag"])
+        idx = a["tag"][order] - 1
+        sc2["atoms"] = dict(sc["atoms"])
+        for k in ("x", "v", "omega"):
+            arr = np.zeros_like(sc["atoms"][k])
+            arr[idx] = a[k][order]
+            sc2["atoms"][k] = arr
+        barrier(dist)
+        t0 = time.perf_counter()
+        e2 = granb200.Engine(sc2, device=local)
+        e2.setup()
+        e2.run(args.steps)
+        out = e2.atoms()
+        e2.sync()
+        dt = time.perf_counter() - t0
+        dt = allmax(dist, dt)
+        h2d = n * (3 * 3 * 8 + 2 * 8 + 2 * 4) + sum(f["nodes"].size * 8 for f in sc["fixes"] if f["kind"] == "wall_mesh")
+        d2h = n * (5 * 3 * 8 + 4)
+        line["e2e"] = {"value": n * args.steps * ws / dt, "unit": UNIT,
+                       "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                       "includes": "context create, materials, atom + mesh upload, Verlet setup, %d steps, "
+                                   "download of x/v/omega/f/torque" % args.steps}
+        del e2, out
+
+    # CPU baseline: the oracle on this rank's state at the start of the window
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        a = eng.atoms()
+        sc3 = dict(sc)
+        order = np.argsort(a["tag"])
+        idx = a["tag"][order] - 1
+        sc3["atoms"] = dict(sc["atoms"])
+        for k in ("x", "v", "omega"):
+            arr = np.zeros_like(sc["atoms"][k])
+            arr[idx] = a[k][order]
+            sc3["atoms"][k] = arr
+        cval, ck = run_oracle_sample(sc3, args.cpu_seconds, 200)
+        line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": "oracle port, 1 thread, same %d-particle state as the GPU window end, "
+                                          "setup + 2 untimed steps, %d timed steps" % (n, ck)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        own_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -84,8 +84,19 @@ typedef struct {
     long ntouch;                 /* pairs with a set contact flag           */
     int maxneigh, maxpartner;    /* current per-atom capacities             */
     double time_pair, time_neigh, time_other;   /* device ms, cumulative    */
-    long kernel_launches;        /* kernels launched by gb2_run so far      */
+    long kernel_launches;        /* kernels launched by this context so far */
+    /* per-kernel device time (ms, cumulative) while profiling is on */
+    double t_integrate, t_pair_reverse, t_pair_main, t_forward, t_rebuild;
+    long n_pair_main;            /* pair-pass launches timed                */
+    long nsteps_rebuild;         /* steps that rebuilt the neighbour list   */
 } gb2_stats;
+
+/* contact census of the current state (device reduction): half-list entries,
+   touching pairs (rsq < (ri+rj)^2), reverse entries, primitive-wall and mesh
+   contacts within reach, mesh candidate slots */
+typedef struct {
+    long nlist, ntouch, nrev, nwall_list, nwall_touch, nmesh_cand, nmesh_touch;
+} gb2_contact_census;
 
 /* context lifecycle */
 int gb2_create(const gb2_params *p, gb2_ctx **out);
@@ -133,6 +144,12 @@ int gb2_mesh_topology(gb2_ctx *ctx, int ifix, int cap, int *ntri, unsigned char 
                       unsigned char *corner_active, int *obtuse);
 
 int gb2_get_stats(gb2_ctx *ctx, gb2_stats *st);
+int gb2_census(gb2_ctx *ctx, gb2_contact_census *out);
+/* per-kernel CUDA-event timing on the context stream (off by default) */
+int gb2_set_profiling(gb2_ctx *ctx, int on);
+/* CUDA-event timer on the context stream: start, then stop returns ms */
+int gb2_timer_start(gb2_ctx *ctx);
+int gb2_timer_stop(gb2_ctx *ctx, double *ms);
 /* copies the last error message (NUL-terminated) into buf */
 int gb2_last_error(gb2_ctx *ctx, char *buf, int len);
 /* library version string, e.g. "granb200 0.1 sm_100a" */

@@ -143,7 +143,17 @@ struct gb2_ctx {
     // stats
     long npairs_last = 0;
     long launches = 0;
+    long nsteps_rebuild = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-kernel event timing (gb2_set_profiling)
+    bool prof = false;
+    struct EvPair {
+        cudaEvent_t a, b;
+        int cls;
+    };
+    std::vector<EvPair> ev_free, ev_pending;
+    double prof_ms[5] = {0, 0, 0, 0, 0};
+    long n_pair_main = 0;
 };
 
 namespace {
@@ -280,6 +290,50 @@ int clear_status(gb2_ctx *c)
 {
     CK(cudaMemsetAsync(c->dstatus.p, 0, sizeof(int), c->st));
     return 0;
+}
+
+// ---------------------------------------------------------------- profiling
+enum { PROF_INTEGRATE = 0, PROF_PAIR_REVERSE = 1, PROF_PAIR_MAIN = 2, PROF_FORWARD = 3, PROF_REBUILD = 4 };
+
+int prof_begin(gb2_ctx *c, int cls, gb2_ctx::EvPair *out)
+{
+    if (!c->prof) return 0;
+    if (c->ev_free.empty()) {
+        gb2_ctx::EvPair e;
+        CK(cudaEventCreate(&e.a));
+        CK(cudaEventCreate(&e.b));
+        c->ev_free.push_back(e);
+    }
+    *out = c->ev_free.back();
+    c->ev_free.pop_back();
+    out->cls = cls;
+    CK(cudaEventRecord(out->a, c->st));
+    return 0;
+}
+
+int prof_end(gb2_ctx *c, gb2_ctx::EvPair *e)
+{
+    if (!c->prof) return 0;
+    CK(cudaEventRecord(e->b, c->st));
+    c->ev_pending.push_back(*e);
+    return 0;
+}
+
+// accumulate every finished pair (called after stream synchronisation points)
+void prof_resolve(gb2_ctx *c)
+{
+    size_t keep = 0;
+    for (size_t k = 0; k < c->ev_pending.size(); k++) {
+        gb2_ctx::EvPair &e = c->ev_pending[k];
+        if (cudaEventQuery(e.b) == cudaSuccess) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) c->prof_ms[e.cls] += ms;
+            if (e.cls == PROF_PAIR_MAIN) c->n_pair_main++;
+            c->ev_free.push_back(e);
+        } else
+            c->ev_pending[keep++] = e;
+    }
+    c->ev_pending.resize(keep);
 }
 
 int cub_tmp(gb2_ctx *c, size_t bytes)
@@ -764,16 +818,21 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
 int do_force(gb2_ctx *c, int shearupdate, int integrate)
 {
     Dev D = make_dev(c);
+    gb2_ctx::EvPair e;
+    if (prof_begin(c, PROF_PAIR_REVERSE, &e)) return GB2_ERR_CUDA;
     if (c->P.rolling_cdt)
         k_pair_reverse<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
     else
         k_pair_reverse<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
     CKL();
+    if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    if (prof_begin(c, PROF_PAIR_MAIN, &e)) return GB2_ERR_CUDA;
     if (c->P.rolling_cdt)
         k_pair_main<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
     else
         k_pair_main<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
     CKL();
+    if (prof_end(c, &e)) return GB2_ERR_CUDA;
     if (integrate) {
         c->vel.swap(c->vel2);
         c->omg.swap(c->omg2);
@@ -820,6 +879,14 @@ int gb2_destroy(gb2_ctx *c)
     if (!c) return 0;
     cudaStreamSynchronize(c->st);
     for (int k = 0; k < c->nfix; k++) delete c->fix[k].mesh;
+    for (auto &e : c->ev_free) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    for (auto &e : c->ev_pending) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1048,27 +1115,87 @@ int gb2_run(gb2_ctx *c, int nsteps)
         const bool check = decide && c->P.neigh_check;
         if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
         Dev D = make_dev(c);
+        gb2_ctx::EvPair e;
+        if (prof_begin(c, PROF_INTEGRATE, &e)) return GB2_ERR_CUDA;
         k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
         CKL();
+        if (prof_end(c, &e)) return GB2_ERR_CUDA;
         bool rebuild = decide && !c->P.neigh_check;
         if (check) {
             CK(cudaMemcpyAsync(&c->h_pinned[1], c->ddflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
             CK(cudaStreamSynchronize(c->st));
             rebuild = c->h_pinned[1] != 0;
+            if (c->prof) prof_resolve(c);
         }
         if (rebuild) {
             const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
+            if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
             int rc = do_rebuild(c, true, sort_now);
             if (rc) return rc;
+            if (prof_end(c, &e)) return GB2_ERR_CUDA;
+            c->nsteps_rebuild++;
         } else if (c->nghost > 0) {
+            if (prof_begin(c, PROF_FORWARD, &e)) return GB2_ERR_CUDA;
             k_forward_comm<<<nblk(c->nghost), kBlock, 0, c->st>>>(D);
             CKL();
+            if (prof_end(c, &e)) return GB2_ERR_CUDA;
         }
         if (do_force(c, 1, 1)) return GB2_ERR_CUDA;
     }
     int st;
     if (read_status(c, &st)) return GB2_ERR_CUDA;
+    if (c->prof) prof_resolve(c);
     if (st & ST_MESH_INTERNAL) return set_err(c, GB2_ERR_STATE, "mesh contact history inconsistent");
+    return 0;
+}
+
+int gb2_set_profiling(gb2_ctx *c, int on)
+{
+    if (!c) return GB2_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    prof_resolve(c);
+    c->prof = on != 0;
+    return 0;
+}
+
+int gb2_timer_start(gb2_ctx *c)
+{
+    if (!c) return GB2_ERR_ARG;
+    CK(cudaEventRecord(c->ev0, c->st));
+    return 0;
+}
+
+int gb2_timer_stop(gb2_ctx *c, double *ms)
+{
+    if (!c || !ms) return GB2_ERR_ARG;
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, c->ev0, c->ev1));
+    *ms = f;
+    return 0;
+}
+
+int gb2_census(gb2_ctx *c, gb2_contact_census *out)
+{
+    if (!c || !out) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "census needs a neighbor list (call gb2_setup)");
+    DBuf<unsigned long long> cnt;
+    CK(cnt.alloc(8));
+    CK(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), c->st));
+    Dev D = make_dev(c);
+    k_census<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, cnt.p);
+    CKL();
+    unsigned long long h[8];
+    CK(cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    out->nlist = (long)h[0];
+    out->ntouch = (long)h[1];
+    out->nrev = (long)h[2];
+    out->nwall_list = (long)h[3];
+    out->nwall_touch = (long)h[4];
+    out->nmesh_cand = (long)h[5];
+    out->nmesh_touch = (long)h[6];
     return 0;
 }
 
@@ -1210,6 +1337,16 @@ int gb2_get_stats(gb2_ctx *c, gb2_stats *s)
     s->maxneigh = c->maxn;
     s->maxpartner = c->maxp;
     s->kernel_launches = c->launches;
+    s->t_integrate = c->prof_ms[PROF_INTEGRATE];
+    s->t_pair_reverse = c->prof_ms[PROF_PAIR_REVERSE];
+    s->t_pair_main = c->prof_ms[PROF_PAIR_MAIN];
+    s->t_forward = c->prof_ms[PROF_FORWARD];
+    s->t_rebuild = c->prof_ms[PROF_REBUILD];
+    s->time_pair = s->t_pair_reverse + s->t_pair_main;
+    s->time_neigh = s->t_rebuild;
+    s->time_other = s->t_integrate + s->t_forward;
+    s->n_pair_main = c->n_pair_main;
+    s->nsteps_rebuild = c->nsteps_rebuild;
     return 0;
 }
 

@@ -902,4 +902,43 @@ __global__ void __launch_bounds__(128) k_pair_main(Dev D, int shearupdate, int i
     }
 }
 
+// contact census (diagnostics and the bench's byte model)
+__global__ void k_census(Dev D, unsigned long long *cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.nlocal) return;
+    const int cap = D.cap;
+    const dbl4 pi = D.pos[i];
+    const int nn = D.nnum[i];
+    unsigned long long touch = 0;
+    for (int s = 0; s < nn; s++) {
+        const dbl4 pj = D.pos[D.nbr[s * cap + i]];
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const double rs = pi.w + pj.w;
+        if (dx * dx + dy * dy + dz * dz < rs * rs) touch++;
+    }
+    unsigned long long wl = 0, wt = 0, mc = 0, mt = 0;
+    for (int k = 0; k < D.nfix; k++) {
+        const FixDev &F = D.fix[k];
+        if (F.kind == FIX_WALL_PLANE && F.inlist[i]) {
+            wl++;
+            const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+            const double dist = x > F.pos ? x - F.pos - pi.w : F.pos - x - pi.w;
+            if (dist <= 0) wt++;
+        } else if (F.kind == FIX_WALL_MESH) {
+            const int tc = F.mesh.tcnt[i];
+            mc += tc;
+            for (int q = 0; q < tc; q++)
+                if (F.mesh.spartner[q * cap + i] >= 0) mt++;
+        }
+    }
+    atomicAdd(&cnt[0], (unsigned long long)nn);
+    if (touch) atomicAdd(&cnt[1], touch);
+    atomicAdd(&cnt[2], (unsigned long long)D.rnum[i]);
+    if (wl) atomicAdd(&cnt[3], wl);
+    if (wt) atomicAdd(&cnt[4], wt);
+    if (mc) atomicAdd(&cnt[5], mc);
+    if (mt) atomicAdd(&cnt[6], mt);
+}
+
 }  // namespace gb2

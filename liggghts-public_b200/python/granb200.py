@@ -26,7 +26,8 @@ EXPORTS = (
     "gb2_create", "gb2_destroy", "gb2_set_materials", "gb2_upload_atoms", "gb2_add_gravity",
     "gb2_add_wall_plane", "gb2_add_wall_mesh", "gb2_setup", "gb2_run", "gb2_sync", "gb2_download_atoms",
     "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
-    "gb2_get_stats", "gb2_last_error", "gb2_version",
+    "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
+    "gb2_timer_stop",
 )
 
 
@@ -64,7 +65,19 @@ class Stats(ctypes.Structure):
         ("time_neigh", ctypes.c_double),
         ("time_other", ctypes.c_double),
         ("kernel_launches", ctypes.c_long),
+        ("t_integrate", ctypes.c_double),
+        ("t_pair_reverse", ctypes.c_double),
+        ("t_pair_main", ctypes.c_double),
+        ("t_forward", ctypes.c_double),
+        ("t_rebuild", ctypes.c_double),
+        ("n_pair_main", ctypes.c_long),
+        ("nsteps_rebuild", ctypes.c_long),
     ]
+
+
+class Census(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_long) for f in
+                ("nlist", "ntouch", "nrev", "nwall_list", "nwall_touch", "nmesh_cand", "nmesh_touch")]
 
 
 def lib(path=LIB_PATH):
@@ -93,6 +106,10 @@ def lib(path=LIB_PATH):
         L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         L.gb2_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.gb2_version.restype = ctypes.c_char_p
+        L.gb2_census.argtypes = [vp, ctypes.POINTER(Census)]
+        L.gb2_set_profiling.argtypes = [vp, ctypes.c_int]
+        L.gb2_timer_start.argtypes = [vp]
+        L.gb2_timer_stop.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         _LIB = L
     return _LIB
 
@@ -207,6 +224,22 @@ class Engine:
         s = Stats()
         self._check(self.L.gb2_get_stats(self.h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def census(self):
+        c = Census()
+        self._check(self.L.gb2_census(self.h, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in Census._fields_}
+
+    def set_profiling(self, on):
+        self._check(self.L.gb2_set_profiling(self.h, 1 if on else 0))
+
+    def timer_start(self):
+        self._check(self.L.gb2_timer_start(self.h))
+
+    def timer_stop(self):
+        ms = ctypes.c_double()
+        self._check(self.L.gb2_timer_stop(self.h, ctypes.byref(ms)))
+        return ms.value
 
     def atoms(self):
         n = self.n

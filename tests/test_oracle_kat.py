@@ -1,0 +1,144 @@
+"""Known-answer tests that pin the CPU oracle (the reference ships no tests,
+golden logs or fixtures, so these analytic cases and symmetry laws stand in
+for them; see DESIGN.md "parity status")."""
+import math
+
+import numpy as np
+import pytest
+
+import gb2_scenarios as S
+import oracle
+
+
+def base(n, box=(1.0, 1.0, 1.0), dt=1e-6, e=0.3, mu=0.5, E=5e6, nu=0.45, periodic=(0, 0, 0)):
+    sc = {"dt": dt, "skin": 0.5e-3, "boxlo": [0.0, 0.0, 0.0], "boxhi": list(box), "periodic": list(periodic),
+          "every": 1, "delay": 0, "check": 1, "sortfreq": 0, "sortbinsize": 0.0, "rolling_cdt": 0,
+          "tangential_damping": 1, "fixes": []}
+    sc.update(S._materials(1, E, nu, e, mu))
+    return sc
+
+
+def atoms(pos, vel, r=1e-3, rho=2500.0, omega=None):
+    pos = np.asarray(pos, dtype=float)
+    a = S._atoms(pos, np.full(len(pos), r), rho, np.asarray(vel, dtype=float), omega)
+    return a
+
+
+def test_hertz_static_overlap_on_plane():
+    # m g = 4/3 Y* sqrt(R d) d  ->  d = (3 m g / (4 Y* sqrt(R)))^(2/3), wall: reff = R, Y* = E / (2 (1 - nu^2))
+    r, rho, E, nu, g = 1e-3, 2500.0, 5e6, 0.45, 9.81
+    sc = base(1, dt=2e-6, e=0.1)
+    sc["atoms"] = atoms([[0.5, 0.5, r]], [[0.0, 0.0, 0.0]], r, rho)
+    sc["fixes"] = [{"kind": "gravity", "magnitude": g, "vector": [0, 0, -1]},
+                   {"kind": "wall_plane", "dim": 2, "pos": 0.0, "wall_type": 1}, {"kind": "nve_sphere"}]
+    o = oracle.Oracle(sc)
+    o.setup()
+    o.run(60000)
+    m = 4.0 / 3.0 * math.pi * r ** 3 * rho
+    ystar = E / (2.0 * (1.0 - nu * nu))
+    d_exact = (3.0 * m * g / (4.0 * ystar * math.sqrt(r))) ** (2.0 / 3.0)
+    d = r - o.atoms()["x"][0, 2]
+    assert abs(d - d_exact) / d_exact < 1e-6
+    assert abs(o.atoms()["v"][0, 2]) < 1e-8
+
+
+def test_head_on_restitution():
+    # Hertz + velocity damping with beta from e: the rebound ratio is the requested e (to a few %)
+    for e in (0.3, 0.7, 0.95):
+        sc = base(2, dt=1e-7, e=e)
+        v0 = 0.1
+        sc["atoms"] = atoms([[0.5 - 1.0005e-3, 0.5, 0.5], [0.5 + 1.0005e-3, 0.5, 0.5]], [[v0, 0, 0], [-v0, 0, 0]])
+        sc["fixes"] = [{"kind": "nve_sphere"}]
+        o = oracle.Oracle(sc)
+        o.setup()
+        o.run(20000)
+        v = o.atoms()["v"]
+        ratio = (v[1, 0] - v[0, 0]) / (2 * v0)
+        assert abs(ratio - e) < 0.05 * e + 0.02, (e, ratio)
+
+
+def test_coulomb_cap_and_sign():
+    # pressed sphere pair sliding: |Ft| <= mu |Fn|, and the friction opposes the slip
+    sc = base(2, e=0.5, mu=0.3)
+    xi, xj = [0.0, 0.0, 0.0], [1.99e-3, 0.0, 0.0]
+    vi, vj = [0.0, 0.5, 0.0], [0.0, -0.5, 0.0]
+    sh = np.zeros(3)
+    for _ in range(200):
+        fi, ti, fj, tj, sh = oracle.pair_force(sc, xi, xj, vi, vj, [0, 0, 0], [0, 0, 0], 1e-3, 1e-3, 1e-5, 1e-5,
+                                               shear=sh)
+    en = np.array([-1.0, 0.0, 0.0])
+    fn = np.dot(fi, en)
+    ft = fi - fn * en
+    assert np.linalg.norm(ft) <= 0.3 * abs(fn) * (1 + 1e-12)
+    assert abs(np.linalg.norm(ft) - 0.3 * abs(fn)) < 1e-9 * abs(fn)
+    assert ft[1] < 0.0
+    # Newton's third law for the force, torques from the two contact radii
+    assert np.array_equal(fj, -fi)
+
+
+def test_pair_swap_symmetry_bitwise():
+    # evaluating a pair from the other side with negated shear is bit-identical
+    rng = np.random.default_rng(4)
+    sc = base(2)
+    sc["rolling_cdt"] = 1
+    sc["rollfriction"] = np.full((1, 1), 0.1)
+    for _ in range(200):
+        ri, rj = rng.uniform(0.5e-3, 2e-3, 2)
+        xi = rng.normal(size=3) * 1e-3
+        d = rng.normal(size=3)
+        xj = xi + d / np.linalg.norm(d) * (ri + rj) * rng.uniform(0.95, 0.999)
+        vi, vj, wi, wj = (rng.normal(size=3) * s for s in (0.1, 0.1, 50, 50))
+        sh = rng.normal(size=3) * 1e-7
+        fi, ti, fj, tj, shi = oracle.pair_force(sc, xi, xj, vi, vj, wi, wj, ri, rj, 1e-5, 2e-5, shear=sh.copy())
+        gj, uj, gi, ui, shj = oracle.pair_force(sc, xj, xi, vj, vi, wj, wi, rj, ri, 2e-5, 1e-5, shear=-sh)
+        assert np.array_equal(gj, fj) and np.array_equal(uj, tj)
+        assert np.array_equal(shj, -shi)
+
+
+def test_momentum_conserved_periodic():
+    # no walls or gravity in a fully periodic box: total pair force vanishes
+    sc = S.sphere_pour(n=448, seed=9, box=(0.02, 0.02, 0.02), spacing=(2.5e-3, 2.5e-3, 2.5e-3), vmax=0.5)
+    sc["periodic"] = [1, 1, 1]
+    sc["fixes"] = [{"kind": "nve_sphere"}]
+    sc["atoms"]["x"][:, 2] = np.mod(sc["atoms"]["x"][:, 2], 0.02)
+    o = oracle.Oracle(sc)
+    o.setup()
+    for _ in range(5):
+        o.run(100)
+        a = o.atoms()
+        fs = np.abs(a["f"]).sum(axis=0)
+        assert np.all(np.abs(a["f"].sum(axis=0)) <= 1e-12 * np.maximum(fs, 1e-30))
+    p = o.pairs()
+    assert (p["flag"] != 0).sum() > 0
+
+
+def test_mesh_face_matches_plane():
+    # a sphere resting on a flat two-triangle mesh floor settles at the plane's overlap
+    r, rho = 1e-3, 2500.0
+    sc = base(1, dt=2e-6, e=0.1)
+    sc["atoms"] = atoms([[0.5, 0.5, r]], [[0.0, 0.0, 0.0]], r, rho)
+    sq = [[[0.1, 0.1, 1e-9], [0.9, 0.1, 1e-9], [0.9, 0.9, 1e-9]], [[0.1, 0.1, 1e-9], [0.9, 0.9, 1e-9], [0.1, 0.9, 1e-9]]]
+    sc["fixes"] = [{"kind": "gravity", "magnitude": 9.81, "vector": [0, 0, -1]},
+                   {"kind": "wall_mesh", "nodes": np.array(sq), "wall_type": 1}, {"kind": "nve_sphere"}]
+    o = oracle.Oracle(sc)
+    o.setup()
+    o.run(60000)
+    sc2 = dict(sc)
+    sc2["fixes"] = [sc["fixes"][0], {"kind": "wall_plane", "dim": 2, "pos": 1e-9, "wall_type": 1}, sc["fixes"][2]]
+    o2 = oracle.Oracle(sc2)
+    o2.setup()
+    o2.run(60000)
+    z1, z2 = o.atoms()["x"][0, 2], o2.atoms()["x"][0, 2]
+    assert abs(z1 - z2) < 1e-12
+    ea, ca, ob = o.mesh_topology(1, 2)
+    assert ea.tolist() == [[1, 1, 0], [0, 1, 1]]   # shared coplanar diagonal inactive on both
+
+
+def test_cone_topology_counts():
+    sc = S.hopper(n=100, n_theta=64, n_z=16)
+    o = oracle.Oracle(sc)
+    ea, ca, ob = o.mesh_topology(1, len(sc["fixes"][1]["nodes"]))
+    # ring edges between coplanar rows and quad diagonals are inactive; boundary rings active;
+    # each generator line shared by two sectors is active on the larger element id only
+    assert ea.sum() == 64 + 64 + 64 * 16
+    assert ca.sum() == 2 * 64            # only boundary-ring nodes keep an active corner
