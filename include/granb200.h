@@ -145,6 +145,23 @@ int gb2_mesh_topology(gb2_ctx *ctx, int ifix, int cap, int *ntri, unsigned char 
 
 int gb2_get_stats(gb2_ctx *ctx, gb2_stats *st);
 int gb2_census(gb2_ctx *ctx, gb2_contact_census *out);
+/* gb2_census_noalloc: the same census for callers that must not allocate
+   device memory -- code running while a CUDA stream is being captured into a
+   graph (cudaMalloc/cudaFree are illegal or force a device-wide sync there),
+   monitoring hooks of a host framework that owns every allocation, or a
+   process already at its memory cap.  It has no counterpart in the reference
+   (LIGGGHTS allocates freely on the host).  Its scratch is a file-scope device
+   array in libgranb200 of (GB2_NOALLOC_MAX_BLOCKS + 1) x 8 64-bit counters
+   (1 MiB), held by every GPU that loads the library until process exit, so
+   it serves at most GB2_NOALLOC_MAX_ATOMS owned atoms; larger contexts get
+   GB2_ERR_CAPACITY.  No cudaMalloc, cudaFree or allocating library call is
+   made.  The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress); make that first call before any stream capture.
+   All calls share the one array: two calls whose work overlaps on a GPU
+   (different streams or host threads) race and may return wrong counts. */
+#define GB2_NOALLOC_MAX_BLOCKS 16384
+#define GB2_NOALLOC_MAX_ATOMS (GB2_NOALLOC_MAX_BLOCKS * 128)
+int gb2_census_noalloc(gb2_ctx *ctx, gb2_contact_census *out);
 /* per-kernel CUDA-event timing on the context stream (off by default) */
 int gb2_set_profiling(gb2_ctx *ctx, int on);
 /* CUDA-event timer on the context stream: start, then stop returns ms */

@@ -842,6 +842,75 @@ int do_force(gb2_ctx *c, int shearupdate, int integrate)
 
 }  // namespace
 
+// ---------------------------------------------------------------- census without allocation
+// Scratch for gb2_census_noalloc: one row of 8 counters per 128-atom block plus
+// a final row for the totals.  Shared by every call in the process.
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[(GB2_NOALLOC_MAX_BLOCKS + 1) * 8];
+
+// same per-atom census as k_census; each block reduces its atoms in shared
+// memory and writes its own row, so no counter needs clearing beforehand
+__global__ void __launch_bounds__(128) k_census_rows(Dev D, unsigned long long *rows)
+{
+    __shared__ unsigned long long red[7][128];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long c[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < D.nlocal) {
+        const int cap = D.cap;
+        const dbl4 pi = D.pos[i];
+        const int nn = D.nnum[i];
+        c[0] = nn;
+        for (int s = 0; s < nn; s++) {
+            const dbl4 pj = D.pos[D.nbr[s * cap + i]];
+            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const double rs = pi.w + pj.w;
+            if (dx * dx + dy * dy + dz * dz < rs * rs) c[1]++;
+        }
+        c[2] = D.rnum[i];
+        for (int k = 0; k < D.nfix; k++) {
+            const FixDev &F = D.fix[k];
+            if (F.kind == FIX_WALL_PLANE && F.inlist[i]) {
+                c[3]++;
+                const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+                const double dist = x > F.pos ? x - F.pos - pi.w : F.pos - x - pi.w;
+                if (dist <= 0) c[4]++;
+            } else if (F.kind == FIX_WALL_MESH) {
+                const int tc = F.mesh.tcnt[i];
+                c[5] += tc;
+                for (int q = 0; q < tc; q++)
+                    if (F.mesh.spartner[q * cap + i] >= 0) c[6]++;
+            }
+        }
+    }
+    for (int k = 0; k < 7; k++) red[k][threadIdx.x] = c[k];
+    __syncthreads();
+    for (int w = 64; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 7; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) rows[(size_t)blockIdx.x * 8 + threadIdx.x] = threadIdx.x < 7 ? red[threadIdx.x][0] : 0ull;
+}
+
+// sums the block rows into the totals row (one block, fixed order)
+__global__ void k_census_total(unsigned long long *rows, int nrows)
+{
+    __shared__ unsigned long long red[8][256];
+    unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x)
+        for (int k = 0; k < 8; k++) c[k] += rows[(size_t)r * 8 + k];
+    for (int k = 0; k < 8; k++) red[k][threadIdx.x] = c[k];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int k = 0; k < 8; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) rows[(size_t)GB2_NOALLOC_MAX_BLOCKS * 8 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// device address of g_noalloc_scratch per device, looked up on first use
+static unsigned long long *g_noalloc_ptr[64];
+
 // ====================================================================== C ABI
 
 extern "C" {
@@ -1188,6 +1257,44 @@ int gb2_census(gb2_ctx *c, gb2_contact_census *out)
     CKL();
     unsigned long long h[8];
     CK(cudaMemcpyAsync(h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    out->nlist = (long)h[0];
+    out->ntouch = (long)h[1];
+    out->nrev = (long)h[2];
+    out->nwall_list = (long)h[3];
+    out->nwall_touch = (long)h[4];
+    out->nmesh_cand = (long)h[5];
+    out->nmesh_touch = (long)h[6];
+    return 0;
+}
+
+int gb2_census_noalloc(gb2_ctx *c, gb2_contact_census *out)
+{
+    if (!c || !out) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "census needs a neighbor list (call gb2_setup)");
+    const int nblocks = nblk(c->nlocal, 128);
+    if (nblocks > GB2_NOALLOC_MAX_BLOCKS)
+        return set_err(c, GB2_ERR_CAPACITY,
+                       "gb2_census_noalloc serves at most %d owned atoms (static scratch); this context has %d",
+                       GB2_NOALLOC_MAX_ATOMS, c->nlocal);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_err(c, GB2_ERR_ARG, "device ordinal %d out of range", dev);
+    if (!g_noalloc_ptr[dev]) {
+        // first call on this device (the device is current): resolve the
+        // host-side stand-in symbol to its device address
+        unsigned long long *p = nullptr;
+        CK(cudaGetSymbolAddress((void **)&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = p;
+    }
+    unsigned long long *rows = g_noalloc_ptr[dev];
+    Dev D = make_dev(c);
+    k_census_rows<<<nblocks, 128, 0, c->st>>>(D, rows);
+    CKL();
+    k_census_total<<<1, 256, 0, c->st>>>(rows, nblocks);
+    CKL();
+    unsigned long long h[8];
+    CK(cudaMemcpyAsync(h, rows + (size_t)GB2_NOALLOC_MAX_BLOCKS * 8, sizeof h, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     out->nlist = (long)h[0];
     out->ntouch = (long)h[1];

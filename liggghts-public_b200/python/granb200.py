@@ -27,8 +27,10 @@ EXPORTS = (
     "gb2_add_wall_plane", "gb2_add_wall_mesh", "gb2_setup", "gb2_run", "gb2_sync", "gb2_download_atoms",
     "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
-    "gb2_timer_stop",
+    "gb2_timer_stop", "gb2_census_noalloc",
 )
+
+NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
 
 
 class Params(ctypes.Structure):
@@ -107,6 +109,7 @@ def lib(path=LIB_PATH):
         L.gb2_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.gb2_version.restype = ctypes.c_char_p
         L.gb2_census.argtypes = [vp, ctypes.POINTER(Census)]
+        L.gb2_census_noalloc.argtypes = [vp, ctypes.POINTER(Census)]
         L.gb2_set_profiling.argtypes = [vp, ctypes.c_int]
         L.gb2_timer_start.argtypes = [vp]
         L.gb2_timer_stop.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
@@ -228,6 +231,12 @@ class Engine:
     def census(self):
         c = Census()
         self._check(self.L.gb2_census(self.h, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in Census._fields_}
+
+    def census_noalloc(self):
+        """gb2_census_noalloc: the census without any device allocation (static scratch)."""
+        c = Census()
+        self._check(self.L.gb2_census_noalloc(self.h, ctypes.byref(c)))
         return {f: getattr(c, f) for f, _ in Census._fields_}
 
     def set_profiling(self, on):
