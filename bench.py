@@ -128,6 +128,12 @@ def algorithmic_bytes(kernel, n, cen, nfix_plane, nfix_mesh):
     records, list indices and shear history that must cross HBM once;
     neighbour-state gathers are served from L2 and not counted."""
     avg = lambda k: 0.5 * (cen[0][k] + cen[1][k])
+    if kernel == "k_pair_step":
+        # own x,v,w,r,m,type 92 + list counts 8 + touch mask 16 + xhold 24 + x,v,w out 72
+        per_atom = 92 + 8 + 16 + 24 + 72 + nfix_plane * 1 + nfix_mesh * 4
+        b = n * per_atom + avg("nlist") * 4 + avg("nrev") * 4 + avg("ntouch") * (52 + 25)
+        b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
+        return b
     if kernel == "k_pair_main":
         per_atom = 92 + 48 + 4 + 48 + 48 + nfix_plane * 1 + nfix_mesh * 4
         b = n * per_atom + avg("nlist") * 4 + avg("ntouch") * 52
@@ -264,12 +270,12 @@ def own_arm(args):
     launches = st1["kernel_launches"] - st0["kernel_launches"]
 
     # per-kernel device time and the roofline of the dominant kernel
-    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_reverse", "t_pair_main", "t_forward", "t_rebuild")}
+    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_forward", "t_rebuild")}
     npm = st1["n_pair_main"] - st0["n_pair_main"]
     nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] == "wall_plane")
     nfix_mesh = sum(1 for f in sc["fixes"] if f["kind"] == "wall_mesh")
-    dom = "k_pair_main" if kt["t_pair_main"] >= kt["t_pair_reverse"] else "k_pair_reverse"
-    dom_ms = kt["t_pair_main" if dom == "k_pair_main" else "t_pair_reverse"] / max(npm, 1)
+    dom = "k_pair_step"
+    dom_ms = kt["t_pair_main"] / max(npm, 1)
     ab = algorithmic_bytes(dom, n, (cen0, cen1), nfix_plane, nfix_mesh)
     peak, peak_kind = peaks()
     achieved = ab / (dom_ms * 1e-3) / 1e9

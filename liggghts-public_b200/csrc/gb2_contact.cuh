@@ -38,6 +38,7 @@ struct ContactOut {
 // in the reference's accumulation order and updates `shear` in place when
 // update_history is set.  Returns nothing; the caller applies the
 // rsq < radsum^2 broad phase.
+template <bool ACCUM = true>
 __device__ __forceinline__ void pair_contact(const MatPair &M, double delx, double dely, double delz, double rsq,
                                              double radi, double radj, const double vi[3], const double vj[3],
                                              const double wi[3], const double wj[3], double mi, double mj,
@@ -160,12 +161,21 @@ __device__ __forceinline__ void pair_contact(const MatPair &M, double delx, doub
         T1 -= rt1;
         T2 -= rt2;
     }
-    out.F[0] += F0;
-    out.F[1] += F1;
-    out.F[2] += F2;
-    out.T[0] += T0;
-    out.T[1] += T1;
-    out.T[2] += T2;
+    if (ACCUM) {
+        out.F[0] += F0;
+        out.F[1] += F1;
+        out.F[2] += F2;
+        out.T[0] += T0;
+        out.T[1] += T1;
+        out.T[2] += T2;
+    } else {   // the pair's own contribution, for a later in-order sum
+        out.F[0] = F0;
+        out.F[1] = F1;
+        out.F[2] = F2;
+        out.T[0] = T0;
+        out.T[1] = T1;
+        out.T[2] = T2;
+    }
 }
 
 // Sphere-wall contact (primitive plane or mesh triangle), following

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -85,6 +86,8 @@ struct MeshFix {
     DBuf<double> shist;
     DBuf<int> snp2, spartner2;   // re-paging target
     DBuf<double> shist2;
+    DBuf<int> tcnt2, tcnt_s, snp_s, spartner_s;   // candidate-count double buffer, atom-sort shadows
+    DBuf<double> shist_s;
     bool bins_valid = false;
     double nl_skin = 0, distmax = 0;
 };
@@ -97,7 +100,7 @@ struct HostFix {
     int wtype = 1;
     int rolling = 0;
     DBuf<uint8_t> inlist;
-    DBuf<double> whist;
+    DBuf<double> whist, whist_s;
     MeshFix *mesh = nullptr;
 };
 
@@ -114,11 +117,17 @@ struct gb2_ctx {
     int nlocal = 0, nghost = 0, nmax = 0, cap = 0;
     std::vector<double> h_radius;
     std::vector<int> h_type;
-    DBuf<dbl4> pos, vel, omg, vel2, omg2, f, tq, fpart, tpart, xhold;
+    DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, fpart, tpart, xhold;
+    DBuf<uint8_t> revs;
+    int minb = 6;                 // register-allocation target of the pair step kernel
+    bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
     DBuf<int> type, tag;
     int maxn = 16, maxr = 16, maxp = 16;
     DBuf<int> nnum, nbr, flag, rnum, rev, pnum, ptag;
-    DBuf<double> hist, phist;
+    DBuf<int> type_s, tag_s, pnum_s, ptag_s;   // atom-sort shadows
+    DBuf<double> phist_s;
+    DBuf<double> hist, hist2, phist;
+    DBuf<unsigned long long> prevmask;
     DBuf<int> gsrc;
     DBuf<dbl4> gshift;
     // bins
@@ -196,6 +205,7 @@ Dev make_dev(gb2_ctx *c)
     D.pos = c->pos.p;
     D.vel = c->vel.p;
     D.omg = c->omg.p;
+    D.pos_out = c->pos2.p;
     D.vel_out = c->vel2.p;
     D.omg_out = c->omg2.p;
     D.type = c->type.p;
@@ -210,9 +220,12 @@ Dev make_dev(gb2_ctx *c)
     D.nbr = c->nbr.p;
     D.flag = c->flag.p;
     D.hist = c->hist.p;
+    D.hist_out = c->hist2.p;
+    D.prevmask = c->prevmask.p;
     D.maxr = c->maxr;
     D.rnum = c->rnum.p;
     D.rev = c->rev.p;
+    D.revs = c->revs.p;
     D.maxp = c->maxp;
     D.pnum = c->pnum.p;
     D.ptag = c->ptag.p;
@@ -352,6 +365,7 @@ int ensure_nmax(gb2_ctx *c, int need)
     CK(c->pos.grow_keep(nm, keep, c->st));
     CK(c->vel.grow_keep(nm, keep, c->st));
     CK(c->omg.grow_keep(nm, keep, c->st));
+    CK(c->pos2.grow_keep(nm, 0, c->st));
     CK(c->vel2.grow_keep(nm, 0, c->st));
     CK(c->omg2.grow_keep(nm, 0, c->st));
     CK(c->type.grow_keep(nm, keep, c->st));
@@ -575,61 +589,48 @@ int do_atom_sort(gb2_ctx *c)
     CK(cub::DeviceRadixSort::SortPairs(c->cubtmp.p, bytes, c->keys.p, c->keys2.p, c->vals.p, c->vals2.p, n, 0, 32,
                                        c->st));
     const int *perm = c->vals2.p;
-    // every per-atom array moves with its atom
+    // every per-atom array moves with its atom: gather into a persistent
+    // shadow buffer and swap (no allocation once the shadows exist)
     {
-        DBuf<dbl4> tmp;
-        CK(tmp.alloc(c->nmax));
-        DBuf<dbl4> *arrs[] = {&c->pos, &c->vel, &c->omg};
-        for (auto *a : arrs) {
-            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a->p, tmp.p, perm, n);
+        DBuf<dbl4> *arrs[][2] = {{&c->pos, &c->pos2}, {&c->vel, &c->vel2}, {&c->omg, &c->omg2}};
+        for (auto &a : arrs) {
+            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a[0]->p, a[1]->p, perm, n);
             CKL();
-            CK(cudaMemcpyAsync(a->p, tmp.p, sizeof(dbl4) * n, cudaMemcpyDeviceToDevice, c->st));
+            a[0]->swap(*a[1]);
         }
-        DBuf<int> itmp;
-        CK(itmp.alloc(std::max(c->nmax, c->cap * std::max(c->maxp, 1))));
-        DBuf<int> *iarrs[] = {&c->type, &c->tag, &c->pnum};
-        for (auto *a : iarrs) {
-            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a->p, itmp.p, perm, n);
+        auto gather_i = [&](DBuf<int> &a, DBuf<int> &sh) -> int {
+            CK(sh.alloc(std::max<size_t>(a.n, 1)));
+            k_gather<<<nblk(n), kBlock, 0, c->st>>>(a.p, sh.p, perm, n);
             CKL();
-            CK(cudaMemcpyAsync(a->p, itmp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, c->st));
-        }
-        auto gather_slots_i = [&](DBuf<int> &a, int nslot) -> int {
-            if (nslot <= 0) return 0;
-            DBuf<int> t2;
-            CK(t2.alloc((size_t)nslot * c->cap));
-            dim3 g(nblk(n), nslot);
-            k_gather_slots<<<g, kBlock, 0, c->st>>>(a.p, t2.p, perm, n, c->cap, nslot);
-            CKL();
-            a.swap(t2);
-            CK(cudaStreamSynchronize(c->st));
+            a.swap(sh);
             return 0;
         };
-        auto gather_slots_d = [&](DBuf<double> &a, int nslot) -> int {
+        // slot-major arrays; only the slots an atom uses (s / div < cnt_old[atom]) are copied
+        auto gather_slots = [&](auto &a, auto &sh, int nslot, const int *cnt_old, int div) -> int {
             if (nslot <= 0) return 0;
-            DBuf<double> t2;
-            CK(t2.alloc((size_t)nslot * c->cap));
+            CK(sh.alloc((size_t)nslot * c->cap));
             dim3 g(nblk(n), nslot);
-            k_gather_slots<<<g, kBlock, 0, c->st>>>(a.p, t2.p, perm, n, c->cap, nslot);
+            k_gather_slots_cnt<<<g, kBlock, 0, c->st>>>(a.p, sh.p, perm, n, c->cap, nslot, cnt_old, div);
             CKL();
-            a.swap(t2);
-            CK(cudaStreamSynchronize(c->st));
+            a.swap(sh);
             return 0;
         };
-        if (gather_slots_i(c->ptag, c->maxp)) return GB2_ERR_CUDA;
-        if (gather_slots_d(c->phist, 3 * c->maxp)) return GB2_ERR_CUDA;
+        if (gather_i(c->type, c->type_s) || gather_i(c->tag, c->tag_s)) return GB2_ERR_CUDA;
+        // partners: slots gathered against the pre-permutation counts, then the counts
+        if (gather_slots(c->ptag, c->ptag_s, c->maxp, c->pnum.p, 1)) return GB2_ERR_CUDA;
+        if (gather_slots(c->phist, c->phist_s, 3 * c->maxp, c->pnum.p, 3)) return GB2_ERR_CUDA;
+        if (gather_i(c->pnum, c->pnum_s)) return GB2_ERR_CUDA;
         for (int k = 0; k < c->nfix; k++) {
             HostFix &H = c->fix[k];
             if (H.kind == FIX_WALL_PLANE)
-                if (gather_slots_d(H.whist, 3)) return GB2_ERR_CUDA;
+                if (gather_slots(H.whist, H.whist_s, 3, nullptr, 1)) return GB2_ERR_CUDA;
             if (H.mesh) {
                 MeshFix &M = *H.mesh;
-                if (gather_slots_i(M.tcnt, 1)) return GB2_ERR_CUDA;
-                if (gather_slots_i(M.snp, 1)) return GB2_ERR_CUDA;
-                if (gather_slots_i(M.spartner, M.maxt)) return GB2_ERR_CUDA;
-                if (gather_slots_d(M.shist, 3 * M.maxt)) return GB2_ERR_CUDA;
+                if (gather_slots(M.spartner, M.spartner_s, M.maxt, M.tcnt.p, 1)) return GB2_ERR_CUDA;
+                if (gather_slots(M.shist, M.shist_s, 3 * M.maxt, M.tcnt.p, 3)) return GB2_ERR_CUDA;
+                if (gather_i(M.snp, M.snp_s) || gather_i(M.tcnt, M.tcnt_s)) return GB2_ERR_CUDA;
             }
         }
-        CK(cudaStreamSynchronize(c->st));
     }
     return 0;
 }
@@ -710,9 +711,11 @@ int do_build(gb2_ctx *c)
         if (st & ST_LOST_ATOM) return set_err(c, GB2_ERR_LOST, "an atom is outside the binned domain");
         if (!(st & ST_NEIGH_OVERFLOW)) break;
         c->maxn *= 2;
+        if (c->maxn > 256) return set_err(c, GB2_ERR_CAPACITY, "more than 256 neighbours per atom");
         CK(c->nbr.alloc((size_t)c->maxn * c->cap));
         CK(c->flag.alloc((size_t)c->maxn * c->cap));
         CK(c->hist.alloc((size_t)3 * c->maxn * c->cap));
+        CK(c->hist2.alloc((size_t)3 * c->maxn * c->cap));
         if (attempt == 7) return set_err(c, GB2_ERR_CAPACITY, "neighbor list capacity could not be grown");
     }
     for (int attempt = 0; attempt < 8; attempt++) {
@@ -726,6 +729,7 @@ int do_build(gb2_ctx *c)
         if (!(st & ST_REV_OVERFLOW)) break;
         c->maxr *= 2;
         CK(c->rev.alloc((size_t)c->maxr * c->cap));
+        CK(c->revs.alloc((size_t)c->maxr * c->cap));
         if (attempt == 7) return set_err(c, GB2_ERR_CAPACITY, "reverse list capacity could not be grown");
     }
     D = make_dev(c);
@@ -752,9 +756,8 @@ int do_pre_force(gb2_ctx *c)
                 if (mesh_bins(c, M)) return GB2_ERR_CUDA;
             // candidates into fresh buffers (old slots are still needed)
             const int old_maxt = M.maxt;
-            DBuf<int> old_tcnt;
-            old_tcnt.swap(M.tcnt);
-            CK(M.tcnt.alloc(c->cap));
+            CK(M.tcnt2.alloc(c->cap));
+            M.tcnt.swap(M.tcnt2);   // the old counts are not needed by the re-paging
             for (int attempt = 0; attempt < 8; attempt++) {
                 CK(M.tlist.alloc((size_t)M.maxt * c->cap));
                 if (clear_status(c)) return GB2_ERR_CUDA;
@@ -783,7 +786,6 @@ int do_pre_force(gb2_ctx *c)
             int st;
             if (read_status(c, &st)) return GB2_ERR_CUDA;
             if (st & ST_MESH_INTERNAL) return set_err(c, GB2_ERR_STATE, "mesh contact history inconsistent");
-            (void)old_tcnt;
         }
     }
     return 0;
@@ -815,28 +817,42 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
     return 0;
 }
 
-int do_force(gb2_ctx *c, int shearupdate, int integrate)
+template <bool R, int MINB>
+void launch_step_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
+    k_pair_step<R, MINB><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+}
+
+void launch_step(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
+{
+    // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
+    if (c->P.rolling_cdt) {
+        if (c->minb == 4) launch_step_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else if (c->minb == 5) launch_step_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_step_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+    } else {
+        if (c->minb == 4) launch_step_kernel<false, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else if (c->minb == 5) launch_step_kernel<false, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_step_kernel<false, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+    }
+}
+
+int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int store_f)
+{
+    if (fuse_next) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
     Dev D = make_dev(c);
     gb2_ctx::EvPair e;
-    if (prof_begin(c, PROF_PAIR_REVERSE, &e)) return GB2_ERR_CUDA;
-    if (c->P.rolling_cdt)
-        k_pair_reverse<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
-    else
-        k_pair_reverse<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate);
-    CKL();
-    if (prof_end(c, &e)) return GB2_ERR_CUDA;
     if (prof_begin(c, PROF_PAIR_MAIN, &e)) return GB2_ERR_CUDA;
-    if (c->P.rolling_cdt)
-        k_pair_main<true><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
-    else
-        k_pair_main<false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate);
+    launch_step(c, D, shearupdate, integrate, fuse_next, store_f);
     CKL();
     if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    if (shearupdate) c->hist.swap(c->hist2);
     if (integrate) {
         c->vel.swap(c->vel2);
         c->omg.swap(c->omg2);
+        if (fuse_next) c->pos.swap(c->pos2);
     }
+    c->fused_pending = integrate && fuse_next;
     return 0;
 }
 
@@ -927,6 +943,7 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     gb2_ctx *c = new gb2_ctx();
     c->P = *p;
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
+    if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) {
         delete c;
@@ -1038,7 +1055,10 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     CK(c->nbr.alloc((size_t)c->maxn * cap));
     CK(c->flag.alloc((size_t)c->maxn * cap));
     CK(c->hist.alloc((size_t)3 * c->maxn * cap));
+    CK(c->hist2.alloc((size_t)3 * c->maxn * cap));
+    CK(c->prevmask.alloc(cap));
     CK(c->rev.alloc((size_t)c->maxr * cap));
+    CK(c->revs.alloc((size_t)c->maxr * cap));
     CK(c->ptag.alloc((size_t)c->maxp * cap));
     CK(c->phist.alloc((size_t)3 * c->maxp * cap));
     CK(cudaMemsetAsync(c->f.p, 0, sizeof(dbl4) * cap, c->st));
@@ -1166,7 +1186,7 @@ int gb2_setup(gb2_ctx *c)
     // neighbor build, setup_pre_force, pair (shearupdate 0), fix setup
     int rc = do_rebuild(c, c->computeflag, c->P.sort_freq > 0);
     if (rc) return rc;
-    if (do_force(c, 0, 0)) return GB2_ERR_CUDA;
+    if (do_force(c, 0, 0, 0, 1)) return GB2_ERR_CUDA;
     CK(cudaStreamSynchronize(c->st));
     c->setup_done = true;
     c->computeflag = true;
@@ -1182,13 +1202,17 @@ int gb2_run(gb2_ctx *c, int nsteps)
         c->ago++;
         const bool decide = c->ago >= c->P.neigh_delay && c->ago % c->P.neigh_every == 0;
         const bool check = decide && c->P.neigh_check;
-        if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
-        Dev D = make_dev(c);
         gb2_ctx::EvPair e;
-        if (prof_begin(c, PROF_INTEGRATE, &e)) return GB2_ERR_CUDA;
-        k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
-        CKL();
-        if (prof_end(c, &e)) return GB2_ERR_CUDA;
+        if (!c->fused_pending) {
+            // first step of this run: initial_integrate as its own kernel (later
+            // steps get it fused into the previous step's pair pass B)
+            if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
+            Dev D = make_dev(c);
+            if (prof_begin(c, PROF_INTEGRATE, &e)) return GB2_ERR_CUDA;
+            k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
+            CKL();
+            if (prof_end(c, &e)) return GB2_ERR_CUDA;
+        }
         bool rebuild = decide && !c->P.neigh_check;
         if (check) {
             CK(cudaMemcpyAsync(&c->h_pinned[1], c->ddflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -1204,12 +1228,14 @@ int gb2_run(gb2_ctx *c, int nsteps)
             if (prof_end(c, &e)) return GB2_ERR_CUDA;
             c->nsteps_rebuild++;
         } else if (c->nghost > 0) {
+            Dev D = make_dev(c);
             if (prof_begin(c, PROF_FORWARD, &e)) return GB2_ERR_CUDA;
             k_forward_comm<<<nblk(c->nghost), kBlock, 0, c->st>>>(D);
             CKL();
             if (prof_end(c, &e)) return GB2_ERR_CUDA;
         }
-        if (do_force(c, 1, 1)) return GB2_ERR_CUDA;
+        const bool last = (step == nsteps - 1);
+        if (do_force(c, 1, 1, last ? 0 : 1, last ? 1 : 0)) return GB2_ERR_CUDA;
     }
     int st;
     if (read_status(c, &st)) return GB2_ERR_CUDA;

@@ -14,7 +14,7 @@
 //     nnum[i], nbr[s*cap+i] (j index), flag[s*cap+i] (contact flag bits),
 //     hist[(3s+c)*cap+i] (shear history, FP64)
 //   reverse list (entries where the atom is the j side, ascending owner):
-//     rnum[k], rev[s*cap+k] = half-list slot e = s'*cap + i'
+//     rnum[k], rev[r*cap+k] = owner i', revs[r*cap+k] = its slot s'
 //   contact-history partners (FixContactHistory::partner_, keyed by tag):
 //     pnum[i], ptag[s*cap+i], phist[(3s+c)*cap+i]
 //   ghosts: gsrc[g] (owned source atom), gshift[g] {dx, dy, dz, -}
@@ -99,16 +99,19 @@ struct FixDev {
 struct Dev {
     int nlocal, nghost, nmax, cap;   // cap: stride of slot-major arrays (>= nlocal)
     dbl4 *pos, *vel, *omg;
-    dbl4 *vel_out, *omg_out;   // final_integrate target (double buffer: pass B reads vel/omg of neighbours)
+    dbl4 *pos_out, *vel_out, *omg_out;   // integrate targets (double buffer: pass B reads neighbours' state)
     int *type, *tag;
     dbl4 *f, *tq, *fpart, *tpart, *xhold;
     // half list
     int maxn;
     int *nnum, *nbr, *flag;
-    double *hist;
+    double *hist;          // shear read buffer (current values)
+    double *hist_out;      // shear write buffer of the pair step
+    unsigned long long *prevmask;   // own slots touching in the previous step
     // reverse list
     int maxr;
-    int *rnum, *rev;
+    int *rnum, *rev;       // rev[r*cap+k] = owner index i of the pair
+    uint8_t *revs;         // revs[r*cap+k] = slot s of the pair in i's list
     // partners
     int maxp;
     int *pnum, *ptag;

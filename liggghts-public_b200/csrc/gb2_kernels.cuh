@@ -120,9 +120,9 @@ __global__ void k_partners(Dev D)
     // entries where k is the j side
     const int nr = D.rnum[k];
     for (int r = 0; r < nr; r++) {
-        const int e = D.rev[r * cap + k];
-        if (!D.flag[e]) continue;
-        const int s = e / cap, i = e - s * cap;
+        const int i = D.rev[r * cap + k];
+        const int s = D.revs[r * cap + k];
+        if (!D.flag[s * cap + i]) continue;
         if (np < D.maxp) {
             D.ptag[np * cap + k] = D.tag[i];
             for (int c = 0; c < 3; c++) D.phist[(3 * np + c) * cap + k] = -D.hist[(3 * s + c) * cap + i];
@@ -205,6 +205,20 @@ __global__ void k_gather_slots(const T *__restrict__ src, T *__restrict__ dst, c
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = blockIdx.y;
     if (i < n && s < nslot) dst[(size_t)s * cap + i] = src[(size_t)s * cap + perm[i]];
+}
+
+// slot-major gather of the slots an atom uses: dst[s*cap+i] = src[s*cap+perm[i]]
+// for s / div < cnt_old[perm[i]] (all slots when cnt_old is null)
+template <typename T>
+__global__ void k_gather_slots_cnt(const T *__restrict__ src, T *__restrict__ dst, const int *__restrict__ perm, int n,
+                                   int cap, int nslot, const int *__restrict__ cnt_old, int div)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (i >= n || s >= nslot) return;
+    const int o = perm[i];
+    if (cnt_old && s / div >= cnt_old[o]) return;
+    dst[(size_t)s * cap + i] = src[(size_t)s * cap + o];
 }
 
 // Comm::borders swap selection (src/comm.cpp:1028, Comm::decide src/comm_I.h:66)
@@ -322,9 +336,13 @@ __global__ void k_build_list(Dev D)
                             }
                     }
                     D.flag[e] = fl;
+                    // both history buffers, so either can serve as the next read buffer
                     D.hist[(3 * n + 0) * cap + i] = h0;
                     D.hist[(3 * n + 1) * cap + i] = h1;
                     D.hist[(3 * n + 2) * cap + i] = h2;
+                    D.hist_out[(3 * n + 0) * cap + i] = h0;
+                    D.hist_out[(3 * n + 1) * cap + i] = h1;
+                    D.hist_out[(3 * n + 2) * cap + i] = h2;
                 }
                 n++;
             }
@@ -332,6 +350,7 @@ __global__ void k_build_list(Dev D)
     }
     if (n > D.maxn) atomicOr(D.status, ST_NEIGH_OVERFLOW);
     D.nnum[i] = min(n, D.maxn);
+    D.prevmask[i] = 0ull;
     dbl4 h;
     h.x = xtmp;
     h.y = ytmp;
@@ -352,9 +371,10 @@ __global__ void k_rev_fill(Dev D)
         const int j = D.nbr[e];
         if (j >= D.nlocal) continue;
         const int r = atomicAdd(&D.rnum[j], 1);
-        if (r < D.maxr)
-            D.rev[r * cap + j] = e;
-        else
+        if (r < D.maxr) {
+            D.rev[r * cap + j] = i;
+            D.revs[r * cap + j] = (uint8_t)s;
+        } else
             atomicOr(D.status, ST_REV_OVERFLOW);
     }
 }
@@ -369,14 +389,16 @@ __global__ void k_rev_sort(Dev D)
     if (n > D.maxr) n = D.maxr;
     D.rnum[k] = n;
     for (int a = 1; a < n; a++) {
-        const int ea = D.rev[a * cap + k];
-        const int ia = ea % cap;
+        const int ia = D.rev[a * cap + k];
+        const uint8_t sa = D.revs[a * cap + k];
         int b = a - 1;
-        while (b >= 0 && D.rev[b * cap + k] % cap > ia) {
+        while (b >= 0 && D.rev[b * cap + k] > ia) {
             D.rev[(b + 1) * cap + k] = D.rev[b * cap + k];
+            D.revs[(b + 1) * cap + k] = D.revs[b * cap + k];
             b--;
         }
-        D.rev[(b + 1) * cap + k] = ea;
+        D.rev[(b + 1) * cap + k] = ia;
+        D.revs[(b + 1) * cap + k] = sa;
     }
 }
 
@@ -648,59 +670,154 @@ __device__ __forceinline__ bool coplanar_node_neighs(const MeshDev &M, int a, in
 }
 
 // ------------------------------------------------------------------
-// pair pass A: contributions of the entries where k is the j side,
-// evaluated from k's side (see file header), in ascending owner order
+// pair passes.  Both walk a per-atom list in two phases: a screening phase
+// issues the neighbour-position gathers of all entries independently (so
+// many loads are in flight per thread) and records which entries touch in a
+// bit mask; the compute phase then evaluates only touching entries, in list
+// order, so the per-atom sums keep the reference's order.
 
-template <bool ROLLING>
-__global__ void __launch_bounds__(128) k_pair_reverse(Dev D, int shearupdate)
+// One 32-byte record through the read-only path as a single 256-bit load
+// (sm_100 vector width): a scattered warp-wide gather then needs one L1
+// wavefront per lane's line instead of two.  Records are 32-byte aligned.
+__device__ __forceinline__ dbl4 ldg4(const dbl4 *p)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= D.nlocal) return;
-    const int cap = D.cap;
-    const dbl4 pk = D.pos[k], vk4 = D.vel[k], wk4 = D.omg[k];
-    const int tk = D.type[k];
-    const double vk[3] = {vk4.x, vk4.y, vk4.z}, wk[3] = {wk4.x, wk4.y, wk4.z};
-    ContactOut acc;
-    acc.F[0] = acc.F[1] = acc.F[2] = 0.0;
-    acc.T[0] = acc.T[1] = acc.T[2] = 0.0;
-    const int nr = D.rnum[k];
-    for (int r = 0; r < nr; r++) {
-        const int e = D.rev[r * cap + k];
-        const int s = e / cap, i = e - s * cap;
-        const dbl4 pi = D.pos[i];
-        const double delx = pk.x - pi.x;
-        const double dely = pk.y - pi.y;
-        const double delz = pk.z - pi.z;
-        const double rsq = delx * delx + dely * dely + delz * delz;
-        const double radsum = pk.w + pi.w;
-        if (!(rsq < radsum * radsum)) continue;
-        const dbl4 vi4 = D.vel[i], wi4 = D.omg[i];
-        const double vi[3] = {vi4.x, vi4.y, vi4.z}, wi[3] = {wi4.x, wi4.y, wi4.z};
-        double sh[3];
-        sh[0] = -D.hist[(3 * s + 0) * cap + i];
-        sh[1] = -D.hist[(3 * s + 1) * cap + i];
-        sh[2] = -D.hist[(3 * s + 2) * cap + i];
-        // material lookup in the reference's (owner, neighbour) order
-        pair_contact(mat(D, D.type[i], tk), delx, dely, delz, rsq, pk.w, pi.w, vk, vi, wk, wi, vk4.w, vi4.w, sh,
-                     shearupdate != 0, D.dt, ROLLING, D.tdamp != 0, acc);
-    }
-    dbl4 F, T;
-    F.x = acc.F[0];
-    F.y = acc.F[1];
-    F.z = acc.F[2];
-    F.w = 0.0;
-    T.x = acc.T[0];
-    T.y = acc.T[1];
-    T.z = acc.T[2];
-    T.w = 0.0;
-    D.fpart[k] = F;
-    D.tpart[k] = T;
+    dbl4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
 }
 
-// ------------------------------------------------------------------
-// pair pass B + post_force fixes + FixNVESphere::final_integrate
+__device__ __forceinline__ bool touching(const dbl4 &a, const dbl4 &b)
+{
+    const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    const double rs = a.w + b.w;
+    return dx * dx + dy * dy + dz * dz < rs * rs;
+}
 
-__device__ void mesh_wall_atom(const Dev &D, const MeshDev &M, int i, const dbl4 &p, const double v[3],
+// Warp-cooperative evaluation of the touching entries found by screening.
+// The warp's touching entries are enumerated owner-lane-major (each owner's
+// entries in list order); in rounds of 32, lane t evaluates item base+t and
+// leaves the pair's raw contribution in shared memory, then every owner lane
+// adds the items it owns in order.  The per-atom sums therefore keep the
+// reference's order while the FP64 contact arithmetic runs on full warps.
+struct WarpItems {
+    int cnt, excl, total;
+};
+
+__device__ __forceinline__ WarpItems warp_items(unsigned long long mask)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    WarpItems it;
+    it.cnt = __popcll(mask);
+    int x = it.cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    it.excl = x - it.cnt;
+    it.total = __shfl_sync(FULL, x, 31);
+    return it;
+}
+
+// Index stream loads: read once per step, evict-first so they do not push
+// the neighbour records out of L2
+__device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
+
+// Screening of the j-side (rev) and own (nbr) entries of one atom in one
+// loop: per round two indices of each list, then four independent record
+// gathers, then the distance tests.  Both lists are <= 64 entries here.
+__device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn, const dbl4 &pk,
+                                            unsigned long long &mrev, unsigned long long &mown)
+{
+    const int cap = D.cap;
+    const int n = max(nr, nn);
+    for (int t = 0; t < n; t += 2) {
+        const int a0 = (t < nr) ? ld_stream(&D.rev[t * cap + k]) : k;
+        const int a1 = (t + 1 < nr) ? ld_stream(&D.rev[(t + 1) * cap + k]) : k;
+        const int b0 = (t < nn) ? ld_stream(&D.nbr[t * cap + k]) : k;
+        const int b1 = (t + 1 < nn) ? ld_stream(&D.nbr[(t + 1) * cap + k]) : k;
+        const dbl4 qa0 = ldg4(&D.pos[a0]);
+        const dbl4 qa1 = ldg4(&D.pos[a1]);
+        const dbl4 qb0 = ldg4(&D.pos[b0]);
+        const dbl4 qb1 = ldg4(&D.pos[b1]);
+        if (t < nr && touching(pk, qa0)) mrev |= 1ull << t;
+        if (t + 1 < nr && touching(pk, qa1)) mrev |= 1ull << (t + 1);
+        if (t < nn && touching(pk, qb0)) mown |= 1ull << t;
+        if (t + 1 < nn && touching(pk, qb1)) mown |= 1ull << (t + 1);
+    }
+}
+
+// Screening of n <= 64 list entries idx[r*cap + k]: four index loads, then
+// four independent neighbour-record gathers, then the four distance tests,
+// so a thread keeps several loads in flight.  Returns the touching mask.
+__device__ __forceinline__ unsigned long long screen_entries(const int *__restrict__ idx, int cap, int k, int n,
+                                                            const dbl4 &pk, const dbl4 *__restrict__ pos)
+{
+    unsigned long long m = 0ull;
+    for (int r0 = 0; r0 < n; r0 += 4) {
+        const int j0 = __ldg(&idx[min(r0 + 0, n - 1) * cap + k]);
+        const int j1 = __ldg(&idx[min(r0 + 1, n - 1) * cap + k]);
+        const int j2 = __ldg(&idx[min(r0 + 2, n - 1) * cap + k]);
+        const int j3 = __ldg(&idx[min(r0 + 3, n - 1) * cap + k]);
+        const dbl4 q0 = ldg4(&pos[j0]);
+        const dbl4 q1 = ldg4(&pos[j1]);
+        const dbl4 q2 = ldg4(&pos[j2]);
+        const dbl4 q3 = ldg4(&pos[j3]);
+        if (touching(pk, q0)) m |= 1ull << r0;
+        if (r0 + 1 < n && touching(pk, q1)) m |= 1ull << (r0 + 1);
+        if (r0 + 2 < n && touching(pk, q2)) m |= 1ull << (r0 + 2);
+        if (r0 + 3 < n && touching(pk, q3)) m |= 1ull << (r0 + 3);
+    }
+    return m;
+}
+
+__device__ __forceinline__ WarpItems warp_items_cnt(int cnt)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    WarpItems it;
+    it.cnt = cnt;
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    it.excl = x - cnt;
+    it.total = __shfl_sync(FULL, x, 31);
+    return it;
+}
+
+// owner lane of item w: the largest lane whose exclusive prefix is <= w
+__device__ __forceinline__ int item_owner(int w, int excl)
+{
+    const unsigned FULL = 0xffffffffu;
+    int L = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const int cand = L + step;
+        const int ex = __shfl_sync(FULL, excl, cand & 31);
+        if (cand < 32 && ex <= w) L = cand;
+    }
+    return L;
+}
+
+__device__ __forceinline__ int nth_set_bit(unsigned long long m, int rank)
+{
+    for (int q = 0; q < rank; q++) m &= m - 1ull;
+    return __ffsll((long long)m) - 1;
+}
+
+__device__ __forceinline__ unsigned long long shfl64(unsigned long long v, int src)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lo = __shfl_sync(FULL, (unsigned)(v & 0xffffffffull), src);
+    const unsigned hi = __shfl_sync(FULL, (unsigned)(v >> 32), src);
+    return ((unsigned long long)hi << 32) | lo;
+}
+
+__device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, int i, const dbl4 &p, const double v[3],
                                const double w[3], double mass, int itype, bool upd, ContactOut &acc)
 {
     const int cap = D.cap;
@@ -790,51 +907,243 @@ __device__ void mesh_wall_atom(const Dev &D, const MeshDev &M, int i, const dbl4
     M.snp[i] = np;
 }
 
+// An atom with more than 64 reverse or own entries, evaluated serially in
+// the reference order (rare; kept out of line so the hot loop stays small).
 template <bool ROLLING>
-__global__ void __launch_bounds__(128) k_pair_main(Dev D, int shearupdate, int integrate)
+__device__ __forceinline__ void serial_atom(const Dev &D, int k, const dbl4 &pk, const dbl4 &vi4, const dbl4 &wi4, int tk,
+                                         int nr, int nn, bool upd, ContactOut &acc)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.nlocal) return;
     const int cap = D.cap;
-    const dbl4 pi = D.pos[i];
-    dbl4 vi4 = D.vel[i], wi4 = D.omg[i];
-    const int ti = D.type[i];
-    const double vi[3] = {vi4.x, vi4.y, vi4.z}, wi[3] = {wi4.x, wi4.y, wi4.z};
-    const bool upd = shearupdate != 0;
-    ContactOut acc;
-    {
-        const dbl4 F = D.fpart[i], T = D.tpart[i];
-        acc.F[0] = F.x;
-        acc.F[1] = F.y;
-        acc.F[2] = F.z;
-        acc.T[0] = T.x;
-        acc.T[1] = T.y;
-        acc.T[2] = T.z;
-    }
-    const int nn = D.nnum[i];
-    for (int s = 0; s < nn; s++) {
-        const int e = s * cap + i;
-        const int j = D.nbr[e];
-        const dbl4 pj = D.pos[j];
-        const double delx = pi.x - pj.x;
-        const double dely = pi.y - pj.y;
-        const double delz = pi.z - pj.z;
+    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
+    // more than 64 entries on one side: every entry in order on this lane
+    for (int r = 0; r < nr; r++) {
+        const int i = __ldg(&D.rev[r * cap + k]);
+        const dbl4 pi = ldg4(&D.pos[i]);
+        const double delx = pk.x - pi.x;
+        const double dely = pk.y - pi.y;
+        const double delz = pk.z - pi.z;
         const double rsq = delx * delx + dely * dely + delz * delz;
-        const double radsum = pi.w + pj.w;
+        const double radsum = pk.w + pi.w;
         if (!(rsq < radsum * radsum)) continue;
-        const dbl4 vj4 = D.vel[j], wj4 = D.omg[j];
-        const double vj[3] = {vj4.x, vj4.y, vj4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
-        const int fl = D.flag[e];
-        if ((fl | 5) != fl) D.flag[e] = fl | 5;   // CONTACT_NORMAL_MODEL | CONTACT_TANGENTIAL_MODEL
-        double sh[3] = {D.hist[(3 * s + 0) * cap + i], D.hist[(3 * s + 1) * cap + i], D.hist[(3 * s + 2) * cap + i]};
-        pair_contact(mat(D, ti, D.type[j]), delx, dely, delz, rsq, pi.w, pj.w, vi, vj, wi, wj, vi4.w, vj4.w, sh, upd,
-                     D.dt, ROLLING, D.tdamp != 0, acc);
-        if (upd) {
-            D.hist[(3 * s + 0) * cap + i] = sh[0];
-            D.hist[(3 * s + 1) * cap + i] = sh[1];
-            D.hist[(3 * s + 2) * cap + i] = sh[2];
+        const int s = D.revs[r * cap + k];
+        const dbl4 v4 = ldg4(&D.vel[i]), w4 = ldg4(&D.omg[i]);
+        const double vi[3] = {v4.x, v4.y, v4.z}, wi[3] = {w4.x, w4.y, w4.z};
+        double sh[3];
+        sh[0] = -D.hist[(3 * s + 0) * cap + i];
+        sh[1] = -D.hist[(3 * s + 1) * cap + i];
+        sh[2] = -D.hist[(3 * s + 2) * cap + i];
+        pair_contact(mat(D, D.type[i], tk), delx, dely, delz, rsq, pk.w, pi.w, vk, vi, wk, wi, vi4.w, v4.w, sh,
+                     upd, D.dt, ROLLING, D.tdamp != 0, acc);
+    }
+    for (int s = 0; s < nn; s++) {
+        const int e = s * cap + k;
+        const int j = __ldg(&D.nbr[e]);
+        const dbl4 pj = ldg4(&D.pos[j]);
+        const double delx = pk.x - pj.x;
+        const double dely = pk.y - pj.y;
+        const double delz = pk.z - pj.z;
+        const double rsq = delx * delx + dely * dely + delz * delz;
+        const double radsum = pk.w + pj.w;
+        double sh[3] = {D.hist[(3 * s + 0) * cap + k], D.hist[(3 * s + 1) * cap + k],
+                        D.hist[(3 * s + 2) * cap + k]};
+        if (rsq < radsum * radsum) {
+            const dbl4 v4 = ldg4(&D.vel[j]), w4 = ldg4(&D.omg[j]);
+            const double vj[3] = {v4.x, v4.y, v4.z}, wj[3] = {w4.x, w4.y, w4.z};
+            const int fl = D.flag[e];
+            if ((fl | 5) != fl) D.flag[e] = fl | 5;
+            pair_contact(mat(D, tk, D.type[j]), delx, dely, delz, rsq, pk.w, pj.w, vk, vj, wk, wj, vi4.w, v4.w,
+                         sh, upd, D.dt, ROLLING, D.tdamp != 0, acc);
+        }
+        if (upd) {   // serial atoms write every slot
+            D.hist_out[(3 * s + 0) * cap + k] = sh[0];
+            D.hist_out[(3 * s + 1) * cap + k] = sh[1];
+            D.hist_out[(3 * s + 2) * cap + k] = sh[2];
         }
     }
+}
+
+// FixWallGran::post_force_primitive for one atom in the plane's neighbour
+// list (src/fix_wall_gran.cpp:1024-1148, Plane<dim>::resolveContact
+// src/primitive_wall_definitions.h:133)
+__device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, int i, const dbl4 &pi, const double *vi,
+                                             const double *wi, double mass, int ti, bool upd, ContactOut &acc)
+{
+    const int cap = D.cap;
+    const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+    double delta_d, deltan;
+    delta_d = F.pos - x;
+    if (x > F.pos)
+        deltan = x - F.pos - pi.w;
+    else
+        deltan = F.pos - x - pi.w;
+    if (deltan > D.cutneighmax) return;
+    if (deltan <= 0) {
+        // -delta with constant indices only (keeps d in registers)
+        const double d[3] = {F.dim == 0 ? -delta_d : -0., F.dim == 1 ? -delta_d : -0., F.dim == 2 ? -delta_d : -0.};
+        double sh[3] = {F.whist[0 * cap + i], F.whist[1 * cap + i], F.whist[2 * cap + i]};
+        const double vwall[3] = {0., 0., 0.};
+        wall_contact(mat(D, ti, F.wtype), d, -deltan, pi.w, vi, wi, vwall, mass, sh, upd, D.dt, F.rolling != 0,
+                     D.tdamp != 0, acc);
+        F.whist[0 * cap + i] = sh[0];
+        F.whist[1 * cap + i] = sh[1];
+        F.whist[2 * cap + i] = sh[2];
+    } else {
+        F.whist[0 * cap + i] = 0.0;
+        F.whist[1 * cap + i] = 0.0;
+        F.whist[2 * cap + i] = 0.0;
+    }
+}
+
+// The pair step: PairGran::compute for one owned atom k with its j-side
+// (reverse) entries and its own half-list entries, the post_force fixes,
+// FixNVESphere::final_integrate and -- when the run continues -- the next
+// step's initial_integrate with the displacement check.
+//
+// Shear history is double-buffered.  Invariant: when a step starts, every
+// slot's current shear is in `hist` (the read buffer); the step writes the
+// write buffer `hist_out`, which becomes the read buffer of the next step.
+// A touching slot is read from hist and its update written to hist_out; a
+// slot that stopped touching this step is copied once (after that both
+// buffers agree); a rebuild writes both buffers.  Reverse entries therefore
+// read the pre-update shear without racing the owner's update, exactly as
+// the reference evaluates the pair once before the owner's shear changes.
+//
+// Per warp, the touching entries of its 32 atoms are enumerated owner-major
+// (reverse entries in ascending owner order, then own entries in list
+// order), evaluated one per lane in rounds of 32 with results staged in
+// shared memory, and summed by each owner lane in that order.  Atoms with
+// more than 64 reverse or own entries are evaluated serially by their owner
+// lane after the rounds, in the same order.
+template <bool ROLLING, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate, int integrate, int fuse_next,
+                                                         int store_f)
+{
+    __shared__ double sres[4][32][6];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int wbase = blockIdx.x * blockDim.x + wid * 32;
+    const bool valid = k < D.nlocal;
+    const int cap = D.cap;
+    const bool upd = shearupdate != 0;
+    dbl4 pk, vi4, wi4, hold;
+    unsigned long long prevm = 0ull;
+    int nr = 0, nn = 0, tk = 0;
+    unsigned long long mrev = 0ull, mown = 0ull;
+    bool serial = false;
+    if (valid) {
+        // the atom's own records, including those only the tail needs, are
+        // requested first so their latency overlaps the screening
+        pk = D.pos[k];
+        nr = D.rnum[k];
+        nn = D.nnum[k];
+        vi4 = D.vel[k];
+        wi4 = D.omg[k];
+        tk = D.type[k];
+        if (fuse_next) hold = D.xhold[k];
+        if (upd) prevm = D.prevmask[k];
+        serial = nr > 64 || nn > 64;
+        if (!serial) screen_both(D, k, nr, nn, pk, mrev, mown);
+    }
+    ContactOut acc;
+    acc.F[0] = acc.F[1] = acc.F[2] = 0.0;
+    acc.T[0] = acc.T[1] = acc.T[2] = 0.0;
+    const int crev = __popcll(mrev);
+    {
+        const WarpItems it = warp_items_cnt(crev + __popcll(mown));
+        for (int base = 0; base < it.total; base += 32) {
+            const int w = base + lane;
+            const int L = item_owner(w, it.excl);
+            const int exL = __shfl_sync(0xffffffffu, it.excl, L);
+            const unsigned long long mrL = shfl64(mrev, L);
+            const unsigned long long moL = shfl64(mown, L);
+            if (w < it.total) {
+                const int kk = wbase + L;
+                const int q = w - exL;
+                const int qr = __popcll(mrL);
+                const dbl4 pkk = ldg4(&D.pos[kk]), vk4 = ldg4(&D.vel[kk]), wk4 = ldg4(&D.omg[kk]);
+                const double vk[3] = {vk4.x, vk4.y, vk4.z}, wk[3] = {wk4.x, wk4.y, wk4.z};
+                // operands of one pair: j-side entries are evaluated from kk's side
+                // with the shear negated, own entries update kk's slot
+                int other, s, e = -1;
+                double sgn;
+                bool own;
+                if (q < qr) {
+                    const int r = nth_set_bit(mrL, q);
+                    other = __ldg(&D.rev[r * cap + kk]);
+                    s = D.revs[r * cap + kk];
+                    sgn = -1.0;
+                    own = false;
+                } else {
+                    s = nth_set_bit(moL, q - qr);
+                    e = s * cap + kk;
+                    other = __ldg(&D.nbr[e]);
+                    sgn = 1.0;
+                    own = true;
+                }
+                const int hrow = own ? kk : other;
+                const dbl4 po = ldg4(&D.pos[other]), vo4 = ldg4(&D.vel[other]), wo4 = ldg4(&D.omg[other]);
+                const double delx = pkk.x - po.x;
+                const double dely = pkk.y - po.y;
+                const double delz = pkk.z - po.z;
+                const double rsq = delx * delx + dely * dely + delz * delz;
+                const double vo[3] = {vo4.x, vo4.y, vo4.z}, wo[3] = {wo4.x, wo4.y, wo4.z};
+                double sh[3];
+                sh[0] = sgn * D.hist[(3 * s + 0) * cap + hrow];   // exact: multiplying by +-1 only flips the sign
+                sh[1] = sgn * D.hist[(3 * s + 1) * cap + hrow];
+                sh[2] = sgn * D.hist[(3 * s + 2) * cap + hrow];
+                const int tkk = D.type[kk], to = D.type[other];
+                // material lookup in the reference's (owner, neighbour) order
+                const MatPair &M = own ? mat(D, tkk, to) : mat(D, to, tkk);
+                if (own) {
+                    const int fl = D.flag[e];
+                    if ((fl | 5) != fl) D.flag[e] = fl | 5;   // CONTACT_NORMAL_MODEL | CONTACT_TANGENTIAL_MODEL
+                }
+                ContactOut res;
+                pair_contact<false>(M, delx, dely, delz, rsq, pkk.w, po.w, vk, vo, wk, wo, vk4.w, vo4.w, sh, upd,
+                                    D.dt, ROLLING, D.tdamp != 0, res);
+                if (own && upd) {
+                    D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
+                    D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
+                    D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
+                }
+                for (int c = 0; c < 3; c++) {
+                    sres[wid][lane][c] = res.F[c];
+                    sres[wid][lane][3 + c] = res.T[c];
+                }
+            }
+            __syncwarp();
+            const int lo = max(it.excl, base), hi = min(it.excl + it.cnt, base + 32);
+            for (int q = lo; q < hi; q++) {
+                acc.F[0] += sres[wid][q - base][0];
+                acc.F[1] += sres[wid][q - base][1];
+                acc.F[2] += sres[wid][q - base][2];
+                acc.T[0] += sres[wid][q - base][3];
+                acc.T[1] += sres[wid][q - base][4];
+                acc.T[2] += sres[wid][q - base][5];
+            }
+            __syncwarp();
+        }
+    }
+    if (!valid) return;
+    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
+    if (serial) {
+        serial_atom<ROLLING>(D, k, pk, vi4, wi4, tk, nr, nn, upd, acc);
+    } else if (upd) {
+        // slots that stopped touching this step: carry their shear into the write buffer
+        unsigned long long stopped = prevm & ~mown;
+        while (stopped) {
+            const int s = __ffsll((long long)stopped) - 1;
+            stopped &= stopped - 1ull;
+            D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
+            D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
+            D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
+        }
+    }
+    if (upd) D.prevmask[k] = serial ? ~0ull : mown;
+    const int i = k;
+    const dbl4 pi = pk;
+    const int ti = tk;
+    const double *vi = vk, *wi = wk;
     // post_force fixes in definition order
     for (int k = 0; k < D.nfix; k++) {
         const FixDev &F = D.fix[k];
@@ -844,59 +1153,55 @@ __global__ void __launch_bounds__(128) k_pair_main(Dev D, int shearupdate, int i
             acc.F[1] += massone * F.acc[1];
             acc.F[2] += massone * F.acc[2];
         } else if (F.kind == FIX_WALL_PLANE) {
-            if (!F.inlist[i]) continue;
-            const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
-            double delta_d, deltan;
-            delta_d = F.pos - x;
-            if (x > F.pos)
-                deltan = x - F.pos - pi.w;
-            else
-                deltan = F.pos - x - pi.w;
-            if (deltan > D.cutneighmax) continue;
-            if (deltan <= 0) {
-                double d[3] = {-0., -0., -0.};
-                d[F.dim] = -delta_d;
-                double sh[3] = {F.whist[0 * cap + i], F.whist[1 * cap + i], F.whist[2 * cap + i]};
-                const double vwall[3] = {0., 0., 0.};
-                wall_contact(mat(D, ti, F.wtype), d, -deltan, pi.w, vi, wi, vwall, vi4.w, sh, upd, D.dt,
-                             F.rolling != 0, D.tdamp != 0, acc);
-                F.whist[0 * cap + i] = sh[0];
-                F.whist[1 * cap + i] = sh[1];
-                F.whist[2 * cap + i] = sh[2];
-            } else {
-                F.whist[0 * cap + i] = 0.0;
-                F.whist[1 * cap + i] = 0.0;
-                F.whist[2 * cap + i] = 0.0;
-            }
+            if (F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
         } else if (F.kind == FIX_WALL_MESH) {
             mesh_wall_atom(D, F.mesh, i, pi, vi, wi, vi4.w, ti, upd, acc);
         }
     }
-    dbl4 Fo, To;
-    Fo.x = acc.F[0];
-    Fo.y = acc.F[1];
-    Fo.z = acc.F[2];
-    Fo.w = 0.0;
-    To.x = acc.T[0];
-    To.y = acc.T[1];
-    To.z = acc.T[2];
-    To.w = 0.0;
-    D.f[i] = Fo;
-    D.tq[i] = To;
+    if (store_f) {
+        dbl4 Fo, To;
+        Fo.x = acc.F[0];
+        Fo.y = acc.F[1];
+        Fo.z = acc.F[2];
+        Fo.w = 0.0;
+        To.x = acc.T[0];
+        To.y = acc.T[1];
+        To.z = acc.T[2];
+        To.w = 0.0;
+        D.f[i] = Fo;
+        D.tq[i] = To;
+    }
     if (integrate) {
         // FixNVESphere::final_integrate (src/fix_nve_sphere.cpp:208-246)
         const double dtf = 0.5 * D.dt * 1.0;
         const double dtfrotate = dtf / 0.4;
         const double dtfm = dtf / (vi4.w * 1.0);
-        vi4.x += dtfm * Fo.x;
-        vi4.y += dtfm * Fo.y;
-        vi4.z += dtfm * Fo.z;
+        vi4.x += dtfm * acc.F[0];
+        vi4.y += dtfm * acc.F[1];
+        vi4.z += dtfm * acc.F[2];
         const double dtirotate = dtfrotate / (pi.w * pi.w * vi4.w);
-        wi4.x += dtirotate * To.x;
-        wi4.y += dtirotate * To.y;
-        wi4.z += dtirotate * To.z;
-        // written to the second buffer: other threads of this pass still
-        // read vel/omg of this atom as neighbour state
+        wi4.x += dtirotate * acc.T[0];
+        wi4.y += dtirotate * acc.T[1];
+        wi4.z += dtirotate * acc.T[2];
+        if (fuse_next) {
+            // next step's FixNVESphere::initial_integrate with the same force,
+            // then Neighbor::check_distance's displacement test
+            const double dtv = D.dt;
+            vi4.x += dtfm * acc.F[0];
+            vi4.y += dtfm * acc.F[1];
+            vi4.z += dtfm * acc.F[2];
+            dbl4 p = pi;
+            p.x += dtv * vi4.x;
+            p.y += dtv * vi4.y;
+            p.z += dtv * vi4.z;
+            wi4.x += dtirotate * acc.T[0];
+            wi4.y += dtirotate * acc.T[1];
+            wi4.z += dtirotate * acc.T[2];
+            D.pos_out[i] = p;
+            const dbl4 h = hold;
+            const double delx = p.x - h.x, dely = p.y - h.y, delz = p.z - h.z;
+            if (delx * delx + dely * dely + delz * delz > D.triggersq) *D.dflag = 1;
+        }
         D.vel_out[i] = vi4;
         D.omg_out[i] = wi4;
     }
