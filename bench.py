@@ -35,7 +35,7 @@ UNIT = "particle-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--workload", default="hopper", choices=["hopper", "pour"])
@@ -76,7 +76,7 @@ class ClockSampler:
         try:
             self.out = open(os.devnull if False else "/tmp/gb2_clocks_%d.csv" % os.getpid(), "w")
             self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                                       "-i", str(device), "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+                                       "-i", str(device), "-lms", "250"], stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 

@@ -119,7 +119,7 @@ struct gb2_ctx {
     std::vector<int> h_type;
     DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, fpart, tpart, xhold;
     DBuf<uint8_t> revs;
-    int minb = 6;                 // register-allocation target of the pair step kernel
+    int minb = 4;                 // register-allocation target of the pair step kernel (blocks/SM)
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
     DBuf<int> type, tag;
     int maxn = 16, maxr = 16, maxp = 16;
@@ -827,13 +827,11 @@ void launch_step(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
 {
     // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
     if (c->P.rolling_cdt) {
-        if (c->minb == 4) launch_step_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else if (c->minb == 5) launch_step_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else launch_step_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+        if (c->minb == 6) launch_step_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_step_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
     } else {
-        if (c->minb == 4) launch_step_kernel<false, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else if (c->minb == 5) launch_step_kernel<false, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else launch_step_kernel<false, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+        if (c->minb == 6) launch_step_kernel<false, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_step_kernel<false, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
     }
 }
 
