@@ -42,6 +42,10 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="particle count (default: 1M hopper, 20k pour)")
     ap.add_argument("--settle", type=int, default=200, help="untimed settling steps before warm-up")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"],
+                    help="precision of the headline arm (split: FP32 contact math on FP64 state)")
+    ap.add_argument("--fp64-steps", type=int, default=1000,
+                    help="timed steps of the plain FP64 form on the same state (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -123,14 +127,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(kernel, n, cen, nfix_plane, nfix_mesh):
+def algorithmic_bytes(kernel, n, cen, nfix_plane, nfix_mesh, split=False):
     """Algorithmic HBM bytes per launch (model in DESIGN.md): owned-atom
     records, list indices and shear history that must cross HBM once;
     neighbour-state gathers are served from L2 and not counted."""
     avg = lambda k: 0.5 * (cen[0][k] + cen[1][k])
     if kernel == "k_pair_step":
         # own x,v,w,r,m,type 92 + list counts 8 + touch mask 16 + xhold 24 + x,v,w out 72
-        per_atom = 92 + 8 + 16 + 24 + 72 + nfix_plane * 1 + nfix_mesh * 4
+        # (+ the 32-byte FP32 kinematics record written in split precision)
+        per_atom = 92 + 8 + 16 + 24 + 72 + (32 if split else 0) + nfix_plane * 1 + nfix_mesh * 4
         b = n * per_atom + avg("nlist") * 4 + avg("nrev") * 4 + avg("ntouch") * (52 + 25)
         b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
         return b
@@ -240,80 +245,119 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def own_arm(args):
-    ws, rank, local, dist = dist_init()
-    import granb200
-    sc, desc, extra = make_workload(args, seed_offset=rank)
-    n = len(sc["atoms"]["tag"])
-    eng = granb200.Engine(sc, device=local)
-    eng.setup()
-    eng.run(args.settle)
-    eng.run(max(args.warmup, 3))
+def state_scenario(sc, a):
+    """Scenario whose x, v, omega are a downloaded engine state (by tag)."""
+    out = dict(sc)
+    order = np.argsort(a["tag"])
+    idx = a["tag"][order] - 1
+    out["atoms"] = dict(sc["atoms"])
+    for k in ("x", "v", "omega"):
+        arr = np.zeros_like(sc["atoms"][k])
+        arr[idx] = a[k][order]
+        out["atoms"][k] = arr
+    return out
+
+
+def timed_window(eng, steps, dist, device, clocks=True):
+    """Device-timed window of `steps` steps with per-kernel event timing."""
     eng.sync()
     cen0 = eng.census()
     st0 = eng.stats()
-    clocks = ClockSampler(local)
+    sampler = ClockSampler(device) if clocks else None
     barrier(dist)
     eng.sync()
     eng.set_profiling(True)
     eng.timer_start()
-    eng.run(args.steps)
+    eng.run(steps)
     ms = eng.timer_stop()
     eng.sync()
     barrier(dist)
-    clk = clocks.stop()
+    clk = sampler.stop() if sampler else None
     st1 = eng.stats()
     eng.set_profiling(False)
     cen1 = eng.census()
-    ms_max = allmax(dist, ms)
-    value = n * args.steps * ws / (ms_max * 1e-3)
-    launches = st1["kernel_launches"] - st0["kernel_launches"]
-
-    # per-kernel device time and the roofline of the dominant kernel
     kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_forward", "t_rebuild")}
-    npm = st1["n_pair_main"] - st0["n_pair_main"]
+    return {"ms": allmax(dist, ms), "clocks": clk, "cen": (cen0, cen1), "kt": kt,
+            "npm": st1["n_pair_main"] - st0["n_pair_main"],
+            "launches": st1["kernel_launches"] - st0["kernel_launches"],
+            "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
+            "growth": st1["ngrow"] - st0["ngrow"],
+            "capacities": {k: st1[k] for k in ("maxneigh", "maxpartner", "maxrev", "maxmesh")}}
+
+
+def own_arm(args):
+    ws, rank, local, dist = dist_init()
+    import granb200
+    split = args.precision == "split"
+    prec = granb200.PREC_SPLIT if split else granb200.PREC_FP64
+    sc, desc, extra = make_workload(args, seed_offset=rank)
+    n = len(sc["atoms"]["tag"])
+    eng = granb200.Engine(sc, precision=prec, device=local)
+    eng.setup()
+    eng.run(args.settle)
+    start_state = state_scenario(sc, eng.atoms()) if args.fp64_steps > 0 and split else None
+    eng.run(max(args.warmup, 3))
+    W = timed_window(eng, args.steps, dist, local)
+    ms_max = W["ms"]
+    value = n * args.steps * ws / (ms_max * 1e-3)
+
+    # roofline of the dominant kernel
     nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] == "wall_plane")
     nfix_mesh = sum(1 for f in sc["fixes"] if f["kind"] == "wall_mesh")
     dom = "k_pair_step"
-    dom_ms = kt["t_pair_main"] / max(npm, 1)
-    ab = algorithmic_bytes(dom, n, (cen0, cen1), nfix_plane, nfix_mesh)
+    dom_ms = W["kt"]["t_pair_main"] / max(W["npm"], 1)
+    ab = algorithmic_bytes(dom, n, W["cen"], nfix_plane, nfix_mesh, split)
     peak, peak_kind = peaks()
     achieved = ab / (dom_ms * 1e-3) / 1e9
-    traffic = load_traffic(dom, args.workload)
+    traffic = load_traffic(dom + ("_split" if split else ""), args.workload)
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic["bytes_per_launch"] if traffic else None,
             "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms}
 
+    pdesc = ("split (FP32 contact math on FP64-differenced positions and FP64 overlap, Kahan FP32 pair sums; "
+             "FP64 walls, gravity, integration)" if split else "fp64 (bit-exact to the oracle)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": dict({"workload": desc, "settle_steps": args.settle, "precision": "fp64 (bit-exact to the oracle)",
+        "dtype": "f32 contact / f64 state" if split else "f64", "data": "synthetic",
+        "config": dict({"workload": desc, "settle_steps": args.settle, "precision": pdesc,
                         "l2": "inputs larger than L2 (per-step working set > 126 MB at 1M particles)",
                         "parallelism": "replicas x%d" % ws if ws > 1 else "single GPU"}, **extra),
         "roofline": roof,
-        "gpu_launches": launches,
-        "clocks": clk,
-        "kernel_ms_per_step": {k: v / args.steps for k, v in kt.items()},
-        "census": {k: 0.5 * (cen0[k] + cen1[k]) for k in cen0},
-        "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
+        "gpu_launches": W["launches"],
+        "clocks": W["clocks"],
+        "kernel_ms_per_step": {k: v / args.steps for k, v in W["kt"].items()},
+        "census": {k: 0.5 * (W["cen"][0][k] + W["cen"][1][k]) for k in W["cen"][0]},
+        "rebuilds": W["rebuilds"],
+        "capacity_growth_in_window": W["growth"],
+        "capacities": W["capacities"],
     }
+
+    # the plain FP64 form on the same starting state (same settle, warm-up)
+    if start_state is not None:
+        e64 = granb200.Engine(start_state, precision=granb200.PREC_FP64, device=local)
+        e64.setup()
+        e64.run(max(args.warmup, 3))
+        W64 = timed_window(e64, args.fp64_steps, dist, local, clocks=False)
+        v64 = n * args.fp64_steps * ws / (W64["ms"] * 1e-3)
+        line["fp64_gpu"] = {"value": v64, "unit": UNIT, "steps": args.fp64_steps,
+                            "ms_per_step": W64["ms"] / args.fp64_steps,
+                            "kernel_ms_per_step": {k: v / args.fp64_steps for k, v in W64["kt"].items()},
+                            "note": "bit-exact FP64 path from the same settled state; the split window runs "
+                                    "%d steps, this one %d" % (args.steps, args.fp64_steps)}
+        # like-for-like ratio over the first fp64-steps steps is not available from one window;
+        # the ratio of per-step rates is reported
+        line["split_over_fp64"] = value / v64
+        e64.close()
+        del e64
 
     # end to end through the C ABI: host arrays in, setup, run, host arrays out
     if not args.no_e2e:
-        a = eng.atoms()
-        sc2 = dict(sc)
-        order = np.argsort(a["tag"])
-        idx = a["tag"][order] - 1
-        sc2["atoms"] = dict(sc["atoms"])
-        for k in ("x", "v", "omega"):
-            arr = np.zeros_like(sc["atoms"][k])
-            arr[idx] = a[k][order]
-            sc2["atoms"][k] = arr
+        sc2 = state_scenario(sc, eng.atoms())
         barrier(dist)
         t0 = time.perf_counter()
-        e2 = granb200.Engine(sc2, device=local)
+        e2 = granb200.Engine(sc2, precision=prec, device=local)
         e2.setup()
         e2.run(args.steps)
         out = e2.atoms()
@@ -330,15 +374,7 @@ def own_arm(args):
 
     # CPU baseline: the oracle on this rank's state at the start of the window
     if rank == 0 and ws == 1 and not args.no_cpu:
-        a = eng.atoms()
-        sc3 = dict(sc)
-        order = np.argsort(a["tag"])
-        idx = a["tag"][order] - 1
-        sc3["atoms"] = dict(sc["atoms"])
-        for k in ("x", "v", "omega"):
-            arr = np.zeros_like(sc["atoms"][k])
-            arr[idx] = a[k][order]
-            sc3["atoms"][k] = arr
+        sc3 = state_scenario(sc, eng.atoms())
         cval, ck = run_oracle_sample(sc3, args.cpu_seconds, 200)
         line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": 1, "kind": "port",
                                 "sample": "oracle port, 1 thread, same %d-particle state as the GPU window end, "

@@ -89,6 +89,8 @@ typedef struct {
     double t_integrate, t_pair_reverse, t_pair_main, t_forward, t_rebuild;
     long n_pair_main;            /* pair-pass launches timed                */
     long nsteps_rebuild;         /* steps that rebuilt the neighbour list   */
+    int maxrev, maxmesh;         /* reverse-entry and mesh-slot capacities  */
+    long ngrow;                  /* capacity growths (device reallocations) */
 } gb2_stats;
 
 /* contact census of the current state (device reduction): half-list entries,

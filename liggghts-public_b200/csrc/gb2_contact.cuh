@@ -28,6 +28,8 @@ struct ContactOut {
     double T[3];
 };
 
+#ifdef __CUDACC__   // device code; host-only units see the structs
+
 // sqrt(5/6) as written in src/normal_model_hertz.h:235
 #define GB2_SQRT_FIVE_OVER_SIX 0.91287092917527685576161630466800355658790782499663875
 
@@ -178,6 +180,131 @@ __device__ __forceinline__ void pair_contact(const MatPair &M, double delx, doub
     }
 }
 
+struct ContactOutF {
+    float F[3];
+    float T[3];
+};
+
+// Split-precision form of pair_contact: the same model chain (surface
+// default -> Hertz -> tangential history -> CDT rolling), evaluated in FP32
+// on operands the caller prepares in FP64 -- the relative position
+// del = x_i - x_j, its length r and the overlap deltan = radsum - r are
+// differenced in FP64 and only then rounded, so the near-touching overlap
+// (a difference of two nearly equal FP64 lengths) keeps its accuracy.  The
+// pair's own contribution is returned in `out` (for an in-order Kahan sum
+// by the caller); `shear` is updated in place when update_history is set.
+__device__ __forceinline__ void pair_contact_f32(const MatPair &M, float delx, float dely, float delz, float r,
+                                                 float deltan, float radi, float radj, const float vi[3],
+                                                 const float vj[3], const float wi[3], const float wj[3], float mi,
+                                                 float mj, float shear[3], bool update_history, float dt,
+                                                 bool rolling, bool tdamp, ContactOutF &out)
+{
+    const float rinv = 1.0f / r;
+    const float enx = delx * rinv;
+    const float eny = dely * rinv;
+    const float enz = delz * rinv;
+    const float meff = mi * mj / (mi + mj);
+
+    // surface model
+    const float vr1 = vi[0] - vj[0];
+    const float vr2 = vi[1] - vj[1];
+    const float vr3 = vi[2] - vj[2];
+    const float vn = vr1 * enx + vr2 * eny + vr3 * enz;
+    const float vt1 = vr1 - vn * enx;
+    const float vt2 = vr2 - vn * eny;
+    const float vt3 = vr3 - vn * enz;
+    const float cri = radi - 0.5f * deltan;
+    const float crj = radj - 0.5f * deltan;
+    const float wr1 = (cri * wi[0] + crj * wj[0]) * rinv;
+    const float wr2 = (cri * wi[1] + crj * wj[1]) * rinv;
+    const float wr3 = (cri * wi[2] + crj * wj[2]) * rinv;
+    const float vtr1 = vt1 - (delz * wr2 - dely * wr3);
+    const float vtr2 = vt2 - (delx * wr3 - delz * wr1);
+    const float vtr3 = vt3 - (dely * wr1 - delx * wr2);
+
+    // normal model (Hertz)
+    const float Yeff = (float)M.Yeff, Geff = (float)M.Geff, beta = (float)M.betaeff;
+    const float reff = radi * radj / (radi + radj);
+    const float sqrtval = sqrtf(reff * deltan);
+    const float Sn = 2.f * Yeff * sqrtval;
+    const float St = 8.f * Geff * sqrtval;
+    const float kn = (4.f / 3.f) * Yeff * sqrtval;
+    const float kt = St;
+    const float c56 = (float)GB2_SQRT_FIVE_OVER_SIX;
+    const float gamman = -2.f * c56 * beta * sqrtf(Sn * meff);
+    const float gammat = tdamp ? -2.f * c56 * beta * sqrtf(St * meff) : 0.f;
+    const float Fn = -gamman * vn + kn * deltan;
+    float F0 = Fn * enx, F1 = Fn * eny, F2 = Fn * enz;
+
+    // tangential model (history)
+    if (update_history) {
+        shear[0] += vtr1 * dt;
+        shear[1] += vtr2 * dt;
+        shear[2] += vtr3 * dt;
+        const float rsht = shear[0] * enx + shear[1] * eny + shear[2] * enz;
+        shear[0] -= rsht * enx;
+        shear[1] -= rsht * eny;
+        shear[2] -= rsht * enz;
+    }
+    const float shrmag = sqrtf(shear[0] * shear[0] + shear[1] * shear[1] + shear[2] * shear[2]);
+    float Ft1 = -(kt * shear[0]);
+    float Ft2 = -(kt * shear[1]);
+    float Ft3 = -(kt * shear[2]);
+    const float Ft_shear = kt * shrmag;
+    const float Ft_friction = (float)M.mu * fabsf(Fn);
+    if (Ft_shear > Ft_friction) {
+        if (shrmag != 0.f) {
+            const float ratio = Ft_friction / Ft_shear;
+            Ft1 *= ratio;
+            Ft2 *= ratio;
+            Ft3 *= ratio;
+            if (update_history) {
+                const float ktinv = 1.0f / kt;
+                shear[0] = -Ft1 * ktinv;
+                shear[1] = -Ft2 * ktinv;
+                shear[2] = -Ft3 * ktinv;
+            }
+        } else {
+            Ft1 = Ft2 = Ft3 = 0.f;
+        }
+    } else {
+        Ft1 -= gammat * vtr1;
+        Ft2 -= gammat * vtr2;
+        Ft3 -= gammat * vtr3;
+    }
+    F0 += Ft1;
+    F1 += Ft2;
+    F2 += Ft3;
+    float T0 = -cri * (eny * Ft3 - enz * Ft2);
+    float T1 = -cri * (enz * Ft1 - enx * Ft3);
+    float T2 = -cri * (enx * Ft2 - eny * Ft1);
+
+    // rolling model (CDT)
+    if (rolling) {
+        const float wrr0 = wi[0] - wj[0];
+        const float wrr1 = wi[1] - wj[1];
+        const float wrr2 = wi[2] - wj[2];
+        const float wr2sum = wrr0 * wrr0 + wrr1 * wrr1 + wrr2 * wrr2;
+        if (wr2sum > 0.f) {
+            const float sc = (float)M.mur * kn * deltan * reff * rsqrtf(wr2sum);
+            float rt0 = sc * wrr0, rt1 = sc * wrr1, rt2 = sc * wrr2;
+            const float d = rt0 * enx + rt1 * eny + rt2 * enz;
+            rt0 -= enx * d;
+            rt1 -= eny * d;
+            rt2 -= enz * d;
+            T0 -= rt0;
+            T1 -= rt1;
+            T2 -= rt2;
+        }
+    }
+    out.F[0] = F0;
+    out.F[1] = F1;
+    out.F[2] = F2;
+    out.T[0] = T0;
+    out.T[1] = T1;
+    out.T[2] = T2;
+}
+
 // Sphere-wall contact (primitive plane or mesh triangle), following
 // Walls::Granular::compute_force (src/fix_wall_gran_base.h:148-306) and the
 // is_wall branches of the model chain.  `d` is the vector from the wall
@@ -309,5 +436,7 @@ __device__ __forceinline__ void wall_contact(const MatPair &M, const double d[3]
     out.T[1] += T1;
     out.T[2] += T2;
 }
+
+#endif  // __CUDACC__
 
 }  // namespace gb2

@@ -1,0 +1,482 @@
+// gb2_device.cuh -- device helpers shared by every kernel of the granular
+// step: bin arithmetic, material lookup, the triangle-sphere narrow phase,
+// neighbour-record gathers, warp item enumeration and the wall contacts of
+// one atom.  Included by both compiled units (the bit-exact FP64 unit built
+// with --fmad=false and the split-precision unit), so everything here is a
+// header-only __device__ function.
+#pragma once
+
+#include "gb2_internal.h"
+
+namespace gb2 {
+__device__ __forceinline__ dbl4 ld4(const dbl4 *p) { return *p; }
+
+__device__ __forceinline__ flt8 make_kin(const dbl4 &v, const dbl4 &w)
+{
+    flt8 k;
+    k.vx = (float)v.x;
+    k.vy = (float)v.y;
+    k.vz = (float)v.z;
+    k.m = (float)v.w;
+    k.wx = (float)w.x;
+    k.wy = (float)w.y;
+    k.wz = (float)w.z;
+    k.pad = 0.0f;
+    return k;
+}
+
+__device__ __forceinline__ int coord2bin3(const Dev &D, double x0, double x1, double x2, int &ix, int &iy, int &iz)
+{
+    // Neighbor::coord2bin src/neighbor.cpp:2112
+    const double x[3] = {x0, x1, x2};
+    int idx[3];
+    for (int d = 0; d < 3; d++) {
+        int v;
+        if (x[d] >= D.bboxhi[d])
+            v = static_cast<int>((x[d] - D.bboxhi[d]) * D.bininv[d]) + D.nbin[d];
+        else if (x[d] >= D.bboxlo[d]) {
+            v = static_cast<int>((x[d] - D.bboxlo[d]) * D.bininv[d]);
+            v = min(v, D.nbin[d] - 1);
+        } else
+            v = static_cast<int>((x[d] - D.bboxlo[d]) * D.bininv[d]) - 1;
+        idx[d] = v - D.mbinlo[d];
+    }
+    ix = idx[0];
+    iy = idx[1];
+    iz = idx[2];
+    return iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
+}
+
+__device__ __forceinline__ int coord2bin(const Dev &D, double x0, double x1, double x2)
+{
+    int a, b, c;
+    return coord2bin3(D, x0, x1, x2, a, b, c);
+}
+
+__device__ __forceinline__ const MatPair &mat(const Dev &D, int ti, int tj)
+{
+    return D.mat[ti * (kMaxTypes + 1) + tj];
+}
+
+
+// ------------------------------------------------------------------
+// mesh support
+
+__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// TriMesh::resolveTriSphereNeighbuild (src/tri_mesh_I.h:255)
+__device__ __forceinline__ bool tri_neighbuild(const TriGeom &T, double rSphere, const double c[3], double treshold)
+{
+    const double maxDist = rSphere + treshold;
+    double v[3] = {c[0] - T.center[0], c[1] - T.center[1], c[2] - T.center[2]};
+    const double dNorm = fabs(dot3(T.surfnorm, v));
+    if (dNorm > maxDist) return false;
+    const double dParaMax = maxDist * maxDist;
+    for (int k = 0; k < 3; k++) {
+        double w[3] = {c[0] - T.node[k][0], c[1] - T.node[k][1], c[2] - T.node[k][2]};
+        const double d = dot3(T.edgenorm[k], w);
+        if (d > 0 && d * d > dParaMax) return false;
+    }
+    return true;
+}
+
+
+// TriMesh::resolveTriSphereContactBary and its edge/corner/face helpers
+// (src/tri_mesh_I.h:65-251).  Returns distance - radius; LARGE (1e6) for an
+// inactive feature.
+__device__ __forceinline__ double calc_dist(const double *cs, const double *cp, double *delta)
+{
+    delta[0] = cp[0] - cs[0];
+    delta[1] = cp[1] - cs[1];
+    delta[2] = cp[2] - cs[2];
+    const double d2 = (cs[0] - cp[0]) * (cs[0] - cp[0]) + (cs[1] - cp[1]) * (cs[1] - cp[1]) +
+                      (cs[2] - cp[2]) * (cs[2] - cp[2]);
+    return sqrt(d2);
+}
+
+#define GB2_SMALL_TRIMESH 1.e-10
+#define GB2_LARGE_TRIMESH 1000000
+#define GB2_EDGE_ACTIVE(T, k) (((T).active >> (k)) & 1)
+#define GB2_CORNER_ACTIVE(T, k) (((T).active >> (3 + (k))) & 1)
+
+static __device__ double tri_edge(const TriGeom &T, int iEdge, const double *p, double *delta)
+{
+    const int ip = (iEdge + 1) % 3;
+    double nodeToP[3] = {p[0] - T.node[iEdge][0], p[1] - T.node[iEdge][1], p[2] - T.node[iEdge][2]};
+    const double distFromNode = dot3(nodeToP, T.edgevec[iEdge]);
+    if (distFromNode < -GB2_SMALL_TRIMESH) {
+        if (!GB2_CORNER_ACTIVE(T, iEdge)) return GB2_LARGE_TRIMESH;
+        return calc_dist(p, T.node[iEdge], delta);
+    } else if (distFromNode > T.edgelen[iEdge] + GB2_SMALL_TRIMESH) {
+        if (!GB2_CORNER_ACTIVE(T, ip)) return GB2_LARGE_TRIMESH;
+        return calc_dist(p, T.node[ip], delta);
+    }
+    if (!GB2_EDGE_ACTIVE(T, iEdge)) return GB2_LARGE_TRIMESH;
+    double cp[3];
+    cp[0] = T.node[iEdge][0] + distFromNode * T.edgevec[iEdge][0];
+    cp[1] = T.node[iEdge][1] + distFromNode * T.edgevec[iEdge][1];
+    cp[2] = T.node[iEdge][2] + distFromNode * T.edgevec[iEdge][2];
+    return calc_dist(p, cp, delta);
+}
+
+static __device__ double tri_corner(const TriGeom &T, int iNode, bool obtuse, const double *p, double *delta)
+{
+    const int ip = (iNode + 1) % 3, ipp = (iNode + 2) % 3;
+    const double *n = T.node[iNode];
+    if (obtuse) {
+        double nodeToP[3] = {p[0] - n[0], p[1] - n[1], p[2] - n[2]};
+        double cp[3];
+        double distFromNode = dot3(nodeToP, T.edgevec[ipp]);
+        if (distFromNode < GB2_SMALL_TRIMESH) {
+            if (distFromNode > -T.edgelen[ipp]) {
+                if (!GB2_EDGE_ACTIVE(T, ipp)) return GB2_LARGE_TRIMESH;
+                cp[0] = n[0] + distFromNode * T.edgevec[ipp][0];
+                cp[1] = n[1] + distFromNode * T.edgevec[ipp][1];
+                cp[2] = n[2] + distFromNode * T.edgevec[ipp][2];
+                return calc_dist(p, cp, delta);
+            }
+            if (!GB2_CORNER_ACTIVE(T, ipp)) return GB2_LARGE_TRIMESH;
+            return calc_dist(p, T.node[ipp], delta);
+        }
+        distFromNode = dot3(nodeToP, T.edgevec[iNode]);
+        if (distFromNode > -GB2_SMALL_TRIMESH) {
+            if (distFromNode < T.edgelen[iNode]) {
+                if (!GB2_EDGE_ACTIVE(T, iNode)) return GB2_LARGE_TRIMESH;
+                cp[0] = n[0] + distFromNode * T.edgevec[iNode][0];
+                cp[1] = n[1] + distFromNode * T.edgevec[iNode][1];
+                cp[2] = n[2] + distFromNode * T.edgevec[iNode][2];
+                return calc_dist(p, cp, delta);
+            }
+            if (!GB2_CORNER_ACTIVE(T, ip)) return GB2_LARGE_TRIMESH;
+            return calc_dist(p, T.node[ip], delta);
+        }
+    }
+    if (!GB2_CORNER_ACTIVE(T, iNode)) return GB2_LARGE_TRIMESH;
+    return calc_dist(p, T.node[iNode], delta);
+}
+
+static __device__ double tri_sphere(const TriGeom &T, double rSphere, const double *cs, double *delta, int &barySign,
+                             double precision)
+{
+    double n0ToC[3] = {cs[0] - T.node[0][0], cs[1] - T.node[0][1], cs[2] - T.node[0][2]};
+    // MathExtraLiggghts::calcBaryTriCoords (src/math_extra_liggghts.h:559)
+    const double a = dot3(n0ToC, T.edgevec[0]);
+    const double b = dot3(n0ToC, T.edgevec[2]);
+    const double c = dot3(T.edgevec[0], T.edgevec[2]);
+    const double oneMinCSqr = 1 - c * c;
+    double bary[3];
+    bary[1] = (a - b * c) / (T.edgelen[0] * oneMinCSqr);
+    bary[2] = (a * c - b) / (T.edgelen[2] * oneMinCSqr);
+    bary[0] = 1. - bary[1] - bary[2];
+    const double invlen = 1. / (2. * T.rbound);
+    barySign = (bary[0] > -precision * invlen) + 2 * (bary[1] > -precision * invlen) +
+               4 * (bary[2] > -precision * invlen);
+    double d;
+    switch (barySign) {
+    case 1: d = tri_corner(T, 0, T.obtuse == 0, cs, delta); break;
+    case 2: d = tri_corner(T, 1, T.obtuse == 1, cs, delta); break;
+    case 3: d = tri_edge(T, 0, cs, delta); break;
+    case 4: d = tri_corner(T, 2, T.obtuse == 2, cs, delta); break;
+    case 5: d = tri_edge(T, 2, cs, delta); break;
+    case 6: d = tri_edge(T, 1, cs, delta); break;
+    case 7: {
+        const double dNorm = dot3(T.surfnorm, n0ToC);
+        const double tmp[3] = {T.surfnorm[0] * dNorm, T.surfnorm[1] * dNorm, T.surfnorm[2] * dNorm};
+        const double csPlane[3] = {cs[0] - tmp[0], cs[1] - tmp[1], cs[2] - tmp[2]};
+        d = calc_dist(cs, csPlane, delta);
+        break;
+    }
+    default: d = 1.; break;
+    }
+    return d - rSphere;
+}
+
+__device__ __forceinline__ bool coplanar_node_neighs(const MeshDev &M, int a, int b)
+{
+    for (int q = M.cnn_start[a]; q < M.cnn_start[a + 1]; q++)
+        if (M.cnn_list[q] == b) return true;
+    return false;
+}
+
+// ------------------------------------------------------------------
+// pair passes.  Both walk a per-atom list in two phases: a screening phase
+// issues the neighbour-position gathers of all entries independently (so
+// many loads are in flight per thread) and records which entries touch in a
+// bit mask; the compute phase then evaluates only touching entries, in list
+// order, so the per-atom sums keep the reference's order.
+
+// One 32-byte record through the read-only path as a single 256-bit load
+// (sm_100 vector width): a scattered warp-wide gather then needs one L1
+// wavefront per lane's line instead of two.  Records are 32-byte aligned.
+__device__ __forceinline__ dbl4 ldg4(const dbl4 *p)
+{
+    dbl4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+    return r;
+}
+
+// One split-precision kinematics record (eight FP32 values) as one 256-bit
+// read-only load.
+__device__ __forceinline__ flt8 ldg8f(const flt8 *p)
+{
+    flt8 r;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r.vx), "=f"(r.vy), "=f"(r.vz), "=f"(r.m), "=f"(r.wx), "=f"(r.wy), "=f"(r.wz), "=f"(r.pad)
+        : "l"(p));
+    return r;
+}
+
+__device__ __forceinline__ bool touching(const dbl4 &a, const dbl4 &b)
+{
+    const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    const double rs = a.w + b.w;
+    return dx * dx + dy * dy + dz * dz < rs * rs;
+}
+
+// Warp-cooperative evaluation of the touching entries found by screening.
+// The warp's touching entries are enumerated owner-lane-major (each owner's
+// entries in list order); in rounds of 32, lane t evaluates item base+t and
+// leaves the pair's raw contribution in shared memory, then every owner lane
+// adds the items it owns in order.  The per-atom sums therefore keep the
+// reference's order while the FP64 contact arithmetic runs on full warps.
+struct WarpItems {
+    int cnt, excl, total;
+};
+
+__device__ __forceinline__ WarpItems warp_items(unsigned long long mask)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    WarpItems it;
+    it.cnt = __popcll(mask);
+    int x = it.cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    it.excl = x - it.cnt;
+    it.total = __shfl_sync(FULL, x, 31);
+    return it;
+}
+
+// Index stream loads: read once per step, evict-first so they do not push
+// the neighbour records out of L2
+__device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
+
+// Screening of the j-side (rev) and own (nbr) entries of one atom in one
+// loop: per round two indices of each list, then four independent record
+// gathers, then the distance tests.  Both lists are <= 64 entries here.
+__device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn, const dbl4 &pk,
+                                            unsigned long long &mrev, unsigned long long &mown)
+{
+    const int cap = D.cap;
+    const int n = max(nr, nn);
+    for (int t = 0; t < n; t += 2) {
+        const int a0 = (t < nr) ? ld_stream(&D.rev[t * cap + k]) : k;
+        const int a1 = (t + 1 < nr) ? ld_stream(&D.rev[(t + 1) * cap + k]) : k;
+        const int b0 = (t < nn) ? ld_stream(&D.nbr[t * cap + k]) : k;
+        const int b1 = (t + 1 < nn) ? ld_stream(&D.nbr[(t + 1) * cap + k]) : k;
+        const dbl4 qa0 = ldg4(&D.pos[a0]);
+        const dbl4 qa1 = ldg4(&D.pos[a1]);
+        const dbl4 qb0 = ldg4(&D.pos[b0]);
+        const dbl4 qb1 = ldg4(&D.pos[b1]);
+        if (t < nr && touching(pk, qa0)) mrev |= 1ull << t;
+        if (t + 1 < nr && touching(pk, qa1)) mrev |= 1ull << (t + 1);
+        if (t < nn && touching(pk, qb0)) mown |= 1ull << t;
+        if (t + 1 < nn && touching(pk, qb1)) mown |= 1ull << (t + 1);
+    }
+}
+
+// Screening of n <= 64 list entries idx[r*cap + k]: four index loads, then
+// four independent neighbour-record gathers, then the four distance tests,
+// so a thread keeps several loads in flight.  Returns the touching mask.
+__device__ __forceinline__ unsigned long long screen_entries(const int *__restrict__ idx, int cap, int k, int n,
+                                                            const dbl4 &pk, const dbl4 *__restrict__ pos)
+{
+    unsigned long long m = 0ull;
+    for (int r0 = 0; r0 < n; r0 += 4) {
+        const int j0 = __ldg(&idx[min(r0 + 0, n - 1) * cap + k]);
+        const int j1 = __ldg(&idx[min(r0 + 1, n - 1) * cap + k]);
+        const int j2 = __ldg(&idx[min(r0 + 2, n - 1) * cap + k]);
+        const int j3 = __ldg(&idx[min(r0 + 3, n - 1) * cap + k]);
+        const dbl4 q0 = ldg4(&pos[j0]);
+        const dbl4 q1 = ldg4(&pos[j1]);
+        const dbl4 q2 = ldg4(&pos[j2]);
+        const dbl4 q3 = ldg4(&pos[j3]);
+        if (touching(pk, q0)) m |= 1ull << r0;
+        if (r0 + 1 < n && touching(pk, q1)) m |= 1ull << (r0 + 1);
+        if (r0 + 2 < n && touching(pk, q2)) m |= 1ull << (r0 + 2);
+        if (r0 + 3 < n && touching(pk, q3)) m |= 1ull << (r0 + 3);
+    }
+    return m;
+}
+
+__device__ __forceinline__ WarpItems warp_items_cnt(int cnt)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    WarpItems it;
+    it.cnt = cnt;
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    it.excl = x - cnt;
+    it.total = __shfl_sync(FULL, x, 31);
+    return it;
+}
+
+// owner lane of item w: the largest lane whose exclusive prefix is <= w
+__device__ __forceinline__ int item_owner(int w, int excl)
+{
+    const unsigned FULL = 0xffffffffu;
+    int L = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const int cand = L + step;
+        const int ex = __shfl_sync(FULL, excl, cand & 31);
+        if (cand < 32 && ex <= w) L = cand;
+    }
+    return L;
+}
+
+__device__ __forceinline__ int nth_set_bit(unsigned long long m, int rank)
+{
+    for (int q = 0; q < rank; q++) m &= m - 1ull;
+    return __ffsll((long long)m) - 1;
+}
+
+__device__ __forceinline__ unsigned long long shfl64(unsigned long long v, int src)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lo = __shfl_sync(FULL, (unsigned)(v & 0xffffffffull), src);
+    const unsigned hi = __shfl_sync(FULL, (unsigned)(v >> 32), src);
+    return ((unsigned long long)hi << 32) | lo;
+}
+
+__device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, int i, const dbl4 &p, const double v[3],
+                               const double w[3], double mass, int itype, bool upd, ContactOut &acc)
+{
+    const int cap = D.cap;
+    const int nn = M.tcnt[i];
+    if (nn == 0) return;
+    unsigned long long keep = 0ull;   // markAllContacts
+    const double cs[3] = {p.x, p.y, p.z};
+    const double vwall[3] = {0.0, 0.0, 0.0};
+    int np = M.snp[i];
+    for (int q = 0; q < nn; q++) {
+        const int t = M.tlist[q * cap + i];
+        const TriGeom &T = M.tri[t];
+        double delta[3];
+        int barysign = -1;
+        const double deltan = tri_sphere(T, p.w, cs, delta, barysign, 1e-8);
+        if (deltan > D.cutneighmax) continue;
+        if (!(deltan <= 0)) continue;
+        const bool faceflag = (7 == barysign);
+        // FixContactHistoryMesh::handleContact
+        int slot = -1;
+        for (int k = 0; k < nn; k++)
+            if (M.spartner[k * cap + i] == t) {
+                slot = k;
+                break;
+            }
+        if (slot >= 0) {
+            keep |= 1ull << slot;
+        } else {
+            bool skip = false;
+            if (faceflag) {
+                for (int k = 0; k < nn; k++) {
+                    const int idp = M.spartner[k * cap + i];
+                    if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) {
+                        skip = true;
+                        break;
+                    }
+                }
+            }
+            if (skip) continue;
+            int ic = -1;
+            for (int k = 0; k < nn; k++)
+                if (-1 == M.spartner[k * cap + i]) {
+                    ic = k;
+                    break;
+                }
+            if (ic < 0 || np >= nn) {
+                atomicOr(D.status, ST_MESH_INTERNAL);
+                continue;
+            }
+            M.spartner[ic * cap + i] = t;
+            keep |= 1ull << ic;
+            double h0 = 0.0, h1 = 0.0, h2 = 0.0;
+            np++;
+            if (faceflag) {
+                for (int k = 0; k < nn; k++) {
+                    const int tri = M.spartner[k * cap + i];
+                    if (tri >= 0 && tri != t && coplanar_node_neighs(M, tri, t)) {
+                        h0 = M.shist[(3 * k + 0) * cap + i];
+                        h1 = M.shist[(3 * k + 1) * cap + i];
+                        h2 = M.shist[(3 * k + 2) * cap + i];
+                    }
+                }
+            }
+            M.shist[(3 * ic + 0) * cap + i] = h0;
+            M.shist[(3 * ic + 1) * cap + i] = h1;
+            M.shist[(3 * ic + 2) * cap + i] = h2;
+            slot = ic;
+        }
+        double sh[3] = {M.shist[(3 * slot + 0) * cap + i], M.shist[(3 * slot + 1) * cap + i],
+                        M.shist[(3 * slot + 2) * cap + i]};
+        const double dvec[3] = {-delta[0], -delta[1], -delta[2]};
+        wall_contact(mat(D, itype, M.wtype), dvec, -deltan, p.w, v, w, vwall, mass, sh, upd, D.dt, M.rolling != 0,
+                     D.tdamp != 0, acc);
+        M.shist[(3 * slot + 0) * cap + i] = sh[0];
+        M.shist[(3 * slot + 1) * cap + i] = sh[1];
+        M.shist[(3 * slot + 2) * cap + i] = sh[2];
+    }
+    // cleanUpContacts
+    for (int k = 0; k < nn; k++)
+        if (!((keep >> k) & 1ull)) {
+            if (M.spartner[k * cap + i] > -1) np--;
+            M.spartner[k * cap + i] = -1;
+            M.shist[(3 * k + 0) * cap + i] = 0.0;
+            M.shist[(3 * k + 1) * cap + i] = 0.0;
+            M.shist[(3 * k + 2) * cap + i] = 0.0;
+        }
+    M.snp[i] = np;
+}
+
+// FixWallGran::post_force_primitive for one atom in the plane's neighbour
+// list (src/fix_wall_gran.cpp:1024-1148, Plane<dim>::resolveContact
+// src/primitive_wall_definitions.h:133)
+__device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, int i, const dbl4 &pi, const double *vi,
+                                             const double *wi, double mass, int ti, bool upd, ContactOut &acc)
+{
+    const int cap = D.cap;
+    const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+    double delta_d, deltan;
+    delta_d = F.pos - x;
+    if (x > F.pos)
+        deltan = x - F.pos - pi.w;
+    else
+        deltan = F.pos - x - pi.w;
+    if (deltan > D.cutneighmax) return;
+    if (deltan <= 0) {
+        // -delta with constant indices only (keeps d in registers)
+        const double d[3] = {F.dim == 0 ? -delta_d : -0., F.dim == 1 ? -delta_d : -0., F.dim == 2 ? -delta_d : -0.};
+        double sh[3] = {F.whist[0 * cap + i], F.whist[1 * cap + i], F.whist[2 * cap + i]};
+        const double vwall[3] = {0., 0., 0.};
+        wall_contact(mat(D, ti, F.wtype), d, -deltan, pi.w, vi, wi, vwall, mass, sh, upd, D.dt, F.rolling != 0,
+                     D.tdamp != 0, acc);
+        F.whist[0 * cap + i] = sh[0];
+        F.whist[1 * cap + i] = sh[1];
+        F.whist[2 * cap + i] = sh[2];
+    } else {
+        F.whist[0 * cap + i] = 0.0;
+        F.whist[1 * cap + i] = 0.0;
+        F.whist[2 * cap + i] = 0.0;
+    }
+}
+
+}  // namespace gb2

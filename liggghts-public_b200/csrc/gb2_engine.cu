@@ -25,6 +25,7 @@
 #include "../../include/granb200.h"
 #include "gb2_internal.h"
 #include "gb2_kernels.cuh"
+#include "gb2_step.cuh"
 
 using namespace gb2;
 
@@ -118,6 +119,8 @@ struct gb2_ctx {
     std::vector<double> h_radius;
     std::vector<int> h_type;
     DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, fpart, tpart, xhold;
+    bool split = false;           // GB2_PREC_SPLIT
+    DBuf<flt8> kin, kin2;         // split precision: FP32 kinematics records (double-buffered like vel)
     DBuf<uint8_t> revs;
     int minb = 4;                 // register-allocation target of the pair step kernel (blocks/SM)
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
@@ -138,7 +141,8 @@ struct gb2_ctx {
     DBuf<unsigned> keys, keys2;
     DBuf<uint8_t> bflags;
     DBuf<char> cubtmp;
-    DBuf<int> dstatus, ddflag;
+    DBuf<int> dstatus, ddflag, dneed;
+    long ngrow = 0;
     int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel
     // neighbor
     double cutneighmax = 0, triggersq = 0;
@@ -208,6 +212,8 @@ Dev make_dev(gb2_ctx *c)
     D.pos_out = c->pos2.p;
     D.vel_out = c->vel2.p;
     D.omg_out = c->omg2.p;
+    D.kin = c->split ? c->kin.p : nullptr;
+    D.kin_out = c->split ? c->kin2.p : nullptr;
     D.type = c->type.p;
     D.tag = c->tag.p;
     D.f = c->f.p;
@@ -288,6 +294,7 @@ Dev make_dev(gb2_ctx *c)
     }
     D.status = c->dstatus.p;
     D.dflag = c->ddflag.p;
+    D.need = c->dneed.p;
     return D;
 }
 
@@ -368,6 +375,10 @@ int ensure_nmax(gb2_ctx *c, int need)
     CK(c->pos2.grow_keep(nm, 0, c->st));
     CK(c->vel2.grow_keep(nm, 0, c->st));
     CK(c->omg2.grow_keep(nm, 0, c->st));
+    if (c->split) {
+        CK(c->kin.grow_keep(nm, keep, c->st));
+        CK(c->kin2.grow_keep(nm, 0, c->st));
+    }
     CK(c->type.grow_keep(nm, keep, c->st));
     CK(c->tag.grow_keep(nm, keep, c->st));
     CK(c->gsrc.grow_keep(nm, (size_t)c->nghost, c->st));
@@ -551,6 +562,18 @@ int mesh_bins(gb2_ctx *c, MeshFix &M)
 
 // ---------------------------------------------------------------- rebuild parts
 
+// New capacity after an overflow: at least double, and half again the
+// largest demand the overflowing kernel recorded in need[which], so a
+// growing bed reallocates rarely (each reallocation synchronises the device).
+int grown_capacity(gb2_ctx *c, int which, int old, int limit)
+{
+    int need = 0;
+    if (cudaMemcpy(&need, c->dneed.p + which, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) need = 0;
+    const long cap = std::max<long>(2l * old, (3l * need + 1) / 2);
+    c->ngrow++;
+    return (int)std::min<long>(cap, limit);
+}
+
 int do_partners(gb2_ctx *c)
 {
     for (int attempt = 0; attempt < 8; attempt++) {
@@ -561,7 +584,7 @@ int do_partners(gb2_ctx *c)
         int st;
         if (read_status(c, &st)) return GB2_ERR_CUDA;
         if (!(st & ST_PARTNER_OVERFLOW)) return 0;
-        c->maxp *= 2;
+        c->maxp = grown_capacity(c, 1, c->maxp, 1 << 20);
         CK(c->ptag.alloc((size_t)c->maxp * c->cap));
         CK(c->phist.alloc((size_t)3 * c->maxp * c->cap));
     }
@@ -710,8 +733,8 @@ int do_build(gb2_ctx *c)
         if (read_status(c, &st)) return GB2_ERR_CUDA;
         if (st & ST_LOST_ATOM) return set_err(c, GB2_ERR_LOST, "an atom is outside the binned domain");
         if (!(st & ST_NEIGH_OVERFLOW)) break;
-        c->maxn *= 2;
-        if (c->maxn > 256) return set_err(c, GB2_ERR_CAPACITY, "more than 256 neighbours per atom");
+        if (c->maxn >= 256) return set_err(c, GB2_ERR_CAPACITY, "more than 256 neighbours per atom");
+        c->maxn = grown_capacity(c, 0, c->maxn, 256);
         CK(c->nbr.alloc((size_t)c->maxn * c->cap));
         CK(c->flag.alloc((size_t)c->maxn * c->cap));
         CK(c->hist.alloc((size_t)3 * c->maxn * c->cap));
@@ -727,7 +750,7 @@ int do_build(gb2_ctx *c)
         int st;
         if (read_status(c, &st)) return GB2_ERR_CUDA;
         if (!(st & ST_REV_OVERFLOW)) break;
-        c->maxr *= 2;
+        c->maxr = grown_capacity(c, 2, c->maxr, 1 << 20);
         CK(c->rev.alloc((size_t)c->maxr * c->cap));
         CK(c->revs.alloc((size_t)c->maxr * c->cap));
         if (attempt == 7) return set_err(c, GB2_ERR_CAPACITY, "reverse list capacity could not be grown");
@@ -767,8 +790,8 @@ int do_pre_force(gb2_ctx *c)
                 int st;
                 if (read_status(c, &st)) return GB2_ERR_CUDA;
                 if (!(st & ST_MESHSLOT_OVERFLOW)) break;
-                M.maxt *= 2;
-                if (M.maxt > 64) return set_err(c, GB2_ERR_CAPACITY, "more than 64 candidate triangles per atom");
+                if (M.maxt >= 64) return set_err(c, GB2_ERR_CAPACITY, "more than 64 candidate triangles per atom");
+                M.maxt = grown_capacity(c, 3, M.maxt, 64);
                 M.tlist.release();
             }
             // re-page history into buffers sized for the new capacity
@@ -814,17 +837,27 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
     if (do_borders(c)) return GB2_ERR_CUDA;
     if (do_build(c)) return c->err.empty() ? GB2_ERR_CUDA : GB2_ERR_CAPACITY;
     if (do_pre_force(c)) return GB2_ERR_CUDA;
+    if (c->split) {   // FP32 kinematics of owned atoms and the new ghosts
+        const int nall = c->nlocal + c->nghost;
+        Dev D2 = make_dev(c);
+        if (nall > 0) k_make_kin<<<nblk(nall), kBlock, 0, c->st>>>(D2, nall);
+        CKL();
+    }
     return 0;
 }
 
 template <bool R, int MINB>
 void launch_step_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
-    k_pair_step<R, MINB><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    k_pair_step<R, MINB, false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
 void launch_step(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
+    if (c->split) {
+        launch_step_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f);
+        return;
+    }
     // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
     if (c->P.rolling_cdt) {
         if (c->minb == 6) launch_step_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
@@ -848,6 +881,7 @@ int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int stor
     if (integrate) {
         c->vel.swap(c->vel2);
         c->omg.swap(c->omg2);
+        if (c->split) c->kin.swap(c->kin2);
         if (fuse_next) c->pos.swap(c->pos2);
     }
     c->fused_pending = integrate && fuse_next;
@@ -937,9 +971,10 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     *out = nullptr;
     if (p->ntypes < 1 || p->ntypes > kMaxTypes) return GB2_ERR_ARG;
     if (p->dt <= 0 || p->skin < 0) return GB2_ERR_ARG;
-    if (p->precision != GB2_PREC_FP64) return GB2_ERR_UNSUPPORTED;
+    if (p->precision != GB2_PREC_FP64 && p->precision != GB2_PREC_SPLIT) return GB2_ERR_UNSUPPORTED;
     gb2_ctx *c = new gb2_ctx();
     c->P = *p;
+    c->split = p->precision == GB2_PREC_SPLIT;
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
     if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
     cudaError_t e = cudaSetDevice(p->device);
@@ -949,7 +984,8 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&c->h_pinned, 4 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
-        c->ddflag.alloc(1) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
+        c->ddflag.alloc(1) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess ||
+        cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
         cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         return GB2_ERR_CUDA;
@@ -1478,6 +1514,10 @@ int gb2_get_stats(gb2_ctx *c, gb2_stats *s)
     s->time_other = s->t_integrate + s->t_forward;
     s->n_pair_main = c->n_pair_main;
     s->nsteps_rebuild = c->nsteps_rebuild;
+    s->maxrev = c->maxr;
+    for (int k = 0; k < c->nfix; k++)
+        if (c->fix[k].mesh) s->maxmesh = std::max(s->maxmesh, c->fix[k].mesh->maxt);
+    s->ngrow = c->ngrow;
     return 0;
 }
 

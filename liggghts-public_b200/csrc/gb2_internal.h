@@ -18,6 +18,8 @@
 //   contact-history partners (FixContactHistory::partner_, keyed by tag):
 //     pnum[i], ptag[s*cap+i], phist[(3s+c)*cap+i]
 //   ghosts: gsrc[g] (owned source atom), gshift[g] {dx, dy, dz, -}
+//   split precision: kin {vx, vy, vz, m, wx, wy, wz, -} as FP32 (32 bytes),
+//     the neighbour-side operands of the FP32 contact math
 #pragma once
 
 #include <cstdint>
@@ -31,6 +33,13 @@ namespace gb2 {
 
 struct __align__(32) dbl4 {
     double x, y, z, w;
+};
+
+// split-precision kinematics record of one atom (one 32-byte sector):
+// velocity, mass and angular velocity rounded to FP32 for the contact math
+struct __align__(32) flt8 {
+    float vx, vy, vz, m;
+    float wx, wy, wz, pad;
 };
 
 constexpr int kMaxTypes = 8;      // material table is [kMaxTypes+1]^2
@@ -100,6 +109,7 @@ struct Dev {
     int nlocal, nghost, nmax, cap;   // cap: stride of slot-major arrays (>= nlocal)
     dbl4 *pos, *vel, *omg;
     dbl4 *pos_out, *vel_out, *omg_out;   // integrate targets (double buffer: pass B reads neighbours' state)
+    flt8 *kin, *kin_out;                 // split precision only (null in the FP64 path)
     int *type, *tag;
     dbl4 *f, *tq, *fpart, *tpart, *xhold;
     // half list
@@ -137,6 +147,8 @@ struct Dev {
     FixDev fix[kMaxFix];
     int *status;
     int *dflag;              // displacement trigger
+    int *need;               // [4] capacity demand seen by the last overflowing kernel:
+                             // neighbour slots, partners, reverse entries, mesh slots
 };
 
 // host-side mesh topology (gb2_mesh.cpp)
@@ -147,6 +159,9 @@ struct MeshTopo {
 };
 bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, double precision, MeshTopo &out,
                          std::string &err);
+// split-precision pair step (gb2_split.cu)
+void launch_step_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
+                       int fuse_next, int store_f);
 bool tri_neighbuild_host(const TriGeom &T, double rSphere, const double *c, double treshold);
 
 }  // namespace gb2

@@ -1,0 +1,33 @@
+// gb2_split.cu -- split-precision instantiation of the fused pair step.
+//
+// Same kernel source as the FP64 path (gb2_step.cuh) with SPLIT = true:
+// neighbour screening, positions, the overlap of each touching pair, walls,
+// gravity and the Velocity-Verlet integration stay FP64; the sphere-sphere
+// contact chain runs in FP32 on FP64-differenced relative positions and the
+// per-atom pair sums are FP32 with Kahan compensation.  This unit is built
+// with FMA contraction and the fast FP32 intrinsics allowed; the FP64 unit
+// is not.
+#include "gb2_step.cuh"
+
+namespace gb2 {
+
+template <bool R, int MINB>
+static void launch(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
+                   int store_f)
+{
+    k_pair_step<R, MINB, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
+}
+
+void launch_step_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
+                       int fuse_next, int store_f)
+{
+    if (D.rolling) {
+        if (minb == 6) launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+    } else {
+        if (minb == 6) launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+    }
+}
+
+}  // namespace gb2

@@ -1,0 +1,330 @@
+// gb2_step.cuh -- the fused pair-step kernel (one full time step per owned
+// atom).  Instantiated with SPLIT=false by the bit-exact FP64 unit and with
+// SPLIT=true by the split-precision unit (gb2_split.cu).
+#pragma once
+
+#include <type_traits>
+
+#include "gb2_device.cuh"
+
+namespace gb2 {
+// An atom with more than 64 reverse or own entries, evaluated serially in
+// the reference order (rare; kept out of line so the hot loop stays small).
+template <bool ROLLING>
+__device__ __forceinline__ void serial_atom(const Dev &D, int k, const dbl4 &pk, const dbl4 &vi4, const dbl4 &wi4, int tk,
+                                         int nr, int nn, bool upd, ContactOut &acc)
+{
+    const int cap = D.cap;
+    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
+    // more than 64 entries on one side: every entry in order on this lane
+    for (int r = 0; r < nr; r++) {
+        const int i = __ldg(&D.rev[r * cap + k]);
+        const dbl4 pi = ldg4(&D.pos[i]);
+        const double delx = pk.x - pi.x;
+        const double dely = pk.y - pi.y;
+        const double delz = pk.z - pi.z;
+        const double rsq = delx * delx + dely * dely + delz * delz;
+        const double radsum = pk.w + pi.w;
+        if (!(rsq < radsum * radsum)) continue;
+        const int s = D.revs[r * cap + k];
+        const dbl4 v4 = ldg4(&D.vel[i]), w4 = ldg4(&D.omg[i]);
+        const double vi[3] = {v4.x, v4.y, v4.z}, wi[3] = {w4.x, w4.y, w4.z};
+        double sh[3];
+        sh[0] = -D.hist[(3 * s + 0) * cap + i];
+        sh[1] = -D.hist[(3 * s + 1) * cap + i];
+        sh[2] = -D.hist[(3 * s + 2) * cap + i];
+        pair_contact(mat(D, D.type[i], tk), delx, dely, delz, rsq, pk.w, pi.w, vk, vi, wk, wi, vi4.w, v4.w, sh,
+                     upd, D.dt, ROLLING, D.tdamp != 0, acc);
+    }
+    for (int s = 0; s < nn; s++) {
+        const int e = s * cap + k;
+        const int j = __ldg(&D.nbr[e]);
+        const dbl4 pj = ldg4(&D.pos[j]);
+        const double delx = pk.x - pj.x;
+        const double dely = pk.y - pj.y;
+        const double delz = pk.z - pj.z;
+        const double rsq = delx * delx + dely * dely + delz * delz;
+        const double radsum = pk.w + pj.w;
+        double sh[3] = {D.hist[(3 * s + 0) * cap + k], D.hist[(3 * s + 1) * cap + k],
+                        D.hist[(3 * s + 2) * cap + k]};
+        if (rsq < radsum * radsum) {
+            const dbl4 v4 = ldg4(&D.vel[j]), w4 = ldg4(&D.omg[j]);
+            const double vj[3] = {v4.x, v4.y, v4.z}, wj[3] = {w4.x, w4.y, w4.z};
+            const int fl = D.flag[e];
+            if ((fl | 5) != fl) D.flag[e] = fl | 5;
+            pair_contact(mat(D, tk, D.type[j]), delx, dely, delz, rsq, pk.w, pj.w, vk, vj, wk, wj, vi4.w, v4.w,
+                         sh, upd, D.dt, ROLLING, D.tdamp != 0, acc);
+        }
+        if (upd) {   // serial atoms write every slot
+            D.hist_out[(3 * s + 0) * cap + k] = sh[0];
+            D.hist_out[(3 * s + 1) * cap + k] = sh[1];
+            D.hist_out[(3 * s + 2) * cap + k] = sh[2];
+        }
+    }
+}
+
+// The pair step: PairGran::compute for one owned atom k with its j-side
+// (reverse) entries and its own half-list entries, the post_force fixes,
+// FixNVESphere::final_integrate and -- when the run continues -- the next
+// step's initial_integrate with the displacement check.
+//
+// Shear history is double-buffered.  Invariant: when a step starts, every
+// slot's current shear is in `hist` (the read buffer); the step writes the
+// write buffer `hist_out`, which becomes the read buffer of the next step.
+// A touching slot is read from hist and its update written to hist_out; a
+// slot that stopped touching this step is copied once (after that both
+// buffers agree); a rebuild writes both buffers.  Reverse entries therefore
+// read the pre-update shear without racing the owner's update, exactly as
+// the reference evaluates the pair once before the owner's shear changes.
+//
+// Per warp, the touching entries of its 32 atoms are enumerated owner-major
+// (reverse entries in ascending owner order, then own entries in list
+// order), evaluated one per lane in rounds of 32 with results staged in
+// shared memory, and summed by each owner lane in that order.  Atoms with
+// more than 64 reverse or own entries are evaluated serially by their owner
+// lane after the rounds, in the same order.
+template <bool ROLLING, int MINB, bool SPLIT>
+__global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate, int integrate, int fuse_next,
+                                                         int store_f)
+{
+    using Real = typename std::conditional<SPLIT, float, double>::type;
+    __shared__ Real sres[4][32][6];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int wbase = blockIdx.x * blockDim.x + wid * 32;
+    const bool valid = k < D.nlocal;
+    const int cap = D.cap;
+    const bool upd = shearupdate != 0;
+    dbl4 pk, vi4, wi4, hold;
+    unsigned long long prevm = 0ull;
+    int nr = 0, nn = 0, tk = 0;
+    unsigned long long mrev = 0ull, mown = 0ull;
+    bool serial = false;
+    if (valid) {
+        // the atom's own records, including those only the tail needs, are
+        // requested first so their latency overlaps the screening
+        pk = D.pos[k];
+        nr = D.rnum[k];
+        nn = D.nnum[k];
+        vi4 = D.vel[k];
+        wi4 = D.omg[k];
+        tk = D.type[k];
+        if (fuse_next) hold = D.xhold[k];
+        if (upd) prevm = D.prevmask[k];
+        serial = nr > 64 || nn > 64;
+        if (!serial) screen_both(D, k, nr, nn, pk, mrev, mown);
+    }
+    // FP64 path: plain in-order sums (bit-exact).  Split path: FP32 sums of
+    // the FP32 pair contributions with Kahan compensation kc.
+    Real as[6], kc[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) as[c] = kc[c] = Real(0);
+    const int crev = __popcll(mrev);
+    {
+        const WarpItems it = warp_items_cnt(crev + __popcll(mown));
+        for (int base = 0; base < it.total; base += 32) {
+            const int w = base + lane;
+            const int L = item_owner(w, it.excl);
+            const int exL = __shfl_sync(0xffffffffu, it.excl, L);
+            const unsigned long long mrL = shfl64(mrev, L);
+            const unsigned long long moL = shfl64(mown, L);
+            if (w < it.total) {
+                const int kk = wbase + L;
+                const int q = w - exL;
+                const int qr = __popcll(mrL);
+                // operands of one pair: j-side entries are evaluated from kk's side
+                // with the shear negated, own entries update kk's slot
+                int other, s, e = -1;
+                double sgn;
+                bool own;
+                if (q < qr) {
+                    const int r = nth_set_bit(mrL, q);
+                    other = __ldg(&D.rev[r * cap + kk]);
+                    s = D.revs[r * cap + kk];
+                    sgn = -1.0;
+                    own = false;
+                } else {
+                    s = nth_set_bit(moL, q - qr);
+                    e = s * cap + kk;
+                    other = __ldg(&D.nbr[e]);
+                    sgn = 1.0;
+                    own = true;
+                }
+                const int hrow = own ? kk : other;
+                const dbl4 pkk = ldg4(&D.pos[kk]);
+                const dbl4 po = ldg4(&D.pos[other]);
+                const double delx = pkk.x - po.x;
+                const double dely = pkk.y - po.y;
+                const double delz = pkk.z - po.z;
+                const double rsq = delx * delx + dely * dely + delz * delz;
+                const int tkk = D.type[kk], to = D.type[other];
+                // material lookup in the reference's (owner, neighbour) order
+                const MatPair &M = own ? mat(D, tkk, to) : mat(D, to, tkk);
+                if (own) {
+                    const int fl = D.flag[e];
+                    if ((fl | 5) != fl) D.flag[e] = fl | 5;   // CONTACT_NORMAL_MODEL | CONTACT_TANGENTIAL_MODEL
+                }
+                Real res[6];
+                if constexpr (SPLIT) {
+                    const flt8 a = ldg8f(&D.kin[kk]), b = ldg8f(&D.kin[other]);
+                    const double r = sqrt(rsq);
+                    const double deltan = (pkk.w + po.w) - r;   // FP64 overlap
+                    const float va[3] = {a.vx, a.vy, a.vz}, wa[3] = {a.wx, a.wy, a.wz};
+                    const float vb[3] = {b.vx, b.vy, b.vz}, wb[3] = {b.wx, b.wy, b.wz};
+                    const float fs = (float)sgn;
+                    float sh[3];
+                    sh[0] = fs * (float)D.hist[(3 * s + 0) * cap + hrow];
+                    sh[1] = fs * (float)D.hist[(3 * s + 1) * cap + hrow];
+                    sh[2] = fs * (float)D.hist[(3 * s + 2) * cap + hrow];
+                    ContactOutF o;
+                    pair_contact_f32(M, (float)delx, (float)dely, (float)delz, (float)r, (float)deltan, (float)pkk.w,
+                                     (float)po.w, va, vb, wa, wb, a.m, b.m, sh, upd, (float)D.dt, ROLLING,
+                                     D.tdamp != 0, o);
+                    if (own && upd) {
+                        D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
+                        D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
+                        D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
+                    }
+                    for (int c = 0; c < 3; c++) {
+                        res[c] = o.F[c];
+                        res[3 + c] = o.T[c];
+                    }
+                } else {
+                    const dbl4 vk4 = ldg4(&D.vel[kk]), wk4 = ldg4(&D.omg[kk]);
+                    const dbl4 vo4 = ldg4(&D.vel[other]), wo4 = ldg4(&D.omg[other]);
+                    const double vk[3] = {vk4.x, vk4.y, vk4.z}, wk[3] = {wk4.x, wk4.y, wk4.z};
+                    const double vo[3] = {vo4.x, vo4.y, vo4.z}, wo[3] = {wo4.x, wo4.y, wo4.z};
+                    double sh[3];
+                    sh[0] = sgn * D.hist[(3 * s + 0) * cap + hrow];   // exact: multiplying by +-1 only flips the sign
+                    sh[1] = sgn * D.hist[(3 * s + 1) * cap + hrow];
+                    sh[2] = sgn * D.hist[(3 * s + 2) * cap + hrow];
+                    ContactOut o;
+                    pair_contact<false>(M, delx, dely, delz, rsq, pkk.w, po.w, vk, vo, wk, wo, vk4.w, vo4.w, sh, upd,
+                                        D.dt, ROLLING, D.tdamp != 0, o);
+                    if (own && upd) {
+                        D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
+                        D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
+                        D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
+                    }
+                    for (int c = 0; c < 3; c++) {
+                        res[c] = o.F[c];
+                        res[3 + c] = o.T[c];
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 6; c++) sres[wid][lane][c] = res[c];
+            }
+            __syncwarp();
+            const int lo = max(it.excl, base), hi = min(it.excl + it.cnt, base + 32);
+            for (int q = lo; q < hi; q++) {
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    if constexpr (SPLIT) {
+                        const float y = sres[wid][q - base][c] - kc[c];
+                        const float t = as[c] + y;
+                        kc[c] = (t - as[c]) - y;
+                        as[c] = t;
+                    } else {
+                        as[c] += sres[wid][q - base][c];
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    ContactOut acc;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if constexpr (SPLIT) {
+            acc.F[c] = (double)as[c] - (double)kc[c];
+            acc.T[c] = (double)as[3 + c] - (double)kc[3 + c];
+        } else {
+            acc.F[c] = as[c];
+            acc.T[c] = as[3 + c];
+        }
+    }
+    if (!valid) return;
+    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
+    if (serial) {
+        serial_atom<ROLLING>(D, k, pk, vi4, wi4, tk, nr, nn, upd, acc);
+    } else if (upd) {
+        // slots that stopped touching this step: carry their shear into the write buffer
+        unsigned long long stopped = prevm & ~mown;
+        while (stopped) {
+            const int s = __ffsll((long long)stopped) - 1;
+            stopped &= stopped - 1ull;
+            D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
+            D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
+            D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
+        }
+    }
+    if (upd) D.prevmask[k] = serial ? ~0ull : mown;
+    const int i = k;
+    const dbl4 pi = pk;
+    const int ti = tk;
+    const double *vi = vk, *wi = wk;
+    // post_force fixes in definition order
+    for (int k = 0; k < D.nfix; k++) {
+        const FixDev &F = D.fix[k];
+        if (F.kind == FIX_GRAVITY) {
+            const double massone = vi4.w * 1.;
+            acc.F[0] += massone * F.acc[0];
+            acc.F[1] += massone * F.acc[1];
+            acc.F[2] += massone * F.acc[2];
+        } else if (F.kind == FIX_WALL_PLANE) {
+            if (F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
+        } else if (F.kind == FIX_WALL_MESH) {
+            mesh_wall_atom(D, F.mesh, i, pi, vi, wi, vi4.w, ti, upd, acc);
+        }
+    }
+    if (store_f) {
+        dbl4 Fo, To;
+        Fo.x = acc.F[0];
+        Fo.y = acc.F[1];
+        Fo.z = acc.F[2];
+        Fo.w = 0.0;
+        To.x = acc.T[0];
+        To.y = acc.T[1];
+        To.z = acc.T[2];
+        To.w = 0.0;
+        D.f[i] = Fo;
+        D.tq[i] = To;
+    }
+    if (integrate) {
+        // FixNVESphere::final_integrate (src/fix_nve_sphere.cpp:208-246)
+        const double dtf = 0.5 * D.dt * 1.0;
+        const double dtfrotate = dtf / 0.4;
+        const double dtfm = dtf / (vi4.w * 1.0);
+        vi4.x += dtfm * acc.F[0];
+        vi4.y += dtfm * acc.F[1];
+        vi4.z += dtfm * acc.F[2];
+        const double dtirotate = dtfrotate / (pi.w * pi.w * vi4.w);
+        wi4.x += dtirotate * acc.T[0];
+        wi4.y += dtirotate * acc.T[1];
+        wi4.z += dtirotate * acc.T[2];
+        if (fuse_next) {
+            // next step's FixNVESphere::initial_integrate with the same force,
+            // then Neighbor::check_distance's displacement test
+            const double dtv = D.dt;
+            vi4.x += dtfm * acc.F[0];
+            vi4.y += dtfm * acc.F[1];
+            vi4.z += dtfm * acc.F[2];
+            dbl4 p = pi;
+            p.x += dtv * vi4.x;
+            p.y += dtv * vi4.y;
+            p.z += dtv * vi4.z;
+            wi4.x += dtirotate * acc.T[0];
+            wi4.y += dtirotate * acc.T[1];
+            wi4.z += dtirotate * acc.T[2];
+            D.pos_out[i] = p;
+            const dbl4 h = hold;
+            const double delx = p.x - h.x, dely = p.y - h.y, delz = p.z - h.z;
+            if (delx * delx + dely * dely + delz * delz > D.triggersq) *D.dflag = 1;
+        }
+        D.vel_out[i] = vi4;
+        D.omg_out[i] = wi4;
+        if constexpr (SPLIT) D.kin_out[i] = make_kin(vi4, wi4);
+    }
+}
+
+}  // namespace gb2

@@ -74,6 +74,9 @@ class Stats(ctypes.Structure):
         ("t_rebuild", ctypes.c_double),
         ("n_pair_main", ctypes.c_long),
         ("nsteps_rebuild", ctypes.c_long),
+        ("maxrev", ctypes.c_int),
+        ("maxmesh", ctypes.c_int),
+        ("ngrow", ctypes.c_long),
     ]
 
 
