@@ -125,6 +125,20 @@ int gb2_add_wall_plane(gb2_ctx *ctx, int dim, double pos, int wall_type, int rol
 int gb2_add_wall_mesh(gb2_ctx *ctx, int ntri, const double *nodes, int wall_type,
                       double curvature, int rolling_cdt);
 
+/* fix ID all move/mesh mesh <mesh-id> rotate origin ox oy oz axis ax ay az period T
+   (src/fix_move_mesh.cpp:221 FixMoveMesh::initial_integrate,
+    src/mesh_mover_rotation.cpp:66-138 MeshMoverRotate) on the mesh wall of
+   fix index ifix_mesh.  Each step rotates the mesh by 2*pi/T*dt about the
+   axis through origin, sets the node velocities omega x (node - origin) that
+   the wall contact interpolates at the contact point, and forces a neighbour
+   rebuild on the step after any node has moved more than skin/2 since the last
+   one (src/fix_mesh.cpp:564-588).  Call before gb2_setup; one mover per mesh. */
+int gb2_add_move_mesh_rotate(gb2_ctx *ctx, int ifix_mesh, const double origin[3], const double axis[3],
+                             double period);
+/* current mesh nodes [ntri][3][3] and node velocities (zero for a static mesh)
+   of mesh fix ifix; *ntri = element count, nothing written when cap < ntri */
+int gb2_download_mesh_nodes(gb2_ctx *ctx, int ifix, int cap, int *ntri, double *nodes, double *vnode);
+
 /* Verlet::setup and Verlet::run(nsteps) */
 int gb2_setup(gb2_ctx *ctx);
 int gb2_run(gb2_ctx *ctx, int nsteps);

@@ -99,16 +99,22 @@ __device__ __forceinline__ double calc_dist(const double *cs, const double *cp, 
 #define GB2_EDGE_ACTIVE(T, k) (((T).active >> (k)) & 1)
 #define GB2_CORNER_ACTIVE(T, k) (((T).active >> (3 + (k))) & 1)
 
-static __device__ double tri_edge(const TriGeom &T, int iEdge, const double *p, double *delta)
+static __device__ double tri_edge(const TriGeom &T, int iEdge, const double *p, double *delta, double *bary)
 {
-    const int ip = (iEdge + 1) % 3;
+    const int ip = (iEdge + 1) % 3, ipp = (iEdge + 2) % 3;
     double nodeToP[3] = {p[0] - T.node[iEdge][0], p[1] - T.node[iEdge][1], p[2] - T.node[iEdge][2]};
     const double distFromNode = dot3(nodeToP, T.edgevec[iEdge]);
     if (distFromNode < -GB2_SMALL_TRIMESH) {
         if (!GB2_CORNER_ACTIVE(T, iEdge)) return GB2_LARGE_TRIMESH;
+        bary[iEdge] = 1.;
+        bary[ip] = 0.;
+        bary[ipp] = 0.;
         return calc_dist(p, T.node[iEdge], delta);
     } else if (distFromNode > T.edgelen[iEdge] + GB2_SMALL_TRIMESH) {
         if (!GB2_CORNER_ACTIVE(T, ip)) return GB2_LARGE_TRIMESH;
+        bary[iEdge] = 0.;
+        bary[ip] = 1.;
+        bary[ipp] = 0.;
         return calc_dist(p, T.node[ip], delta);
     }
     if (!GB2_EDGE_ACTIVE(T, iEdge)) return GB2_LARGE_TRIMESH;
@@ -116,10 +122,15 @@ static __device__ double tri_edge(const TriGeom &T, int iEdge, const double *p, 
     cp[0] = T.node[iEdge][0] + distFromNode * T.edgevec[iEdge][0];
     cp[1] = T.node[iEdge][1] + distFromNode * T.edgevec[iEdge][1];
     cp[2] = T.node[iEdge][2] + distFromNode * T.edgevec[iEdge][2];
-    return calc_dist(p, cp, delta);
+    const double d = calc_dist(p, cp, delta);
+    bary[ipp] = 0.;
+    bary[iEdge] = 1. - distFromNode / T.edgelen[iEdge];
+    bary[ip] = 1. - bary[iEdge];
+    return d;
 }
 
-static __device__ double tri_corner(const TriGeom &T, int iNode, bool obtuse, const double *p, double *delta)
+static __device__ double tri_corner(const TriGeom &T, int iNode, bool obtuse, const double *p, double *delta,
+                                    double *bary)
 {
     const int ip = (iNode + 1) % 3, ipp = (iNode + 2) % 3;
     const double *n = T.node[iNode];
@@ -133,9 +144,14 @@ static __device__ double tri_corner(const TriGeom &T, int iNode, bool obtuse, co
                 cp[0] = n[0] + distFromNode * T.edgevec[ipp][0];
                 cp[1] = n[1] + distFromNode * T.edgevec[ipp][1];
                 cp[2] = n[2] + distFromNode * T.edgevec[ipp][2];
+                bary[ip] = 0.;
+                bary[iNode] = 1. + distFromNode / T.edgelen[ipp];
+                bary[ipp] = 1. - bary[iNode];
                 return calc_dist(p, cp, delta);
             }
             if (!GB2_CORNER_ACTIVE(T, ipp)) return GB2_LARGE_TRIMESH;
+            bary[ipp] = 1.;
+            bary[iNode] = bary[ip] = 0.;
             return calc_dist(p, T.node[ipp], delta);
         }
         distFromNode = dot3(nodeToP, T.edgevec[iNode]);
@@ -145,18 +161,28 @@ static __device__ double tri_corner(const TriGeom &T, int iNode, bool obtuse, co
                 cp[0] = n[0] + distFromNode * T.edgevec[iNode][0];
                 cp[1] = n[1] + distFromNode * T.edgevec[iNode][1];
                 cp[2] = n[2] + distFromNode * T.edgevec[iNode][2];
+                bary[ipp] = 0.;
+                bary[iNode] = 1. - distFromNode / T.edgelen[iNode];
+                bary[ip] = 1. - bary[iNode];
                 return calc_dist(p, cp, delta);
             }
             if (!GB2_CORNER_ACTIVE(T, ip)) return GB2_LARGE_TRIMESH;
+            bary[ip] = 1.;
+            bary[iNode] = bary[ipp] = 0.;
             return calc_dist(p, T.node[ip], delta);
         }
     }
     if (!GB2_CORNER_ACTIVE(T, iNode)) return GB2_LARGE_TRIMESH;
+    bary[iNode] = 1.;
+    bary[ip] = bary[ipp] = 0.;
     return calc_dist(p, T.node[iNode], delta);
 }
 
+// bary: barycentric coordinates of the contact point as the reference's
+// resolveTriSphereContactBary leaves them (the moving-wall velocity is
+// interpolated with them)
 static __device__ double tri_sphere(const TriGeom &T, double rSphere, const double *cs, double *delta, int &barySign,
-                             double precision)
+                                    double precision, double *bary)
 {
     double n0ToC[3] = {cs[0] - T.node[0][0], cs[1] - T.node[0][1], cs[2] - T.node[0][2]};
     // MathExtraLiggghts::calcBaryTriCoords (src/math_extra_liggghts.h:559)
@@ -164,7 +190,6 @@ static __device__ double tri_sphere(const TriGeom &T, double rSphere, const doub
     const double b = dot3(n0ToC, T.edgevec[2]);
     const double c = dot3(T.edgevec[0], T.edgevec[2]);
     const double oneMinCSqr = 1 - c * c;
-    double bary[3];
     bary[1] = (a - b * c) / (T.edgelen[0] * oneMinCSqr);
     bary[2] = (a * c - b) / (T.edgelen[2] * oneMinCSqr);
     bary[0] = 1. - bary[1] - bary[2];
@@ -173,12 +198,12 @@ static __device__ double tri_sphere(const TriGeom &T, double rSphere, const doub
                4 * (bary[2] > -precision * invlen);
     double d;
     switch (barySign) {
-    case 1: d = tri_corner(T, 0, T.obtuse == 0, cs, delta); break;
-    case 2: d = tri_corner(T, 1, T.obtuse == 1, cs, delta); break;
-    case 3: d = tri_edge(T, 0, cs, delta); break;
-    case 4: d = tri_corner(T, 2, T.obtuse == 2, cs, delta); break;
-    case 5: d = tri_edge(T, 2, cs, delta); break;
-    case 6: d = tri_edge(T, 1, cs, delta); break;
+    case 1: d = tri_corner(T, 0, T.obtuse == 0, cs, delta, bary); break;
+    case 2: d = tri_corner(T, 1, T.obtuse == 1, cs, delta, bary); break;
+    case 3: d = tri_edge(T, 0, cs, delta, bary); break;
+    case 4: d = tri_corner(T, 2, T.obtuse == 2, cs, delta, bary); break;
+    case 5: d = tri_edge(T, 2, cs, delta, bary); break;
+    case 6: d = tri_edge(T, 1, cs, delta, bary); break;
     case 7: {
         const double dNorm = dot3(T.surfnorm, n0ToC);
         const double tmp[3] = {T.surfnorm[0] * dNorm, T.surfnorm[1] * dNorm, T.surfnorm[2] * dNorm};
@@ -365,14 +390,13 @@ __device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, i
     if (nn == 0) return;
     unsigned long long keep = 0ull;   // markAllContacts
     const double cs[3] = {p.x, p.y, p.z};
-    const double vwall[3] = {0.0, 0.0, 0.0};
     int np = M.snp[i];
     for (int q = 0; q < nn; q++) {
         const int t = M.tlist[q * cap + i];
         const TriGeom &T = M.tri[t];
-        double delta[3];
+        double delta[3], bary[3] = {0., 0., 0.};
         int barysign = -1;
-        const double deltan = tri_sphere(T, p.w, cs, delta, barysign, 1e-8);
+        const double deltan = tri_sphere(T, p.w, cs, delta, barysign, 1e-8, bary);
         if (deltan > D.cutneighmax) continue;
         if (!(deltan <= 0)) continue;
         const bool faceflag = (7 == barysign);
@@ -429,6 +453,11 @@ __device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, i
         double sh[3] = {M.shist[(3 * slot + 0) * cap + i], M.shist[(3 * slot + 1) * cap + i],
                         M.shist[(3 * slot + 2) * cap + i]};
         const double dvec[3] = {-delta[0], -delta[1], -delta[2]};
+        double vwall[3] = {0.0, 0.0, 0.0};
+        if (M.vnode) {   // moving mesh: barycentric node velocity (src/fix_wall_gran.cpp:992-996)
+            const double *vn = M.vnode + 9 * t;
+            for (int c = 0; c < 3; c++) vwall[c] = (bary[0] * vn[c] + bary[1] * vn[3 + c] + bary[2] * vn[6 + c]);
+        }
         wall_contact(mat(D, itype, M.wtype), dvec, -deltan, p.w, v, w, vwall, mass, sh, upd, D.dt, M.rolling != 0,
                      D.tdamp != 0, acc);
         M.shist[(3 * slot + 0) * cap + i] = sh[0];

@@ -91,6 +91,13 @@ struct MeshFix {
     DBuf<double> shist_s;
     bool bins_valid = false;
     double nl_skin = 0, distmax = 0;
+    // fix move/mesh rotate
+    bool moving = false;
+    double mv_point[3] = {0, 0, 0}, mv_axis[3] = {0, 0, 1}, mv_omega = 0;
+    DBuf<double> vnode, node_last;
+    DBuf<int> trange, tcount, toff, bincnt, pvals;
+    DBuf<unsigned> pkeys, pkeys2;
+    long next_reneighbor = -1;   // FixMesh::next_reneighbor
 };
 
 struct HostFix {
@@ -290,6 +297,7 @@ Dev make_dev(gb2_ctx *c)
             m.snp = M.snp.p;
             m.spartner = M.spartner.p;
             m.shist = M.shist.p;
+            m.vnode = M.moving ? M.vnode.p : nullptr;
         }
     }
     D.status = c->dstatus.p;
@@ -562,6 +570,26 @@ int mesh_bins(gb2_ctx *c, MeshFix &M)
 
 // ---------------------------------------------------------------- rebuild parts
 
+// Rotation of one step as MultiNodeMesh::rotate(dAngle, axis, p) builds it
+// (src/multi_node_mesh_I.h:620-640): the axis normalised again, the
+// quaternion from the host's cos/sin of half the increment omega*dt.
+void mesh_rotation(const gb2_ctx *c, const MeshFix &M, MeshRotate &mv)
+{
+    const double dAngle = M.mv_omega * c->P.dt;
+    double an[3] = {M.mv_axis[0], M.mv_axis[1], M.mv_axis[2]};
+    const double mag = std::sqrt(an[0] * an[0] + an[1] * an[1] + an[2] * an[2]);
+    const double sinv = 1. / mag;
+    for (int d = 0; d < 3; d++) an[d] = sinv * an[d];
+    mv.dQ[0] = std::cos(dAngle * 0.5);
+    for (int d = 0; d < 3; d++) mv.dQ[d + 1] = an[d] * std::sin(dAngle * 0.5);
+    for (int d = 0; d < 3; d++) {
+        mv.origin[d] = M.mv_point[d];
+        mv.omegaVec[d] = M.mv_axis[d] * M.mv_omega;
+    }
+    mv.trans = (M.mv_point[0] * M.mv_point[0] + M.mv_point[1] * M.mv_point[1] + M.mv_point[2] * M.mv_point[2]) > 0.;
+    mv.triggersq = 0.25 * c->P.skin * c->P.skin;
+}
+
 // New capacity after an overflow: at least double, and half again the
 // largest demand the overflowing kernel recorded in need[which], so a
 // growing bed reallocates rarely (each reallocation synchronises the device).
@@ -572,6 +600,64 @@ int grown_capacity(gb2_ctx *c, int which, int old, int limit)
     const long cap = std::max<long>(2l * old, (3l * need + 1) / 2);
     c->ngrow++;
     return (int)std::min<long>(cap, limit);
+}
+
+// Bin -> triangle lists of a moving mesh from its current nodes, on the
+// device: per-triangle bin ranges, pairs in triangle order, a stable sort by
+// bin (so each bin lists its triangles in ascending order) and a scan of the
+// per-bin counts.
+int mesh_bins_moving(gb2_ctx *c, MeshFix &M)
+{
+    M.nl_skin = c->P.skin;   // changingMesh: full skin, distmax = cutneighmax + SMALL_DELTA
+    M.distmax = c->cutneighmax + M.nl_skin / (70. * M_PI);
+    const int n = (int)M.topo.tri.size();
+    CK(M.trange.alloc((size_t)6 * n));
+    CK(M.tcount.alloc((size_t)n + 1));
+    CK(M.toff.alloc((size_t)n + 1));
+    CK(M.bincnt.alloc((size_t)c->mbins + 1));
+    CK(M.bin_tri_start.alloc((size_t)c->mbins + 1));
+    if (clear_status(c)) return GB2_ERR_CUDA;
+    Dev D = make_dev(c);
+    k_tri_bin_range<<<nblk(n), kBlock, 0, c->st>>>(D, M.tri.p, n, M.distmax, c->P.boxlo[0], c->P.boxlo[1],
+                                                   c->P.boxlo[2], c->P.boxhi[0], c->P.boxhi[1], c->P.boxhi[2],
+                                                   M.trange.p, M.tcount.p);
+    CKL();
+    CK(cudaMemsetAsync(M.tcount.p + n, 0, sizeof(int), c->st));
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, M.tcount.p, M.toff.p, n + 1, c->st);
+    if (cub_tmp(c, bytes)) return GB2_ERR_CUDA;
+    bytes = c->cubtmp.n;
+    CK(cub::DeviceScan::ExclusiveSum(c->cubtmp.p, bytes, M.tcount.p, M.toff.p, n + 1, c->st));
+    int npairs = 0, st = 0;
+    CK(cudaMemcpyAsync(&c->h_pinned[3], M.toff.p + n, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    if (read_status(c, &st)) return GB2_ERR_CUDA;
+    npairs = c->h_pinned[3];
+    if (st & ST_MESH_OUTSIDE_GRID)
+        return set_err(c, GB2_ERR_UNSUPPORTED, "moving mesh within the neighbour cutoff of the box boundary");
+    const size_t np = std::max(npairs, 1);
+    if (M.pkeys.n < np) {   // headroom: the mesh turns, its bounding boxes change size
+        CK(M.pkeys.alloc(np + np / 2));
+        CK(M.pkeys2.alloc(np + np / 2));
+        CK(M.pvals.alloc(np + np / 2));
+        CK(M.bin_tri_list.alloc(np + np / 2));
+    }
+    CK(cudaMemsetAsync(M.bincnt.p, 0, sizeof(int) * ((size_t)c->mbins + 1), c->st));
+    k_tri_bin_fill<<<nblk(n), kBlock, 0, c->st>>>(D, n, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p, M.bincnt.p);
+    CKL();
+    int endbit = 1;
+    while ((1l << endbit) < (long)c->mbins + 1) endbit++;
+    size_t b1 = 0, b2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b1, M.pkeys.p, M.pkeys2.p, M.pvals.p, M.bin_tri_list.p, npairs, 0,
+                                    endbit, c->st);
+    cub::DeviceScan::ExclusiveSum(nullptr, b2, M.bincnt.p, M.bin_tri_start.p, c->mbins + 1, c->st);
+    if (cub_tmp(c, std::max(b1, b2))) return GB2_ERR_CUDA;
+    bytes = c->cubtmp.n;
+    if (npairs > 0)
+        CK(cub::DeviceRadixSort::SortPairs(c->cubtmp.p, bytes, M.pkeys.p, M.pkeys2.p, M.pvals.p, M.bin_tri_list.p,
+                                           npairs, 0, endbit, c->st));
+    bytes = c->cubtmp.n;
+    CK(cub::DeviceScan::ExclusiveSum(c->cubtmp.p, bytes, M.bincnt.p, M.bin_tri_start.p, c->mbins + 1, c->st));
+    return 0;
 }
 
 int do_partners(gb2_ctx *c)
@@ -775,8 +861,16 @@ int do_pre_force(gb2_ctx *c)
             CKL();
         } else if (H.kind == FIX_WALL_MESH) {
             MeshFix &M = *H.mesh;
-            if (!M.bins_valid)
+            if (M.moving) {
+                // FixMesh::pre_force on a rebuild step stores the nodes (src/fix_mesh.cpp:567-572)
+                const int nt = (int)M.topo.tri.size();
+                k_mesh_store_last<<<nblk(nt), kBlock, 0, c->st>>>(M.tri.p, nt, M.node_last.p);
+                CKL();
+                int rc = mesh_bins_moving(c, M);
+                if (rc) return rc;
+            } else if (!M.bins_valid) {
                 if (mesh_bins(c, M)) return GB2_ERR_CUDA;
+            }
             // candidates into fresh buffers (old slots are still needed)
             const int old_maxt = M.maxt;
             CK(M.tcnt2.alloc(c->cap));
@@ -836,7 +930,10 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
         if (do_atom_sort(c)) return GB2_ERR_CUDA;
     if (do_borders(c)) return GB2_ERR_CUDA;
     if (do_build(c)) return c->err.empty() ? GB2_ERR_CUDA : GB2_ERR_CAPACITY;
-    if (do_pre_force(c)) return GB2_ERR_CUDA;
+    {
+        const int rc = do_pre_force(c);
+        if (rc) return (rc == GB2_ERR_UNSUPPORTED || rc == GB2_ERR_STATE) ? rc : GB2_ERR_CUDA;
+    }
     if (c->split) {   // FP32 kinematics of owned atoms and the new ghosts
         const int nall = c->nlocal + c->nghost;
         Dev D2 = make_dev(c);
@@ -983,8 +1080,8 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
         return GB2_ERR_CUDA;
     }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&c->h_pinned, 4 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
-        c->ddflag.alloc(1) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess ||
+        cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
+        c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess ||
         cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
         cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
@@ -1198,6 +1295,61 @@ int gb2_add_wall_mesh(gb2_ctx *c, int ntri, const double *nodes, int wall_type, 
     return c->nfix++;
 }
 
+int gb2_add_move_mesh_rotate(gb2_ctx *c, int ifix_mesh, const double origin[3], const double axis[3], double period)
+{
+    if (!c || !origin || !axis) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fix move/mesh must be defined before setup");
+    if (ifix_mesh < 0 || ifix_mesh >= c->nfix || !c->fix[ifix_mesh].mesh)
+        return set_err(c, GB2_ERR_ARG, "fix move/mesh: mesh fix index does not name a mesh wall");
+    MeshFix &M = *c->fix[ifix_mesh].mesh;
+    if (M.moving) return set_err(c, GB2_ERR_UNSUPPORTED, "one fix move/mesh per mesh is supported");
+    if (!(period != 0.0) || !std::isfinite(period)) return set_err(c, GB2_ERR_ARG, "fix move/mesh: period must be non-zero");
+    for (int d = 0; d < 3; d++) {
+        M.mv_point[d] = origin[d];
+        M.mv_axis[d] = axis[d];
+    }
+    // vectorNormalize3D (src/vector_liggghts.h:62) as in the MeshMoverRotate constructor
+    const double norm = std::sqrt(M.mv_axis[0] * M.mv_axis[0] + M.mv_axis[1] * M.mv_axis[1] + M.mv_axis[2] * M.mv_axis[2]);
+    if (norm == 0.) return set_err(c, GB2_ERR_ARG, "fix move/mesh: zero rotation axis");
+    const double invnorm = 1. / norm;
+    for (int d = 0; d < 3; d++) M.mv_axis[d] *= invnorm;
+    M.mv_omega = 2. * M_PI / period;
+    const size_t nt = M.topo.tri.size();
+    CK(M.vnode.alloc(9 * nt));
+    CK(M.node_last.alloc(9 * nt));
+    CK(cudaMemsetAsync(M.vnode.p, 0, sizeof(double) * 9 * nt, c->st));   // FixMoveMesh::setup: v = 0
+    CK(cudaStreamSynchronize(c->st));
+    M.moving = true;
+    return 0;
+}
+
+int gb2_download_mesh_nodes(gb2_ctx *c, int ifix, int cap, int *ntri, double *nodes, double *vnode)
+{
+    if (!c || !ntri) return GB2_ERR_ARG;
+    if (ifix < 0 || ifix >= c->nfix || !c->fix[ifix].mesh) return set_err(c, GB2_ERR_ARG, "not a mesh fix");
+    MeshFix &M = *c->fix[ifix].mesh;
+    const int n = (int)M.topo.tri.size();
+    *ntri = n;
+    if (cap < n) return 0;
+    if (nodes) {
+        std::vector<TriGeom> h(n);
+        CK(cudaMemcpyAsync(h.data(), M.tri.p, sizeof(TriGeom) * n, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        for (int t = 0; t < n; t++)
+            for (int j = 0; j < 3; j++)
+                for (int d = 0; d < 3; d++) nodes[9 * t + 3 * j + d] = h[t].node[j][d];
+    }
+    if (vnode) {
+        if (M.moving) {
+            CK(cudaMemcpyAsync(vnode, M.vnode.p, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+        } else {
+            std::memset(vnode, 0, sizeof(double) * 9 * n);
+        }
+    }
+    return 0;
+}
+
 int gb2_setup(gb2_ctx *c)
 {
     if (!c) return GB2_ERR_ARG;
@@ -1247,13 +1399,35 @@ int gb2_run(gb2_ctx *c, int nsteps)
             CKL();
             if (prof_end(c, &e)) return GB2_ERR_CUDA;
         }
+        // fix move/mesh: rotate moving meshes (initial_integrate) and test
+        // their displacement since the last rebuild
+        bool moving = false, forced = false;
+        for (int k = 0; k < c->nfix; k++) {
+            MeshFix *M = c->fix[k].mesh;
+            if (!M || !M->moving) continue;
+            if (!moving) CK(cudaMemsetAsync(c->ddflag.p + 1, 0, sizeof(int), c->st));
+            moving = true;
+            if (M->next_reneighbor == c->ntimestep) forced = true;   // Neighbor::decide must_check
+            MeshRotate mv;
+            mesh_rotation(c, *M, mv);
+            const int nt = (int)M->topo.tri.size();
+            k_mesh_rotate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p, mv,
+                                                          c->ddflag.p + 1);
+            CKL();
+        }
         bool rebuild = decide && !c->P.neigh_check;
-        if (check) {
-            CK(cudaMemcpyAsync(&c->h_pinned[1], c->ddflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        bool mesh_far = false;
+        if (check || moving) {
+            CK(cudaMemcpyAsync(&c->h_pinned[4], c->ddflag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
             CK(cudaStreamSynchronize(c->st));
-            rebuild = c->h_pinned[1] != 0;
+            if (check) rebuild = c->h_pinned[4] != 0;
+            mesh_far = moving && c->h_pinned[5] != 0;
             if (c->prof) prof_resolve(c);
         }
+        if (forced) rebuild = true;
+        if (!rebuild && mesh_far)   // FixMesh::pre_force on a regular step (src/fix_mesh.cpp:577-583)
+            for (int k = 0; k < c->nfix; k++)
+                if (c->fix[k].mesh && c->fix[k].mesh->moving) c->fix[k].mesh->next_reneighbor = c->ntimestep + 1;
         if (rebuild) {
             const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
             if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;

@@ -54,6 +54,7 @@ enum : int {
     ST_LOST_ATOM = 1 << 3,
     ST_REV_OVERFLOW = 1 << 4,
     ST_MESH_INTERNAL = 1 << 5,
+    ST_MESH_OUTSIDE_GRID = 1 << 6,
 };
 
 enum FixKind : int { FIX_NONE = 0, FIX_GRAVITY = 1, FIX_WALL_PLANE = 2, FIX_WALL_MESH = 3 };
@@ -90,6 +91,7 @@ struct MeshDev {
     int *snp;              // npartner
     int *spartner;         // [s*cap + i] triangle id or -1
     double *shist;         // [(3s+c)*cap + i]
+    const double *vnode;   // moving mesh: node velocities [9*t + 3*node + c]; null when static
 };
 
 struct FixDev {

@@ -517,6 +517,153 @@ __global__ void k_mesh_repage(Dev D, int ifix, int *old_snp, int *old_spartner, 
     M.snp[i] = min(np, nn);
 }
 
+// ------------------------------------------------------------------
+// moving mesh (fix move/mesh rotate)
+
+// MathExtraLiggghts::vec_quat_rotate (src/math_extra_liggghts.h:451-468):
+// q * (0, v) * conj(q) with MathExtra::quatquat's operation order
+// (src/math_extra.h:596), the zero scalar part included so signed zeros match
+__device__ __forceinline__ void vec_quat_rotate(double *vec, const double *q)
+{
+    const double vq[4] = {0., vec[0], vec[1], vec[2]};
+    const double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+    double t[4], r[4];
+    t[0] = q[0] * vq[0] - q[1] * vq[1] - q[2] * vq[2] - q[3] * vq[3];
+    t[1] = q[0] * vq[1] + vq[0] * q[1] + q[2] * vq[3] - q[3] * vq[2];
+    t[2] = q[0] * vq[2] + vq[0] * q[2] + q[3] * vq[1] - q[1] * vq[3];
+    t[3] = q[0] * vq[3] + vq[0] * q[3] + q[1] * vq[2] - q[2] * vq[1];
+    r[0] = t[0] * qc[0] - t[1] * qc[1] - t[2] * qc[2] - t[3] * qc[3];
+    r[1] = t[0] * qc[1] + qc[0] * t[1] + t[2] * qc[3] - t[3] * qc[2];
+    r[2] = t[0] * qc[2] + qc[0] * t[2] + t[3] * qc[1] - t[1] * qc[3];
+    r[3] = t[0] * qc[3] + qc[0] * t[3] + t[1] * qc[2] - t[2] * qc[1];
+    vec[0] = r[1];
+    vec[1] = r[2];
+    vec[2] = r[3];
+}
+
+struct MeshRotate {
+    double dQ[4];          // rotation of one step
+    double origin[3];      // axis point
+    int trans;             // origin != 0
+    double omegaVec[3];    // axis * omega
+    double triggersq;      // (skin/2)^2
+};
+
+// One step of MeshMoverRotate::initial_integrate (src/mesh_mover_rotation.cpp:110-138)
+// per triangle: nodes and centre (MultiNodeMesh::rotate src/multi_node_mesh_I.h:643-660),
+// edge vectors, edge normals and the surface normal (rotated element
+// properties, src/surface_mesh_I.h:75-77, src/general_container_I.h:642),
+// node velocities omega x (node - origin); and MultiNodeMesh::decideRebuild's
+// displacement test against the nodes of the last rebuild (src/multi_node_mesh_I.h:791)
+__global__ void k_mesh_rotate(TriGeom *tri, int ntri, double *vnode, const double *node_last, MeshRotate mv, int *flag)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    TriGeom &T = tri[t];
+    double ctr[3] = {0., 0., 0.};
+    for (int j = 0; j < 3; j++) {
+        double nd[3] = {T.node[j][0], T.node[j][1], T.node[j][2]};
+        if (mv.trans)
+            for (int c = 0; c < 3; c++) nd[c] = nd[c] - mv.origin[c];
+        vec_quat_rotate(nd, mv.dQ);
+        if (mv.trans)
+            for (int c = 0; c < 3; c++) nd[c] = nd[c] + mv.origin[c];
+        for (int c = 0; c < 3; c++) {
+            T.node[j][c] = nd[c];
+            ctr[c] = nd[c] + ctr[c];
+        }
+    }
+    const double sinv = 1. / 3.0;
+    for (int c = 0; c < 3; c++) T.center[c] = sinv * ctr[c];
+    for (int j = 0; j < 3; j++) {
+        vec_quat_rotate(T.edgevec[j], mv.dQ);
+        vec_quat_rotate(T.edgenorm[j], mv.dQ);
+    }
+    vec_quat_rotate(T.surfnorm, mv.dQ);
+    bool far = false;
+    for (int j = 0; j < 3; j++) {
+        const double r0 = T.node[j][0] - mv.origin[0], r1 = T.node[j][1] - mv.origin[1],
+                     r2 = T.node[j][2] - mv.origin[2];
+        const double w0 = mv.omegaVec[0], w1 = mv.omegaVec[1], w2 = mv.omegaVec[2];
+        double *vn = vnode + 9 * t + 3 * j;
+        vn[0] = 0. + (w1 * r2 - w2 * r1);
+        vn[1] = 0. + (w2 * r0 - w0 * r2);
+        vn[2] = 0. + (w0 * r1 - w1 * r0);
+        const double *o = node_last + 9 * t + 3 * j;
+        const double d0 = T.node[j][0] - o[0], d1 = T.node[j][1] - o[1], d2 = T.node[j][2] - o[2];
+        if (d0 * d0 + d1 * d1 + d2 * d2 > mv.triggersq) far = true;
+    }
+    if (far) *flag = 1;
+}
+
+// MultiNodeMesh::storeNodePosRebuild (src/multi_node_mesh_I.h:833)
+__global__ void k_mesh_store_last(const TriGeom *tri, int ntri, double *node_last)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    for (int j = 0; j < 3; j++)
+        for (int c = 0; c < 3; c++) node_last[9 * t + 3 * j + c] = tri[t].node[j][c];
+}
+
+// FixNeighlistMesh with a moving mesh (src/fix_neighlist_mesh.cpp:383-395,
+// :411-424): every bin of the triangle's bounding box (shrunk to the box)
+// extended by distmax.  Pass 1: per-axis bin ranges and their pair count.
+// A range that leaves the bin grid is rejected (the reference would alias it
+// to a neighbouring row of bins).
+__global__ void k_tri_bin_range(Dev D, const TriGeom *tri, int ntri, double distmax, double lo0, double lo1,
+                                double lo2, double hi0, double hi1, double hi2, int *range, int *count)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    const TriGeom &T = tri[t];
+    double blo[3] = {1e300, 1e300, 1e300}, bhi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 3; k++)
+        for (int d = 0; d < 3; d++) {
+            blo[d] = fmin(blo[d], T.node[k][d]);
+            bhi[d] = fmax(bhi[d], T.node[k][d]);
+        }
+    const double boxlo[3] = {lo0, lo1, lo2}, boxhi[3] = {hi0, hi1, hi2};
+    for (int d = 0; d < 3; d++) {   // BoundingBox::shrinkToSubbox
+        if (blo[d] < boxlo[d]) blo[d] = boxlo[d];
+        if (bhi[d] > boxhi[d]) bhi[d] = boxhi[d];
+    }
+    int l[3], h[3];
+    coord2bin3(D, blo[0] - distmax, blo[1] - distmax, blo[2] - distmax, l[0], l[1], l[2]);
+    coord2bin3(D, bhi[0] + distmax, bhi[1] + distmax, bhi[2] + distmax, h[0], h[1], h[2]);
+    long n = 1;
+    for (int d = 0; d < 3; d++) {
+        if (l[d] < 0 || h[d] >= D.mbin[d] || h[d] < l[d]) {
+            atomicOr(D.status, ST_MESH_OUTSIDE_GRID);
+            n = 0;
+        }
+        range[6 * t + d] = l[d];
+        range[6 * t + 3 + d] = h[d];
+    }
+    if (n) n = (long)(h[0] - l[0] + 1) * (h[1] - l[1] + 1) * (h[2] - l[2] + 1);
+    count[t] = (int)n;
+}
+
+// Pass 2: (bin, triangle) pairs in triangle order, and per-bin counts
+__global__ void k_tri_bin_fill(Dev D, int ntri, const int *range, const int *off, unsigned *keys, int *vals,
+                               int *bincnt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    int p = off[t];
+    const int end = off[t + 1];
+    if (p == end) return;
+    const int *r = range + 6 * t;
+    for (int iz = r[2]; iz <= r[5]; iz++)
+        for (int iy = r[1]; iy <= r[4]; iy++)
+            for (int ix = r[0]; ix <= r[3]; ix++) {
+                const int b = iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
+                keys[p] = (unsigned)b;
+                vals[p] = t;
+                atomicAdd(&bincnt[b], 1);
+                p++;
+            }
+}
+
 // contact census (diagnostics and the bench's byte model)
 __global__ void k_census(Dev D, unsigned long long *cnt)
 {

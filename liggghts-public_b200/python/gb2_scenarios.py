@@ -6,6 +6,8 @@ configurations name:
 
 * ``sphere_pour``  -- monodisperse Hertz/history pour on a flat floor with
   periodic x/y (20,000 spheres, r = 1 mm, 40 x 40 x 200 mm box).
+* ``drum``         -- rotating drum: spheres of radius U(0.8, 1.2) mm in a
+  closed, triangulated cylinder (axis x) turned by ``fix move/mesh rotate``.
 * ``hopper``       -- polydisperse spheres (lognormal radius, median 1 mm,
   sigma 0.25, clipped to 0.5-2 mm) with Hertz/history + rolling friction cdt
   in a procedurally triangulated conical hopper (60 deg half-angle, 30 mm
@@ -165,6 +167,105 @@ def hopper(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z=32, ha
         ],
     }
     sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5, 0.1))
+    return sc
+
+
+def drum_mesh(diameter=0.5, length=0.85, n_theta=128, n_ax=121, cap_rings=4):
+    """Closed cylinder along x centred on the origin: a side of
+    ``2 * n_theta * n_ax`` triangles (axial rings, so no triangle spans the
+    drum) and two end caps on polar grids (a fan of ``n_theta`` triangles
+    around the axis, then ``cap_rings - 1`` annuli of ``2 * n_theta``).
+    The defaults give 32,768 triangles."""
+    R = 0.5 * diameter
+    th = np.linspace(0.0, 2.0 * math.pi, n_theta + 1)[:-1]
+    cs, sn = np.cos(th), np.sin(th)
+    xs = np.linspace(-0.5 * length, 0.5 * length, n_ax + 1)
+    tris = []
+    for l in range(n_ax):
+        for k in range(n_theta):
+            k2 = (k + 1) % n_theta
+            p00 = (xs[l], R * cs[k], R * sn[k])
+            p01 = (xs[l], R * cs[k2], R * sn[k2])
+            p10 = (xs[l + 1], R * cs[k], R * sn[k])
+            p11 = (xs[l + 1], R * cs[k2], R * sn[k2])
+            tris.append((p00, p11, p01))
+            tris.append((p00, p10, p11))
+    radii = np.linspace(0.0, R, cap_rings + 1)
+    for x0 in (-0.5 * length, 0.5 * length):
+        for q in range(cap_rings):
+            r0, r1 = radii[q], radii[q + 1]
+            for k in range(n_theta):
+                k2 = (k + 1) % n_theta
+                a1 = (x0, r1 * cs[k], r1 * sn[k])
+                b1 = (x0, r1 * cs[k2], r1 * sn[k2])
+                if q == 0:
+                    tris.append(((x0, 0.0, 0.0), a1, b1))
+                else:
+                    a0 = (x0, r0 * cs[k], r0 * sn[k])
+                    b0 = (x0, r0 * cs[k2], r0 * sn[k2])
+                    tris.append((a0, a1, b1))
+                    tris.append((a0, b1, b0))
+    return np.asarray(tris, dtype=np.float64)
+
+
+def drum(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length=0.85, n_theta=128, n_ax=121,
+         cap_rings=4, omega=2.0, gap=0.05, margin=0.01, clearance=1.5e-3, vmax=0.0):
+    """Rotating drum (Hertz/history): radius U(0.8, 1.2) mm, density 2700,
+    E 1e7, nu 0.45, e 0.5, mu 0.4; drum of ``diameter`` x ``length`` turning
+    at ``omega`` rad/s about the x axis (fix move/mesh rotate).  Particles
+    are sorted by radius and stacked bottom-up in simple-cubic layers of
+    spacing (2 + gap) x the largest radius of the layer, inside the drum with
+    ``clearance`` to its wall, with uniform +-vmax velocities; ``margin``
+    keeps the box clear of the mesh by more than the neighbour cutoff."""
+    rng = np.random.default_rng(seed)
+    rad = np.sort(rng.uniform(0.8e-3, 1.2e-3, size=n))[::-1].copy()
+    R = 0.5 * diameter
+    pos = np.zeros((n, 3))
+    placed = 0
+    z = -R + clearance
+    xlim = 0.5 * length - clearance
+    while placed < n:
+        rmax = rad[placed]
+        s = (2.0 + gap) * rmax
+        zc = z + rmax
+        if zc + rmax > R - clearance:
+            raise ValueError("drum too small for %d particles" % n)
+        half = math.sqrt(max((R - clearance - rmax) ** 2 - zc ** 2, 0.0))
+        ny = int(half // s)
+        nx = int((xlim - rmax) // s)
+        if ny < 0 or nx < 0:
+            z += s
+            continue
+        gy = np.arange(-ny, ny + 1) * s
+        gx = np.arange(-nx, nx + 1) * s
+        gxx, gyy = np.meshgrid(gx, gy, indexing="ij")
+        pts = np.stack([gxx.ravel(), gyy.ravel()], axis=1)
+        take = min(len(pts), n - placed)
+        sl = slice(placed, placed + take)
+        pos[sl, 0] = pts[:take, 0]
+        pos[sl, 1] = pts[:take, 1]
+        pos[sl, 2] = zc
+        placed += take
+        z = zc + rmax + gap * rmax
+    nodes = drum_mesh(diameter, length, n_theta, n_ax, cap_rings)
+    lo = [-0.5 * length - margin, -R - margin, -R - margin]
+    hi = [0.5 * length + margin, R + margin, R + margin]
+    sc = {
+        "name": "drum",
+        "dt": dt, "skin": skin,
+        "boxlo": lo, "boxhi": hi, "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": 1000, "sortbinsize": 0.0,
+        "rolling_cdt": 0, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2700.0, rng.uniform(-vmax, vmax, size=(n, 3)) if vmax > 0 else np.zeros((n, 3))),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_mesh", "nodes": nodes, "wall_type": 1, "curvature": 0.0, "rolling_cdt": 0},
+            {"kind": "move_mesh_rotate", "mesh": 1, "origin": [0.0, 0.0, 0.0], "axis": [1.0, 0.0, 0.0],
+             "period": 2.0 * math.pi / omega},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 1e7, 0.45, 0.5, 0.4))
     return sc
 
 

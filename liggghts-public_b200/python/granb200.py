@@ -27,7 +27,7 @@ EXPORTS = (
     "gb2_add_wall_plane", "gb2_add_wall_mesh", "gb2_setup", "gb2_run", "gb2_sync", "gb2_download_atoms",
     "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
-    "gb2_timer_stop", "gb2_census_noalloc",
+    "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -116,6 +116,8 @@ def lib(path=LIB_PATH):
         L.gb2_set_profiling.argtypes = [vp, ctypes.c_int]
         L.gb2_timer_start.argtypes = [vp]
         L.gb2_timer_stop.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.gb2_add_move_mesh_rotate.argtypes = [vp, ctypes.c_int, D, D, ctypes.c_double]
+        L.gb2_download_mesh_nodes.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, D, D]
         _LIB = L
     return _LIB
 
@@ -188,6 +190,11 @@ class Engine:
                                         int(fx.get("rolling_cdt", 0)))
                 if k >= 0:
                     self.ntri[len(self.fix_ids)] = len(nodes) // 9
+            elif kind == "move_mesh_rotate":
+                mesh_id = self.fix_ids[fx["mesh"]]
+                self._check(L.gb2_add_move_mesh_rotate(self.h, mesh_id, _dp(arr(fx["origin"])), _dp(arr(fx["axis"])),
+                                                       float(fx["period"])))
+                k = None
             elif kind == "nve_sphere":
                 k = None
             else:
@@ -289,6 +296,16 @@ class Engine:
         h = np.zeros((n, 3))
         self._check(self.L.gb2_download_mesh_contacts(self.h, k, n, ctypes.byref(cnt), _ip(tag), _ip(tri), _dp(h)))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_nodes(self, ifix):
+        """Current nodes (ntri, 3, 3) and node velocities of the mesh of fix ifix."""
+        n = ctypes.c_int()
+        self._check(self.L.gb2_download_mesh_nodes(self.h, self.fix_ids[ifix], 0, ctypes.byref(n), None, None))
+        nodes = np.zeros((n.value, 3, 3))
+        vel = np.zeros((n.value, 3, 3))
+        self._check(self.L.gb2_download_mesh_nodes(self.h, self.fix_ids[ifix], n.value, ctypes.byref(n), _dp(nodes),
+                                                   _dp(vel)))
+        return nodes, vel
 
     def mesh_topology(self, ifix):
         k = self.fix_ids[ifix]

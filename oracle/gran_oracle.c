@@ -78,9 +78,15 @@ typedef struct {
     int build_neighlist_ch;   /* FixContactHistoryMesh::build_neighlist_ */
     int *nneighs; int *npartner; int **partner; double **chist;
     unsigned char **keep; unsigned char **isect;
+    /* fix move/mesh rotate (MeshMoverRotate) and FixMesh rebuild trigger */
+    int moving;
+    double mv_point[3], mv_axis[3], mv_omega;
+    double (*vnode)[3][3];       /* element property "v" */
+    double (*node_last)[3][3];   /* nodesLastRe_ */
+    long next_reneighbor;        /* FixMesh::next_reneighbor */
 } wall_mesh;
 
-typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; } fixrec;
+typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; int imesh; } fixrec;
 
 struct orc_sim {
     orc_params p;
@@ -446,7 +452,8 @@ void orc_destroy(orc_sim *s)
             free(m->nneighs); free(m->npartner); free(m->partner); free(m->chist); free(m->keep); free(m->isect);
             free(m->node); free(m->center); free(m->rbound); free(m->edgevec); free(m->edgelen); free(m->edgenorm);
             free(m->surfnorm); free(m->obtuse); free(m->edge_active); free(m->corner_active); free(m->nneigh); free(m->neighfaces);
-            free(m);
+            free(m->vnode); free(m->node_last);
+            if (s->fix[k].kind == ORC_FIX_WALL_MESH) free(m);
         }
     }
     free_matrix(s->Yeff); free_matrix(s->Geff); free_matrix(s->betaeff); free_matrix(s->mu); free_matrix(s->mur);
@@ -538,6 +545,129 @@ int orc_add_wall_mesh(orc_sim *s, int ntri, const double *nodes, int wall_type, 
     m->isect = calloc(s->nmax, sizeof(unsigned char*));
     fr->wm = m;
     return s->nfix-1;
+}
+
+/* fix move/mesh ... rotate origin <p> axis <a> period <T>
+   (MeshMoverRotate constructor src/mesh_mover_rotation.cpp:66-96,
+   FixMoveMesh::setup src/fix_move_mesh.cpp:195-216: node velocities 0) */
+int orc_add_move_mesh_rotate(orc_sim *s, int ifix_mesh, double ox, double oy, double oz,
+                             double ax, double ay, double az, double period)
+{
+    if (ifix_mesh < 0 || ifix_mesh >= s->nfix || s->fix[ifix_mesh].kind != ORC_FIX_WALL_MESH) return -1;
+    if (!(period != 0.0)) return -1;
+    wall_mesh *m = s->fix[ifix_mesh].wm;
+    if (m->moving) return -1;   /* one mover per mesh */
+    fixrec *fr = &s->fix[s->nfix++];
+    fr->kind = ORC_FIX_MOVE_MESH;
+    fr->imesh = ifix_mesh;
+    m->moving = 1;
+    m->mv_point[0] = ox; m->mv_point[1] = oy; m->mv_point[2] = oz;
+    m->mv_axis[0] = ax; m->mv_axis[1] = ay; m->mv_axis[2] = az;
+    {   /* vectorNormalize3D src/vector_liggghts.h:62 */
+        double *v = m->mv_axis;
+        const double norm = sqrt(v[0]*v[0]+v[1]*v[1]+v[2]*v[2]);
+        const double invnorm = (norm == 0.) ? 0. : 1./norm;
+        v[0] *= invnorm; v[1] *= invnorm; v[2] *= invnorm;
+    }
+    m->mv_omega = 2.*M_PI/period;
+    int nt = m->ntri > 0 ? m->ntri : 1;
+    m->vnode = calloc((size_t)nt, sizeof(double)*9);
+    m->node_last = calloc((size_t)nt, sizeof(double)*9);
+    m->next_reneighbor = -1;
+    return s->nfix-1;
+}
+
+int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    if (nodes) memcpy(nodes, m->node, sizeof(double)*9*m->ntri);
+    if (vnode) {
+        if (m->vnode) memcpy(vnode, m->vnode, sizeof(double)*9*m->ntri);
+        else memset(vnode, 0, sizeof(double)*9*m->ntri);
+    }
+    return m->ntri;
+}
+
+/* MathExtraLiggghts::vec_quat_rotate src/math_extra_liggghts.h:451-468 with
+   MathExtra::quatquat src/math_extra.h:596 and qconjugate :560 */
+static void vec_quat_rotate(double *vec, const double *q)
+{
+    double vq[4] = {0., vec[0], vec[1], vec[2]};
+    double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+    double t[4], r[4];
+    t[0] = q[0]*vq[0] - q[1]*vq[1] - q[2]*vq[2] - q[3]*vq[3];
+    t[1] = q[0]*vq[1] + vq[0]*q[1] + q[2]*vq[3] - q[3]*vq[2];
+    t[2] = q[0]*vq[2] + vq[0]*q[2] + q[3]*vq[1] - q[1]*vq[3];
+    t[3] = q[0]*vq[3] + vq[0]*q[3] + q[1]*vq[2] - q[2]*vq[1];
+    r[0] = t[0]*qc[0] - t[1]*qc[1] - t[2]*qc[2] - t[3]*qc[3];
+    r[1] = t[0]*qc[1] + qc[0]*t[1] + t[2]*qc[3] - t[3]*qc[2];
+    r[2] = t[0]*qc[2] + qc[0]*t[2] + t[3]*qc[1] - t[1]*qc[3];
+    r[3] = t[0]*qc[3] + qc[0]*t[3] + t[1]*qc[2] - t[2]*qc[1];
+    vec[0] = r[1]; vec[1] = r[2]; vec[2] = r[3];
+}
+
+/* MeshMoverRotate::initial_integrate src/mesh_mover_rotation.cpp:110-138:
+   FixMoveMesh::initial_integrate zeroes "v" (first mover), FixMesh::rotate ->
+   MultiNodeMesh::rotate(dAngle, axis, p) src/multi_node_mesh_I.h:620-660
+   (nodes and centres) and TrackingMesh::rotate src/tracking_mesh_I.h:375
+   (edgeVec, edgeNorm, surfaceNorm are rotated, src/surface_mesh_I.h:75-77),
+   then v += omega x (node - p) */
+static void move_mesh_rotate(orc_sim *s, wall_mesh *m)
+{
+    const double dAngle = m->mv_omega*s->p.dt;
+    double axisNorm[3] = {m->mv_axis[0], m->mv_axis[1], m->mv_axis[2]};
+    sdiv3(axisNorm, mag3(axisNorm));
+    double dQ[4];
+    dQ[0] = cos(dAngle*0.5);
+    for (int i = 0; i < 3; i++) dQ[i+1] = axisNorm[i]*sin(dAngle*0.5);
+    const double *origin = m->mv_point;
+    const int trans = (origin[0]*origin[0] + origin[1]*origin[1] + origin[2]*origin[2]) > 0.;
+    for (int t = 0; t < m->ntri; t++) {
+        m->center[t][0] = m->center[t][1] = m->center[t][2] = 0.;
+        for (int j = 0; j < 3; j++) {
+            double *nd = m->node[t][j];
+            if (trans) sub3(nd, origin, nd);
+            vec_quat_rotate(nd, dQ);
+            if (trans) { nd[0] = nd[0]+origin[0]; nd[1] = nd[1]+origin[1]; nd[2] = nd[2]+origin[2]; }
+            for (int c = 0; c < 3; c++) m->center[t][c] = nd[c] + m->center[t][c];
+        }
+        sdiv3(m->center[t], 3.0);
+        for (int j = 0; j < 3; j++) { vec_quat_rotate(m->edgevec[t][j], dQ); vec_quat_rotate(m->edgenorm[t][j], dQ); }
+        vec_quat_rotate(m->surfnorm[t], dQ);
+    }
+    double omegaVec[3] = {m->mv_axis[0]*m->mv_omega, m->mv_axis[1]*m->mv_omega, m->mv_axis[2]*m->mv_omega};
+    for (int t = 0; t < m->ntri; t++)
+        for (int j = 0; j < 3; j++) {
+            double rPA[3], vRot[3];
+            m->vnode[t][j][0] = m->vnode[t][j][1] = m->vnode[t][j][2] = 0.;
+            sub3(m->node[t][j], m->mv_point, rPA);
+            cross3(omegaVec, rPA, vRot);
+            for (int c = 0; c < 3; c++) m->vnode[t][j][c] = m->vnode[t][j][c] + vRot[c];
+        }
+}
+
+/* MultiNodeMesh::storeNodePosRebuild src/multi_node_mesh_I.h:833 */
+static void mesh_store_node_last(wall_mesh *m)
+{
+    if (m->moving) memcpy(m->node_last, m->node, sizeof(double)*9*m->ntri);
+}
+
+/* MultiNodeMesh::decideRebuild src/multi_node_mesh_I.h:791-823 */
+static int mesh_decide_rebuild(orc_sim *s, wall_mesh *m)
+{
+    if (!m->moving) return 0;
+    const double triggersq = 0.25*s->p.skin*s->p.skin;
+    for (int t = 0; t < m->ntri; t++) {
+        int flag = 0;
+        for (int j = 0; j < 3; j++) {
+            double d[3]; sub3(m->node[t][j], m->node_last[t][j], d);
+            double distSq = d[0]*d[0] + d[1]*d[1] + d[2]*d[2];
+            if (distSq > triggersq) flag = 1;
+        }
+        if (flag) return 1;
+    }
+    return 0;
 }
 
 /* ------------------------------------------------------------------ */
@@ -1080,6 +1210,10 @@ static void neighbor_build(orc_sim *s)
 /* Neighbor::decide / check_distance src/neighbor.cpp:1357-1460 */
 static int neighbor_decide(orc_sim *s)
 {
+    /* must_check: fixes with force_reneighbor (FixMesh::next_reneighbor) src/neighbor.cpp:1359-1364 */
+    for (int k = 0; k < s->nfix; k++)
+        if (s->fix[k].kind == ORC_FIX_WALL_MESH && s->fix[k].wm->moving && s->fix[k].wm->next_reneighbor == s->ntimestep)
+            return 1;
     s->ago++;
     if (s->ago >= s->p.delay && s->ago % s->p.every == 0) {
         if (!s->p.check) return 1;
@@ -1282,11 +1416,40 @@ static void mesh_neighlist_pre_force(orc_sim *s, wall_mesh *m)
     if (!m->build_neighlist_nl) return;
     m->build_neighlist_nl = 0;
     for (int i = 0; i < s->nlocal + s->nghost; i++) m->nneighs[i] = 0;
-    /* static mesh, non-changing domain */
     double prev_skin = m->nl_skin, prev_distmax = m->nl_distmax;
     double rmax = 0.5*(s->cutneighmax - s->p.skin);
-    m->nl_skin = 0.5*s->p.skin;
-    m->nl_distmax = s->cutneighmax - rmax + m->nl_skin/(70.*M_PI);
+    if (m->moving) {   /* changingMesh src/fix_neighlist_mesh.cpp:252-258 */
+        m->nl_skin = s->p.skin;
+        m->nl_distmax = s->cutneighmax + m->nl_skin/(70.*M_PI);
+    } else {
+        m->nl_skin = 0.5*s->p.skin;
+        m->nl_distmax = s->cutneighmax - rmax + m->nl_skin/(70.*M_PI);
+    }
+    if (m->moving) {
+        /* handleTriangle with changingMesh: every bin of the current bounding
+           box +- distmax, src/fix_neighlist_mesh.cpp:383-395 */
+        for (int t = 0; t < m->ntri; t++) {
+            m->tri_n[t] = 0;
+            if (!s->nlocal) continue;
+            int lo[3], hi[3];
+            mesh_bin_bounds(s, m, t, lo, hi);
+            for (int ix = lo[0]; ix <= hi[0]; ix++)
+                for (int iy = lo[1]; iy <= hi[1]; iy++)
+                    for (int iz = lo[2]; iz <= hi[2]; iz++) {
+                        int iBin = iz*s->mbiny*s->mbinx + iy*s->mbinx + ix;
+                        if (iBin < 0 || iBin >= s->mbins) continue;
+                        for (int ia = s->binhead[iBin]; ia != -1; ia = s->bins[ia]) {
+                            if (tri_sphere_neighbuild(m, t, s->radius[ia]*1.0, &s->x[3*ia], m->nl_skin)) {
+                                if (m->tri_n[t] >= m->tri_cap[t]) { m->tri_cap[t] = m->tri_cap[t] ? 2*m->tri_cap[t] : 8; m->tri_list[t] = xrealloc(m->tri_list[t], sizeof(int)*m->tri_cap[t]); }
+                                m->tri_list[t][m->tri_n[t]++] = ia;
+                                m->nneighs[ia]++;
+                            }
+                        }
+                    }
+        }
+        m->last_bin_update = s->ntimestep;
+        return;
+    }
     if (m->nl_skin != prev_skin || m->nl_distmax != prev_distmax || m->last_bin_update < 0) {
         /* generate_bin_list :456 */
         double dx = s->binsizex / 2.0, dy = s->binsizey / 2.0, dz = s->binsizez / 2.0;
@@ -1584,10 +1747,14 @@ static void mesh_post_force(orc_sim *s, wall_mesh *m, int shearupdate)
             if (deltan <= 0 || (deltan < 0.0*s->radius[ip])) {
                 double *hist = NULL;
                 if (!mesh_handle_contact(s, m, ip, t, &hist, intersectflag, 7 == barysign)) continue;
+                double vw[3] = {vwall[0], vwall[1], vwall[2]};
+                if (m->moving)   /* barycentric wall velocity src/fix_wall_gran.cpp:992-996 */
+                    for (int c = 0; c < 3; c++)
+                        vw[c] = (bary[0]*m->vnode[t][0][c] + bary[1]*m->vnode[t][1][c] + bary[2]*m->vnode[t][2][c]);
                 sd.deltan = -deltan;
                 sd.delta[0] = -delta[0]; sd.delta[1] = -delta[1]; sd.delta[2] = -delta[2];
                 sd.contact_history = hist;
-                wall_compute_force(s, ip, &sd, vwall, m->wtype, m->rolling, shearupdate);
+                wall_compute_force(s, ip, &sd, vw, m->wtype, m->rolling, shearupdate);
             }
         }
     }
@@ -1655,10 +1822,15 @@ static void post_force_all(orc_sim *s, int shearupdate)
     }
 }
 
-static void pre_force_all(orc_sim *s)
+static void pre_force_all(orc_sim *s, int reneigh)
 {
     for (int k = 0; k < s->nfix; k++) {
         fixrec *fr = &s->fix[k];
+        if (fr->kind == ORC_FIX_WALL_MESH && fr->wm->moving) {
+            /* FixMesh::pre_force src/fix_mesh.cpp:564-588 */
+            if (reneigh) mesh_store_node_last(fr->wm);
+            else if (mesh_decide_rebuild(s, fr->wm)) fr->wm->next_reneighbor = s->ntimestep + 1;
+        }
         if (fr->kind == ORC_FIX_WALL_PLANE) wall_plane_pre_force(s, fr->wp);
         else if (fr->kind == ORC_FIX_WALL_MESH) { mesh_neighlist_pre_force(s, fr->wm); mesh_history_pre_force(s, fr->wm); }
     }
@@ -1695,7 +1867,7 @@ int orc_setup(orc_sim *s)
     pre_neighbor_all(s);
     neighbor_build(s);
     force_clear(s);
-    pre_force_all(s);
+    pre_force_all(s, 1);
     pair_compute(s, 0);
     post_force_all(s, 0);
     s->setupflag = 0;
@@ -1708,6 +1880,8 @@ int orc_run(orc_sim *s, int nsteps)
     for (int step = 0; step < nsteps; step++) {
         s->ntimestep++;
         nve_initial(s);
+        for (int k = 0; k < s->nfix; k++)
+            if (s->fix[k].kind == ORC_FIX_MOVE_MESH) move_mesh_rotate(s, s->fix[s->fix[k].imesh].wm);
         int nflag = neighbor_decide(s);
         if (nflag == 0) comm_forward(s);
         else {
@@ -1721,7 +1895,7 @@ int orc_run(orc_sim *s, int nsteps)
             neighbor_build(s);
         }
         force_clear(s);
-        pre_force_all(s);
+        pre_force_all(s, nflag);
         pair_compute(s, 1);
         post_force_all(s, 1);
         nve_final(s);

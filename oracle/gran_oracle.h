@@ -47,7 +47,7 @@ typedef struct {
 } orc_params;
 
 /* post_force fix kinds, processed in the order they were added */
-enum { ORC_FIX_GRAVITY = 1, ORC_FIX_WALL_PLANE = 2, ORC_FIX_WALL_MESH = 3 };
+enum { ORC_FIX_GRAVITY = 1, ORC_FIX_WALL_PLANE = 2, ORC_FIX_WALL_MESH = 3, ORC_FIX_MOVE_MESH = 4 };
 
 orc_sim *orc_create(const orc_params *p, int n,
                     const double *x, const double *v, const double *omega,
@@ -64,6 +64,13 @@ int orc_add_wall_plane(orc_sim *s, int dim, double pos, int wall_type, int rolli
    fix wall/gran ... mesh n_meshes 1 meshes <id>; returns fix index */
 int orc_add_wall_mesh(orc_sim *s, int ntri, const double *nodes, int wall_type,
                       double curvature, int rolling_cdt);
+
+/* fix move/mesh mesh <id> rotate origin ox oy oz axis ax ay az period T
+   on the mesh of fix index ifix_mesh; returns fix index */
+int orc_add_move_mesh_rotate(orc_sim *s, int ifix_mesh, double ox, double oy, double oz,
+                             double ax, double ay, double az, double period);
+/* current nodes (ntri x 3 x 3) and node velocities of a mesh fix; returns ntri */
+int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode);
 
 /* Verlet::setup */
 int orc_setup(orc_sim *s);

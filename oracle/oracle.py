@@ -70,6 +70,8 @@ def lib():
         L.orc_get_mesh_contacts.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
         L.orc_get_mesh_topology.argtypes = [ctypes.c_void_p, ctypes.c_int, U8, U8, I]
         L.orc_get_mesh_nneighs.argtypes = [ctypes.c_void_p, ctypes.c_int, I]
+        L.orc_add_move_mesh_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 7
+        L.orc_get_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_error.restype = ctypes.c_char_p
         L.orc_error.argtypes = [ctypes.c_void_p]
         L.orc_pair_force.argtypes = [ctypes.POINTER(OrcParams), D, D, D, D, D, D, ctypes.c_double, ctypes.c_double,
@@ -138,6 +140,12 @@ class Oracle:
                 self._keep.append(nodes)
                 k = L.orc_add_wall_mesh(self.h, nodes.shape[0], _dp(nodes), fx["wall_type"],
                                         fx.get("curvature", 0.0), int(fx.get("rolling_cdt", 0)))
+            elif kind == "move_mesh_rotate":
+                o, a = fx["origin"], fx["axis"]
+                k = L.orc_add_move_mesh_rotate(self.h, self.fix_ids[fx["mesh"]], o[0], o[1], o[2], a[0], a[1], a[2],
+                                               float(fx["period"]))
+                if k < 0:
+                    raise ValueError("oracle: bad move_mesh_rotate")
             elif kind == "nve_sphere":
                 k = None   # the oracle always integrates with fix nve/sphere
             else:
@@ -205,6 +213,13 @@ class Oracle:
         h = np.zeros((n, 3))
         self.L.orc_get_mesh_contacts(self.h, k, n, _ip(tag), _ip(tri), _dp(h))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_nodes(self, ifix):
+        n = self.L.orc_get_mesh_nodes(self.h, self.fix_ids[ifix], None, None)
+        nodes = np.zeros((n, 3, 3))
+        vel = np.zeros((n, 3, 3))
+        self.L.orc_get_mesh_nodes(self.h, self.fix_ids[ifix], _dp(nodes), _dp(vel))
+        return nodes, vel
 
     def mesh_topology(self, ifix, ntri_max):
         k = self.fix_ids[ifix]

@@ -142,3 +142,25 @@ def test_cone_topology_counts():
     # each generator line shared by two sectors is active on the larger element id only
     assert ea.sum() == 64 + 64 + 64 * 16
     assert ca.sum() == 2 * 64            # only boundary-ring nodes keep an active corner
+
+
+def test_move_mesh_rotate_kinematics():
+    """fix move/mesh rotate in the oracle: after k steps every node is the
+    initial node turned by k*omega*dt about the axis (to rounding), and the
+    node velocity is omega x r."""
+    sc = S.drum(n=200, diameter=0.05, length=0.03, n_theta=24, n_ax=4, cap_rings=2, omega=30.0)
+    n0 = np.asarray(sc["fixes"][1]["nodes"]).reshape(-1, 3, 3)
+    o = oracle.Oracle(sc)
+    o.setup()
+    nodes, vel = o.mesh_nodes(1)
+    assert np.array_equal(nodes, n0) and not vel.any()
+    k = 400
+    o.run(k)
+    nodes, vel = o.mesh_nodes(1)
+    phi = 30.0 * sc["dt"] * k
+    c, s_ = np.cos(phi), np.sin(phi)
+    rot = np.array([[1, 0, 0], [0, c, -s_], [0, s_, c]])
+    expect = n0 @ rot.T
+    assert np.max(np.abs(nodes - expect)) < 1e-12
+    w = np.array([30.0, 0.0, 0.0])
+    assert np.max(np.abs(vel - np.cross(w, nodes))) < 1e-13

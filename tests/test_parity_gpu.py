@@ -72,6 +72,30 @@ def test_hopper_mesh_run():
     assert total > 0
 
 
+def test_drum_rotating_mesh():
+    """fix move/mesh rotate: mesh nodes and node velocities, the forced
+    rebuilds when the mesh has moved more than skin/2, the moving-wall
+    velocity at each contact and the mesh contact history, bit for bit."""
+    sc = S.drum(n=1500, diameter=0.05, length=0.03, n_theta=48, n_ax=12, cap_rings=3, omega=50.0,
+                clearance=0.3e-3, vmax=0.05)
+    sc["sortfreq"] = 300
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    total = 0
+    for _ in range(8):
+        e.run(500)
+        o.run(500)
+        assert_atoms_equal(e, o)
+        assert_pairs_equal(e, o)
+        total += assert_mesh_equal(e, o, 1)
+        en, ev = e.mesh_nodes(1)
+        on, ov = o.mesh_nodes(1)
+        assert np.array_equal(en, on) and np.array_equal(ev, ov), "mesh nodes or node velocities differ"
+    assert total > 0, "no particle reached the rotating wall"
+    assert e.stats()["nbuilds"] == o.nbuilds and o.nbuilds > 50
+
+
 def test_deterministic():
     sc = S.sphere_pour(n=2000, seed=3)
     a = __import__("granb200").Engine(sc)
