@@ -269,6 +269,66 @@ def drum(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length=0.85, n
     return sc
 
 
+def sq_volume(shape, n):
+    """Volume of a superquadric with n1 = n2 = n (Jaklic et al.,
+    Segmentation and Recovery of Superquadrics, eq. 2.60; the reference's
+    volume_superquadric)."""
+    from scipy.special import beta
+    e = 2.0 / np.asarray(n, dtype=np.float64)
+    a, b, c = (np.asarray(shape)[..., k] for k in range(3))
+    return 2.0 * a * b * c * e * e * beta(0.5 * e, e + 1.0) * beta(0.5 * e, 0.5 * e + 1.0)
+
+
+def sq_inertia(shape, n, density):
+    """Principal moments of inertia of a superquadric, n1 = n2 = n (the
+    same published formulas as the reference's inertia_superquadric)."""
+    from scipy.special import beta
+    e = 2.0 / np.asarray(n, dtype=np.float64)
+    a1, a2, a3 = (np.asarray(shape)[..., k] for k in range(3))
+    pre = 0.5 * a1 * a2 * a3 * e * e * density
+    t1 = beta(1.5 * e, 0.5 * e) * beta(0.5 * e, 2.0 * e + 1.0)
+    t2 = 4.0 * beta(0.5 * e, 0.5 * e + 1.0) * beta(1.5 * e, e + 1.0)
+    ixx = pre * (a2 * a2 * t1 + a3 * a3 * t2)
+    iyy = pre * (a1 * a1 * t1 + a3 * a3 * t2)
+    izz = pre * (a1 * a1 + a2 * a2) * t1
+    return np.stack([ixx, iyy, izz], axis=-1)
+
+
+def random_quaternions(rng, n):
+    """Uniformly distributed unit quaternions (w, x, y, z) (Shoemake)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * math.pi * u2), np.sqrt(1 - u1) * np.cos(2 * math.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * math.pi * u3), np.sqrt(u1) * np.cos(2 * math.pi * u3)], axis=1)
+    return q[:, [3, 0, 1, 2]].copy()
+
+
+def sq_packing(n=200_000, seed=11, dt=1e-5, skin=0.5e-3, vin=1.0, density=2500.0, fill=0.8):
+    """Superquadric packing: half-axes U(1, 2) mm, blockiness U(2, 8) (one
+    exponent per particle, n1 = n2), uniformly random orientations, Hertz
+    contact with config-1 materials (E 5e6, nu 0.45, e 0.3, mu 0.5), on a
+    cubic lattice of spacing ``fill`` x the largest bounding diameter, with
+    uniform random velocities of +-``vin`` so contacts form and break."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    shape = rng.uniform(1e-3, 2e-3, size=(n, 3))
+    blk = rng.uniform(2.0, 8.0, size=n)
+    quat = random_quaternions(rng, n)
+    rb = np.array([oracle.sq_bounding_radius(shape[i], blk[i]) for i in range(n)]) if n <= 20000 else None
+    if rb is None:   # vectorised bound for large n: the corner of the box bounds every blockiness
+        rb = np.linalg.norm(shape, axis=1) * 1.0001
+    s = fill * 2.0 * rb.max()
+    m = int(math.ceil(n ** (1.0 / 3.0)))
+    idx = np.arange(n)
+    pos = np.stack([idx % m, (idx // m) % m, idx // (m * m)], axis=1).astype(np.float64) * s
+    pos -= pos.mean(axis=0)
+    vel = rng.uniform(-vin, vin, size=(n, 3))
+    vol = sq_volume(shape, blk)
+    atoms = {"x": pos, "v": vel, "quat": quat, "angmom": np.zeros((n, 3)), "shape": shape, "blockiness": blk,
+             "rmass": vol * density, "inertia": sq_inertia(shape, blk, density), "volume": vol}
+    return {"name": "sq_packing", "dt": dt, "skin": skin, "atoms": atoms,
+            "youngs": 5e6, "poisson": 0.45, "restitution": 0.3, "friction": 0.5}
+
+
 def subset(sc, n):
     """First ``n`` atoms of a scenario (same box, fixes and materials)."""
     out = dict(sc)

@@ -246,3 +246,135 @@ def pair_force(sc, xi, xj, vi, vj, wi, wj, ri, rj, mi, mj, ti=1, tj=1, shear=Non
     L.orc_pair_force(ctypes.byref(p), *[_dp(a) for a in arrs], ri, rj, mi, mj, ti, tj, _dp(sh), shearupdate,
                      *[_dp(o) for o in outs])
     return outs[0], outs[1], outs[2], outs[3], sh
+
+
+# ---------------------------------------------------------------- superquadrics
+
+class SqParticle(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_double * 3), ("quat", ctypes.c_double * 4), ("shape", ctypes.c_double * 3),
+                ("n", ctypes.c_double)]
+
+
+class SqSolution(ctypes.Structure):
+    _fields_ = [("point", ctypes.c_double * 3), ("mu", ctypes.c_double), ("fi", ctypes.c_double),
+                ("fj", ctypes.c_double), ("gradi", ctypes.c_double * 3), ("gradj", ctypes.c_double * 3),
+                ("merit", ctypes.c_double), ("iters", ctypes.c_int), ("solves", ctypes.c_int), ("fail", ctypes.c_int)]
+
+
+class SqParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("skin", ctypes.c_double), ("youngs", ctypes.c_double),
+                ("poisson", ctypes.c_double), ("restitution", ctypes.c_double), ("friction", ctypes.c_double)]
+
+
+def _sq_lib():
+    L = lib()
+    if not hasattr(L, "_sq_ready"):
+        L.orc_sq_contact_point.argtypes = [ctypes.POINTER(SqParticle), ctypes.POINTER(SqParticle), ctypes.c_int, D,
+                                           ctypes.POINTER(SqSolution)]
+        L.orc_sq_shape_props.argtypes = [ctypes.POINTER(SqParticle), D, D, D, D]
+        L.orc_sq_bounding_radius.restype = ctypes.c_double
+        L.orc_sq_bounding_radius.argtypes = [D, ctypes.c_double]
+        L.orc_sq_create.restype = ctypes.c_void_p
+        L.orc_sq_create.argtypes = [ctypes.POINTER(SqParams), ctypes.c_int] + [D] * 9
+        L.orc_sq_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_sq_setup.argtypes = [ctypes.c_void_p]
+        L.orc_sq_run.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_sq_get_atoms.argtypes = [ctypes.c_void_p] + [D] * 7
+        L.orc_sq_get_pairs.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, I, D, D]
+        LP = ctypes.POINTER(ctypes.c_long)
+        L.orc_sq_counters.argtypes = [ctypes.c_void_p, LP, LP, LP, LP]
+        L._sq_ready = True
+    return L
+
+
+def sq_particle(center, quat, shape, n):
+    p = SqParticle()
+    for k in range(3):
+        p.center[k] = center[k]
+        p.shape[k] = shape[k]
+    for k in range(4):
+        p.quat[k] = quat[k]
+    p.n = n
+    return p
+
+
+def sq_contact_point(pa, pb, guess=None):
+    """Contact-point solve for two superquadrics (dicts with center, quat,
+    shape, n): homotopy from spheres when guess is None, else one Newton
+    solve from guess.  Returns a dict of the solution."""
+    L = _sq_lib()
+    A = sq_particle(pa["center"], pa["quat"], pa["shape"], pa["n"])
+    B = sq_particle(pb["center"], pb["quat"], pb["shape"], pb["n"])
+    out = SqSolution()
+    g = np.ascontiguousarray(guess if guess is not None else np.zeros(3), dtype=np.float64)
+    L.orc_sq_contact_point(ctypes.byref(A), ctypes.byref(B), 0 if guess is None else 1, _dp(g), ctypes.byref(out))
+    return {"point": np.array(out.point[:]), "mu": out.mu, "fi": out.fi, "fj": out.fj,
+            "gradi": np.array(out.gradi[:]), "gradj": np.array(out.gradj[:]), "merit": out.merit,
+            "iters": out.iters, "solves": out.solves, "fail": out.fail}
+
+
+def sq_shape_props(p, x):
+    L = _sq_lib()
+    P = sq_particle(p["center"], p["quat"], p["shape"], p["n"])
+    f = ctypes.c_double()
+    g = np.zeros(3)
+    h = np.zeros(9)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    L.orc_sq_shape_props(ctypes.byref(P), _dp(xx), ctypes.cast(ctypes.byref(f), D), _dp(g), _dp(h))
+    return f.value, g, h.reshape(3, 3)
+
+
+def sq_bounding_radius(shape, n):
+    s = np.ascontiguousarray(shape, dtype=np.float64)
+    return _sq_lib().orc_sq_bounding_radius(_dp(s), float(n))
+
+
+class SqOracle:
+    """Superquadric DEM run in the oracle (see sq_oracle.h)."""
+
+    def __init__(self, sc):
+        L = _sq_lib()
+        self.L = L
+        p = SqParams(sc["dt"], sc["skin"], sc["youngs"], sc["poisson"], sc["restitution"], sc["friction"])
+        a = sc["atoms"]
+        self._keep = [np.ascontiguousarray(a[k], dtype=np.float64) for k in
+                      ("x", "v", "quat", "angmom", "shape", "blockiness", "rmass", "inertia", "volume")]
+        self.n = len(a["rmass"])
+        self.h = L.orc_sq_create(ctypes.byref(p), self.n, *[_dp(k) for k in self._keep])
+
+    def close(self):
+        if self.h:
+            self.L.orc_sq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self):
+        self.L.orc_sq_setup(self.h)
+
+    def run(self, n):
+        self.L.orc_sq_run(self.h, n)
+
+    def atoms(self):
+        n = self.n
+        out = {k: np.zeros((n, 3)) for k in ("x", "v", "angmom", "omega", "f", "torque")}
+        out["quat"] = np.zeros((n, 4))
+        self.L.orc_sq_get_atoms(self.h, _dp(out["x"]), _dp(out["v"]), _dp(out["quat"]), _dp(out["angmom"]),
+                                _dp(out["omega"]), _dp(out["f"]), _dp(out["torque"]))
+        return out
+
+    def pairs(self):
+        n = self.L.orc_sq_get_pairs(self.h, 0, None, None, None, None, None)
+        ti, tj, st = (np.zeros(n, dtype=np.int32) for _ in range(3))
+        cp, sh = np.zeros((n, 3)), np.zeros((n, 3))
+        self.L.orc_sq_get_pairs(self.h, n, _ip(ti), _ip(tj), _ip(st), _dp(cp), _dp(sh))
+        return {"tag_i": ti, "tag_j": tj, "state": st, "cp": cp, "shear": sh}
+
+    def counters(self):
+        v = [ctypes.c_long() for _ in range(4)]
+        self.L.orc_sq_counters(self.h, *[ctypes.byref(x) for x in v])
+        return {"iters": v[0].value, "solves": v[1].value, "pairs_solved": v[2].value, "nbuilds": v[3].value}
