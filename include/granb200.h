@@ -188,6 +188,56 @@ int gb2_last_error(gb2_ctx *ctx, char *buf, int len);
 /* library version string, e.g. "granb200 0.1 sm_100a" */
 const char *gb2_version(void);
 
+/* ====================================================================
+   Superquadric particles: pair_style gran model hertz tangential history
+   surface superquadric + fix nve/asphere (integration_scheme 1) on
+   atom_style superquadric (one blockiness per particle, n1 = n2), open
+   domain, one atom type.  Replaces the run of PairGran::compute with the
+   superquadric surface model (src/pair_gran_base.h:187-500,
+   src/surface_model_superquadric.h:108-205) and FixNVEAsphereBase
+   (src/fix_nve_asphere_base.cpp:319-620) under run_style verlet/b200.
+   ==================================================================== */
+typedef struct gb2_sq_ctx gb2_sq_ctx;
+
+typedef struct {
+    double dt, skin;
+    double youngs, poisson, restitution, friction;   /* one atom type */
+    int device;
+} gb2_sq_params;
+
+/* number of float parameters of the learned initial guess (see gb2_sq_set_learned_guess) */
+#define GB2_SQ_MLP_SIZE 9576
+
+int gb2_sq_create(const gb2_sq_params *p, gb2_sq_ctx **out);
+int gb2_sq_destroy(gb2_sq_ctx *ctx);
+/* per particle: x[3], v[3], quaternion[4] (w,i,j,k), angmom[3], shape[3]
+   (half-axes), blockiness, rmass, inertia[3] (principal), volume --
+   the AtomVecSuperquadric fields (src/atom_vec_superquadric.cpp) */
+int gb2_sq_upload(gb2_sq_ctx *ctx, int n, const double *x, const double *v, const double *quat,
+                  const double *angmom, const double *shape, const double *blockiness, const double *rmass,
+                  const double *inertia, const double *volume);
+/* learned initial guess for pairs without a previous contact point: the
+   parameters of an MLP 14 -> 64 -> 64 -> 64 -> 4 (layout in gb2_sq_kernels.cuh);
+   NULL switches it off.  No counterpart in the reference: the reference always
+   starts those pairs from spheres (calc_contact_point_if_no_previous_point_avaialable,
+   src/math_extra_liggghts_superquadric.cpp:1391), which stays the fallback. */
+int gb2_sq_set_learned_guess(gb2_sq_ctx *ctx, const float *params, int nparams);
+int gb2_sq_setup(gb2_sq_ctx *ctx);
+int gb2_sq_run(gb2_sq_ctx *ctx, int nsteps);
+/* gb2_sq_run timed with device events (ms) */
+int gb2_sq_run_timed(gb2_sq_ctx *ctx, int nsteps, double *ms);
+int gb2_sq_download(gb2_sq_ctx *ctx, int cap, double *x, double *v, double *quat, double *angmom,
+                    double *omega, double *f, double *torque);
+/* half-list pairs: owner and neighbour tags, contact state (0 far, 1 close,
+   2 intersecting), contact point of the last solve, shear history */
+int gb2_sq_download_pairs(gb2_sq_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *state, double *cp,
+                          double *shear);
+/* out[7]: Newton iterations, Newton solves, pairs solved, learned guesses
+   accepted, learned guesses rejected (homotopy fallback), neighbour builds,
+   half-list pairs */
+int gb2_sq_counters(gb2_sq_ctx *ctx, long long *out);
+int gb2_sq_last_error(gb2_sq_ctx *ctx, char *buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,707 @@
+// gb2_sq.cu -- superquadric time step (pair gran hertz/history on
+// superquadric surfaces + fix nve/asphere) and its C ABI (gb2_sq_* in
+// include/granb200.h).
+//
+// Step sequence as Verlet::run with these styles: initial_integrate,
+// displacement check, neighbour rebuild with contact-history transfer when
+// any particle moved more than skin/2, pair pass (one thread per half-list
+// slot), deterministic per-particle sums (reverse slots in ascending owner
+// order, then own slots), final_integrate.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/granb200.h"
+#include "gb2_sq_kernels.cuh"
+
+using namespace gb2;
+using namespace gb2::sq;
+
+namespace {
+
+constexpr int kB = 128;
+inline int nb(long n) { return (int)((n + kB - 1) / kB); }
+
+template <typename T>
+struct Buf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~Buf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t m)
+    {
+        if (m <= n && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
+        if (e == cudaSuccess) n = m;
+        return e;
+    }
+    void swap(Buf &o)
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
+};
+
+// ------------------------------------------------------------------ neighbour build kernels
+
+struct Grid {
+    double lo[3];
+    double inv;
+    int nc[3];
+};
+
+__global__ void k_sq_cellkey(SqDev D, Grid G, unsigned *keys, int *vals, int *counts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const dbl4 x = D.x[i];
+    const double c[3] = {x.x, x.y, x.z};
+    int ix[3];
+    for (int d = 0; d < 3; d++) ix[d] = min(max((int)((c[d] - G.lo[d]) * G.inv), 0), G.nc[d] - 1);
+    const int key = (ix[2] * G.nc[1] + ix[1]) * G.nc[0] + ix[0];
+    keys[i] = (unsigned)key;
+    vals[i] = i;
+    atomicAdd(&counts[key], 1);
+}
+
+// count (fill == false) or write (fill == true) the half-list neighbours
+// j > i within rb_i + rb_j + skin, then sort the row ascending
+__global__ void k_sq_neigh(SqDev D, Grid G, const int *cell_start, const int *cell_atoms, int *cnt, int *nbr,
+                           int *own, int fill)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const dbl4 xi = D.x[i];
+    const double c[3] = {xi.x, xi.y, xi.z};
+    int ix[3];
+    for (int d = 0; d < 3; d++) ix[d] = min(max((int)((c[d] - G.lo[d]) * G.inv), 0), G.nc[d] - 1);
+    int m = 0;
+    const int base = fill ? D.start[i] : 0;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const int cx = ix[0] + dx, cy = ix[1] + dy, cz = ix[2] + dz;
+                if (cx < 0 || cy < 0 || cz < 0 || cx >= G.nc[0] || cy >= G.nc[1] || cz >= G.nc[2]) continue;
+                const int cell = (cz * G.nc[1] + cy) * G.nc[0] + cx;
+                for (int a = cell_start[cell]; a < cell_start[cell + 1]; a++) {
+                    const int j = cell_atoms[a];
+                    if (j <= i) continue;
+                    const dbl4 xj = D.x[j];
+                    const double ddx = xi.x - xj.x, ddy = xi.y - xj.y, ddz = xi.z - xj.z;
+                    const double cut = xi.w + xj.w + D.skin;
+                    if (ddx * ddx + ddy * ddy + ddz * ddz > cut * cut) continue;
+                    if (fill) {
+                        nbr[base + m] = j;
+                        own[base + m] = i;
+                    }
+                    m++;
+                }
+            }
+    if (!fill) {
+        cnt[i] = m;
+        return;
+    }
+    for (int a = 1; a < m; a++) {   // ascending j within the row
+        const int v = nbr[base + a];
+        int b = a - 1;
+        while (b >= 0 && nbr[base + b] > v) {
+            nbr[base + b + 1] = nbr[base + b];
+            b--;
+        }
+        nbr[base + b + 1] = v;
+    }
+}
+
+// FixContactHistory transfer at a rebuild: a new slot (i, j) takes the old
+// slot's history when the old pair was flagged (touching), else zeros
+__global__ void k_sq_transfer(SqDev D, int nslots, const int *own, const int *ostart, const int *onbr,
+                              const int *oflag, const int *ostate, const dbl4 *ocp, const double2 *oalpha,
+                              const dbl4 *oshear)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int i = own[s], j = D.nbr[s];
+    int lo = ostart[i], hi = ostart[i + 1] - 1, hit = -1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int v = onbr[mid];
+        if (v == j) {
+            hit = mid;
+            break;
+        }
+        if (v < j) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    if (hit >= 0 && oflag[hit]) {
+        D.flag[s] = oflag[hit];
+        D.state[s] = ostate[hit];
+        D.cp[s] = ocp[hit];
+        D.alpha[s] = oalpha[hit];
+        D.shear[s] = oshear[hit];
+    } else {
+        D.flag[s] = 0;
+        D.state[s] = FAR;
+        D.cp[s] = dbl4{0, 0, 0, 0};
+        D.alpha[s] = double2{0, 0};
+        D.shear[s] = dbl4{0, 0, 0, 0};
+    }
+}
+
+__global__ void k_sq_rcount(SqDev D, int nslots, int *rcnt)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    atomicAdd(&rcnt[D.nbr[s]], 1);
+}
+__global__ void k_sq_rfill(SqDev D, int nslots, int *rfill)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int j = D.nbr[s];
+    D.rslot[D.rstart[j] + atomicAdd(&rfill[j], 1)] = s;
+}
+__global__ void k_sq_rsort(SqDev D)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.n) return;
+    const int b0 = D.rstart[k], m = D.rstart[k + 1] - b0;
+    for (int a = 1; a < m; a++) {
+        const int v = D.rslot[b0 + a];
+        int b = a - 1;
+        while (b >= 0 && D.rslot[b0 + b] > v) {
+            D.rslot[b0 + b + 1] = D.rslot[b0 + b];
+            b--;
+        }
+        D.rslot[b0 + b + 1] = v;
+    }
+}
+
+__global__ void k_sq_hold(SqDev D)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    D.xhold[i] = D.x[i];
+}
+
+__global__ void k_sq_coords(SqDev D, double *xs)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const dbl4 x = D.x[i];
+    xs[i] = x.x;
+    xs[D.n + i] = x.y;
+    xs[2 * D.n + i] = x.z;
+}
+
+}  // namespace
+
+struct gb2_sq_ctx {
+    gb2_sq_params P{};
+    std::string err;
+    cudaStream_t st = nullptr;
+    int n = 0;
+    bool setup_done = false;
+    double rbmax = 0;
+    Buf<dbl4> x, v, q, L, w, f, t, shape, inert, xhold;
+    // list (current and previous for the history transfer)
+    long nslots = 0;
+    Buf<int> start, nbr, own, flag, state, ostart, onbr, oown, oflag, ostate;
+    Buf<dbl4> cp, shear, ocp, oshear, pfi, pti, ptj;
+    Buf<double2> alpha, oalpha;
+    Buf<int> rstart, rslot, rcnt, cnt;
+    // grid
+    Buf<unsigned> keys, keys2;
+    Buf<int> vals, cell_atoms, cell_start, counts;
+    Buf<double> xs, red;
+    Buf<char> tmp;
+    Buf<unsigned long long> counters;
+    Buf<int> dflag;
+    int *h_pin = nullptr;
+    double Yeff = 0, Geff = 0, betaeff = 0, mu = 0;
+    long nbuilds = 0;
+    Buf<float> mlp;
+    bool mlp_on = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+namespace {
+
+int sq_err(gb2_sq_ctx *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+    return code;
+}
+
+#define SQCK(call)                                                                                                \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) return sq_err(c, GB2_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));          \
+    } while (0)
+#define SQCKL() SQCK(cudaGetLastError())
+
+SqDev sq_dev(gb2_sq_ctx *c)
+{
+    SqDev D;
+    std::memset(&D, 0, sizeof D);
+    D.n = c->n;
+    D.x = c->x.p;
+    D.v = c->v.p;
+    D.q = c->q.p;
+    D.L = c->L.p;
+    D.w = c->w.p;
+    D.f = c->f.p;
+    D.t = c->t.p;
+    D.shape = c->shape.p;
+    D.inert = c->inert.p;
+    D.xhold = c->xhold.p;
+    D.start = c->start.p;
+    D.nbr = c->nbr.p;
+    D.flag = c->flag.p;
+    D.state = c->state.p;
+    D.cp = c->cp.p;
+    D.shear = c->shear.p;
+    D.alpha = c->alpha.p;
+    D.pfi = c->pfi.p;
+    D.pti = c->pti.p;
+    D.ptj = c->ptj.p;
+    D.rstart = c->rstart.p;
+    D.rslot = c->rslot.p;
+    D.dt = c->P.dt;
+    D.skin = c->P.skin;
+    D.triggersq = 0.25 * c->P.skin * c->P.skin;
+    D.Yeff = c->Yeff;
+    D.Geff = c->Geff;
+    D.betaeff = c->betaeff;
+    D.mu = c->mu;
+    D.cnt = c->counters.p;
+    D.dflag = c->dflag.p;
+    D.mlp = c->mlp_on ? c->mlp.p : nullptr;
+    return D;
+}
+
+int scan(gb2_sq_ctx *c, const int *in, int *out, int n)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, c->st);
+    SQCK(c->tmp.alloc(bytes));
+    bytes = c->tmp.n;
+    SQCK(cub::DeviceScan::ExclusiveSum(c->tmp.p, bytes, in, out, n, c->st));
+    return 0;
+}
+
+// neighbour list (half, bounding spheres + skin) with history transfer
+int sq_build(gb2_sq_ctx *c, bool transfer)
+{
+    const int n = c->n;
+    SqDev D = sq_dev(c);
+    // grid over the current particle extent
+    SQCK(c->xs.alloc((size_t)3 * n));
+    SQCK(c->red.alloc(6));
+    k_sq_coords<<<nb(n), kB, 0, c->st>>>(D, c->xs.p);
+    SQCKL();
+    size_t bytes = 0;
+    cub::DeviceReduce::Min(nullptr, bytes, c->xs.p, c->red.p, n, c->st);
+    SQCK(c->tmp.alloc(bytes));
+    for (int d = 0; d < 3; d++) {
+        bytes = c->tmp.n;
+        SQCK(cub::DeviceReduce::Min(c->tmp.p, bytes, c->xs.p + (size_t)d * n, c->red.p + d, n, c->st));
+        bytes = c->tmp.n;
+        SQCK(cub::DeviceReduce::Max(c->tmp.p, bytes, c->xs.p + (size_t)d * n, c->red.p + 3 + d, n, c->st));
+    }
+    double ext[6];
+    SQCK(cudaMemcpyAsync(ext, c->red.p, sizeof ext, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    Grid G;
+    const double cell = 2.0 * c->rbmax + c->P.skin;
+    G.inv = 1.0 / cell;
+    long ncell = 1;
+    for (int d = 0; d < 3; d++) {
+        G.lo[d] = ext[d];
+        G.nc[d] = std::max(1, (int)((ext[3 + d] - ext[d]) * G.inv) + 1);
+        ncell *= G.nc[d];
+    }
+    if (ncell > (1l << 28)) return sq_err(c, GB2_ERR_UNSUPPORTED, "particle extent too large for the cell grid");
+    SQCK(c->keys.alloc(n));
+    SQCK(c->keys2.alloc(n));
+    SQCK(c->vals.alloc(n));
+    SQCK(c->cell_atoms.alloc(n));
+    SQCK(c->counts.alloc((size_t)ncell + 1));
+    SQCK(c->cell_start.alloc((size_t)ncell + 1));
+    SQCK(cudaMemsetAsync(c->counts.p, 0, sizeof(int) * (ncell + 1), c->st));
+    k_sq_cellkey<<<nb(n), kB, 0, c->st>>>(D, G, c->keys.p, c->vals.p, c->counts.p);
+    SQCKL();
+    int endbit = 1;
+    while ((1l << endbit) < ncell + 1) endbit++;
+    bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, c->keys.p, c->keys2.p, c->vals.p, c->cell_atoms.p, n, 0, endbit,
+                                    c->st);
+    SQCK(c->tmp.alloc(bytes));
+    bytes = c->tmp.n;
+    SQCK(cub::DeviceRadixSort::SortPairs(c->tmp.p, bytes, c->keys.p, c->keys2.p, c->vals.p, c->cell_atoms.p, n, 0,
+                                         endbit, c->st));
+    if (scan(c, c->counts.p, c->cell_start.p, (int)ncell + 1)) return GB2_ERR_CUDA;
+    // keep the old list for the transfer
+    if (transfer) {
+        c->start.swap(c->ostart);
+        c->nbr.swap(c->onbr);
+        c->own.swap(c->oown);
+        c->flag.swap(c->oflag);
+        c->state.swap(c->ostate);
+        c->cp.swap(c->ocp);
+        c->alpha.swap(c->oalpha);
+        c->shear.swap(c->oshear);
+    }
+    SQCK(c->cnt.alloc((size_t)n + 1));
+    SQCK(c->start.alloc((size_t)n + 1));
+    SQCK(cudaMemsetAsync(c->cnt.p, 0, sizeof(int) * (n + 1), c->st));
+    D = sq_dev(c);
+    k_sq_neigh<<<nb(n), kB, 0, c->st>>>(D, G, c->cell_start.p, c->cell_atoms.p, c->cnt.p, nullptr, nullptr, 0);
+    SQCKL();
+    if (scan(c, c->cnt.p, c->start.p, n + 1)) return GB2_ERR_CUDA;
+    int tot = 0;
+    SQCK(cudaMemcpyAsync(&c->h_pin[0], c->start.p + n, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    tot = c->h_pin[0];
+    c->nslots = tot;
+    const size_t ns = std::max(tot, 1);
+    SQCK(c->nbr.alloc(ns));
+    SQCK(c->own.alloc(ns));
+    SQCK(c->flag.alloc(ns));
+    SQCK(c->state.alloc(ns));
+    SQCK(c->cp.alloc(ns));
+    SQCK(c->alpha.alloc(ns));
+    SQCK(c->shear.alloc(ns));
+    SQCK(c->pfi.alloc(ns));
+    SQCK(c->pti.alloc(ns));
+    SQCK(c->ptj.alloc(ns));
+    SQCK(c->rslot.alloc(ns));
+    D = sq_dev(c);
+    k_sq_neigh<<<nb(n), kB, 0, c->st>>>(D, G, c->cell_start.p, c->cell_atoms.p, nullptr, c->nbr.p, c->own.p, 1);
+    SQCKL();
+    if (tot > 0) {
+        if (transfer && c->ostart.p) {
+            k_sq_transfer<<<nb(tot), kB, 0, c->st>>>(D, tot, c->own.p, c->ostart.p, c->onbr.p, c->oflag.p,
+                                                      c->ostate.p, c->ocp.p, c->oalpha.p, c->oshear.p);
+            SQCKL();
+        } else {
+            SQCK(cudaMemsetAsync(c->flag.p, 0, sizeof(int) * tot, c->st));
+            SQCK(cudaMemsetAsync(c->state.p, 0, sizeof(int) * tot, c->st));
+            SQCK(cudaMemsetAsync(c->cp.p, 0, sizeof(dbl4) * tot, c->st));
+            SQCK(cudaMemsetAsync(c->alpha.p, 0, sizeof(double2) * tot, c->st));
+            SQCK(cudaMemsetAsync(c->shear.p, 0, sizeof(dbl4) * tot, c->st));
+        }
+    }
+    // reverse CSR
+    SQCK(c->rcnt.alloc((size_t)n + 1));
+    SQCK(c->rstart.alloc((size_t)n + 1));
+    SQCK(cudaMemsetAsync(c->rcnt.p, 0, sizeof(int) * (n + 1), c->st));
+    if (tot > 0) k_sq_rcount<<<nb(tot), kB, 0, c->st>>>(D, tot, c->rcnt.p);
+    SQCKL();
+    if (scan(c, c->rcnt.p, c->rstart.p, n + 1)) return GB2_ERR_CUDA;
+    SQCK(cudaMemsetAsync(c->rcnt.p, 0, sizeof(int) * (n + 1), c->st));
+    D = sq_dev(c);
+    if (tot > 0) k_sq_rfill<<<nb(tot), kB, 0, c->st>>>(D, tot, c->rcnt.p);
+    SQCKL();
+    k_sq_rsort<<<nb(n), kB, 0, c->st>>>(D);
+    SQCKL();
+    k_sq_hold<<<nb(n), kB, 0, c->st>>>(D);
+    SQCKL();
+    c->nbuilds++;
+    return 0;
+}
+
+int sq_force(gb2_sq_ctx *c, int shearupdate)
+{
+    SqDev D = sq_dev(c);
+    if (c->nslots > 0) k_sq_pair<<<nb(c->nslots), kB, 0, c->st>>>(D, c->own.p, (int)c->nslots, shearupdate);
+    SQCKL();
+    k_sq_sum<<<nb(c->n), kB, 0, c->st>>>(D);
+    SQCKL();
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gb2_sq_create(const gb2_sq_params *p, gb2_sq_ctx **out)
+{
+    if (!p || !out) return GB2_ERR_ARG;
+    *out = nullptr;
+    if (!(p->dt > 0) || p->skin < 0) return GB2_ERR_ARG;
+    if (p->poisson < 0. || p->poisson > 0.5 || p->restitution <= 0.05 || p->restitution > 1) return GB2_ERR_ARG;
+    if (cudaSetDevice(p->device) != cudaSuccess) return GB2_ERR_CUDA;
+    gb2_sq_ctx *c = new gb2_sq_ctx();
+    c->P = *p;
+    // material constants (src/global_properties.cpp:432-540), one atom type
+    const double E = p->youngs, nu = p->poisson;
+    c->Yeff = 1. / ((1. - std::pow(nu, 2.)) / E + (1. - std::pow(nu, 2.)) / E);
+    c->Geff = 1. / (2. * (2. - nu) * (1. + nu) / E + 2. * (2. - nu) * (1. + nu) / E);
+    const double lg = std::log(p->restitution);
+    c->betaeff = lg / std::sqrt(std::pow(lg, 2.) + std::pow(M_PI, 2.));
+    c->mu = p->friction;
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&c->h_pin, 4 * sizeof(int)) != cudaSuccess || c->counters.alloc(8) != cudaSuccess ||
+        c->dflag.alloc(1) != cudaSuccess || cudaMemset(c->counters.p, 0, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess) {
+        delete c;
+        return GB2_ERR_CUDA;
+    }
+    *out = c;
+    return 0;
+}
+
+int gb2_sq_destroy(gb2_sq_ctx *c)
+{
+    if (!c) return 0;
+    cudaStreamSynchronize(c->st);
+    if (c->h_pin) cudaFreeHost(c->h_pin);
+    if (c->e0) cudaEventDestroy(c->e0);
+    if (c->e1) cudaEventDestroy(c->e1);
+    cudaStream_t st = c->st;
+    delete c;
+    if (st) cudaStreamDestroy(st);
+    return 0;
+}
+
+// bounding_sphere_radius_superquadric with n1 = n2 = n, times scale_koef 1.0001
+// (src/math_extra_liggghts_superquadric.cpp:206-233)
+static double host_pow_abs(double base, double e)
+{
+    base = std::fabs(base);
+    const double tol = 1e-12;
+    if (std::fabs(e) < tol || std::fabs(base - 1.0) < tol) return 1.0;
+    if (std::fabs(base) < tol) return 0.0;
+    const double nn = std::floor(std::fabs(e));
+    double r = 1.0;
+    for (int i = 0; i < (int)nn; i++) r *= base;
+    const double nd = std::fabs(e) - nn;
+    if (nd > 0.0) r *= (std::fabs(2.0 * nd - 1.0) < 2.0 * tol) ? std::sqrt(base) : std::pow(base, nd);
+    return e > 0.0 ? r : 1.0 / r;
+}
+static double bounding_radius(const double *shape, double n)
+{
+    if (n == 2.0 || std::fabs(n - 2.0) < 1e-13) return std::max(std::max(shape[0], shape[1]), shape[2]) * 1.0001;
+    const double a = std::max(shape[0], shape[1]), b = std::min(shape[0], shape[1]), c = shape[2];
+    const double n1 = std::max(2.1, n), n2 = std::max(2.1, n);
+    const double alpha = host_pow_abs(b / a, 2.0 / (n2 - 2.0));
+    const double gamma = host_pow_abs(1.0 + host_pow_abs(alpha, n2), n1 / n2 - 1.0);
+    const double beta = host_pow_abs(c * c / (a * a) * gamma, 1.0 / (n1 - 2.0));
+    const double x0 = 1.0 / host_pow_abs(host_pow_abs(1.0 + host_pow_abs(alpha, n2), n1 / n2) + host_pow_abs(beta, n1), 1.0 / n1);
+    const double xt = x0 * a, yt = alpha * x0 * b, zt = beta * x0 * c;
+    return std::sqrt(xt * xt + yt * yt + zt * zt) * 1.0001;
+}
+
+int gb2_sq_upload(gb2_sq_ctx *c, int n, const double *x, const double *v, const double *quat, const double *angmom,
+                  const double *shape, const double *blockiness, const double *rmass, const double *inertia,
+                  const double *volume)
+{
+    if (!c || n <= 0 || !x || !v || !quat || !angmom || !shape || !blockiness || !rmass || !inertia || !volume)
+        return GB2_ERR_ARG;
+    std::vector<dbl4> hx(n), hv(n), hq(n), hL(n), hs(n), hi(n);
+    double rbmax = 0;
+    for (int i = 0; i < n; i++) {
+        if (!(blockiness[i] >= 2.0) || !(shape[3 * i] > 0) || !(shape[3 * i + 1] > 0) || !(shape[3 * i + 2] > 0) ||
+            !(rmass[i] > 0) || !(volume[i] > 0))
+            return sq_err(c, GB2_ERR_ARG, "superquadric %d: shape, blockiness (>= 2), mass and volume must be positive", i);
+        const double rb = bounding_radius(&shape[3 * i], blockiness[i]);
+        rbmax = std::max(rbmax, rb);
+        hx[i] = dbl4{x[3 * i], x[3 * i + 1], x[3 * i + 2], rb};
+        hv[i] = dbl4{v[3 * i], v[3 * i + 1], v[3 * i + 2], rmass[i]};
+        hq[i] = dbl4{quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]};
+        hL[i] = dbl4{angmom[3 * i], angmom[3 * i + 1], angmom[3 * i + 2], 0.0};
+        hs[i] = dbl4{shape[3 * i], shape[3 * i + 1], shape[3 * i + 2], blockiness[i]};
+        // volume-equivalent radius used for the Hertz reff (src/pair_gran_base.h:266-270)
+        hi[i] = dbl4{inertia[3 * i], inertia[3 * i + 1], inertia[3 * i + 2], std::cbrt(0.75 * volume[i] / M_PI)};
+    }
+    c->n = n;
+    c->rbmax = rbmax;
+    SQCK(c->x.alloc(n));
+    SQCK(c->v.alloc(n));
+    SQCK(c->q.alloc(n));
+    SQCK(c->L.alloc(n));
+    SQCK(c->w.alloc(n));
+    SQCK(c->f.alloc(n));
+    SQCK(c->t.alloc(n));
+    SQCK(c->shape.alloc(n));
+    SQCK(c->inert.alloc(n));
+    SQCK(c->xhold.alloc(n));
+    SQCK(cudaMemcpyAsync(c->x.p, hx.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemcpyAsync(c->v.p, hv.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemcpyAsync(c->q.p, hq.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemcpyAsync(c->L.p, hL.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemcpyAsync(c->shape.p, hs.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemcpyAsync(c->inert.p, hi.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaMemsetAsync(c->f.p, 0, sizeof(dbl4) * n, c->st));
+    SQCK(cudaMemsetAsync(c->t.p, 0, sizeof(dbl4) * n, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    c->setup_done = false;
+    return 0;
+}
+
+int gb2_sq_set_learned_guess(gb2_sq_ctx *c, const float *params, int nparams)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!params) {
+        c->mlp_on = false;
+        return 0;
+    }
+    if (nparams != kMlpSize) return sq_err(c, GB2_ERR_ARG, "learned guess: expected %d parameters, got %d", kMlpSize, nparams);
+    SQCK(c->mlp.alloc(kMlpSize));
+    SQCK(cudaMemcpyAsync(c->mlp.p, params, sizeof(float) * kMlpSize, cudaMemcpyHostToDevice, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    c->mlp_on = true;
+    return 0;
+}
+
+int gb2_sq_setup(gb2_sq_ctx *c)
+{
+    if (!c || c->n <= 0) return GB2_ERR_ARG;
+    c->err.clear();
+    SqDev D = sq_dev(c);
+    k_sq_omega<<<nb(c->n), kB, 0, c->st>>>(D);
+    SQCKL();
+    int rc = sq_build(c, false);
+    if (rc) return rc;
+    rc = sq_force(c, 0);
+    if (rc) return rc;
+    SQCK(cudaStreamSynchronize(c->st));
+    c->setup_done = true;
+    return 0;
+}
+
+int gb2_sq_run(gb2_sq_ctx *c, int nsteps)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->setup_done) return sq_err(c, GB2_ERR_STATE, "gb2_sq_setup must precede gb2_sq_run");
+    for (int s = 0; s < nsteps; s++) {
+        SQCK(cudaMemsetAsync(c->dflag.p, 0, sizeof(int), c->st));
+        SqDev D = sq_dev(c);
+        k_sq_initial<<<nb(c->n), kB, 0, c->st>>>(D, 1);
+        SQCKL();
+        SQCK(cudaMemcpyAsync(&c->h_pin[1], c->dflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        SQCK(cudaStreamSynchronize(c->st));
+        if (c->h_pin[1]) {
+            const int rc = sq_build(c, true);
+            if (rc) return rc;
+        }
+        int rc = sq_force(c, 1);
+        if (rc) return rc;
+        D = sq_dev(c);
+        k_sq_final<<<nb(c->n), kB, 0, c->st>>>(D);
+        SQCKL();
+    }
+    SQCK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int gb2_sq_run_timed(gb2_sq_ctx *c, int nsteps, double *ms)
+{
+    if (!c || !ms) return GB2_ERR_ARG;
+    SQCK(cudaStreamSynchronize(c->st));
+    SQCK(cudaEventRecord(c->e0, c->st));
+    const int rc = gb2_sq_run(c, nsteps);
+    if (rc) return rc;
+    SQCK(cudaEventRecord(c->e1, c->st));
+    SQCK(cudaEventSynchronize(c->e1));
+    float f = 0;
+    SQCK(cudaEventElapsedTime(&f, c->e0, c->e1));
+    *ms = f;
+    return 0;
+}
+
+int gb2_sq_download(gb2_sq_ctx *c, int cap, double *x, double *v, double *quat, double *angmom, double *omega,
+                    double *f, double *torque)
+{
+    if (!c || cap < c->n) return GB2_ERR_ARG;
+    const int n = c->n;
+    std::vector<dbl4> h(n);
+    struct Item {
+        Buf<dbl4> *b;
+        double *out;
+        int k;
+    } items[] = {{&c->x, x, 3}, {&c->v, v, 3}, {&c->q, quat, 4}, {&c->L, angmom, 3},
+                 {&c->w, omega, 3}, {&c->f, f, 3}, {&c->t, torque, 3}};
+    for (auto &it : items) {
+        if (!it.out) continue;
+        SQCK(cudaMemcpyAsync(h.data(), it.b->p, sizeof(dbl4) * n, cudaMemcpyDeviceToHost, c->st));
+        SQCK(cudaStreamSynchronize(c->st));
+        for (int i = 0; i < n; i++) {
+            const double r[4] = {h[i].x, h[i].y, h[i].z, h[i].w};
+            for (int k = 0; k < it.k; k++) it.out[it.k * i + k] = r[k];
+        }
+    }
+    return 0;
+}
+
+int gb2_sq_download_pairs(gb2_sq_ctx *c, int cap, int *n, int *tag_i, int *tag_j, int *state, double *cp,
+                          double *shear)
+{
+    if (!c || !n) return GB2_ERR_ARG;
+    const long ns = c->nslots;
+    *n = (int)ns;
+    if (cap < ns || ns == 0) return 0;
+    std::vector<int> own(ns), nbr(ns), st(ns);
+    std::vector<dbl4> hcp(ns), hsh(ns);
+    SQCK(cudaMemcpyAsync(own.data(), c->own.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaMemcpyAsync(nbr.data(), c->nbr.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaMemcpyAsync(st.data(), c->state.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaMemcpyAsync(hcp.data(), c->cp.p, sizeof(dbl4) * ns, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaMemcpyAsync(hsh.data(), c->shear.p, sizeof(dbl4) * ns, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    for (long s = 0; s < ns; s++) {
+        if (tag_i) tag_i[s] = own[s] + 1;
+        if (tag_j) tag_j[s] = nbr[s] + 1;
+        if (state) state[s] = st[s];
+        if (cp) {
+            cp[3 * s] = hcp[s].x;
+            cp[3 * s + 1] = hcp[s].y;
+            cp[3 * s + 2] = hcp[s].z;
+        }
+        if (shear) {
+            shear[3 * s] = hsh[s].x;
+            shear[3 * s + 1] = hsh[s].y;
+            shear[3 * s + 2] = hsh[s].z;
+        }
+    }
+    return 0;
+}
+
+int gb2_sq_counters(gb2_sq_ctx *c, long long *out)
+{
+    if (!c || !out) return GB2_ERR_ARG;
+    unsigned long long h[8];
+    SQCK(cudaMemcpyAsync(h, c->counters.p, sizeof h, cudaMemcpyDeviceToHost, c->st));
+    SQCK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < 5; k++) out[k] = (long long)h[k];
+    out[5] = c->nbuilds;
+    out[6] = c->nslots;
+    return 0;
+}
+
+int gb2_sq_last_error(gb2_sq_ctx *c, char *buf, int len)
+{
+    if (!c || !buf || len <= 0) return GB2_ERR_ARG;
+    snprintf(buf, len, "%s", c->err.c_str());
+    return 0;
+}
+
+}  // extern "C"

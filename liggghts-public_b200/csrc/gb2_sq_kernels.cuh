@@ -1,0 +1,440 @@
+// gb2_sq_kernels.cuh -- kernels of the superquadric time step.
+//
+// Layout (structure of arrays, 32-byte records):
+//   per atom: x {x, y, z, rbound}, v {vx, vy, vz, m}, q {w, i, j, k},
+//             L {angmom, -}, w {omega, -}, f, t, shape {a, b, c, n},
+//             inert {Ixx, Iyy, Izz, rvol}, xhold
+//   half list in CSR form by owner i (neighbours j > i, ascending):
+//             start[i] .. start[i+1], nbr[s]; per slot s the contact history
+//             flag, state (far/close/intersect), cp {contact point, -},
+//             alpha {alphaA, alphaB}, shear {s0, s1, s2, -}
+//   per slot results of the pair pass: fi (force on i), ti, tj (torques)
+//   reverse CSR by j: rstart[j] .. rstart[j+1], rslot[r] = slot index (ascending i)
+#pragma once
+
+#include "gb2_sq.cuh"
+#include "gb2_internal.h"
+
+namespace gb2 {
+namespace sq {
+
+struct SqDev {
+    int n;
+    dbl4 *x, *v, *q, *L, *w, *f, *t, *shape, *inert, *xhold;
+    // list
+    int *start, *nbr, *flag, *state;
+    dbl4 *cp, *shear;
+    double2 *alpha;
+    dbl4 *pfi, *pti, *ptj;
+    int *rstart, *rslot;
+    // physics
+    double dt, skin, triggersq;
+    double Yeff, Geff, betaeff, mu;
+    // counters: iterations, solves, pairs solved, learned guesses used, learned guesses rejected
+    unsigned long long *cnt;
+    int *dflag;
+    // learned initial guess (null when off)
+    const float *mlp;
+};
+
+// FixNVEAsphereBase::initial_integrate, integration_scheme 1
+// (src/fix_nve_asphere_base.cpp:319-444), and Neighbor::check_distance
+__global__ void k_sq_initial(SqDev D, int check)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const double dtv = D.dt, dtf = 0.5 * D.dt * 1.0, dtf2 = 2.0 * dtf, dtq = 0.5 * dtv;
+    dbl4 x = D.x[i], v = D.v[i], q4 = D.q[i];
+    const dbl4 f = D.f[i], tq = D.t[i], in4 = D.inert[i], L4 = D.L[i];
+    double q[4] = {q4.x, q4.y, q4.z, q4.w};
+    const double in[3] = {in4.x, in4.y, in4.z};
+    double R[9], mbody[3], conjqm[4], tbody[3], fquat[4], wbody[3];
+    quat_to_mat(q, R);
+    const double dtfm = dtf / v.w;
+    v.x += dtfm * f.x;
+    v.y += dtfm * f.y;
+    v.z += dtfm * f.z;
+    x.x += dtv * v.x;
+    x.y += dtv * v.y;
+    x.z += dtv * v.z;
+    const double Lv[3] = {L4.x, L4.y, L4.z}, Tv[3] = {tq.x, tq.y, tq.z};
+    tmatvec(R, Lv, mbody);
+    quatvec(q, mbody, conjqm);
+    for (int k = 0; k < 4; k++) conjqm[k] *= 2.0;
+    tmatvec(R, Tv, tbody);
+    quatvec(q, tbody, fquat);
+    for (int k = 0; k < 4; k++) conjqm[k] += dtf2 * fquat[k];
+    no_squish_rotate(3, conjqm, q, in, dtq);
+    no_squish_rotate(2, conjqm, q, in, dtq);
+    no_squish_rotate(1, conjqm, q, in, dtv);
+    no_squish_rotate(2, conjqm, q, in, dtq);
+    no_squish_rotate(3, conjqm, q, in, dtq);
+    const double norm = 1.0 / sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (int k = 0; k < 4; k++) q[k] *= norm;
+    quat_to_mat(q, R);
+    invquatvec(q, conjqm, mbody);
+    for (int d = 0; d < 3; d++) mbody[d] *= 0.5;
+    for (int d = 0; d < 3; d++) wbody[d] = mbody[d] / in[d];
+    double Lo[3], wo[3];
+    matvec(R, mbody, Lo);
+    matvec(R, wbody, wo);
+    D.x[i] = x;
+    D.v[i] = v;
+    D.q[i] = dbl4{q[0], q[1], q[2], q[3]};
+    D.L[i] = dbl4{Lo[0], Lo[1], Lo[2], 0.0};
+    D.w[i] = dbl4{wo[0], wo[1], wo[2], 0.0};
+    if (check) {
+        const dbl4 h = D.xhold[i];
+        const double dx = x.x - h.x, dy = x.y - h.y, dz = x.z - h.z;
+        if (dx * dx + dy * dy + dz * dz > D.triggersq) *D.dflag = 1;
+    }
+}
+
+// FixNVEAsphereBase::final_integrate, integration_scheme 1 (:523-620)
+__global__ void k_sq_final(SqDev D)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const double dtf = 0.5 * D.dt * 1.0, dtf2 = dtf * 2.0;
+    dbl4 v = D.v[i];
+    const dbl4 q4 = D.q[i], f = D.f[i], tq = D.t[i], in4 = D.inert[i], L4 = D.L[i];
+    const double q[4] = {q4.x, q4.y, q4.z, q4.w};
+    const double in[3] = {in4.x, in4.y, in4.z};
+    double R[9], tbody[3], mbody[3], conjqm[4], fquat[4], wbody[3];
+    const double dtfm = dtf / v.w;
+    quat_to_mat(q, R);
+    v.x += dtfm * f.x;
+    v.y += dtfm * f.y;
+    v.z += dtfm * f.z;
+    const double Tv[3] = {tq.x, tq.y, tq.z}, Lv[3] = {L4.x, L4.y, L4.z};
+    tmatvec(R, Tv, tbody);
+    tmatvec(R, Lv, mbody);
+    quatvec(q, mbody, conjqm);
+    for (int k = 0; k < 4; k++) conjqm[k] *= 2.0;
+    quatvec(q, tbody, fquat);
+    for (int k = 0; k < 4; k++) conjqm[k] += dtf2 * fquat[k];
+    invquatvec(q, conjqm, mbody);
+    for (int d = 0; d < 3; d++) mbody[d] *= 0.5;
+    for (int d = 0; d < 3; d++) wbody[d] = mbody[d] / in[d];
+    double Lo[3], wo[3];
+    matvec(R, mbody, Lo);
+    matvec(R, wbody, wo);
+    D.v[i] = v;
+    D.L[i] = dbl4{Lo[0], Lo[1], Lo[2], 0.0};
+    D.w[i] = dbl4{wo[0], wo[1], wo[2], 0.0};
+}
+
+// omega from angular momentum (set-up)
+__global__ void k_sq_omega(SqDev D)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const dbl4 q4 = D.q[i], L4 = D.L[i], in4 = D.inert[i];
+    const double q[4] = {q4.x, q4.y, q4.z, q4.w}, Lv[3] = {L4.x, L4.y, L4.z};
+    double R[9], mb[3], wb[3], wo[3];
+    quat_to_mat(q, R);
+    tmatvec(R, Lv, mb);
+    wb[0] = mb[0] / in4.x;
+    wb[1] = mb[1] / in4.y;
+    wb[2] = mb[2] / in4.z;
+    matvec(R, wb, wo);
+    D.w[i] = dbl4{wo[0], wo[1], wo[2], 0.0};
+}
+
+// ------------------------------------------------------------------
+// learned initial guess: MLP 14 -> 64 -> 64 -> 64 -> 4 (ReLU), BF16 weights
+// and activations with FP32 accumulation, parameters packed as
+//   in_mean[14] in_std[14] out_mean[4] out_std[4]
+//   W1[64][14] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[4][64] b4[4]
+constexpr int kMlpIn = 14, kMlpH = 64, kMlpOut = 4;
+constexpr int kMlpOffW1 = 36, kMlpOffB1 = kMlpOffW1 + kMlpH * kMlpIn, kMlpOffW2 = kMlpOffB1 + kMlpH,
+              kMlpOffB2 = kMlpOffW2 + kMlpH * kMlpH, kMlpOffW3 = kMlpOffB2 + kMlpH,
+              kMlpOffB3 = kMlpOffW3 + kMlpH * kMlpH, kMlpOffW4 = kMlpOffB3 + kMlpH,
+              kMlpOffB4 = kMlpOffW4 + kMlpOut * kMlpH, kMlpSize = kMlpOffB4 + kMlpOut;
+
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// pair features in particle i's body frame, lengths over s = ri + rj
+// (ri = cbrt(abc)): centre of j (3), rotation vector of q_i^-1 q_j (3),
+// half-axes of i and j (6), (n - 2) / 6 of i and j (2)
+__device__ __forceinline__ double pair_features(const double *ci, const double *qi, const double *si, double ni,
+                                                const double *cj, const double *qj, const double *sj, double nj,
+                                                const double *Ri, float *feat)
+{
+    const double ri = cbrt(si[0] * si[1] * si[2]), rj = cbrt(sj[0] * sj[1] * sj[2]);
+    const double s = ri + rj, sinv = 1.0 / s;
+    const double d[3] = {cj[0] - ci[0], cj[1] - ci[1], cj[2] - ci[2]};
+    double dl[3];
+    tmatvec(Ri, d, dl);
+    // q_rel = conj(q_i) * q_j
+    const double a0 = qi[0], a1 = -qi[1], a2 = -qi[2], a3 = -qi[3];
+    double r0 = a0 * qj[0] - a1 * qj[1] - a2 * qj[2] - a3 * qj[3];
+    double r1 = a0 * qj[1] + qj[0] * a1 + a2 * qj[3] - a3 * qj[2];
+    double r2 = a0 * qj[2] + qj[0] * a2 + a3 * qj[1] - a1 * qj[3];
+    double r3 = a0 * qj[3] + qj[0] * a3 + a1 * qj[2] - a2 * qj[1];
+    if (r0 < 0) {
+        r0 = -r0;
+        r1 = -r1;
+        r2 = -r2;
+        r3 = -r3;
+    }
+    const double vn = sqrt(r1 * r1 + r2 * r2 + r3 * r3);
+    const double ang = 2.0 * atan2(vn, r0);
+    const double k = vn > 0 ? ang / vn : 2.0;
+    feat[0] = (float)(dl[0] * sinv);
+    feat[1] = (float)(dl[1] * sinv);
+    feat[2] = (float)(dl[2] * sinv);
+    feat[3] = (float)(k * r1);
+    feat[4] = (float)(k * r2);
+    feat[5] = (float)(k * r3);
+    for (int c = 0; c < 3; c++) {
+        feat[6 + c] = (float)(si[c] * sinv);
+        feat[9 + c] = (float)(sj[c] * sinv);
+    }
+    feat[12] = (float)((ni - 2.0) / 6.0);
+    feat[13] = (float)((nj - 2.0) / 6.0);
+    return s;
+}
+
+// forward pass of one sample (the same BF16 rounding points as the training
+// kernels): out = de-normalised (point in i's frame / s, mu)
+__device__ __forceinline__ void mlp_infer(const float *__restrict__ P, const float *feat, float *out)
+{
+    float x[kMlpH], h[kMlpH];
+    for (int c = 0; c < kMlpIn; c++) x[c] = bf16_round((feat[c] - __ldg(&P[c])) / __ldg(&P[kMlpIn + c]));
+    for (int o = 0; o < kMlpH; o++) {
+        float acc = 0.f;
+        for (int c = 0; c < kMlpIn; c++) acc += __ldg(&P[kMlpOffW1 + o * kMlpIn + c]) * x[c];
+        h[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB1 + o]), 0.f));
+    }
+    for (int o = 0; o < kMlpH; o++) {
+        float acc = 0.f;
+        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW2 + o * kMlpH + c]) * h[c];
+        x[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB2 + o]), 0.f));
+    }
+    for (int o = 0; o < kMlpH; o++) {
+        float acc = 0.f;
+        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW3 + o * kMlpH + c]) * x[c];
+        h[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB3 + o]), 0.f));
+    }
+    for (int o = 0; o < kMlpOut; o++) {
+        float acc = 0.f;
+        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW4 + o * kMlpH + c]) * h[c];
+        out[o] = (acc + __ldg(&P[kMlpOffB4 + o])) * __ldg(&P[2 * kMlpIn + kMlpOut + o]) + __ldg(&P[2 * kMlpIn + o]);
+    }
+}
+
+// Contact point of a pair without a previous point: the learned guess, one
+// Newton solve, and the homotopy as the fallback when that solve does not
+// reach the merit tolerance.  used: 1 learned guess accepted, -1 rejected, 0 off.
+__device__ __forceinline__ void first_contact(const float *mlp, const double *ci, const double *qi, const double *si,
+                                              double ni, const double *cj, const double *qj, const double *sj,
+                                              double nj, Newton &o, int &iters, int &solves, int &used)
+{
+    used = 0;
+    if (mlp) {
+        double Ri[9];
+        quat_to_mat(qi, Ri);
+        float feat[kMlpIn], out[kMlpOut];
+        const double s = pair_features(ci, qi, si, ni, cj, qj, sj, nj, Ri, feat);
+        mlp_infer(mlp, feat, out);
+        const double pl[3] = {out[0] * s, out[1] * s, out[2] * s};
+        double g[3];
+        matvec(Ri, pl, g);
+        for (int k = 0; k < 3; k++) g[k] += ci[k];
+        int it1, sv1;
+        contact_point(ci, qi, si, ni, cj, qj, sj, nj, 1, g, true, (double)fabsf(out[3]), o, it1, sv1);
+        if (!o.fail && o.merit < 1e-10) {
+            iters = it1;
+            solves = sv1;
+            used = 1;
+            return;
+        }
+        int it2, sv2;
+        contact_point(ci, qi, si, ni, cj, qj, sj, nj, 0, nullptr, false, 0.0, o, it2, sv2);
+        iters = it1 + it2;
+        solves = sv1 + sv2;
+        used = -1;
+        return;
+    }
+    contact_point(ci, qi, si, ni, cj, qj, sj, nj, 0, nullptr, false, 0.0, o, iters, solves);
+}
+
+// ------------------------------------------------------------------
+// pair pass: one thread per half-list slot (PairGran::compute with the
+// superquadric surface model, src/pair_gran_base.h:255-430,
+// src/surface_model_superquadric.h:108-205, non-spherical Hertz/history)
+__global__ void k_sq_pair(SqDev D, const int *__restrict__ own, int nslots, int shearupdate)
+{
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= nslots) return;
+    const int i = own[sl], j = D.nbr[sl];
+    const dbl4 xi4 = D.x[i], xj4 = D.x[j];
+    dbl4 fo{0, 0, 0, 0}, ti{0, 0, 0, 0}, tj{0, 0, 0, 0};
+    const double dx = xi4.x - xj4.x, dy = xi4.y - xj4.y, dz = xi4.z - xj4.z;
+    const double rsq = dx * dx + dy * dy + dz * dz, radsum = xi4.w + xj4.w;
+    if (rsq < radsum * radsum) {
+        const dbl4 qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
+        const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
+        const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
+        const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
+        int state = D.state[sl];
+        double Ri[9], Rj[9];
+        quat_to_mat(qi, Ri);
+        quat_to_mat(qj, Rj);
+        const bool obb = state == INTERSECT ? true : obb_intersect(ci, Ri, si, cj, Rj, sj);
+        bool contact = false;
+        if (obb) {
+            Newton o;
+            int it = 0, sv = 0, used = 0;
+            if (state == FAR) {
+                first_contact(D.mlp, ci, qi, si, si4.w, cj, qj, sj, sj4.w, o, it, sv, used);
+            } else {
+                // previous point advanced with the mass-weighted contact-point velocity
+                const dbl4 cp4 = D.cp[sl], wi4 = D.w[i], wj4 = D.w[j], vi4 = D.v[i], vj4 = D.v[j];
+                const double cp[3] = {cp4.x, cp4.y, cp4.z}, wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
+                double xci[3], xcj[3], vri[3], vrj[3], est[3];
+                for (int k = 0; k < 3; k++) {
+                    xci[k] = cp[k] - ci[k];
+                    xcj[k] = cp[k] - cj[k];
+                }
+                cross3(wi, xci, vri);
+                cross3(wj, xcj, vrj);
+                const double mi = vi4.w, mj = vj4.w;
+                const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
+                for (int k = 0; k < 3; k++) {
+                    const double a = vi[k] + vri[k], b = vj[k] + vrj[k];
+                    est[k] = cp[k] + (a * mi + b * mj) / (mi + mj) * D.dt;
+                }
+                contact_point(ci, qi, si, si4.w, cj, qj, sj, sj4.w, 1, est, false, 0.0, o, it, sv);
+            }
+            atomicAdd(&D.cnt[0], (unsigned long long)it);
+            atomicAdd(&D.cnt[1], (unsigned long long)sv);
+            atomicAdd(&D.cnt[2], 1ull);
+            if (used == 1) atomicAdd(&D.cnt[3], 1ull);
+            if (used == -1) atomicAdd(&D.cnt[4], 1ull);
+            D.cp[sl] = dbl4{o.point[0], o.point[1], o.point[2], 0.0};
+            contact = fmax(o.fi, o.fj) < 0.0;
+            if (contact) {
+                double en[3] = {o.gB[0] - o.gA[0], o.gB[1] - o.gA[1], o.gB[2] - o.gA[2]};
+                const double nrm = sqrt(en[0] * en[0] + en[1] * en[1] + en[2] * en[2]);
+                const double inv = nrm == 0. ? 0. : 1. / nrm;
+                for (int k = 0; k < 3; k++) en[k] *= inv;
+                Body A, B;
+                body_set(A, ci, qi, si, si4.w);
+                body_set(B, cj, qj, sj, sj4.w);
+                double2 al = D.alpha[sl];
+                const double ne[3] = {-en[0], -en[1], -en[2]};
+                double cpa[3], cpb[3];
+                al.x = line_intersection(A, o.point, ne, al.x, cpa);
+                al.y = line_intersection(B, o.point, en, al.y, cpb);
+                D.alpha[sl] = al;
+                const double deltan = fabs(al.x) + fabs(al.y);
+                state = INTERSECT;
+                // forces: non-spherical kinematics, Hertz, tangential history
+                const dbl4 vi4 = D.v[i], vj4 = D.v[j], wi4 = D.w[i], wj4 = D.w[j], ii4 = D.inert[i], ij4 = D.inert[j];
+                const double wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
+                double xci[3], xcj[3], vri[3], vrj[3], vrel[3];
+                for (int k = 0; k < 3; k++) {
+                    xci[k] = o.point[k] - ci[k];
+                    xcj[k] = o.point[k] - cj[k];
+                }
+                cross3(wi, xci, vri);
+                cross3(wj, xcj, vrj);
+                const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
+                for (int k = 0; k < 3; k++) vrel[k] = vi[k] - vj[k] + (vri[k] - vrj[k]);
+                const double vn = dot3(vrel, en);
+                const double vtr[3] = {vrel[0] - vn * en[0], vrel[1] - vn * en[1], vrel[2] - vn * en[2]};
+                const double radi = ii4.w, radj = ij4.w, mi = vi4.w, mj = vj4.w, meff = mi * mj / (mi + mj);
+                const double reff = radi * radj / (radi + radj);
+                const double sqrtval = sqrt(reff * deltan);
+                const double Sn = 2. * D.Yeff * sqrtval, St = 8. * D.Geff * sqrtval;
+                const double kn = 4. / 3. * D.Yeff * sqrtval, kt = St;
+                const double c56 = 0.91287092917527685576161630466800355658790782499663875;
+                const double gamman = -2. * c56 * D.betaeff * sqrt(Sn * meff);
+                const double gammat = -2. * c56 * D.betaeff * sqrt(St * meff);
+                const double Fn = -gamman * vn + kn * deltan;
+                const double Fi[3] = {Fn * en[0], Fn * en[1], Fn * en[2]}, Fnj[3] = {-Fi[0], -Fi[1], -Fi[2]};
+                double Ti[3], Tj[3];
+                cross3(xci, Fi, Ti);
+                cross3(xcj, Fnj, Tj);
+                dbl4 sh4 = D.shear[sl];
+                double sh[3] = {sh4.x, sh4.y, sh4.z};
+                if (shearupdate) {
+                    for (int k = 0; k < 3; k++) sh[k] += vtr[k] * D.dt;
+                    const double rsht = dot3(sh, en);
+                    for (int k = 0; k < 3; k++) sh[k] -= rsht * en[k];
+                }
+                const double shrmag = sqrt(dot3(sh, sh));
+                double Ft[3] = {-(kt * sh[0]), -(kt * sh[1]), -(kt * sh[2])};
+                const double Ft_shear = kt * shrmag, Ft_friction = D.mu * fabs(Fn);
+                if (Ft_shear > Ft_friction) {
+                    if (shrmag != 0.0) {
+                        const double ratio = Ft_friction / Ft_shear;
+                        for (int k = 0; k < 3; k++) Ft[k] *= ratio;
+                        if (shearupdate)
+                            for (int k = 0; k < 3; k++) sh[k] = -Ft[k] / kt;
+                    } else {
+                        Ft[0] = Ft[1] = Ft[2] = 0.0;
+                    }
+                } else {
+                    for (int k = 0; k < 3; k++) Ft[k] -= gammat * vtr[k];
+                }
+                D.shear[sl] = dbl4{sh[0], sh[1], sh[2], 0.0};
+                double tti[3], ttj[3];
+                const double Ftj[3] = {-Ft[0], -Ft[1], -Ft[2]};
+                cross3(xci, Ft, tti);
+                cross3(xcj, Ftj, ttj);
+                fo = dbl4{Fi[0] + Ft[0], Fi[1] + Ft[1], Fi[2] + Ft[2], 1.0};
+                ti = dbl4{Ti[0] + tti[0], Ti[1] + tti[1], Ti[2] + tti[2], 0.0};
+                tj = dbl4{Tj[0] + ttj[0], Tj[1] + ttj[1], Tj[2] + ttj[2], 0.0};
+                D.flag[sl] |= 5;
+            } else {
+                state = CLOSE;
+            }
+        } else {
+            state = FAR;
+        }
+        D.state[sl] = state;
+    }
+    D.pfi[sl] = fo;
+    D.pti[sl] = ti;
+    D.ptj[sl] = tj;
+}
+
+// per-atom sums in the reference's order: slots where the atom is the j
+// side (ascending i), then its own slots
+__global__ void k_sq_sum(SqDev D)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.n) return;
+    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+    for (int r = D.rstart[k]; r < D.rstart[k + 1]; r++) {
+        const int sl = D.rslot[r];
+        const dbl4 f = D.pfi[sl];
+        if (f.w == 0.0) continue;
+        const dbl4 t = D.ptj[sl];
+        F[0] += -f.x;
+        F[1] += -f.y;
+        F[2] += -f.z;
+        T[0] += t.x;
+        T[1] += t.y;
+        T[2] += t.z;
+    }
+    for (int sl = D.start[k]; sl < D.start[k + 1]; sl++) {
+        const dbl4 f = D.pfi[sl];
+        if (f.w == 0.0) continue;
+        const dbl4 t = D.pti[sl];
+        F[0] += f.x;
+        F[1] += f.y;
+        F[2] += f.z;
+        T[0] += t.x;
+        T[1] += t.y;
+        T[2] += t.z;
+    }
+    D.f[k] = dbl4{F[0], F[1], F[2], 0.0};
+    D.t[k] = dbl4{T[0], T[1], T[2], 0.0};
+}
+
+}  // namespace sq
+}  // namespace gb2

@@ -318,3 +318,113 @@ class Engine:
                                              ca.ctypes.data_as(U8), _ip(ob)))
         n = nt.value
         return ea[:3 * n].reshape(n, 3), ca[:3 * n].reshape(n, 3), ob[:n]
+
+
+# ---------------------------------------------------------------- superquadrics
+
+SQ_MLP_SIZE = 9576   # GB2_SQ_MLP_SIZE
+
+
+class SqParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("skin", ctypes.c_double), ("youngs", ctypes.c_double),
+                ("poisson", ctypes.c_double), ("restitution", ctypes.c_double), ("friction", ctypes.c_double),
+                ("device", ctypes.c_int)]
+
+
+def _sq_lib():
+    L = lib()
+    if not getattr(L, "_sq_ready", False):
+        vp = ctypes.c_void_p
+        L.gb2_sq_create.argtypes = [ctypes.POINTER(SqParams), ctypes.POINTER(vp)]
+        L.gb2_sq_destroy.argtypes = [vp]
+        L.gb2_sq_upload.argtypes = [vp, ctypes.c_int] + [D] * 9
+        L.gb2_sq_set_learned_guess.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+        L.gb2_sq_setup.argtypes = [vp]
+        L.gb2_sq_run.argtypes = [vp, ctypes.c_int]
+        L.gb2_sq_run_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.gb2_sq_download.argtypes = [vp, ctypes.c_int] + [D] * 7
+        L.gb2_sq_download_pairs.argtypes = [vp, ctypes.c_int, I, I, I, I, D, D]
+        L.gb2_sq_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.gb2_sq_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L._sq_ready = True
+    return L
+
+
+class SqEngine:
+    """Device-resident superquadric simulation (one gb2_sq_ctx)."""
+
+    def __init__(self, sc, device=0, learned=None):
+        L = _sq_lib()
+        self.L = L
+        p = SqParams(sc["dt"], sc["skin"], sc["youngs"], sc["poisson"], sc["restitution"], sc["friction"], device)
+        self.h = ctypes.c_void_p()
+        rc = L.gb2_sq_create(ctypes.byref(p), ctypes.byref(self.h))
+        if rc != 0:
+            raise GB2Error("gb2_sq_create failed (%d)" % rc)
+        a = sc["atoms"]
+        self.n = len(a["rmass"])
+        keep = [np.ascontiguousarray(a[k], dtype=np.float64) for k in
+                ("x", "v", "quat", "angmom", "shape", "blockiness", "rmass", "inertia", "volume")]
+        self._check(L.gb2_sq_upload(self.h, self.n, *[_dp(k) for k in keep]))
+        if learned is not None:
+            self.set_learned_guess(learned)
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.L.gb2_sq_last_error(self.h, buf, 512)
+            raise GB2Error("granb200 sq error %d: %s" % (rc, buf.value.decode()))
+
+    def close(self):
+        if self.h:
+            self.L.gb2_sq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_learned_guess(self, params):
+        if params is None:
+            self._check(self.L.gb2_sq_set_learned_guess(self.h, None, 0))
+            return
+        self._w = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.L.gb2_sq_set_learned_guess(self.h, self._w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                    len(self._w)))
+
+    def setup(self):
+        self._check(self.L.gb2_sq_setup(self.h))
+
+    def run(self, n):
+        self._check(self.L.gb2_sq_run(self.h, n))
+
+    def run_timed(self, n):
+        ms = ctypes.c_double()
+        self._check(self.L.gb2_sq_run_timed(self.h, n, ctypes.byref(ms)))
+        return ms.value
+
+    def atoms(self):
+        n = self.n
+        out = {k: np.zeros((n, 3)) for k in ("x", "v", "angmom", "omega", "f", "torque")}
+        out["quat"] = np.zeros((n, 4))
+        self._check(self.L.gb2_sq_download(self.h, n, _dp(out["x"]), _dp(out["v"]), _dp(out["quat"]),
+                                           _dp(out["angmom"]), _dp(out["omega"]), _dp(out["f"]), _dp(out["torque"])))
+        return out
+
+    def pairs(self):
+        cnt = ctypes.c_int()
+        self._check(self.L.gb2_sq_download_pairs(self.h, 0, ctypes.byref(cnt), None, None, None, None, None))
+        n = cnt.value
+        ti, tj, st = (np.zeros(n, dtype=np.int32) for _ in range(3))
+        cp, sh = np.zeros((n, 3)), np.zeros((n, 3))
+        self._check(self.L.gb2_sq_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(st), _dp(cp),
+                                                 _dp(sh)))
+        return {"tag_i": ti, "tag_j": tj, "state": st, "cp": cp, "shear": sh}
+
+    def counters(self):
+        out = (ctypes.c_longlong * 7)()
+        self._check(self.L.gb2_sq_counters(self.h, out))
+        keys = ("iters", "solves", "pairs_solved", "learned_used", "learned_rejected", "nbuilds", "npairs")
+        return dict(zip(keys, [int(v) for v in out]))
