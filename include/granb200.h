@@ -238,6 +238,37 @@ int gb2_sq_download_pairs(gb2_sq_ctx *ctx, int cap, int *n, int *tag_i, int *tag
 int gb2_sq_counters(gb2_sq_ctx *ctx, long long *out);
 int gb2_sq_last_error(gb2_sq_ctx *ctx, char *buf, int len);
 
+/* --------------------------------------------------------------------
+   Training of the learned initial guess (no counterpart in the reference).
+   Samples are random superquadric pairs near contact (half-axes U(1, 2) mm,
+   blockiness U(2, 8), random orientations, oriented boxes intersecting),
+   labelled on the device by the plain solver (homotopy from spheres); the
+   network is trained on the device by BF16 tensor-core forward/backward
+   kernels with FP32 accumulation and Adam.
+   -------------------------------------------------------------------- */
+typedef struct gb2_mlp_ctx gb2_mlp_ctx;
+int gb2_mlp_create(int device, gb2_mlp_ctx **out);
+int gb2_mlp_destroy(gb2_mlp_ctx *ctx);
+/* n samples from seed; out[3] = valid samples, mean Newton iterations and
+   mean solves per sample of the plain solver */
+int gb2_mlp_make_data(gb2_mlp_ctx *ctx, long n, unsigned long long seed, double *out);
+/* normalisation statistics from the data, He-uniform weights */
+int gb2_mlp_init(gb2_mlp_ctx *ctx, unsigned long long seed);
+/* loss[2] = first mini-batch, mean of the last epoch */
+int gb2_mlp_train(gb2_mlp_ctx *ctx, int epochs, int batch, float lr, float *loss);
+int gb2_mlp_get_params(gb2_mlp_ctx *ctx, float *out, int n);
+int gb2_mlp_set_params(gb2_mlp_ctx *ctx, const float *in, int n);
+/* one forward + backward pass over nrows samples of 22 floats (features
+   0..13, targets 14..17): loss and gradient (GB2_SQ_MLP_SIZE floats) */
+int gb2_mlp_grad(gb2_mlp_ctx *ctx, int nrows, const float *samples, float *loss, float *grad);
+/* learned guess vs plain method on n fresh pairs: stats[9] = pairs, plain
+   iterations, plain solves, learned iterations, learned solves, learned
+   guesses accepted, plain failures, learned failures, pairs whose two
+   solutions differ by more than 1e-4 of the smallest half-axis; *maxdiff =
+   largest such difference over the smallest half-axis */
+int gb2_mlp_evaluate(gb2_mlp_ctx *ctx, long n, unsigned long long seed, long long *stats, double *maxdiff);
+int gb2_mlp_last_error(gb2_mlp_ctx *ctx, char *buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <random>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -19,7 +20,7 @@
 #include <vector>
 
 #include "../../include/granb200.h"
-#include "gb2_sq_kernels.cuh"
+#include "gb2_mlp.cuh"
 
 using namespace gb2;
 using namespace gb2::sq;
@@ -698,6 +699,269 @@ int gb2_sq_counters(gb2_sq_ctx *c, long long *out)
 }
 
 int gb2_sq_last_error(gb2_sq_ctx *c, char *buf, int len)
+{
+    if (!c || !buf || len <= 0) return GB2_ERR_ARG;
+    snprintf(buf, len, "%s", c->err.c_str());
+    return 0;
+}
+
+}  // extern "C"
+
+// ==================================================================== learned initial guess: training
+
+namespace {
+
+__global__ void k_mlp_stats(const float *data, const int *idx, long n, double *acc)
+{
+    __shared__ double s[2 * 18];
+    for (int e = threadIdx.x; e < 36; e += blockDim.x) s[e] = 0.0;
+    __syncthreads();
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        const float *o = data + (long)idx[k] * kMlpSample;
+        for (int c = 0; c < 18; c++) {
+            const double v = o[c];
+            atomicAdd(&s[c], v);
+            atomicAdd(&s[18 + c], v * v);
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 36; e += blockDim.x) atomicAdd(&acc[e], s[e]);
+}
+
+}  // namespace
+
+struct gb2_mlp_ctx {
+    std::string err;
+    cudaStream_t st = nullptr;
+    Buf<float> data, P, G, m, v, loss;
+    Buf<int> idx;
+    Buf<double> acc, maxd;
+    Buf<long long> stats;
+    std::vector<int> hidx;
+    long nsamples = 0, nvalid = 0;
+    long adam_t = 0;
+    std::mt19937_64 rng{12345};
+};
+
+namespace {
+int mlp_err(gb2_mlp_ctx *c, int code, const char *msg)
+{
+    c->err = msg;
+    return code;
+}
+#define MLCK(call)                                                                                                \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) return mlp_err(c, GB2_ERR_CUDA, cudaGetErrorString(e_));                          \
+    } while (0)
+}  // namespace
+
+extern "C" {
+
+int gb2_mlp_create(int device, gb2_mlp_ctx **out)
+{
+    if (!out) return GB2_ERR_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return GB2_ERR_CUDA;
+    gb2_mlp_ctx *c = new gb2_mlp_ctx();
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess || c->P.alloc(kMlpSize) ||
+        c->G.alloc(kMlpSize) || c->m.alloc(kMlpSize) || c->v.alloc(kMlpSize) || c->loss.alloc(1) ||
+        c->acc.alloc(36) || c->maxd.alloc(1) || c->stats.alloc(16) ||
+        cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem)) !=
+            cudaSuccess) {
+        delete c;
+        return GB2_ERR_CUDA;
+    }
+    *out = c;
+    return 0;
+}
+
+int gb2_mlp_destroy(gb2_mlp_ctx *c)
+{
+    if (!c) return 0;
+    cudaStreamSynchronize(c->st);
+    cudaStream_t st = c->st;
+    delete c;
+    if (st) cudaStreamDestroy(st);
+    return 0;
+}
+
+// n random near-contact pairs labelled by the plain solver; out[0] valid
+// samples, out[1] mean Newton iterations, out[2] mean solves per sample
+int gb2_mlp_make_data(gb2_mlp_ctx *c, long n, unsigned long long seed, double *out)
+{
+    if (!c || n <= 0 || !out) return GB2_ERR_ARG;
+    MLCK(c->data.alloc((size_t)n * kMlpSample));
+    k_mlp_make<<<nb(n), kB, 0, c->st>>>(seed, n, c->data.p);
+    MLCK(cudaGetLastError());
+    std::vector<float> h((size_t)n * kMlpSample);
+    MLCK(cudaMemcpyAsync(h.data(), c->data.p, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    c->hidx.clear();
+    double it = 0, sv = 0;
+    for (long k = 0; k < n; k++) {
+        const float *o = &h[(size_t)k * kMlpSample];
+        if (o[21] != 1.f) continue;
+        c->hidx.push_back((int)k);
+        it += o[18];
+        sv += o[19];
+    }
+    c->nsamples = n;
+    c->nvalid = (long)c->hidx.size();
+    if (c->nvalid == 0) return mlp_err(c, GB2_ERR_STATE, "no valid samples");
+    MLCK(c->idx.alloc(c->nvalid));
+    MLCK(cudaMemcpyAsync(c->idx.p, c->hidx.data(), sizeof(int) * c->nvalid, cudaMemcpyHostToDevice, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    out[0] = (double)c->nvalid;
+    out[1] = it / c->nvalid;
+    out[2] = sv / c->nvalid;
+    return 0;
+}
+
+// normalisation statistics from the data, He-uniform weights, zero biases
+int gb2_mlp_init(gb2_mlp_ctx *c, unsigned long long seed)
+{
+    if (!c || c->nvalid == 0) return GB2_ERR_STATE;
+    MLCK(cudaMemsetAsync(c->acc.p, 0, sizeof(double) * 36, c->st));
+    k_mlp_stats<<<nb(c->nvalid), kB, 0, c->st>>>(c->data.p, c->idx.p, c->nvalid, c->acc.p);
+    MLCK(cudaGetLastError());
+    double acc[36];
+    MLCK(cudaMemcpyAsync(acc, c->acc.p, sizeof acc, cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    std::vector<float> P(kMlpSize, 0.f);
+    for (int k = 0; k < 18; k++) {
+        const double mean = acc[k] / c->nvalid;
+        const double var = std::max(acc[18 + k] / c->nvalid - mean * mean, 0.0);
+        const double sd = std::sqrt(var) > 1e-6 ? std::sqrt(var) : 1.0;
+        if (k < kMlpIn) {
+            P[k] = (float)mean;
+            P[kMlpIn + k] = (float)sd;
+        } else {
+            P[2 * kMlpIn + (k - kMlpIn)] = (float)mean;
+            P[2 * kMlpIn + kMlpOut + (k - kMlpIn)] = (float)sd;
+        }
+    }
+    std::mt19937_64 g(seed);
+    auto fill = [&](int off, int nout, int nin) {
+        const float lim = std::sqrt(6.0f / nin);
+        std::uniform_real_distribution<float> U(-lim, lim);
+        for (int e = 0; e < nout * nin; e++) P[off + e] = U(g);
+    };
+    fill(kMlpOffW1, kMlpH, kMlpIn);
+    fill(kMlpOffW2, kMlpH, kMlpH);
+    fill(kMlpOffW3, kMlpH, kMlpH);
+    fill(kMlpOffW4, kMlpOut, kMlpH);
+    MLCK(cudaMemcpyAsync(c->P.p, P.data(), sizeof(float) * kMlpSize, cudaMemcpyHostToDevice, c->st));
+    MLCK(cudaMemsetAsync(c->m.p, 0, sizeof(float) * kMlpSize, c->st));
+    MLCK(cudaMemsetAsync(c->v.p, 0, sizeof(float) * kMlpSize, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    c->adam_t = 0;
+    c->rng.seed(seed ^ 0x5DEECE66Dull);
+    return 0;
+}
+
+// epochs of shuffled mini-batches with Adam; loss[0] = first batch, loss[1] =
+// mean over the last epoch
+int gb2_mlp_train(gb2_mlp_ctx *c, int epochs, int batch, float lr, float *loss)
+{
+    if (!c || epochs <= 0 || batch <= 0 || !loss || c->nvalid == 0) return GB2_ERR_ARG;
+    const int rows_per_cta = kWarps * kTile;
+    double last = 0;
+    long nlast = 0;
+    loss[0] = -1.f;
+    for (int ep = 0; ep < epochs; ep++) {
+        std::shuffle(c->hidx.begin(), c->hidx.end(), c->rng);
+        MLCK(cudaMemcpyAsync(c->idx.p, c->hidx.data(), sizeof(int) * c->nvalid, cudaMemcpyHostToDevice, c->st));
+        std::vector<float> losses;
+        for (long b0 = 0; b0 + batch <= c->nvalid; b0 += batch) {
+            MLCK(cudaMemsetAsync(c->G.p, 0, sizeof(float) * kMlpSize, c->st));
+            MLCK(cudaMemsetAsync(c->loss.p, 0, sizeof(float), c->st));
+            const int ncta = (batch + rows_per_cta - 1) / rows_per_cta;
+            k_mlp_fwd_bwd<<<ncta, 128, sizeof(MlpSmem), c->st>>>(c->P.p, c->data.p, c->idx.p + b0, batch, c->G.p,
+                                                                   c->loss.p);
+            MLCK(cudaGetLastError());
+            c->adam_t++;
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float c1 = 1.f - std::pow(b1, (float)c->adam_t), c2 = 1.f - std::pow(b2, (float)c->adam_t);
+            k_mlp_adam<<<nb(kMlpSize - kMlpOffW1), kB, 0, c->st>>>(c->P.p, c->G.p, c->m.p, c->v.p, kMlpSize, lr, b1,
+                                                                  b2, 1e-8f, c1, c2);
+            MLCK(cudaGetLastError());
+            if (ep == epochs - 1 || loss[0] < 0) {
+                float l;
+                MLCK(cudaMemcpyAsync(&l, c->loss.p, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+                MLCK(cudaStreamSynchronize(c->st));
+                if (loss[0] < 0) loss[0] = l;
+                if (ep == epochs - 1) {
+                    last += l;
+                    nlast++;
+                }
+            }
+        }
+    }
+    MLCK(cudaStreamSynchronize(c->st));
+    loss[1] = nlast ? (float)(last / nlast) : loss[0];
+    return 0;
+}
+
+int gb2_mlp_get_params(gb2_mlp_ctx *c, float *out, int n)
+{
+    if (!c || !out || n != kMlpSize) return GB2_ERR_ARG;
+    MLCK(cudaMemcpyAsync(out, c->P.p, sizeof(float) * kMlpSize, cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int gb2_mlp_set_params(gb2_mlp_ctx *c, const float *in, int n)
+{
+    if (!c || !in || n != kMlpSize) return GB2_ERR_ARG;
+    MLCK(cudaMemcpyAsync(c->P.p, in, sizeof(float) * kMlpSize, cudaMemcpyHostToDevice, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// one forward + backward pass over caller-given samples (kMlpSample floats
+// each: features 0..13, targets 14..17): loss and the full gradient
+int gb2_mlp_grad(gb2_mlp_ctx *c, int nrows, const float *samples, float *loss, float *grad)
+{
+    if (!c || nrows <= 0 || !samples || !loss || !grad) return GB2_ERR_ARG;
+    Buf<float> d;
+    Buf<int> ix;
+    MLCK(d.alloc((size_t)nrows * kMlpSample));
+    MLCK(ix.alloc(nrows));
+    std::vector<int> h(nrows);
+    for (int k = 0; k < nrows; k++) h[k] = k;
+    MLCK(cudaMemcpyAsync(d.p, samples, sizeof(float) * nrows * kMlpSample, cudaMemcpyHostToDevice, c->st));
+    MLCK(cudaMemcpyAsync(ix.p, h.data(), sizeof(int) * nrows, cudaMemcpyHostToDevice, c->st));
+    MLCK(cudaMemsetAsync(c->G.p, 0, sizeof(float) * kMlpSize, c->st));
+    MLCK(cudaMemsetAsync(c->loss.p, 0, sizeof(float), c->st));
+    const int ncta = (nrows + kWarps * kTile - 1) / (kWarps * kTile);
+    k_mlp_fwd_bwd<<<ncta, 128, sizeof(MlpSmem), c->st>>>(c->P.p, d.p, ix.p, nrows, c->G.p, c->loss.p);
+    MLCK(cudaGetLastError());
+    MLCK(cudaMemcpyAsync(grad, c->G.p, sizeof(float) * kMlpSize, cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaMemcpyAsync(loss, c->loss.p, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// learned guess against the plain method on n fresh pairs; stats[9]:
+// pairs, plain iterations, plain solves, learned iterations, learned solves,
+// learned guesses accepted, plain failures, learned failures, converged more
+// than 1e-4 of the size apart; maxdiff = largest point difference / smallest half-axis
+int gb2_mlp_evaluate(gb2_mlp_ctx *c, long n, unsigned long long seed, long long *stats, double *maxdiff)
+{
+    if (!c || n <= 0 || !stats || !maxdiff) return GB2_ERR_ARG;
+    MLCK(cudaMemsetAsync(c->stats.p, 0, sizeof(long long) * 16, c->st));
+    MLCK(cudaMemsetAsync(c->maxd.p, 0, sizeof(double), c->st));
+    k_mlp_eval<<<nb(n), kB, 0, c->st>>>(seed, n, c->P.p, c->stats.p, c->maxd.p);
+    MLCK(cudaGetLastError());
+    MLCK(cudaMemcpyAsync(stats, c->stats.p, sizeof(long long) * 9, cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaMemcpyAsync(maxdiff, c->maxd.p, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int gb2_mlp_last_error(gb2_mlp_ctx *c, char *buf, int len)
 {
     if (!c || !buf || len <= 0) return GB2_ERR_ARG;
     snprintf(buf, len, "%s", c->err.c_str());

@@ -428,3 +428,86 @@ class SqEngine:
         self._check(self.L.gb2_sq_counters(self.h, out))
         keys = ("iters", "solves", "pairs_solved", "learned_used", "learned_rejected", "nbuilds", "npairs")
         return dict(zip(keys, [int(v) for v in out]))
+
+
+class MlpTrainer:
+    """Device-side training of the learned initial guess (one gb2_mlp_ctx)."""
+
+    def __init__(self, device=0):
+        L = lib()
+        if not getattr(L, "_mlp_ready", False):
+            vp = ctypes.c_void_p
+            F = ctypes.POINTER(ctypes.c_float)
+            L.gb2_mlp_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+            L.gb2_mlp_destroy.argtypes = [vp]
+            L.gb2_mlp_make_data.argtypes = [vp, ctypes.c_long, ctypes.c_ulonglong, D]
+            L.gb2_mlp_init.argtypes = [vp, ctypes.c_ulonglong]
+            L.gb2_mlp_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, F]
+            L.gb2_mlp_get_params.argtypes = [vp, F, ctypes.c_int]
+            L.gb2_mlp_set_params.argtypes = [vp, F, ctypes.c_int]
+            L.gb2_mlp_grad.argtypes = [vp, ctypes.c_int, F, F, F]
+            L.gb2_mlp_evaluate.argtypes = [vp, ctypes.c_long, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong), D]
+            L.gb2_mlp_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+            L._mlp_ready = True
+        self.L = L
+        self.h = ctypes.c_void_p()
+        rc = L.gb2_mlp_create(device, ctypes.byref(self.h))
+        if rc != 0:
+            raise GB2Error("gb2_mlp_create failed (%d)" % rc)
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.L.gb2_mlp_last_error(self.h, buf, 512)
+            raise GB2Error("granb200 mlp error %d: %s" % (rc, buf.value.decode()))
+
+    def close(self):
+        if self.h:
+            self.L.gb2_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def make_data(self, n, seed):
+        out = np.zeros(3)
+        self._check(self.L.gb2_mlp_make_data(self.h, n, seed, _dp(out)))
+        return {"valid": int(out[0]), "plain_iters": float(out[1]), "plain_solves": float(out[2])}
+
+    def init(self, seed):
+        self._check(self.L.gb2_mlp_init(self.h, seed))
+
+    def train(self, epochs, batch, lr):
+        loss = np.zeros(2, dtype=np.float32)
+        self._check(self.L.gb2_mlp_train(self.h, epochs, batch, lr, loss.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return float(loss[0]), float(loss[1])
+
+    def params(self):
+        p = np.zeros(SQ_MLP_SIZE, dtype=np.float32)
+        self._check(self.L.gb2_mlp_get_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), SQ_MLP_SIZE))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self.L.gb2_mlp_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), SQ_MLP_SIZE))
+
+    def grad(self, samples):
+        s = np.ascontiguousarray(samples, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.zeros(SQ_MLP_SIZE, dtype=np.float32)
+        F = ctypes.POINTER(ctypes.c_float)
+        self._check(self.L.gb2_mlp_grad(self.h, len(s), s.ctypes.data_as(F), loss.ctypes.data_as(F), g.ctypes.data_as(F)))
+        return float(loss[0]), g
+
+    def evaluate(self, n, seed):
+        st = (ctypes.c_longlong * 9)()
+        md = ctypes.c_double()
+        self._check(self.L.gb2_mlp_evaluate(self.h, n, seed, st, ctypes.byref(md)))
+        keys = ("pairs", "plain_iters", "plain_solves", "learned_iters", "learned_solves", "learned_accepted",
+                "plain_fail", "learned_fail", "differ")
+        out = dict(zip(keys, [int(v) for v in st]))
+        out["maxdiff"] = md.value
+        return out
