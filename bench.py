@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
-    ap.add_argument("--workload", default="hopper", choices=["hopper", "pour"])
+    ap.add_argument("--workload", default="hopper", choices=["hopper", "pour", "drum", "sq"])
     ap.add_argument("--n", type=int, default=0, help="particle count (default: 1M hopper, 20k pour)")
     ap.add_argument("--settle", type=int, default=200, help="untimed settling steps before warm-up")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
@@ -53,6 +53,15 @@ def parse():
 
 def make_workload(args, seed_offset=0):
     import gb2_scenarios as S
+    if args.workload == "drum":
+        n = args.n or 1_000_000
+        length = 0.85 * (n / 8_000_000)
+        sc = S.drum(n=n, seed=7 + seed_offset, length=max(length, 0.05), n_ax=max(8, int(121 * length / 0.85)))
+        ntri = len(sc["fixes"][1]["nodes"])
+        desc = ("drum-%d: spheres r U(0.8, 1.2) mm, Hertz/history, 0.5 m drum (length scaled to the particle "
+                "count for a 35%% fill of the 8M/0.85 m configuration), %d triangles, fix move/mesh rotate 2 rad/s, "
+                "dt 5e-6" % (n, ntri))
+        return sc, desc, {"n_particles": n, "triangles": ntri}
     if args.workload == "hopper":
         n = args.n or 1_000_000
         sc = S.hopper(n=n, seed=2024 + seed_offset, gap=0.01, vmax=0.05)
@@ -385,10 +394,59 @@ def own_arm(args):
         dist.destroy_process_group()
 
 
+def sq_arm(args):
+    """Superquadric packing: plain first-contact solve against the learned
+    initial guess, same particles, same steps, device-timed."""
+    import granb200
+    import gb2_scenarios as S
+    n = args.n or 200_000
+    t0 = time.perf_counter()
+    tr = granb200.MlpTrainer()
+    info = tr.make_data(1_000_000, seed=1)
+    tr.init(seed=2)
+    l0, l1 = tr.train(epochs=4, batch=4096, lr=2e-3)
+    ev = tr.evaluate(100_000, seed=99)
+    train_s = time.perf_counter() - t0
+    params = tr.params()
+    sc = S.sq_packing(n=n, seed=11)
+    res = {}
+    for name, learned in (("plain", None), ("learned", params)):
+        e = granb200.SqEngine(sc, learned=learned)
+        e.setup()
+        e.run(args.settle)
+        e.run(max(args.warmup, 3))
+        c0 = e.counters()
+        ms = e.run_timed(args.steps)
+        c1 = e.counters()
+        res[name] = {"ms_per_step": ms / args.steps, "value": n * args.steps / (ms * 1e-3),
+                     "newton_iters": c1["iters"] - c0["iters"], "newton_solves": c1["solves"] - c0["solves"],
+                     "pairs_solved": c1["pairs_solved"] - c0["pairs_solved"],
+                     "learned_accepted": c1["learned_used"] - c0["learned_used"],
+                     "learned_rejected": c1["learned_rejected"] - c0["learned_rejected"]}
+        e.close()
+    line = {
+        "metric": "particle-steps/s @200k superquadrics, learned vs plain initial guess", "unit": UNIT,
+        "value": res["learned"]["value"], "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 contact solve, bf16 MLP", "data": "synthetic",
+        "config": {"workload": "sq-packing-%d: half-axes U(1,2) mm, blockiness U(2,8), random orientations, "
+                               "Hertz/history, dt 1e-5, random velocities +-1 m/s" % n,
+                   "settle_steps": args.settle},
+        "plain": res["plain"], "learned": res["learned"],
+        "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
+        "training": {"samples": info["valid"], "plain_iters_per_sample": info["plain_iters"],
+                     "plain_solves_per_sample": info["plain_solves"], "loss_first": l0, "loss_last": l1,
+                     "seconds": train_s, "held_out": ev},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "sq":
+        sq_arm(args)
     else:
         own_arm(args)
 
