@@ -82,7 +82,7 @@ struct MeshFix {
     MeshTopo topo;
     DBuf<TriGeom> tri;
     DBuf<int> cnn_start, cnn_list, bin_tri_start, bin_tri_list;
-    int maxt = 8;
+    int maxt = 32;   // candidate-triangle slots per atom (grown on demand up to 64)
     DBuf<int> tcnt, tlist, snp, spartner;
     DBuf<double> shist;
     DBuf<int> snp2, spartner2;   // re-paging target
@@ -131,6 +131,13 @@ struct gb2_ctx {
     DBuf<uint8_t> revs;
     int minb = 4;                 // register-allocation target of the pair step kernel (blocks/SM)
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
+    // steps queued ahead of the rebuild decision (see gb2_run)
+    bool queue_ok = true;         // GB2_QUEUE_DEPTH=0 turns it off
+    int queue_depth = 4;
+    bool queue_active = false;
+    DBuf<int> dstop;
+    int *h_stop = nullptr;        // pinned ring of stop words read back per queued step
+    cudaEvent_t qev[16] = {};
     DBuf<int> type, tag;
     int maxn = 16, maxr = 16, maxp = 16;
     DBuf<int> nnum, nbr, flag, rnum, rev, pnum, ptag;
@@ -303,6 +310,8 @@ Dev make_dev(gb2_ctx *c)
     D.status = c->dstatus.p;
     D.dflag = c->ddflag.p;
     D.need = c->dneed.p;
+    D.dstop = c->queue_active ? c->dstop.p : nullptr;
+    D.step = (int)c->ntimestep;
     return D;
 }
 
@@ -967,7 +976,7 @@ void launch_step(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
 
 int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int store_f)
 {
-    if (fuse_next) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
+    if (fuse_next && !c->queue_active) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
     Dev D = make_dev(c);
     gb2_ctx::EvPair e;
     if (prof_begin(c, PROF_PAIR_MAIN, &e)) return GB2_ERR_CUDA;
@@ -1074,6 +1083,10 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     c->split = p->precision == GB2_PREC_SPLIT;
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
     if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
+    if (const char *qd = std::getenv("GB2_QUEUE_DEPTH")) {
+        c->queue_depth = std::min(std::max(std::atoi(qd), 0), 15);
+        c->queue_ok = c->queue_depth > 0;
+    }
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) {
         delete c;
@@ -1081,7 +1094,8 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
-        c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess ||
+        c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess || c->dstop.alloc(1) != cudaSuccess ||
+        cudaMallocHost(&c->h_stop, 16 * sizeof(int)) != cudaSuccess ||
         cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
         cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
@@ -1105,6 +1119,9 @@ int gb2_destroy(gb2_ctx *c)
         cudaEventDestroy(e.b);
     }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->h_stop) cudaFreeHost(c->h_stop);
+    for (auto &e : c->qev)
+        if (e) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     cudaStream_t st = c->st;
@@ -1379,71 +1396,162 @@ int gb2_setup(gb2_ctx *c)
     return 0;
 }
 
+// One Verlet step.  mode 0: the rebuild decision from the device flags
+// (one host synchronisation); mode 1: a rebuild requested by a queued step;
+// mode 2: queued ahead of the decision (no rebuild, no synchronisation).
+static int one_step(gb2_ctx *c, bool last, int mode)
+{
+    c->ntimestep++;
+    c->ago++;
+    const bool decide = c->ago >= c->P.neigh_delay && c->ago % c->P.neigh_every == 0;
+    const bool check = decide && c->P.neigh_check && mode == 0;
+    gb2_ctx::EvPair e;
+    if (!c->fused_pending) {
+        // first step of this run: initial_integrate as its own kernel (later
+        // steps get it fused into the previous step's pair step)
+        if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
+        Dev D = make_dev(c);
+        if (prof_begin(c, PROF_INTEGRATE, &e)) return GB2_ERR_CUDA;
+        k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
+        CKL();
+        if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    }
+    // fix move/mesh: rotate moving meshes (initial_integrate) and test
+    // their displacement since the last rebuild
+    bool moving = false, forced = mode == 1;
+    for (int k = 0; k < c->nfix; k++) {
+        MeshFix *M = c->fix[k].mesh;
+        if (!M || !M->moving) continue;
+        if (!moving) CK(cudaMemsetAsync(c->ddflag.p + 1, 0, sizeof(int), c->st));
+        moving = true;
+        if (M->next_reneighbor == c->ntimestep) forced = true;   // Neighbor::decide must_check
+        MeshRotate mv;
+        mesh_rotation(c, *M, mv);
+        const int nt = (int)M->topo.tri.size();
+        k_mesh_rotate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p, mv,
+                                                      c->ddflag.p + 1);
+        CKL();
+    }
+    bool rebuild = decide && !c->P.neigh_check && mode != 2;
+    bool mesh_far = false;
+    if (check || (moving && mode != 2)) {
+        CK(cudaMemcpyAsync(&c->h_pinned[4], c->ddflag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (check) rebuild = c->h_pinned[4] != 0;
+        mesh_far = moving && c->h_pinned[5] != 0;
+        if (c->prof) prof_resolve(c);
+    }
+    if (forced) rebuild = true;
+    if (!rebuild && mesh_far)   // FixMesh::pre_force on a regular step (src/fix_mesh.cpp:577-583)
+        for (int k = 0; k < c->nfix; k++)
+            if (c->fix[k].mesh && c->fix[k].mesh->moving) c->fix[k].mesh->next_reneighbor = c->ntimestep + 1;
+    if (rebuild) {
+        const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
+        if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
+        int rc = do_rebuild(c, true, sort_now);
+        if (rc) return rc;
+        if (prof_end(c, &e)) return GB2_ERR_CUDA;
+        c->nsteps_rebuild++;
+    } else if (c->nghost > 0) {
+        Dev D = make_dev(c);
+        if (prof_begin(c, PROF_FORWARD, &e)) return GB2_ERR_CUDA;
+        k_forward_comm<<<nblk(c->nghost), kBlock, 0, c->st>>>(D);
+        CKL();
+        if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    }
+    return do_force(c, 1, 1, last ? 0 : 1, last ? 1 : 0);
+}
+
+// Undo the host side of a queued step whose kernels returned at once (an
+// earlier step asked for a rebuild): the step counters, the buffer swaps of
+// do_force and its profiling events.
+static void unqueue_step(gb2_ctx *c, bool last, size_t nev)
+{
+    c->ntimestep--;
+    c->ago--;
+    c->hist.swap(c->hist2);
+    c->vel.swap(c->vel2);
+    c->omg.swap(c->omg2);
+    if (c->split) c->kin.swap(c->kin2);
+    if (!last) c->pos.swap(c->pos2);
+    c->fused_pending = true;
+    while (c->ev_pending.size() > nev) {
+        c->ev_free.push_back(c->ev_pending.back());
+        c->ev_pending.pop_back();
+    }
+}
+
 int gb2_run(gb2_ctx *c, int nsteps)
 {
     if (!c) return GB2_ERR_ARG;
     if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "gb2_setup must precede gb2_run");
-    for (int step = 0; step < nsteps; step++) {
-        c->ntimestep++;
-        c->ago++;
-        const bool decide = c->ago >= c->P.neigh_delay && c->ago % c->P.neigh_every == 0;
-        const bool check = decide && c->P.neigh_check;
-        gb2_ctx::EvPair e;
-        if (!c->fused_pending) {
-            // first step of this run: initial_integrate as its own kernel (later
-            // steps get it fused into the previous step's pair pass B)
-            if (check) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
-            Dev D = make_dev(c);
-            if (prof_begin(c, PROF_INTEGRATE, &e)) return GB2_ERR_CUDA;
-            k_initial_integrate<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, check ? 1 : 0);
-            CKL();
-            if (prof_end(c, &e)) return GB2_ERR_CUDA;
-        }
-        // fix move/mesh: rotate moving meshes (initial_integrate) and test
-        // their displacement since the last rebuild
-        bool moving = false, forced = false;
-        for (int k = 0; k < c->nfix; k++) {
-            MeshFix *M = c->fix[k].mesh;
-            if (!M || !M->moving) continue;
-            if (!moving) CK(cudaMemsetAsync(c->ddflag.p + 1, 0, sizeof(int), c->st));
-            moving = true;
-            if (M->next_reneighbor == c->ntimestep) forced = true;   // Neighbor::decide must_check
-            MeshRotate mv;
-            mesh_rotation(c, *M, mv);
-            const int nt = (int)M->topo.tri.size();
-            k_mesh_rotate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p, mv,
-                                                          c->ddflag.p + 1);
-            CKL();
-        }
-        bool rebuild = decide && !c->P.neigh_check;
-        bool mesh_far = false;
-        if (check || moving) {
-            CK(cudaMemcpyAsync(&c->h_pinned[4], c->ddflag.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
-            CK(cudaStreamSynchronize(c->st));
-            if (check) rebuild = c->h_pinned[4] != 0;
-            mesh_far = moving && c->h_pinned[5] != 0;
-            if (c->prof) prof_resolve(c);
-        }
-        if (forced) rebuild = true;
-        if (!rebuild && mesh_far)   // FixMesh::pre_force on a regular step (src/fix_mesh.cpp:577-583)
-            for (int k = 0; k < c->nfix; k++)
-                if (c->fix[k].mesh && c->fix[k].mesh->moving) c->fix[k].mesh->next_reneighbor = c->ntimestep + 1;
-        if (rebuild) {
-            const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
-            if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
-            int rc = do_rebuild(c, true, sort_now);
+    // Steps are queued up to queue_depth ahead of the rebuild decision when
+    // it can only come from the displacement test (neigh_modify every 1
+    // delay 0 check yes, no moving mesh): each queued step's kernels return
+    // at once if an earlier step's tail found a displacement beyond skin/2
+    // (device word dstop = lowest such step).  The host confirms steps in
+    // order from per-step copies of dstop; at the first step that asked, it
+    // undoes the queued successors, rebuilds and continues.  Device results
+    // are those of the one-step-at-a-time loop; the GPU no longer idles
+    // while the host reads the flag every step.
+    bool queueable = c->queue_ok && c->P.neigh_check && c->P.neigh_every == 1 && c->P.neigh_delay == 0;
+    for (int k = 0; k < c->nfix; k++)
+        if (c->fix[k].mesh && c->fix[k].mesh->moving) queueable = false;
+    int s = 0;
+    while (s < nsteps) {
+        if (!queueable || !c->fused_pending) {
+            int rc = one_step(c, s == nsteps - 1, 0);
             if (rc) return rc;
-            if (prof_end(c, &e)) return GB2_ERR_CUDA;
-            c->nsteps_rebuild++;
-        } else if (c->nghost > 0) {
-            Dev D = make_dev(c);
-            if (prof_begin(c, PROF_FORWARD, &e)) return GB2_ERR_CUDA;
-            k_forward_comm<<<nblk(c->nghost), kBlock, 0, c->st>>>(D);
-            CKL();
-            if (prof_end(c, &e)) return GB2_ERR_CUDA;
+            s++;
+            continue;
         }
-        const bool last = (step == nsteps - 1);
-        if (do_force(c, 1, 1, last ? 0 : 1, last ? 1 : 0)) return GB2_ERR_CUDA;
+        CK(cudaMemsetAsync(c->dstop.p, 0x7f, sizeof(int), c->st));
+        c->queue_active = true;
+        struct Queued {
+            long ntimestep;
+            bool last;
+            size_t nev;
+        };
+        Queued q[16];
+        int head = s, launched = s;
+        bool stop = false;
+        for (;;) {
+            while (launched < nsteps && launched - head < c->queue_depth) {
+                Queued &Q = q[launched % 16];
+                Q.last = launched == nsteps - 1;
+                Q.nev = c->ev_pending.size();
+                int rc = one_step(c, Q.last, 2);
+                if (rc) {
+                    c->queue_active = false;
+                    return rc;
+                }
+                Q.ntimestep = c->ntimestep;
+                cudaEvent_t &ev = c->qev[launched % 16];
+                if (!ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                CK(cudaMemcpyAsync(&c->h_stop[launched % 16], c->dstop.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaEventRecord(ev, c->st));
+                launched++;
+            }
+            if (head == launched) break;
+            CK(cudaEventSynchronize(c->qev[head % 16]));
+            const int v = c->h_stop[head % 16];
+            if (v == 0x7f7f7f7f || (long)v > q[head % 16].ntimestep) {
+                head++;
+                continue;
+            }
+            // step `head` asked for a rebuild of the next step: its queued successors did nothing
+            for (int r = launched - 1; r > head; r--) unqueue_step(c, q[r % 16].last, q[r % 16].nev);
+            launched = head + 1;
+            stop = true;
+            break;
+        }
+        c->queue_active = false;
+        s = launched;
+        if (stop && s < nsteps) {
+            int rc = one_step(c, s == nsteps - 1, 1);
+            if (rc) return rc;
+            s++;
+        }
     }
     int st;
     if (read_status(c, &st)) return GB2_ERR_CUDA;

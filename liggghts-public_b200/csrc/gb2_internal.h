@@ -149,6 +149,8 @@ struct Dev {
     FixDev fix[kMaxFix];
     int *status;
     int *dflag;              // displacement trigger
+    int *dstop;              // queued-ahead steps: lowest step whose tail asked for a rebuild (null when not queuing)
+    int step;                // step number of this launch (compared with *dstop)
     int *need;               // [4] capacity demand seen by the last overflowing kernel:
                              // neighbour slots, partners, reverse entries, mesh slots
 };

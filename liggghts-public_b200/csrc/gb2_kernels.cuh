@@ -58,6 +58,7 @@ __global__ void k_forward_comm(Dev D)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= D.nghost) return;
+    if (D.dstop && *(volatile int *)D.dstop < D.step) return;   // queued step after a rebuild request
     const int src = D.gsrc[g];
     const dbl4 s = D.gshift[g];
     const dbl4 p = D.pos[src];

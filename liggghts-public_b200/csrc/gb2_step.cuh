@@ -63,6 +63,221 @@ __device__ __forceinline__ void serial_atom(const Dev &D, int k, const dbl4 &pk,
     }
 }
 
+// A kernel of a step queued ahead returns at once when an earlier step has
+// asked for a neighbour rebuild (that step's successors are redone after it).
+__device__ __forceinline__ bool step_cancelled(const Dev &D) { return D.dstop && *(volatile int *)D.dstop < D.step; }
+
+// One touching pair of the warp-compacted evaluation: owner kk, the other
+// atom, the half-list slot s of the pair (in kk's list when own, in other's
+// list otherwise).  A j-side entry is evaluated from kk's side with the
+// shear negated; an own entry updates kk's shear slot in the write buffer
+// and sets the contact flag.  res receives the pair's force and torque on kk.
+template <bool ROLLING, bool SPLIT, typename Real>
+__device__ __forceinline__ void eval_item(const Dev &D, int kk, int other, int s, bool own, bool upd, Real *res)
+{
+    const int cap = D.cap;
+    const int e = s * cap + kk;
+    const double sgn = own ? 1.0 : -1.0;
+    const int hrow = own ? kk : other;
+    const dbl4 pkk = ldg4(&D.pos[kk]);
+    const dbl4 po = ldg4(&D.pos[other]);
+    const double delx = pkk.x - po.x;
+    const double dely = pkk.y - po.y;
+    const double delz = pkk.z - po.z;
+    const double rsq = delx * delx + dely * dely + delz * delz;
+    const int tkk = D.type[kk], to = D.type[other];
+    // material lookup in the reference's (owner, neighbour) order
+    const MatPair &M = own ? mat(D, tkk, to) : mat(D, to, tkk);
+    if (own) {
+        const int fl = D.flag[e];
+        if ((fl | 5) != fl) D.flag[e] = fl | 5;   // CONTACT_NORMAL_MODEL | CONTACT_TANGENTIAL_MODEL
+    }
+    if constexpr (SPLIT) {
+        const flt8 a = ldg8f(&D.kin[kk]), b = ldg8f(&D.kin[other]);
+        const double r = sqrt(rsq);
+        const double deltan = (pkk.w + po.w) - r;   // FP64 overlap
+        const float va[3] = {a.vx, a.vy, a.vz}, wa[3] = {a.wx, a.wy, a.wz};
+        const float vb[3] = {b.vx, b.vy, b.vz}, wb[3] = {b.wx, b.wy, b.wz};
+        const float fs = (float)sgn;
+        float sh[3];
+        sh[0] = fs * (float)D.hist[(3 * s + 0) * cap + hrow];
+        sh[1] = fs * (float)D.hist[(3 * s + 1) * cap + hrow];
+        sh[2] = fs * (float)D.hist[(3 * s + 2) * cap + hrow];
+        ContactOutF o;
+        pair_contact_f32(M, (float)delx, (float)dely, (float)delz, (float)r, (float)deltan, (float)pkk.w,
+                         (float)po.w, va, vb, wa, wb, a.m, b.m, sh, upd, (float)D.dt, ROLLING, D.tdamp != 0, o);
+        if (own && upd) {
+            D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
+            D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
+            D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
+        }
+        for (int c = 0; c < 3; c++) {
+            res[c] = o.F[c];
+            res[3 + c] = o.T[c];
+        }
+    } else {
+        const dbl4 vk4 = ldg4(&D.vel[kk]), wk4 = ldg4(&D.omg[kk]);
+        const dbl4 vo4 = ldg4(&D.vel[other]), wo4 = ldg4(&D.omg[other]);
+        const double vk[3] = {vk4.x, vk4.y, vk4.z}, wk[3] = {wk4.x, wk4.y, wk4.z};
+        const double vo[3] = {vo4.x, vo4.y, vo4.z}, wo[3] = {wo4.x, wo4.y, wo4.z};
+        double sh[3];
+        sh[0] = sgn * D.hist[(3 * s + 0) * cap + hrow];   // exact: multiplying by +-1 only flips the sign
+        sh[1] = sgn * D.hist[(3 * s + 1) * cap + hrow];
+        sh[2] = sgn * D.hist[(3 * s + 2) * cap + hrow];
+        ContactOut o;
+        pair_contact<false>(M, delx, dely, delz, rsq, pkk.w, po.w, vk, vo, wk, wo, vk4.w, vo4.w, sh, upd, D.dt,
+                            ROLLING, D.tdamp != 0, o);
+        if (own && upd) {
+            D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
+            D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
+            D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
+        }
+        for (int c = 0; c < 3; c++) {
+            res[c] = o.F[c];
+            res[3 + c] = o.T[c];
+        }
+    }
+}
+
+// FP64: plain in-order sum.  Split: FP32 sum with Kahan compensation kc.
+template <bool SPLIT, typename Real>
+__device__ __forceinline__ void sum_item(Real *as, Real *kc, const Real *v)
+{
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        if constexpr (SPLIT) {
+            const float y = v[c] - kc[c];
+            const float t = as[c] + y;
+            kc[c] = (t - as[c]) - y;
+            as[c] = t;
+        } else {
+            as[c] += v[c];
+        }
+    }
+}
+
+template <bool SPLIT, typename Real>
+__device__ __forceinline__ void pair_total(const Real *as, const Real *kc, ContactOut &acc)
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if constexpr (SPLIT) {
+            acc.F[c] = (double)as[c] - (double)kc[c];
+            acc.T[c] = (double)as[3 + c] - (double)kc[3 + c];
+        } else {
+            acc.F[c] = as[c];
+            acc.T[c] = as[3 + c];
+        }
+    }
+}
+
+// store_f / FixNVESphere::final_integrate / the next step's initial_integrate
+// with the displacement test, for one atom whose total force is in acc
+template <bool SPLIT>
+__device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const dbl4 &pi, dbl4 vi4, dbl4 wi4,
+                                                     const dbl4 &hold, int integrate, int fuse_next, int store_f,
+                                                     const ContactOut &acc)
+{
+    if (store_f) {
+        dbl4 Fo, To;
+        Fo.x = acc.F[0];
+        Fo.y = acc.F[1];
+        Fo.z = acc.F[2];
+        Fo.w = 0.0;
+        To.x = acc.T[0];
+        To.y = acc.T[1];
+        To.z = acc.T[2];
+        To.w = 0.0;
+        D.f[i] = Fo;
+        D.tq[i] = To;
+    }
+    if (integrate) {
+        // FixNVESphere::final_integrate (src/fix_nve_sphere.cpp:208-246)
+        const double dtf = 0.5 * D.dt * 1.0;
+        const double dtfrotate = dtf / 0.4;
+        const double dtfm = dtf / (vi4.w * 1.0);
+        vi4.x += dtfm * acc.F[0];
+        vi4.y += dtfm * acc.F[1];
+        vi4.z += dtfm * acc.F[2];
+        const double dtirotate = dtfrotate / (pi.w * pi.w * vi4.w);
+        wi4.x += dtirotate * acc.T[0];
+        wi4.y += dtirotate * acc.T[1];
+        wi4.z += dtirotate * acc.T[2];
+        if (fuse_next) {
+            // next step's FixNVESphere::initial_integrate with the same force,
+            // then Neighbor::check_distance's displacement test
+            const double dtv = D.dt;
+            vi4.x += dtfm * acc.F[0];
+            vi4.y += dtfm * acc.F[1];
+            vi4.z += dtfm * acc.F[2];
+            dbl4 p = pi;
+            p.x += dtv * vi4.x;
+            p.y += dtv * vi4.y;
+            p.z += dtv * vi4.z;
+            wi4.x += dtirotate * acc.T[0];
+            wi4.y += dtirotate * acc.T[1];
+            wi4.z += dtirotate * acc.T[2];
+            D.pos_out[i] = p;
+            const dbl4 h = hold;
+            const double delx = p.x - h.x, dely = p.y - h.y, delz = p.z - h.z;
+            if (delx * delx + dely * dely + delz * delz > D.triggersq) {
+                *D.dflag = 1;
+                if (D.dstop) atomicMin(D.dstop, D.step);
+            }
+        }
+        D.vel_out[i] = vi4;
+        D.omg_out[i] = wi4;
+        if constexpr (SPLIT) D.kin_out[i] = make_kin(vi4, wi4);
+    }
+}
+
+// The per-atom end of the step once the pair sums are in acc: serial atoms,
+// carried shear of slots that stopped touching, the post_force fixes in
+// definition order, FixNVESphere::final_integrate and -- when the run
+// continues -- the next step's initial_integrate with the displacement test.
+template <bool ROLLING, bool SPLIT>
+__device__ __forceinline__ void atom_tail(const Dev &D, int k, const dbl4 &pk, dbl4 vi4, dbl4 wi4, const dbl4 &hold,
+                                          unsigned long long prevm, int tk, int nr, int nn, unsigned long long mown,
+                                          bool serial, bool upd, int integrate, int fuse_next, int store_f,
+                                          ContactOut &acc)
+{
+    const int cap = D.cap;
+    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
+    if (serial) {
+        serial_atom<ROLLING>(D, k, pk, vi4, wi4, tk, nr, nn, upd, acc);
+    } else if (upd) {
+        // slots that stopped touching this step: carry their shear into the write buffer
+        unsigned long long stopped = prevm & ~mown;
+        while (stopped) {
+            const int s = __ffsll((long long)stopped) - 1;
+            stopped &= stopped - 1ull;
+            D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
+            D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
+            D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
+        }
+    }
+    if (upd) D.prevmask[k] = serial ? ~0ull : mown;
+    const int i = k;
+    const dbl4 pi = pk;
+    const int ti = tk;
+    const double *vi = vk, *wi = wk;
+    // post_force fixes in definition order
+    for (int q = 0; q < D.nfix; q++) {
+        const FixDev &F = D.fix[q];
+        if (F.kind == FIX_GRAVITY) {
+            const double massone = vi4.w * 1.;
+            acc.F[0] += massone * F.acc[0];
+            acc.F[1] += massone * F.acc[1];
+            acc.F[2] += massone * F.acc[2];
+        } else if (F.kind == FIX_WALL_PLANE) {
+            if (F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
+        } else if (F.kind == FIX_WALL_MESH) {
+            mesh_wall_atom(D, F.mesh, i, pi, vi, wi, vi4.w, ti, upd, acc);
+        }
+    }
+    atom_store_integrate<SPLIT>(D, i, pi, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
+}
+
 // The pair step: PairGran::compute for one owned atom k with its j-side
 // (reverse) entries and its own half-list entries, the post_force fixes,
 // FixNVESphere::final_integrate and -- when the run continues -- the next
@@ -89,6 +304,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
 {
     using Real = typename std::conditional<SPLIT, float, double>::type;
     __shared__ Real sres[4][32][6];
+    if (step_cancelled(D)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int wbase = blockIdx.x * blockDim.x + wid * 32;
@@ -132,199 +348,34 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
                 const int kk = wbase + L;
                 const int q = w - exL;
                 const int qr = __popcll(mrL);
-                // operands of one pair: j-side entries are evaluated from kk's side
-                // with the shear negated, own entries update kk's slot
-                int other, s, e = -1;
-                double sgn;
+                int other, s;
                 bool own;
                 if (q < qr) {
                     const int r = nth_set_bit(mrL, q);
                     other = __ldg(&D.rev[r * cap + kk]);
                     s = D.revs[r * cap + kk];
-                    sgn = -1.0;
                     own = false;
                 } else {
                     s = nth_set_bit(moL, q - qr);
-                    e = s * cap + kk;
-                    other = __ldg(&D.nbr[e]);
-                    sgn = 1.0;
+                    other = __ldg(&D.nbr[s * cap + kk]);
                     own = true;
                 }
-                const int hrow = own ? kk : other;
-                const dbl4 pkk = ldg4(&D.pos[kk]);
-                const dbl4 po = ldg4(&D.pos[other]);
-                const double delx = pkk.x - po.x;
-                const double dely = pkk.y - po.y;
-                const double delz = pkk.z - po.z;
-                const double rsq = delx * delx + dely * dely + delz * delz;
-                const int tkk = D.type[kk], to = D.type[other];
-                // material lookup in the reference's (owner, neighbour) order
-                const MatPair &M = own ? mat(D, tkk, to) : mat(D, to, tkk);
-                if (own) {
-                    const int fl = D.flag[e];
-                    if ((fl | 5) != fl) D.flag[e] = fl | 5;   // CONTACT_NORMAL_MODEL | CONTACT_TANGENTIAL_MODEL
-                }
                 Real res[6];
-                if constexpr (SPLIT) {
-                    const flt8 a = ldg8f(&D.kin[kk]), b = ldg8f(&D.kin[other]);
-                    const double r = sqrt(rsq);
-                    const double deltan = (pkk.w + po.w) - r;   // FP64 overlap
-                    const float va[3] = {a.vx, a.vy, a.vz}, wa[3] = {a.wx, a.wy, a.wz};
-                    const float vb[3] = {b.vx, b.vy, b.vz}, wb[3] = {b.wx, b.wy, b.wz};
-                    const float fs = (float)sgn;
-                    float sh[3];
-                    sh[0] = fs * (float)D.hist[(3 * s + 0) * cap + hrow];
-                    sh[1] = fs * (float)D.hist[(3 * s + 1) * cap + hrow];
-                    sh[2] = fs * (float)D.hist[(3 * s + 2) * cap + hrow];
-                    ContactOutF o;
-                    pair_contact_f32(M, (float)delx, (float)dely, (float)delz, (float)r, (float)deltan, (float)pkk.w,
-                                     (float)po.w, va, vb, wa, wb, a.m, b.m, sh, upd, (float)D.dt, ROLLING,
-                                     D.tdamp != 0, o);
-                    if (own && upd) {
-                        D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
-                        D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
-                        D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
-                    }
-                    for (int c = 0; c < 3; c++) {
-                        res[c] = o.F[c];
-                        res[3 + c] = o.T[c];
-                    }
-                } else {
-                    const dbl4 vk4 = ldg4(&D.vel[kk]), wk4 = ldg4(&D.omg[kk]);
-                    const dbl4 vo4 = ldg4(&D.vel[other]), wo4 = ldg4(&D.omg[other]);
-                    const double vk[3] = {vk4.x, vk4.y, vk4.z}, wk[3] = {wk4.x, wk4.y, wk4.z};
-                    const double vo[3] = {vo4.x, vo4.y, vo4.z}, wo[3] = {wo4.x, wo4.y, wo4.z};
-                    double sh[3];
-                    sh[0] = sgn * D.hist[(3 * s + 0) * cap + hrow];   // exact: multiplying by +-1 only flips the sign
-                    sh[1] = sgn * D.hist[(3 * s + 1) * cap + hrow];
-                    sh[2] = sgn * D.hist[(3 * s + 2) * cap + hrow];
-                    ContactOut o;
-                    pair_contact<false>(M, delx, dely, delz, rsq, pkk.w, po.w, vk, vo, wk, wo, vk4.w, vo4.w, sh, upd,
-                                        D.dt, ROLLING, D.tdamp != 0, o);
-                    if (own && upd) {
-                        D.hist_out[(3 * s + 0) * cap + kk] = sh[0];
-                        D.hist_out[(3 * s + 1) * cap + kk] = sh[1];
-                        D.hist_out[(3 * s + 2) * cap + kk] = sh[2];
-                    }
-                    for (int c = 0; c < 3; c++) {
-                        res[c] = o.F[c];
-                        res[3 + c] = o.T[c];
-                    }
-                }
+                eval_item<ROLLING, SPLIT>(D, kk, other, s, own, upd, res);
 #pragma unroll
                 for (int c = 0; c < 6; c++) sres[wid][lane][c] = res[c];
             }
             __syncwarp();
             const int lo = max(it.excl, base), hi = min(it.excl + it.cnt, base + 32);
-            for (int q = lo; q < hi; q++) {
-#pragma unroll
-                for (int c = 0; c < 6; c++) {
-                    if constexpr (SPLIT) {
-                        const float y = sres[wid][q - base][c] - kc[c];
-                        const float t = as[c] + y;
-                        kc[c] = (t - as[c]) - y;
-                        as[c] = t;
-                    } else {
-                        as[c] += sres[wid][q - base][c];
-                    }
-                }
-            }
+            for (int q = lo; q < hi; q++) sum_item<SPLIT>(as, kc, &sres[wid][q - base][0]);
             __syncwarp();
         }
     }
     ContactOut acc;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        if constexpr (SPLIT) {
-            acc.F[c] = (double)as[c] - (double)kc[c];
-            acc.T[c] = (double)as[3 + c] - (double)kc[3 + c];
-        } else {
-            acc.F[c] = as[c];
-            acc.T[c] = as[3 + c];
-        }
-    }
+    pair_total<SPLIT>(as, kc, acc);
     if (!valid) return;
-    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
-    if (serial) {
-        serial_atom<ROLLING>(D, k, pk, vi4, wi4, tk, nr, nn, upd, acc);
-    } else if (upd) {
-        // slots that stopped touching this step: carry their shear into the write buffer
-        unsigned long long stopped = prevm & ~mown;
-        while (stopped) {
-            const int s = __ffsll((long long)stopped) - 1;
-            stopped &= stopped - 1ull;
-            D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
-            D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
-            D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
-        }
-    }
-    if (upd) D.prevmask[k] = serial ? ~0ull : mown;
-    const int i = k;
-    const dbl4 pi = pk;
-    const int ti = tk;
-    const double *vi = vk, *wi = wk;
-    // post_force fixes in definition order
-    for (int k = 0; k < D.nfix; k++) {
-        const FixDev &F = D.fix[k];
-        if (F.kind == FIX_GRAVITY) {
-            const double massone = vi4.w * 1.;
-            acc.F[0] += massone * F.acc[0];
-            acc.F[1] += massone * F.acc[1];
-            acc.F[2] += massone * F.acc[2];
-        } else if (F.kind == FIX_WALL_PLANE) {
-            if (F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
-        } else if (F.kind == FIX_WALL_MESH) {
-            mesh_wall_atom(D, F.mesh, i, pi, vi, wi, vi4.w, ti, upd, acc);
-        }
-    }
-    if (store_f) {
-        dbl4 Fo, To;
-        Fo.x = acc.F[0];
-        Fo.y = acc.F[1];
-        Fo.z = acc.F[2];
-        Fo.w = 0.0;
-        To.x = acc.T[0];
-        To.y = acc.T[1];
-        To.z = acc.T[2];
-        To.w = 0.0;
-        D.f[i] = Fo;
-        D.tq[i] = To;
-    }
-    if (integrate) {
-        // FixNVESphere::final_integrate (src/fix_nve_sphere.cpp:208-246)
-        const double dtf = 0.5 * D.dt * 1.0;
-        const double dtfrotate = dtf / 0.4;
-        const double dtfm = dtf / (vi4.w * 1.0);
-        vi4.x += dtfm * acc.F[0];
-        vi4.y += dtfm * acc.F[1];
-        vi4.z += dtfm * acc.F[2];
-        const double dtirotate = dtfrotate / (pi.w * pi.w * vi4.w);
-        wi4.x += dtirotate * acc.T[0];
-        wi4.y += dtirotate * acc.T[1];
-        wi4.z += dtirotate * acc.T[2];
-        if (fuse_next) {
-            // next step's FixNVESphere::initial_integrate with the same force,
-            // then Neighbor::check_distance's displacement test
-            const double dtv = D.dt;
-            vi4.x += dtfm * acc.F[0];
-            vi4.y += dtfm * acc.F[1];
-            vi4.z += dtfm * acc.F[2];
-            dbl4 p = pi;
-            p.x += dtv * vi4.x;
-            p.y += dtv * vi4.y;
-            p.z += dtv * vi4.z;
-            wi4.x += dtirotate * acc.T[0];
-            wi4.y += dtirotate * acc.T[1];
-            wi4.z += dtirotate * acc.T[2];
-            D.pos_out[i] = p;
-            const dbl4 h = hold;
-            const double delx = p.x - h.x, dely = p.y - h.y, delz = p.z - h.z;
-            if (delx * delx + dely * dely + delz * delz > D.triggersq) *D.dflag = 1;
-        }
-        D.vel_out[i] = vi4;
-        D.omg_out[i] = wi4;
-        if constexpr (SPLIT) D.kin_out[i] = make_kin(vi4, wi4);
-    }
+    atom_tail<ROLLING, SPLIT>(D, k, pk, vi4, wi4, hold, prevm, tk, nr, nn, mown, serial, upd, integrate, fuse_next,
+                              store_f, acc);
 }
 
 }  // namespace gb2

@@ -153,37 +153,51 @@ def test_split_forces_after_steps():
     assert np.quantile(herr, 0.999) <= TOL and herr.max() <= 1e-3
 
 
+def _pour_stats(e, r, box):
+    """Coordination number, packing fraction and cumulative overlap histogram."""
+    a = e.atoms()
+    p = e.pairs()
+    x = by_tag(a)["x"]
+    i, j = p["tag_i"] - 1, p["tag_j"] - 1
+    d = x[i] - x[j]
+    for k in (0, 1):   # periodic x/y minimum image
+        d[:, k] -= box[k] * np.round(d[:, k] / box[k])
+    ov = 2 * r - np.sqrt((d ** 2).sum(axis=1))
+    touch = ov > 0
+    z = np.sort(x[:, 2])
+    top = z[int(0.98 * len(z))] + r
+    phi = len(z) * 4.0 / 3.0 * np.pi * r ** 3 / (box[0] * box[1] * top)
+    hist, _ = np.histogram(ov[touch] / r, bins=8, range=(0.0, 0.02))
+    return np.array([2.0 * touch.sum() / len(x), phi]), np.cumsum(hist) / max(touch.sum(), 1)
+
+
 def test_split_pour_statistics():
-    """Sphere pour (20,000 spheres) settled in each precision: coordination
-    number, packing fraction of the bed and the overlap histogram agree
-    within 1% (trajectories are chaotic, so only statistics compare)."""
-    sc = S.sphere_pour(n=20000, seed=12345)
+    """Sphere pour (80,000 spheres, config 1's pour on an 80 x 80 mm
+    periodic floor) settled 0.8 s in each precision, then sampled 10 times
+    over the next 0.2 s: the time-averaged coordination number, packing
+    fraction and overlap distribution (cumulative histogram over 8 bins)
+    agree within 1%.  Trajectories are chaotic, so only statistics compare;
+    the spread between two FP64 realisations (another seed) is printed for
+    reference."""
+    box = (0.08, 0.08, 0.2)
     res = []
-    for split in (False, True):
+    for split, seed in ((False, 12345), (True, 12345), (False, 777)):
+        sc = S.sphere_pour(n=80000, seed=seed, box=box)
         e = _engine(sc, split)
         e.setup()
-        e.run(40000)
-        a = e.atoms()
-        p = e.pairs()
-        x = by_tag(a)["x"]
-        r = 1e-3
-        i, j = p["tag_i"] - 1, p["tag_j"] - 1
-        d = x[i] - x[j]
-        # periodic x/y minimum image
-        for k, L in ((0, 0.04), (1, 0.04)):
-            d[:, k] -= L * np.round(d[:, k] / L)
-        dist = np.sqrt((d ** 2).sum(axis=1))
-        ov = 2 * r - dist
-        touch = ov > 0
-        z = np.sort(x[:, 2])
-        top = z[int(0.98 * len(z))] + r
-        phi = len(z) * 4.0 / 3.0 * np.pi * r ** 3 / (0.04 * 0.04 * top)
-        hist, _ = np.histogram(ov[touch] / r, bins=8, range=(0.0, 0.02))
-        res.append({"coord": 2.0 * touch.sum() / len(x), "phi": phi, "hist": hist / max(touch.sum(), 1)})
+        e.run(80000)
+        sa, ha = np.zeros(2), np.zeros(8)
+        for _ in range(10):
+            e.run(2000)
+            st, h = _pour_stats(e, 1e-3, box)
+            sa += st / 10
+            ha += h / 10
+        res.append((sa, ha))
         e.close()
-    a, b = res
-    print("coordination %.4f / %.4f, packing %.4f / %.4f" % (a["coord"], b["coord"], a["phi"], b["phi"]))
-    print("overlap histogram", np.round(a["hist"], 4), np.round(b["hist"], 4))
-    assert abs(a["coord"] - b["coord"]) <= 0.01 * a["coord"]
-    assert abs(a["phi"] - b["phi"]) <= 0.01 * a["phi"]
-    assert np.max(np.abs(a["hist"] - b["hist"])) <= 0.01
+    (a, ha), (b, hb), (c, hc) = res
+    print("coordination %.4f / %.4f (other seed %.4f), packing %.4f / %.4f (%.4f)" % (a[0], b[0], c[0], a[1], b[1], c[1]))
+    print("cumulative overlap histogram", np.round(ha, 4), np.round(hb, 4), "other seed", np.round(hc, 4))
+    print("split vs fp64 %.4f, fp64 seed spread %.4f" % (np.abs(ha - hb).max(), np.abs(ha - hc).max()))
+    assert abs(a[0] - b[0]) <= 0.01 * a[0]
+    assert abs(a[1] - b[1]) <= 0.01 * a[1]
+    assert np.abs(ha - hb).max() <= 0.01
