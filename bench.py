@@ -44,8 +44,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--precision", default="split", choices=["split", "fp64"],
                     help="precision of the headline arm (split: FP32 contact math on FP64 state)")
-    ap.add_argument("--fp64-steps", type=int, default=1000,
-                    help="timed steps of the plain FP64 form on the same state (0: skip)")
+    ap.add_argument("--fp64-steps", type=int, default=-1,
+                    help="timed steps of the plain FP64 form on the same state (-1: as many as --steps, 0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -304,6 +304,8 @@ def own_arm(args):
     eng = granb200.Engine(sc, precision=prec, device=local)
     eng.setup()
     eng.run(args.settle)
+    if args.fp64_steps < 0:
+        args.fp64_steps = args.steps
     start_state = state_scenario(sc, eng.atoms()) if args.fp64_steps > 0 and split else None
     eng.run(max(args.warmup, 3))
     W = timed_window(eng, args.steps, dist, local)
@@ -353,10 +355,8 @@ def own_arm(args):
         line["fp64_gpu"] = {"value": v64, "unit": UNIT, "steps": args.fp64_steps,
                             "ms_per_step": W64["ms"] / args.fp64_steps,
                             "kernel_ms_per_step": {k: v / args.fp64_steps for k, v in W64["kt"].items()},
-                            "note": "bit-exact FP64 path from the same settled state; the split window runs "
-                                    "%d steps, this one %d" % (args.steps, args.fp64_steps)}
-        # like-for-like ratio over the first fp64-steps steps is not available from one window;
-        # the ratio of per-step rates is reported
+                            "note": "bit-exact FP64 path from the same settled state (same settle and warm-up "
+                                    "steps, %d timed steps; split window %d)" % (args.fp64_steps, args.steps)}
         line["split_over_fp64"] = value / v64
         e64.close()
         del e64

@@ -615,10 +615,16 @@ int grown_capacity(gb2_ctx *c, int which, int old, int limit)
 // device: per-triangle bin ranges, pairs in triangle order, a stable sort by
 // bin (so each bin lists its triangles in ascending order) and a scan of the
 // per-bin counts.
-int mesh_bins_moving(gb2_ctx *c, MeshFix &M)
+int mesh_bins_device(gb2_ctx *c, MeshFix &M, bool moving)
 {
-    M.nl_skin = c->P.skin;   // changingMesh: full skin, distmax = cutneighmax + SMALL_DELTA
-    M.distmax = c->cutneighmax + M.nl_skin / (70. * M_PI);
+    if (moving) {   // changingMesh: full skin, distmax = cutneighmax + SMALL_DELTA
+        M.nl_skin = c->P.skin;
+        M.distmax = c->cutneighmax + M.nl_skin / (70. * M_PI);
+    } else {        // static mesh: half skin, distmax = cutneighmax - rmax + SMALL_DELTA
+        const double rmax = 0.5 * (c->cutneighmax - c->P.skin);
+        M.nl_skin = 0.5 * c->P.skin;
+        M.distmax = c->cutneighmax - rmax + M.nl_skin / (70. * M_PI);
+    }
     const int n = (int)M.topo.tri.size();
     CK(M.trange.alloc((size_t)6 * n));
     CK(M.tcount.alloc((size_t)n + 1));
@@ -641,8 +647,10 @@ int mesh_bins_moving(gb2_ctx *c, MeshFix &M)
     CK(cudaMemcpyAsync(&c->h_pinned[3], M.toff.p + n, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     if (read_status(c, &st)) return GB2_ERR_CUDA;
     npairs = c->h_pinned[3];
-    if (st & ST_MESH_OUTSIDE_GRID)
+    if (st & ST_MESH_OUTSIDE_GRID) {
+        if (!moving) return GB2_ERR_CAPACITY;   // static: the host list (exact bin aliasing) takes over
         return set_err(c, GB2_ERR_UNSUPPORTED, "moving mesh within the neighbour cutoff of the box boundary");
+    }
     const size_t np = std::max(npairs, 1);
     if (M.pkeys.n < np) {   // headroom: the mesh turns, its bounding boxes change size
         CK(M.pkeys.alloc(np + np / 2));
@@ -651,10 +659,18 @@ int mesh_bins_moving(gb2_ctx *c, MeshFix &M)
         CK(M.bin_tri_list.alloc(np + np / 2));
     }
     CK(cudaMemsetAsync(M.bincnt.p, 0, sizeof(int) * ((size_t)c->mbins + 1), c->st));
-    k_tri_bin_fill<<<nblk(n), kBlock, 0, c->st>>>(D, n, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p, M.bincnt.p);
-    CKL();
     int endbit = 1;
-    while ((1l << endbit) < (long)c->mbins + 1) endbit++;
+    if (moving) {
+        k_tri_bin_fill<<<nblk(n), kBlock, 0, c->st>>>(D, n, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p, M.bincnt.p);
+        while ((1l << endbit) < (long)c->mbins + 1) endbit++;
+    } else {
+        const double dx = c->binsize[0] / 2.0, dy = c->binsize[1] / 2.0, dz = c->binsize[2] / 2.0;
+        const double maxdiag = std::sqrt(dx * dx + dy * dy + dz * dz);
+        k_tri_bin_fill_cull<<<nblk(n), kBlock, 0, c->st>>>(D, M.tri.p, n, M.trange.p, M.toff.p, M.pkeys.p,
+                                                             M.pvals.p, M.bincnt.p, maxdiag, M.distmax + M.nl_skin);
+        endbit = 32;   // dropped pairs carry key 0xffffffff
+    }
+    CKL();
     size_t b1 = 0, b2 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b1, M.pkeys.p, M.pkeys2.p, M.pvals.p, M.bin_tri_list.p, npairs, 0,
                                     endbit, c->st);
@@ -875,10 +891,16 @@ int do_pre_force(gb2_ctx *c)
                 const int nt = (int)M.topo.tri.size();
                 k_mesh_store_last<<<nblk(nt), kBlock, 0, c->st>>>(M.tri.p, nt, M.node_last.p);
                 CKL();
-                int rc = mesh_bins_moving(c, M);
+                int rc = mesh_bins_device(c, M, true);
                 if (rc) return rc;
             } else if (!M.bins_valid) {
-                if (mesh_bins(c, M)) return GB2_ERR_CUDA;
+                const int rc = mesh_bins_device(c, M, false);
+                if (rc == GB2_ERR_CAPACITY) {   // bins outside the grid: host list with the reference's aliasing
+                    if (mesh_bins(c, M)) return GB2_ERR_CUDA;
+                } else if (rc) {
+                    return rc;
+                }
+                M.bins_valid = true;
             }
             // candidates into fresh buffers (old slots are still needed)
             const int old_maxt = M.maxt;

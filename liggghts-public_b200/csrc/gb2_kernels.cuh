@@ -644,6 +644,37 @@ __global__ void k_tri_bin_range(Dev D, const TriGeom *tri, int ntri, double dist
     count[t] = (int)n;
 }
 
+// Static mesh (FixNeighlistMesh::generate_bin_list, src/fix_neighlist_mesh.cpp:456-490):
+// the same pairs, but a bin is kept only when a sphere of the bin's half
+// diagonal at the bin centre passes the neighbour-build test against the
+// triangle with threshold distmax + skin; dropped pairs get key 0xffffffff
+// and sort to the end.
+__global__ void k_tri_bin_fill_cull(Dev D, const TriGeom *tri, int ntri, const int *range, const int *off,
+                                    unsigned *keys, int *vals, int *bincnt, double maxdiag, double thresh)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    int p = off[t];
+    const int end = off[t + 1];
+    if (p == end) return;
+    const int *r = range + 6 * t;
+    const TriGeom &T = tri[t];
+    for (int ix = r[0]; ix <= r[3]; ix++)
+        for (int iy = r[1]; iy <= r[4]; iy++)
+            for (int iz = r[2]; iz <= r[5]; iz++) {
+                const int b = iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
+                double center[3];
+                center[0] = (D.mbinlo[0] + ix + 0.5) * D.binsize[0] + D.bboxlo[0];
+                center[1] = (D.mbinlo[1] + iy + 0.5) * D.binsize[1] + D.bboxlo[1];
+                center[2] = (D.mbinlo[2] + iz + 0.5) * D.binsize[2] + D.bboxlo[2];
+                const bool keep = tri_neighbuild(T, maxdiag, center, thresh);
+                keys[p] = keep ? (unsigned)b : 0xffffffffu;
+                vals[p] = t;
+                if (keep) atomicAdd(&bincnt[b], 1);
+                p++;
+            }
+}
+
 // Pass 2: (bin, triangle) pairs in triangle order, and per-bin counts
 __global__ void k_tri_bin_fill(Dev D, int ntri, const int *range, const int *off, unsigned *keys, int *vals,
                                int *bincnt)
