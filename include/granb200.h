@@ -120,6 +120,13 @@ int gb2_upload_atoms(gb2_ctx *ctx, int n, const double *x, const double *v,
 /* post_force fixes, applied in the order they are added */
 int gb2_add_gravity(gb2_ctx *ctx, double magnitude, const double dir[3]);
 int gb2_add_wall_plane(gb2_ctx *ctx, int dim, double pos, int wall_type, int rolling_cdt);
+/* fix ID all wall/gran ... primitive type <wall_type> {x,y,z}cylinder <radius> <c1> <c2>
+   (FixWallGran::post_force_primitive with Cylinder<dim>,
+   src/primitive_wall_definitions.h:157-206): axis along dim through (c1, c2)
+   in the coordinates (dim+1)%3, (dim+2)%3; contact inside and outside the
+   shell.  Returns the fix index or a negative error. */
+int gb2_add_wall_cylinder(gb2_ctx *ctx, int dim, double radius, double c1, double c2, int wall_type,
+                          int rolling_cdt);
 /* ntri triangles as read from an STL file, nodes[ntri][3][3]; curvature <= 0
    selects the default 1 - 1e-5.  Returns the fix index (>= 0) or an error. */
 int gb2_add_wall_mesh(gb2_ctx *ctx, int ntri, const double *nodes, int wall_type,
@@ -135,6 +142,11 @@ int gb2_add_wall_mesh(gb2_ctx *ctx, int ntri, const double *nodes, int wall_type
    one (src/fix_mesh.cpp:564-588).  Call before gb2_setup; one mover per mesh. */
 int gb2_add_move_mesh_rotate(gb2_ctx *ctx, int ifix_mesh, const double origin[3], const double axis[3],
                              double period);
+/* fix ID all move/mesh mesh <mesh-id> linear vx vy vz
+   (src/mesh_mover_linear.cpp:66-112 MeshMoverLinear): each step shifts the
+   mesh by v dt, sets the node velocities to v and forces the rebuild after
+   skin/2 as for the rotation.  Call before gb2_setup; one mover per mesh. */
+int gb2_add_move_mesh_linear(gb2_ctx *ctx, int ifix_mesh, const double vel[3]);
 /* current mesh nodes [ntri][3][3] and node velocities (zero for a static mesh)
    of mesh fix ifix; *ntri = element count, nothing written when cap < ntri */
 int gb2_download_mesh_nodes(gb2_ctx *ctx, int ifix, int cap, int *ntri, double *nodes, double *vnode);

@@ -476,6 +476,16 @@ __device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, i
     M.snp[i] = np;
 }
 
+// Cylinder<dim>::calcRadialDistance (src/primitive_wall_definitions.h:165)
+__device__ __forceinline__ double cyl_radial(const FixDev &F, const dbl4 &p, double &dy, double &dz)
+{
+    const double c[3] = {p.x, p.y, p.z};
+    const int y = F.dim == 0 ? 1 : (F.dim == 1 ? 2 : 0), z = F.dim == 0 ? 2 : (F.dim == 1 ? 0 : 1);
+    dy = (y == 0 ? c[0] : (y == 1 ? c[1] : c[2])) - F.cc1;
+    dz = (z == 0 ? c[0] : (z == 1 ? c[1] : c[2])) - F.cc2;
+    return sqrt(dy * dy + dz * dz);
+}
+
 // FixWallGran::post_force_primitive for one atom in the plane's neighbour
 // list (src/fix_wall_gran.cpp:1024-1148, Plane<dim>::resolveContact
 // src/primitive_wall_definitions.h:133)
@@ -483,17 +493,42 @@ __device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, i
                                              const double *wi, double mass, int ti, bool upd, ContactOut &acc)
 {
     const int cap = D.cap;
-    const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
-    double delta_d, deltan;
-    delta_d = F.pos - x;
-    if (x > F.pos)
-        deltan = x - F.pos - pi.w;
-    else
-        deltan = F.pos - x - pi.w;
+    double deltan;
+    double d[3];   // -delta, with constant indices only (keeps d in registers)
+    if (F.cyl) {   // Cylinder<dim>::resolveContact (src/primitive_wall_definitions.h:172-197)
+        double dy, dz, ey = 0.0, ez = 0.0;
+        const double dist = cyl_radial(F, pi, dy, dz);
+        if (dist < 1e-13 && dist > -1e-13) {   // compDouble(dist, 0.0): zero delta, zero distance
+            deltan = 0.0;
+        } else if (dist > F.cr) {
+            deltan = dist - F.cr - pi.w;
+            const double fact = (dist - F.cr) / dist;
+            ey = -dy * fact;
+            ez = -dz * fact;
+        } else {
+            deltan = F.cr - dist - pi.w;
+            const double fact = (F.cr - dist) / dist;
+            ey = +dy * fact;
+            ez = +dz * fact;
+        }
+        // delta[dim] = 0, delta[(dim+1)%3] = ey, delta[(dim+2)%3] = ez
+        const int y = F.dim == 0 ? 1 : (F.dim == 1 ? 2 : 0);
+        d[0] = -(y == 0 ? ey : (F.dim == 0 ? 0. : ez));
+        d[1] = -(y == 1 ? ey : (F.dim == 1 ? 0. : ez));
+        d[2] = -(y == 2 ? ey : (F.dim == 2 ? 0. : ez));
+    } else {
+        const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+        const double delta_d = F.pos - x;
+        if (x > F.pos)
+            deltan = x - F.pos - pi.w;
+        else
+            deltan = F.pos - x - pi.w;
+        d[0] = F.dim == 0 ? -delta_d : -0.;
+        d[1] = F.dim == 1 ? -delta_d : -0.;
+        d[2] = F.dim == 2 ? -delta_d : -0.;
+    }
     if (deltan > D.cutneighmax) return;
     if (deltan <= 0) {
-        // -delta with constant indices only (keeps d in registers)
-        const double d[3] = {F.dim == 0 ? -delta_d : -0., F.dim == 1 ? -delta_d : -0., F.dim == 2 ? -delta_d : -0.};
         double sh[3] = {F.whist[0 * cap + i], F.whist[1 * cap + i], F.whist[2 * cap + i]};
         const double vwall[3] = {0., 0., 0.};
         wall_contact(mat(D, ti, F.wtype), d, -deltan, pi.w, vi, wi, vwall, mass, sh, upd, D.dt, F.rolling != 0,

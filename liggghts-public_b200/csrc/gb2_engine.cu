@@ -93,7 +93,8 @@ struct MeshFix {
     double nl_skin = 0, distmax = 0;
     // fix move/mesh rotate
     bool moving = false;
-    double mv_point[3] = {0, 0, 0}, mv_axis[3] = {0, 0, 1}, mv_omega = 0;
+    int mover = 0;   // 1 rotate, 2 linear
+    double mv_point[3] = {0, 0, 0}, mv_axis[3] = {0, 0, 1}, mv_omega = 0, mv_vel[3] = {0, 0, 0};
     DBuf<double> vnode, node_last;
     DBuf<int> trange, tcount, toff, bincnt, pvals;
     DBuf<unsigned> pkeys, pkeys2;
@@ -105,6 +106,8 @@ struct HostFix {
     double acc[3] = {0, 0, 0};
     int dim = 2;
     double pos = 0;
+    int cyl = 0;
+    double cr = 0, cc1 = 0, cc2 = 0;
     int wtype = 1;
     int rolling = 0;
     DBuf<uint8_t> inlist;
@@ -282,6 +285,10 @@ Dev make_dev(gb2_ctx *c)
         for (int q = 0; q < 3; q++) F.acc[q] = H.acc[q];
         F.dim = H.dim;
         F.pos = H.pos;
+        F.cyl = H.cyl;
+        F.cr = H.cr;
+        F.cc1 = H.cc1;
+        F.cc2 = H.cc2;
         F.wtype = H.wtype;
         F.rolling = H.rolling;
         F.inlist = H.inlist.p;
@@ -1284,6 +1291,21 @@ int gb2_add_wall_plane(gb2_ctx *c, int dim, double pos, int wall_type, int rolli
     return c->nfix++;
 }
 
+int gb2_add_wall_cylinder(gb2_ctx *c, int dim, double radius, double c1, double c2, int wall_type, int rolling_cdt)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!(radius > 0) || !std::isfinite(c1) || !std::isfinite(c2))
+        return set_err(c, GB2_ERR_ARG, "cylinder radius must be positive and its axis finite");
+    const int k = gb2_add_wall_plane(c, dim, 0.0, wall_type, rolling_cdt);
+    if (k < 0) return k;
+    HostFix &H = c->fix[k];
+    H.cyl = 1;
+    H.cr = radius;
+    H.cc1 = c1;
+    H.cc2 = c2;
+    return k;
+}
+
 int gb2_add_wall_mesh(gb2_ctx *c, int ntri, const double *nodes, int wall_type, double curvature, int rolling_cdt)
 {
     int rc = add_fix_common(c);
@@ -1353,12 +1375,35 @@ int gb2_add_move_mesh_rotate(gb2_ctx *c, int ifix_mesh, const double origin[3], 
     const double invnorm = 1. / norm;
     for (int d = 0; d < 3; d++) M.mv_axis[d] *= invnorm;
     M.mv_omega = 2. * M_PI / period;
+    M.mover = 1;
     const size_t nt = M.topo.tri.size();
     CK(M.vnode.alloc(9 * nt));
     CK(M.node_last.alloc(9 * nt));
     CK(cudaMemsetAsync(M.vnode.p, 0, sizeof(double) * 9 * nt, c->st));   // FixMoveMesh::setup: v = 0
     CK(cudaStreamSynchronize(c->st));
     M.moving = true;
+    return 0;
+}
+
+int gb2_add_move_mesh_linear(gb2_ctx *c, int ifix_mesh, const double vel[3])
+{
+    if (!c || !vel) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fix move/mesh must be defined before setup");
+    if (ifix_mesh < 0 || ifix_mesh >= c->nfix || !c->fix[ifix_mesh].mesh)
+        return set_err(c, GB2_ERR_ARG, "fix move/mesh: mesh fix index does not name a mesh wall");
+    MeshFix &M = *c->fix[ifix_mesh].mesh;
+    if (M.moving) return set_err(c, GB2_ERR_UNSUPPORTED, "one fix move/mesh per mesh is supported");
+    for (int d = 0; d < 3; d++) {
+        if (!std::isfinite(vel[d])) return set_err(c, GB2_ERR_ARG, "fix move/mesh: non-finite velocity");
+        M.mv_vel[d] = vel[d];
+    }
+    const size_t nt = M.topo.tri.size();
+    CK(M.vnode.alloc(9 * nt));
+    CK(M.node_last.alloc(9 * nt));
+    CK(cudaMemsetAsync(M.vnode.p, 0, sizeof(double) * 9 * nt, c->st));   // FixMoveMesh::setup: v = 0
+    CK(cudaStreamSynchronize(c->st));
+    M.moving = true;
+    M.mover = 2;
     return 0;
 }
 
@@ -1447,11 +1492,19 @@ static int one_step(gb2_ctx *c, bool last, int mode)
         if (!moving) CK(cudaMemsetAsync(c->ddflag.p + 1, 0, sizeof(int), c->st));
         moving = true;
         if (M->next_reneighbor == c->ntimestep) forced = true;   // Neighbor::decide must_check
-        MeshRotate mv;
-        mesh_rotation(c, *M, mv);
         const int nt = (int)M->topo.tri.size();
-        k_mesh_rotate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p, mv,
-                                                      c->ddflag.p + 1);
+        if (M->mover == 2) {
+            const double dt = c->P.dt;
+            k_mesh_translate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p,
+                                                             M->mv_vel[0] * dt, M->mv_vel[1] * dt, M->mv_vel[2] * dt,
+                                                             M->mv_vel[0], M->mv_vel[1], M->mv_vel[2],
+                                                             0.25 * c->P.skin * c->P.skin, c->ddflag.p + 1);
+        } else {
+            MeshRotate mv;
+            mesh_rotation(c, *M, mv);
+            k_mesh_rotate<<<nblk(nt), kBlock, 0, c->st>>>(M->tri.p, nt, M->vnode.p, M->node_last.p, mv,
+                                                          c->ddflag.p + 1);
+        }
         CKL();
     }
     bool rebuild = decide && !c->P.neigh_check && mode != 2;

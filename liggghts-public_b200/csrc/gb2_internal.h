@@ -97,8 +97,10 @@ struct MeshDev {
 struct FixDev {
     int kind;
     double acc[3];         // gravity
-    int dim;               // plane
+    int dim;               // plane: axis; cylinder: axis direction
     double pos;
+    int cyl;               // 1: {x,y,z}cylinder
+    double cr, cc1, cc2;   // cylinder radius and axis position (the other two coordinates, cyclic order)
     int wtype;
     int rolling;
     uint8_t *inlist;       // primitive-wall neighbour flag per owned atom

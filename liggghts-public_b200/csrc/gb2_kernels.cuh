@@ -393,8 +393,14 @@ __global__ void k_plane_neighlist(Dev D, int ifix)
     if (i >= D.nlocal) return;
     const FixDev &F = D.fix[ifix];
     const dbl4 p = D.pos[i];
-    const double x = F.dim == 0 ? p.x : (F.dim == 1 ? p.y : p.z);
     const double dMax = p.w + D.skin;
+    if (F.cyl) {   // Cylinder<dim>::resolveNeighlist (src/primitive_wall_definitions.h:199-205), as written
+        double dy, dz;
+        const double dist = cyl_radial(F, p, dy, dz) - F.cr;
+        F.inlist[i] = (dMax < dist || -dMax < dist) ? 1 : 0;
+        return;
+    }
+    const double x = F.dim == 0 ? p.x : (F.dim == 1 ? p.y : p.z);
     const double dist = x - F.pos;
     const double absdist = (dist > 0.0) ? dist : -dist;
     F.inlist[i] = (absdist <= dMax) ? 1 : 0;
@@ -594,6 +600,32 @@ __global__ void k_mesh_rotate(TriGeom *tri, int ntri, double *vnode, const doubl
         const double d0 = T.node[j][0] - o[0], d1 = T.node[j][1] - o[1], d2 = T.node[j][2] - o[2];
         if (d0 * d0 + d1 * d1 + d2 * d2 > mv.triggersq) far = true;
     }
+    if (far) *flag = 1;
+}
+
+// One step of MeshMoverLinear::initial_integrate (src/mesh_mover_linear.cpp:94-112)
+// per triangle: nodes and centre shifted by v dt (MultiNodeMesh::move
+// src/multi_node_mesh_I.h:502-513), node velocities 0 + v, and the
+// displacement test of MultiNodeMesh::decideRebuild
+__global__ void k_mesh_translate(TriGeom *tri, int ntri, double *vnode, const double *node_last, double dx0,
+                                 double dx1, double dx2, double v0, double v1, double v2, double triggersq, int *flag)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntri) return;
+    TriGeom &T = tri[t];
+    const double dx[3] = {dx0, dx1, dx2}, v[3] = {v0, v1, v2};
+    bool far = false;
+    for (int j = 0; j < 3; j++) {
+        double *vn = vnode + 9 * t + 3 * j;
+        const double *o = node_last + 9 * t + 3 * j;
+        for (int c = 0; c < 3; c++) {
+            T.node[j][c] = T.node[j][c] + dx[c];
+            vn[c] = 0. + v[c];
+        }
+        const double d0 = T.node[j][0] - o[0], d1 = T.node[j][1] - o[1], d2 = T.node[j][2] - o[2];
+        if (d0 * d0 + d1 * d1 + d2 * d2 > triggersq) far = true;
+    }
+    for (int c = 0; c < 3; c++) T.center[c] = T.center[c] + dx[c];
     if (far) *flag = 1;
 }
 

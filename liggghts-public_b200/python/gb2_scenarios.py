@@ -170,6 +170,62 @@ def hopper(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z=32, ha
     return sc
 
 
+def plate_mesh(half=0.025, z=0.0, k=8):
+    """Square plate at height z, side 2 * half, 2 * k * k triangles (normal +z)."""
+    g = np.linspace(-half, half, k + 1)
+    tris = []
+    for a in range(k):
+        for b in range(k):
+            p00, p10 = (g[a], g[b], z), (g[a + 1], g[b], z)
+            p01, p11 = (g[a], g[b + 1], z), (g[a + 1], g[b + 1], z)
+            tris.append((p00, p10, p11))
+            tris.append((p00, p11, p01))
+    return np.asarray(tris, dtype=np.float64)
+
+
+def silo(n=2000, seed=21, dt=5e-6, skin=0.5e-3, radius=0.02, piston_speed=1.0, vmax=0.1):
+    """Spheres (r U(0.8, 1.2) mm) on a jittered lattice inside a vertical
+    cylinder wall (primitive zcylinder, radius 20 mm, axis at x = y = 0) on a
+    flat floor, pressed by a triangulated square piston that moves down at
+    ``piston_speed`` (fix move/mesh linear)."""
+    rng = np.random.default_rng(seed)
+    rad = rng.uniform(0.8e-3, 1.2e-3, size=n)
+    s = 2.6e-3
+    m = int((radius - 1.5e-3) // s)
+    g = np.arange(-m, m + 1) * s
+    gx, gy = np.meshgrid(g, g, indexing="ij")
+    ok = gx ** 2 + gy ** 2 <= (radius - 1.5e-3) ** 2
+    layer = np.stack([gx[ok], gy[ok]], axis=1)
+    nl = (n + len(layer) - 1) // len(layer)
+    pos = np.zeros((n, 3))
+    for l in range(nl):
+        sl = slice(l * len(layer), min(n, (l + 1) * len(layer)))
+        cnt = sl.stop - sl.start
+        pos[sl, 0:2] = layer[:cnt]
+        pos[sl, 2] = 1.5e-3 + l * s
+    pos[:, :2] += rng.uniform(-0.1e-3, 0.1e-3, size=(n, 2))
+    top = pos[:, 2].max() + 3e-3
+    vel = rng.uniform(-vmax, vmax, size=(n, 3))
+    box = 0.03
+    sc = {
+        "name": "silo", "dt": dt, "skin": skin,
+        "boxlo": [-box, -box, -0.01], "boxhi": [box, box, top + 0.02], "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": 500, "sortbinsize": 0.0,
+        "rolling_cdt": 0, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2500.0, vel),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_cylinder", "dim": 2, "radius": radius, "c1": 0.0, "c2": 0.0, "wall_type": 1},
+            {"kind": "wall_plane", "dim": 2, "pos": 0.0, "wall_type": 1},
+            {"kind": "wall_mesh", "nodes": plate_mesh(0.025, top, 8), "wall_type": 1, "curvature": 0.0},
+            {"kind": "move_mesh_linear", "mesh": 3, "velocity": [0.0, 0.0, -piston_speed]},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5))
+    return sc
+
+
 def drum_mesh(diameter=0.5, length=0.85, n_theta=128, n_ax=121, cap_rings=4):
     """Closed cylinder along x centred on the origin: a side of
     ``2 * n_theta * n_ax`` triangles (axial rings, so no triangle spans the

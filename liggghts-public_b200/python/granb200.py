@@ -28,6 +28,7 @@ EXPORTS = (
     "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
     "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
+    "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -117,6 +118,9 @@ def lib(path=LIB_PATH):
         L.gb2_timer_start.argtypes = [vp]
         L.gb2_timer_stop.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.gb2_add_move_mesh_rotate.argtypes = [vp, ctypes.c_int, D, D, ctypes.c_double]
+        L.gb2_add_move_mesh_linear.argtypes = [vp, ctypes.c_int, D]
+        L.gb2_add_wall_cylinder.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_int, ctypes.c_int]
         L.gb2_download_mesh_nodes.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, D, D]
         _LIB = L
     return _LIB
@@ -184,6 +188,9 @@ class Engine:
                 k = L.gb2_add_gravity(self.h, fx["magnitude"], _dp(arr(fx["vector"])))
             elif kind == "wall_plane":
                 k = L.gb2_add_wall_plane(self.h, fx["dim"], fx["pos"], fx["wall_type"], int(fx.get("rolling_cdt", 0)))
+            elif kind == "wall_cylinder":
+                k = L.gb2_add_wall_cylinder(self.h, fx["dim"], fx["radius"], fx["c1"], fx["c2"], fx["wall_type"],
+                                            int(fx.get("rolling_cdt", 0)))
             elif kind == "wall_mesh":
                 nodes = arr(fx["nodes"])
                 k = L.gb2_add_wall_mesh(self.h, len(nodes) // 9, _dp(nodes), fx["wall_type"], fx.get("curvature", 0.0),
@@ -194,6 +201,9 @@ class Engine:
                 mesh_id = self.fix_ids[fx["mesh"]]
                 self._check(L.gb2_add_move_mesh_rotate(self.h, mesh_id, _dp(arr(fx["origin"])), _dp(arr(fx["axis"])),
                                                        float(fx["period"])))
+                k = None
+            elif kind == "move_mesh_linear":
+                self._check(L.gb2_add_move_mesh_linear(self.h, self.fix_ids[fx["mesh"]], _dp(arr(fx["velocity"]))))
                 k = None
             elif kind == "nve_sphere":
                 k = None

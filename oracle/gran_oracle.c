@@ -48,6 +48,7 @@ static inline int comp_double(double a, double b, double prec)   /* src/math_ext
 
 typedef struct {
     int dim; double pos; int wtype; int rolling;
+    int cyl; double cyl_r, cyl_c1, cyl_c2;   /* {x,y,z}cylinder radius and axis position */
     int rebuild;            /* rebuildPrimitiveNeighlist_ */
     int *list; int nlist, caplist;
     double *hist;           /* property/atom history, 3 per atom */
@@ -79,8 +80,9 @@ typedef struct {
     int *nneighs; int *npartner; int **partner; double **chist;
     unsigned char **keep; unsigned char **isect;
     /* fix move/mesh rotate (MeshMoverRotate) and FixMesh rebuild trigger */
-    int moving;
+    int moving;            /* 0 static, 1 rotate, 2 linear */
     double mv_point[3], mv_axis[3], mv_omega;
+    double mv_vel[3];
     double (*vnode)[3][3];       /* element property "v" */
     double (*node_last)[3][3];   /* nodesLastRe_ */
     long next_reneighbor;        /* FixMesh::next_reneighbor */
@@ -491,6 +493,15 @@ int orc_add_wall_plane(orc_sim *s, int dim, double pos, int wall_type, int rolli
     return s->nfix-1;
 }
 
+/* fix wall/gran ... primitive type <wtype> {x,y,z}cylinder <radius> <c1> <c2> */
+int orc_add_wall_cylinder(orc_sim *s, int dim, double radius, double c1, double c2, int wall_type, int rolling_cdt)
+{
+    int k = orc_add_wall_plane(s, dim, 0.0, wall_type, rolling_cdt);
+    wall_plane *w = s->fix[k].wp;
+    w->cyl = 1; w->cyl_r = radius; w->cyl_c1 = c1; w->cyl_c2 = c2;
+    return k;
+}
+
 /* forward decl */
 static void mesh_build_topology(orc_sim *s, wall_mesh *m);
 
@@ -587,6 +598,42 @@ int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode)
         else memset(vnode, 0, sizeof(double)*9*m->ntri);
     }
     return m->ntri;
+}
+
+/* fix move/mesh ... linear vx vy vz (MeshMoverLinear constructor
+   src/mesh_mover_linear.cpp:66-77) */
+int orc_add_move_mesh_linear(orc_sim *s, int ifix_mesh, double vx, double vy, double vz)
+{
+    if (ifix_mesh < 0 || ifix_mesh >= s->nfix || s->fix[ifix_mesh].kind != ORC_FIX_WALL_MESH) return -1;
+    wall_mesh *m = s->fix[ifix_mesh].wm;
+    if (m->moving) return -1;
+    fixrec *fr = &s->fix[s->nfix++];
+    fr->kind = ORC_FIX_MOVE_MESH;
+    fr->imesh = ifix_mesh;
+    m->moving = 2;
+    m->mv_vel[0] = vx; m->mv_vel[1] = vy; m->mv_vel[2] = vz;
+    int nt = m->ntri > 0 ? m->ntri : 1;
+    m->vnode = calloc((size_t)nt, sizeof(double)*9);
+    m->node_last = calloc((size_t)nt, sizeof(double)*9);
+    m->next_reneighbor = -1;
+    return s->nfix-1;
+}
+
+/* MeshMoverLinear::initial_integrate src/mesh_mover_linear.cpp:94-112 with
+   MultiNodeMesh::move src/multi_node_mesh_I.h:502-513: nodes and centres
+   shifted by v dt (no translation-variant element property on a surface
+   mesh), node velocities 0 + v */
+static void move_mesh_linear(orc_sim *s, wall_mesh *m)
+{
+    double dx[3] = {m->mv_vel[0]*s->p.dt, m->mv_vel[1]*s->p.dt, m->mv_vel[2]*s->p.dt};
+    for (int t = 0; t < m->ntri; t++) {
+        for (int j = 0; j < 3; j++)
+            for (int c = 0; c < 3; c++) m->node[t][j][c] = m->node[t][j][c] + dx[c];
+        for (int c = 0; c < 3; c++) m->center[t][c] = m->center[t][c] + dx[c];
+    }
+    for (int t = 0; t < m->ntri; t++)
+        for (int j = 0; j < 3; j++)
+            for (int c = 0; c < 3; c++) m->vnode[t][j][c] = 0. + m->mv_vel[c];
 }
 
 /* MathExtraLiggghts::vec_quat_rotate src/math_extra_liggghts.h:451-468 with
@@ -1324,6 +1371,14 @@ static void wall_compute_force(orc_sim *s, int ip, sidata_t *sd, const double *v
 /* FixWallGran::pre_force (primitive neighlist) src/fix_wall_gran.cpp:708,
    PrimitiveWall::buildNeighList src/primitive_wall.h:129,
    Plane::resolveNeighlist src/primitive_wall_definitions.h:145 */
+/* Cylinder<dim>::calcRadialDistance src/primitive_wall_definitions.h:165 */
+static double cyl_radial(const wall_plane *w, const double *pos, double *dy, double *dz)
+{
+    *dy = pos[(w->dim+1)%3] - w->cyl_c1;
+    *dz = pos[(w->dim+2)%3] - w->cyl_c2;
+    return sqrt((*dy)*(*dy) + (*dz)*(*dz));
+}
+
 static void wall_plane_pre_force(orc_sim *s, wall_plane *w)
 {
     if (!w->rebuild) return;
@@ -1331,9 +1386,17 @@ static void wall_plane_pre_force(orc_sim *s, wall_plane *w)
     w->nlist = 0;
     for (int i = 0; i < s->nlocal; i++) {
         double dMax = s->radius[i] + s->p.skin;
-        double dist = s->x[3*i+w->dim] - w->pos;
-        double absdist = (dist > 0.0) ? dist : -dist;
-        if (absdist <= dMax) {
+        int in;
+        if (w->cyl) {   /* Cylinder<dim>::resolveNeighlist :201 (as written: near inside, or beyond dMax outside) */
+            double dy, dz;
+            double dist = cyl_radial(w, &s->x[3*i], &dy, &dz) - w->cyl_r;
+            in = (dMax < dist || -dMax < dist);
+        } else {
+            double dist = s->x[3*i+w->dim] - w->pos;
+            double absdist = (dist > 0.0) ? dist : -dist;
+            in = absdist <= dMax;
+        }
+        if (in) {
             if (w->nlist >= w->caplist) { w->caplist = w->caplist ? 2*w->caplist : 256; w->list = xrealloc(w->list, sizeof(int)*w->caplist); }
             w->list[w->nlist++] = i;
         }
@@ -1349,12 +1412,28 @@ static void wall_plane_post_force(orc_sim *s, wall_plane *w, int shearupdate)
         sidata_t sd; memset(&sd, 0, sizeof sd);
         sd.is_wall = 1;
         sd.radi = s->radius[ip];
-        /* Plane<dim>::resolveContact src/primitive_wall_definitions.h:133 */
         double delta[3] = {0., 0., 0.}, deltan;
         const double *pos = &s->x[3*ip];
-        delta[w->dim] = w->pos - pos[w->dim];
-        if (pos[w->dim] > w->pos) deltan = pos[w->dim] - w->pos - sd.radi;
-        else deltan = w->pos - pos[w->dim] - sd.radi;
+        if (w->cyl) {   /* Cylinder<dim>::resolveContact src/primitive_wall_definitions.h:172-197 */
+            double dy, dz;
+            const double dist = cyl_radial(w, pos, &dy, &dz);
+            const int y = (w->dim+1)%3, z = (w->dim+2)%3;
+            if (dist < 1e-13 && dist > -1e-13) {   /* compDouble(dist, 0.0) */
+                deltan = 0.0;
+            } else if (dist > w->cyl_r) {
+                deltan = dist - w->cyl_r - sd.radi;
+                const double fact = (dist - w->cyl_r) / dist;
+                delta[y] = -dy*fact; delta[z] = -dz*fact;
+            } else {
+                deltan = w->cyl_r - dist - sd.radi;
+                const double fact = (w->cyl_r - dist) / dist;
+                delta[y] = +dy*fact; delta[z] = +dz*fact;
+            }
+        } else {        /* Plane<dim>::resolveContact src/primitive_wall_definitions.h:133 */
+            delta[w->dim] = w->pos - pos[w->dim];
+            if (pos[w->dim] > w->pos) deltan = pos[w->dim] - w->pos - sd.radi;
+            else deltan = w->pos - pos[w->dim] - sd.radi;
+        }
         if (deltan > s->cutneighmax) continue;
         double *hist = &w->hist[3*ip];
         if (deltan <= 0 || deltan < 0.0*s->radius[ip]) {
@@ -1881,7 +1960,11 @@ int orc_run(orc_sim *s, int nsteps)
         s->ntimestep++;
         nve_initial(s);
         for (int k = 0; k < s->nfix; k++)
-            if (s->fix[k].kind == ORC_FIX_MOVE_MESH) move_mesh_rotate(s, s->fix[s->fix[k].imesh].wm);
+            if (s->fix[k].kind == ORC_FIX_MOVE_MESH) {
+                wall_mesh *mm = s->fix[s->fix[k].imesh].wm;
+                if (mm->moving == 2) move_mesh_linear(s, mm);
+                else move_mesh_rotate(s, mm);
+            }
         int nflag = neighbor_decide(s);
         if (nflag == 0) comm_forward(s);
         else {

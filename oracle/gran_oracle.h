@@ -60,6 +60,9 @@ int orc_add_gravity(orc_sim *s, double mag, double dx, double dy, double dz);
 /* fix ID all wall/gran model hertz tangential history [rolling_friction cdt]
    primitive type <wtype> {x,y,z}plane <pos> ; dim = 0,1,2 */
 int orc_add_wall_plane(orc_sim *s, int dim, double pos, int wall_type, int rolling_cdt);
+/* fix ID all wall/gran ... primitive type <wtype> {x,y,z}cylinder <radius> <c1> <c2>
+   (axis along dim through (c1, c2) in the other two coordinates, in cyclic order) */
+int orc_add_wall_cylinder(orc_sim *s, int dim, double radius, double c1, double c2, int wall_type, int rolling_cdt);
 /* fix mesh/surface (nodes as read from the STL: ntri x 3 x 3) + its own
    fix wall/gran ... mesh n_meshes 1 meshes <id>; returns fix index */
 int orc_add_wall_mesh(orc_sim *s, int ntri, const double *nodes, int wall_type,
@@ -69,6 +72,8 @@ int orc_add_wall_mesh(orc_sim *s, int ntri, const double *nodes, int wall_type,
    on the mesh of fix index ifix_mesh; returns fix index */
 int orc_add_move_mesh_rotate(orc_sim *s, int ifix_mesh, double ox, double oy, double oz,
                              double ax, double ay, double az, double period);
+/* fix move/mesh mesh <id> linear vx vy vz; returns fix index */
+int orc_add_move_mesh_linear(orc_sim *s, int ifix_mesh, double vx, double vy, double vz);
 /* current nodes (ntri x 3 x 3) and node velocities of a mesh fix; returns ntri */
 int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode);
 

@@ -72,6 +72,8 @@ def lib():
         L.orc_get_mesh_nneighs.argtypes = [ctypes.c_void_p, ctypes.c_int, I]
         L.orc_add_move_mesh_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 7
         L.orc_get_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_add_move_mesh_linear.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
+        L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
         L.orc_error.restype = ctypes.c_char_p
         L.orc_error.argtypes = [ctypes.c_void_p]
         L.orc_pair_force.argtypes = [ctypes.POINTER(OrcParams), D, D, D, D, D, D, ctypes.c_double, ctypes.c_double,
@@ -135,6 +137,9 @@ class Oracle:
                 k = L.orc_add_gravity(self.h, fx["magnitude"], d[0], d[1], d[2])
             elif kind == "wall_plane":
                 k = L.orc_add_wall_plane(self.h, fx["dim"], fx["pos"], fx["wall_type"], int(fx.get("rolling_cdt", 0)))
+            elif kind == "wall_cylinder":
+                k = L.orc_add_wall_cylinder(self.h, fx["dim"], fx["radius"], fx["c1"], fx["c2"], fx["wall_type"],
+                                            int(fx.get("rolling_cdt", 0)))
             elif kind == "wall_mesh":
                 nodes = np.ascontiguousarray(fx["nodes"], dtype=np.float64)
                 self._keep.append(nodes)
@@ -146,6 +151,11 @@ class Oracle:
                                                float(fx["period"]))
                 if k < 0:
                     raise ValueError("oracle: bad move_mesh_rotate")
+            elif kind == "move_mesh_linear":
+                v = fx["velocity"]
+                k = L.orc_add_move_mesh_linear(self.h, self.fix_ids[fx["mesh"]], v[0], v[1], v[2])
+                if k < 0:
+                    raise ValueError("oracle: bad move_mesh_linear")
             elif kind == "nve_sphere":
                 k = None   # the oracle always integrates with fix nve/sphere
             else:

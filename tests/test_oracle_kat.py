@@ -164,3 +164,24 @@ def test_move_mesh_rotate_kinematics():
     assert np.max(np.abs(nodes - expect)) < 1e-12
     w = np.array([30.0, 0.0, 0.0])
     assert np.max(np.abs(vel - np.cross(w, nodes))) < 1e-13
+
+
+def test_cylinder_wall_matches_plane():
+    """A sphere pressed against a zcylinder wall from inside feels the same
+    wall force as against a plane with the same overlap, pointing inward."""
+    def one(fix):
+        sc = S.sphere_pour(n=1)
+        sc["periodic"] = [0, 0, 0]
+        sc["boxlo"], sc["boxhi"] = [-0.05, -0.05, -0.05], [0.05, 0.05, 0.05]
+        a = sc["atoms"]
+        r, ov = 1e-3, 2e-5
+        a["x"] = np.array([[0.02 - r + ov, 0.0, 0.0]])
+        a["v"] = np.zeros((1, 3))
+        sc["fixes"] = [fix, {"kind": "nve_sphere"}]
+        o = oracle.Oracle(sc)
+        o.setup()
+        return o.atoms()["f"][0]
+    fc = one({"kind": "wall_cylinder", "dim": 2, "radius": 0.02, "c1": 0.0, "c2": 0.0, "wall_type": 1})
+    fp = one({"kind": "wall_plane", "dim": 0, "pos": 0.02, "wall_type": 1})
+    assert fc[0] < 0 and abs(fc[1]) < 1e-15 and abs(fc[2]) < 1e-15
+    assert abs(fc[0] - fp[0]) <= 1e-9 * abs(fp[0])

@@ -106,3 +106,26 @@ def test_deterministic():
     pa, pb = a.atoms(), b.atoms()
     for k in ("x", "v", "omega", "f", "torque"):
         assert np.array_equal(pa[k], pb[k])
+
+
+def test_silo_cylinder_wall_and_linear_piston():
+    """zcylinder primitive wall (inside contact), floor plane and a
+    triangulated piston driven by fix move/mesh linear, bit for bit."""
+    sc = S.silo(n=1500, piston_speed=0.5)
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    for _ in range(6):
+        e.run(500)
+        o.run(500)
+        assert_atoms_equal(e, o)
+        assert_pairs_equal(e, o)
+        assert np.array_equal(e.wall_hist(1), o.wall_hist(1)), "cylinder wall history differs"
+        assert np.array_equal(e.wall_hist(2), o.wall_hist(2))
+        assert_mesh_equal(e, o, 3)
+        en, ev = e.mesh_nodes(3)
+        on, ov = o.mesh_nodes(3)
+        assert np.array_equal(en, on) and np.array_equal(ev, ov)
+    assert np.abs(o.wall_hist(1)).sum() > 0, "no particle touched the cylinder"
+    assert len(o.mesh_contacts(3)["tag"]) > 0, "the piston touched nothing"
+    assert e.stats()["nbuilds"] == o.nbuilds
