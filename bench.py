@@ -285,7 +285,7 @@ def timed_window(eng, steps, dist, device, clocks=True):
     st1 = eng.stats()
     eng.set_profiling(False)
     cen1 = eng.census()
-    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_forward", "t_rebuild")}
+    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_pair_tail", "t_forward", "t_rebuild")}
     return {"ms": allmax(dist, ms), "clocks": clk, "cen": (cen0, cen1), "kt": kt,
             "npm": st1["n_pair_main"] - st0["n_pair_main"],
             "launches": st1["kernel_launches"] - st0["kernel_launches"],

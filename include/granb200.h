@@ -86,7 +86,7 @@ typedef struct {
     double time_pair, time_neigh, time_other;   /* device ms, cumulative    */
     long kernel_launches;        /* kernels launched by this context so far */
     /* per-kernel device time (ms, cumulative) while profiling is on */
-    double t_integrate, t_pair_reverse, t_pair_main, t_forward, t_rebuild;
+    double t_integrate, t_pair_tail, t_pair_main, t_forward, t_rebuild;
     long n_pair_main;            /* pair-pass launches timed                */
     long nsteps_rebuild;         /* steps that rebuilt the neighbour list   */
     int maxrev, maxmesh;         /* reverse-entry and mesh-slot capacities  */

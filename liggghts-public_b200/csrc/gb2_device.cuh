@@ -251,6 +251,19 @@ __device__ __forceinline__ flt8 ldg8f(const flt8 *p)
     return r;
 }
 
+// A 32-byte record copied to shared memory without passing through
+// registers (two 16-byte cp.async, L2 only); complete after cp_async_wait().
+// Each thread reads back only what it copied itself, so no barrier is needed.
+__device__ __forceinline__ void stage4(dbl4 *dst, const dbl4 *src)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n\t"
+                 "cp.async.cg.shared.global [%2], [%3], 16;" ::"r"(s),
+                 "l"(src), "r"(s + 16u), "l"((const char *)src + 16)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ bool touching(const dbl4 &a, const dbl4 &b)
 {
     const double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
@@ -382,98 +395,168 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long v, int s
     return ((unsigned long long)hi << 32) | lo;
 }
 
-__device__ __forceinline__ void mesh_wall_atom(const Dev &D, const MeshDev &M, int i, const dbl4 &p, const double v[3],
-                               const double w[3], double mass, int itype, bool upd, ContactOut &acc)
+// One candidate triangle t in contact with atom i (deltan <= 0): the body of
+// FixWallGran::post_force_mesh's loop -- FixContactHistoryMesh::handleContact
+// (slot lookup, new slot with the shear of a coplanar neighbour for face
+// contacts, or skip when a coplanar neighbour already holds the contact) and
+// the wall contact force.  keep/np: markAllContacts mask and npartner.
+static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t, const dbl4 &p, const double v[3],
+                                    const double w[3], double mass, int itype, bool upd, int nn,
+                                    unsigned long long &keep, int &np, ContactOut &acc)
 {
     const int cap = D.cap;
-    const int nn = M.tcnt[i];
-    if (nn == 0) return;
-    unsigned long long keep = 0ull;   // markAllContacts
     const double cs[3] = {p.x, p.y, p.z};
-    int np = M.snp[i];
-    for (int q = 0; q < nn; q++) {
-        const int t = M.tlist[q * cap + i];
-        const TriGeom &T = M.tri[t];
-        double delta[3], bary[3] = {0., 0., 0.};
-        int barysign = -1;
-        const double deltan = tri_sphere(T, p.w, cs, delta, barysign, 1e-8, bary);
-        if (deltan > D.cutneighmax) continue;
-        if (!(deltan <= 0)) continue;
-        const bool faceflag = (7 == barysign);
-        // FixContactHistoryMesh::handleContact
-        int slot = -1;
+    const TriGeom &T = M.tri[t];
+    double delta[3], bary[3] = {0., 0., 0.};
+    int barysign = -1;
+    const double deltan = tri_sphere(T, p.w, cs, delta, barysign, 1e-8, bary);
+    const bool faceflag = (7 == barysign);
+    int slot = -1;
+    for (int k = 0; k < nn; k++)
+        if (M.spartner[k * cap + i] == t) {
+            slot = k;
+            break;
+        }
+    if (slot >= 0) {
+        keep |= 1ull << slot;
+    } else {
+        if (faceflag) {
+            for (int k = 0; k < nn; k++) {
+                const int idp = M.spartner[k * cap + i];
+                if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) return;
+            }
+        }
+        int ic = -1;
         for (int k = 0; k < nn; k++)
-            if (M.spartner[k * cap + i] == t) {
-                slot = k;
+            if (-1 == M.spartner[k * cap + i]) {
+                ic = k;
                 break;
             }
-        if (slot >= 0) {
-            keep |= 1ull << slot;
-        } else {
-            bool skip = false;
-            if (faceflag) {
-                for (int k = 0; k < nn; k++) {
-                    const int idp = M.spartner[k * cap + i];
-                    if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) {
-                        skip = true;
-                        break;
-                    }
-                }
-            }
-            if (skip) continue;
-            int ic = -1;
-            for (int k = 0; k < nn; k++)
-                if (-1 == M.spartner[k * cap + i]) {
-                    ic = k;
-                    break;
-                }
-            if (ic < 0 || np >= nn) {
-                atomicOr(D.status, ST_MESH_INTERNAL);
-                continue;
-            }
-            M.spartner[ic * cap + i] = t;
-            keep |= 1ull << ic;
-            double h0 = 0.0, h1 = 0.0, h2 = 0.0;
-            np++;
-            if (faceflag) {
-                for (int k = 0; k < nn; k++) {
-                    const int tri = M.spartner[k * cap + i];
-                    if (tri >= 0 && tri != t && coplanar_node_neighs(M, tri, t)) {
-                        h0 = M.shist[(3 * k + 0) * cap + i];
-                        h1 = M.shist[(3 * k + 1) * cap + i];
-                        h2 = M.shist[(3 * k + 2) * cap + i];
-                    }
-                }
-            }
-            M.shist[(3 * ic + 0) * cap + i] = h0;
-            M.shist[(3 * ic + 1) * cap + i] = h1;
-            M.shist[(3 * ic + 2) * cap + i] = h2;
-            slot = ic;
+        if (ic < 0 || np >= nn) {
+            atomicOr(D.status, ST_MESH_INTERNAL);
+            return;
         }
-        double sh[3] = {M.shist[(3 * slot + 0) * cap + i], M.shist[(3 * slot + 1) * cap + i],
-                        M.shist[(3 * slot + 2) * cap + i]};
-        const double dvec[3] = {-delta[0], -delta[1], -delta[2]};
-        double vwall[3] = {0.0, 0.0, 0.0};
-        if (M.vnode) {   // moving mesh: barycentric node velocity (src/fix_wall_gran.cpp:992-996)
-            const double *vn = M.vnode + 9 * t;
-            for (int c = 0; c < 3; c++) vwall[c] = (bary[0] * vn[c] + bary[1] * vn[3 + c] + bary[2] * vn[6 + c]);
+        M.spartner[ic * cap + i] = t;
+        keep |= 1ull << ic;
+        double h0 = 0.0, h1 = 0.0, h2 = 0.0;
+        np++;
+        if (faceflag) {
+            for (int k = 0; k < nn; k++) {
+                const int tri = M.spartner[k * cap + i];
+                if (tri >= 0 && tri != t && coplanar_node_neighs(M, tri, t)) {
+                    h0 = M.shist[(3 * k + 0) * cap + i];
+                    h1 = M.shist[(3 * k + 1) * cap + i];
+                    h2 = M.shist[(3 * k + 2) * cap + i];
+                }
+            }
         }
-        wall_contact(mat(D, itype, M.wtype), dvec, -deltan, p.w, v, w, vwall, mass, sh, upd, D.dt, M.rolling != 0,
-                     D.tdamp != 0, acc);
-        M.shist[(3 * slot + 0) * cap + i] = sh[0];
-        M.shist[(3 * slot + 1) * cap + i] = sh[1];
-        M.shist[(3 * slot + 2) * cap + i] = sh[2];
+        M.shist[(3 * ic + 0) * cap + i] = h0;
+        M.shist[(3 * ic + 1) * cap + i] = h1;
+        M.shist[(3 * ic + 2) * cap + i] = h2;
+        slot = ic;
     }
-    // cleanUpContacts
-    for (int k = 0; k < nn; k++)
-        if (!((keep >> k) & 1ull)) {
-            if (M.spartner[k * cap + i] > -1) np--;
-            M.spartner[k * cap + i] = -1;
-            M.shist[(3 * k + 0) * cap + i] = 0.0;
-            M.shist[(3 * k + 1) * cap + i] = 0.0;
-            M.shist[(3 * k + 2) * cap + i] = 0.0;
+    double sh[3] = {M.shist[(3 * slot + 0) * cap + i], M.shist[(3 * slot + 1) * cap + i],
+                    M.shist[(3 * slot + 2) * cap + i]};
+    const double dvec[3] = {-delta[0], -delta[1], -delta[2]};
+    double vwall[3] = {0.0, 0.0, 0.0};
+    if (M.vnode) {   // moving mesh: barycentric node velocity (src/fix_wall_gran.cpp:992-996)
+        const double *vn = M.vnode + 9 * t;
+        for (int c = 0; c < 3; c++) vwall[c] = (bary[0] * vn[c] + bary[1] * vn[3 + c] + bary[2] * vn[6 + c]);
+    }
+    wall_contact(mat(D, itype, M.wtype), dvec, -deltan, p.w, v, w, vwall, mass, sh, upd, D.dt, M.rolling != 0,
+                 D.tdamp != 0, acc);
+    M.shist[(3 * slot + 0) * cap + i] = sh[0];
+    M.shist[(3 * slot + 1) * cap + i] = sh[1];
+    M.shist[(3 * slot + 2) * cap + i] = sh[2];
+}
+
+// FixWallGran::post_force_mesh for the atoms owned by the lanes of a warp
+// (own: lane holds atom i; acc is the owner's).  The sphere-triangle
+// distances of all candidates of the warp's atoms are independent of one
+// another and of the contact history, so they are evaluated one candidate
+// per lane (owner-major items, rounds of 32); each owner then handles its
+// candidates in contact (deltan <= 0) in ascending order with mesh_contact,
+// exactly as the sequential loop, and FixContactHistoryMesh::cleanUpContacts
+// clears the slots that lost their contact.  At most 64 candidates per atom.
+__device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, bool own, int i, const dbl4 &p,
+                                                const double v[3], const double w[3], double mass, int itype,
+                                                bool upd, ContactOut &acc)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int cap = D.cap;
+    const int nn = own ? M.tcnt[i] : 0;
+    int np = own ? M.snp[i] : 0;
+    const WarpItems it = warp_items_cnt(nn);
+    if (it.total == 0) return;
+    unsigned long long touch = 0ull;
+    for (int base = 0; base < it.total; base += 32) {
+        const int wq = base + lane;
+        const int L = item_owner(min(wq, it.total - 1), it.excl);
+        const int iL = __shfl_sync(FULL, i, L);
+        const int exL = __shfl_sync(FULL, it.excl, L);
+        const double px = __shfl_sync(FULL, p.x, L), py = __shfl_sync(FULL, p.y, L);
+        const double pz = __shfl_sync(FULL, p.z, L), pr = __shfl_sync(FULL, p.w, L);
+        bool hit = false;
+        if (wq < it.total) {
+            const double cs[3] = {px, py, pz};
+            double delta[3], bary[3] = {0., 0., 0.};
+            int barysign = -1;
+            const int t = M.tlist[(wq - exL) * cap + iL];
+            const double deltan = tri_sphere(M.tri[t], pr, cs, delta, barysign, 1e-8, bary);
+            hit = !(deltan > D.cutneighmax) && (deltan <= 0);
         }
-    M.snp[i] = np;
+        const unsigned bal = __ballot_sync(FULL, hit);
+        const int lo = max(it.excl, base), hi = min(it.excl + nn, base + 32);
+        if (lo < hi) {
+            const unsigned long long bits = (unsigned long long)(bal >> (lo - base)) & ((1ull << (hi - lo)) - 1ull);
+            touch |= bits << (lo - it.excl);
+        }
+    }
+    unsigned long long keep = 0ull;
+    for (unsigned long long m = touch; m; m &= m - 1ull) {
+        const int q = __ffsll((long long)m) - 1;
+        mesh_contact(D, M, i, M.tlist[q * cap + i], p, v, w, mass, itype, upd, nn, keep, np, acc);
+    }
+    __syncwarp();
+    // cleanUpContacts, one slot per lane (the slots of one atom are
+    // independent; npartner drops by the cleared slots that held a partner)
+    for (int base = 0; base < it.total; base += 32) {
+        const int wq = base + lane;
+        const int L = item_owner(min(wq, it.total - 1), it.excl);
+        const int iL = __shfl_sync(FULL, i, L);
+        const int exL = __shfl_sync(FULL, it.excl, L);
+        const unsigned long long keepL = shfl64(keep, L);
+        bool held = false;
+        if (wq < it.total) {
+            const int k = wq - exL;
+            if (!((keepL >> k) & 1ull)) {
+                held = M.spartner[k * cap + iL] > -1;
+                M.spartner[k * cap + iL] = -1;
+                M.shist[(3 * k + 0) * cap + iL] = 0.0;
+                M.shist[(3 * k + 1) * cap + iL] = 0.0;
+                M.shist[(3 * k + 2) * cap + iL] = 0.0;
+            }
+        }
+        const unsigned bal = __ballot_sync(FULL, held);
+        const int lo = max(it.excl, base), hi = min(it.excl + nn, base + 32);
+        if (lo < hi) np -= __popc((bal >> (lo - base)) & (unsigned)((1ull << (hi - lo)) - 1ull));
+    }
+    if (nn > 0) M.snp[i] = np;
+}
+
+// True when the atom's step is finished by the tail kernel: more than 64
+// entries on a side, a primitive wall that lists it, or mesh candidate
+// triangles.  The inputs change only at a neighbour build.
+__device__ __forceinline__ bool tail_atom(const Dev &D, int k, int nr, int nn)
+{
+    if (nr > 64 || nn > 64) return true;
+    for (int q = 0; q < D.nfix; q++) {
+        const FixDev &F = D.fix[q];
+        if (F.kind == FIX_WALL_PLANE && F.inlist[k]) return true;
+        if (F.kind == FIX_WALL_MESH && F.mesh.tcnt[k] != 0) return true;
+    }
+    return false;
 }
 
 // Cylinder<dim>::calcRadialDistance (src/primitive_wall_definitions.h:165)

@@ -128,11 +128,13 @@ struct gb2_ctx {
     int nlocal = 0, nghost = 0, nmax = 0, cap = 0;
     std::vector<double> h_radius;
     std::vector<int> h_type;
-    DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, fpart, tpart, xhold;
+    DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, tailf, tailt, xhold;
     bool split = false;           // GB2_PREC_SPLIT
     DBuf<flt8> kin, kin2;         // split precision: FP32 kinematics records (double-buffered like vel)
     DBuf<uint8_t> revs;
-    int minb = 4;                 // register-allocation target of the pair step kernel (blocks/SM)
+    int minb = 0;                 // register-allocation target of the pair step kernel (blocks/SM; 0: default)
+    int nsm = 148;                // SMs of the device
+    int tail_per_sm = 8;          // blocks of the tail kernel per SM (kTailAtoms atoms per warp)
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
     // steps queued ahead of the rebuild decision (see gb2_run)
     bool queue_ok = true;         // GB2_QUEUE_DEPTH=0 turns it off
@@ -143,7 +145,7 @@ struct gb2_ctx {
     cudaEvent_t qev[16] = {};
     DBuf<int> type, tag;
     int maxn = 16, maxr = 16, maxp = 16;
-    DBuf<int> nnum, nbr, flag, rnum, rev, pnum, ptag;
+    DBuf<int> nnum, nbr, flag, rnum, rev, pnum, ptag, tail;
     DBuf<int> type_s, tag_s, pnum_s, ptag_s;   // atom-sort shadows
     DBuf<double> phist_s;
     DBuf<double> hist, hist2, phist;
@@ -158,7 +160,7 @@ struct gb2_ctx {
     DBuf<unsigned> keys, keys2;
     DBuf<uint8_t> bflags;
     DBuf<char> cubtmp;
-    DBuf<int> dstatus, ddflag, dneed;
+    DBuf<int> dstatus, ddflag, dneed, dtailcnt;
     long ngrow = 0;
     int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel
     // neighbor
@@ -235,8 +237,10 @@ Dev make_dev(gb2_ctx *c)
     D.tag = c->tag.p;
     D.f = c->f.p;
     D.tq = c->tq.p;
-    D.fpart = c->fpart.p;
-    D.tpart = c->tpart.p;
+    D.tailf = c->tailf.p;
+    D.tailt = c->tailt.p;
+    D.tail = c->tail.p;
+    D.tailcnt = c->dtailcnt.p;
     D.xhold = c->xhold.p;
     D.maxn = c->maxn;
     D.nnum = c->nnum.p;
@@ -337,7 +341,7 @@ int clear_status(gb2_ctx *c)
 }
 
 // ---------------------------------------------------------------- profiling
-enum { PROF_INTEGRATE = 0, PROF_PAIR_REVERSE = 1, PROF_PAIR_MAIN = 2, PROF_FORWARD = 3, PROF_REBUILD = 4 };
+enum { PROF_INTEGRATE = 0, PROF_PAIR_TAIL = 1, PROF_PAIR_MAIN = 2, PROF_FORWARD = 3, PROF_REBUILD = 4 };
 
 int prof_begin(gb2_ctx *c, int cls, gb2_ctx::EvPair *out)
 {
@@ -978,29 +982,52 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
         if (nall > 0) k_make_kin<<<nblk(nall), kBlock, 0, c->st>>>(D2, nall);
         CKL();
     }
+    // atoms finished by the tail kernel until the next build
+    CK(cudaMemsetAsync(c->dtailcnt.p, 0, sizeof(int), c->st));
+    if (c->nlocal > 0) {
+        Dev D3 = make_dev(c);
+        k_tail_list<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D3);
+        CKL();
+    }
     return 0;
 }
 
 template <bool R, int MINB>
-void launch_step_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
+void launch_pair_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
     k_pair_step<R, MINB, false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
-void launch_step(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
+// The pair step kernel of one time step (every atom's pair sums; the
+// whole step for atoms without wall work).
+void launch_pair(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
     if (c->split) {
-        launch_step_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f);
+        launch_pair_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f);
         return;
     }
     // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
+    const int mb = c->minb ? c->minb : 5;
     if (c->P.rolling_cdt) {
-        if (c->minb == 6) launch_step_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else launch_step_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch_pair_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 5) launch_pair_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_pair_kernel<true, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
     } else {
-        if (c->minb == 6) launch_step_kernel<false, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
-        else launch_step_kernel<false, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch_pair_kernel<false, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 5) launch_pair_kernel<false, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
+        else launch_pair_kernel<false, 6>(c, D, shearupdate, integrate, fuse_next, store_f);
     }
+}
+
+// The tail kernel: the atoms with wall work or more than 64 entries on a side.
+void launch_tail(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
+{
+    const int tblocks = c->tail_per_sm * c->nsm;
+    if (c->split) launch_tail_split(D, tblocks, c->st, shearupdate, integrate, fuse_next, store_f);
+    else if (c->P.rolling_cdt)
+        k_pair_tail<true, false><<<tblocks, kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    else
+        k_pair_tail<false, false><<<tblocks, kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
 int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int store_f)
@@ -1009,7 +1036,11 @@ int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int stor
     Dev D = make_dev(c);
     gb2_ctx::EvPair e;
     if (prof_begin(c, PROF_PAIR_MAIN, &e)) return GB2_ERR_CUDA;
-    launch_step(c, D, shearupdate, integrate, fuse_next, store_f);
+    launch_pair(c, D, shearupdate, integrate, fuse_next, store_f);
+    CKL();
+    if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    if (prof_begin(c, PROF_PAIR_TAIL, &e)) return GB2_ERR_CUDA;
+    launch_tail(c, D, shearupdate, integrate, fuse_next, store_f);
     CKL();
     if (prof_end(c, &e)) return GB2_ERR_CUDA;
     if (shearupdate) c->hist.swap(c->hist2);
@@ -1112,6 +1143,7 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     c->split = p->precision == GB2_PREC_SPLIT;
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
     if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
+    if (const char *tb = std::getenv("GB2_TAIL_BLOCKS")) c->tail_per_sm = std::max(1, std::atoi(tb));
     if (const char *qd = std::getenv("GB2_QUEUE_DEPTH")) {
         c->queue_depth = std::min(std::max(std::atoi(qd), 0), 15);
         c->queue_ok = c->queue_depth > 0;
@@ -1124,8 +1156,11 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
         c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess || c->dstop.alloc(1) != cudaSuccess ||
-        cudaMallocHost(&c->h_stop, 16 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
+        c->dtailcnt.alloc(1) != cudaSuccess || cudaMallocHost(&c->h_stop, 16 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->dtailcnt.p, 0, sizeof(int)) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess ||
         cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         return GB2_ERR_CUDA;
@@ -1223,8 +1258,9 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     const size_t cap = c->cap;
     CK(c->f.alloc(cap));
     CK(c->tq.alloc(cap));
-    CK(c->fpart.alloc(cap));
-    CK(c->tpart.alloc(cap));
+    CK(c->tailf.alloc(cap));
+    CK(c->tailt.alloc(cap));
+    CK(c->tail.alloc(cap));
     CK(c->xhold.alloc(cap));
     CK(c->nnum.alloc(cap));
     CK(c->rnum.alloc(cap));
@@ -1862,11 +1898,11 @@ int gb2_get_stats(gb2_ctx *c, gb2_stats *s)
     s->maxpartner = c->maxp;
     s->kernel_launches = c->launches;
     s->t_integrate = c->prof_ms[PROF_INTEGRATE];
-    s->t_pair_reverse = c->prof_ms[PROF_PAIR_REVERSE];
+    s->t_pair_tail = c->prof_ms[PROF_PAIR_TAIL];
     s->t_pair_main = c->prof_ms[PROF_PAIR_MAIN];
     s->t_forward = c->prof_ms[PROF_FORWARD];
     s->t_rebuild = c->prof_ms[PROF_REBUILD];
-    s->time_pair = s->t_pair_reverse + s->t_pair_main;
+    s->time_pair = s->t_pair_tail + s->t_pair_main;
     s->time_neigh = s->t_rebuild;
     s->time_other = s->t_integrate + s->t_forward;
     s->n_pair_main = c->n_pair_main;

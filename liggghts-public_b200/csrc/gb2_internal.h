@@ -7,7 +7,9 @@
 //     omg  {wx, wy, wz, -}        type, tag (int32)
 //   per owned atom:
 //     f, tq {., ., ., -}          force / torque of the last step
-//     fpart, tpart                reverse-entry partial sums (pair pass A)
+//     tail[w]                     atoms finished by the tail kernel (wall candidates or
+//                                 more than 64 entries on a side), listed at each build
+//     tailf, tailt                their pair sums, left by the pair step kernel
 //     xhold {x, y, z, -}          positions at the last neighbour build
 //   half neighbour list, slot-major so a warp reads consecutive atoms
 //   (capacity maxn slots per owned atom, stride `cap`):
@@ -115,7 +117,8 @@ struct Dev {
     dbl4 *pos_out, *vel_out, *omg_out;   // integrate targets (double buffer: pass B reads neighbours' state)
     flt8 *kin, *kin_out;                 // split precision only (null in the FP64 path)
     int *type, *tag;
-    dbl4 *f, *tq, *fpart, *tpart, *xhold;
+    dbl4 *f, *tq, *tailf, *tailt, *xhold;
+    int *tail, *tailcnt;   // tail-kernel atom list and its length
     // half list
     int maxn;
     int *nnum, *nbr, *flag;
@@ -166,8 +169,10 @@ struct MeshTopo {
 bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, double precision, MeshTopo &out,
                          std::string &err);
 // split-precision pair step (gb2_split.cu)
-void launch_step_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
+void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
                        int fuse_next, int store_f);
+void launch_tail_split(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
+                       int store_f);
 bool tri_neighbuild_host(const TriGeom &T, double rSphere, const double *c, double treshold);
 
 }  // namespace gb2

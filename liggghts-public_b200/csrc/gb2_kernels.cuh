@@ -767,5 +767,14 @@ __global__ void k_census(Dev D, unsigned long long *cnt)
     if (mt) atomicAdd(&cnt[6], mt);
 }
 
+// The tail kernel's atom list, after each neighbour build (count zeroed
+// before the launch; the order of the list does not affect any result).
+__global__ void k_tail_list(Dev D)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.nlocal) return;
+    if (tail_atom(D, k, D.rnum[k], D.nnum[k])) D.tail[atomicAdd(D.tailcnt, 1)] = k;
+}
+
 }  // namespace gb2
 

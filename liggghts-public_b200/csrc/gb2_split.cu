@@ -18,16 +18,26 @@ static void launch(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, 
     k_pair_step<R, MINB, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
-void launch_step_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
+void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
                        int fuse_next, int store_f)
 {
+    const int mb = minb ? minb : 6;
     if (D.rolling) {
-        if (minb == 6) launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 5) launch<true, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
     } else {
-        if (minb == 6) launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 5) launch<false, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
     }
+}
+
+void launch_tail_split(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
+                       int store_f)
+{
+    if (D.rolling) k_pair_tail<true, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    else k_pair_tail<false, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
 }  // namespace gb2

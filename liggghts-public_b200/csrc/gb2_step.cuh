@@ -231,37 +231,34 @@ __device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const 
     }
 }
 
-// The per-atom end of the step once the pair sums are in acc: serial atoms,
-// carried shear of slots that stopped touching, the post_force fixes in
-// definition order, FixNVESphere::final_integrate and -- when the run
-// continues -- the next step's initial_integrate with the displacement test.
-template <bool ROLLING, bool SPLIT>
-__device__ __forceinline__ void atom_tail(const Dev &D, int k, const dbl4 &pk, dbl4 vi4, dbl4 wi4, const dbl4 &hold,
-                                          unsigned long long prevm, int tk, int nr, int nn, unsigned long long mown,
-                                          bool serial, bool upd, int integrate, int fuse_next, int store_f,
-                                          ContactOut &acc)
+// Shear of own slots that stopped touching this step is carried into the
+// write buffer, and the touching mask is kept for the next step.
+__device__ __forceinline__ void atom_hist_tail(const Dev &D, int k, unsigned long long prevm,
+                                               unsigned long long mown, bool upd)
 {
+    if (!upd) return;
     const int cap = D.cap;
-    const double vk[3] = {vi4.x, vi4.y, vi4.z}, wk[3] = {wi4.x, wi4.y, wi4.z};
-    if (serial) {
-        serial_atom<ROLLING>(D, k, pk, vi4, wi4, tk, nr, nn, upd, acc);
-    } else if (upd) {
-        // slots that stopped touching this step: carry their shear into the write buffer
-        unsigned long long stopped = prevm & ~mown;
-        while (stopped) {
-            const int s = __ffsll((long long)stopped) - 1;
-            stopped &= stopped - 1ull;
-            D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
-            D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
-            D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
-        }
+    unsigned long long stopped = prevm & ~mown;
+    while (stopped) {
+        const int s = __ffsll((long long)stopped) - 1;
+        stopped &= stopped - 1ull;
+        D.hist_out[(3 * s + 0) * cap + k] = D.hist[(3 * s + 0) * cap + k];
+        D.hist_out[(3 * s + 1) * cap + k] = D.hist[(3 * s + 1) * cap + k];
+        D.hist_out[(3 * s + 2) * cap + k] = D.hist[(3 * s + 2) * cap + k];
     }
-    if (upd) D.prevmask[k] = serial ? ~0ull : mown;
-    const int i = k;
-    const dbl4 pi = pk;
-    const int ti = tk;
-    const double *vi = vk, *wi = wk;
-    // post_force fixes in definition order
+    D.prevmask[k] = mown;
+}
+
+// The per-atom end of the step once the pair sums are in acc, for an atom
+// without wall or serial work (tail_atom is false): of the post_force
+// fixes only gravity acts, then FixNVESphere::final_integrate and -- when
+// the run continues -- the next step's initial_integrate with the
+// displacement test.
+template <bool SPLIT>
+__device__ __forceinline__ void atom_fix_tail(const Dev &D, int k, const dbl4 &pk, dbl4 vi4, dbl4 wi4,
+                                              const dbl4 &hold, int integrate, int fuse_next, int store_f,
+                                              ContactOut &acc)
+{
     for (int q = 0; q < D.nfix; q++) {
         const FixDev &F = D.fix[q];
         if (F.kind == FIX_GRAVITY) {
@@ -269,13 +266,9 @@ __device__ __forceinline__ void atom_tail(const Dev &D, int k, const dbl4 &pk, d
             acc.F[0] += massone * F.acc[0];
             acc.F[1] += massone * F.acc[1];
             acc.F[2] += massone * F.acc[2];
-        } else if (F.kind == FIX_WALL_PLANE) {
-            if (F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
-        } else if (F.kind == FIX_WALL_MESH) {
-            mesh_wall_atom(D, F.mesh, i, pi, vi, wi, vi4.w, ti, upd, acc);
         }
     }
-    atom_store_integrate<SPLIT>(D, i, pi, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
+    atom_store_integrate<SPLIT>(D, k, pk, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
 }
 
 // The pair step: PairGran::compute for one owned atom k with its j-side
@@ -304,6 +297,10 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
 {
     using Real = typename std::conditional<SPLIT, float, double>::type;
     __shared__ Real sres[4][32][6];
+    // the atom's records that only the tail needs (velocity, angular
+    // velocity, position at the last rebuild) wait here, not in registers,
+    // while the screening and the contact rounds run
+    __shared__ __align__(16) dbl4 stail[3][128];
     if (step_cancelled(D)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -311,24 +308,27 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     const bool valid = k < D.nlocal;
     const int cap = D.cap;
     const bool upd = shearupdate != 0;
-    dbl4 pk, vi4, wi4, hold;
+    dbl4 pk;
     unsigned long long prevm = 0ull;
     int nr = 0, nn = 0, tk = 0;
     unsigned long long mrev = 0ull, mown = 0ull;
-    bool serial = false;
+    bool serial = false, tail = false;
     if (valid) {
         // the atom's own records, including those only the tail needs, are
         // requested first so their latency overlaps the screening
+        stage4(&stail[0][threadIdx.x], &D.vel[k]);
+        stage4(&stail[1][threadIdx.x], &D.omg[k]);
+        if (fuse_next) stage4(&stail[2][threadIdx.x], &D.xhold[k]);
         pk = D.pos[k];
         nr = D.rnum[k];
         nn = D.nnum[k];
-        vi4 = D.vel[k];
-        wi4 = D.omg[k];
         tk = D.type[k];
-        if (fuse_next) hold = D.xhold[k];
-        if (upd) prevm = D.prevmask[k];
         serial = nr > 64 || nn > 64;
-        if (!serial) screen_both(D, k, nr, nn, pk, mrev, mown);
+        tail = tail_atom(D, k, nr, nn);
+        if (!serial) {
+            if (upd) prevm = D.prevmask[k];
+            screen_both(D, k, nr, nn, pk, mrev, mown);
+        }
     }
     // FP64 path: plain in-order sums (bit-exact).  Split path: FP32 sums of
     // the FP32 pair contributions with Kahan compensation kc.
@@ -374,8 +374,86 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     ContactOut acc;
     pair_total<SPLIT>(as, kc, acc);
     if (!valid) return;
-    atom_tail<ROLLING, SPLIT>(D, k, pk, vi4, wi4, hold, prevm, tk, nr, nn, mown, serial, upd, integrate, fuse_next,
-                              store_f, acc);
+    cp_async_wait();
+    if (!serial) atom_hist_tail(D, k, prevm, mown, upd);
+    if (tail) {   // finished by k_pair_tail from these pair sums
+        D.tailf[k] = dbl4{acc.F[0], acc.F[1], acc.F[2], 0.0};
+        D.tailt[k] = dbl4{acc.T[0], acc.T[1], acc.T[2], 0.0};
+        return;
+    }
+    const dbl4 vi4 = stail[0][threadIdx.x], wi4 = stail[1][threadIdx.x];
+    dbl4 hold;
+    if (fuse_next) hold = stail[2][threadIdx.x];
+    atom_fix_tail<SPLIT>(D, k, pk, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
+}
+
+// Atoms per warp of the tail kernel: lanes 0..kTailAtoms-1 own one atom
+// each, all 32 lanes share the evaluation of their mesh candidates.
+#ifndef GB2_TAIL_ATOMS
+#define GB2_TAIL_ATOMS 8
+#endif
+constexpr int kTailAtoms = GB2_TAIL_ATOMS;
+
+// Second kernel of the step: the atoms listed at the last neighbour build
+// as having wall candidates or more than 64 entries on a side, finished
+// from the pair sums k_pair_step left in tailf/tailt (zero for an atom with
+// more than 64 entries on a side, whose contacts are evaluated here in the
+// reference order).  The post_force fixes follow in definition order, then
+// final_integrate and the fused next initial_integrate.  Every atom's end
+// of step touches only that atom's records, so the split into two kernels
+// leaves each result bit for bit as in one.
+template <bool ROLLING, bool SPLIT>
+__global__ void __launch_bounds__(128) k_pair_tail(Dev D, int shearupdate, int integrate, int fuse_next, int store_f)
+{
+    if (step_cancelled(D)) return;
+    const int n = *D.tailcnt;
+    const bool upd = shearupdate != 0;
+    const int lane = threadIdx.x & 31;
+    const int nwarp = gridDim.x * (blockDim.x >> 5);
+    for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kTailAtoms; base < n;
+         base += nwarp * kTailAtoms) {
+        const bool own = lane < kTailAtoms && base + lane < n;
+        int i = 0, ti = 0;
+        ContactOut acc;
+        dbl4 pi, vi4, wi4, hold;
+        pi = vi4 = wi4 = hold = dbl4{0.0, 0.0, 0.0, 0.0};
+        for (int c = 0; c < 3; c++) acc.F[c] = acc.T[c] = 0.0;
+        if (own) {
+            i = D.tail[base + lane];
+            const dbl4 F4 = D.tailf[i], T4 = D.tailt[i];
+            acc.F[0] = F4.x;
+            acc.F[1] = F4.y;
+            acc.F[2] = F4.z;
+            acc.T[0] = T4.x;
+            acc.T[1] = T4.y;
+            acc.T[2] = T4.z;
+            pi = D.pos[i];
+            vi4 = D.vel[i];
+            wi4 = D.omg[i];
+            if (fuse_next) hold = D.xhold[i];
+            ti = D.type[i];
+            const int nr = D.rnum[i], nn = D.nnum[i];
+            if (nr > 64 || nn > 64) {
+                serial_atom<ROLLING>(D, i, pi, vi4, wi4, ti, nr, nn, upd, acc);
+                if (upd) D.prevmask[i] = ~0ull;   // every own slot written this step
+            }
+        }
+        const double vi[3] = {vi4.x, vi4.y, vi4.z}, wi[3] = {wi4.x, wi4.y, wi4.z};
+        for (int q = 0; q < D.nfix; q++) {
+            const FixDev &F = D.fix[q];
+            if (F.kind == FIX_GRAVITY) {
+                const double massone = vi4.w * 1.;
+                acc.F[0] += massone * F.acc[0];
+                acc.F[1] += massone * F.acc[1];
+                acc.F[2] += massone * F.acc[2];
+            } else if (F.kind == FIX_WALL_PLANE) {
+                if (own && F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
+            } else if (F.kind == FIX_WALL_MESH) {
+                mesh_wall_items(D, F.mesh, own, i, pi, vi, wi, vi4.w, ti, upd, acc);
+            }
+        }
+        if (own) atom_store_integrate<SPLIT>(D, i, pi, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
+    }
 }
 
 }  // namespace gb2

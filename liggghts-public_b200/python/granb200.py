@@ -69,7 +69,7 @@ class Stats(ctypes.Structure):
         ("time_other", ctypes.c_double),
         ("kernel_launches", ctypes.c_long),
         ("t_integrate", ctypes.c_double),
-        ("t_pair_reverse", ctypes.c_double),
+        ("t_pair_tail", ctypes.c_double),
         ("t_pair_main", ctypes.c_double),
         ("t_forward", ctypes.c_double),
         ("t_rebuild", ctypes.c_double),
