@@ -399,9 +399,10 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long v, int s
 // FixWallGran::post_force_mesh's loop -- FixContactHistoryMesh::handleContact
 // (slot lookup, new slot with the shear of a coplanar neighbour for face
 // contacts, or skip when a coplanar neighbour already holds the contact) and
-// the wall contact force.  keep/np: markAllContacts mask and npartner.
+// the wall contact force.  keep/np: markAllContacts mask and npartner; sp:
+// the atom's slot partners (a shared-memory copy of spartner, kept in step).
 static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t, const dbl4 &p, const double v[3],
-                                    const double w[3], double mass, int itype, bool upd, int nn,
+                                    const double w[3], double mass, int itype, bool upd, int nn, int *sp,
                                     unsigned long long &keep, int &np, ContactOut &acc)
 {
     const int cap = D.cap;
@@ -413,7 +414,7 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
     const bool faceflag = (7 == barysign);
     int slot = -1;
     for (int k = 0; k < nn; k++)
-        if (M.spartner[k * cap + i] == t) {
+        if (sp[k] == t) {
             slot = k;
             break;
         }
@@ -422,13 +423,13 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
     } else {
         if (faceflag) {
             for (int k = 0; k < nn; k++) {
-                const int idp = M.spartner[k * cap + i];
+                const int idp = sp[k];
                 if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) return;
             }
         }
         int ic = -1;
         for (int k = 0; k < nn; k++)
-            if (-1 == M.spartner[k * cap + i]) {
+            if (-1 == sp[k]) {
                 ic = k;
                 break;
             }
@@ -436,13 +437,14 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
             atomicOr(D.status, ST_MESH_INTERNAL);
             return;
         }
+        sp[ic] = t;
         M.spartner[ic * cap + i] = t;
         keep |= 1ull << ic;
         double h0 = 0.0, h1 = 0.0, h2 = 0.0;
         np++;
         if (faceflag) {
             for (int k = 0; k < nn; k++) {
-                const int tri = M.spartner[k * cap + i];
+                const int tri = sp[k];
                 if (tri >= 0 && tri != t && coplanar_node_neighs(M, tri, t)) {
                     h0 = M.shist[(3 * k + 0) * cap + i];
                     h1 = M.shist[(3 * k + 1) * cap + i];
@@ -478,9 +480,13 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
 // candidates in contact (deltan <= 0) in ascending order with mesh_contact,
 // exactly as the sequential loop, and FixContactHistoryMesh::cleanUpContacts
 // clears the slots that lost their contact.  At most 64 candidates per atom.
+//
+// sp: shared-memory scratch of the warp (at least kTailAtoms * 64 ints) for
+// the slot partners of its atoms, loaded with the candidates (one slot per
+// candidate item) so the slot searches of mesh_contact read shared memory.
 __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, bool own, int i, const dbl4 &p,
                                                 const double v[3], const double w[3], double mass, int itype,
-                                                bool upd, ContactOut &acc)
+                                                bool upd, int *sp, ContactOut &acc)
 {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -503,6 +509,7 @@ __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, 
             double delta[3], bary[3] = {0., 0., 0.};
             int barysign = -1;
             const int t = M.tlist[(wq - exL) * cap + iL];
+            sp[wq] = M.spartner[(wq - exL) * cap + iL];
             const double deltan = tri_sphere(M.tri[t], pr, cs, delta, barysign, 1e-8, bary);
             hit = !(deltan > D.cutneighmax) && (deltan <= 0);
         }
@@ -513,10 +520,11 @@ __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, 
             touch |= bits << (lo - it.excl);
         }
     }
+    __syncwarp();
     unsigned long long keep = 0ull;
     for (unsigned long long m = touch; m; m &= m - 1ull) {
         const int q = __ffsll((long long)m) - 1;
-        mesh_contact(D, M, i, M.tlist[q * cap + i], p, v, w, mass, itype, upd, nn, keep, np, acc);
+        mesh_contact(D, M, i, M.tlist[q * cap + i], p, v, w, mass, itype, upd, nn, sp + it.excl, keep, np, acc);
     }
     __syncwarp();
     // cleanUpContacts, one slot per lane (the slots of one atom are
@@ -531,7 +539,7 @@ __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, 
         if (wq < it.total) {
             const int k = wq - exL;
             if (!((keepL >> k) & 1ull)) {
-                held = M.spartner[k * cap + iL] > -1;
+                held = sp[wq] > -1;
                 M.spartner[k * cap + iL] = -1;
                 M.shist[(3 * k + 0) * cap + iL] = 0.0;
                 M.shist[(3 * k + 1) * cap + iL] = 0.0;

@@ -403,8 +403,10 @@ constexpr int kTailAtoms = GB2_TAIL_ATOMS;
 // of step touches only that atom's records, so the split into two kernels
 // leaves each result bit for bit as in one.
 template <bool ROLLING, bool SPLIT>
-__global__ void __launch_bounds__(128) k_pair_tail(Dev D, int shearupdate, int integrate, int fuse_next, int store_f)
+__global__ void __launch_bounds__(128, 4) k_pair_tail(Dev D, int shearupdate, int integrate, int fuse_next,
+                                                      int store_f)
 {
+    __shared__ int s_sp[4][kTailAtoms * 64];   // slot partners of the warp's atoms (mesh walls)
     if (step_cancelled(D)) return;
     const int n = *D.tailcnt;
     const bool upd = shearupdate != 0;
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(128) k_pair_tail(Dev D, int shearupdate, int i
             } else if (F.kind == FIX_WALL_PLANE) {
                 if (own && F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
             } else if (F.kind == FIX_WALL_MESH) {
-                mesh_wall_items(D, F.mesh, own, i, pi, vi, wi, vi4.w, ti, upd, acc);
+                mesh_wall_items(D, F.mesh, own, i, pi, vi, wi, vi4.w, ti, upd, s_sp[threadIdx.x >> 5], acc);
             }
         }
         if (own) atom_store_integrate<SPLIT>(D, i, pi, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
