@@ -310,15 +310,22 @@ __device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn,
 {
     const int cap = D.cap;
     const int n = max(nr, nn);
+    // the indices of the next pair of entries are requested while this
+    // pair's records are in flight (one dependent round trip per pair)
+    int a0 = (0 < nr) ? ld_stream(&D.rev[k]) : k;
+    int a1 = (1 < nr) ? ld_stream(&D.rev[cap + k]) : k;
+    int b0 = (0 < nn) ? ld_stream(&D.nbr[k]) : k;
+    int b1 = (1 < nn) ? ld_stream(&D.nbr[cap + k]) : k;
     for (int t = 0; t < n; t += 2) {
-        const int a0 = (t < nr) ? ld_stream(&D.rev[t * cap + k]) : k;
-        const int a1 = (t + 1 < nr) ? ld_stream(&D.rev[(t + 1) * cap + k]) : k;
-        const int b0 = (t < nn) ? ld_stream(&D.nbr[t * cap + k]) : k;
-        const int b1 = (t + 1 < nn) ? ld_stream(&D.nbr[(t + 1) * cap + k]) : k;
         const dbl4 qa0 = ldg4(&D.pos[a0]);
         const dbl4 qa1 = ldg4(&D.pos[a1]);
         const dbl4 qb0 = ldg4(&D.pos[b0]);
         const dbl4 qb1 = ldg4(&D.pos[b1]);
+        const int u = t + 2;
+        a0 = (u < nr) ? ld_stream(&D.rev[u * cap + k]) : k;
+        a1 = (u + 1 < nr) ? ld_stream(&D.rev[(u + 1) * cap + k]) : k;
+        b0 = (u < nn) ? ld_stream(&D.nbr[u * cap + k]) : k;
+        b1 = (u + 1 < nn) ? ld_stream(&D.nbr[(u + 1) * cap + k]) : k;
         if (t < nr && touching(pk, qa0)) mrev |= 1ull << t;
         if (t + 1 < nr && touching(pk, qa1)) mrev |= 1ull << (t + 1);
         if (t < nn && touching(pk, qb0)) mown |= 1ull << t;

@@ -21,15 +21,19 @@ static void launch(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, 
 void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
                        int fuse_next, int store_f)
 {
-    const int mb = minb ? minb : 6;
+    const int mb = minb ? minb : 7;
     if (D.rolling) {
         if (mb == 4) launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch<true, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 6) launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 7) launch<true, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<true, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
     } else {
         if (mb == 4) launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch<false, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 6) launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else if (mb == 7) launch<false, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        else launch<false, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
     }
 }
 
