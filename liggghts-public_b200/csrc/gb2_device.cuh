@@ -333,30 +333,6 @@ __device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn,
     }
 }
 
-// Screening of n <= 64 list entries idx[r*cap + k]: four index loads, then
-// four independent neighbour-record gathers, then the four distance tests,
-// so a thread keeps several loads in flight.  Returns the touching mask.
-__device__ __forceinline__ unsigned long long screen_entries(const int *__restrict__ idx, int cap, int k, int n,
-                                                            const dbl4 &pk, const dbl4 *__restrict__ pos)
-{
-    unsigned long long m = 0ull;
-    for (int r0 = 0; r0 < n; r0 += 4) {
-        const int j0 = __ldg(&idx[min(r0 + 0, n - 1) * cap + k]);
-        const int j1 = __ldg(&idx[min(r0 + 1, n - 1) * cap + k]);
-        const int j2 = __ldg(&idx[min(r0 + 2, n - 1) * cap + k]);
-        const int j3 = __ldg(&idx[min(r0 + 3, n - 1) * cap + k]);
-        const dbl4 q0 = ldg4(&pos[j0]);
-        const dbl4 q1 = ldg4(&pos[j1]);
-        const dbl4 q2 = ldg4(&pos[j2]);
-        const dbl4 q3 = ldg4(&pos[j3]);
-        if (touching(pk, q0)) m |= 1ull << r0;
-        if (r0 + 1 < n && touching(pk, q1)) m |= 1ull << (r0 + 1);
-        if (r0 + 2 < n && touching(pk, q2)) m |= 1ull << (r0 + 2);
-        if (r0 + 3 < n && touching(pk, q3)) m |= 1ull << (r0 + 3);
-    }
-    return m;
-}
-
 __device__ __forceinline__ WarpItems warp_items_cnt(int cnt)
 {
     const unsigned FULL = 0xffffffffu;
