@@ -378,13 +378,38 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long v, int s
     return ((unsigned long long)hi << 32) | lo;
 }
 
+// Wall-contact records: the force and torque one wall contact adds to its
+// atom, kept (shared memory) until the pair sums they must follow are
+// available.  A record starts from negative zeros, so -0.0 + x == x for
+// every x (signed zeros included) and adding the record later is the same
+// operation as adding the contact force in place.
+constexpr int kWallRec = 4;   // records per atom
+typedef double WallRec[6];
+
+__device__ __forceinline__ ContactOut wall_record_zero()
+{
+    ContactOut o;
+    for (int c = 0; c < 3; c++) o.F[c] = o.T[c] = -0.0;
+    return o;
+}
+
+__device__ __forceinline__ void wall_record_put(WallRec *rec, int &n, const ContactOut &o)
+{
+    for (int c = 0; c < 3; c++) {
+        rec[n][c] = o.F[c];
+        rec[n][3 + c] = o.T[c];
+    }
+    n++;
+}
+
 // One candidate triangle t in contact with atom i (deltan <= 0): the body of
 // FixWallGran::post_force_mesh's loop -- FixContactHistoryMesh::handleContact
 // (slot lookup, new slot with the shear of a coplanar neighbour for face
 // contacts, or skip when a coplanar neighbour already holds the contact) and
 // the wall contact force.  keep/np: markAllContacts mask and npartner; sp:
 // the atom's slot partners (a shared-memory copy of spartner, kept in step).
-static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t, const dbl4 &p, const double v[3],
+// Returns true when the contact force was added to acc.
+static __device__ bool mesh_contact(const Dev &D, const MeshDev &M, int i, int t, const dbl4 &p, const double v[3],
                                     const double w[3], double mass, int itype, bool upd, int nn, int *sp,
                                     unsigned long long &keep, int &np, ContactOut &acc)
 {
@@ -407,7 +432,7 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
         if (faceflag) {
             for (int k = 0; k < nn; k++) {
                 const int idp = sp[k];
-                if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) return;
+                if (idp >= 0 && idp != t && coplanar_node_neighs(M, idp, t) && ((keep >> k) & 1ull)) return false;
             }
         }
         int ic = -1;
@@ -418,7 +443,7 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
             }
         if (ic < 0 || np >= nn) {
             atomicOr(D.status, ST_MESH_INTERNAL);
-            return;
+            return false;
         }
         sp[ic] = t;
         M.spartner[ic * cap + i] = t;
@@ -453,6 +478,7 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
     M.shist[(3 * slot + 0) * cap + i] = sh[0];
     M.shist[(3 * slot + 1) * cap + i] = sh[1];
     M.shist[(3 * slot + 2) * cap + i] = sh[2];
+    return true;
 }
 
 // FixWallGran::post_force_mesh for the atoms owned by the lanes of a warp
@@ -467,9 +493,16 @@ static __device__ void mesh_contact(const Dev &D, const MeshDev &M, int i, int t
 // sp: shared-memory scratch of the warp (at least kTailAtoms * 64 ints) for
 // the slot partners of its atoms, loaded with the candidates (one slot per
 // candidate item) so the slot searches of mesh_contact read shared memory.
+//
+// REC: each contact's force goes to the owner's records (rec, nrec) instead
+// of acc; an owner with more candidates in contact than records left is
+// dropped before anything of it changes (recok cleared) and is handled
+// later with REC=false.
+template <bool REC>
 __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, bool own, int i, const dbl4 &p,
                                                 const double v[3], const double w[3], double mass, int itype,
-                                                bool upd, int *sp, ContactOut &acc)
+                                                bool upd, int *sp, ContactOut &acc, WallRec *rec = nullptr,
+                                                int *nrec = nullptr, bool *recok = nullptr)
 {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -504,10 +537,26 @@ __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, 
         }
     }
     __syncwarp();
-    unsigned long long keep = 0ull;
-    for (unsigned long long m = touch; m; m &= m - 1ull) {
-        const int q = __ffsll((long long)m) - 1;
-        mesh_contact(D, M, i, M.tlist[q * cap + i], p, v, w, mass, itype, upd, nn, sp + it.excl, keep, np, acc);
+    bool act = nn > 0;
+    if constexpr (REC) {
+        if (act && *nrec + __popcll(touch) > kWallRec) {
+            act = false;
+            *recok = false;
+        }
+    }
+    unsigned long long keep = act ? 0ull : ~0ull;   // an owner left for later keeps every slot here
+    if (act) {
+        for (unsigned long long m = touch; m; m &= m - 1ull) {
+            const int q = __ffsll((long long)m) - 1;
+            const int t = M.tlist[q * cap + i];
+            if constexpr (REC) {
+                ContactOut o = wall_record_zero();
+                if (mesh_contact(D, M, i, t, p, v, w, mass, itype, upd, nn, sp + it.excl, keep, np, o))
+                    wall_record_put(rec, *nrec, o);
+            } else {
+                mesh_contact(D, M, i, t, p, v, w, mass, itype, upd, nn, sp + it.excl, keep, np, acc);
+            }
+        }
     }
     __syncwarp();
     // cleanUpContacts, one slot per lane (the slots of one atom are
@@ -533,7 +582,7 @@ __device__ __forceinline__ void mesh_wall_items(const Dev &D, const MeshDev &M, 
         const int lo = max(it.excl, base), hi = min(it.excl + nn, base + 32);
         if (lo < hi) np -= __popc((bal >> (lo - base)) & (unsigned)((1ull << (hi - lo)) - 1ull));
     }
-    if (nn > 0) M.snp[i] = np;
+    if (act) M.snp[i] = np;
 }
 
 // True when the atom's step is finished by the tail kernel: more than 64
@@ -563,7 +612,8 @@ __device__ __forceinline__ double cyl_radial(const FixDev &F, const dbl4 &p, dou
 // FixWallGran::post_force_primitive for one atom in the plane's neighbour
 // list (src/fix_wall_gran.cpp:1024-1148, Plane<dim>::resolveContact
 // src/primitive_wall_definitions.h:133)
-__device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, int i, const dbl4 &pi, const double *vi,
+// Returns true when the contact force was added to acc.
+__device__ __forceinline__ bool plane_wall_atom(const Dev &D, const FixDev &F, int i, const dbl4 &pi, const double *vi,
                                              const double *wi, double mass, int ti, bool upd, ContactOut &acc)
 {
     const int cap = D.cap;
@@ -601,7 +651,7 @@ __device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, i
         d[1] = F.dim == 1 ? -delta_d : -0.;
         d[2] = F.dim == 2 ? -delta_d : -0.;
     }
-    if (deltan > D.cutneighmax) return;
+    if (deltan > D.cutneighmax) return false;
     if (deltan <= 0) {
         double sh[3] = {F.whist[0 * cap + i], F.whist[1 * cap + i], F.whist[2 * cap + i]};
         const double vwall[3] = {0., 0., 0.};
@@ -610,11 +660,12 @@ __device__ __forceinline__ void plane_wall_atom(const Dev &D, const FixDev &F, i
         F.whist[0 * cap + i] = sh[0];
         F.whist[1 * cap + i] = sh[1];
         F.whist[2 * cap + i] = sh[2];
-    } else {
-        F.whist[0 * cap + i] = 0.0;
-        F.whist[1 * cap + i] = 0.0;
-        F.whist[2 * cap + i] = 0.0;
+        return true;
     }
+    F.whist[0 * cap + i] = 0.0;
+    F.whist[1 * cap + i] = 0.0;
+    F.whist[2 * cap + i] = 0.0;
+    return false;
 }
 
 }  // namespace gb2

@@ -1025,9 +1025,9 @@ void launch_tail(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
     const int tblocks = c->tail_per_sm * c->nsm;
     if (c->split) launch_tail_split(D, tblocks, c->st, shearupdate, integrate, fuse_next, store_f);
     else if (c->P.rolling_cdt)
-        k_pair_tail<true, false><<<tblocks, kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+        launch_pair_tail<true, false>(D, tblocks, c->st, shearupdate, integrate, fuse_next, store_f);
     else
-        k_pair_tail<false, false><<<tblocks, kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+        launch_pair_tail<false, false>(D, tblocks, c->st, shearupdate, integrate, fuse_next, store_f);
 }
 
 int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int store_f)

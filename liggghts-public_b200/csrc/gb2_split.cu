@@ -40,8 +40,8 @@ void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int
 void launch_tail_split(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
                        int store_f)
 {
-    if (D.rolling) k_pair_tail<true, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
-    else k_pair_tail<false, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    if (D.rolling) launch_pair_tail<true, true>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+    else launch_pair_tail<false, true>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
 }
 
 }  // namespace gb2

@@ -63,6 +63,13 @@ __device__ __forceinline__ void serial_atom(const Dev &D, int k, const dbl4 &pk,
     }
 }
 
+// Programmatic dependent launch: the pair step lets the tail kernel be
+// scheduled as soon as all of its blocks are running; the tail kernel does
+// what does not need the pair sums first and then waits for the pair step
+// to complete (all its memory operations visible).
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // A kernel of a step queued ahead returns at once when an earlier step has
 // asked for a neighbour rebuild (that step's successors are redone after it).
 __device__ __forceinline__ bool step_cancelled(const Dev &D) { return D.dstop && *(volatile int *)D.dstop < D.step; }
@@ -301,6 +308,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     // velocity, position at the last rebuild) wait here, not in registers,
     // while the screening and the contact rounds run
     __shared__ __align__(16) dbl4 stail[3][128];
+    grid_dep_launch();   // the tail kernel may be scheduled once every block of this grid runs
     if (step_cancelled(D)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,52 +403,94 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
 constexpr int kTailAtoms = GB2_TAIL_ATOMS;
 
 // Second kernel of the step: the atoms listed at the last neighbour build
-// as having wall candidates or more than 64 entries on a side, finished
-// from the pair sums k_pair_step left in tailf/tailt (zero for an atom with
-// more than 64 entries on a side, whose contacts are evaluated here in the
-// reference order).  The post_force fixes follow in definition order, then
-// final_integrate and the fused next initial_integrate.  Every atom's end
-// of step touches only that atom's records, so the split into two kernels
-// leaves each result bit for bit as in one.
+// as having wall candidates or more than 64 entries on a side, kTailAtoms
+// per warp.  Launched as a programmatic dependent of k_pair_step, it starts
+// while the pair step's last blocks run: the wall contacts of an atom with
+// one wall fix at work depend only on the step's input state and that
+// wall's contact history, so they are evaluated first (mesh candidates
+// spread over the lanes, slot partners staged in shared memory) and their
+// forces kept as records.  After the wait, each atom is finished from the
+// pair sums k_pair_step left in tailf/tailt (an atom with more than 64
+// entries on a side evaluates its pairs here in the reference order): the
+// post_force fixes in definition order with the records added at their
+// fix, walls not yet done evaluated now, then final_integrate and the
+// fused next initial_integrate.  Every atom's end of step touches only that
+// atom's records, so the result is bit for bit that of one kernel.
 template <bool ROLLING, bool SPLIT>
 __global__ void __launch_bounds__(128, 4) k_pair_tail(Dev D, int shearupdate, int integrate, int fuse_next,
                                                       int store_f)
 {
-    __shared__ int s_sp[4][kTailAtoms * 64];   // slot partners of the warp's atoms (mesh walls)
-    if (step_cancelled(D)) return;
+    __shared__ int s_sp[4][kTailAtoms * 64];            // slot partners of the warp's atoms (mesh walls)
+    __shared__ WallRec s_rec[4][kTailAtoms][kWallRec];  // wall-contact records of the warp's atoms
+    // every thread waits for the pair step before it exits, so this grid's
+    // completion implies the pair step's for the launches after it
+    if (step_cancelled(D)) {
+        grid_dep_wait();
+        return;
+    }
     const int n = *D.tailcnt;
     const bool upd = shearupdate != 0;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nwarp = gridDim.x * (blockDim.x >> 5);
-    for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kTailAtoms; base < n;
-         base += nwarp * kTailAtoms) {
+    WallRec *rec = s_rec[wid][lane < kTailAtoms ? lane : 0];
+    for (int base = (blockIdx.x * (blockDim.x >> 5) + wid) * kTailAtoms; base < n; base += nwarp * kTailAtoms) {
         const bool own = lane < kTailAtoms && base + lane < n;
-        int i = 0, ti = 0;
-        ContactOut acc;
+        int i = 0, ti = 0, nr = 0, nn = 0, qw = -1, nwork = 0;
         dbl4 pi, vi4, wi4, hold;
         pi = vi4 = wi4 = hold = dbl4{0.0, 0.0, 0.0, 0.0};
-        for (int c = 0; c < 3; c++) acc.F[c] = acc.T[c] = 0.0;
         if (own) {
             i = D.tail[base + lane];
-            const dbl4 F4 = D.tailf[i], T4 = D.tailt[i];
-            acc.F[0] = F4.x;
-            acc.F[1] = F4.y;
-            acc.F[2] = F4.z;
-            acc.T[0] = T4.x;
-            acc.T[1] = T4.y;
-            acc.T[2] = T4.z;
             pi = D.pos[i];
             vi4 = D.vel[i];
             wi4 = D.omg[i];
             if (fuse_next) hold = D.xhold[i];
             ti = D.type[i];
-            const int nr = D.rnum[i], nn = D.nnum[i];
-            if (nr > 64 || nn > 64) {
-                serial_atom<ROLLING>(D, i, pi, vi4, wi4, ti, nr, nn, upd, acc);
-                if (upd) D.prevmask[i] = ~0ull;   // every own slot written this step
+            nr = D.rnum[i];
+            nn = D.nnum[i];
+            for (int q = 0; q < D.nfix; q++) {
+                const FixDev &F = D.fix[q];
+                if ((F.kind == FIX_WALL_PLANE && F.inlist[i]) || (F.kind == FIX_WALL_MESH && F.mesh.tcnt[i] != 0)) {
+                    qw = q;
+                    nwork++;
+                }
             }
         }
+        const bool serial = nr > 64 || nn > 64;
         const double vi[3] = {vi4.x, vi4.y, vi4.z}, wi[3] = {wi4.x, wi4.y, wi4.z};
+        // walls before the wait: atoms with one wall fix at work
+        bool early = own && !serial && nwork == 1;
+        int nrec = 0;
+        ContactOut unused;
+        for (int q = 0; q < D.nfix; q++) {
+            const FixDev &F = D.fix[q];
+            if (F.kind == FIX_WALL_PLANE) {
+                if (early && qw == q) {
+                    ContactOut o = wall_record_zero();
+                    if (plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, o)) wall_record_put(rec, nrec, o);
+                }
+            } else if (F.kind == FIX_WALL_MESH && __any_sync(0xffffffffu, early && qw == q)) {
+                mesh_wall_items<true>(D, F.mesh, early && qw == q, i, pi, vi, wi, vi4.w, ti, upd, s_sp[wid], unused,
+                                      rec, &nrec, &early);
+            }
+        }
+        grid_dep_wait();
+        ContactOut acc;
+        for (int c = 0; c < 3; c++) acc.F[c] = acc.T[c] = 0.0;
+        if (own) {
+            if (serial) {
+                serial_atom<ROLLING>(D, i, pi, vi4, wi4, ti, nr, nn, upd, acc);
+                if (upd) D.prevmask[i] = ~0ull;   // every own slot written this step
+            } else {
+                const dbl4 F4 = D.tailf[i], T4 = D.tailt[i];
+                acc.F[0] = F4.x;
+                acc.F[1] = F4.y;
+                acc.F[2] = F4.z;
+                acc.T[0] = T4.x;
+                acc.T[1] = T4.y;
+                acc.T[2] = T4.z;
+            }
+        }
+        const bool late = own && !early;   // walls evaluated after the wait
         for (int q = 0; q < D.nfix; q++) {
             const FixDev &F = D.fix[q];
             if (F.kind == FIX_GRAVITY) {
@@ -448,14 +498,48 @@ __global__ void __launch_bounds__(128, 4) k_pair_tail(Dev D, int shearupdate, in
                 acc.F[0] += massone * F.acc[0];
                 acc.F[1] += massone * F.acc[1];
                 acc.F[2] += massone * F.acc[2];
-            } else if (F.kind == FIX_WALL_PLANE) {
-                if (own && F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
-            } else if (F.kind == FIX_WALL_MESH) {
-                mesh_wall_items(D, F.mesh, own, i, pi, vi, wi, vi4.w, ti, upd, s_sp[threadIdx.x >> 5], acc);
+            } else if (F.kind == FIX_WALL_PLANE || F.kind == FIX_WALL_MESH) {
+                if (early && qw == q) {   // this fix's records, in the order they were made
+                    for (int r = 0; r < nrec; r++) {
+                        acc.F[0] += rec[r][0];
+                        acc.F[1] += rec[r][1];
+                        acc.F[2] += rec[r][2];
+                        acc.T[0] += rec[r][3];
+                        acc.T[1] += rec[r][4];
+                        acc.T[2] += rec[r][5];
+                    }
+                }
+                // walls left for now; the mesh routine is warp-collective, so
+                // every lane calls it (owners without work pass own = false)
+                if (F.kind == FIX_WALL_PLANE) {
+                    if (late && F.inlist[i]) plane_wall_atom(D, F, i, pi, vi, wi, vi4.w, ti, upd, acc);
+                } else if (__any_sync(0xffffffffu, late)) {
+                    mesh_wall_items<false>(D, F.mesh, late, i, pi, vi, wi, vi4.w, ti, upd, s_sp[wid], acc);
+                }
             }
         }
         if (own) atom_store_integrate<SPLIT>(D, i, pi, vi4, wi4, hold, integrate, fuse_next, store_f, acc);
     }
+    grid_dep_wait();
+}
+
+// Host side: the tail kernel launched as a programmatic dependent of the
+// pair step launched just before it on the same stream.
+template <bool ROLLING, bool SPLIT>
+inline cudaError_t launch_pair_tail(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate,
+                                    int fuse_next, int store_f)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_pair_tail<ROLLING, SPLIT>, D, shearupdate, integrate, fuse_next, store_f);
 }
 
 }  // namespace gb2
