@@ -267,15 +267,21 @@ def state_scenario(sc, a):
     return out
 
 
+PROFILE_EVERY = 16   # per-kernel CUDA events on every 16th step of the timed window
+
+
 def timed_window(eng, steps, dist, device, clocks=True):
-    """Device-timed window of `steps` steps (CUDA events on the engine stream
-    at its ends only: per-kernel events would sit between the pair step and
-    its programmatically dependent tail kernel and serialise them)."""
+    """Device-timed window of `steps` steps: CUDA events at its ends give the
+    window time; per-kernel CUDA events on every PROFILE_EVERY-th step give
+    each kernel's average launch time (the events serialise the pair step
+    and its dependent tail kernel on those steps only)."""
     eng.sync()
+    cen0 = eng.census()
     st0 = eng.stats()
     sampler = ClockSampler(device) if clocks else None
     barrier(dist)
     eng.sync()
+    eng.set_profiling(True, every=PROFILE_EVERY)
     eng.timer_start()
     eng.run(steps)
     ms = eng.timer_stop()
@@ -283,27 +289,18 @@ def timed_window(eng, steps, dist, device, clocks=True):
     barrier(dist)
     clk = sampler.stop() if sampler else None
     st1 = eng.stats()
-    return {"ms": allmax(dist, ms), "clocks": clk,
+    eng.set_profiling(False)
+    cen1 = eng.census()
+    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_pair_tail", "t_forward", "t_rebuild")}
+    npm = st1["n_pair_main"] - st0["n_pair_main"]
+    return {"ms": allmax(dist, ms), "clocks": clk, "cen": (cen0, cen1), "kt": kt, "npm": npm,
+            "kernel_ms_per_step": dict({k: v / max(npm, 1) for k, v in kt.items()},
+                                       note="CUDA events on every %dth step of the timed window (%d steps timed)"
+                                            % (PROFILE_EVERY, npm)),
             "launches": st1["kernel_launches"] - st0["kernel_launches"],
             "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
             "growth": st1["ngrow"] - st0["ngrow"],
             "capacities": {k: st1[k] for k in ("maxneigh", "maxpartner", "maxrev", "maxmesh")}}
-
-
-def profiled_window(eng, steps):
-    """Per-kernel device times (CUDA events around every launch) over `steps`
-    steps after the timed window, with the contact census at both ends."""
-    eng.sync()
-    cen0 = eng.census()
-    st0 = eng.stats()
-    eng.set_profiling(True)
-    eng.run(steps)
-    eng.sync()
-    st1 = eng.stats()
-    eng.set_profiling(False)
-    cen1 = eng.census()
-    kt = {k: st1[k] - st0[k] for k in ("t_integrate", "t_pair_main", "t_pair_tail", "t_forward", "t_rebuild")}
-    return {"steps": steps, "cen": (cen0, cen1), "kt": kt, "npm": st1["n_pair_main"] - st0["n_pair_main"]}
 
 
 def own_arm(args):
@@ -323,14 +320,13 @@ def own_arm(args):
     W = timed_window(eng, args.steps, dist, local)
     ms_max = W["ms"]
     value = n * args.steps * ws / (ms_max * 1e-3)
-    P = profiled_window(eng, min(args.steps, 1000))
 
     # roofline of the dominant kernel
     nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] == "wall_plane")
     nfix_mesh = sum(1 for f in sc["fixes"] if f["kind"] == "wall_mesh")
     dom = "k_pair_step"
-    dom_ms = P["kt"]["t_pair_main"] / max(P["npm"], 1)
-    ab = algorithmic_bytes(dom, n, P["cen"], nfix_plane, nfix_mesh, split)
+    dom_ms = W["kt"]["t_pair_main"] / max(W["npm"], 1)
+    ab = algorithmic_bytes(dom, n, W["cen"], nfix_plane, nfix_mesh, split)
     peak, peak_kind = peaks()
     achieved = ab / (dom_ms * 1e-3) / 1e9
     traffic = load_traffic(dom + ("_split" if split else ""), args.workload)
@@ -338,7 +334,8 @@ def own_arm(args):
             "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "traffic": traffic["bytes_per_launch"] if traffic else None,
             "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms,
-            "timing": "pair-step launches timed with CUDA events over %d steps after the timed window" % P["steps"]}
+            "timing": "pair-step launches timed with CUDA events on every %dth step of the timed window"
+                      % PROFILE_EVERY}
 
     pdesc = ("split (FP32 contact math on FP64-differenced positions and FP64 overlap, Kahan FP32 pair sums; "
              "FP64 walls, gravity, integration)" if split else "fp64 (bit-exact to the oracle)")
@@ -352,9 +349,8 @@ def own_arm(args):
         "roofline": roof,
         "gpu_launches": W["launches"],
         "clocks": W["clocks"],
-        "kernel_ms_per_step": dict({k: v / P["steps"] for k, v in P["kt"].items()},
-                                   note="per-kernel CUDA events over %d steps after the timed window" % P["steps"]),
-        "census": {k: 0.5 * (P["cen"][0][k] + P["cen"][1][k]) for k in P["cen"][0]},
+        "kernel_ms_per_step": W["kernel_ms_per_step"],
+        "census": {k: 0.5 * (W["cen"][0][k] + W["cen"][1][k]) for k in W["cen"][0]},
         "rebuilds": W["rebuilds"],
         "capacity_growth_in_window": W["growth"],
         "capacities": W["capacities"],
@@ -367,10 +363,9 @@ def own_arm(args):
         e64.run(max(args.warmup, 3))
         W64 = timed_window(e64, args.fp64_steps, dist, local, clocks=False)
         v64 = n * args.fp64_steps * ws / (W64["ms"] * 1e-3)
-        P64 = profiled_window(e64, min(args.fp64_steps, 1000))
         line["fp64_gpu"] = {"value": v64, "unit": UNIT, "steps": args.fp64_steps,
                             "ms_per_step": W64["ms"] / args.fp64_steps,
-                            "kernel_ms_per_step": {k: v / P64["steps"] for k, v in P64["kt"].items()},
+                            "kernel_ms_per_step": W64["kernel_ms_per_step"],
                             "note": "bit-exact FP64 path from the same settled state (same settle and warm-up "
                                     "steps, %d timed steps; split window %d)" % (args.fp64_steps, args.steps)}
         line["split_over_fp64"] = value / v64
@@ -383,18 +378,24 @@ def own_arm(args):
         barrier(dist)
         t0 = time.perf_counter()
         e2 = granb200.Engine(sc2, precision=prec, device=local)
+        t1 = time.perf_counter()
         e2.setup()
+        t2 = time.perf_counter()
         e2.run(args.steps)
+        e2.sync()
+        t3 = time.perf_counter()
         out = e2.atoms()
         e2.sync()
-        dt = time.perf_counter() - t0
+        t4 = time.perf_counter()
+        dt = t4 - t0
         dt = allmax(dist, dt)
         h2d = n * (3 * 3 * 8 + 2 * 8 + 2 * 4) + sum(f["nodes"].size * 8 for f in sc["fixes"] if f["kind"] == "wall_mesh")
         d2h = n * (5 * 3 * 8 + 4)
         line["e2e"] = {"value": n * args.steps * ws / dt, "unit": UNIT,
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                        "includes": "context create, materials, atom + mesh upload, Verlet setup, %d steps, "
-                                   "download of x/v/omega/f/torque" % args.steps}
+                                   "download of x/v/omega/f/torque" % args.steps,
+                       "seconds": {"create_upload": t1 - t0, "setup": t2 - t1, "run": t3 - t2, "download": t4 - t3}}
         del e2, out
 
     # CPU baseline: the oracle on this rank's state at the start of the window

@@ -190,7 +190,9 @@ int gb2_census(gb2_ctx *ctx, gb2_contact_census *out);
 #define GB2_NOALLOC_MAX_BLOCKS 16384
 #define GB2_NOALLOC_MAX_ATOMS (GB2_NOALLOC_MAX_BLOCKS * 128)
 int gb2_census_noalloc(gb2_ctx *ctx, gb2_contact_census *out);
-/* per-kernel CUDA-event timing on the context stream (off by default) */
+/* per-kernel CUDA-event timing on the context stream (off by default):
+ * on = 0 off, 1 every step, N > 1 every N-th step (events between the pair
+ * step and its dependent tail kernel serialise the two on the steps timed) */
 int gb2_set_profiling(gb2_ctx *ctx, int on);
 /* CUDA-event timer on the context stream: start, then stop returns ms */
 int gb2_timer_start(gb2_ctx *ctx);

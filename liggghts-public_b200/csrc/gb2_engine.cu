@@ -177,8 +177,9 @@ struct gb2_ctx {
     long launches = 0;
     long nsteps_rebuild = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // per-kernel event timing (gb2_set_profiling)
+    // per-kernel event timing (gb2_set_profiling): every prof_every-th step
     bool prof = false;
+    int prof_every = 1;
     struct EvPair {
         cudaEvent_t a, b;
         int cls;
@@ -345,7 +346,8 @@ enum { PROF_INTEGRATE = 0, PROF_PAIR_TAIL = 1, PROF_PAIR_MAIN = 2, PROF_FORWARD 
 
 int prof_begin(gb2_ctx *c, int cls, gb2_ctx::EvPair *out)
 {
-    if (!c->prof) return 0;
+    out->cls = -1;
+    if (!c->prof || (c->prof_every > 1 && c->ntimestep % c->prof_every != 0)) return 0;
     if (c->ev_free.empty()) {
         gb2_ctx::EvPair e;
         CK(cudaEventCreate(&e.a));
@@ -361,7 +363,7 @@ int prof_begin(gb2_ctx *c, int cls, gb2_ctx::EvPair *out)
 
 int prof_end(gb2_ctx *c, gb2_ctx::EvPair *e)
 {
-    if (!c->prof) return 0;
+    if (!c->prof || e->cls < 0) return 0;
     CK(cudaEventRecord(e->b, c->st));
     c->ev_pending.push_back(*e);
     return 0;
@@ -1676,7 +1678,8 @@ int gb2_set_profiling(gb2_ctx *c, int on)
     if (!c) return GB2_ERR_ARG;
     CK(cudaStreamSynchronize(c->st));
     prof_resolve(c);
-    c->prof = on != 0;
+    c->prof = on > 0;
+    c->prof_every = on > 1 ? on : 1;
     return 0;
 }
 

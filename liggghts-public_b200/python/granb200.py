@@ -259,8 +259,9 @@ class Engine:
         self._check(self.L.gb2_census_noalloc(self.h, ctypes.byref(c)))
         return {f: getattr(c, f) for f, _ in Census._fields_}
 
-    def set_profiling(self, on):
-        self._check(self.L.gb2_set_profiling(self.h, 1 if on else 0))
+    def set_profiling(self, on, every=1):
+        """Per-kernel CUDA-event timing, on every `every`-th step."""
+        self._check(self.L.gb2_set_profiling(self.h, max(1, int(every)) if on else 0))
 
     def timer_start(self):
         self._check(self.L.gb2_timer_start(self.h))
