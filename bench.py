@@ -315,7 +315,9 @@ def own_arm(args):
     eng.run(args.settle)
     if args.fp64_steps < 0:
         args.fp64_steps = args.steps
-    start_state = state_scenario(sc, eng.atoms()) if args.fp64_steps > 0 and split else None
+    # the settled state the timed window starts from (warm-up aside): the FP64
+    # arm and the end-to-end run start from it too
+    start_state = state_scenario(sc, eng.atoms()) if (args.fp64_steps > 0 and split) or not args.no_e2e else None
     eng.run(max(args.warmup, 3))
     W = timed_window(eng, args.steps, dist, local)
     ms_max = W["ms"]
@@ -357,7 +359,7 @@ def own_arm(args):
     }
 
     # the plain FP64 form on the same starting state (same settle, warm-up)
-    if start_state is not None:
+    if start_state is not None and args.fp64_steps > 0 and split:
         e64 = granb200.Engine(start_state, precision=granb200.PREC_FP64, device=local)
         e64.setup()
         e64.run(max(args.warmup, 3))
@@ -374,7 +376,7 @@ def own_arm(args):
 
     # end to end through the C ABI: host arrays in, setup, run, host arrays out
     if not args.no_e2e:
-        sc2 = state_scenario(sc, eng.atoms())
+        sc2 = start_state
         barrier(dist)
         t0 = time.perf_counter()
         e2 = granb200.Engine(sc2, precision=prec, device=local)
@@ -393,8 +395,9 @@ def own_arm(args):
         d2h = n * (5 * 3 * 8 + 4)
         line["e2e"] = {"value": n * args.steps * ws / dt, "unit": UNIT,
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                       "includes": "context create, materials, atom + mesh upload, Verlet setup, %d steps, "
-                                   "download of x/v/omega/f/torque" % args.steps,
+                       "includes": "context create, materials, atom + mesh upload, Verlet setup, %d steps from the "
+                                   "settled state the timed window starts from, download of x/v/omega/f/torque"
+                                   % args.steps,
                        "seconds": {"create_upload": t1 - t0, "setup": t2 - t1, "run": t3 - t2, "download": t4 - t3}}
         del e2, out
 
@@ -424,6 +427,7 @@ def sq_arm(args):
     l0, l1 = tr.train(epochs=4, batch=4096, lr=2e-3)
     ev = tr.evaluate(100_000, seed=99)
     train_s = time.perf_counter() - t0
+    solve = tr.time_solves(400_000, seed=123)   # first-contact solves alone, same pairs both ways
     params = tr.params()
     sc = S.sq_packing(n=n, seed=11)
     res = {}
@@ -451,6 +455,11 @@ def sq_arm(args):
                    "settle_steps": args.settle},
         "plain": res["plain"], "learned": res["learned"],
         "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
+        "first_contact_solve": dict(solve, note="contact-point solve of fresh pairs near contact (a new "
+                                                "contact's first solve), plain homotopy vs learned guess with "
+                                                "homotopy fallback, each launch timed alone; a launch lasts as "
+                                                "long as its slowest pairs (those both methods fail on after "
+                                                "the iteration cap)"),
         "training": {"samples": info["valid"], "plain_iters_per_sample": info["plain_iters"],
                      "plain_solves_per_sample": info["plain_solves"], "loss_first": l0, "loss_last": l1,
                      "seconds": train_s, "held_out": ev},

@@ -281,6 +281,12 @@ int gb2_mlp_grad(gb2_mlp_ctx *ctx, int nrows, const float *samples, float *loss,
    solutions differ by more than 1e-4 of the smallest half-axis; *maxdiff =
    largest such difference over the smallest half-axis */
 int gb2_mlp_evaluate(gb2_mlp_ctx *ctx, long n, unsigned long long seed, long long *stats, double *maxdiff);
+/* device time of the first-contact solve of n fresh pairs (those near
+   contact): the plain homotopy from spheres against the learned guess with
+   the homotopy as fallback, each launch timed alone with CUDA events after
+   an untimed pass; counts[3] = pairs, plain iterations, learned iterations */
+int gb2_mlp_time_solves(gb2_mlp_ctx *ctx, long n, unsigned long long seed, double *ms_plain, double *ms_learned,
+                        long long *counts);
 int gb2_mlp_last_error(gb2_mlp_ctx *ctx, char *buf, int len);
 
 #ifdef __cplusplus

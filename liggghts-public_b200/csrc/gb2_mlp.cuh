@@ -151,6 +151,37 @@ __global__ void k_mlp_eval(unsigned long long seed, long n, const float *__restr
     }
 }
 
+// Timed comparison of the two first-contact solves on the same stored pairs:
+// k_mlp_store_pairs keeps the valid samples, k_mlp_solve runs one method per
+// pair (the plain homotopy from spheres, or the learned guess with the
+// homotopy as fallback) and keeps its point and iteration count, so each
+// launch can be timed alone with CUDA events.
+__global__ void k_mlp_store_pairs(unsigned long long seed, long n, PairSample *out, int *nvalid)
+{
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    PairSample S;
+    if (!sample_pair(seed, k, S)) return;
+    out[atomicAdd(nvalid, 1)] = S;
+}
+
+template <bool LEARNED>
+__global__ void k_mlp_solve(const PairSample *pairs, const int *nvalid, const float *__restrict__ P, double *point,
+                            long long *iters)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nvalid) return;
+    const PairSample S = pairs[k];
+    Newton o;
+    int it, sv, used;
+    if constexpr (LEARNED)
+        first_contact(P, S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, o, it, sv, used);
+    else
+        contact_point(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, 0, nullptr, false, 0.0, o, it, sv);
+    for (int c = 0; c < 3; c++) point[3 * k + c] = o.point[c];
+    atomicAdd((unsigned long long *)iters, (unsigned long long)it);
+}
+
 // ------------------------------------------------------------------ training (BF16 tensor cores)
 
 // padded layer shapes: in 14 -> 16, out 4 -> 8 (zero rows/columns)

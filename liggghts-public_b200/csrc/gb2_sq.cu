@@ -961,6 +961,48 @@ int gb2_mlp_evaluate(gb2_mlp_ctx *c, long n, unsigned long long seed, long long 
     return 0;
 }
 
+int gb2_mlp_time_solves(gb2_mlp_ctx *c, long n, unsigned long long seed, double *ms_plain, double *ms_learned,
+                        long long *counts)
+{
+    if (!c || n <= 0 || n > (1L << 24) || !ms_plain || !ms_learned || !counts) return GB2_ERR_ARG;
+    Buf<PairSample> pairs;
+    Buf<double> pt;
+    Buf<int> nv;
+    Buf<long long> it;
+    MLCK(pairs.alloc(n));
+    MLCK(pt.alloc(3 * n));
+    MLCK(nv.alloc(1));
+    MLCK(it.alloc(2));
+    MLCK(cudaMemsetAsync(nv.p, 0, sizeof(int), c->st));
+    MLCK(cudaMemsetAsync(it.p, 0, 2 * sizeof(long long), c->st));
+    k_mlp_store_pairs<<<nb(n), kB, 0, c->st>>>(seed, n, pairs.p, nv.p);
+    MLCK(cudaGetLastError());
+    cudaEvent_t e[3];
+    for (auto &x : e) MLCK(cudaEventCreate(&x));
+    // one untimed pass of each (code and data warm), then the timed ones
+    k_mlp_solve<false><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p);
+    k_mlp_solve<true><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p + 1);
+    MLCK(cudaMemsetAsync(it.p, 0, 2 * sizeof(long long), c->st));
+    MLCK(cudaEventRecord(e[0], c->st));
+    k_mlp_solve<false><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p);
+    MLCK(cudaEventRecord(e[1], c->st));
+    k_mlp_solve<true><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p + 1);
+    MLCK(cudaEventRecord(e[2], c->st));
+    MLCK(cudaGetLastError());
+    int hv = 0;
+    MLCK(cudaMemcpyAsync(&hv, nv.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaMemcpyAsync(counts + 1, it.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    MLCK(cudaStreamSynchronize(c->st));
+    float a = 0.f, b = 0.f;
+    MLCK(cudaEventElapsedTime(&a, e[0], e[1]));
+    MLCK(cudaEventElapsedTime(&b, e[1], e[2]));
+    for (auto &x : e) cudaEventDestroy(x);
+    counts[0] = hv;
+    *ms_plain = a;
+    *ms_learned = b;
+    return 0;
+}
+
 int gb2_mlp_last_error(gb2_mlp_ctx *c, char *buf, int len)
 {
     if (!c || !buf || len <= 0) return GB2_ERR_ARG;

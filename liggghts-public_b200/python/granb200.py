@@ -458,6 +458,8 @@ class MlpTrainer:
             L.gb2_mlp_set_params.argtypes = [vp, F, ctypes.c_int]
             L.gb2_mlp_grad.argtypes = [vp, ctypes.c_int, F, F, F]
             L.gb2_mlp_evaluate.argtypes = [vp, ctypes.c_long, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong), D]
+            L.gb2_mlp_time_solves.argtypes = [vp, ctypes.c_long, ctypes.c_ulonglong, D, D,
+                                              ctypes.POINTER(ctypes.c_longlong)]
             L.gb2_mlp_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
             L._mlp_ready = True
         self.L = L
@@ -522,3 +524,13 @@ class MlpTrainer:
         out = dict(zip(keys, [int(v) for v in st]))
         out["maxdiff"] = md.value
         return out
+
+    def time_solves(self, n, seed):
+        """Device time of the first-contact solve of the same fresh pairs,
+        plain homotopy against the learned guess (each launch timed alone)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        cnt = (ctypes.c_longlong * 3)()
+        self._check(self.L.gb2_mlp_time_solves(self.h, n, seed, ctypes.byref(a), ctypes.byref(b), cnt))
+        return {"pairs": int(cnt[0]), "plain_ms": a.value, "learned_ms": b.value,
+                "plain_iters": int(cnt[1]), "learned_iters": int(cnt[2]),
+                "speedup": a.value / b.value if b.value > 0 else None}

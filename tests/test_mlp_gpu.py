@@ -101,3 +101,17 @@ def test_learned_guess_in_simulation(trained):
     assert np.abs(fa - fb).max() <= 1e-3 * np.abs(fa).max()
     assert cb["learned_used"] > 0
     assert cb["solves"] < ca["solves"]
+
+
+def test_learned_guess_solve_time(trained):
+    """The first-contact solve itself on the same fresh pairs both ways: the
+    learned guess needs about half the Newton iterations.  The kernel times
+    are reported, not asserted: each launch lasts as long as its slowest
+    pairs, those the plain solver also fails on after the iteration cap, and
+    for them the learned attempt comes on top of the homotopy."""
+    t, info, l0, l1 = trained
+    ts = t.time_solves(100_000, seed=7)
+    print(ts)
+    assert ts["pairs"] > 40_000
+    assert ts["learned_iters"] < 0.6 * ts["plain_iters"]
+    assert ts["plain_ms"] > 0 and ts["learned_ms"] > 0
