@@ -358,19 +358,39 @@ def random_quaternions(rng, n):
     return q[:, [3, 0, 1, 2]].copy()
 
 
+def sq_bounding_radius(shape, blk):
+    """Bounding-sphere radius of superquadrics with n1 = n2 = blk (the closed
+    form of Superquadric's bounding sphere, src/superquadric.cpp, with its
+    1.0001 margin), vectorised over particles."""
+    shape = np.asarray(shape, dtype=np.float64)
+    blk = np.asarray(blk, dtype=np.float64)
+    a = np.maximum(shape[:, 0], shape[:, 1])
+    b = np.minimum(shape[:, 0], shape[:, 1])
+    c = shape[:, 2]
+    n = np.maximum(2.1, blk)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        alpha = np.power(b / a, 2.0 / (n - 2.0))
+        gamma = np.power(1.0 + np.power(alpha, n), 0.0)
+        beta = np.power(c * c / (a * a) * gamma, 1.0 / (n - 2.0))
+        x0 = 1.0 / np.power(1.0 + np.power(alpha, n) + np.power(beta, n), 1.0 / n)
+    r = np.sqrt((x0 * a) ** 2 + (alpha * x0 * b) ** 2 + (beta * x0 * c) ** 2) * 1.0001
+    ellipsoid = np.abs(blk - 2.0) < 1e-13
+    return np.where(ellipsoid, shape.max(axis=1) * 1.0001, r)
+
+
 def sq_packing(n=200_000, seed=11, dt=1e-5, skin=0.5e-3, vin=1.0, density=2500.0, fill=0.8):
     """Superquadric packing: half-axes U(1, 2) mm, blockiness U(2, 8) (one
     exponent per particle, n1 = n2), uniformly random orientations, Hertz
     contact with config-1 materials (E 5e6, nu 0.45, e 0.3, mu 0.5), on a
     cubic lattice of spacing ``fill`` x the largest bounding diameter, with
     uniform random velocities of +-``vin`` so contacts form and break."""
-    import oracle
     rng = np.random.default_rng(seed)
     shape = rng.uniform(1e-3, 2e-3, size=(n, 3))
     blk = rng.uniform(2.0, 8.0, size=n)
     quat = random_quaternions(rng, n)
-    rb = np.array([oracle.sq_bounding_radius(shape[i], blk[i]) for i in range(n)]) if n <= 20000 else None
-    if rb is None:   # vectorised bound for large n: the corner of the box bounds every blockiness
+    if n <= 20000:
+        rb = sq_bounding_radius(shape, blk)
+    else:   # large packings: the corner of the box bounds every blockiness
         rb = np.linalg.norm(shape, axis=1) * 1.0001
     s = fill * 2.0 * rb.max()
     m = int(math.ceil(n ** (1.0 / 3.0)))
