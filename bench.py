@@ -198,9 +198,12 @@ def dist_init():
     if ws > 1:
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        else:   # host-only runs (tests of the multi-rank plumbing)
+            dist.init_process_group("gloo", timeout=timedelta(seconds=60))
         return ws, rank, local, dist
     return 1, 0, 0, None
 
@@ -214,7 +217,8 @@ def allmax(dist, x):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
