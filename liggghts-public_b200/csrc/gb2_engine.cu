@@ -1618,7 +1618,9 @@ int gb2_run(gb2_ctx *c, int nsteps)
             s++;
             continue;
         }
-        CK(cudaMemsetAsync(c->dstop.p, 0x7f, sizeof(int), c->st));
+        // the step just run (not queued) may have asked for a rebuild of the next
+        k_queue_start<<<1, 1, 0, c->st>>>(c->dstop.p, c->ddflag.p, (int)c->ntimestep);
+        CKL();
         c->queue_active = true;
         struct Queued {
             long ntimestep;
@@ -1652,9 +1654,12 @@ int gb2_run(gb2_ctx *c, int nsteps)
                 head++;
                 continue;
             }
-            // step `head` asked for a rebuild of the next step: its queued successors did nothing
-            for (int r = launched - 1; r > head; r--) unqueue_step(c, q[r % 16].last, q[r % 16].nev);
-            launched = head + 1;
+            // step v asked for a rebuild of step v + 1: v is `head`, or the step
+            // run just before the queue (then `head` itself did nothing); the
+            // queued steps after v did nothing
+            const int first = (long)v < q[head % 16].ntimestep ? head : head + 1;
+            for (int r = launched - 1; r >= first; r--) unqueue_step(c, q[r % 16].last, q[r % 16].nev);
+            launched = first;
             stop = true;
             break;
         }

@@ -776,5 +776,9 @@ __global__ void k_tail_list(Dev D)
     if (tail_atom(D, k, D.rnum[k], D.nnum[k])) D.tail[atomicAdd(D.tailcnt, 1)] = k;
 }
 
+// Start of a queue of steps: the step just run (not queued) may already
+// have asked for a rebuild of the next one through the displacement flag.
+__global__ void k_queue_start(int *dstop, const int *dflag, int step) { *dstop = *dflag ? step : 0x7f7f7f7f; }
+
 }  // namespace gb2
 

@@ -83,6 +83,46 @@ def sphere_pour(n=20000, seed=12345, dt=1e-5, skin=0.5e-3, jitter=0.2e-3, vmax=0
     return sc
 
 
+def bidisperse_bed(nx=26, nlayers=12, r_small=0.3e-3, r_big=3e-3, n_big=2, seed=5, dt=2e-6, skin=0.5e-3,
+                   vmax=0.3):
+    """Small spheres on a jittered lattice (0.75 mm spacing) with a few large
+    spheres buried in it (small ones overlapping them removed), periodic in
+    x and y, floor at z = 0, gravity -z.  A large sphere has far more than 64
+    neighbours within the cutoff, so its pairs take the serial path."""
+    rng = np.random.default_rng(seed)
+    sp = 0.75e-3
+    L = nx * sp
+    ii = np.arange(nx * nx * nlayers)
+    pos = np.stack([(ii % nx + 0.5) * sp, ((ii // nx) % nx + 0.5) * sp, r_small + 0.05e-3 + (ii // (nx * nx)) * sp],
+                   axis=1)
+    pos = pos + rng.uniform(-0.05e-3, 0.05e-3, size=pos.shape)
+    zmid = 0.5 * (pos[:, 2].min() + pos[:, 2].max())
+    big = np.stack([np.array([(k + 0.5) * L / n_big, 0.5 * L, zmid]) for k in range(n_big)])
+    keep = np.ones(len(pos), dtype=bool)
+    for c in big:
+        keep &= np.linalg.norm(pos - c, axis=1) > r_big + r_small + 0.05e-3
+    pos = np.concatenate([big, pos[keep]])
+    rad = np.concatenate([np.full(n_big, r_big), np.full(int(keep.sum()), r_small)])
+    n = len(pos)
+    vel = rng.uniform(-vmax, vmax, size=(n, 3))
+    sc = {
+        "name": "bidisperse_bed",
+        "dt": dt, "skin": skin,
+        "boxlo": [0.0, 0.0, 0.0], "boxhi": [L, L, pos[:, 2].max() + 2 * r_big + 5e-3], "periodic": [1, 1, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": 1000, "sortbinsize": 0.0,
+        "rolling_cdt": 1, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2500.0, vel, None),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_plane", "dim": 2, "pos": 0.0, "wall_type": 1, "rolling_cdt": 1},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5))
+    sc["rollfriction"] = np.array([[0.1]])
+    return sc
+
+
 def cone_mesh(n_theta=128, n_z=32, r_out=0.015, half_angle_deg=60.0, height=0.17, z0=0.0):
     """Triangulated cone frustum (a hopper), ``2 * n_theta * n_z`` triangles.
 

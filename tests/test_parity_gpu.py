@@ -129,3 +129,28 @@ def test_silo_cylinder_wall_and_linear_piston():
     assert np.abs(o.wall_hist(1)).sum() > 0, "no particle touched the cylinder"
     assert len(o.mesh_contacts(3)["tag"]) > 0, "the piston touched nothing"
     assert e.stats()["nbuilds"] == o.nbuilds
+
+
+def test_bidisperse_long_lists_serial_path():
+    """Two 3 mm spheres buried in a bed of 0.3 mm ones: each has ~177
+    neighbour-list pairs, more than 64 on a side, so its pairs are evaluated
+    serially in the reference order by the tail kernel; bit for bit."""
+    sc = S.bidisperse_bed()
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    p = o.pairs()
+    tags, counts = np.unique(np.concatenate([p["tag_i"], p["tag_j"]]), return_counts=True)
+    assert counts.max() > 128, "no atom with a long list"
+    big_touch = 0
+    for _ in range(6):
+        e.run(250)
+        o.run(250)
+        assert_atoms_equal(e, o)
+        assert_pairs_equal(e, o)
+        q = o.pairs()
+        big = np.isin(q["tag_i"], [1, 2]) | np.isin(q["tag_j"], [1, 2])
+        big_touch += int(((q["flag"] != 0) & big).sum())
+        assert np.array_equal(e.wall_hist(1), o.wall_hist(1))
+    assert big_touch > 0, "the large spheres touched nothing"
+    assert e.stats()["nbuilds"] == o.nbuilds
