@@ -154,3 +154,31 @@ def test_bidisperse_long_lists_serial_path():
         assert np.array_equal(e.wall_hist(1), o.wall_hist(1))
     assert big_touch > 0, "the large spheres touched nothing"
     assert e.stats()["nbuilds"] == o.nbuilds
+
+
+def test_two_types_neighbor_schedule_no_tangential_damping():
+    """Two atom types with different materials (type-pair lookups in both
+    orders), neigh_modify every 3 delay 6 check yes and every 5 check no
+    (the decide() schedule without the queue), tangential damping off;
+    bit for bit, including the rebuild count."""
+    for every, delay, check in ((3, 6, 1), (5, 0, 0)):
+        sc = S.sphere_pour(n=2000, seed=21, vmax=0.3)
+        n = len(sc["atoms"]["tag"])
+        sc["atoms"]["type"] = np.where(np.arange(n) % 3 == 0, 2, 1).astype(np.int32)
+        sc["ntypes"] = 2
+        sc["youngs"] = np.array([5e6, 2e7])
+        sc["poisson"] = np.array([0.45, 0.3])
+        sc["restitution"] = np.array([[0.3, 0.5], [0.5, 0.7]])
+        sc["friction"] = np.array([[0.5, 0.2], [0.2, 0.4]])
+        sc["rollfriction"] = np.array([[0.0, 0.0], [0.0, 0.0]])
+        sc["every"], sc["delay"], sc["check"] = every, delay, check
+        sc["tangential_damping"] = 0
+        e, o = _pair(sc)
+        e.setup()
+        o.setup()
+        for _ in range(4):
+            e.run(300)
+            o.run(300)
+            assert_atoms_equal(e, o)
+            assert_pairs_equal(e, o)
+        assert e.stats()["nbuilds"] == o.nbuilds > 1
