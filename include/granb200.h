@@ -164,6 +164,12 @@ int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, doub
    the pair count in *n, writes at most cap entries */
 int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
 /* per-atom shear history of primitive-wall fix ifix, [nlocal][3] */
+/* compute contact/atom (src/compute_contact_atom.cpp ComputeContactAtom::
+ * compute_peratom, skin 0): per owned atom the number of half-list pairs with
+ * rsq <= (r_i + r_j)^2, as a double, with its tag; cap < nlocal or contact ==
+ * NULL only reports the count in *n.  Positions are those of the last step
+ * (or of setup). */
+int gb2_contact_atom(gb2_ctx *ctx, int cap, int *n, int *tag, double *contact);
 int gb2_download_wall_history(gb2_ctx *ctx, int ifix, int cap, double *hist);
 /* occupied mesh-contact slots of mesh fix ifix: (atom tag, triangle id, shear[3]) */
 int gb2_download_mesh_contacts(gb2_ctx *ctx, int ifix, int cap, int *n, int *tag, int *tri, double *hist);

@@ -1834,6 +1834,26 @@ int gb2_download_pairs(gb2_ctx *c, int cap, int *n, int *tag_i, int *tag_j, int 
     return 0;
 }
 
+int gb2_contact_atom(gb2_ctx *c, int cap, int *n, int *tag, double *contact)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no neighbor list before setup");
+    const int nl = c->nlocal;
+    if (n) *n = nl;
+    if (!contact || cap < nl) return 0;
+    DBuf<double> d;
+    CK(d.alloc(nl > 0 ? nl : 1));
+    if (nl > 0) {
+        Dev D = make_dev(c);
+        k_contact_atom<<<nblk(nl), kBlock, 0, c->st>>>(D, d.p);
+        CKL();
+        CK(cudaMemcpyAsync(contact, d.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, c->st));
+        if (tag) CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
 int gb2_download_wall_history(gb2_ctx *c, int ifix, int cap, double *hist)
 {
     if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_PLANE) return GB2_ERR_ARG;

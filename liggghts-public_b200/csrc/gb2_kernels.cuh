@@ -780,5 +780,33 @@ __global__ void k_tail_list(Dev D)
 // have asked for a rebuild of the next one through the displacement flag.
 __global__ void k_queue_start(int *dstop, const int *dflag, int step) { *dstop = *dflag ? step : 0x7f7f7f7f; }
 
+// ComputeContactAtom::compute_peratom with skin 0 (src/compute_contact_atom.cpp):
+// contact if rsq <= (radi + radj)^2; an owned atom counts its own half-list
+// entries and the entries where it is the j side (newton off: an image pair
+// across a periodic boundary is in both owners' lists).
+__global__ void k_contact_atom(Dev D, double *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.nlocal) return;
+    const int cap = D.cap;
+    const dbl4 pk = D.pos[k];
+    int cnt = 0;
+    for (int s = 0; s < D.nnum[k]; s++) {
+        const dbl4 pj = D.pos[D.nbr[s * cap + k]];
+        const double delx = pk.x - pj.x, dely = pk.y - pj.y, delz = pk.z - pj.z;
+        const double rsq = delx * delx + dely * dely + delz * delz;
+        const double radsum = pk.w + pj.w + 0.0;
+        if (rsq <= radsum * radsum) cnt++;
+    }
+    for (int r = 0; r < D.rnum[k]; r++) {
+        const dbl4 pi = D.pos[D.rev[r * cap + k]];
+        const double delx = pi.x - pk.x, dely = pi.y - pk.y, delz = pi.z - pk.z;
+        const double rsq = delx * delx + dely * dely + delz * delz;
+        const double radsum = pi.w + pk.w + 0.0;
+        if (rsq <= radsum * radsum) cnt++;
+    }
+    out[k] = (double)cnt;
+}
+
 }  // namespace gb2
 

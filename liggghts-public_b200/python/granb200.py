@@ -28,7 +28,7 @@ EXPORTS = (
     "gb2_download_pairs", "gb2_download_wall_history", "gb2_download_mesh_contacts", "gb2_mesh_topology",
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
     "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
-    "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder",
+    "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -107,6 +107,7 @@ def lib(path=LIB_PATH):
         L.gb2_download_atoms.argtypes = [vp, ctypes.c_int, I, D, D, D, D, D, I]
         L.gb2_download_pairs.argtypes = [vp, ctypes.c_int, I, I, I, I, D]
         L.gb2_download_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
+        L.gb2_contact_atom.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), I, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
         L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -291,6 +292,14 @@ class Engine:
         hi = np.zeros((n, 3))
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def contact_atom(self):
+        """compute contact/atom (skin 0) on the device: {tag, contact}."""
+        n = ctypes.c_int()
+        tag = np.zeros(self.n, dtype=np.int32)
+        out = np.zeros(self.n)
+        self._check(self.L.gb2_contact_atom(self.h, self.n, ctypes.byref(n), _ip(tag), _dp(out)))
+        return {"tag": tag, "contact": out}
 
     def wall_hist(self, ifix):
         h = np.zeros((self.n, 3))

@@ -2018,6 +2018,32 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
     return k;
 }
 
+/* ComputeContactAtom::compute_peratom with skin 0 (src/compute_contact_atom.cpp:
+   contact if rsq <= (radi + radj)^2 over the half list, tallied for i and j;
+   newton off, so ghost tallies are dropped): per owned atom, in atom order */
+int orc_contact_atom(orc_sim *s, double *out)
+{
+    const int nall = s->nlocal + s->nghost;
+    double *contact = calloc((size_t)(nall > 0 ? nall : 1), sizeof(double));
+    for (int i = 0; i < s->nlocal; i++) {
+        const double xtmp = s->x[3*i], ytmp = s->x[3*i+1], ztmp = s->x[3*i+2], radi = s->radius[i];
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            const int j = s->nbr[s->nstart[i] + jj];
+            const double delx = xtmp - s->x[3*j], dely = ytmp - s->x[3*j+1], delz = ztmp - s->x[3*j+2];
+            const double rsq = delx*delx + dely*dely + delz*delz;
+            const double radsum = radi + s->radius[j] + 0.0;
+            const double radsumsq = radsum*radsum;
+            if (rsq <= radsumsq) {
+                contact[i] += 1.0;
+                contact[j] += 1.0;
+            }
+        }
+    }
+    memcpy(out, contact, sizeof(double)*s->nlocal);
+    free(contact);
+    return s->nlocal;
+}
+
 int orc_get_wall_hist(orc_sim *s, int ifix, double *hist)
 {
     if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wp) return -1;

@@ -91,6 +91,8 @@ void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega,
                    double *f, double *torque, int *tag);
 /* half-list pairs: returns count; arrays may be NULL to query count */
 int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist);
+/* compute contact/atom (skin 0) per owned atom, atom order */
+int orc_contact_atom(orc_sim *s, double *out);
 /* per-atom primitive-wall shear history of fix index ifix (3 per atom) */
 int orc_get_wall_hist(orc_sim *s, int ifix, double *hist);
 /* mesh contacts of fix ifix: (tag, tri id, hist[3]) for every occupied slot */

@@ -73,6 +73,7 @@ def lib():
         L.orc_add_move_mesh_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 7
         L.orc_get_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_add_move_mesh_linear.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
+        L.orc_contact_atom.argtypes = [ctypes.c_void_p, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
         L.orc_error.restype = ctypes.c_char_p
         L.orc_error.argtypes = [ctypes.c_void_p]
@@ -199,6 +200,12 @@ class Oracle:
                              _dp(out["torque"]), _ip(tag))
         out["tag"] = tag
         return out
+
+    def contact_atom(self):
+        """compute contact/atom (skin 0): {tag, contact} per owned atom."""
+        out = np.zeros(self.nlocal)
+        self.L.orc_contact_atom(self.h, _dp(out))
+        return {"tag": self.atoms()["tag"], "contact": out}
 
     def pairs(self):
         n = self.L.orc_get_pairs(self.h, 0, None, None, None, None)

@@ -152,7 +152,10 @@ def test_bidisperse_long_lists_serial_path():
         big = np.isin(q["tag_i"], [1, 2]) | np.isin(q["tag_j"], [1, 2])
         big_touch += int(((q["flag"] != 0) & big).sum())
         assert np.array_equal(e.wall_hist(1), o.wall_hist(1))
+        ca, cb = e.contact_atom(), o.contact_atom()
+        assert np.array_equal(ca["tag"], cb["tag"]) and np.array_equal(ca["contact"], cb["contact"])
     assert big_touch > 0, "the large spheres touched nothing"
+    assert e.contact_atom()["contact"].max() > 10, "no large sphere with many contacts"
     assert e.stats()["nbuilds"] == o.nbuilds
 
 
