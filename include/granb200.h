@@ -164,6 +164,21 @@ int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, doub
    the pair count in *n, writes at most cap entries */
 int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
 /* per-atom shear history of primitive-wall fix ifix, [nlocal][3] */
+/* restart interoperability: the contact history in FixContactHistory's
+ * per-atom partner layout (src/fix_contact_history.cpp:588-640 pack_restart /
+ * unpack_restart): per atom npartner, then per partner its tag and 3 shear
+ * values as seen from the atom, concatenated over atoms.  Upload: after
+ * gb2_upload_atoms (same atom order), before gb2_setup; the setup's build
+ * restores the history of pairs touching there.  Download: the current
+ * history (FixContactHistory::pre_exchange from the current list), per owned
+ * atom in the current order with its tag; *n atoms, *ntotal partners, and
+ * with caps too small only the counts. */
+int gb2_upload_history(gb2_ctx *ctx, int n, const int *npartner, const int *partner_tag, const double *hist);
+int gb2_download_history(gb2_ctx *ctx, int cap_atoms, int cap_partners, int *n, int *ntotal, int *tag,
+                         int *npartner, int *partner_tag, double *hist);
+/* primitive-wall shear history of wall fix ifix for the uploaded atoms (3 per
+ * atom, upload order), before gb2_setup (FixWallGran restart data) */
+int gb2_upload_wall_history(gb2_ctx *ctx, int ifix, int n, const double *hist);
 /* compute contact/atom (src/compute_contact_atom.cpp ComputeContactAtom::
  * compute_peratom, skin 0): per owned atom the number of half-list pairs with
  * rsq <= (r_i + r_j)^2, as a double, with its tag; cap < nlocal or contact ==

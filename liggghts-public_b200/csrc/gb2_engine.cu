@@ -1854,6 +1854,98 @@ int gb2_contact_atom(gb2_ctx *c, int cap, int *n, int *tag, double *contact)
     return 0;
 }
 
+// Restart: the contact history in FixContactHistory's per-atom partner layout
+// (src/fix_contact_history.cpp:588-640, pack_restart / unpack_restart): per
+// atom its partner count, then each partner's tag and 3 shear values as seen
+// from the atom.  The upload fills the partner arrays before setup, so the
+// setup's neighbour build restores the history of pairs touching there,
+// as after read_restart (setup_pre_exchange skips the rebuild of the
+// partner arrays).
+int gb2_upload_history(gb2_ctx *c, int n, const int *npartner, const int *partner_tag, const double *hist)
+{
+    if (!c || !npartner || (n > 0 && (!partner_tag || !hist))) return GB2_ERR_ARG;
+    if (!c->have_atoms || c->setup_done) return set_err(c, GB2_ERR_STATE, "history is uploaded after the atoms, before setup");
+    if (n != c->nlocal) return set_err(c, GB2_ERR_ARG, "history for %d atoms, %d uploaded", n, c->nlocal);
+    int mx = 0;
+    for (int i = 0; i < n; i++) {
+        if (npartner[i] < 0) return set_err(c, GB2_ERR_ARG, "negative partner count");
+        mx = std::max(mx, npartner[i]);
+    }
+    if (mx > c->maxp) {
+        c->maxp = grown_capacity(c, 1, mx, 1 << 20);
+        CK(c->ptag.alloc((size_t)c->maxp * c->cap));
+        CK(c->phist.alloc((size_t)3 * c->maxp * c->cap));
+    }
+    const size_t cp = c->cap;
+    std::vector<int> pn(cp, 0), pt((size_t)c->maxp * cp, 0);
+    std::vector<double> ph((size_t)3 * c->maxp * cp, 0.0);
+    size_t off = 0;
+    for (int i = 0; i < n; i++) {
+        pn[i] = npartner[i];
+        for (int m = 0; m < npartner[i]; m++, off++) {
+            pt[(size_t)m * cp + i] = partner_tag[off];
+            for (int q = 0; q < 3; q++) ph[(size_t)(3 * m + q) * cp + i] = hist[3 * off + q];
+        }
+    }
+    CK(cudaMemcpyAsync(c->pnum.p, pn.data(), sizeof(int) * cp, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->ptag.p, pt.data(), sizeof(int) * pt.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->phist.p, ph.data(), sizeof(double) * ph.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->computeflag = false;
+    return 0;
+}
+
+// The current contact history in the same layout (FixContactHistory::
+// pre_exchange run on the device from the current list), per owned atom in
+// the current atom order with its tag.  *n = atoms, *ntotal = partners; with
+// caps too small only the counts are reported.
+int gb2_download_history(gb2_ctx *c, int cap_atoms, int cap_partners, int *n, int *ntotal, int *tag, int *npartner,
+                         int *partner_tag, double *hist)
+{
+    if (!c) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no neighbor list before setup");
+    if (do_partners(c)) return c->err.empty() ? GB2_ERR_CUDA : GB2_ERR_CAPACITY;
+    const size_t cp = c->cap;
+    const int nl = c->nlocal;
+    std::vector<int> pn(nl > 0 ? nl : 1), pt((size_t)c->maxp * cp), tg(nl > 0 ? nl : 1);
+    std::vector<double> ph((size_t)3 * c->maxp * cp);
+    CK(cudaMemcpyAsync(pn.data(), c->pnum.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(pt.data(), c->ptag.p, sizeof(int) * pt.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ph.data(), c->phist.p, sizeof(double) * ph.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(tg.data(), c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    long tot = 0;
+    for (int i = 0; i < nl; i++) tot += pn[i];
+    if (n) *n = nl;
+    if (ntotal) *ntotal = (int)tot;
+    if (cap_atoms < nl || cap_partners < tot || !tag || !npartner || !partner_tag || !hist) return 0;
+    size_t off = 0;
+    for (int i = 0; i < nl; i++) {
+        tag[i] = tg[i];
+        npartner[i] = pn[i];
+        for (int m = 0; m < pn[i]; m++, off++) {
+            partner_tag[off] = pt[(size_t)m * cp + i];
+            for (int q = 0; q < 3; q++) hist[3 * off + q] = ph[(size_t)(3 * m + q) * cp + i];
+        }
+    }
+    return 0;
+}
+
+// Primitive-wall shear history (FixWallGran's per-atom history, part of its
+// restart data) for the uploaded atoms, before setup.
+int gb2_upload_wall_history(gb2_ctx *c, int ifix, int n, const double *hist)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_PLANE || !hist) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "wall history is uploaded before setup");
+    if (n != c->nlocal) return set_err(c, GB2_ERR_ARG, "wall history for %d atoms, %d uploaded", n, c->nlocal);
+    std::vector<double> h((size_t)3 * c->cap, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int q = 0; q < 3; q++) h[(size_t)q * c->cap + i] = hist[3 * i + q];
+    CK(cudaMemcpyAsync(c->fix[ifix].whist.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
 int gb2_download_wall_history(gb2_ctx *c, int ifix, int cap, double *hist)
 {
     if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_PLANE) return GB2_ERR_ARG;

@@ -29,6 +29,7 @@ EXPORTS = (
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
     "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
+    "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -108,6 +109,10 @@ def lib(path=LIB_PATH):
         L.gb2_download_pairs.argtypes = [vp, ctypes.c_int, I, I, I, I, D]
         L.gb2_download_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_contact_atom.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), I, D]
+        L.gb2_upload_history.argtypes = [vp, ctypes.c_int, I, I, D]
+        L.gb2_download_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int), I, I, I, D]
+        L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
         L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -292,6 +297,30 @@ class Engine:
         hi = np.zeros((n, 3))
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def upload_history(self, npartner, partner_tag, hist):
+        """FixContactHistory restart data (per atom: partner count, tags and
+        shear) for the atoms as uploaded; before setup."""
+        a = [np.ascontiguousarray(npartner, dtype=np.int32), np.ascontiguousarray(partner_tag, dtype=np.int32),
+             np.ascontiguousarray(hist, dtype=np.float64)]
+        self._check(self.L.gb2_upload_history(self.h, len(a[0]), _ip(a[0]), _ip(a[1]), _dp(a[2])))
+
+    def upload_wall_hist(self, ifix, hist):
+        h = np.ascontiguousarray(hist, dtype=np.float64)
+        self._check(self.L.gb2_upload_wall_history(self.h, self.fix_ids[ifix], len(h), _dp(h)))
+
+    def history(self):
+        """Current contact history in the partner layout: tag, npartner, partner_tag, hist."""
+        n, tot = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.gb2_download_history(self.h, 0, 0, ctypes.byref(n), ctypes.byref(tot), None, None, None,
+                                                None))
+        tag = np.zeros(n.value, dtype=np.int32)
+        npart = np.zeros(n.value, dtype=np.int32)
+        pt = np.zeros(tot.value, dtype=np.int32)
+        ph = np.zeros((tot.value, 3))
+        self._check(self.L.gb2_download_history(self.h, n.value, tot.value, ctypes.byref(n), ctypes.byref(tot),
+                                                _ip(tag), _ip(npart), _ip(pt), _dp(ph)))
+        return {"tag": tag, "npartner": npart, "partner_tag": pt, "hist": ph}
 
     def contact_atom(self):
         """compute contact/atom (skin 0) on the device: {tag, contact}."""

@@ -2018,6 +2018,51 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
     return k;
 }
 
+/* restart: FixContactHistory::unpack_restart (src/fix_contact_history.cpp:608)
+   for the atoms as added (before setup; computeflag 0 so setup keeps them) */
+int orc_upload_history(orc_sim *s, int n, const int *npartner, const int *ptag, const double *hist)
+{
+    if (n != s->nlocal) { fail(s, "history for %d atoms, %d added", n, s->nlocal); return -1; }
+    size_t off = 0;
+    for (int i = 0; i < n; i++) {
+        free(s->partner[i]); free(s->phist[i]);
+        s->npartner[i] = npartner[i];
+        s->partner[i] = malloc(sizeof(int)*(npartner[i] > 0 ? npartner[i] : 1));
+        s->phist[i] = malloc(sizeof(double)*3*(npartner[i] > 0 ? npartner[i] : 1));
+        for (int m = 0; m < npartner[i]; m++, off++) {
+            s->partner[i][m] = ptag[off];
+            for (int d = 0; d < 3; d++) s->phist[i][3*m+d] = hist[3*off+d];
+        }
+    }
+    s->computeflag = 0;
+    return 0;
+}
+
+/* pack_restart after FixContactHistory::pre_exchange: per owned atom (atom
+   order) its partners; returns the partner total (arrays may be NULL) */
+int orc_get_history(orc_sim *s, int *npartner, int *ptag, double *hist)
+{
+    history_pre_exchange(s);
+    s->computeflag = 1;   /* the pair keeps computing; the next build rebuilds the arrays */
+    int tot = 0;
+    for (int i = 0; i < s->nlocal; i++) {
+        if (npartner) npartner[i] = s->npartner[i];
+        for (int m = 0; m < s->npartner[i]; m++, tot++) {
+            if (ptag) ptag[tot] = s->partner[i][m];
+            if (hist) for (int d = 0; d < 3; d++) hist[3*tot+d] = s->phist[i][3*m+d];
+        }
+    }
+    return tot;
+}
+
+/* FixWallGran restart data: per-atom wall shear history, before setup */
+int orc_upload_wall_hist(orc_sim *s, int ifix, int n, const double *hist)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wp || n != s->nlocal) return -1;
+    memcpy(s->fix[ifix].wp->hist, hist, sizeof(double)*3*n);
+    return 0;
+}
+
 /* ComputeContactAtom::compute_peratom with skin 0 (src/compute_contact_atom.cpp:
    contact if rsq <= (radi + radj)^2 over the half list, tallied for i and j;
    newton off, so ghost tallies are dropped): per owned atom, in atom order */

@@ -91,6 +91,10 @@ void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega,
                    double *f, double *torque, int *tag);
 /* half-list pairs: returns count; arrays may be NULL to query count */
 int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist);
+/* restart: contact history in FixContactHistory's partner layout */
+int orc_upload_history(orc_sim *s, int n, const int *npartner, const int *ptag, const double *hist);
+int orc_get_history(orc_sim *s, int *npartner, int *ptag, double *hist);
+int orc_upload_wall_hist(orc_sim *s, int ifix, int n, const double *hist);
 /* compute contact/atom (skin 0) per owned atom, atom order */
 int orc_contact_atom(orc_sim *s, double *out);
 /* per-atom primitive-wall shear history of fix index ifix (3 per atom) */

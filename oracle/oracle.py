@@ -74,6 +74,9 @@ def lib():
         L.orc_get_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_add_move_mesh_linear.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_contact_atom.argtypes = [ctypes.c_void_p, D]
+        L.orc_upload_history.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, D]
+        L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
+        L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
         L.orc_error.restype = ctypes.c_char_p
         L.orc_error.argtypes = [ctypes.c_void_p]
@@ -200,6 +203,27 @@ class Oracle:
                              _dp(out["torque"]), _ip(tag))
         out["tag"] = tag
         return out
+
+    def upload_history(self, npartner, partner_tag, hist):
+        """FixContactHistory restart data for the atoms as added (before setup)."""
+        a = [np.ascontiguousarray(npartner, dtype=np.int32), np.ascontiguousarray(partner_tag, dtype=np.int32),
+             np.ascontiguousarray(hist, dtype=np.float64)]
+        if self.L.orc_upload_history(self.h, len(a[0]), _ip(a[0]), _ip(a[1]), _dp(a[2])) != 0:
+            raise RuntimeError("orc_upload_history failed")
+
+    def upload_wall_hist(self, ifix, hist):
+        h = np.ascontiguousarray(hist, dtype=np.float64)
+        if self.L.orc_upload_wall_hist(self.h, self.fix_ids[ifix], len(h), _dp(h)) != 0:
+            raise RuntimeError("orc_upload_wall_hist failed")
+
+    def history(self):
+        """Current contact history in the partner layout: tag, npartner, partner_tag, hist."""
+        npart = np.zeros(self.nlocal, dtype=np.int32)
+        tot = self.L.orc_get_history(self.h, _ip(npart), None, None)
+        pt = np.zeros(tot, dtype=np.int32)
+        ph = np.zeros((tot, 3))
+        self.L.orc_get_history(self.h, _ip(npart), _ip(pt), _dp(ph))
+        return {"tag": self.atoms()["tag"], "npartner": npart, "partner_tag": pt, "hist": ph}
 
     def contact_atom(self):
         """compute contact/atom (skin 0): {tag, contact} per owned atom."""

@@ -185,3 +185,65 @@ def test_two_types_neighbor_schedule_no_tangential_damping():
             assert_atoms_equal(e, o)
             assert_pairs_equal(e, o)
         assert e.stats()["nbuilds"] == o.nbuilds > 1
+
+
+def _restart_scenario(sc, atoms):
+    """The scenario with its atoms replaced by a run's current state (same
+    tags, the run's atom order), as read_restart would bring them back."""
+    out = dict(sc)
+    a = dict(sc["atoms"])
+    pos_of_tag = {t: k for k, t in enumerate(a["tag"])}
+    idx = np.array([pos_of_tag[t] for t in atoms["tag"]])
+    for k in a:
+        a[k] = np.ascontiguousarray(np.asarray(a[k])[idx])
+    for k in ("x", "v", "omega"):
+        a[k] = np.ascontiguousarray(atoms[k])
+    a["tag"] = np.ascontiguousarray(atoms["tag"])
+    out["atoms"] = a
+    return out
+
+
+def test_restart_history_roundtrip():
+    """Restart interoperability: the contact history downloaded in
+    FixContactHistory's partner layout equals the oracle's, and a run
+    restarted from it (atoms, partner history, wall history) matches the
+    oracle restarted from the same data bit for bit; right after the restart
+    every touching pair carries the shear it had before."""
+    sc = S.sphere_pour(n=2000, seed=8, vmax=0.3)
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    e.run(700)
+    o.run(700)
+    assert_atoms_equal(e, o)
+    he, ho = e.history(), o.history()
+    for k in ("tag", "npartner", "partner_tag", "hist"):
+        assert np.array_equal(he[k], ho[k]), "history %s differs from the oracle" % k
+    assert he["npartner"].sum() > 100, "too few contacts to test a restart"
+    before = e.pairs()
+    sc2 = _restart_scenario(sc, e.atoms())
+    wall = e.wall_hist(1)
+    import granb200
+    e2, o2 = granb200.Engine(sc2), oracle.Oracle(sc2)
+    for x in (e2, o2):
+        x.upload_history(he["npartner"], he["partner_tag"], he["hist"])
+        x.upload_wall_hist(1, wall)
+        x.setup()
+    assert_atoms_equal(e2, o2)
+    assert_pairs_equal(e2, o2)
+    after = e2.pairs()
+    key = {(i, j): h for i, j, h, f in zip(before["tag_i"], before["tag_j"], before["hist"], before["flag"]) if f}
+    carried = 0
+    for i, j, h, f in zip(after["tag_i"], after["tag_j"], after["hist"], after["flag"]):
+        if f and (i, j) in key:
+            assert np.array_equal(h, key[(i, j)]), "shear of pair %d-%d not carried over" % (i, j)
+            carried += 1
+        elif f and (j, i) in key:
+            assert np.array_equal(h, -key[(j, i)]), "shear of pair %d-%d not carried over" % (i, j)
+            carried += 1
+    assert carried > 50
+    for _ in range(3):
+        e2.run(300)
+        o2.run(300)
+        assert_atoms_equal(e2, o2)
+        assert_pairs_equal(e2, o2)
