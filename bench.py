@@ -33,6 +33,10 @@ UNIT = "particle-steps/s"
 
 
 def parse():
+    return parse_list(None)
+
+
+def parse_list(argv):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4000)
@@ -48,7 +52,7 @@ def parse():
                     help="timed steps of the plain FP64 form on the same state (-1: as many as --steps, 0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def make_workload(args, seed_offset=0):
@@ -223,36 +227,69 @@ def allmax(dist, x):
     return float(t.item())
 
 
-def reference_arm(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
+def _ref_worker(argv, seconds, barrier, out):
+    """One replica of the reference arm: the oracle port (the reference's
+    algorithm, single-threaded) on the workload, timed for ~`seconds`."""
+    args = parse_list(argv)
     sc, desc, extra = make_workload(args)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     o = oracle.Oracle(sc)
     o.setup()
-    settle = min(args.settle, 200)
-    o.run(settle)
-    w = min(args.warmup, 3)
-    o.run(w)
+    o.run(min(args.settle, 200))
+    o.run(min(args.warmup, 3))
     n = len(sc["atoms"]["tag"])
-    t0 = time.perf_counter()
-    o.run(1)
-    one = time.perf_counter() - t0
-    k = int(max(1, min(args.steps, 30.0 / max(one, 1e-6))))
-    t0 = time.perf_counter()
-    o.run(k)
+    barrier.wait()
+    k, t0 = 0, time.perf_counter()
+    while k < max(args.steps, 1):
+        o.run(1)
+        k += 1
+        if time.perf_counter() - t0 > seconds:
+            break
     dt = time.perf_counter() - t0
-    val = n * k / dt
-    sample = "%s; oracle port (1 thread) after %d settle + %d warm-up steps, %d timed steps" % (desc, settle, w, k)
+    out.put((n * k / dt, k, dt))
+
+
+def reference_arm(args):
+    """The reference's CPU path (the oracle port: its algorithm, restated in
+    C, single-threaded like the reference without MPI) on all host cores the
+    process may use: one replica per core on the same workload, timed
+    together; value = the replicas' summed particle-steps/s."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    n_est = args.n or (20_000 if args.workload == "pour" else 1_000_000)
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        avail = 8 << 30
+    per = 400 + 900 * n_est          # bytes per replica (measured ~0.84 GB at 1M atoms)
+    nproc = max(1, min(cores, int(0.6 * avail // per)))
+    ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(nproc), ctx.Queue()
+    seconds = 20.0
+    procs = [ctx.Process(target=_ref_worker, args=(sys.argv[1:], seconds, barrier, out)) for _ in range(nproc)]
+    for p in procs:
+        p.start()
+    res = [out.get() for _ in range(nproc)]
+    for p in procs:
+        p.join()
+    val = sum(r[0] for r in res)
+    k = min(r[1] for r in res)
+    dt = max(r[2] for r in res)
+    sc, desc, extra = make_workload(args)
+    settle, w = min(args.settle, 200), min(args.warmup, 3)
+    sample = ("%s; oracle port, %d single-threaded replicas on %d host cores, each after %d settle + %d warm-up "
+              "steps, ~%.0f s timed together (>= %d steps each)" % (desc, nproc, cores, settle, w, seconds, k))
     line = {
         "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": k, "warmup": w,
         "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": dict({"workload": desc, "settle_steps": settle}, **extra),
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
