@@ -164,6 +164,16 @@ int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, doub
    the pair count in *n, writes at most cap entries */
 int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
 /* per-atom shear history of primitive-wall fix ifix, [nlocal][3] */
+/* fix mesh/surface/stress on mesh wall fix ifix (before setup): the force of
+ * every wall contact, negated, is added to its triangle and to the mesh's
+ * f_total / torque_total about p_ref each step (MeshModuleStress::
+ * add_particle_contribution, src/mesh_module_stress.cpp:276-304; zeroed per
+ * step as FixMesh::pre_force / MeshModuleStress::pre_force do).  Sums are
+ * device atomics: equal to the reference to rounding, not bit for bit. */
+int gb2_add_mesh_stress(gb2_ctx *ctx, int ifix, const double p_ref[3]);
+/* the last step's per-triangle force (3 per triangle, cap >= ntri) and
+ * tot6 = f_total[3], torque_total[3] */
+int gb2_download_mesh_stress(gb2_ctx *ctx, int ifix, int cap, double *tri_f, double *tot6);
 /* restart interoperability: the contact history in FixContactHistory's
  * per-atom partner layout (src/fix_contact_history.cpp:588-640 pack_restart /
  * unpack_restart): per atom npartner, then per partner its tag and 3 shear

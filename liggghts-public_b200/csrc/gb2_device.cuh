@@ -473,11 +473,30 @@ static __device__ bool mesh_contact(const Dev &D, const MeshDev &M, int i, int t
         const double *vn = M.vnode + 9 * t;
         for (int c = 0; c < 3; c++) vwall[c] = (bary[0] * vn[c] + bary[1] * vn[3 + c] + bary[2] * vn[6 + c]);
     }
+    // the contact's own force first (-0.0 + x == x), then added to acc: the
+    // same IEEE additions as accumulating in place
+    ContactOut wc;
+    for (int c = 0; c < 3; c++) wc.F[c] = wc.T[c] = -0.0;
     wall_contact(mat(D, itype, M.wtype), dvec, -deltan, p.w, v, w, vwall, mass, sh, upd, D.dt, M.rolling != 0,
-                 D.tdamp != 0, acc);
+                 D.tdamp != 0, wc);
+    for (int c = 0; c < 3; c++) {
+        acc.F[c] += wc.F[c];
+        acc.T[c] += wc.T[c];
+    }
     M.shist[(3 * slot + 0) * cap + i] = sh[0];
     M.shist[(3 * slot + 1) * cap + i] = sh[1];
     M.shist[(3 * slot + 2) * cap + i] = sh[2];
+    if (M.trif) {   // MeshModuleStress::add_particle_contribution (src/mesh_module_stress.cpp:276-304)
+        const double frc[3] = {-wc.F[0], -wc.F[1], -wc.F[2]};
+        const double tmp[3] = {p.x + delta[0] - M.pref[0], p.y + delta[1] - M.pref[1], p.z + delta[2] - M.pref[2]};
+        const double tq[3] = {tmp[1] * frc[2] - tmp[2] * frc[1], tmp[2] * frc[0] - tmp[0] * frc[2],
+                              tmp[0] * frc[1] - tmp[1] * frc[0]};
+        for (int c = 0; c < 3; c++) {
+            atomicAdd(&M.trif[3 * t + c], frc[c]);
+            atomicAdd(&M.ftot[c], frc[c]);
+            atomicAdd(&M.ftot[3 + c], tq[c]);
+        }
+    }
     return true;
 }
 

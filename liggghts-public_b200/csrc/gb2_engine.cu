@@ -99,6 +99,10 @@ struct MeshFix {
     DBuf<int> trange, tcount, toff, bincnt, pvals;
     DBuf<unsigned> pkeys, pkeys2;
     long next_reneighbor = -1;   // FixMesh::next_reneighbor
+    // fix mesh/surface/stress
+    bool stress = false;
+    double pref[3] = {0, 0, 0};
+    DBuf<double> trif, ftot;
 };
 
 struct HostFix {
@@ -317,6 +321,9 @@ Dev make_dev(gb2_ctx *c)
             m.spartner = M.spartner.p;
             m.shist = M.shist.p;
             m.vnode = M.moving ? M.vnode.p : nullptr;
+            m.trif = M.stress ? M.trif.p : nullptr;
+            m.ftot = M.stress ? M.ftot.p : nullptr;
+            for (int d = 0; d < 3; d++) m.pref[d] = M.pref[d];
         }
     }
     D.status = c->dstatus.p;
@@ -1035,6 +1042,15 @@ void launch_tail(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
 int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int store_f)
 {
     if (fuse_next && !c->queue_active) CK(cudaMemsetAsync(c->ddflag.p, 0, sizeof(int), c->st));
+    // mesh/surface/stress: FixMesh::pre_force clears the per-element force,
+    // MeshModuleStress::pre_force the totals (before the pair step, so the
+    // tail kernel stays the pair step's dependent launch)
+    for (int k = 0; k < c->nfix; k++) {
+        MeshFix *M = c->fix[k].mesh;
+        if (!M || !M->stress) continue;
+        CK(cudaMemsetAsync(M->trif.p, 0, sizeof(double) * 3 * M->topo.tri.size(), c->st));
+        CK(cudaMemsetAsync(M->ftot.p, 0, sizeof(double) * 6, c->st));
+    }
     Dev D = make_dev(c);
     gb2_ctx::EvPair e;
     if (prof_begin(c, PROF_PAIR_MAIN, &e)) return GB2_ERR_CUDA;
@@ -1850,6 +1866,36 @@ int gb2_contact_atom(gb2_ctx *c, int cap, int *n, int *tag, double *contact)
         CK(cudaMemcpyAsync(contact, d.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, c->st));
         if (tag) CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
     }
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// fix mesh/surface/stress on mesh wall fix ifix (before setup): per-element
+// force and the totals about p_ref accumulated from the wall contacts of each
+// step (MeshModuleStress::add_particle_contribution, src/mesh_module_stress.cpp:276)
+int gb2_add_mesh_stress(gb2_ctx *c, int ifix, const double p_ref[3])
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !p_ref) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "mesh/surface/stress is added before setup");
+    MeshFix &M = *c->fix[ifix].mesh;
+    CK(M.trif.alloc((size_t)3 * std::max<size_t>(M.topo.tri.size(), 1)));
+    CK(M.ftot.alloc(6));
+    CK(cudaMemsetAsync(M.trif.p, 0, sizeof(double) * 3 * M.topo.tri.size(), c->st));
+    CK(cudaMemsetAsync(M.ftot.p, 0, sizeof(double) * 6, c->st));
+    M.stress = true;
+    for (int d = 0; d < 3; d++) M.pref[d] = p_ref[d];
+    return 0;
+}
+
+// per-element force of the last step (3 per triangle) and f_total, torque_total
+int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, double *tot6)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH) return GB2_ERR_ARG;
+    MeshFix &M = *c->fix[ifix].mesh;
+    if (!M.stress) return set_err(c, GB2_ERR_STATE, "mesh/surface/stress not enabled on this mesh");
+    const int nt = (int)M.topo.tri.size();
+    if (tri_f && cap >= nt) CK(cudaMemcpyAsync(tri_f, M.trif.p, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->st));
+    if (tot6) CK(cudaMemcpyAsync(tot6, M.ftot.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return 0;
 }

@@ -94,6 +94,10 @@ struct MeshDev {
     int *spartner;         // [s*cap + i] triangle id or -1
     double *shist;         // [(3s+c)*cap + i]
     const double *vnode;   // moving mesh: node velocities [9*t + 3*node + c]; null when static
+    // mesh/surface/stress: per-element force [3t+c] and f_total, torque_total
+    // about pref of the current step; null when not tracked
+    double *trif, *ftot;
+    double pref[3];
 };
 
 struct FixDev {

@@ -29,7 +29,8 @@ EXPORTS = (
     "gb2_get_stats", "gb2_last_error", "gb2_version", "gb2_census", "gb2_set_profiling", "gb2_timer_start",
     "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
-    "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history",
+    "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
+    "gb2_download_mesh_stress",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -113,6 +114,8 @@ def lib(path=LIB_PATH):
         L.gb2_download_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int), I, I, I, D]
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
+        L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
+        L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
         L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -297,6 +300,19 @@ class Engine:
         hi = np.zeros((n, 3))
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def add_mesh_stress(self, ifix, p_ref):
+        """fix mesh/surface/stress on the mesh wall of scenario fix ifix (before setup)."""
+        pr = np.ascontiguousarray(p_ref, dtype=np.float64)
+        self._check(self.L.gb2_add_mesh_stress(self.h, self.fix_ids[ifix], _dp(pr)))
+
+    def mesh_stress(self, ifix):
+        """Per-triangle force of the last step and f_total / torque_total."""
+        nt = self.ntri[ifix]
+        f = np.zeros((nt, 3))
+        tot = np.zeros(6)
+        self._check(self.L.gb2_download_mesh_stress(self.h, self.fix_ids[ifix], nt, _dp(f), _dp(tot)))
+        return {"tri_f": f, "f_total": tot[:3], "torque_total": tot[3:]}
 
     def upload_history(self, npartner, partner_tag, hist):
         """FixContactHistory restart data (per atom: partner count, tags and

@@ -86,6 +86,8 @@ typedef struct {
     double (*vnode)[3][3];       /* element property "v" */
     double (*node_last)[3][3];   /* nodesLastRe_ */
     long next_reneighbor;        /* FixMesh::next_reneighbor */
+    /* mesh/surface/stress (MeshModuleStress): per-element force, totals */
+    int stress; double p_ref[3]; double (*tri_f)[3]; double f_total[3], torque_total[3];
 } wall_mesh;
 
 typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; int imesh; } fixrec;
@@ -454,7 +456,7 @@ void orc_destroy(orc_sim *s)
             free(m->nneighs); free(m->npartner); free(m->partner); free(m->chist); free(m->keep); free(m->isect);
             free(m->node); free(m->center); free(m->rbound); free(m->edgevec); free(m->edgelen); free(m->edgenorm);
             free(m->surfnorm); free(m->obtuse); free(m->edge_active); free(m->corner_active); free(m->nneigh); free(m->neighfaces);
-            free(m->vnode); free(m->node_last);
+            free(m->vnode); free(m->node_last); free(m->tri_f);
             if (s->fix[k].kind == ORC_FIX_WALL_MESH) free(m);
         }
     }
@@ -1349,7 +1351,8 @@ void orc_pair_force(const orc_params *p, const double xi[3], const double xj[3],
 /* ------------------------------------------------------------------ */
 /* walls: Walls::Granular::compute_force src/fix_wall_gran_base.h:148  */
 
-static void wall_compute_force(orc_sim *s, int ip, sidata_t *sd, const double *vwall, int wtype, int rolling, int shearupdate)
+static void wall_compute_force(orc_sim *s, int ip, sidata_t *sd, const double *vwall, int wtype, int rolling, int shearupdate,
+                               double *fout)
 {
     force_t fi, fj; memset(&fi, 0, sizeof fi); memset(&fj, 0, sizeof fj);
     sd->v_i = &s->v[3*ip]; sd->v_j = vwall; sd->omega_i = &s->omega[3*ip];
@@ -1366,6 +1369,7 @@ static void wall_compute_force(orc_sim *s, int ip, sidata_t *sd, const double *v
     sd->radsum = sd->radi;
     contact_chain(s, sd, &fi, &fj, rolling);
     for (int c = 0; c < 3; c++) { s->f[3*ip+c] += fi.F[c]; s->torque[3*ip+c] += fi.T[c]; }
+    if (fout) for (int c = 0; c < 3; c++) fout[c] = fi.F[c];
 }
 
 /* FixWallGran::pre_force (primitive neighlist) src/fix_wall_gran.cpp:708,
@@ -1440,7 +1444,7 @@ static void wall_plane_post_force(orc_sim *s, wall_plane *w, int shearupdate)
             sd.contact_history = hist;
             sd.deltan = -deltan;
             sd.delta[0] = -delta[0]; sd.delta[1] = -delta[1]; sd.delta[2] = -delta[2];
-            wall_compute_force(s, ip, &sd, vwall, w->wtype, w->rolling, shearupdate);
+            wall_compute_force(s, ip, &sd, vwall, w->wtype, w->rolling, shearupdate, NULL);
         } else {
             hist[0] = hist[1] = hist[2] = 0.0;
         }
@@ -1833,7 +1837,20 @@ static void mesh_post_force(orc_sim *s, wall_mesh *m, int shearupdate)
                 sd.deltan = -deltan;
                 sd.delta[0] = -delta[0]; sd.delta[1] = -delta[1]; sd.delta[2] = -delta[2];
                 sd.contact_history = hist;
-                wall_compute_force(s, ip, &sd, vw, m->wtype, m->rolling, shearupdate);
+                double frc[3];
+                wall_compute_force(s, ip, &sd, vw, m->wtype, m->rolling, shearupdate, frc);
+                if (m->stress) {   /* MeshModuleStress::add_particle_contribution src/mesh_module_stress.cpp:276-304 */
+                    double cp[3], tmp[3], tq[3];
+                    for (int c = 0; c < 3; c++) frc[c] = -frc[c];
+                    for (int c = 0; c < 3; c++) cp[c] = s->x[3*ip+c] + delta[c];
+                    for (int c = 0; c < 3; c++) m->tri_f[t][c] += frc[c];
+                    for (int c = 0; c < 3; c++) m->f_total[c] += frc[c];
+                    for (int c = 0; c < 3; c++) tmp[c] = cp[c] - m->p_ref[c];
+                    tq[0] = tmp[1]*frc[2] - tmp[2]*frc[1];
+                    tq[1] = tmp[2]*frc[0] - tmp[0]*frc[2];
+                    tq[2] = tmp[0]*frc[1] - tmp[1]*frc[0];
+                    for (int c = 0; c < 3; c++) m->torque_total[c] += tq[c];
+                }
             }
         }
     }
@@ -1912,6 +1929,12 @@ static void pre_force_all(orc_sim *s, int reneigh)
         }
         if (fr->kind == ORC_FIX_WALL_PLANE) wall_plane_pre_force(s, fr->wp);
         else if (fr->kind == ORC_FIX_WALL_MESH) { mesh_neighlist_pre_force(s, fr->wm); mesh_history_pre_force(s, fr->wm); }
+        if (fr->kind == ORC_FIX_WALL_MESH && fr->wm->stress) {
+            /* FixMesh::pre_force clearReverse (per-element "f"), MeshModuleStress::pre_force (totals) */
+            memset(fr->wm->tri_f, 0, sizeof(double)*3*fr->wm->ntri);
+            memset(fr->wm->f_total, 0, sizeof fr->wm->f_total);
+            memset(fr->wm->torque_total, 0, sizeof fr->wm->torque_total);
+        }
     }
 }
 
@@ -2016,6 +2039,27 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
             k++;
         }
     return k;
+}
+
+/* fix mesh/surface/stress on mesh wall fix ifix with reference point p_ref */
+int orc_add_mesh_stress(orc_sim *s, int ifix, double px, double py, double pz)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    m->stress = 1;
+    m->p_ref[0] = px; m->p_ref[1] = py; m->p_ref[2] = pz;
+    m->tri_f = calloc((size_t)(m->ntri > 0 ? m->ntri : 1), sizeof(double)*3);
+    return 0;
+}
+
+/* per-element force of the last step (3 per triangle) and f_total, torque_total */
+int orc_get_mesh_stress(orc_sim *s, int ifix, double *tri_f, double *tot6)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm || !s->fix[ifix].wm->stress) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    if (tri_f) memcpy(tri_f, m->tri_f, sizeof(double)*3*m->ntri);
+    if (tot6) { memcpy(tot6, m->f_total, sizeof(double)*3); memcpy(tot6 + 3, m->torque_total, sizeof(double)*3); }
+    return m->ntri;
 }
 
 /* restart: FixContactHistory::unpack_restart (src/fix_contact_history.cpp:608)

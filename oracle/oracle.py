@@ -75,6 +75,8 @@ def lib():
         L.orc_add_move_mesh_linear.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_contact_atom.argtypes = [ctypes.c_void_p, D]
         L.orc_upload_history.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, D]
+        L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
+        L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
         L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
@@ -203,6 +205,18 @@ class Oracle:
                              _dp(out["torque"]), _ip(tag))
         out["tag"] = tag
         return out
+
+    def add_mesh_stress(self, ifix, p_ref):
+        if self.L.orc_add_mesh_stress(self.h, self.fix_ids[ifix], *[float(v) for v in p_ref]) != 0:
+            raise RuntimeError("orc_add_mesh_stress failed")
+
+    def mesh_stress(self, ifix):
+        """Per-element force of the last step and f_total / torque_total."""
+        n = self.L.orc_get_mesh_stress(self.h, self.fix_ids[ifix], None, None)
+        f = np.zeros((n, 3))
+        tot = np.zeros(6)
+        self.L.orc_get_mesh_stress(self.h, self.fix_ids[ifix], _dp(f), _dp(tot))
+        return {"tri_f": f, "f_total": tot[:3], "torque_total": tot[3:]}
 
     def upload_history(self, npartner, partner_tag, hist):
         """FixContactHistory restart data for the atoms as added (before setup)."""

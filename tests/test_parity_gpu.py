@@ -247,3 +247,29 @@ def test_restart_history_roundtrip():
         o2.run(300)
         assert_atoms_equal(e2, o2)
         assert_pairs_equal(e2, o2)
+
+
+def test_mesh_surface_stress():
+    """fix mesh/surface/stress on the silo piston: per-triangle force and the
+    mesh's total force and torque about a reference point, each step; the
+    device sums in another order (atomics), so they equal the oracle to
+    1e-12 of the largest value, not bit for bit."""
+    sc = S.silo(n=1500, piston_speed=0.5)
+    e, o = _pair(sc)
+    for x in (e, o):
+        x.add_mesh_stress(3, [0.001, -0.002, 0.01])
+        x.setup()
+    hits = 0
+    for _ in range(6):
+        e.run(500)
+        o.run(500)
+        assert_atoms_equal(e, o)
+        a, b = e.mesh_stress(3), o.mesh_stress(3)
+        scale = max(np.abs(b["tri_f"]).max(), 1e-30)
+        assert np.abs(a["tri_f"] - b["tri_f"]).max() <= 1e-12 * scale
+        assert np.abs(a["f_total"] - b["f_total"]).max() <= 1e-12 * max(np.abs(b["f_total"]).max(), scale)
+        tq = max(np.abs(b["torque_total"]).max(), 1e-30)
+        assert np.abs(a["torque_total"] - b["torque_total"]).max() <= 1e-12 * tq
+        hits += int((np.abs(b["tri_f"]).sum(axis=1) > 0).sum())
+    assert hits > 0, "the piston carried no force"
+    assert b["f_total"][2] > 0, "particles should push the piston up"
