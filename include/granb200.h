@@ -171,9 +171,11 @@ int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, in
  * step as FixMesh::pre_force / MeshModuleStress::pre_force do).  Sums are
  * device atomics: equal to the reference to rounding, not bit for bit. */
 int gb2_add_mesh_stress(gb2_ctx *ctx, int ifix, const double p_ref[3]);
-/* the last step's per-triangle force (3 per triangle, cap >= ntri) and
- * tot6 = f_total[3], torque_total[3] */
-int gb2_download_mesh_stress(gb2_ctx *ctx, int ifix, int cap, double *tri_f, double *tot6);
+/* the last step's per-triangle force (3 per triangle), normal and shear
+ * stress per triangle (MeshModuleStress::calc_total_force) -- cap >= ntri, any
+ * of the three may be NULL -- and tot6 = f_total[3], torque_total[3] */
+int gb2_download_mesh_stress(gb2_ctx *ctx, int ifix, int cap, double *tri_f, double *sigma_n, double *sigma_t,
+                             double *tot6);
 /* restart interoperability: the contact history in FixContactHistory's
  * per-atom partner layout (src/fix_contact_history.cpp:588-640 pack_restart /
  * unpack_restart): per atom npartner, then per partner its tag and 3 shear

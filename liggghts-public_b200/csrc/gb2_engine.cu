@@ -1887,16 +1887,44 @@ int gb2_add_mesh_stress(gb2_ctx *c, int ifix, const double p_ref[3])
     return 0;
 }
 
-// per-element force of the last step (3 per triangle) and f_total, torque_total
-int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, double *tot6)
+// per-element force of the last step (3 per triangle), the element normal and
+// shear stresses of MeshModuleStress::calc_total_force
+// (src/mesh_module_stress.cpp:335-375: |f.n| / area and |f - (f.n) n| / area
+// with the current normal and TriMesh::calcArea's area of the element as
+// created, src/tri_mesh_I.h:305), and f_total, torque_total
+int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, double *sigma_n, double *sigma_t,
+                             double *tot6)
 {
     if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH) return GB2_ERR_ARG;
     MeshFix &M = *c->fix[ifix].mesh;
     if (!M.stress) return set_err(c, GB2_ERR_STATE, "mesh/surface/stress not enabled on this mesh");
     const int nt = (int)M.topo.tri.size();
-    if (tri_f && cap >= nt) CK(cudaMemcpyAsync(tri_f, M.trif.p, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->st));
+    std::vector<double> f((size_t)3 * nt);
+    std::vector<TriGeom> geo(nt);
+    CK(cudaMemcpyAsync(f.data(), M.trif.p, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(geo.data(), M.tri.p, sizeof(TriGeom) * nt, cudaMemcpyDeviceToHost, c->st));
     if (tot6) CK(cudaMemcpyAsync(tot6, M.ftot.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    if (cap < nt) return 0;
+    for (int t = 0; t < nt; t++) {
+        const double *fi = &f[3 * (size_t)t];
+        if (tri_f)
+            for (int k = 0; k < 3; k++) tri_f[3 * t + k] = fi[k];
+        const TriGeom &T0 = M.topo.tri[t];   // as created
+        const double cx = T0.edgevec[0][1] * T0.edgevec[1][2] - T0.edgevec[0][2] * T0.edgevec[1][1];
+        const double cy = T0.edgevec[0][2] * T0.edgevec[1][0] - T0.edgevec[0][0] * T0.edgevec[1][2];
+        const double cz = T0.edgevec[0][0] * T0.edgevec[1][1] - T0.edgevec[0][1] * T0.edgevec[1][0];
+        const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz) * T0.edgelen[0] * T0.edgelen[1];
+        const double invSurfArea = 1. / area;
+        const double *sn = geo[t].surfnorm;
+        double sn_ = fi[0] * sn[0] + fi[1] * sn[1] + fi[2] * sn[2];
+        const double tmp[3] = {fi[0] - sn[0] * sn_, fi[1] - sn[1] * sn_, fi[2] - sn[2] * sn_};
+        double st_ = std::sqrt(tmp[0] * tmp[0] + tmp[1] * tmp[1] + tmp[2] * tmp[2]);
+        sn_ = std::fabs(sn_);
+        st_ = std::fabs(st_);
+        if (sigma_n) sigma_n[t] = sn_ * invSurfArea;
+        if (sigma_t) sigma_t[t] = st_ * invSurfArea;
+    }
     return 0;
 }
 

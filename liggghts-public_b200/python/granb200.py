@@ -115,7 +115,7 @@ def lib(path=LIB_PATH):
                                            ctypes.POINTER(ctypes.c_int), I, I, I, D]
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
-        L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D]
+        L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D, D, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
         L.gb2_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -310,9 +310,10 @@ class Engine:
         """Per-triangle force of the last step and f_total / torque_total."""
         nt = self.ntri[ifix]
         f = np.zeros((nt, 3))
+        sn, st = np.zeros(nt), np.zeros(nt)
         tot = np.zeros(6)
-        self._check(self.L.gb2_download_mesh_stress(self.h, self.fix_ids[ifix], nt, _dp(f), _dp(tot)))
-        return {"tri_f": f, "f_total": tot[:3], "torque_total": tot[3:]}
+        self._check(self.L.gb2_download_mesh_stress(self.h, self.fix_ids[ifix], nt, _dp(f), _dp(sn), _dp(st), _dp(tot)))
+        return {"tri_f": f, "sigma_n": sn, "sigma_t": st, "f_total": tot[:3], "torque_total": tot[3:]}
 
     def upload_history(self, npartner, partner_tag, hist):
         """FixContactHistory restart data (per atom: partner count, tags and

@@ -88,6 +88,7 @@ typedef struct {
     long next_reneighbor;        /* FixMesh::next_reneighbor */
     /* mesh/surface/stress (MeshModuleStress): per-element force, totals */
     int stress; double p_ref[3]; double (*tri_f)[3]; double f_total[3], torque_total[3];
+    double (*area_ev)[2][3]; double (*area_el)[2];   /* edge vectors and lengths as created (calcArea) */
 } wall_mesh;
 
 typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; int imesh; } fixrec;
@@ -456,7 +457,7 @@ void orc_destroy(orc_sim *s)
             free(m->nneighs); free(m->npartner); free(m->partner); free(m->chist); free(m->keep); free(m->isect);
             free(m->node); free(m->center); free(m->rbound); free(m->edgevec); free(m->edgelen); free(m->edgenorm);
             free(m->surfnorm); free(m->obtuse); free(m->edge_active); free(m->corner_active); free(m->nneigh); free(m->neighfaces);
-            free(m->vnode); free(m->node_last); free(m->tri_f);
+            free(m->vnode); free(m->node_last); free(m->tri_f); free(m->area_ev); free(m->area_el);
             if (s->fix[k].kind == ORC_FIX_WALL_MESH) free(m);
         }
     }
@@ -2049,6 +2050,13 @@ int orc_add_mesh_stress(orc_sim *s, int ifix, double px, double py, double pz)
     m->stress = 1;
     m->p_ref[0] = px; m->p_ref[1] = py; m->p_ref[2] = pz;
     m->tri_f = calloc((size_t)(m->ntri > 0 ? m->ntri : 1), sizeof(double)*3);
+    m->area_ev = calloc((size_t)(m->ntri > 0 ? m->ntri : 1), sizeof(double)*6);
+    m->area_el = calloc((size_t)(m->ntri > 0 ? m->ntri : 1), sizeof(double)*2);
+    for (int t = 0; t < m->ntri; t++) {   /* added before setup: the elements as created */
+        memcpy(m->area_ev[t][0], m->edgevec[t][0], sizeof(double)*3);
+        memcpy(m->area_ev[t][1], m->edgevec[t][1], sizeof(double)*3);
+        m->area_el[t][0] = m->edgelen[t][0]; m->area_el[t][1] = m->edgelen[t][1];
+    }
     return 0;
 }
 
@@ -2059,6 +2067,30 @@ int orc_get_mesh_stress(orc_sim *s, int ifix, double *tri_f, double *tot6)
     wall_mesh *m = s->fix[ifix].wm;
     if (tri_f) memcpy(tri_f, m->tri_f, sizeof(double)*3*m->ntri);
     if (tot6) { memcpy(tot6, m->f_total, sizeof(double)*3); memcpy(tot6 + 3, m->torque_total, sizeof(double)*3); }
+    return m->ntri;
+}
+
+/* MeshModuleStress::calc_total_force src/mesh_module_stress.cpp:335-375 with
+   TriMesh::calcArea src/tri_mesh_I.h:305 of the element as created */
+int orc_get_mesh_sigma(orc_sim *s, int ifix, double *sigma_n, double *sigma_t)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm || !s->fix[ifix].wm->stress) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    for (int i = 0; i < m->ntri; i++) {
+        const double *e0 = m->area_ev[i][0], *e1 = m->area_ev[i][1];
+        double cr[3] = {e0[1]*e1[2] - e0[2]*e1[1], e0[2]*e1[0] - e0[0]*e1[2], e0[0]*e1[1] - e0[1]*e1[0]};
+        double area = 0.5*sqrt(cr[0]*cr[0] + cr[1]*cr[1] + cr[2]*cr[2]) * m->area_el[i][0] * m->area_el[i][1];
+        double invSurfArea = 1./area;
+        const double *sn = m->surfnorm[i];
+        const double *f = m->tri_f[i];
+        double sgn = f[0]*sn[0] + f[1]*sn[1] + f[2]*sn[2];
+        double tmp[3] = {sn[0]*sgn, sn[1]*sgn, sn[2]*sgn};
+        tmp[0] = f[0] - tmp[0]; tmp[1] = f[1] - tmp[1]; tmp[2] = f[2] - tmp[2];
+        double sgt = sqrt(tmp[0]*tmp[0] + tmp[1]*tmp[1] + tmp[2]*tmp[2]);
+        sgn = fabs(sgn); sgt = fabs(sgt);
+        sigma_n[i] = sgn * invSurfArea;
+        sigma_t[i] = sgt * invSurfArea;
+    }
     return m->ntri;
 }
 

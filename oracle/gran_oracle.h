@@ -94,6 +94,7 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
 /* fix mesh/surface/stress: per-element force and totals of the last step */
 int orc_add_mesh_stress(orc_sim *s, int ifix, double px, double py, double pz);
 int orc_get_mesh_stress(orc_sim *s, int ifix, double *tri_f, double *tot6);
+int orc_get_mesh_sigma(orc_sim *s, int ifix, double *sigma_n, double *sigma_t);
 /* restart: contact history in FixContactHistory's partner layout */
 int orc_upload_history(orc_sim *s, int n, const int *npartner, const int *ptag, const double *hist);
 int orc_get_history(orc_sim *s, int *npartner, int *ptag, double *hist);

@@ -77,6 +77,7 @@ def lib():
         L.orc_upload_history.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, D]
         L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
         L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
@@ -216,7 +217,9 @@ class Oracle:
         f = np.zeros((n, 3))
         tot = np.zeros(6)
         self.L.orc_get_mesh_stress(self.h, self.fix_ids[ifix], _dp(f), _dp(tot))
-        return {"tri_f": f, "f_total": tot[:3], "torque_total": tot[3:]}
+        sn, st = np.zeros(n), np.zeros(n)
+        self.L.orc_get_mesh_sigma(self.h, self.fix_ids[ifix], _dp(sn), _dp(st))
+        return {"tri_f": f, "sigma_n": sn, "sigma_t": st, "f_total": tot[:3], "torque_total": tot[3:]}
 
     def upload_history(self, npartner, partner_tag, hist):
         """FixContactHistory restart data for the atoms as added (before setup)."""

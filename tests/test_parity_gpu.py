@@ -270,6 +270,8 @@ def test_mesh_surface_stress():
         assert np.abs(a["f_total"] - b["f_total"]).max() <= 1e-12 * max(np.abs(b["f_total"]).max(), scale)
         tq = max(np.abs(b["torque_total"]).max(), 1e-30)
         assert np.abs(a["torque_total"] - b["torque_total"]).max() <= 1e-12 * tq
+        for k in ("sigma_n", "sigma_t"):
+            assert np.abs(a[k] - b[k]).max() <= 1e-10 * max(np.abs(b[k]).max(), 1e-30), k
         hits += int((np.abs(b["tri_f"]).sum(axis=1) > 0).sum())
     assert hits > 0, "the piston carried no force"
     assert b["f_total"][2] > 0, "particles should push the piston up"
