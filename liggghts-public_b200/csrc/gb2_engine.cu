@@ -1016,7 +1016,7 @@ void launch_pair(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
         return;
     }
     // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
-    const int mb = c->minb ? c->minb : 5;
+    const int mb = c->minb ? c->minb : 6;
     if (c->P.rolling_cdt) {
         if (mb == 4) launch_pair_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch_pair_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
