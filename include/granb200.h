@@ -164,6 +164,14 @@ int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, doub
    the pair count in *n, writes at most cap entries */
 int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
 /* per-atom shear history of primitive-wall fix ifix, [nlocal][3] */
+/* compute pair/gran/local with keywords id force torque history
+ * (src/compute_pair_gran_local.cpp, via PairGran::compute_pgl
+ * src/pair_gran.cpp:676: the pair loop with shearupdate 0 on the current
+ * state): one row of 12 doubles per touching pair in list order -- tag_i,
+ * tag_j, periodic (1 for a pair through a periodic boundary, kept once, when
+ * tag_i > tag_j), force on i[3], torque on i[3], shear history[3].  *nrows is
+ * always set; rows are written when cap >= *nrows. */
+int gb2_pair_gran_local(gb2_ctx *ctx, int cap, int *nrows, double *rows);
 /* fix mesh/surface/stress on mesh wall fix ifix (before setup): the force of
  * every wall contact, negated, is added to its triangle and to the mesh's
  * f_total / torque_total about p_ref each step (MeshModuleStress::

@@ -126,6 +126,9 @@ struct gb2_ctx {
     std::string err;
     cudaStream_t st = nullptr;
     bool have_mat = false, have_atoms = false, setup_done = false, computeflag = false;
+    // after an integrating step the ghost slots of vel/omg are two swaps old;
+    // the values forwarded at that step's start are in vel2/omg2
+    bool ghost_v_prev = false;
     MatPair hmat[(kMaxTypes + 1) * (kMaxTypes + 1)];
     DBuf<MatPair> dmat;
 
@@ -1069,6 +1072,7 @@ int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int stor
         if (fuse_next) c->pos.swap(c->pos2);
     }
     c->fused_pending = integrate && fuse_next;
+    c->ghost_v_prev = integrate != 0;
     return 0;
 }
 
@@ -1866,6 +1870,48 @@ int gb2_contact_atom(gb2_ctx *c, int cap, int *n, int *tag, double *contact)
         CK(cudaMemcpyAsync(contact, d.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, c->st));
         if (tag) CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
     }
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// compute pair/gran/local id force torque history on the device: rows of 12
+// doubles (tag_i, tag_j, periodic, f_i[3], torque_i[3], history[3]) in list order
+int gb2_pair_gran_local(gb2_ctx *c, int cap, int *nrows, double *rows)
+{
+    if (!c || !nrows) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no neighbor list before setup");
+    const int nl = c->nlocal;
+    DBuf<int> cnt, off;
+    CK(cnt.alloc(nl + 1));
+    CK(off.alloc(nl + 1));
+    CK(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (nl + 1), c->st));
+    if (c->ghost_v_prev && c->nghost > 0) {
+        // ghosts carry the velocities forwarded at the last step's start, as
+        // in the reference between steps
+        const size_t g0 = (size_t)c->nlocal, ng = (size_t)c->nghost;
+        CK(cudaMemcpyAsync(c->vel.p + g0, c->vel2.p + g0, sizeof(dbl4) * ng, cudaMemcpyDeviceToDevice, c->st));
+        CK(cudaMemcpyAsync(c->omg.p + g0, c->omg2.p + g0, sizeof(dbl4) * ng, cudaMemcpyDeviceToDevice, c->st));
+        c->ghost_v_prev = false;
+    }
+    Dev D = make_dev(c);
+    if (nl > 0) {
+        k_pgl_count<<<nblk(nl), kBlock, 0, c->st>>>(D, cnt.p);
+        CKL();
+    }
+    size_t tmp = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, nl + 1, c->st));
+    if (cub_tmp(c, tmp)) return GB2_ERR_CUDA;
+    CK(cub::DeviceScan::ExclusiveSum(c->cubtmp.p, tmp, cnt.p, off.p, nl + 1, c->st));
+    int total = 0;
+    CK(cudaMemcpyAsync(&total, off.p + nl, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *nrows = total;
+    if (!rows || cap < total || total == 0) return 0;
+    DBuf<double> d;
+    CK(d.alloc((size_t)12 * total));
+    k_pgl_rows<<<nblk(nl), kBlock, 0, c->st>>>(D, off.p, d.p);
+    CKL();
+    CK(cudaMemcpyAsync(rows, d.p, sizeof(double) * 12 * total, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return 0;
 }

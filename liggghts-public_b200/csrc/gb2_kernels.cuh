@@ -808,5 +808,71 @@ __global__ void k_contact_atom(Dev D, double *out)
     out[k] = (double)cnt;
 }
 
+// compute pair/gran/local id force torque history (src/compute_pair_gran_local.cpp
+// add_pair via PairGran::compute_pgl, src/pair_gran.cpp:676-707): every touching
+// own-list pair (a pair with a ghost only when tag_i > tag_j), its force and
+// torque on i evaluated with shearupdate 0 from the current state.  Count pass
+// and row pass (rows in list order: per-atom offsets from a scan of the counts).
+__device__ __forceinline__ bool pgl_pair(const Dev &D, int i, int s, const dbl4 &pi, int &j, double &delx,
+                                         double &dely, double &delz, double &rsq)
+{
+    j = D.nbr[s * D.cap + i];
+    const dbl4 pj = D.pos[j];
+    delx = pi.x - pj.x;
+    dely = pi.y - pj.y;
+    delz = pi.z - pj.z;
+    rsq = delx * delx + dely * dely + delz * delz;
+    const double radsum = pi.w + pj.w;
+    if (!(rsq < radsum * radsum)) return false;
+    return !(j >= D.nlocal && D.tag[i] <= D.tag[j]);
+}
+
+__global__ void k_pgl_count(Dev D, int *cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.nlocal) return;
+    const dbl4 pi = D.pos[i];
+    int n = 0;
+    for (int s = 0; s < D.nnum[i]; s++) {
+        int j;
+        double dx, dy, dz, rsq;
+        if (pgl_pair(D, i, s, pi, j, dx, dy, dz, rsq)) n++;
+    }
+    cnt[i] = n;
+}
+
+__global__ void k_pgl_rows(Dev D, const int *off, double *rows)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.nlocal) return;
+    const int cap = D.cap;
+    const dbl4 pi = D.pos[i], vi4 = D.vel[i], wi4 = D.omg[i];
+    const double vi[3] = {vi4.x, vi4.y, vi4.z}, wi[3] = {wi4.x, wi4.y, wi4.z};
+    const int ti = D.type[i];
+    int k = off[i];
+    for (int s = 0; s < D.nnum[i]; s++) {
+        int j;
+        double delx, dely, delz, rsq;
+        if (!pgl_pair(D, i, s, pi, j, delx, dely, delz, rsq)) continue;
+        const dbl4 pj = D.pos[j], vj4 = D.vel[j], wj4 = D.omg[j];
+        const double vj[3] = {vj4.x, vj4.y, vj4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
+        double sh[3] = {D.hist[(3 * s + 0) * cap + i], D.hist[(3 * s + 1) * cap + i], D.hist[(3 * s + 2) * cap + i]};
+        const double h0[3] = {sh[0], sh[1], sh[2]};
+        ContactOut o;
+        pair_contact<false>(mat(D, ti, D.type[j]), delx, dely, delz, rsq, pi.w, pj.w, vi, vj, wi, wj, vi4.w, vj4.w,
+                            sh, false, D.dt, D.rolling != 0, D.tdamp != 0, o);
+        double *row = rows + 12 * (size_t)k;
+        row[0] = (double)D.tag[i];
+        row[1] = (double)D.tag[j];
+        row[2] = j < D.nlocal ? 0. : 1.;
+        for (int c = 0; c < 3; c++) {
+            row[3 + c] = o.F[c];
+            row[6 + c] = o.T[c];
+            row[9 + c] = h0[c];
+        }
+        k++;
+    }
+}
+
 }  // namespace gb2
 

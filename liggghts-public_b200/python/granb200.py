@@ -30,7 +30,7 @@ EXPORTS = (
     "gb2_timer_stop", "gb2_census_noalloc", "gb2_add_move_mesh_rotate", "gb2_download_mesh_nodes",
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
-    "gb2_download_mesh_stress",
+    "gb2_download_mesh_stress", "gb2_pair_gran_local",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -115,6 +115,7 @@ def lib(path=LIB_PATH):
                                            ctypes.POINTER(ctypes.c_int), I, I, I, D]
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
+        L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
         L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D, D, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
@@ -300,6 +301,15 @@ class Engine:
         hi = np.zeros((n, 3))
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def pair_gran_local(self):
+        """compute pair/gran/local id force torque history on the device: (nrows, 12)."""
+        n = ctypes.c_int()
+        self._check(self.L.gb2_pair_gran_local(self.h, 0, ctypes.byref(n), None))
+        rows = np.zeros((n.value, 12))
+        if n.value:
+            self._check(self.L.gb2_pair_gran_local(self.h, n.value, ctypes.byref(n), _dp(rows)))
+        return rows
 
     def add_mesh_stress(self, ifix, p_ref):
         """fix mesh/surface/stress on the mesh wall of scenario fix ifix (before setup)."""

@@ -2042,6 +2042,60 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
     return k;
 }
 
+/* compute pair/gran/local with the keywords id force torque history
+   (src/compute_pair_gran_local.cpp add_pair, through PairGran::compute_pgl
+   src/pair_gran.cpp:676-707: the pair loop with computeflag 0 and
+   shearupdate 0, add_pair for every touching pair, newton off: a pair with a
+   ghost is kept only when tag_i > tag_j).  Row: tag_i, tag_j, periodic,
+   f_i[3], torque_i[3], history[3].  Returns the row count. */
+int orc_pair_gran_local(orc_sim *s, int cap, double *rows)
+{
+    int k = 0;
+    for (int i = 0; i < s->nlocal; i++) {
+        const double xtmp = s->x[3*i], ytmp = s->x[3*i+1], ztmp = s->x[3*i+2];
+        const double radi = s->radius[i];
+        for (int jj = 0; jj < s->nnum[i]; jj++) {
+            const int e = s->nstart[i] + jj;
+            const int j = s->nbr[e];
+            const double delx = xtmp - s->x[3*j], dely = ytmp - s->x[3*j+1], delz = ztmp - s->x[3*j+2];
+            const double rsq = delx * delx + dely * dely + delz * delz;
+            const double radj = s->radius[j];
+            const double radsum = radi + radj;
+            if (!(rsq < radsum * radsum)) continue;
+            if (j >= s->nlocal && s->tag[i] <= s->tag[j]) continue;
+            sidata_t sd; memset(&sd, 0, sizeof sd);
+            force_t fi, fj; memset(&fi, 0, sizeof fi); memset(&fj, 0, sizeof fj);
+            int flag = s->flag[e];
+            double hist[3] = {s->hist[3*e], s->hist[3*e+1], s->hist[3*e+2]};
+            sd.is_wall = 0;
+            sd.radi = radi; sd.radj = radj; sd.radsum = radsum; sd.rsq = rsq;
+            sd.delta[0] = delx; sd.delta[1] = dely; sd.delta[2] = delz;
+            sd.contact_flags = &flag;
+            sd.contact_history = hist;
+            sd.v_i = &s->v[3*i]; sd.v_j = &s->v[3*j];
+            sd.itype = s->type[i]; sd.jtype = s->type[j];
+            sd.computeflag = 0; sd.shearupdate = 0;
+            const double r = sqrt(rsq);
+            const double rinv = 1.0 / r;
+            const double mi = s->rmass[i], mj = s->rmass[j];
+            const double meff = mi * mj / (mi + mj);
+            sd.r = r; sd.rinv = rinv; sd.meff = meff; sd.mi = mi; sd.mj = mj;
+            sd.en[0] = delx * rinv; sd.en[1] = dely * rinv; sd.en[2] = delz * rinv;
+            sd.omega_i = &s->omega[3*i]; sd.omega_j = &s->omega[3*j];
+            contact_chain(s, &sd, &fi, &fj, s->p.rolling_cdt);
+            if (rows && k < cap) {
+                double *row = rows + 12 * (size_t)k;
+                row[0] = (double)s->tag[i];
+                row[1] = (double)s->tag[j];
+                row[2] = j < s->nlocal ? 0. : 1.;
+                for (int c = 0; c < 3; c++) { row[3+c] = fi.F[c]; row[6+c] = fi.T[c]; row[9+c] = hist[c]; }
+            }
+            k++;
+        }
+    }
+    return k;
+}
+
 /* fix mesh/surface/stress on mesh wall fix ifix with reference point p_ref */
 int orc_add_mesh_stress(orc_sim *s, int ifix, double px, double py, double pz)
 {

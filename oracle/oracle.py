@@ -78,6 +78,7 @@ def lib():
         L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_pair_gran_local.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
         L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
         L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
@@ -206,6 +207,13 @@ class Oracle:
                              _dp(out["torque"]), _ip(tag))
         out["tag"] = tag
         return out
+
+    def pair_gran_local(self):
+        """compute pair/gran/local id force torque history: (nrows, 12)."""
+        n = self.L.orc_pair_gran_local(self.h, 0, None)
+        rows = np.zeros((n, 12))
+        self.L.orc_pair_gran_local(self.h, n, _dp(rows))
+        return rows
 
     def add_mesh_stress(self, ifix, p_ref):
         if self.L.orc_add_mesh_stress(self.h, self.fix_ids[ifix], *[float(v) for v in p_ref]) != 0:

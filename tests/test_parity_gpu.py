@@ -142,7 +142,7 @@ def test_bidisperse_long_lists_serial_path():
     p = o.pairs()
     tags, counts = np.unique(np.concatenate([p["tag_i"], p["tag_j"]]), return_counts=True)
     assert counts.max() > 128, "no atom with a long list"
-    big_touch = 0
+    big_touch = pgl_rows = pgl_periodic = 0
     for _ in range(6):
         e.run(250)
         o.run(250)
@@ -154,8 +154,13 @@ def test_bidisperse_long_lists_serial_path():
         assert np.array_equal(e.wall_hist(1), o.wall_hist(1))
         ca, cb = e.contact_atom(), o.contact_atom()
         assert np.array_equal(ca["tag"], cb["tag"]) and np.array_equal(ca["contact"], cb["contact"])
+        ra, rb = e.pair_gran_local(), o.pair_gran_local()
+        assert ra.shape == rb.shape and np.array_equal(ra, rb), "pair/gran/local rows differ"
+        pgl_rows += len(rb)
+        pgl_periodic += int(rb[:, 2].sum())
     assert big_touch > 0, "the large spheres touched nothing"
     assert e.contact_atom()["contact"].max() > 10, "no large sphere with many contacts"
+    assert pgl_rows > 100 and pgl_periodic > 0, "pair/gran/local saw too few pairs"
     assert e.stats()["nbuilds"] == o.nbuilds
 
 
