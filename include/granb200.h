@@ -172,6 +172,32 @@ int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, in
  * tag_i > tag_j), force on i[3], torque on i[3], shear history[3].  *nrows is
  * always set; rows are written when cap >= *nrows. */
 int gb2_pair_gran_local(gb2_ctx *ctx, int cap, int *nrows, double *rows);
+/* compute pair/gran/local with any of its per-pair keywords
+ * (src/compute_pair_gran_local.cpp:96-110, columns in the order of add_pair,
+ * :445-606): keys is an OR of GB2_PGL_*; *ncols (when not NULL) receives the
+ * row width (pos 6, vel 6, id 3, force / force_normal / force_tangential /
+ * torque / torque_normal / torque_tangential 3 each, history 3, contactArea 1,
+ * delta 1, contactPoint 3).  pos is remapped into the periodic box as
+ * Domain::remap does.  GB2_PGL_DEFAULT is the keyword set the reference uses
+ * when the command names none.  heatFlux and ms_id need models outside this
+ * library and are refused (GB2_ERR_ARG), as are unknown bits and keys == 0. */
+#define GB2_PGL_POS               0x0001u
+#define GB2_PGL_VEL               0x0002u
+#define GB2_PGL_ID                0x0004u
+#define GB2_PGL_FORCE             0x0008u
+#define GB2_PGL_FORCE_NORMAL      0x0010u
+#define GB2_PGL_FORCE_TANGENTIAL  0x0020u
+#define GB2_PGL_TORQUE            0x0040u
+#define GB2_PGL_TORQUE_NORMAL     0x0080u
+#define GB2_PGL_TORQUE_TANGENTIAL 0x0100u
+#define GB2_PGL_HISTORY           0x0200u
+#define GB2_PGL_CONTACT_AREA      0x0400u
+#define GB2_PGL_DELTA             0x0800u
+#define GB2_PGL_CONTACT_POINT     0x1000u
+#define GB2_PGL_ALL               0x1fffu
+#define GB2_PGL_DEFAULT (GB2_PGL_POS | GB2_PGL_VEL | GB2_PGL_ID | GB2_PGL_FORCE | GB2_PGL_TORQUE | \
+                         GB2_PGL_HISTORY | GB2_PGL_CONTACT_AREA)
+int gb2_pair_gran_local_keys(gb2_ctx *ctx, unsigned keys, int cap, int *nrows, int *ncols, double *rows);
 /* fix mesh/surface/stress on mesh wall fix ifix (before setup): the force of
  * every wall contact, negated, is added to its triangle and to the mesh's
  * f_total / torque_total about p_ref each step (MeshModuleStress::

@@ -1874,12 +1874,24 @@ int gb2_contact_atom(gb2_ctx *c, int cap, int *n, int *tag, double *contact)
     return 0;
 }
 
-// compute pair/gran/local id force torque history on the device: rows of 12
-// doubles (tag_i, tag_j, periodic, f_i[3], torque_i[3], history[3]) in list order
-int gb2_pair_gran_local(gb2_ctx *c, int cap, int *nrows, double *rows)
+// columns of a pair/gran/local row for a keyword mask
+static int pgl_ncols(unsigned keys)
 {
-    if (!c || !nrows) return GB2_ERR_ARG;
+    static const int width[13] = {6, 6, 3, 3, 3, 3, 3, 3, 3, 3, 1, 1, 3};
+    int n = 0;
+    for (int b = 0; b < 13; b++)
+        if (keys & (1u << b)) n += width[b];
+    return n;
+}
+
+// compute pair/gran/local on the device: one row per touching pair in list
+// order with the columns keys selects
+int gb2_pair_gran_local_keys(gb2_ctx *c, unsigned keys, int cap, int *nrows, int *ncols, double *rows)
+{
+    if (!c || !nrows || keys == 0 || (keys & ~GB2_PGL_ALL)) return GB2_ERR_ARG;
     if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no neighbor list before setup");
+    const int nc = pgl_ncols(keys);
+    if (ncols) *ncols = nc;
     const int nl = c->nlocal;
     DBuf<int> cnt, off;
     CK(cnt.alloc(nl + 1));
@@ -1907,13 +1919,27 @@ int gb2_pair_gran_local(gb2_ctx *c, int cap, int *nrows, double *rows)
     CK(cudaStreamSynchronize(c->st));
     *nrows = total;
     if (!rows || cap < total || total == 0) return 0;
+    PglBox B;
+    for (int d = 0; d < 3; d++) {
+        B.lo[d] = c->P.boxlo[d];
+        B.hi[d] = c->P.boxhi[d];
+        B.periodic[d] = c->P.periodic[d];
+    }
     DBuf<double> d;
-    CK(d.alloc((size_t)12 * total));
-    k_pgl_rows<<<nblk(nl), kBlock, 0, c->st>>>(D, off.p, d.p);
+    CK(d.alloc((size_t)nc * total));
+    k_pgl_rows<<<nblk(nl), kBlock, 0, c->st>>>(D, off.p, d.p, B, keys, nc);
     CKL();
-    CK(cudaMemcpyAsync(rows, d.p, sizeof(double) * 12 * total, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(rows, d.p, sizeof(double) * nc * total, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return 0;
+}
+
+// compute pair/gran/local id force torque history: rows of 12 doubles
+// (tag_i, tag_j, periodic, f_i[3], torque_i[3], history[3])
+int gb2_pair_gran_local(gb2_ctx *c, int cap, int *nrows, double *rows)
+{
+    return gb2_pair_gran_local_keys(c, GB2_PGL_ID | GB2_PGL_FORCE | GB2_PGL_TORQUE | GB2_PGL_HISTORY, cap, nrows,
+                                    nullptr, rows);
 }
 
 // fix mesh/surface/stress on mesh wall fix ifix (before setup): per-element

@@ -13,6 +13,7 @@
 // the result is bit-identical to the reference's j_forces for that pair.
 #pragma once
 
+#include "../../include/granb200.h"
 #include "gb2_device.cuh"
 
 namespace gb2 {
@@ -813,6 +814,11 @@ __global__ void k_contact_atom(Dev D, double *out)
 // own-list pair (a pair with a ghost only when tag_i > tag_j), its force and
 // torque on i evaluated with shearupdate 0 from the current state.  Count pass
 // and row pass (rows in list order: per-atom offsets from a scan of the counts).
+struct PglBox {
+    double lo[3], hi[3];
+    int periodic[3];
+};
+
 __device__ __forceinline__ bool pgl_pair(const Dev &D, int i, int s, const dbl4 &pi, int &j, double &delx,
                                          double &dely, double &delz, double &rsq)
 {
@@ -841,7 +847,38 @@ __global__ void k_pgl_count(Dev D, int *cnt)
     cnt[i] = n;
 }
 
-__global__ void k_pgl_rows(Dev D, const int *off, double *rows)
+// Domain::remap (src/domain.cpp:1136-1173) for an orthogonal box: the
+// periodic image inside [lo, hi).  Ghost images lie within the ghost cutoff of
+// the box, so a few shifts always suffice for finite coordinates.
+__device__ __forceinline__ double pgl_remap(double x, double lo, double hi, int periodic)
+{
+    if (!periodic) return x;
+    const double prd = hi - lo;
+    for (int it = 0; it < 64 && x < lo; it++) x += prd;
+    for (int it = 0; it < 64 && x >= hi; it++) x -= prd;
+    return x > lo ? x : lo;
+}
+
+// the component of c along the unit vector from x_i to x_j
+// (vectorSubtract3D / vectorNormalize3D, src/vector_liggghts.h:62-69)
+__device__ __forceinline__ void pgl_along(const dbl4 &pi, const dbl4 &pj, const double c[3], double out[3])
+{
+    double n[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+    const double norm = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const double inv = (norm == 0.) ? 0. : 1. / norm;
+    n[0] *= inv;
+    n[1] *= inv;
+    n[2] *= inv;
+    const double mag = c[0] * n[0] + c[1] * n[1] + c[2] * n[2];
+    out[0] = n[0] * mag;
+    out[1] = n[1] * mag;
+    out[2] = n[2] * mag;
+}
+
+// one row per touching pair with the columns the keyword mask selects, in
+// the order ComputePairGranLocal::add_pair writes them
+// (src/compute_pair_gran_local.cpp:445-606)
+__global__ void k_pgl_rows(Dev D, const int *off, double *rows, PglBox B, unsigned keys, int ncols)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.nlocal) return;
@@ -861,14 +898,56 @@ __global__ void k_pgl_rows(Dev D, const int *off, double *rows)
         ContactOut o;
         pair_contact<false>(mat(D, ti, D.type[j]), delx, dely, delz, rsq, pi.w, pj.w, vi, vj, wi, wj, vi4.w, vj4.w,
                             sh, false, D.dt, D.rolling != 0, D.tdamp != 0, o);
-        double *row = rows + 12 * (size_t)k;
-        row[0] = (double)D.tag[i];
-        row[1] = (double)D.tag[j];
-        row[2] = j < D.nlocal ? 0. : 1.;
-        for (int c = 0; c < 3; c++) {
-            row[3 + c] = o.F[c];
-            row[6 + c] = o.T[c];
-            row[9 + c] = h0[c];
+        double *row = rows + (size_t)ncols * k;
+        int n = 0;
+        if (keys & GB2_PGL_POS) {
+            const double xi[3] = {pi.x, pi.y, pi.z}, xj[3] = {pj.x, pj.y, pj.z};
+            for (int d = 0; d < 3; d++) row[n++] = pgl_remap(xi[d], B.lo[d], B.hi[d], B.periodic[d]);
+            for (int d = 0; d < 3; d++) row[n++] = pgl_remap(xj[d], B.lo[d], B.hi[d], B.periodic[d]);
+        }
+        if (keys & GB2_PGL_VEL) {
+            for (int d = 0; d < 3; d++) row[n++] = vi[d];
+            for (int d = 0; d < 3; d++) row[n++] = vj[d];
+        }
+        if (keys & GB2_PGL_ID) {
+            row[n++] = (double)D.tag[i];
+            row[n++] = (double)D.tag[j];
+            row[n++] = j < D.nlocal ? 0. : 1.;
+        }
+        if (keys & GB2_PGL_FORCE)
+            for (int d = 0; d < 3; d++) row[n++] = o.F[d];
+        if (keys & (GB2_PGL_FORCE_NORMAL | GB2_PGL_FORCE_TANGENTIAL)) {
+            double fn[3];
+            pgl_along(pi, pj, o.F, fn);
+            if (keys & GB2_PGL_FORCE_NORMAL)
+                for (int d = 0; d < 3; d++) row[n++] = fn[d];
+            if (keys & GB2_PGL_FORCE_TANGENTIAL)
+                for (int d = 0; d < 3; d++) row[n++] = o.F[d] - fn[d];
+        }
+        if (keys & GB2_PGL_TORQUE)
+            for (int d = 0; d < 3; d++) row[n++] = o.T[d];
+        if (keys & (GB2_PGL_TORQUE_NORMAL | GB2_PGL_TORQUE_TANGENTIAL)) {
+            double tn[3];
+            pgl_along(pi, pj, o.T, tn);
+            if (keys & GB2_PGL_TORQUE_NORMAL)
+                for (int d = 0; d < 3; d++) row[n++] = tn[d];
+            if (keys & GB2_PGL_TORQUE_TANGENTIAL)
+                for (int d = 0; d < 3; d++) row[n++] = o.T[d] - tn[d];
+        }
+        if (keys & GB2_PGL_HISTORY)
+            for (int d = 0; d < 3; d++) row[n++] = h0[d];
+        if (keys & (GB2_PGL_CONTACT_AREA | GB2_PGL_DELTA)) {
+            // del = x_i - x_j as recomputed by add_pair (the same rsq as the pair test)
+            const double r = sqrt(rsq);
+            const double radi = pi.w, radj = pj.w;
+            if (keys & GB2_PGL_CONTACT_AREA)
+                row[n++] = -M_PI / 4 * ((r - radi - radj) * (r + radi - radj) * (r - radi + radj) * (r + radi + radj)) /
+                           rsq;
+            if (keys & GB2_PGL_DELTA) row[n++] = radi + radj - r;
+        }
+        if (keys & GB2_PGL_CONTACT_POINT) {
+            const double xi[3] = {pi.x, pi.y, pi.z}, xj[3] = {pj.x, pj.y, pj.z};
+            for (int d = 0; d < 3; d++) row[n++] = (xi[d] * pj.w + xj[d] * pi.w) / (pi.w + pj.w);
         }
         k++;
     }

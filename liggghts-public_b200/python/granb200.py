@@ -31,9 +31,37 @@ EXPORTS = (
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
+    "gb2_pair_gran_local_keys",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
+
+# compute pair/gran/local keywords (GB2_PGL_*), in the reference's column order,
+# with their column counts
+PGL_KEYWORDS = (("pos", 6), ("vel", 6), ("id", 3), ("force", 3), ("force_normal", 3), ("force_tangential", 3),
+                ("torque", 3), ("torque_normal", 3), ("torque_tangential", 3), ("history", 3), ("contactArea", 1),
+                ("delta", 1), ("contactPoint", 3))
+PGL_DEFAULT = ("pos", "vel", "id", "force", "torque", "history", "contactArea")
+
+
+def pgl_keys(keywords):
+    """Bit mask of a pair/gran/local keyword list; unknown names raise ValueError."""
+    names = [k for k, _ in PGL_KEYWORDS]
+    keys = 0
+    for w in keywords:
+        if w not in names:
+            raise ValueError("compute pair/gran/local: unknown or unsupported keyword %r" % (w,))
+        keys |= 1 << names.index(w)
+    return keys
+
+
+def pgl_columns(keys):
+    """Column names of a pair/gran/local row for a keyword bit mask."""
+    cols = []
+    for b, (name, n) in enumerate(PGL_KEYWORDS):
+        if keys & (1 << b):
+            cols += [name] if n == 1 else ["%s[%d]" % (name, c) for c in range(n)]
+    return cols
 
 
 class Params(ctypes.Structure):
@@ -116,6 +144,8 @@ def lib(path=LIB_PATH):
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
         L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
+        L.gb2_pair_gran_local_keys.argtypes = [vp, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int), D]
         L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D, D, D]
         L.gb2_download_mesh_contacts.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, I, D]
         L.gb2_mesh_topology.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, U8, U8, I]
@@ -302,13 +332,24 @@ class Engine:
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
 
-    def pair_gran_local(self):
-        """compute pair/gran/local id force torque history on the device: (nrows, 12)."""
+    def pair_gran_local(self, keywords=None):
+        """compute pair/gran/local on the device: (nrows, ncols).  Without
+        keywords the 12 columns id force torque history; a keyword list gives
+        the columns in the reference's order (pgl_columns)."""
         n = ctypes.c_int()
-        self._check(self.L.gb2_pair_gran_local(self.h, 0, ctypes.byref(n), None))
-        rows = np.zeros((n.value, 12))
+        if keywords is None:
+            self._check(self.L.gb2_pair_gran_local(self.h, 0, ctypes.byref(n), None))
+            rows = np.zeros((n.value, 12))
+            if n.value:
+                self._check(self.L.gb2_pair_gran_local(self.h, n.value, ctypes.byref(n), _dp(rows)))
+            return rows
+        keys = pgl_keys(keywords)
+        nc = ctypes.c_int()
+        self._check(self.L.gb2_pair_gran_local_keys(self.h, keys, 0, ctypes.byref(n), ctypes.byref(nc), None))
+        rows = np.zeros((n.value, nc.value))
         if n.value:
-            self._check(self.L.gb2_pair_gran_local(self.h, n.value, ctypes.byref(n), _dp(rows)))
+            self._check(self.L.gb2_pair_gran_local_keys(self.h, keys, n.value, ctypes.byref(n), ctypes.byref(nc),
+                                                        _dp(rows)))
         return rows
 
     def add_mesh_stress(self, ifix, p_ref):

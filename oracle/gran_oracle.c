@@ -2042,14 +2042,45 @@ int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double
     return k;
 }
 
-/* compute pair/gran/local with the keywords id force torque history
-   (src/compute_pair_gran_local.cpp add_pair, through PairGran::compute_pgl
-   src/pair_gran.cpp:676-707: the pair loop with computeflag 0 and
-   shearupdate 0, add_pair for every touching pair, newton off: a pair with a
-   ghost is kept only when tag_i > tag_j).  Row: tag_i, tag_j, periodic,
-   f_i[3], torque_i[3], history[3].  Returns the row count. */
-int orc_pair_gran_local(orc_sim *s, int cap, double *rows)
+/* Domain::remap, src/domain.cpp:1136-1173 (orthogonal box) */
+static double pgl_remap(const orc_sim *s, int d, double x)
 {
+    if (!s->p.periodic[d]) return x;
+    const double lo = s->p.boxlo[d], hi = s->p.boxhi[d], prd = hi - lo;
+    while (x < lo) x += prd;
+    while (x >= hi) x -= prd;
+    return x > lo ? x : lo;
+}
+
+/* component of c along the unit vector x_j - x_i, as add_pair builds
+   force_normal / torque_normal (src/compute_pair_gran_local.cpp:481-545 with
+   vectorNormalize3D, src/vector_liggghts.h:62-69) */
+static void pgl_along(const double *xi, const double *xj, const double *c, double *out)
+{
+    double n[3] = {xj[0] - xi[0], xj[1] - xi[1], xj[2] - xi[2]};
+    const double norm = sqrt(n[0]*n[0] + n[1]*n[1] + n[2]*n[2]);
+    const double inv = (norm == 0.) ? 0. : 1. / norm;
+    n[0] *= inv; n[1] *= inv; n[2] *= inv;
+    const double mag = c[0]*n[0] + c[1]*n[1] + c[2]*n[2];
+    out[0] = mag * n[0]; out[1] = mag * n[1]; out[2] = mag * n[2];
+}
+
+static int pgl_ncols(unsigned keys)
+{
+    static const int width[13] = {6, 6, 3, 3, 3, 3, 3, 3, 3, 3, 1, 1, 3};
+    int n = 0;
+    for (int b = 0; b < 13; b++) if (keys & (1u << b)) n += width[b];
+    return n;
+}
+
+/* compute pair/gran/local (src/compute_pair_gran_local.cpp add_pair,
+   :417-609, fed by PairGran::compute_pgl, src/pair_gran.cpp:676-707:
+   computeflag 0, shearupdate 0, add_pair for every touching pair, newton
+   off: a pair with a ghost is kept only when tag_i > tag_j).  Columns in
+   add_pair's order for the keyword bits set in keys.  Returns the row count. */
+int orc_pair_gran_local(orc_sim *s, unsigned keys, int cap, double *rows)
+{
+    const int nc = pgl_ncols(keys);
     int k = 0;
     for (int i = 0; i < s->nlocal; i++) {
         const double xtmp = s->x[3*i], ytmp = s->x[3*i+1], ztmp = s->x[3*i+2];
@@ -2084,11 +2115,42 @@ int orc_pair_gran_local(orc_sim *s, int cap, double *rows)
             sd.omega_i = &s->omega[3*i]; sd.omega_j = &s->omega[3*j];
             contact_chain(s, &sd, &fi, &fj, s->p.rolling_cdt);
             if (rows && k < cap) {
-                double *row = rows + 12 * (size_t)k;
-                row[0] = (double)s->tag[i];
-                row[1] = (double)s->tag[j];
-                row[2] = j < s->nlocal ? 0. : 1.;
-                for (int c = 0; c < 3; c++) { row[3+c] = fi.F[c]; row[6+c] = fi.T[c]; row[9+c] = hist[c]; }
+                double *row = rows + (size_t)nc * k;
+                const double *xi = &s->x[3*i], *xj = &s->x[3*j];
+                int n = 0;
+                if (keys & 0x1u) {
+                    for (int d = 0; d < 3; d++) row[n++] = pgl_remap(s, d, xi[d]);
+                    for (int d = 0; d < 3; d++) row[n++] = pgl_remap(s, d, xj[d]);
+                }
+                if (keys & 0x2u) {
+                    for (int d = 0; d < 3; d++) row[n++] = s->v[3*i+d];
+                    for (int d = 0; d < 3; d++) row[n++] = s->v[3*j+d];
+                }
+                if (keys & 0x4u) {
+                    row[n++] = (double)s->tag[i];
+                    row[n++] = (double)s->tag[j];
+                    row[n++] = j < s->nlocal ? 0. : 1.;
+                }
+                if (keys & 0x8u) for (int d = 0; d < 3; d++) row[n++] = fi.F[d];
+                double fn[3], tn[3];
+                pgl_along(xi, xj, fi.F, fn);
+                pgl_along(xi, xj, fi.T, tn);
+                if (keys & 0x10u) for (int d = 0; d < 3; d++) row[n++] = fn[d];
+                if (keys & 0x20u) for (int d = 0; d < 3; d++) row[n++] = fi.F[d] - fn[d];
+                if (keys & 0x40u) for (int d = 0; d < 3; d++) row[n++] = fi.T[d];
+                if (keys & 0x80u) for (int d = 0; d < 3; d++) row[n++] = tn[d];
+                if (keys & 0x100u) for (int d = 0; d < 3; d++) row[n++] = fi.T[d] - tn[d];
+                if (keys & 0x200u) for (int d = 0; d < 3; d++) row[n++] = hist[d];
+                if (keys & 0xc00u) {
+                    double del[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+                    const double rs = del[0]*del[0] + del[1]*del[1] + del[2]*del[2];
+                    const double rr = sqrt(rs);
+                    if (keys & 0x400u)
+                        row[n++] = - M_PI/4 * ((rr-radi-radj)*(rr+radi-radj)*(rr-radi+radj)*(rr+radi+radj)) / rs;
+                    if (keys & 0x800u) row[n++] = radi + radj - rr;
+                }
+                if (keys & 0x1000u)
+                    for (int d = 0; d < 3; d++) row[n++] = (xi[d]*radj + xj[d]*radi) / (radi + radj);
             }
             k++;
         }

@@ -91,8 +91,10 @@ void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega,
                    double *f, double *torque, int *tag);
 /* half-list pairs: returns count; arrays may be NULL to query count */
 int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist);
-/* compute pair/gran/local id force torque history: rows of 12 doubles */
-int orc_pair_gran_local(orc_sim *s, int cap, double *rows);
+/* compute pair/gran/local: rows of the columns keys selects (bit b of keys:
+   pos, vel, id, force, force_normal, force_tangential, torque, torque_normal,
+   torque_tangential, history, contactArea, delta, contactPoint) */
+int orc_pair_gran_local(orc_sim *s, unsigned keys, int cap, double *rows);
 /* fix mesh/surface/stress: per-element force and totals of the last step */
 int orc_add_mesh_stress(orc_sim *s, int ifix, double px, double py, double pz);
 int orc_get_mesh_stress(orc_sim *s, int ifix, double *tri_f, double *tot6);

@@ -78,7 +78,7 @@ def lib():
         L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
-        L.orc_pair_gran_local.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
+        L.orc_pair_gran_local.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int, D]
         L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
         L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
         L.orc_add_wall_cylinder.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 2
@@ -208,11 +208,16 @@ class Oracle:
         out["tag"] = tag
         return out
 
-    def pair_gran_local(self):
-        """compute pair/gran/local id force torque history: (nrows, 12)."""
-        n = self.L.orc_pair_gran_local(self.h, 0, None)
-        rows = np.zeros((n, 12))
-        self.L.orc_pair_gran_local(self.h, n, _dp(rows))
+    def pair_gran_local(self, keys=0x4 | 0x8 | 0x40 | 0x200):
+        """compute pair/gran/local: (nrows, ncols) for a keyword bit mask
+        (bit b: pos, vel, id, force, force_normal, force_tangential, torque,
+        torque_normal, torque_tangential, history, contactArea, delta,
+        contactPoint); the default is id force torque history, 12 columns."""
+        width = (6, 6, 3, 3, 3, 3, 3, 3, 3, 3, 1, 1, 3)
+        nc = sum(w for b, w in enumerate(width) if keys & (1 << b))
+        n = self.L.orc_pair_gran_local(self.h, keys, 0, None)
+        rows = np.zeros((n, nc))
+        self.L.orc_pair_gran_local(self.h, keys, n, _dp(rows))
         return rows
 
     def add_mesh_stress(self, ifix, p_ref):

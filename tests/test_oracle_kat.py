@@ -185,3 +185,34 @@ def test_cylinder_wall_matches_plane():
     fp = one({"kind": "wall_plane", "dim": 0, "pos": 0.02, "wall_type": 1})
     assert fc[0] < 0 and abs(fc[1]) < 1e-15 and abs(fc[2]) < 1e-15
     assert abs(fc[0] - fp[0]) <= 1e-9 * abs(fp[0])
+
+
+def test_pair_gran_local_keywords_periodic_pair():
+    # two equal spheres touching through the periodic x boundary: one row
+    # (kept from the side with the larger tag), pos remapped into the box,
+    # contactPoint at the unremapped midpoint, contactArea = pi (r^2 - d^2/4),
+    # delta = 2 r - d, a head-on force purely normal
+    r = 1e-3
+    sc = base(2, periodic=(1, 0, 0))
+    sc["atoms"] = atoms([[0.0009, 0.5, 0.5], [0.9993, 0.5, 0.5]], [[-0.1, 0, 0], [0.1, 0, 0]], r=r)
+    sc["fixes"] = [{"kind": "nve_sphere"}]
+    o = oracle.Oracle(sc)
+    o.setup()
+    rows = o.pair_gran_local(0x1fff)
+    assert rows.shape == (1, 41)
+    row = rows[0]
+    d = (1.0 - 0.9993) + 0.0009
+    assert np.array_equal(row[0:3], [0.9993, 0.5, 0.5])
+    assert row[3] == pytest.approx(0.0009, rel=1e-9) and np.array_equal(row[4:6], [0.5, 0.5])
+    assert np.array_equal(row[6:12], [0.1, 0, 0, -0.1, 0, 0])
+    assert np.array_equal(row[12:15], [2.0, 1.0, 1.0])
+    F, fn, ft, T, tn, tt, h = (row[15:18], row[18:21], row[21:24], row[24:27], row[27:30], row[30:33], row[33:36])
+    assert F[0] < 0 and F[1] == 0 and F[2] == 0
+    assert fn == pytest.approx(F, rel=1e-14) and np.all(np.abs(ft) <= 1e-14 * abs(F[0]))
+    assert np.array_equal(T, [0, 0, 0]) and np.array_equal(tn, [0, 0, 0]) and np.array_equal(tt, [0, 0, 0])
+    assert np.array_equal(h, [0, 0, 0])
+    assert row[36] == pytest.approx(math.pi * (r * r - d * d / 4), rel=1e-9)
+    assert row[37] == pytest.approx(2 * r - d, rel=1e-9)
+    assert row[38] == pytest.approx(1.0001, rel=1e-12) and np.array_equal(row[39:41], [0.5, 0.5])
+    # the default id force torque history columns are the same numbers
+    assert np.array_equal(o.pair_gran_local(), row[np.r_[12:18, 24:27, 33:36]][None, :])

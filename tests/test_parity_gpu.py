@@ -135,6 +135,7 @@ def test_bidisperse_long_lists_serial_path():
     """Two 3 mm spheres buried in a bed of 0.3 mm ones: each has ~177
     neighbour-list pairs, more than 64 on a side, so its pairs are evaluated
     serially in the reference order by the tail kernel; bit for bit."""
+    import granb200
     sc = S.bidisperse_bed()
     e, o = _pair(sc)
     e.setup()
@@ -158,6 +159,22 @@ def test_bidisperse_long_lists_serial_path():
         assert ra.shape == rb.shape and np.array_equal(ra, rb), "pair/gran/local rows differ"
         pgl_rows += len(rb)
         pgl_periodic += int(rb[:, 2].sum())
+        # every keyword at once (pos remapped into the periodic box, the
+        # normal / tangential splits, contactArea, delta, contactPoint)
+        names = [k for k, _ in granb200.PGL_KEYWORDS]
+        ka, kb = e.pair_gran_local(names), o.pair_gran_local(granb200.pgl_keys(names))
+        assert ka.shape == kb.shape == (len(rb), 41) and np.array_equal(ka, kb), "pair/gran/local keyword rows differ"
+        cols = granb200.pgl_columns(granb200.pgl_keys(names))
+        assert np.array_equal(ka[:, cols.index("id[0]"):cols.index("id[0]") + 3], ra[:, :3])
+        pos = ka[:, :6].reshape(-1, 2, 3)
+        lo, hi = np.asarray(sc["boxlo"]), np.asarray(sc["boxhi"])
+        per = np.asarray(sc["periodic"], dtype=bool)
+        assert np.all((pos[..., per] >= lo[per]) & (pos[..., per] < hi[per])), "pos not remapped into the box"
+        fn = ka[:, cols.index("force_normal[0]"):][:, :3]
+        ft = ka[:, cols.index("force_tangential[0]"):][:, :3]
+        assert np.allclose(fn + ft, ra[:, 3:6], rtol=1e-12, atol=1e-18)
+        dl = ka[:, cols.index("delta")]
+        assert np.all(dl > 0) and np.all(np.isfinite(ka[:, cols.index("contactArea")]))
     assert big_touch > 0, "the large spheres touched nothing"
     assert e.contact_atom()["contact"].max() > 10, "no large sphere with many contacts"
     assert pgl_rows > 100 and pgl_periodic > 0, "pair/gran/local saw too few pairs"
