@@ -147,6 +147,49 @@ int gb2_add_move_mesh_rotate(gb2_ctx *ctx, int ifix_mesh, const double origin[3]
    mesh by v dt, sets the node velocities to v and forces the rebuild after
    skin/2 as for the rotation.  Call before gb2_setup; one mover per mesh. */
 int gb2_add_move_mesh_linear(gb2_ctx *ctx, int ifix_mesh, const double vel[3]);
+/* fix insert/pack (src/fix_insert_pack.cpp with src/fix_insert.cpp) over a
+ * region block, fed by fix particledistribution/discrete
+ * (src/fix_particledistribution_discrete.cpp) of fix particletemplate/sphere
+ * templates with constant radius and density (src/fix_template_sphere.cpp).
+ * Every insertion step (start, then every insert_every steps; insert_every 0
+ * = once) forces a neighbour rebuild; the particles already in the region
+ * are counted and the particles near it gathered on the device, the
+ * reference's Park-Miller draws (src/random_park.cpp) pick positions and
+ * velocities on the host, accepted particles are appended to the device
+ * arrays with tags beyond the largest tag.  Call after gb2_upload_atoms and
+ * before gb2_setup; max_atoms reserves device room for the owned atoms
+ * (initial + inserted: an insertion beyond it returns GB2_ERR_CAPACITY).
+ * Out of scope here: other region styles, radius / density distributions
+ * other than constant, multisphere templates, orientation, set_property. */
+#define GB2_INSERT_MAX_TEMPLATES 8
+typedef struct {
+    int seed;                        /* prime > 10000 (Random::Random, src/random.cpp:55-95) */
+    double region_lo[3], region_hi[3];   /* region block, units box */
+    /* exactly one target (FixInsertPack::calc_insertion_properties) */
+    double volumefraction_region;
+    int particles_in_region;
+    double mass_in_region;
+    int insert_every;                /* >= 0; 0 = once */
+    int start;                       /* first insertion step; 0 = the step after the current one */
+    int maxattempt;                  /* default 50 */
+    int overlapcheck;                /* default 1 */
+    int all_in;                      /* default 0 */
+    int exact_number;                /* random_distribute exact (1, default) or uncorrelated (0) */
+    int vel_style;                   /* 0 constant, 1 uniform, 2 gaussian */
+    double vel[3], vel_fluct[3], omega[3];
+    int ntry_mc;                     /* region volume Monte Carlo samples, default 100000 */
+    int check_dist_from_subdomain_border;   /* default 1 */
+    int dist_seed;                   /* particledistribution/discrete seed, prime > 10000 */
+    int dist_mass_based;             /* 1: weights are mass fractions; 0: numberbased */
+    int ntemplates;
+    int tmpl_type[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_radius[GB2_INSERT_MAX_TEMPLATES], tmpl_density[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_weight[GB2_INSERT_MAX_TEMPLATES];
+    int max_atoms;
+} gb2_insert_pack;
+int gb2_add_insert_pack(gb2_ctx *ctx, const gb2_insert_pack *p);
+/* inserted count and mass so far, and the next insertion step (-1 / 0: none) */
+int gb2_insert_stats(gb2_ctx *ctx, int ifix, long *ninserted, double *massinserted, long *next_step);
 /* current mesh nodes [ntri][3][3] and node velocities (zero for a static mesh)
    of mesh fix ifix; *ntri = element count, nothing written when cap < ntri */
 int gb2_download_mesh_nodes(gb2_ctx *ctx, int ifix, int cap, int *ntri, double *nodes, double *vnode);

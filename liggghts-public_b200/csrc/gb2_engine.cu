@@ -24,6 +24,7 @@
 
 #include "../../include/granb200.h"
 #include "gb2_internal.h"
+#include "gb2_insert.h"
 #include "gb2_kernels.cuh"
 #include "gb2_step.cuh"
 
@@ -194,6 +195,13 @@ struct gb2_ctx {
     std::vector<EvPair> ev_free, ev_pending;
     double prof_ms[5] = {0, 0, 0, 0, 0};
     long n_pair_main = 0;
+    // fix insert/pack (at most one)
+    InsertPack *ins = nullptr;
+    long maxtag = 0;
+    DBuf<uint8_t> insflag;
+    DBuf<int> insidx;
+    DBuf<dbl4> insrec;
+    ~gb2_ctx() { delete ins; }
 };
 
 namespace {
@@ -435,6 +443,9 @@ void neighbor_init(gb2_ctx *c)
     // PairGran::init_one (src/pair_gran.cpp:623): cut = maxrad_i + maxrad_j
     const int nt = c->P.ntypes;
     std::vector<double> maxrad(nt + 1, 0.0);
+    // future particles of an insertion fix count as dynamic (src/pair_gran.cpp:540-554)
+    if (c->ins)
+        for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->ins->max_rad(t));
     for (int i = 0; i < c->nlocal; i++) maxrad[c->h_type[i]] = std::max(maxrad[c->h_type[i]], c->h_radius[i]);
     c->triggersq = 0.25 * c->P.skin * c->P.skin;
     c->cutneighmax = 0.0;
@@ -1302,6 +1313,8 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     CK(cudaMemsetAsync(c->rnum.p, 0, sizeof(int) * cap, c->st));
     CK(cudaMemsetAsync(c->pnum.p, 0, sizeof(int) * cap, c->st));
     CK(cudaStreamSynchronize(c->st));
+    c->maxtag = 0;
+    for (int i = 0; i < n; i++) c->maxtag = std::max<long>(c->maxtag, tag[i]);
     c->have_atoms = true;
     return 0;
 }
@@ -1465,6 +1478,96 @@ int gb2_add_move_mesh_linear(gb2_ctx *c, int ifix_mesh, const double vel[3])
     return 0;
 }
 
+// room for `want` owned atoms in every capacity-strided array (before setup,
+// when those arrays hold their initial zeros)
+static int reserve_cap(gb2_ctx *c, int want)
+{
+    const size_t cap = ((size_t)want + 31) / 32 * 32;
+    if (cap <= (size_t)c->cap) return 0;
+    c->cap = (int)cap;
+    if (ensure_nmax(c, (int)(cap + cap / 4 + 1024))) return GB2_ERR_CUDA;
+    CK(c->f.alloc(cap));
+    CK(c->tq.alloc(cap));
+    CK(c->tailf.alloc(cap));
+    CK(c->tailt.alloc(cap));
+    CK(c->tail.alloc(cap));
+    CK(c->xhold.alloc(cap));
+    CK(c->nnum.alloc(cap));
+    CK(c->rnum.alloc(cap));
+    CK(c->pnum.alloc(cap));
+    CK(c->nbr.alloc((size_t)c->maxn * cap));
+    CK(c->flag.alloc((size_t)c->maxn * cap));
+    CK(c->hist.alloc((size_t)3 * c->maxn * cap));
+    CK(c->hist2.alloc((size_t)3 * c->maxn * cap));
+    CK(c->prevmask.alloc(cap));
+    CK(c->rev.alloc((size_t)c->maxr * cap));
+    CK(c->revs.alloc((size_t)c->maxr * cap));
+    CK(c->ptag.alloc((size_t)c->maxp * cap));
+    CK(c->phist.alloc((size_t)3 * c->maxp * cap));
+    CK(cudaMemsetAsync(c->f.p, 0, sizeof(dbl4) * cap, c->st));
+    CK(cudaMemsetAsync(c->tq.p, 0, sizeof(dbl4) * cap, c->st));
+    CK(cudaMemsetAsync(c->nnum.p, 0, sizeof(int) * cap, c->st));
+    CK(cudaMemsetAsync(c->rnum.p, 0, sizeof(int) * cap, c->st));
+    CK(cudaMemsetAsync(c->pnum.p, 0, sizeof(int) * cap, c->st));
+    for (int k = 0; k < c->nfix; k++) {
+        HostFix &H = c->fix[k];
+        if (H.kind == FIX_WALL_PLANE) {
+            CK(H.inlist.alloc(cap));
+            CK(H.whist.alloc(3 * cap));
+            CK(cudaMemsetAsync(H.inlist.p, 0, cap, c->st));
+            CK(cudaMemsetAsync(H.whist.p, 0, sizeof(double) * 3 * cap, c->st));
+        }
+        if (H.mesh) {
+            MeshFix &M = *H.mesh;
+            CK(M.tcnt.alloc(cap));
+            CK(M.snp.alloc(cap));
+            CK(M.spartner.alloc((size_t)M.maxt * cap));
+            CK(M.shist.alloc((size_t)3 * M.maxt * cap));
+            CK(M.tlist.alloc((size_t)M.maxt * cap));
+            CK(cudaMemsetAsync(M.tcnt.p, 0, sizeof(int) * cap, c->st));
+            CK(cudaMemsetAsync(M.snp.p, 0, sizeof(int) * cap, c->st));
+            CK(cudaMemsetAsync(M.spartner.p, 0xff, sizeof(int) * M.maxt * cap, c->st));
+            CK(cudaMemsetAsync(M.shist.p, 0, sizeof(double) * 3 * M.maxt * cap, c->st));
+        }
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+int gb2_add_insert_pack(gb2_ctx *c, const gb2_insert_pack *p)
+{
+    if (!c || !p) return GB2_ERR_ARG;
+    if (!c->have_atoms) return set_err(c, GB2_ERR_STATE, "upload atoms before adding fixes");
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fixes must be added before setup");
+    if (c->ins) return set_err(c, GB2_ERR_UNSUPPORTED, "one fix insert/pack per context");
+    InsertPack *I = new InsertPack();
+    const std::string e = I->init(*p, c->P.boxlo, c->P.boxhi, c->P.ntypes, c->ntimestep);
+    if (!e.empty()) {
+        delete I;
+        return set_err(c, GB2_ERR_ARG, "fix insert/pack: %s", e.c_str());
+    }
+    if (p->max_atoms < c->nlocal) {
+        delete I;
+        return set_err(c, GB2_ERR_ARG, "fix insert/pack: max_atoms below the current atom count");
+    }
+    const int rc = reserve_cap(c, p->max_atoms);
+    if (rc) {
+        delete I;
+        return rc;
+    }
+    c->ins = I;
+    return 0;
+}
+
+int gb2_insert_stats(gb2_ctx *c, int ifix, long *ninserted, double *massinserted, long *next_step)
+{
+    if (!c || ifix != 0 || !c->ins) return GB2_ERR_ARG;
+    if (ninserted) *ninserted = c->ins->ninserted;
+    if (massinserted) *massinserted = c->ins->massinserted;
+    if (next_step) *next_step = c->ins->next_reneighbor;
+    return 0;
+}
+
 int gb2_download_mesh_nodes(gb2_ctx *c, int ifix, int cap, int *ntri, double *nodes, double *vnode)
 {
     if (!c || !ntri) return GB2_ERR_ARG;
@@ -1516,8 +1619,120 @@ int gb2_setup(gb2_ctx *c)
     if (rc) return rc;
     if (do_force(c, 0, 0, 0, 1)) return GB2_ERR_CUDA;
     CK(cudaStreamSynchronize(c->st));
+    if (c->ins) {   // FixInsert::setup: region volume by Monte Carlo
+        const std::string e = c->ins->setup();
+        if (!e.empty()) return set_err(c, GB2_ERR_ARG, "fix insert/pack: %s", e.c_str());
+    }
     c->setup_done = true;
     c->computeflag = true;
+    return 0;
+}
+
+// fix insert/pack on an insertion step, before the rebuild's history
+// packing (FixInsert::pre_exchange precedes FixContactHistory::pre_exchange,
+// which the pair style adds last): the device selects the owned particles in
+// the region and the particles near it, the host places new particles, and
+// they are appended after the owned ones -- over the first ghost slots, so
+// that, as in the reference, a ghost partner whose slot a new particle took
+// is packed with the new particle's tag.  ghosts_prev: the previous step's
+// ghost positions are in pos2 (the step's integration was fused into the
+// previous pair step and swapped the buffers).
+static int do_insert(gb2_ctx *c, bool ghosts_prev)
+{
+    InsertPack &I = *c->ins;
+    const int nl = c->nlocal, nall = c->nlocal + c->nghost;
+    const dbl4 *gpos = ghosts_prev ? c->pos2.p : c->pos.p;
+    std::vector<double> rr, rm;
+    std::vector<NearParticle> nearp;
+    if (nall > 0) {
+        CK(c->insflag.alloc(2 * (size_t)nall));
+        CK(c->insidx.alloc(2 * (size_t)nall + 2));
+        k_ins_flags<<<nblk(nall), kBlock, 0, c->st>>>(c->pos.p, gpos, nl, nall, I.R, c->insflag.p,
+                                                      c->insflag.p + nall);
+        CKL();
+        thrust::counting_iterator<int> it(0);
+        size_t bytes = 0;
+        cub::DeviceSelect::Flagged(nullptr, bytes, it, c->insflag.p, c->insidx.p, c->insidx.p + 2 * nall, nall, c->st);
+        if (cub_tmp(c, bytes)) return GB2_ERR_CUDA;
+        for (int w = 0; w < 2; w++) {
+            bytes = c->cubtmp.n;
+            CK(cub::DeviceSelect::Flagged(c->cubtmp.p, bytes, it, c->insflag.p + (size_t)w * nall,
+                                          c->insidx.p + (size_t)w * nall, c->insidx.p + 2 * nall + w, nall, c->st));
+        }
+        int cnt[2] = {0, 0};
+        CK(cudaMemcpyAsync(cnt, c->insidx.p + 2 * nall, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        const int ntot = cnt[0] + cnt[1];
+        if (ntot > 0) {
+            CK(c->insrec.alloc(ntot));
+            k_ins_gather<<<nblk(ntot), kBlock, 0, c->st>>>(c->pos.p, c->vel.p, gpos, nl, c->insidx.p, cnt[0],
+                                                           c->insidx.p + nall, cnt[1], c->insrec.p);
+            CKL();
+            std::vector<dbl4> rec(ntot);
+            CK(cudaMemcpyAsync(rec.data(), c->insrec.p, sizeof(dbl4) * ntot, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            rr.resize(cnt[0]);
+            rm.resize(cnt[0]);
+            for (int k = 0; k < cnt[0]; k++) {
+                rr[k] = rec[k].x;
+                rm[k] = rec[k].y;
+            }
+            nearp.resize(cnt[1]);
+            for (int k = 0; k < cnt[1]; k++) {
+                const dbl4 &q = rec[cnt[0] + k];
+                nearp[k] = NearParticle{{q.x, q.y, q.z}, q.w};
+            }
+        }
+    }
+    std::vector<InsertedParticle> out;
+    const std::string e = I.insert(c->ntimestep, rr, rm, std::move(nearp), out);
+    if (!e.empty()) return set_err(c, GB2_ERR_STATE, "fix insert/pack: %s", e.c_str());
+    const int k = (int)out.size();
+    if (k == 0) return 0;
+    if (nl + k > c->cap)
+        return set_err(c, GB2_ERR_CAPACITY, "fix insert/pack: %d atoms exceed the %d reserved (max_atoms)", nl + k,
+                       c->cap);
+    // Atom::tag_extend: tags beyond the largest one, in insertion order
+    std::vector<dbl4> hp(k), hv(k), hw(k);
+    std::vector<int> ht(k), hg(k);
+    for (int q = 0; q < k; q++) {
+        const InsertedParticle &a = out[q];
+        hp[q] = {a.x[0], a.x[1], a.x[2], a.radius};
+        hv[q] = {a.v[0], a.v[1], a.v[2], a.mass};
+        hw[q] = {a.omega[0], a.omega[1], a.omega[2], 0.0};
+        ht[q] = a.type;
+        hg[q] = (int)(c->maxtag + 1 + q);
+        c->h_radius.push_back(a.radius);
+        c->h_type.push_back(a.type);
+    }
+    if ((long)c->maxtag + k > 0x7fffffffL) return set_err(c, GB2_ERR_CAPACITY, "atom tags beyond INT_MAX");
+    c->maxtag += k;
+    if (ensure_nmax(c, nall > nl + k ? nall : nl + k)) return GB2_ERR_CUDA;
+    CK(cudaMemcpyAsync(c->pos.p + nl, hp.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->vel.p + nl, hv.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->omg.p + nl, hw.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->type.p + nl, ht.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->tag.p + nl, hg.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->st));
+    // new atoms start with no list entries, partners or wall history
+    CK(cudaMemsetAsync(c->nnum.p + nl, 0, sizeof(int) * k, c->st));
+    CK(cudaMemsetAsync(c->rnum.p + nl, 0, sizeof(int) * k, c->st));
+    CK(cudaMemsetAsync(c->pnum.p + nl, 0, sizeof(int) * k, c->st));
+    CK(cudaMemsetAsync(c->f.p + nl, 0, sizeof(dbl4) * k, c->st));
+    CK(cudaMemsetAsync(c->tq.p + nl, 0, sizeof(dbl4) * k, c->st));
+    for (int q = 0; q < c->nfix; q++) {
+        HostFix &H = c->fix[q];
+        if (H.kind == FIX_WALL_PLANE) {
+            CK(cudaMemsetAsync(H.inlist.p + nl, 0, k, c->st));
+            for (int d = 0; d < 3; d++)
+                CK(cudaMemsetAsync(H.whist.p + (size_t)d * c->cap + nl, 0, sizeof(double) * k, c->st));
+        }
+        if (H.mesh) {
+            CK(cudaMemsetAsync(H.mesh->tcnt.p + nl, 0, sizeof(int) * k, c->st));
+            CK(cudaMemsetAsync(H.mesh->snp.p + nl, 0, sizeof(int) * k, c->st));
+        }
+    }
+    c->nlocal = nl + k;
+    CK(cudaStreamSynchronize(c->st));
     return 0;
 }
 
@@ -1526,6 +1741,7 @@ int gb2_setup(gb2_ctx *c)
 // mode 2: queued ahead of the decision (no rebuild, no synchronisation).
 static int one_step(gb2_ctx *c, bool last, int mode)
 {
+    const bool ghosts_prev = c->fused_pending;
     c->ntimestep++;
     c->ago++;
     const bool decide = c->ago >= c->P.neigh_delay && c->ago % c->P.neigh_every == 0;
@@ -1565,6 +1781,9 @@ static int one_step(gb2_ctx *c, bool last, int mode)
         }
         CKL();
     }
+    // fix insert/pack: its next_reneighbor forces the rebuild (Neighbor::decide must_check)
+    const bool insert_now = c->ins && c->ins->due(c->ntimestep);
+    if (insert_now) forced = true;
     bool rebuild = decide && !c->P.neigh_check && mode != 2;
     bool mesh_far = false;
     if (check || (moving && mode != 2)) {
@@ -1581,6 +1800,10 @@ static int one_step(gb2_ctx *c, bool last, int mode)
     if (rebuild) {
         const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
         if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
+        if (insert_now) {
+            const int rci = do_insert(c, ghosts_prev);
+            if (rci) return rci;
+        }
         int rc = do_rebuild(c, true, sort_now);
         if (rc) return rc;
         if (prof_end(c, &e)) return GB2_ERR_CUDA;
@@ -1632,7 +1855,7 @@ int gb2_run(gb2_ctx *c, int nsteps)
         if (c->fix[k].mesh && c->fix[k].mesh->moving) queueable = false;
     int s = 0;
     while (s < nsteps) {
-        if (!queueable || !c->fused_pending) {
+        if (!queueable || !c->fused_pending || (c->ins && c->ins->due(c->ntimestep + 1))) {
             int rc = one_step(c, s == nsteps - 1, 0);
             if (rc) return rc;
             s++;
@@ -1651,7 +1874,9 @@ int gb2_run(gb2_ctx *c, int nsteps)
         int head = s, launched = s;
         bool stop = false;
         for (;;) {
-            while (launched < nsteps && launched - head < c->queue_depth) {
+            // an insertion step is never queued (it rebuilds unconditionally)
+            while (launched < nsteps && launched - head < c->queue_depth &&
+                   !(c->ins && c->ins->due(c->ntimestep + 1))) {
                 Queued &Q = q[launched % 16];
                 Q.last = launched == nsteps - 1;
                 Q.nev = c->ev_pending.size();

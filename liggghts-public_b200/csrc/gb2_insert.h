@@ -1,0 +1,549 @@
+// fix insert/pack over a region block with a particledistribution/discrete
+// of constant-radius particletemplate/sphere templates: the host side of
+// particle insertion.  The engine gathers, on the device, the particles in
+// the region and the ones near it (InsertRegion below is shared with those
+// kernels); this file draws the reference's random numbers in the reference's
+// order and places the particles one by one.
+//
+// Behaviour followed:
+//   RanPark::uniform / gaussian          src/random_park.cpp:56-91
+//   Random::Random seed checks            src/random.cpp:55-95
+//   RegBlock inside / surface_interior / surface_exterior
+//                                         src/region_block.cpp:147-259
+//   Region::generate_random(_shrinkby_cut), match_cut, match_expandby_cut,
+//   volume_mc                             src/region.cpp:531-703
+//   FixTemplateSphere volume / mass expectancy, randomize_ptilist
+//                                         src/fix_template_sphere.cpp:244-245, 333-361
+//   FixParticledistributionDiscrete weights, order, randomize_list
+//                                         src/fix_particledistribution_discrete.cpp:130-240, 398-480
+//   FixInsert::pre_exchange, distribute_ninsert_this, load_xnear,
+//   generate_random_velocity              src/fix_insert.cpp:652-972
+//   FixInsertPack::calc_insertion_properties, calc_ninsert_this,
+//   is_nearby, getBoundingBox, calc_maxtry, x_v_omega
+//                                         src/fix_insert_pack.cpp:199-514
+//   RegionNeighborList::hasOverlap (rsq <= radsum^2)
+//                                         src/region_neighbor_list_I.h:72-97
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/granb200.h"
+
+#ifdef __CUDACC__
+#define GB2_HD __host__ __device__
+#else
+#define GB2_HD
+#endif
+
+namespace gb2 {
+
+// region block (interior side) and the bounding box of the near-particle list
+struct InsertRegion {
+    double lo[3], hi[3];     // the block
+    double blo[3], bhi[3];   // FixInsertPack::getBoundingBox: block within the box, widened by 2 maxrad
+    double maxrad;
+    int all_in;
+
+    GB2_HD bool inside(const double *x) const
+    {
+        return x[0] >= lo[0] && x[0] <= hi[0] && x[1] >= lo[1] && x[1] <= hi[1] && x[2] >= lo[2] && x[2] <= hi[2];
+    }
+    // RegBlock::surface_interior != 0: inside and closer than cut to a face
+    GB2_HD bool surface_interior(const double *x, double cut) const
+    {
+        if (x[0] < lo[0] || x[0] > hi[0] || x[1] < lo[1] || x[1] > hi[1] || x[2] < lo[2] || x[2] > hi[2])
+            return false;
+        for (int d = 0; d < 3; d++)
+            if (x[d] - lo[d] < cut || hi[d] - x[d] < cut) return true;
+        return false;
+    }
+    // RegBlock::surface_exterior != 0: outside (or on the surface) and closer than cut
+    GB2_HD bool surface_exterior(const double *x, double cut) const
+    {
+        if (x[0] <= lo[0] - cut || x[0] >= hi[0] + cut || x[1] <= lo[1] - cut || x[1] >= hi[1] + cut ||
+            x[2] <= lo[2] - cut || x[2] >= hi[2] + cut)
+            return false;
+        if (x[0] > lo[0] && x[0] < hi[0] && x[1] > lo[1] && x[1] < hi[1] && x[2] > lo[2] && x[2] < hi[2])
+            return false;
+        double p[3];
+        for (int d = 0; d < 3; d++) p[d] = x[d] < lo[d] ? lo[d] : (x[d] > hi[d] ? hi[d] : x[d]);
+        const double dx = x[0] - p[0], dy = x[1] - p[1], dz = x[2] - p[2];
+        return sqrt(dx * dx + dy * dy + dz * dz) < cut;
+    }
+    // FixInsertPack::is_nearby and RegionNeighborList::isInBoundingBox
+    GB2_HD bool near(const double *x, double rad) const
+    {
+        const double cut = all_in ? maxrad : rad + maxrad;
+        if (!(inside(x) || surface_exterior(x, cut))) return false;
+        return x[0] >= blo[0] && x[0] <= bhi[0] && x[1] >= blo[1] && x[1] <= bhi[1] && x[2] >= blo[2] &&
+               x[2] <= bhi[2];
+    }
+};
+
+// Park-Miller minimal standard generator with Schrage's factorisation
+struct ParkRandom {
+    int seed = 1;
+    int save = 0;
+    double second = 0.0;
+    void reset(int s)
+    {
+        seed = s;
+        save = 0;
+    }
+    double uniform()
+    {
+        const int k = seed / 127773;
+        seed = 16807 * (seed - k * 127773) - 2836 * k;
+        if (seed < 0) seed += 2147483647;
+        return (1.0 / 2147483647) * seed;
+    }
+    // polar Box-Muller, one pair per two calls
+    double gaussian()
+    {
+        double first;
+        if (!save) {
+            double v1, v2, rsq;
+            for (;;) {
+                v1 = 2.0 * uniform() - 1.0;
+                v2 = 2.0 * uniform() - 1.0;
+                rsq = v1 * v1 + v2 * v2;
+                if (rsq < 1.0 && rsq != 0.0) break;
+            }
+            const double fac = std::sqrt(-2.0 * std::log(rsq) / rsq);
+            second = v1 * fac;
+            first = v2 * fac;
+            save = 1;
+        } else {
+            first = second;
+            save = 0;
+        }
+        return first;
+    }
+};
+
+inline bool insert_seed_ok(int seed)
+{
+    if (seed < 10000) return false;
+    for (long d = 2; d * d <= seed; d++)
+        if (seed % d == 0) return false;
+    return true;
+}
+
+struct InsertedParticle {
+    double x[3], v[3], omega[3];
+    double radius, density, mass;
+    int type;
+};
+
+// a particle the overlap test sees (existing or accepted this step)
+struct NearParticle {
+    double x[3], r;
+};
+
+class InsertPack {
+public:
+    gb2_insert_pack P{};
+    InsertRegion R{};
+    double boxlo[3] = {0, 0, 0}, boxhi[3] = {0, 0, 0};
+    double distweight[GB2_INSERT_MAX_TEMPLATES] = {};
+    double tvol[GB2_INSERT_MAX_TEMPLATES] = {}, tmass[GB2_INSERT_MAX_TEMPLATES] = {};
+    int distorder[GB2_INSERT_MAX_TEMPLATES] = {};
+    double volexpect = 0, massexpect = 0, maxrad = 0, maxrbound = 0;
+    double region_volume = 0, region_volume_local = 0, insertion_ratio = 0;
+    long next_reneighbor = 0, most_recent = -1;
+    long ninserted = 0;
+    double massinserted = 0;
+    bool props_done = false;
+    ParkRandom rnd, rreg, rdist;   // fix insert, its region, the distribution
+
+    // constructor checks of the three commands; returns an error message or ""
+    std::string init(const gb2_insert_pack &p, const double lo[3], const double hi[3], int ntypes, long ntimestep)
+    {
+        P = p;
+        for (int d = 0; d < 3; d++) {
+            boxlo[d] = lo[d];
+            boxhi[d] = hi[d];
+        }
+        if (!insert_seed_ok(P.seed) || !insert_seed_ok(P.dist_seed))
+            return "random seeds must be prime numbers > 10000";
+        if (P.ntemplates < 1 || P.ntemplates > GB2_INSERT_MAX_TEMPLATES) return "illegal number of templates";
+        if (P.maxattempt <= 0 || P.ntry_mc <= 0) return "maxattempt and ntry_mc must be positive";
+        if (P.insert_every < 0) return "insert_every must be >= 0";
+        if (P.vel_style < 0 || P.vel_style > 2) return "vel style must be constant, uniform or gaussian";
+        int n_defined = (P.volumefraction_region > 0.) + (P.particles_in_region > 0) + (P.mass_in_region > 0.);
+        if (n_defined != 1)
+            return "must define exactly one keyword out of 'volumefraction_region', 'particles_in_region', and "
+                   "'mass_in_region'";
+        if (P.volumefraction_region < 0. || P.volumefraction_region > 1.) return "illegal volumefraction_region";
+        for (int d = 0; d < 3; d++)
+            if (!(P.region_lo[d] < P.region_hi[d])) return "empty region block";
+        const int nt = P.ntemplates;
+        for (int i = 0; i < nt; i++) {
+            if (P.tmpl_type[i] < 1 || P.tmpl_type[i] > ntypes) return "template atom type out of range";
+            if (!(P.tmpl_radius[i] > 0.) || !(P.tmpl_density[i] > 0.)) return "template radius and density > 0";
+            if (P.tmpl_weight[i] < 0) return "invalid weight";
+            // FixTemplateSphere: volume_expect = cubic expectancy * 4 pi / 3, mass_expect = density * volume
+            const double r = P.tmpl_radius[i];
+            tvol[i] = r * r * r * 4. * M_PI / 3.;
+            tmass[i] = P.tmpl_density[i] * tvol[i];
+            if (tvol[i] < 1e-12) return "Volume expectancy too small";
+            distweight[i] = P.tmpl_weight[i];
+        }
+        double weightsum = 0;
+        for (int i = 0; i < nt; i++) weightsum += distweight[i];
+        for (int i = 0; i < nt; i++) distweight[i] /= weightsum;
+        if (P.dist_mass_based) {
+            for (int i = 0; i < nt; i++) distweight[i] = distweight[i] / tmass[i];
+            weightsum = 0;
+            for (int i = 0; i < nt; i++) weightsum += distweight[i];
+            for (int i = 0; i < nt; i++) distweight[i] /= weightsum;
+        }
+        volexpect = massexpect = 0.;
+        for (int i = 0; i < nt; i++) {
+            volexpect += tvol[i] * distweight[i];
+            massexpect += tmass[i] * distweight[i];
+        }
+        // templates by volume, descending (the reference's bubble sort)
+        for (int i = 0; i < nt; i++) distorder[i] = i;
+        bool swapped;
+        int n = nt;
+        do {
+            swapped = false;
+            for (int i = 0; i < nt - 1; i++)
+                if (tvol[distorder[i]] < tvol[distorder[i + 1]]) {
+                    std::swap(distorder[i], distorder[i + 1]);
+                    swapped = true;
+                }
+            n--;
+        } while (swapped && n > 0);
+        maxrbound = 0.;
+        for (int i = 0; i < nt; i++) maxrbound = std::max(maxrbound, P.tmpl_radius[i]);
+        maxrad = 0.;
+        for (int t = 1; t <= ntypes; t++) maxrad = std::max(maxrad, max_rad(t));
+        rnd.reset(P.seed);
+        rdist.reset(P.dist_seed);
+        long first = P.start > 0 ? P.start : ntimestep + 1;
+        if (first < ntimestep + 1) return "'start' step can not be before current step";
+        next_reneighbor = first;
+        for (int d = 0; d < 3; d++) {
+            R.lo[d] = P.region_lo[d];
+            R.hi[d] = P.region_hi[d];
+        }
+        R.all_in = P.all_in;
+        R.maxrad = maxrad;
+        // FixInsertPack::getBoundingBox: the block shrunk to the (single) subdomain, widened by 2 maxrad
+        for (int d = 0; d < 3; d++) {
+            double a = R.lo[d], b = R.hi[d];
+            if (a < boxlo[d]) a = boxlo[d];
+            if (b > boxhi[d]) b = boxhi[d];
+            R.blo[d] = a - 2 * maxrad;
+            R.bhi[d] = b + 2 * maxrad;
+        }
+        return "";
+    }
+
+    // FixParticledistributionDiscrete::max_rad(type): largest template radius of that type
+    double max_rad(int type) const
+    {
+        double m = 0.;
+        for (int i = 0; i < P.ntemplates; i++)
+            if (P.tmpl_type[i] == type && P.tmpl_radius[i] > m) m = P.tmpl_radius[i];
+        return m;
+    }
+
+    // FixInsertPack::calc_insertion_properties (FixInsert::setup, once)
+    std::string setup()
+    {
+        if (props_done) return "";
+        props_done = true;
+        rreg.reset(P.seed + 12);   // reset_random(seed + SEED_OFFSET)
+        // Region::volume_mc(ntry_mc, all_in, max_r_bound)
+        const double *lo = P.region_lo, *hi = P.region_hi;
+        long n_in_global = 0, n_in_local = 0;
+        for (int i = 0; i < P.ntry_mc; i++) {
+            double pos[3];
+            pos[0] = lo[0] + rreg.uniform() * (hi[0] - lo[0]);
+            pos[1] = lo[1] + rreg.uniform() * (hi[1] - lo[1]);
+            pos[2] = lo[2] + rreg.uniform() * (hi[2] - lo[2]);
+            if (!(pos[0] >= boxlo[0] && pos[0] <= boxhi[0] && pos[1] >= boxlo[1] && pos[1] <= boxhi[1] &&
+                  pos[2] >= boxlo[2] && pos[2] <= boxhi[2]))
+                continue;
+            if (R.inside(pos)) {
+                n_in_global++;
+                if (!P.all_in || !R.surface_interior(pos, maxrbound)) n_in_local++;
+            }
+        }
+        if (n_in_global == 0) return "Unable to calculate region volume";
+        const double vol_bbox = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+        const double vol_global = static_cast<double>(n_in_global) / static_cast<double>(P.ntry_mc) * vol_bbox;
+        double vol_local = static_cast<double>(n_in_local) / static_cast<double>(P.ntry_mc) * vol_bbox;
+        const double vol_local_all = vol_local;
+        if (vol_local_all < 1.e-10) return "Unable to calculate region volume (too small for all_in)";
+        vol_local *= (vol_global / vol_local_all);
+        region_volume = vol_global;
+        region_volume_local = vol_local;
+        if (region_volume <= 0. || region_volume_local < 0. ||
+            (region_volume_local - region_volume) / region_volume > 1e-3)
+            return "Fix insert: Region volume calculation with MC failed";
+        return "";
+    }
+
+    bool due(long step) const { return next_reneighbor == step && most_recent != step; }
+
+    // one insertion (FixInsert::pre_exchange on step `step`): rreg_r / rreg_m
+    // are radius and mass of the owned particles inside the region in index
+    // order, nearp the particles near it; the accepted particles are appended
+    // to out.  Returns an error message or "".
+    std::string insert(long step, const std::vector<double> &rreg_r, const std::vector<double> &rreg_m,
+                       std::vector<NearParticle> nearp, std::vector<InsertedParticle> &out)
+    {
+        out.clear();
+        most_recent = step;
+        // FixInsertPack::calc_ninsert_this
+        int np_region = (int)rreg_r.size();
+        double vol_region = 0., mass_region = 0.;
+        const double _4Pi3 = 4. * M_PI / 3.;
+        for (int i = 0; i < np_region; i++) {
+            vol_region += _4Pi3 * rreg_r[i] * rreg_r[i] * rreg_r[i];
+            mass_region += rreg_m[i];
+        }
+        int ninsert_this = 0;
+        if (P.volumefraction_region > 0.) {
+            ninsert_this = static_cast<int>((P.volumefraction_region * region_volume - vol_region) / volexpect +
+                                            rnd.uniform());
+            insertion_ratio = vol_region / (P.volumefraction_region * region_volume);
+        } else if (P.particles_in_region > 0) {
+            ninsert_this = P.particles_in_region - np_region;
+            insertion_ratio = static_cast<double>(np_region) / static_cast<double>(P.particles_in_region);
+        } else {
+            ninsert_this = static_cast<int>((P.mass_in_region - mass_region) / massexpect + rnd.uniform());
+            insertion_ratio = mass_region / P.mass_in_region;
+        }
+        if (ninsert_this < -200000) return "overflow in particle number calculation";
+        if (ninsert_this < 0) ninsert_this = 0;
+        if (insertion_ratio < 0.) insertion_ratio = 0.;
+        if (insertion_ratio > 1.) insertion_ratio = 1.;
+        // distribute_ninsert_this on one process
+        const double fraction_local = region_volume_local / region_volume;
+        int nlocal_ins;
+        if (!P.exact_number) {
+            nlocal_ins = static_cast<int>(fraction_local * static_cast<double>(ninsert_this) + rnd.uniform());
+        } else {
+            double f = fraction_local;
+            if (f < 0.02) f = 0.;
+            if (f == 0.) return "Internal error distributing particles to processes";
+            f /= f;
+            nlocal_ins = static_cast<int>(f * static_cast<double>(ninsert_this));
+            // the remainder f * n - n is zero: no gap draws
+        }
+        // FixParticledistributionDiscrete::randomize_list
+        const int nt = P.ntemplates;
+        int parttogen[GB2_INSERT_MAX_TEMPLATES];
+        if (!P.exact_number) {
+            for (int i = 0; i < nt; i++)
+                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i] + rdist.uniform());
+        } else {
+            int ntrunc = 0;
+            double remainder[GB2_INSERT_MAX_TEMPLATES];
+            for (int i = 0; i < nt; i++) {
+                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i]);
+                ntrunc += parttogen[i];
+                remainder[i] = static_cast<double>(nlocal_ins) * distweight[i] - static_cast<double>(parttogen[i]);
+            }
+            const int gap = nlocal_ins - ntrunc;
+            for (int i = 0; i < gap; i++) {
+                const double r = rdist.uniform() * static_cast<double>(gap);
+                int j = 0;
+                double rsum = remainder[0];
+                while (rsum < r && j < nt - 1) {
+                    j++;
+                    rsum += remainder[j];
+                }
+                parttogen[j]++;
+            }
+        }
+        // particles to insert, large to small templates
+        std::vector<int> plist;
+        for (int i = 0; i < nt; i++) {
+            const int t = distorder[i];
+            for (int j = 0; j < parttogen[t]; j++) plist.push_back(t);
+        }
+        const int ntot = (int)plist.size();
+        if (ntot == 0) {
+            if (P.insert_every) next_reneighbor += P.insert_every;
+            else next_reneighbor = -1;
+            return "";
+        }
+        // the near list grows by each accepted particle
+        NearGrid grid(R, maxrad);
+        if (P.overlapcheck)
+            for (const NearParticle &q : nearp) grid.add(q);
+        // FixInsertPack::x_v_omega
+        const int maxtry = insertion_ratio >= 1.
+                               ? ntot * P.maxattempt
+                               : static_cast<int>(static_cast<double>(ntot * P.maxattempt) / (1. - insertion_ratio));
+        int ntry = 0;
+        int done = 0;
+        double mass_this = 0.;
+        if (!P.overlapcheck) {
+            for (int it = 0; it < ntot; it++) {
+                const int t = plist[done];
+                double pos[3], v[3];
+                if (!random_position(pos, P.tmpl_radius[t])) return "region too small for all_in";
+                random_velocity(v);
+                if (pos[0] == 0. && pos[1] == 0. && pos[2] == 0.) return "FixInsertPack::x_v_omega() illegal position";
+                out.push_back(make(t, pos, v));
+                mass_this += out.back().mass;
+                done++;
+            }
+        } else {
+            while (ntry < maxtry && done < ntot) {
+                const int t = plist[done];
+                const double rbound = P.tmpl_radius[t];
+                int nins = 0;
+                while (nins == 0 && ntry < maxtry) {
+                    double pos[3];
+                    do {
+                        if (!random_position(pos, rbound)) return "region too small for all_in";
+                        ntry++;
+                    } while (P.check_dist_from_subdomain_border && ntry < maxtry && dist_box_borders(pos) < rbound);
+                    if (ntry == maxtry) break;
+                    double v[3];
+                    random_velocity(v);
+                    if (!grid.overlaps(pos, rbound)) {
+                        grid.add(NearParticle{{pos[0], pos[1], pos[2]}, rbound});
+                        out.push_back(make(t, pos, v));
+                        nins = 1;
+                    }
+                }
+                if (nins > 0) {
+                    mass_this += out.back().mass;
+                    done++;
+                }
+            }
+        }
+        ninserted += done;
+        massinserted += mass_this;
+        if (P.insert_every) next_reneighbor += P.insert_every;
+        else next_reneighbor = 0;
+        return "";
+    }
+
+private:
+    // cell list over the near particles: a test sees every particle whose
+    // sphere reaches the candidate's (exact, unlike a fixed stencil)
+    struct NearGrid {
+        double h, inv;
+        double rmax = 0.;
+        std::unordered_map<long long, std::vector<NearParticle>> cells;
+        NearGrid(const InsertRegion &, double maxrad_)
+        {
+            h = 4 * maxrad_ > 0 ? 4 * maxrad_ : 1.0;
+            inv = 1.0 / h;
+        }
+        static long long key(long long a, long long b, long long c)
+        {
+            return ((a & 0x1fffff) << 42) | ((b & 0x1fffff) << 21) | (c & 0x1fffff);
+        }
+        void add(const NearParticle &q)
+        {
+            rmax = std::max(rmax, q.r);
+            cells[key((long long)std::floor(q.x[0] * inv), (long long)std::floor(q.x[1] * inv),
+                      (long long)std::floor(q.x[2] * inv))]
+                .push_back(q);
+        }
+        bool overlaps(const double *x, double r) const
+        {
+            const double reach = r + rmax;
+            long long lo[3], hi[3];
+            for (int d = 0; d < 3; d++) {
+                lo[d] = (long long)std::floor((x[d] - reach) * inv);
+                hi[d] = (long long)std::floor((x[d] + reach) * inv);
+            }
+            for (long long a = lo[0]; a <= hi[0]; a++)
+                for (long long b = lo[1]; b <= hi[1]; b++)
+                    for (long long c = lo[2]; c <= hi[2]; c++) {
+                        auto it = cells.find(key(a, b, c));
+                        if (it == cells.end()) continue;
+                        for (const NearParticle &p : it->second) {
+                            double del[3] = {x[0] - p.x[0], x[1] - p.x[1], x[2] - p.x[2]};
+                            const double rsq = del[0] * del[0] + del[1] * del[1] + del[2] * del[2];
+                            const double radsum = r + p.r;
+                            if (rsq <= radsum * radsum) return true;
+                        }
+                    }
+            return false;
+        }
+    };
+
+    InsertedParticle make(int t, const double *pos, const double *v) const
+    {
+        InsertedParticle q;
+        for (int d = 0; d < 3; d++) {
+            q.x[d] = pos[d];
+            q.v[d] = v[d];
+            q.omega[d] = P.omega[d];
+        }
+        q.radius = P.tmpl_radius[t];
+        q.density = P.tmpl_density[t];
+        q.mass = q.density * (q.radius * q.radius * q.radius * 4. * M_PI / 3.);
+        q.type = P.tmpl_type[t];
+        return q;
+    }
+
+    // Region::generate_random / generate_random_shrinkby_cut on the block
+    // within the single subdomain (the box)
+    bool random_position(double *pos, double rbound)
+    {
+        double lo[3], hi[3], diff[3];
+        for (int d = 0; d < 3; d++) {
+            lo[d] = std::max(P.region_lo[d], boxlo[d]);
+            hi[d] = std::min(P.region_hi[d], boxhi[d]);
+            diff[d] = hi[d] - lo[d];
+        }
+        if (P.all_in)
+            for (int d = 0; d < 3; d++)
+                if (P.region_hi[d] - P.region_lo[d] < 2. * rbound) return false;
+        for (;;) {
+            pos[0] = lo[0] + rreg.uniform() * diff[0];
+            pos[1] = lo[1] + rreg.uniform() * diff[1];
+            pos[2] = lo[2] + rreg.uniform() * diff[2];
+            if (!R.inside(pos)) continue;
+            if (P.all_in && R.surface_interior(pos, rbound)) continue;
+            return true;
+        }
+    }
+
+    // FixInsert::generate_random_velocity
+    void random_velocity(double *v)
+    {
+        for (int d = 0; d < 3; d++) v[d] = P.vel[d];
+        if (P.vel_style == 1) {
+            v[0] = P.vel[0] + P.vel_fluct[0] * 2.0 * (rnd.uniform() - 0.50);
+            v[1] = P.vel[1] + P.vel_fluct[1] * 2.0 * (rnd.uniform() - 0.50);
+            v[2] = P.vel[2] + P.vel_fluct[2] * 2.0 * (rnd.uniform() - 0.50);
+        } else if (P.vel_style == 2) {
+            v[0] = P.vel[0] + P.vel_fluct[0] * rnd.gaussian();
+            v[1] = P.vel[1] + P.vel_fluct[1] * rnd.gaussian();
+            v[2] = P.vel[2] + P.vel_fluct[2] * rnd.gaussian();
+        }
+    }
+
+    // Domain::dist_subbox_borders with the box as the subdomain
+    double dist_box_borders(const double *pos) const
+    {
+        double dlo = std::fabs(boxlo[0] - pos[0]), dhi = std::fabs(boxhi[0] - pos[0]);
+        for (int d = 1; d < 3; d++) {
+            dlo = std::min(dlo, std::fabs(boxlo[d] - pos[d]));
+            dhi = std::min(dhi, std::fabs(boxhi[d] - pos[d]));
+        }
+        return dlo < dhi ? dlo : dhi;
+    }
+};
+
+
+}  // namespace gb2

@@ -15,6 +15,7 @@
 
 #include "../../include/granb200.h"
 #include "gb2_device.cuh"
+#include "gb2_insert.h"
 
 namespace gb2 {
 
@@ -807,6 +808,36 @@ __global__ void k_contact_atom(Dev D, double *out)
         if (rsq <= radsum * radsum) cnt++;
     }
     out[k] = (double)cnt;
+}
+
+// fix insert/pack selections (FixInsertPack::calc_ninsert_this counts owned
+// particles inside the region; FixInsert::load_xnear loads owned and ghost
+// particles near it).  Ghost positions are those of the previous step's
+// forward communication (gpos); owned ones the current ones.
+__global__ void k_ins_flags(const dbl4 *pos, const dbl4 *gpos, int nlocal, int nall, InsertRegion R, uint8_t *freg,
+                            uint8_t *fnear)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nall) return;
+    const dbl4 p = i < nlocal ? pos[i] : gpos[i];
+    const double x[3] = {p.x, p.y, p.z};
+    freg[i] = (i < nlocal && R.inside(x)) ? 1 : 0;
+    fnear[i] = R.near(x, p.w) ? 1 : 0;
+}
+
+// records of the selected particles: region ones (radius, mass) first, then
+// near ones (x, y, z, radius)
+__global__ void k_ins_gather(const dbl4 *pos, const dbl4 *vel, const dbl4 *gpos, int nlocal, const int *ireg, int nreg,
+                             const int *inear, int nnear, dbl4 *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nreg) {
+        const int i = ireg[k];
+        out[k] = dbl4{pos[i].w, vel[i].w, 0.0, 0.0};
+    } else if (k < nreg + nnear) {
+        const int i = inear[k - nreg];
+        out[k] = i < nlocal ? pos[i] : gpos[i];
+    }
 }
 
 // compute pair/gran/local id force torque history (src/compute_pair_gran_local.cpp

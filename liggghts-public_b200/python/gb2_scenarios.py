@@ -450,3 +450,32 @@ def subset(sc, n):
     out = dict(sc)
     out["atoms"] = {k: np.ascontiguousarray(v[:n]) for k, v in sc["atoms"].items()}
     return out
+
+
+def insert_pour(n_bed=400, seed=77, periodic=True, dt=2e-6, vel_style="uniform", all_in=0, exact_number=1,
+                target=("volumefraction_region", 0.25), insert_every=300, max_atoms=8000):
+    """fix insert/pack above a settled-looking bed: a 20 x 20 x 60 mm box (x/y
+    periodic or walled), n_bed spheres of r = 1 mm at the bottom, and a region
+    block 2-18 x 2-18 x 30-55 mm refilled every insert_every steps from two
+    templates (r = 1.2 mm and 0.8 mm, 2500 kg/m^3, mass fractions 0.5 / 0.5)
+    falling at -0.5 m/s (+- 0.1 m/s per component for vel uniform)."""
+    sc = sphere_pour(n=n_bed, seed=seed, dt=dt, box=(0.02, 0.02, 0.06), spacing=(2.5e-3, 2.5e-3, 2.4e-3), vmax=0.05)
+    sc["name"] = "insert_pour"
+    sc["periodic"] = [1, 1, 0] if periodic else [0, 0, 0]
+    fixes = [sc["fixes"][0], sc["fixes"][1]]
+    if not periodic:
+        for dim in (0, 1):
+            fixes.append({"kind": "wall_plane", "dim": dim, "pos": 0.0, "wall_type": 1, "rolling_cdt": 0})
+            fixes.append({"kind": "wall_plane", "dim": dim, "pos": 0.02, "wall_type": 1, "rolling_cdt": 0})
+    fx = {
+        "kind": "insert_pack", "seed": 32452843, "dist_seed": 15485863,
+        "region_lo": [0.002, 0.002, 0.03], "region_hi": [0.018, 0.018, 0.055],
+        target[0]: target[1], "insert_every": insert_every, "all_in": all_in, "exact_number": exact_number,
+        "vel_style": vel_style, "vel": [0.0, 0.0, -0.5], "vel_fluct": [0.1, 0.1, 0.1],
+        "templates": [{"type": 1, "radius": 1.2e-3, "density": 2500.0, "weight": 0.5},
+                      {"type": 1, "radius": 0.8e-3, "density": 2500.0, "weight": 0.5}],
+        "max_atoms": max_atoms,
+    }
+    fixes += [fx, {"kind": "nve_sphere"}]
+    sc["fixes"] = fixes
+    return sc

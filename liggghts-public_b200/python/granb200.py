@@ -31,7 +31,7 @@ EXPORTS = (
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
-    "gb2_pair_gran_local_keys",
+    "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -62,6 +62,82 @@ def pgl_columns(keys):
         if keys & (1 << b):
             cols += [name] if n == 1 else ["%s[%d]" % (name, c) for c in range(n)]
     return cols
+
+
+INSERT_MAX_TEMPLATES = 8   # GB2_INSERT_MAX_TEMPLATES
+
+
+class InsertPackParams(ctypes.Structure):
+    """gb2_insert_pack: fix insert/pack + particledistribution/discrete + particletemplate/sphere."""
+    _fields_ = [
+        ("seed", ctypes.c_int),
+        ("region_lo", ctypes.c_double * 3),
+        ("region_hi", ctypes.c_double * 3),
+        ("volumefraction_region", ctypes.c_double),
+        ("particles_in_region", ctypes.c_int),
+        ("mass_in_region", ctypes.c_double),
+        ("insert_every", ctypes.c_int),
+        ("start", ctypes.c_int),
+        ("maxattempt", ctypes.c_int),
+        ("overlapcheck", ctypes.c_int),
+        ("all_in", ctypes.c_int),
+        ("exact_number", ctypes.c_int),
+        ("vel_style", ctypes.c_int),
+        ("vel", ctypes.c_double * 3),
+        ("vel_fluct", ctypes.c_double * 3),
+        ("omega", ctypes.c_double * 3),
+        ("ntry_mc", ctypes.c_int),
+        ("check_dist_from_subdomain_border", ctypes.c_int),
+        ("dist_seed", ctypes.c_int),
+        ("dist_mass_based", ctypes.c_int),
+        ("ntemplates", ctypes.c_int),
+        ("tmpl_type", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("tmpl_radius", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_density", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_weight", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("max_atoms", ctypes.c_int),
+    ]
+
+
+VEL_STYLES = {"constant": 0, "uniform": 1, "gaussian": 2}
+
+
+def insert_pack_params(fx, struct=InsertPackParams):
+    """Fill the insertion parameter struct from a scenario fix dict (the
+    reference's keyword defaults where a key is absent)."""
+    p = struct()
+    p.seed = int(fx["seed"])
+    for d in range(3):
+        p.region_lo[d] = fx["region_lo"][d]
+        p.region_hi[d] = fx["region_hi"][d]
+        p.vel[d] = fx.get("vel", (0.0, 0.0, 0.0))[d]
+        p.vel_fluct[d] = fx.get("vel_fluct", (0.0, 0.0, 0.0))[d]
+        p.omega[d] = fx.get("omega", (0.0, 0.0, 0.0))[d]
+    p.volumefraction_region = float(fx.get("volumefraction_region", 0.0))
+    p.particles_in_region = int(fx.get("particles_in_region", 0))
+    p.mass_in_region = float(fx.get("mass_in_region", 0.0))
+    p.insert_every = int(fx["insert_every"])
+    p.start = int(fx.get("start", 0))
+    p.maxattempt = int(fx.get("maxattempt", 50))
+    p.overlapcheck = int(fx.get("overlapcheck", 1))
+    p.all_in = int(fx.get("all_in", 0))
+    p.exact_number = int(fx.get("exact_number", 1))
+    p.vel_style = VEL_STYLES[fx.get("vel_style", "constant")]
+    p.ntry_mc = int(fx.get("ntry_mc", 100000))
+    p.check_dist_from_subdomain_border = int(fx.get("check_dist_from_subdomain_border", 1))
+    p.dist_seed = int(fx["dist_seed"])
+    p.dist_mass_based = int(fx.get("dist_mass_based", 1))
+    tm = fx["templates"]
+    if not 1 <= len(tm) <= INSERT_MAX_TEMPLATES:
+        raise ValueError("1 to %d templates" % INSERT_MAX_TEMPLATES)
+    p.ntemplates = len(tm)
+    for i, t in enumerate(tm):
+        p.tmpl_type[i] = int(t["type"])
+        p.tmpl_radius[i] = float(t["radius"])
+        p.tmpl_density[i] = float(t["density"])
+        p.tmpl_weight[i] = float(t["weight"])
+    p.max_atoms = int(fx.get("max_atoms", 0))
+    return p
 
 
 class Params(ctypes.Structure):
@@ -144,6 +220,9 @@ def lib(path=LIB_PATH):
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
         L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
+        L.gb2_add_insert_pack.argtypes = [vp, ctypes.POINTER(InsertPackParams)]
+        L.gb2_insert_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long), D,
+                                       ctypes.POINTER(ctypes.c_long)]
         L.gb2_pair_gran_local_keys.argtypes = [vp, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(ctypes.c_int), D]
         L.gb2_download_mesh_stress.argtypes = [vp, ctypes.c_int, ctypes.c_int, D, D, D, D]
@@ -247,6 +326,11 @@ class Engine:
                 k = None
             elif kind == "nve_sphere":
                 k = None
+            elif kind == "insert_pack":
+                ip = insert_pack_params(fx)
+                keep.append(ip)
+                self._check(L.gb2_add_insert_pack(self.h, ctypes.byref(ip)))
+                k = 0
             else:
                 raise ValueError("unsupported fix kind " + kind)
             if k is not None and k < 0:
@@ -311,8 +395,15 @@ class Engine:
         self._check(self.L.gb2_timer_stop(self.h, ctypes.byref(ms)))
         return ms.value
 
+    def count(self):
+        """Current number of owned atoms (fix insert/pack adds atoms)."""
+        cnt0 = ctypes.c_int()
+        self._check(self.L.gb2_download_atoms(self.h, 0, ctypes.byref(cnt0), None, None, None, None, None, None))
+        self.n = cnt0.value
+        return self.n
+
     def atoms(self):
-        n = self.n
+        n = self.count()
         out = {k: np.zeros((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
         tag = np.zeros(n, dtype=np.int32)
         cnt = ctypes.c_int()
@@ -331,6 +422,12 @@ class Engine:
         hi = np.zeros((n, 3))
         self._check(self.L.gb2_download_pairs(self.h, n, ctypes.byref(cnt), _ip(ti), _ip(tj), _ip(fl), _dp(hi)))
         return {"tag_i": ti, "tag_j": tj, "flag": fl, "hist": hi}
+
+    def insert_stats(self):
+        """fix insert/pack: particles and mass inserted so far, next insertion step."""
+        n, nxt, m = ctypes.c_long(), ctypes.c_long(), np.zeros(1)
+        self._check(self.L.gb2_insert_stats(self.h, 0, ctypes.byref(n), _dp(m), ctypes.byref(nxt)))
+        return {"ninserted": n.value, "massinserted": float(m[0]), "next_step": nxt.value}
 
     def pair_gran_local(self, keywords=None):
         """compute pair/gran/local on the device: (nrows, ncols).  Without
@@ -393,12 +490,14 @@ class Engine:
     def contact_atom(self):
         """compute contact/atom (skin 0) on the device: {tag, contact}."""
         n = ctypes.c_int()
+        self.count()
         tag = np.zeros(self.n, dtype=np.int32)
         out = np.zeros(self.n)
         self._check(self.L.gb2_contact_atom(self.h, self.n, ctypes.byref(n), _ip(tag), _dp(out)))
         return {"tag": tag, "contact": out}
 
     def wall_hist(self, ifix):
+        self.count()
         h = np.zeros((self.n, 3))
         self._check(self.L.gb2_download_wall_history(self.h, self.fix_ids[ifix], self.n, _dp(h)))
         return h

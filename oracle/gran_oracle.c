@@ -123,9 +123,14 @@ struct orc_sim {
     long nextsort; int snbinx, snbiny, snbinz; double sbboxlo[3], sbininvx, sbininvy, sbininvz;
     /* fixes */
     int nfix; fixrec fix[MAXFIX]; int has_nve;
+    struct ins_state *ins;   /* fix insert/pack, at most one */
     int setupflag;
     char err[256];
 };
+
+struct ins_state;
+static void ins_max_rad(const struct ins_state *I, int type, double *mx);
+static long ins_next(const struct ins_state *I);
 
 static void fail(orc_sim *s, const char *fmt, ...)
 {
@@ -438,7 +443,7 @@ void orc_destroy(orc_sim *s)
     if (!s) return;
     free(s->x); free(s->v); free(s->omega); free(s->f); free(s->torque); free(s->radius); free(s->rmass);
     free(s->type); free(s->tag); free(s->bins); free(s->binhead); free(s->stencil); free(s->xhold);
-    free(s->gsrc); free(s->gshift); free(s->maxrad);
+    free(s->gsrc); free(s->gshift); free(s->maxrad); free(s->ins);
     free(s->nstart); free(s->nnum); free(s->nbr); free(s->flag); free(s->hist);
     for (int i = 0; i < s->nmax; i++) { if (s->partner) free(s->partner[i]); if (s->phist) free(s->phist[i]); }
     free(s->npartner); free(s->partner); free(s->phist);
@@ -907,6 +912,8 @@ static void neighbor_init(orc_sim *s)
     const int nt = s->ntypes;
     free(s->maxrad);
     s->maxrad = calloc(nt+1, sizeof(double));
+    if (s->ins)   /* future particles count as dynamic, src/pair_gran.cpp:540-554 */
+        for (int t = 1; t <= nt; t++) ins_max_rad(s->ins, t, &s->maxrad[t]);
     for (int i = 0; i < s->nlocal; i++)
         if (s->radius[i] > s->maxrad[s->type[i]]) s->maxrad[s->type[i]] = s->radius[i];
     s->triggersq = 0.25*s->p.skin*s->p.skin;
@@ -1264,6 +1271,7 @@ static int neighbor_decide(orc_sim *s)
     for (int k = 0; k < s->nfix; k++)
         if (s->fix[k].kind == ORC_FIX_WALL_MESH && s->fix[k].wm->moving && s->fix[k].wm->next_reneighbor == s->ntimestep)
             return 1;
+    if (s->ins && ins_next(s->ins) == s->ntimestep) return 1;   /* FixInsert::next_reneighbor */
     s->ago++;
     if (s->ago >= s->p.delay && s->ago % s->p.every == 0) {
         if (!s->p.check) return 1;
@@ -1949,6 +1957,463 @@ static void pre_neighbor_all(orc_sim *s)
 }
 
 /* ------------------------------------------------------------------ */
+/* fix insert/pack (restated; see the header)                           */
+
+typedef struct { int seed, save; double second; } park_t;
+
+/* RanPark::uniform src/random_park.cpp:56-62 */
+static double park_uniform(park_t *r)
+{
+    int k = r->seed / 127773;
+    r->seed = 16807 * (r->seed - k * 127773) - 2836 * k;
+    if (r->seed < 0) r->seed += 2147483647;
+    return (1.0 / 2147483647) * r->seed;
+}
+
+/* RanPark::gaussian src/random_park.cpp:68-91 */
+static double park_gaussian(park_t *r)
+{
+    double first;
+    if (!r->save) {
+        double v1, v2, rsq;
+        int again = 1;
+        while (again) {
+            v1 = 2.0 * park_uniform(r) - 1.0;
+            v2 = 2.0 * park_uniform(r) - 1.0;
+            rsq = v1 * v1 + v2 * v2;
+            if (rsq < 1.0 && rsq != 0.0) again = 0;
+        }
+        double fac = sqrt(-2.0 * log(rsq) / rsq);
+        r->second = v1 * fac;
+        first = v2 * fac;
+        r->save = 1;
+    } else {
+        first = r->second;
+        r->save = 0;
+    }
+    return first;
+}
+
+struct ins_state {
+    orc_insert_pack p;
+    park_t rnd, rreg, rdist;
+    double distweight[8], tvol[8], tmass[8];
+    int distorder[8];
+    double volexpect, massexpect, maxrad, maxrbound;
+    double region_volume, region_volume_local, insertion_ratio;
+    long next_reneighbor, most_recent, ninserted;
+    double massinserted;
+    int props;
+};
+
+/* MathExtraLiggghts::isPrime-style check of Random::Random src/random.cpp:79-95 */
+static int seed_valid(int seed)
+{
+    if (seed < 10000) return 0;
+    for (int d = 2; (long)d * d <= seed; d++) if (seed % d == 0) return 0;
+    return 1;
+}
+
+/* RegBlock::inside src/region_block.cpp:147-152 */
+static int blk_inside(const orc_insert_pack *p, const double *x)
+{
+    return x[0] >= p->region_lo[0] && x[0] <= p->region_hi[0] && x[1] >= p->region_lo[1] && x[1] <= p->region_hi[1]
+        && x[2] >= p->region_lo[2] && x[2] <= p->region_hi[2];
+}
+
+/* RegBlock::surface_interior src/region_block.cpp:161-220 (contact count) */
+static int blk_surface_interior(const orc_insert_pack *p, const double *x, double cutoff)
+{
+    const double *lo = p->region_lo, *hi = p->region_hi;
+    if (x[0] < lo[0] || x[0] > hi[0] || x[1] < lo[1] || x[1] > hi[1] || x[2] < lo[2] || x[2] > hi[2]) return 0;
+    int n = 0;
+    for (int d = 0; d < 3; d++) {
+        if (x[d] - lo[d] < cutoff) n++;
+        if (hi[d] - x[d] < cutoff) n++;
+    }
+    return n;
+}
+
+/* RegBlock::surface_exterior src/region_block.cpp:228-259 with Region::add_contact src/region.cpp:248-257 */
+static int blk_surface_exterior(const orc_insert_pack *p, const double *x, double cutoff)
+{
+    const double *lo = p->region_lo, *hi = p->region_hi;
+    if (x[0] <= lo[0]-cutoff || x[0] >= hi[0]+cutoff || x[1] <= lo[1]-cutoff || x[1] >= hi[1]+cutoff ||
+        x[2] <= lo[2]-cutoff || x[2] >= hi[2]+cutoff) return 0;
+    if (x[0] > lo[0] && x[0] < hi[0] && x[1] > lo[1] && x[1] < hi[1] && x[2] > lo[2] && x[2] < hi[2]) return 0;
+    double xp, yp, zp;
+    if (x[0] < lo[0]) xp = lo[0]; else if (x[0] > hi[0]) xp = hi[0]; else xp = x[0];
+    if (x[1] < lo[1]) yp = lo[1]; else if (x[1] > hi[1]) yp = hi[1]; else yp = x[1];
+    if (x[2] < lo[2]) zp = lo[2]; else if (x[2] > hi[2]) zp = hi[2]; else zp = x[2];
+    double delx = x[0] - xp, dely = x[1] - yp, delz = x[2] - zp;
+    double r = sqrt(delx*delx + dely*dely + delz*delz);
+    return r < cutoff;
+}
+
+static void ins_max_rad(const struct ins_state *I, int type, double *mx)
+{
+    double m = 0.;
+    for (int i = 0; i < I->p.ntemplates; i++)
+        if (I->p.tmpl_type[i] == type && I->p.tmpl_radius[i] > m) m = I->p.tmpl_radius[i];
+    *mx = m;
+}
+
+int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p)
+{
+    if (s->ins) { fail(s, "one fix insert/pack"); return -1; }
+    if (!seed_valid(p->seed) || !seed_valid(p->dist_seed)) { fail(s, "seeds must be primes > 10000"); return -1; }
+    if (p->ntemplates < 1 || p->ntemplates > 8) { fail(s, "illegal number of templates"); return -1; }
+    int ndef = (p->volumefraction_region > 0.) + (p->particles_in_region > 0) + (p->mass_in_region > 0.);
+    if (ndef != 1) { fail(s, "exactly one insertion target"); return -1; }
+    struct ins_state *I = calloc(1, sizeof *I);
+    I->p = *p;
+    const int nt = p->ntemplates;
+    /* FixTemplateSphere: cubic_expectancy(radius)*4.*M_PI/3., density * volume (src/fix_template_sphere.cpp:244-245) */
+    for (int i = 0; i < nt; i++) {
+        double mu = p->tmpl_radius[i];
+        I->tvol[i] = mu*mu*mu*4.*M_PI/3.;
+        I->tmass[i] = p->tmpl_density[i] * I->tvol[i];
+        I->distweight[i] = p->tmpl_weight[i];
+    }
+    /* FixParticledistributionDiscrete constructor src/fix_particledistribution_discrete.cpp:130-220 */
+    double wsum = 0;
+    for (int i = 0; i < nt; i++) wsum += I->distweight[i];
+    for (int i = 0; i < nt; i++) I->distweight[i] /= wsum;
+    if (p->dist_mass_based) {
+        for (int i = 0; i < nt; i++) I->distweight[i] = I->distweight[i] / I->tmass[i];
+        wsum = 0;
+        for (int i = 0; i < nt; i++) wsum += I->distweight[i];
+        for (int i = 0; i < nt; i++) I->distweight[i] /= wsum;
+    }
+    I->volexpect = 0.; I->massexpect = 0.;
+    for (int i = 0; i < nt; i++) {
+        I->volexpect += I->tvol[i] * I->distweight[i];
+        I->massexpect += I->tmass[i] * I->distweight[i];
+    }
+    for (int i = 0; i < nt; i++) I->distorder[i] = i;
+    int swaped, n = nt;
+    do {
+        swaped = 0;
+        for (int i = 0; i < nt-1; i++)
+            if (I->tvol[I->distorder[i]] < I->tvol[I->distorder[i+1]]) {
+                int tmp = I->distorder[i]; I->distorder[i] = I->distorder[i+1]; I->distorder[i+1] = tmp;
+                swaped = 1;
+            }
+        n--;
+    } while (swaped && n > 0);
+    I->maxrbound = 0.;
+    for (int i = 0; i < nt; i++) if (p->tmpl_radius[i] > I->maxrbound) I->maxrbound = p->tmpl_radius[i];
+    I->maxrad = 0.;
+    for (int t = 1; t <= s->ntypes; t++) { double m; ins_max_rad(I, t, &m); if (m > I->maxrad) I->maxrad = m; }
+    I->rnd.seed = p->seed;
+    I->rdist.seed = p->dist_seed;
+    I->next_reneighbor = p->start > 0 ? p->start : s->ntimestep + 1;
+    I->most_recent = -1;
+    s->ins = I;
+    return 0;
+}
+
+static long ins_next(const struct ins_state *I) { return I->next_reneighbor; }
+
+/* state of the Park-Miller generator after n uniform() draws from seed */
+int orc_park_after(int seed, int n)
+{
+    park_t r = {seed, 0, 0.};
+    for (int i = 0; i < n; i++) park_uniform(&r);
+    return r.seed;
+}
+
+int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step)
+{
+    if (!s->ins) return -1;
+    *ninserted = s->ins->ninserted;
+    *massinserted = s->ins->massinserted;
+    *next_step = s->ins->next_reneighbor;
+    return 0;
+}
+
+/* FixInsertPack::calc_insertion_properties with Region::volume_mc src/region.cpp:634-703 */
+static void ins_setup(orc_sim *s)
+{
+    struct ins_state *I = s->ins;
+    if (I->props) return;
+    I->props = 1;
+    I->rreg.seed = I->p.seed + 12; I->rreg.save = 0;
+    const double *lo = I->p.region_lo, *hi = I->p.region_hi;
+    int n_in_global = 0, n_in_local = 0;
+    for (int i = 0; i < I->p.ntry_mc; i++) {
+        double pos[3];
+        pos[0] = lo[0] + park_uniform(&I->rreg) * (hi[0] - lo[0]);
+        pos[1] = lo[1] + park_uniform(&I->rreg) * (hi[1] - lo[1]);
+        pos[2] = lo[2] + park_uniform(&I->rreg) * (hi[2] - lo[2]);
+        int in_domain = pos[0] >= s->p.boxlo[0] && pos[0] <= s->p.boxhi[0] && pos[1] >= s->p.boxlo[1] &&
+                        pos[1] <= s->p.boxhi[1] && pos[2] >= s->p.boxlo[2] && pos[2] <= s->p.boxhi[2];
+        if (!in_domain) continue;
+        if (!I->p.all_in) {
+            if (blk_inside(&I->p, pos)) { n_in_global++; n_in_local++; }
+        } else {
+            if (blk_inside(&I->p, pos)) {
+                n_in_global++;
+                if (!blk_surface_interior(&I->p, pos, I->maxrbound)) n_in_local++;
+            }
+        }
+    }
+    if (n_in_global == 0) { fail(s, "Unable to calculate region volume"); return; }
+    double vol_bbox = (hi[0]-lo[0]) * (hi[1]-lo[1]) * (hi[2]-lo[2]);
+    double vol_global = (double)n_in_global / (double)(I->p.ntry_mc * 1) * vol_bbox;
+    double vol_local = (double)n_in_local / (double)I->p.ntry_mc * vol_bbox;
+    double vol_local_all = vol_local;
+    if (vol_local_all < 1.e-10) { fail(s, "Unable to calculate region volume"); return; }
+    vol_local *= (vol_global / vol_local_all);
+    I->region_volume = vol_global;
+    I->region_volume_local = vol_local;
+    if (I->region_volume <= 0. || I->region_volume_local < 0. ||
+        (I->region_volume_local - I->region_volume) / I->region_volume > 1e-3)
+        fail(s, "Fix insert: Region volume calculation with MC failed");
+}
+
+/* Region::generate_random(_shrinkby_cut) src/region.cpp:531-573, subdomain = box */
+static int ins_random_pos(orc_sim *s, struct ins_state *I, double rbound, double *pos)
+{
+    const orc_insert_pack *p = &I->p;
+    double lo[3], hi[3], diff[3];
+    for (int d = 0; d < 3; d++) {
+        lo[d] = p->region_lo[d] > s->p.boxlo[d] ? p->region_lo[d] : s->p.boxlo[d];
+        hi[d] = p->region_hi[d] < s->p.boxhi[d] ? p->region_hi[d] : s->p.boxhi[d];
+        diff[d] = hi[d] - lo[d];
+    }
+    if (p->all_in) {
+        for (int d = 0; d < 3; d++) if (p->region_hi[d] - p->region_lo[d] < 2.*rbound) return -1;
+        do {
+            pos[0] = lo[0] + park_uniform(&I->rreg)*diff[0];
+            pos[1] = lo[1] + park_uniform(&I->rreg)*diff[1];
+            pos[2] = lo[2] + park_uniform(&I->rreg)*diff[2];
+        } while (!blk_inside(p, pos) || blk_surface_interior(p, pos, rbound));
+    } else {
+        do {
+            pos[0] = lo[0] + park_uniform(&I->rreg)*diff[0];
+            pos[1] = lo[1] + park_uniform(&I->rreg)*diff[1];
+            pos[2] = lo[2] + park_uniform(&I->rreg)*diff[2];
+        } while (!blk_inside(p, pos));
+    }
+    return 0;
+}
+
+/* FixInsert::generate_random_velocity src/fix_insert.cpp:956-972 */
+static void ins_velocity(struct ins_state *I, double *v)
+{
+    const orc_insert_pack *p = &I->p;
+    v[0] = p->vel[0]; v[1] = p->vel[1]; v[2] = p->vel[2];
+    if (p->vel_style == 1) {
+        v[0] = p->vel[0] + p->vel_fluct[0] * 2.0 * (park_uniform(&I->rnd)-0.50);
+        v[1] = p->vel[1] + p->vel_fluct[1] * 2.0 * (park_uniform(&I->rnd)-0.50);
+        v[2] = p->vel[2] + p->vel_fluct[2] * 2.0 * (park_uniform(&I->rnd)-0.50);
+    } else if (p->vel_style == 2) {
+        v[0] = p->vel[0] + p->vel_fluct[0] * park_gaussian(&I->rnd);
+        v[1] = p->vel[1] + p->vel_fluct[1] * park_gaussian(&I->rnd);
+        v[2] = p->vel[2] + p->vel_fluct[2] * park_gaussian(&I->rnd);
+    }
+}
+
+/* Domain::dist_subbox_borders src/domain_I.h:126-142 (subdomain = box) */
+static double ins_dist_borders(orc_sim *s, const double *pos)
+{
+    double dl[3], dh[3];
+    for (int d = 0; d < 3; d++) { dl[d] = fabs(s->p.boxlo[d] - pos[d]); dh[d] = fabs(s->p.boxhi[d] - pos[d]); }
+    double dlo = dl[0], dhi = dh[0];
+    for (int d = 1; d < 3; d++) { if (dl[d] < dlo) dlo = dl[d]; if (dh[d] < dhi) dhi = dh[d]; }
+    return dlo < dhi ? dlo : dhi;
+}
+
+/* FixInsert::pre_exchange src/fix_insert.cpp:652-827 for fix insert/pack on
+   one process; appends the new atoms after the owned ones (over the first
+   ghost slots, as Atom::avec->create_atom does) with tags from tag_extend */
+static void ins_pre_exchange(orc_sim *s)
+{
+    struct ins_state *I = s->ins;
+    const orc_insert_pack *p = &I->p;
+    if (I->next_reneighbor != s->ntimestep || I->most_recent == s->ntimestep) return;
+    I->most_recent = s->ntimestep;
+    /* FixInsertPack::calc_ninsert_this src/fix_insert_pack.cpp:254-351 */
+    int np_region = 0;
+    double vol_region = 0., mass_region = 0.;
+    double _4Pi3 = 4.*M_PI/3.;
+    for (int i = 0; i < s->nlocal; i++)
+        if (blk_inside(p, &s->x[3*i])) {
+            np_region++;
+            vol_region += _4Pi3*s->radius[i]*s->radius[i]*s->radius[i];
+            mass_region += s->rmass[i];
+        }
+    int ninsert_this;
+    if (p->volumefraction_region > 0.) {
+        ninsert_this = (int)((p->volumefraction_region*I->region_volume - vol_region) / I->volexpect + park_uniform(&I->rnd));
+        I->insertion_ratio = vol_region / (p->volumefraction_region*I->region_volume);
+    } else if (p->particles_in_region > 0) {
+        ninsert_this = p->particles_in_region - np_region;
+        I->insertion_ratio = (double)np_region / (double)p->particles_in_region;
+    } else {
+        ninsert_this = (int)((p->mass_in_region - mass_region) / I->massexpect + park_uniform(&I->rnd));
+        I->insertion_ratio = mass_region / p->mass_in_region;
+    }
+    if (ninsert_this < 0) ninsert_this = 0;
+    if (I->insertion_ratio < 0.) I->insertion_ratio = 0.;
+    if (I->insertion_ratio > 1.) I->insertion_ratio = 1.;
+    /* distribute_ninsert_this src/fix_insert.cpp:829-914, nprocs = 1 */
+    double fraction_local = I->region_volume_local / I->region_volume;
+    int nloc;
+    if (!p->exact_number) nloc = (int)(fraction_local*(double)ninsert_this + park_uniform(&I->rnd));
+    else {
+        double fr = fraction_local;
+        if (fr < 0.02 / 1.) fr = 0.;
+        double sum = 0. + fr;
+        if (sum == 0.) { fail(s, "Internal error distributing particles to processes"); return; }
+        fr /= sum;
+        nloc = (int)(fr*(double)ninsert_this);
+        double rem = fr*(double)ninsert_this - nloc;
+        int ngap = (int)round(rem);
+        for (int g = 0; g < ngap; g++) { park_uniform(&I->rnd); nloc++; }
+    }
+    /* randomize_list src/fix_particledistribution_discrete.cpp:398-480 */
+    const int nt = p->ntemplates;
+    int parttogen[8];
+    if (!p->exact_number) {
+        for (int i = 0; i < nt; i++) parttogen[i] = (int)((double)nloc*I->distweight[i] + park_uniform(&I->rdist));
+    } else {
+        int ntrunc = 0; double remainder[8];
+        for (int i = 0; i < nt; i++) {
+            parttogen[i] = (int)((double)nloc*I->distweight[i]);
+            ntrunc += parttogen[i];
+            remainder[i] = (double)nloc*I->distweight[i] - (double)parttogen[i];
+        }
+        int gap = nloc - ntrunc;
+        for (int i = 0; i < gap; i++) {
+            double r = park_uniform(&I->rdist) * (double)gap;
+            int j = 0; double rsum = remainder[0];
+            while (rsum < r && j < nt-1) { j++; rsum += remainder[j]; }
+            parttogen[j]++;
+        }
+    }
+    int ntot = 0;
+    for (int i = 0; i < nt; i++) ntot += parttogen[i];
+    if (ntot == 0) {
+        if (p->insert_every) I->next_reneighbor += p->insert_every;
+        else I->next_reneighbor = -1;
+        return;
+    }
+    int *plist = malloc(sizeof(int)*ntot), q = 0;
+    for (int i = 0; i < nt; i++) for (int j = 0; j < parttogen[I->distorder[i]]; j++) plist[q++] = I->distorder[i];
+    /* load_xnear src/fix_insert.cpp:916-954: owned and ghost atoms near the region, within getBoundingBox */
+    const int nall = s->nlocal + s->nghost;
+    double *near = malloc(sizeof(double)*4*(nall + ntot + 1));
+    int nnear = 0;
+    if (p->overlapcheck) {
+        double blo[3], bhi[3];
+        for (int d = 0; d < 3; d++) {
+            blo[d] = p->region_lo[d]; bhi[d] = p->region_hi[d];
+            if (blo[d] < s->p.boxlo[d]) blo[d] = s->p.boxlo[d];
+            if (bhi[d] > s->p.boxhi[d]) bhi[d] = s->p.boxhi[d];
+            blo[d] = blo[d] - (2*I->maxrad + 0.);
+            bhi[d] = bhi[d] + (2*I->maxrad + 0.);
+        }
+        for (int i = 0; i < nall; i++) {
+            const double *xi = &s->x[3*i];
+            double cut = p->all_in ? I->maxrad : s->radius[i] + I->maxrad;
+            int nearby = blk_inside(p, xi) || blk_surface_exterior(p, xi, cut);
+            int inbb = xi[0] >= blo[0] && xi[0] <= bhi[0] && xi[1] >= blo[1] && xi[1] <= bhi[1] && xi[2] >= blo[2] && xi[2] <= bhi[2];
+            if (nearby && inbb) {
+                near[4*nnear] = xi[0]; near[4*nnear+1] = xi[1]; near[4*nnear+2] = xi[2]; near[4*nnear+3] = s->radius[i];
+                nnear++;
+            }
+        }
+    }
+    /* x_v_omega src/fix_insert_pack.cpp:415-514 */
+    double *nx = malloc(sizeof(double)*9*ntot);
+    int *nty = malloc(sizeof(int)*ntot);
+    double *nr = malloc(sizeof(double)*ntot), *nm = malloc(sizeof(double)*ntot);
+    int done = 0, ntry = 0;
+    int maxtry = I->insertion_ratio >= 1. ? ntot*p->maxattempt : (int)((double)(ntot*p->maxattempt) / (1.-I->insertion_ratio));
+    double mass_this = 0.;
+    while (done < ntot && (!p->overlapcheck || ntry < maxtry)) {
+        int t = plist[done];
+        double rb = p->tmpl_radius[t];
+        double pos[3], v[3];
+        int ok = 0;
+        if (!p->overlapcheck) {
+            if (ins_random_pos(s, I, rb, pos)) { fail(s, "region too small"); break; }
+            ins_velocity(I, v);
+            if (pos[0] == 0. && pos[1] == 0. && pos[2] == 0.) { fail(s, "illegal position"); break; }
+            ok = 1;
+        } else {
+            while (!ok && ntry < maxtry) {
+                do {
+                    if (ins_random_pos(s, I, rb, pos)) { fail(s, "region too small"); goto out; }
+                    ntry++;
+                } while (p->check_dist_from_subdomain_border && ntry < maxtry && ins_dist_borders(s, pos) < rb);
+                if (ntry == maxtry) break;
+                ins_velocity(I, v);
+                int hit = 0;
+                for (int k = 0; k < nnear && !hit; k++) {
+                    double del[3] = {pos[0]-near[4*k], pos[1]-near[4*k+1], pos[2]-near[4*k+2]};
+                    double rsq = del[0]*del[0] + del[1]*del[1] + del[2]*del[2];
+                    double radsum = rb + near[4*k+3];
+                    if (rsq <= radsum*radsum) hit = 1;
+                }
+                if (!hit) {
+                    near[4*nnear] = pos[0]; near[4*nnear+1] = pos[1]; near[4*nnear+2] = pos[2]; near[4*nnear+3] = rb;
+                    nnear++;
+                    ok = 1;
+                }
+            }
+        }
+        if (!ok) break;
+        for (int d = 0; d < 3; d++) { nx[9*done+d] = pos[d]; nx[9*done+3+d] = v[d]; nx[9*done+6+d] = p->omega[d]; }
+        nty[done] = p->tmpl_type[t];
+        nr[done] = rb;
+        nm[done] = p->tmpl_density[t] * (rb*rb*rb*4.*M_PI/3.);
+        mass_this += nm[done];
+        done++;
+    }
+out:
+    if (!s->err[0] && done > 0) {
+        /* ParticleToInsert::insert src/particleToInsert.cpp:101-158 and Atom::tag_extend */
+        int maxtag = 0;
+        for (int i = 0; i < s->nlocal; i++) if (s->tag[i] > maxtag) maxtag = s->tag[i];
+        const int nl = s->nlocal;
+        if (nl + done > s->nmax) grow_all(s, 2*(nl + done) + 64);
+        for (int k = 0; k < done; k++) {
+            int m = nl + k;
+            memcpy(&s->x[3*m], &nx[9*k], sizeof(double)*3);
+            memcpy(&s->v[3*m], &nx[9*k+3], sizeof(double)*3);
+            memcpy(&s->omega[3*m], &nx[9*k+6], sizeof(double)*3);
+            s->radius[m] = nr[k]; s->rmass[m] = nm[k]; s->type[m] = nty[k];
+            s->tag[m] = maxtag + 1 + k;
+            s->f[3*m] = s->f[3*m+1] = s->f[3*m+2] = 0.;
+            s->torque[3*m] = s->torque[3*m+1] = s->torque[3*m+2] = 0.;
+            free(s->partner[m]); free(s->phist[m]); s->partner[m] = NULL; s->phist[m] = NULL; s->npartner[m] = 0;
+            for (int f = 0; f < s->nfix; f++) {
+                if (s->fix[f].wp) { double *h = s->fix[f].wp->hist; h[3*m] = h[3*m+1] = h[3*m+2] = 0.; }
+                if (s->fix[f].wm) {
+                    wall_mesh *wm = s->fix[f].wm;
+                    wm->nneighs[m] = 0; wm->npartner[m] = 0;
+                    free(wm->partner[m]); free(wm->chist[m]); free(wm->keep[m]); free(wm->isect[m]);
+                    wm->partner[m] = NULL; wm->chist[m] = NULL; wm->keep[m] = NULL; wm->isect[m] = NULL;
+                }
+            }
+        }
+        s->nlocal = nl + done;
+        s->nstart = xrealloc(s->nstart, sizeof(int)*s->nlocal);
+        s->nnum = xrealloc(s->nnum, sizeof(int)*s->nlocal);
+        for (int k = nl; k < s->nlocal; k++) { s->nstart[k] = 0; s->nnum[k] = 0; }
+        I->ninserted += done;
+        I->massinserted += mass_this;
+    }
+    free(plist); free(near); free(nx); free(nty); free(nr); free(nm);
+    if (s->err[0]) return;
+    if (p->insert_every) I->next_reneighbor += p->insert_every;
+    else I->next_reneighbor = 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Verlet::setup src/verlet.cpp:134-197                                 */
 
 int orc_setup(orc_sim *s)
@@ -1973,6 +2438,7 @@ int orc_setup(orc_sim *s)
     pre_force_all(s, 1);
     pair_compute(s, 0);
     post_force_all(s, 0);
+    if (s->ins) ins_setup(s);   /* FixInsert::setup */
     s->setupflag = 0;
     return s->err[0] ? -1 : 0;
 }
@@ -1992,6 +2458,7 @@ int orc_run(orc_sim *s, int nsteps)
         int nflag = neighbor_decide(s);
         if (nflag == 0) comm_forward(s);
         else {
+            if (s->ins) { ins_pre_exchange(s); if (s->err[0]) return -1; }   /* fix insert precedes the history fix */
             history_pre_exchange(s);
             for (int k = 0; k < s->nfix; k++) if (s->fix[k].wm) mesh_sort_contacts(s, s->fix[k].wm);
             domain_pbc(s);

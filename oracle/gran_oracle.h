@@ -91,6 +91,28 @@ void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega,
                    double *f, double *torque, int *tag);
 /* half-list pairs: returns count; arrays may be NULL to query count */
 int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist);
+/* fix insert/pack over a region block + particledistribution/discrete of
+   particletemplate/sphere templates with constant radius and density
+   (src/fix_insert.cpp, src/fix_insert_pack.cpp,
+   src/fix_particledistribution_discrete.cpp, src/fix_template_sphere.cpp).
+   Field layout identical to the library's gb2_insert_pack. */
+typedef struct {
+    int seed;
+    double region_lo[3], region_hi[3];
+    double volumefraction_region;
+    int particles_in_region;
+    double mass_in_region;
+    int insert_every, start, maxattempt, overlapcheck, all_in, exact_number, vel_style;
+    double vel[3], vel_fluct[3], omega[3];
+    int ntry_mc, check_dist_from_subdomain_border;
+    int dist_seed, dist_mass_based, ntemplates;
+    int tmpl_type[8];
+    double tmpl_radius[8], tmpl_density[8], tmpl_weight[8];
+    int max_atoms;
+} orc_insert_pack;
+int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p);
+int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step);
+int orc_park_after(int seed, int n);
 /* compute pair/gran/local: rows of the columns keys selects (bit b of keys:
    pos, vel, id, force, force_normal, force_tangential, torque, torque_normal,
    torque_tangential, history, contactArea, delta, contactPoint) */

@@ -78,6 +78,10 @@ def lib():
         L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_park_after.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.orc_add_insert_pack.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrcInsertPack)]
+        L.orc_insert_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), D,
+                                       ctypes.POINTER(ctypes.c_long)]
         L.orc_pair_gran_local.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int, D]
         L.orc_get_history.argtypes = [ctypes.c_void_p, I, I, D]
         L.orc_upload_wall_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D]
@@ -97,6 +101,51 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(I)
+
+
+class OrcInsertPack(ctypes.Structure):
+    """orc_insert_pack (fix insert/pack with its distribution and templates)."""
+    _fields_ = [("seed", ctypes.c_int), ("region_lo", ctypes.c_double * 3), ("region_hi", ctypes.c_double * 3),
+                ("volumefraction_region", ctypes.c_double), ("particles_in_region", ctypes.c_int),
+                ("mass_in_region", ctypes.c_double), ("insert_every", ctypes.c_int), ("start", ctypes.c_int),
+                ("maxattempt", ctypes.c_int), ("overlapcheck", ctypes.c_int), ("all_in", ctypes.c_int),
+                ("exact_number", ctypes.c_int), ("vel_style", ctypes.c_int), ("vel", ctypes.c_double * 3),
+                ("vel_fluct", ctypes.c_double * 3), ("omega", ctypes.c_double * 3), ("ntry_mc", ctypes.c_int),
+                ("check_dist_from_subdomain_border", ctypes.c_int), ("dist_seed", ctypes.c_int),
+                ("dist_mass_based", ctypes.c_int), ("ntemplates", ctypes.c_int), ("tmpl_type", ctypes.c_int * 8),
+                ("tmpl_radius", ctypes.c_double * 8), ("tmpl_density", ctypes.c_double * 8),
+                ("tmpl_weight", ctypes.c_double * 8), ("max_atoms", ctypes.c_int)]
+
+
+def make_insert(fx):
+    """OrcInsertPack from a scenario fix dict (kind "insert_pack"), keyword defaults as the reference's."""
+    p = OrcInsertPack()
+    p.seed = int(fx["seed"])
+    for d in range(3):
+        p.region_lo[d], p.region_hi[d] = fx["region_lo"][d], fx["region_hi"][d]
+        p.vel[d] = fx.get("vel", (0.0, 0.0, 0.0))[d]
+        p.vel_fluct[d] = fx.get("vel_fluct", (0.0, 0.0, 0.0))[d]
+        p.omega[d] = fx.get("omega", (0.0, 0.0, 0.0))[d]
+    p.volumefraction_region = float(fx.get("volumefraction_region", 0.0))
+    p.particles_in_region = int(fx.get("particles_in_region", 0))
+    p.mass_in_region = float(fx.get("mass_in_region", 0.0))
+    p.insert_every = int(fx["insert_every"])
+    p.start = int(fx.get("start", 0))
+    p.maxattempt = int(fx.get("maxattempt", 50))
+    p.overlapcheck = int(fx.get("overlapcheck", 1))
+    p.all_in = int(fx.get("all_in", 0))
+    p.exact_number = int(fx.get("exact_number", 1))
+    p.vel_style = {"constant": 0, "uniform": 1, "gaussian": 2}[fx.get("vel_style", "constant")]
+    p.ntry_mc = int(fx.get("ntry_mc", 100000))
+    p.check_dist_from_subdomain_border = int(fx.get("check_dist_from_subdomain_border", 1))
+    p.dist_seed = int(fx["dist_seed"])
+    p.dist_mass_based = int(fx.get("dist_mass_based", 1))
+    p.ntemplates = len(fx["templates"])
+    for i, t in enumerate(fx["templates"]):
+        p.tmpl_type[i], p.tmpl_radius[i] = int(t["type"]), float(t["radius"])
+        p.tmpl_density[i], p.tmpl_weight[i] = float(t["density"]), float(t["weight"])
+    p.max_atoms = int(fx.get("max_atoms", 0))
+    return p
 
 
 def make_params(sc):
@@ -166,6 +215,12 @@ class Oracle:
                     raise ValueError("oracle: bad move_mesh_linear")
             elif kind == "nve_sphere":
                 k = None   # the oracle always integrates with fix nve/sphere
+            elif kind == "insert_pack":
+                ip = make_insert(fx)
+                self._keep.append(ip)
+                if L.orc_add_insert_pack(self.h, ctypes.byref(ip)) != 0:
+                    raise ValueError("oracle: " + L.orc_error(self.h).decode())
+                k = 0
             else:
                 raise ValueError(kind)
             self.fix_ids.append(k)
@@ -207,6 +262,12 @@ class Oracle:
                              _dp(out["torque"]), _ip(tag))
         out["tag"] = tag
         return out
+
+    def insert_stats(self):
+        n, nxt, m = ctypes.c_long(), ctypes.c_long(), np.zeros(1)
+        if self.L.orc_insert_stats(self.h, ctypes.byref(n), _dp(m), ctypes.byref(nxt)) != 0:
+            raise ValueError("no fix insert/pack")
+        return {"ninserted": n.value, "massinserted": float(m[0]), "next_step": nxt.value}
 
     def pair_gran_local(self, keys=0x4 | 0x8 | 0x40 | 0x200):
         """compute pair/gran/local: (nrows, ncols) for a keyword bit mask

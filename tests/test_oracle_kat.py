@@ -216,3 +216,53 @@ def test_pair_gran_local_keywords_periodic_pair():
     assert row[38] == pytest.approx(1.0001, rel=1e-12) and np.array_equal(row[39:41], [0.5, 0.5])
     # the default id force torque history columns are the same numbers
     assert np.array_equal(o.pair_gran_local(), row[np.r_[12:18, 24:27, 33:36]][None, :])
+
+
+def test_park_miller_minimal_standard():
+    # Park & Miller (1988): from seed 1 the 10,000th state is 1043618065
+    assert oracle.lib().orc_park_after(1, 10000) == 1043618065
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(periodic=False, vel_style="constant", all_in=1),
+                                dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian")])
+def test_insert_pack_places_non_overlapping_particles(kw):
+    # fix insert/pack at the first step: the new particles lie in the region
+    # (all_in: a radius away from its faces), overlap neither each other nor
+    # the bed, follow the templates, and get tags after the bed's
+    sc = S.insert_pour(**kw)
+    n_bed = len(sc["atoms"]["tag"])
+    fx = [f for f in sc["fixes"] if f["kind"] == "insert_pack"][0]
+    o = oracle.Oracle(sc)
+    o.setup()
+    o.run(1)
+    a = o.atoms()
+    st = o.insert_stats()
+    new = a["tag"] > n_bed
+    k = int(new.sum())
+    assert k == st["ninserted"] > 50 and st["next_step"] == 1 + fx["insert_every"]
+    assert np.array_equal(np.sort(a["tag"][new]), np.arange(n_bed + 1, n_bed + k + 1))
+    if "particles_in_region" in fx:
+        # random_distribute uncorrelated draws each template's count
+        slack = 0 if fx["exact_number"] else len(fx["templates"])
+        assert abs(k - fx["particles_in_region"]) <= slack
+    x = a["x"]
+    rad = np.array(sorted({t["radius"] for t in fx["templates"]}))
+    # radii from the masses (rmass = density * 4/3 pi r^3)
+    lo, hi = np.array(fx["region_lo"]), np.array(fx["region_hi"])
+    xn = x[new]
+    assert np.all((xn >= lo) & (xn <= hi))
+    vz = a["v"][new][:, 2]
+    if kw.get("vel_style", "uniform") == "uniform":
+        assert np.all(np.abs(a["v"][new] - [0, 0, -0.5]) <= 0.1 + 1e-9)
+    elif kw.get("vel_style") == "constant":
+        assert np.all(vz < 0)
+    # gaps: new-new at least two of the smaller template radius, new-bed at
+    # least that radius plus the bed's 1 mm (the bed has not moved since)
+    d = np.linalg.norm(xn[:, None, :] - xn[None, :, :], axis=2)
+    np.fill_diagonal(d, np.inf)
+    assert d.min() > 2 * rad.min()
+    db = np.linalg.norm(xn[:, None, :] - x[~new][None, :, :], axis=2)
+    assert db.min() > rad.min() + 1e-3
+    if fx.get("all_in"):
+        gap = np.minimum(xn - lo, hi - xn).min(axis=1)
+        assert np.all(gap >= rad.min())

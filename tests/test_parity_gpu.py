@@ -297,3 +297,28 @@ def test_mesh_surface_stress():
         hits += int((np.abs(b["tri_f"]).sum(axis=1) > 0).sum())
     assert hits > 0, "the piston carried no force"
     assert b["f_total"][2] > 0, "particles should push the piston up"
+
+
+@pytest.mark.parametrize("kw", [dict(insert_every=250),
+                                dict(periodic=False, vel_style="constant", all_in=1),
+                                dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian",
+                                     insert_every=200)])
+def test_insert_pack(kw):
+    """fix insert/pack refilling a region block above a bed (periodic x/y with
+    ghosts near the region, or walled; vel uniform / constant / gaussian;
+    volume-fraction or count target; insertion steps at run starts and in
+    the middle of a run): the same particles appear at the same steps with
+    the same tags, and every state stays bit for bit equal to the oracle."""
+    sc = S.insert_pour(**kw)
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    n0 = len(sc["atoms"]["tag"])
+    for _ in range(4):
+        e.run(300)
+        o.run(300)
+        assert e.insert_stats() == o.insert_stats()
+        assert_atoms_equal(e, o)
+        assert_pairs_equal(e, o)
+    assert o.insert_stats()["ninserted"] > 100 and o.nlocal > n0
+    assert e.stats()["nbuilds"] == o.nbuilds

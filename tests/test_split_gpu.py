@@ -201,3 +201,26 @@ def test_split_pour_statistics():
     assert abs(a[0] - b[0]) <= 0.01 * a[0]
     assert abs(a[1] - b[1]) <= 0.01 * a[1]
     assert np.abs(ha - hb).max() <= 0.01
+
+
+def test_split_insert_pack():
+    """fix insert/pack in split precision: insertion draws on the FP64 state,
+    so the first insertion (before any step integrates) places exactly the
+    FP64 path's particles; later ones follow the slightly different fill
+    level of the region."""
+    sc = S.insert_pour(insert_every=200)
+    a, b = _engine(sc, True), _engine(sc, False)
+    a.setup()
+    b.setup()
+    a.run(1)
+    b.run(1)
+    assert a.insert_stats() == b.insert_stats()
+    xa, xb = by_tag(a.atoms()), by_tag(b.atoms())
+    assert np.array_equal(xa["tag"], xb["tag"])
+    new = xa["tag"] > len(sc["atoms"]["tag"])
+    assert np.array_equal(xa["x"][new], xb["x"][new])
+    a.run(600)
+    b.run(600)
+    sa, sb = a.insert_stats(), b.insert_stats()
+    assert sa["next_step"] == sb["next_step"] == 801
+    assert abs(sa["ninserted"] - sb["ninserted"]) <= 0.05 * sb["ninserted"]
