@@ -277,6 +277,19 @@ int gb2_contact_atom(gb2_ctx *ctx, int cap, int *n, int *tag, double *contact);
 int gb2_download_wall_history(gb2_ctx *ctx, int ifix, int cap, double *hist);
 /* occupied mesh-contact slots of mesh fix ifix: (atom tag, triangle id, shear[3]) */
 int gb2_download_mesh_contacts(gb2_ctx *ctx, int ifix, int cap, int *n, int *tag, int *tri, double *hist);
+/* mesh contact history in the restart layout (FixContactHistoryMesh::
+ * write_restart's sort_contacts, src/fix_contact_history_mesh.cpp:375-405
+ * and :653-658, then FixContactHistory::pack_restart,
+ * src/fix_contact_history.cpp:588-604): per owned atom (current order, with
+ * its tag) the partner count; per partner, concatenated over atoms, the
+ * triangle id and its 3 shear values.  The slot sort happens in place, as
+ * in the reference.  Caps too small: only *n and *ntotal. */
+int gb2_download_mesh_history(gb2_ctx *ctx, int ifix, int cap_atoms, int cap_entries, int *n, int *ntotal,
+                              int *tag, int *npartner, int *tri, double *hist);
+/* FixContactHistoryMesh::unpack_restart (src/fix_contact_history_mesh.cpp:
+ * 613-650): after gb2_upload_atoms (same atom order), before gb2_setup */
+int gb2_upload_mesh_history(gb2_ctx *ctx, int ifix, int n, const int *npartner, const int *tri,
+                            const double *hist);
 /* mesh topology after load: per triangle edge/corner active flags and obtuse index */
 int gb2_mesh_topology(gb2_ctx *ctx, int ifix, int cap, int *ntri, unsigned char *edge_active,
                       unsigned char *corner_active, int *obtuse);

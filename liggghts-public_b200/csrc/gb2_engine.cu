@@ -2359,6 +2359,99 @@ int gb2_download_mesh_contacts(gb2_ctx *c, int ifix, int cap, int *n, int *tag, 
     return 0;
 }
 
+// restart layout of the mesh contact history (FixContactHistoryMesh::
+// write_restart sorts the slots first, then FixContactHistory::pack_restart):
+// per owned atom its partner count, then per partner the triangle id and 3
+// shear values.  The sort runs in place, as in the reference.
+int gb2_download_mesh_history(gb2_ctx *c, int ifix, int cap_atoms, int cap_entries, int *n, int *ntotal, int *tag,
+                              int *npartner, int *tri, double *hist)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH) return GB2_ERR_ARG;
+    if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "no mesh contact history before setup");
+    MeshFix &M = *c->fix[ifix].mesh;
+    const size_t cp = c->cap;
+    const int nl = c->nlocal;
+    if (nl > 0) {
+        Dev D = make_dev(c);
+        k_mesh_sort_contacts<<<nblk(nl), kBlock, 0, c->st>>>(D, ifix);
+        CKL();
+    }
+    std::vector<int> np(nl), tg(nl);
+    CK(cudaMemcpyAsync(np.data(), M.snp.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(tg.data(), c->tag.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    long total = 0;
+    for (int i = 0; i < nl; i++) total += np[i];
+    if (n) *n = nl;
+    if (ntotal) *ntotal = (int)total;
+    if (tag && npartner && cap_atoms >= nl)
+        for (int i = 0; i < nl; i++) {
+            tag[i] = tg[i];
+            npartner[i] = np[i];
+        }
+    if (!tri || !hist || cap_entries < total || total == 0) return 0;
+    std::vector<int> sp((size_t)M.maxt * cp);
+    std::vector<double> h((size_t)3 * M.maxt * cp);
+    CK(cudaMemcpyAsync(sp.data(), M.spartner.p, sizeof(int) * sp.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(h.data(), M.shist.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    long k = 0;
+    for (int i = 0; i < nl; i++)
+        for (int s2 = 0; s2 < np[i]; s2++, k++) {
+            tri[k] = sp[(size_t)s2 * cp + i];
+            for (int q = 0; q < 3; q++) hist[3 * k + q] = h[(size_t)(3 * s2 + q) * cp + i];
+        }
+    return 0;
+}
+
+// FixContactHistoryMesh::unpack_restart (src/fix_contact_history_mesh.cpp:
+// 613-650): the partner triangles and shear of each uploaded atom, in the
+// uploaded order (before setup; the setup's mesh list keeps the partners
+// that are still candidates, as setup_pre_force does after read_restart)
+int gb2_upload_mesh_history(gb2_ctx *c, int ifix, int n, const int *npartner, const int *tri, const double *hist)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !npartner) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "mesh contact history is uploaded before setup");
+    if (n != c->nlocal) return set_err(c, GB2_ERR_ARG, "mesh history for %d atoms, %d uploaded", n, c->nlocal);
+    MeshFix &M = *c->fix[ifix].mesh;
+    const int ntri = (int)M.topo.tri.size();
+    int maxnp = 0;
+    long total = 0;
+    for (int i = 0; i < n; i++) {
+        if (npartner[i] < 0 || npartner[i] > 64)
+            return set_err(c, GB2_ERR_ARG, "atom %d: %d mesh partners (0..64)", i, npartner[i]);
+        maxnp = std::max(maxnp, npartner[i]);
+        total += npartner[i];
+    }
+    if (total > 0 && (!tri || !hist)) return GB2_ERR_ARG;
+    for (long k = 0; k < total; k++)
+        if (tri[k] < 0 || tri[k] >= ntri) return set_err(c, GB2_ERR_ARG, "mesh partner %d out of range", tri[k]);
+    const size_t cp = c->cap;
+    if (maxnp > M.maxt) {
+        M.maxt = maxnp;
+        CK(M.spartner.alloc((size_t)M.maxt * cp));
+        CK(M.shist.alloc((size_t)3 * M.maxt * cp));
+        CK(M.tlist.alloc((size_t)M.maxt * cp));
+    }
+    std::vector<int> sp((size_t)M.maxt * cp, -1), np(cp, 0);
+    std::vector<double> h((size_t)3 * M.maxt * cp, 0.0);
+    long k = 0;
+    for (int i = 0; i < n; i++) {
+        np[i] = npartner[i];
+        for (int s2 = 0; s2 < npartner[i]; s2++, k++) {
+            sp[(size_t)s2 * cp + i] = tri[k];
+            for (int q = 0; q < 3; q++) h[(size_t)(3 * s2 + q) * cp + i] = hist[3 * k + q];
+        }
+    }
+    CK(cudaMemcpyAsync(M.spartner.p, sp.data(), sizeof(int) * sp.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(M.shist.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(M.snp.p, np.data(), sizeof(int) * cp, cudaMemcpyHostToDevice, c->st));
+    // the slot count the setup's sort walks: the unpacked partners
+    CK(cudaMemcpyAsync(M.tcnt.p, np.data(), sizeof(int) * cp, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
 int gb2_mesh_topology(gb2_ctx *c, int ifix, int cap, int *ntri, unsigned char *edge_active,
                       unsigned char *corner_active, int *obtuse)
 {

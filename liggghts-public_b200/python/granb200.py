@@ -31,7 +31,8 @@ EXPORTS = (
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
-    "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats",
+    "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
+    "gb2_upload_mesh_history",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -220,6 +221,8 @@ def lib(path=LIB_PATH):
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
         L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
+        L.gb2_download_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, I, I, I, I, I, D]
+        L.gb2_upload_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, D]
         L.gb2_add_insert_pack.argtypes = [vp, ctypes.POINTER(InsertPackParams)]
         L.gb2_insert_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long), D,
                                        ctypes.POINTER(ctypes.c_long)]
@@ -512,6 +515,27 @@ class Engine:
         h = np.zeros((n, 3))
         self._check(self.L.gb2_download_mesh_contacts(self.h, k, n, ctypes.byref(cnt), _ip(tag), _ip(tri), _dp(h)))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_history(self, ifix):
+        """Mesh contact history in the restart layout: {tag, npartner, tri, hist}."""
+        k = self.fix_ids[ifix]
+        n, tot = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.gb2_download_mesh_history(self.h, k, 0, 0, ctypes.byref(n), ctypes.byref(tot), None, None,
+                                                     None, None))
+        tag = np.zeros(n.value, dtype=np.int32)
+        npart = np.zeros(n.value, dtype=np.int32)
+        tri = np.zeros(tot.value, dtype=np.int32)
+        h = np.zeros((tot.value, 3))
+        self._check(self.L.gb2_download_mesh_history(self.h, k, n.value, tot.value, ctypes.byref(n), ctypes.byref(tot),
+                                                     _ip(tag), _ip(npart), _ip(tri), _dp(h)))
+        return {"tag": tag, "npartner": npart, "tri": tri, "hist": h}
+
+    def upload_mesh_hist(self, ifix, npartner, tri, hist):
+        """Mesh contact history of the uploaded atoms (restart layout), before setup."""
+        npart = np.ascontiguousarray(npartner, dtype=np.int32)
+        t = np.ascontiguousarray(tri, dtype=np.int32)
+        h = np.ascontiguousarray(hist, dtype=np.float64).reshape(-1)
+        self._check(self.L.gb2_upload_mesh_history(self.h, self.fix_ids[ifix], len(npart), _ip(npart), _ip(t), _dp(h)))
 
     def mesh_nodes(self, ifix):
         """Current nodes (ntri, 3, 3) and node velocities of the mesh of fix ifix."""

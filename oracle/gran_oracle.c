@@ -2755,6 +2755,50 @@ int orc_get_wall_hist(orc_sim *s, int ifix, double *hist)
     return s->nlocal;
 }
 
+/* FixContactHistoryMesh::write_restart (sort_contacts, src/fix_contact_history_mesh.cpp:
+   375-405, 653-658) then FixContactHistory::pack_restart (src/fix_contact_history.cpp:
+   588-604): per owned atom its partner count, per partner the triangle id and 3 shear
+   values.  Returns the partner total; npartner / tri / hist may be NULL. */
+int orc_get_mesh_history(orc_sim *s, int ifix, int cap, int *npartner, int *tri, double *hist)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    mesh_sort_contacts(s, m);
+    int k = 0;
+    for (int i = 0; i < s->nlocal; i++) {
+        if (npartner) npartner[i] = m->npartner[i];
+        for (int q = 0; q < m->npartner[i]; q++, k++)
+            if (k < cap) {
+                if (tri) tri[k] = m->partner[i][q];
+                if (hist) memcpy(&hist[3*k], &m->chist[i][3*q], sizeof(double)*3);
+            }
+    }
+    return k;
+}
+
+/* FixContactHistoryMesh::unpack_restart src/fix_contact_history_mesh.cpp:613-650 */
+int orc_upload_mesh_hist(orc_sim *s, int ifix, int n, const int *npartner, const int *tri, const double *hist)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm || n != s->nlocal) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    int k = 0;
+    for (int i = 0; i < n; i++) {
+        int np = npartner[i];
+        free(m->partner[i]); free(m->chist[i]); free(m->keep[i]); free(m->isect[i]);
+        m->partner[i] = malloc(sizeof(int)*(np > 0 ? np : 1));
+        m->chist[i] = calloc((size_t)3*(np > 0 ? np : 1), sizeof(double));
+        m->keep[i] = calloc(np > 0 ? np : 1, 1);
+        m->isect[i] = calloc(np > 0 ? np : 1, 1);
+        for (int q = 0; q < np; q++, k++) {
+            m->partner[i][q] = tri[k];
+            memcpy(&m->chist[i][3*q], &hist[3*k], sizeof(double)*3);
+        }
+        m->npartner[i] = np;
+        m->nneighs[i] = np;
+    }
+    return 0;
+}
+
 int orc_get_mesh_contacts(orc_sim *s, int ifix, int cap, int *tag, int *tri, double *hist)
 {
     if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;

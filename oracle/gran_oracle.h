@@ -113,6 +113,9 @@ typedef struct {
 int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p);
 int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step);
 int orc_park_after(int seed, int n);
+/* mesh contact history in the restart layout (sorts the slots first, as write_restart does) */
+int orc_get_mesh_history(orc_sim *s, int ifix, int cap, int *npartner, int *tri, double *hist);
+int orc_upload_mesh_hist(orc_sim *s, int ifix, int n, const int *npartner, const int *tri, const double *hist);
 /* compute pair/gran/local: rows of the columns keys selects (bit b of keys:
    pos, vel, id, force, force_normal, force_tangential, torque, torque_normal,
    torque_tangential, history, contactArea, delta, contactPoint) */

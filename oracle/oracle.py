@@ -78,6 +78,8 @@ def lib():
         L.orc_add_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_get_mesh_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_get_mesh_history.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
+        L.orc_upload_mesh_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
         L.orc_park_after.argtypes = [ctypes.c_int, ctypes.c_int]
         L.orc_add_insert_pack.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrcInsertPack)]
         L.orc_insert_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), D,
@@ -345,6 +347,24 @@ class Oracle:
         h = np.zeros((n, 3))
         self.L.orc_get_mesh_contacts(self.h, k, n, _ip(tag), _ip(tri), _dp(h))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def mesh_history(self, ifix):
+        """Mesh contact history in the restart layout: {tag, npartner, tri, hist}."""
+        k = self.fix_ids[ifix]
+        tot = self.L.orc_get_mesh_history(self.h, k, 0, None, None, None)
+        npart = np.zeros(self.nlocal, dtype=np.int32)
+        tri = np.zeros(tot, dtype=np.int32)
+        h = np.zeros((tot, 3))
+        self.L.orc_get_mesh_history(self.h, k, tot, _ip(npart), _ip(tri), _dp(h))
+        return {"tag": self.atoms()["tag"], "npartner": npart, "tri": tri, "hist": h}
+
+    def upload_mesh_hist(self, ifix, npartner, tri, hist):
+        npart = np.ascontiguousarray(npartner, dtype=np.int32)
+        t = np.ascontiguousarray(tri, dtype=np.int32)
+        h = np.ascontiguousarray(hist, dtype=np.float64).reshape(-1)
+        self._keep += [npart, t, h]
+        if self.L.orc_upload_mesh_hist(self.h, self.fix_ids[ifix], len(npart), _ip(npart), _ip(t), _dp(h)) != 0:
+            raise ValueError("orc_upload_mesh_hist failed")
 
     def mesh_nodes(self, ifix):
         n = self.L.orc_get_mesh_nodes(self.h, self.fix_ids[ifix], None, None)

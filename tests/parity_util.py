@@ -41,3 +41,24 @@ def assert_mesh_equal(eng, orc, ifix):
     assert np.array_equal(p["tag"], q["tag"]) and np.array_equal(p["tri"], q["tri"]), "mesh contact slots differ"
     assert np.array_equal(p["hist"], q["hist"]), "mesh shear history differs"
     return len(p["tag"])
+
+
+def restart_scenario(sc, atoms):
+    """The scenario with its atoms replaced by a run's current state (same
+    tags, the run's atom order), as read_restart would bring them back."""
+    out = dict(sc)
+    a = dict(sc["atoms"])
+    pos_of_tag = {t: k for k, t in enumerate(a["tag"])}
+    idx = np.array([pos_of_tag[t] for t in atoms["tag"]])
+    for k in a:
+        a[k] = np.ascontiguousarray(np.asarray(a[k])[idx])
+    for k in ("x", "v", "omega"):
+        a[k] = np.ascontiguousarray(atoms[k])
+    a["tag"] = np.ascontiguousarray(atoms["tag"])
+    out["atoms"] = a
+    return out
+
+
+def mesh_contact_map(mc):
+    """{(tag, triangle): shear} of a mesh_contacts() download."""
+    return {(int(t), int(r)): tuple(h) for t, r, h in zip(mc["tag"], mc["tri"], mc["hist"])}

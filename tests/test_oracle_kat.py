@@ -266,3 +266,24 @@ def test_insert_pack_places_non_overlapping_particles(kw):
     if fx.get("all_in"):
         gap = np.minimum(xn - lo, hi - xn).min(axis=1)
         assert np.all(gap >= rad.min())
+
+
+def test_restart_carries_mesh_history():
+    # write_restart / read_restart of the mesh contact history: a run
+    # restarted from the restart layout (atoms, pair, plane-wall and mesh
+    # histories) has, right after its setup, every mesh contact of the
+    # original run with the same shear
+    from parity_util import mesh_contact_map, restart_scenario
+    sc = S.hopper(n=4000, n_theta=48, n_z=12, seed=5, gap=0.002, vmax=0.5)
+    o = oracle.Oracle(sc)
+    o.setup()
+    o.run(900)
+    before = mesh_contact_map(o.mesh_contacts(1))
+    mh, he = o.mesh_history(1), o.history()
+    assert mh["npartner"].sum() == len(before) > 20 and mh["npartner"].max() >= 2
+    o2 = oracle.Oracle(restart_scenario(sc, o.atoms()))
+    o2.upload_history(he["npartner"], he["partner_tag"], he["hist"])
+    o2.upload_wall_hist(2, o.wall_hist(2))
+    o2.upload_mesh_hist(1, mh["npartner"], mh["tri"], mh["hist"])
+    o2.setup()
+    assert mesh_contact_map(o2.mesh_contacts(1)) == before

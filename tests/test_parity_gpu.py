@@ -210,19 +210,8 @@ def test_two_types_neighbor_schedule_no_tangential_damping():
 
 
 def _restart_scenario(sc, atoms):
-    """The scenario with its atoms replaced by a run's current state (same
-    tags, the run's atom order), as read_restart would bring them back."""
-    out = dict(sc)
-    a = dict(sc["atoms"])
-    pos_of_tag = {t: k for k, t in enumerate(a["tag"])}
-    idx = np.array([pos_of_tag[t] for t in atoms["tag"]])
-    for k in a:
-        a[k] = np.ascontiguousarray(np.asarray(a[k])[idx])
-    for k in ("x", "v", "omega"):
-        a[k] = np.ascontiguousarray(atoms[k])
-    a["tag"] = np.ascontiguousarray(atoms["tag"])
-    out["atoms"] = a
-    return out
+    from parity_util import restart_scenario
+    return restart_scenario(sc, atoms)
 
 
 def test_restart_history_roundtrip():
@@ -322,3 +311,40 @@ def test_insert_pack(kw):
         assert_pairs_equal(e, o)
     assert o.insert_stats()["ninserted"] > 100 and o.nlocal > n0
     assert e.stats()["nbuilds"] == o.nbuilds
+
+
+def test_restart_mesh_history_roundtrip():
+    """Restart of the mesh contact history: the restart layout (slots sorted
+    as write_restart does) equals the oracle's, and a run restarted from it
+    with the pair and wall histories matches the oracle restarted from the
+    same data bit for bit, every mesh contact carried over with its shear."""
+    from parity_util import mesh_contact_map, restart_scenario
+    sc = S.hopper(n=4000, n_theta=48, n_z=12, seed=5, gap=0.002, vmax=0.5)
+    e, o = _pair(sc)
+    e.setup()
+    o.setup()
+    e.run(900)
+    o.run(900)
+    me, mo = e.mesh_history(1), o.mesh_history(1)
+    for k in ("tag", "npartner", "tri", "hist"):
+        assert np.array_equal(me[k], mo[k]), "mesh history %s differs from the oracle" % k
+    assert me["npartner"].sum() > 20
+    assert_mesh_equal(e, o, 1)
+    before = mesh_contact_map(e.mesh_contacts(1))
+    he = e.history()
+    import granb200
+    sc2 = restart_scenario(sc, e.atoms())
+    e2, o2 = granb200.Engine(sc2), oracle.Oracle(sc2)
+    for x in (e2, o2):
+        x.upload_history(he["npartner"], he["partner_tag"], he["hist"])
+        x.upload_wall_hist(2, e.wall_hist(2))
+        x.upload_mesh_hist(1, me["npartner"], me["tri"], me["hist"])
+        x.setup()
+    assert mesh_contact_map(e2.mesh_contacts(1)) == before
+    assert_atoms_equal(e2, o2)
+    for _ in range(3):
+        e2.run(300)
+        o2.run(300)
+        assert_atoms_equal(e2, o2)
+        assert_pairs_equal(e2, o2)
+        assert_mesh_equal(e2, o2, 1)
