@@ -159,8 +159,8 @@ int gb2_add_move_mesh_linear(gb2_ctx *ctx, int ifix_mesh, const double vel[3]);
  * arrays with tags beyond the largest tag.  Call after gb2_upload_atoms and
  * before gb2_setup; max_atoms reserves device room for the owned atoms
  * (initial + inserted: an insertion beyond it returns GB2_ERR_CAPACITY).
- * Out of scope here: other region styles, radius / density distributions
- * other than constant, multisphere templates, orientation, set_property. */
+ * Out of scope here: other region styles, density distributions other than
+ * constant, multisphere templates, orientation, set_property. */
 #define GB2_INSERT_MAX_TEMPLATES 8
 typedef struct {
     int seed;                        /* prime > 10000 (Random::Random, src/random.cpp:55-95) */
@@ -186,6 +186,14 @@ typedef struct {
     double tmpl_radius[GB2_INSERT_MAX_TEMPLATES], tmpl_density[GB2_INSERT_MAX_TEMPLATES];
     double tmpl_weight[GB2_INSERT_MAX_TEMPLATES];
     int max_atoms;
+    /* radius distribution of each template (ProbabilityDistribution,
+     * src/probability_distribution.h): 0 constant tmpl_radius; 1 uniform
+     * between tmpl_radius and tmpl_radius2; 2 gaussian, mean tmpl_radius and
+     * sigma tmpl_radius2, cut at +-3 sigma; drawn from the template's own
+     * generator (tmpl_seed, prime > 10000) */
+    int tmpl_radius_style[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_radius2[GB2_INSERT_MAX_TEMPLATES];
+    int tmpl_seed[GB2_INSERT_MAX_TEMPLATES];
 } gb2_insert_pack;
 int gb2_add_insert_pack(gb2_ctx *ctx, const gb2_insert_pack *p);
 /* inserted count and mass so far, and the next insertion step (-1 / 0: none) */

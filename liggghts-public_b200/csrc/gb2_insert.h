@@ -150,6 +150,10 @@ public:
     InsertRegion R{};
     double boxlo[3] = {0, 0, 0}, boxhi[3] = {0, 0, 0};
     double distweight[GB2_INSERT_MAX_TEMPLATES] = {};
+    // radius distributions: bounds, uniform's h1/h2, cubic expectancy
+    double rmin[GB2_INSERT_MAX_TEMPLATES] = {}, rmax[GB2_INSERT_MAX_TEMPLATES] = {};
+    double h1[GB2_INSERT_MAX_TEMPLATES] = {}, h2[GB2_INSERT_MAX_TEMPLATES] = {};
+    ParkRandom rtmpl[GB2_INSERT_MAX_TEMPLATES];   // each template's random_insertion
     double tvol[GB2_INSERT_MAX_TEMPLATES] = {}, tmass[GB2_INSERT_MAX_TEMPLATES] = {};
     int distorder[GB2_INSERT_MAX_TEMPLATES] = {};
     double volexpect = 0, massexpect = 0, maxrad = 0, maxrbound = 0;
@@ -186,9 +190,32 @@ public:
             if (P.tmpl_type[i] < 1 || P.tmpl_type[i] > ntypes) return "template atom type out of range";
             if (!(P.tmpl_radius[i] > 0.) || !(P.tmpl_density[i] > 0.)) return "template radius and density > 0";
             if (P.tmpl_weight[i] < 0) return "invalid weight";
+            if (!insert_seed_ok(P.tmpl_seed[i])) return "template seeds must be prime numbers > 10000";
+            rtmpl[i].reset(P.tmpl_seed[i]);
+            // ProbabilityDistribution set_params / cubic_expectancy
+            const double r = P.tmpl_radius[i], r2 = P.tmpl_radius2[i];
+            double cube;
+            if (P.tmpl_radius_style[i] == 0) {
+                rmin[i] = rmax[i] = r;
+                cube = r * r * r;
+            } else if (P.tmpl_radius_style[i] == 1) {
+                if (!(r2 > r)) return "uniform radius distribution needs max > min";
+                rmin[i] = r;
+                rmax[i] = r2;
+                h1[i] = 2. / (1. / (r * r) - 1. / (r2 * r2));
+                h2[i] = h1[i] / (2. * r * r);
+                cube = 0.25 * (r2 * r2 * r2 + r2 * r2 * r + r2 * r * r + r * r * r);
+            } else if (P.tmpl_radius_style[i] == 2) {
+                if (!(r2 > 0.)) return "gaussian radius distribution needs sigma > 0";
+                rmin[i] = r - 3. * r2;
+                rmax[i] = r + 3. * r2;
+                if (rmin[i] < 0.) return "Probablity distribution: mu-3*sigma < 0, please increase mu or decrease sigma";
+                cube = r * (r * r + 3 * r2 * r2);
+            } else {
+                return "radius distribution must be constant, uniform or gaussian";
+            }
             // FixTemplateSphere: volume_expect = cubic expectancy * 4 pi / 3, mass_expect = density * volume
-            const double r = P.tmpl_radius[i];
-            tvol[i] = r * r * r * 4. * M_PI / 3.;
+            tvol[i] = cube * 4. * M_PI / 3.;
             tmass[i] = P.tmpl_density[i] * tvol[i];
             if (tvol[i] < 1e-12) return "Volume expectancy too small";
             distweight[i] = P.tmpl_weight[i];
@@ -221,7 +248,7 @@ public:
             n--;
         } while (swapped && n > 0);
         maxrbound = 0.;
-        for (int i = 0; i < nt; i++) maxrbound = std::max(maxrbound, P.tmpl_radius[i]);
+        for (int i = 0; i < nt; i++) maxrbound = std::max(maxrbound, rmax[i]);
         maxrad = 0.;
         for (int t = 1; t <= ntypes; t++) maxrad = std::max(maxrad, max_rad(t));
         rnd.reset(P.seed);
@@ -251,7 +278,7 @@ public:
     {
         double m = 0.;
         for (int i = 0; i < P.ntemplates; i++)
-            if (P.tmpl_type[i] == type && P.tmpl_radius[i] > m) m = P.tmpl_radius[i];
+            if (P.tmpl_type[i] == type && rmax[i] > m) m = rmax[i];
         return m;
     }
 
@@ -366,11 +393,20 @@ public:
                 parttogen[j]++;
             }
         }
+        // FixTemplateSphere::randomize_ptilist, template by template: each
+        // particle's radius from the template's own generator
+        std::vector<double> rad[GB2_INSERT_MAX_TEMPLATES];
+        for (int i = 0; i < nt; i++)
+            for (int j = 0; j < parttogen[i]; j++) rad[i].push_back(draw_radius(i));
         // particles to insert, large to small templates
         std::vector<int> plist;
+        std::vector<double> prad;
         for (int i = 0; i < nt; i++) {
             const int t = distorder[i];
-            for (int j = 0; j < parttogen[t]; j++) plist.push_back(t);
+            for (int j = 0; j < parttogen[t]; j++) {
+                plist.push_back(t);
+                prad.push_back(rad[t][j]);
+            }
         }
         const int ntot = (int)plist.size();
         if (ntot == 0) {
@@ -393,17 +429,17 @@ public:
             for (int it = 0; it < ntot; it++) {
                 const int t = plist[done];
                 double pos[3], v[3];
-                if (!random_position(pos, P.tmpl_radius[t])) return "region too small for all_in";
+                if (!random_position(pos, prad[done])) return "region too small for all_in";
                 random_velocity(v);
                 if (pos[0] == 0. && pos[1] == 0. && pos[2] == 0.) return "FixInsertPack::x_v_omega() illegal position";
-                out.push_back(make(t, pos, v));
+                out.push_back(make(t, prad[done], pos, v));
                 mass_this += out.back().mass;
                 done++;
             }
         } else {
             while (ntry < maxtry && done < ntot) {
                 const int t = plist[done];
-                const double rbound = P.tmpl_radius[t];
+                const double rbound = prad[done];
                 int nins = 0;
                 while (nins == 0 && ntry < maxtry) {
                     double pos[3];
@@ -416,7 +452,7 @@ public:
                     random_velocity(v);
                     if (!grid.overlaps(pos, rbound)) {
                         grid.add(NearParticle{{pos[0], pos[1], pos[2]}, rbound});
-                        out.push_back(make(t, pos, v));
+                        out.push_back(make(t, rbound, pos, v));
                         nins = 1;
                     }
                 }
@@ -480,7 +516,25 @@ private:
         }
     };
 
-    InsertedParticle make(int t, const double *pos, const double *v) const
+    // ProbabilityDistribution rand_value (src/probability_distribution.h:143-226)
+    double draw_radius(int t)
+    {
+        const double r = P.tmpl_radius[t], r2 = P.tmpl_radius2[t];
+        if (P.tmpl_radius_style[t] == 1) {
+            const double rn = rtmpl[t].uniform();
+            return std::sqrt(h1[t] / (2. * (h2[t] - rn)));
+        }
+        if (P.tmpl_radius_style[t] == 2) {
+            double value;
+            do {
+                value = r + rtmpl[t].gaussian() * r2;
+            } while (value < rmin[t] || value > rmax[t]);
+            return value;
+        }
+        return r;
+    }
+
+    InsertedParticle make(int t, double radius, const double *pos, const double *v) const
     {
         InsertedParticle q;
         for (int d = 0; d < 3; d++) {
@@ -488,7 +542,7 @@ private:
             q.v[d] = v[d];
             q.omega[d] = P.omega[d];
         }
-        q.radius = P.tmpl_radius[t];
+        q.radius = radius;
         q.density = P.tmpl_density[t];
         q.mass = q.density * (q.radius * q.radius * q.radius * 4. * M_PI / 3.);
         q.type = P.tmpl_type[t];

@@ -97,10 +97,14 @@ class InsertPackParams(ctypes.Structure):
         ("tmpl_density", ctypes.c_double * INSERT_MAX_TEMPLATES),
         ("tmpl_weight", ctypes.c_double * INSERT_MAX_TEMPLATES),
         ("max_atoms", ctypes.c_int),
+        ("tmpl_radius_style", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("tmpl_radius2", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_seed", ctypes.c_int * INSERT_MAX_TEMPLATES),
     ]
 
 
 VEL_STYLES = {"constant": 0, "uniform": 1, "gaussian": 2}
+RADIUS_STYLES = {"constant": 0, "uniform": 1, "gaussian": 2}
 
 
 def insert_pack_params(fx, struct=InsertPackParams):
@@ -137,6 +141,9 @@ def insert_pack_params(fx, struct=InsertPackParams):
         p.tmpl_radius[i] = float(t["radius"])
         p.tmpl_density[i] = float(t["density"])
         p.tmpl_weight[i] = float(t["weight"])
+        p.tmpl_radius_style[i] = RADIUS_STYLES[t.get("radius_style", "constant")]
+        p.tmpl_radius2[i] = float(t.get("radius2", 0.0))
+        p.tmpl_seed[i] = int(t.get("seed", 67867967))
     p.max_atoms = int(fx.get("max_atoms", 0))
     return p
 

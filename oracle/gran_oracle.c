@@ -1996,7 +1996,8 @@ static double park_gaussian(park_t *r)
 
 struct ins_state {
     orc_insert_pack p;
-    park_t rnd, rreg, rdist;
+    park_t rnd, rreg, rdist, rtmpl[8];
+    double rlo[8], rhi[8], h1[8], h2[8];   /* radius pdf bounds, uniform's h1/h2 */
     double distweight[8], tvol[8], tmass[8];
     int distorder[8];
     double volexpect, massexpect, maxrad, maxrbound;
@@ -2054,7 +2055,7 @@ static void ins_max_rad(const struct ins_state *I, int type, double *mx)
 {
     double m = 0.;
     for (int i = 0; i < I->p.ntemplates; i++)
-        if (I->p.tmpl_type[i] == type && I->p.tmpl_radius[i] > m) m = I->p.tmpl_radius[i];
+        if (I->p.tmpl_type[i] == type && I->rhi[i] > m) m = I->rhi[i];   /* pdf_max(pdf_radius) */
     *mx = m;
 }
 
@@ -2070,8 +2071,23 @@ int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p)
     const int nt = p->ntemplates;
     /* FixTemplateSphere: cubic_expectancy(radius)*4.*M_PI/3., density * volume (src/fix_template_sphere.cpp:244-245) */
     for (int i = 0; i < nt; i++) {
-        double mu = p->tmpl_radius[i];
-        I->tvol[i] = mu*mu*mu*4.*M_PI/3.;
+        double mu = p->tmpl_radius[i], s2 = p->tmpl_radius2[i], ce;
+        if (!seed_valid(p->tmpl_seed[i])) { free(I); fail(s, "template seed"); return -1; }
+        I->rtmpl[i].seed = p->tmpl_seed[i];
+        /* PDF::set_params and cubic_expectancy_value, src/probability_distribution.h:120-200 */
+        if (p->tmpl_radius_style[i] == 1) {
+            I->rlo[i] = mu; I->rhi[i] = s2;
+            I->h1[i] = 2./(1./(mu*mu)-1./(s2*s2));
+            I->h2[i] = I->h1[i]/(2.*mu*mu);
+            ce = 0.25*(s2*s2*s2 + s2*s2*mu + s2*mu*mu + mu*mu*mu);
+        } else if (p->tmpl_radius_style[i] == 2) {
+            I->rlo[i] = mu-3.*s2; I->rhi[i] = mu+3.*s2;
+            ce = mu*(mu*mu+3*s2*s2);
+        } else {
+            I->rlo[i] = I->rhi[i] = mu;
+            ce = mu*mu*mu;
+        }
+        I->tvol[i] = ce*4.*M_PI/3.;
         I->tmass[i] = p->tmpl_density[i] * I->tvol[i];
         I->distweight[i] = p->tmpl_weight[i];
     }
@@ -2102,7 +2118,7 @@ int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p)
         n--;
     } while (swaped && n > 0);
     I->maxrbound = 0.;
-    for (int i = 0; i < nt; i++) if (p->tmpl_radius[i] > I->maxrbound) I->maxrbound = p->tmpl_radius[i];
+    for (int i = 0; i < nt; i++) if (I->rhi[i] > I->maxrbound) I->maxrbound = I->rhi[i];
     I->maxrad = 0.;
     for (int t = 1; t <= s->ntypes; t++) { double m; ins_max_rad(I, t, &m); if (m > I->maxrad) I->maxrad = m; }
     I->rnd.seed = p->seed;
@@ -2300,8 +2316,30 @@ static void ins_pre_exchange(orc_sim *s)
         else I->next_reneighbor = -1;
         return;
     }
+    /* FixTemplateSphere::randomize_ptilist (src/fix_template_sphere.cpp:333-361), template by template */
+    double *trad = malloc(sizeof(double)*ntot);
+    int *tstart = calloc(nt + 1, sizeof(int));
+    for (int i = 0; i < nt; i++) tstart[i+1] = tstart[i] + parttogen[i];
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < parttogen[i]; j++) {
+            double r = p->tmpl_radius[i];
+            if (p->tmpl_radius_style[i] == 1) {
+                double rn = park_uniform(&I->rtmpl[i]);
+                r = sqrt(I->h1[i]/(2.*(I->h2[i]-rn)));
+            } else if (p->tmpl_radius_style[i] == 2) {
+                do r = p->tmpl_radius[i] + park_gaussian(&I->rtmpl[i]) * p->tmpl_radius2[i];
+                while (r < I->rlo[i] || r > I->rhi[i]);
+            }
+            trad[tstart[i] + j] = r;
+        }
     int *plist = malloc(sizeof(int)*ntot), q = 0;
-    for (int i = 0; i < nt; i++) for (int j = 0; j < parttogen[I->distorder[i]]; j++) plist[q++] = I->distorder[i];
+    double *prad = malloc(sizeof(double)*ntot);
+    for (int i = 0; i < nt; i++)
+        for (int j = 0; j < parttogen[I->distorder[i]]; j++) {
+            prad[q] = trad[tstart[I->distorder[i]] + j];
+            plist[q++] = I->distorder[i];
+        }
+    free(trad); free(tstart);
     /* load_xnear src/fix_insert.cpp:916-954: owned and ghost atoms near the region, within getBoundingBox */
     const int nall = s->nlocal + s->nghost;
     double *near = malloc(sizeof(double)*4*(nall + ntot + 1));
@@ -2335,7 +2373,7 @@ static void ins_pre_exchange(orc_sim *s)
     double mass_this = 0.;
     while (done < ntot && (!p->overlapcheck || ntry < maxtry)) {
         int t = plist[done];
-        double rb = p->tmpl_radius[t];
+        double rb = prad[done];
         double pos[3], v[3];
         int ok = 0;
         if (!p->overlapcheck) {
@@ -2407,7 +2445,7 @@ out:
         I->ninserted += done;
         I->massinserted += mass_this;
     }
-    free(plist); free(near); free(nx); free(nty); free(nr); free(nm);
+    free(plist); free(prad); free(near); free(nx); free(nty); free(nr); free(nm);
     if (s->err[0]) return;
     if (p->insert_every) I->next_reneighbor += p->insert_every;
     else I->next_reneighbor = 0;
@@ -2490,6 +2528,12 @@ void orc_get_atoms(orc_sim *s, double *x, double *v, double *omega, double *f, d
     if (f) memcpy(f, s->f, sizeof(double)*3*n);
     if (torque) memcpy(torque, s->torque, sizeof(double)*3*n);
     if (tag) memcpy(tag, s->tag, sizeof(int)*n);
+}
+
+void orc_get_radius_mass(orc_sim *s, double *radius, double *rmass)
+{
+    memcpy(radius, s->radius, sizeof(double)*s->nlocal);
+    memcpy(rmass, s->rmass, sizeof(double)*s->nlocal);
 }
 
 int orc_get_pairs(orc_sim *s, int cap, int *tag_i, int *tag_j, int *flag, double *hist)

@@ -109,10 +109,14 @@ typedef struct {
     int tmpl_type[8];
     double tmpl_radius[8], tmpl_density[8], tmpl_weight[8];
     int max_atoms;
+    int tmpl_radius_style[8];   /* 0 constant, 1 uniform(radius, radius2), 2 gaussian(radius, radius2) */
+    double tmpl_radius2[8];
+    int tmpl_seed[8];
 } orc_insert_pack;
 int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p);
 int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step);
 int orc_park_after(int seed, int n);
+void orc_get_radius_mass(orc_sim *s, double *radius, double *rmass);
 /* mesh contact history in the restart layout (sorts the slots first, as write_restart does) */
 int orc_get_mesh_history(orc_sim *s, int ifix, int cap, int *npartner, int *tri, double *hist);
 int orc_upload_mesh_hist(orc_sim *s, int ifix, int n, const int *npartner, const int *tri, const double *hist);

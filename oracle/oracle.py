@@ -80,6 +80,7 @@ def lib():
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_history.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
         L.orc_upload_mesh_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
+        L.orc_get_radius_mass.argtypes = [ctypes.c_void_p, D, D]
         L.orc_park_after.argtypes = [ctypes.c_int, ctypes.c_int]
         L.orc_add_insert_pack.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrcInsertPack)]
         L.orc_insert_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), D,
@@ -116,7 +117,9 @@ class OrcInsertPack(ctypes.Structure):
                 ("check_dist_from_subdomain_border", ctypes.c_int), ("dist_seed", ctypes.c_int),
                 ("dist_mass_based", ctypes.c_int), ("ntemplates", ctypes.c_int), ("tmpl_type", ctypes.c_int * 8),
                 ("tmpl_radius", ctypes.c_double * 8), ("tmpl_density", ctypes.c_double * 8),
-                ("tmpl_weight", ctypes.c_double * 8), ("max_atoms", ctypes.c_int)]
+                ("tmpl_weight", ctypes.c_double * 8), ("max_atoms", ctypes.c_int),
+                ("tmpl_radius_style", ctypes.c_int * 8), ("tmpl_radius2", ctypes.c_double * 8),
+                ("tmpl_seed", ctypes.c_int * 8)]
 
 
 def make_insert(fx):
@@ -146,6 +149,9 @@ def make_insert(fx):
     for i, t in enumerate(fx["templates"]):
         p.tmpl_type[i], p.tmpl_radius[i] = int(t["type"]), float(t["radius"])
         p.tmpl_density[i], p.tmpl_weight[i] = float(t["density"]), float(t["weight"])
+        p.tmpl_radius_style[i] = {"constant": 0, "uniform": 1, "gaussian": 2}[t.get("radius_style", "constant")]
+        p.tmpl_radius2[i] = float(t.get("radius2", 0.0))
+        p.tmpl_seed[i] = int(t.get("seed", 67867967))
     p.max_atoms = int(fx.get("max_atoms", 0))
     return p
 
@@ -347,6 +353,12 @@ class Oracle:
         h = np.zeros((n, 3))
         self.L.orc_get_mesh_contacts(self.h, k, n, _ip(tag), _ip(tri), _dp(h))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def radius_mass(self):
+        """Radius and mass of the owned atoms (current order)."""
+        r, m = np.zeros(self.nlocal), np.zeros(self.nlocal)
+        self.L.orc_get_radius_mass(self.h, _dp(r), _dp(m))
+        return r, m
 
     def mesh_history(self, ifix):
         """Mesh contact history in the restart layout: {tag, npartner, tri, hist}."""

@@ -224,7 +224,8 @@ def test_park_miller_minimal_standard():
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(periodic=False, vel_style="constant", all_in=1),
-                                dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian")])
+                                dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian"),
+                                dict(polydisperse=True, all_in=1)])
 def test_insert_pack_places_non_overlapping_particles(kw):
     # fix insert/pack at the first step: the new particles lie in the region
     # (all_in: a radius away from its faces), overlap neither each other nor
@@ -246,7 +247,9 @@ def test_insert_pack_places_non_overlapping_particles(kw):
         slack = 0 if fx["exact_number"] else len(fx["templates"])
         assert abs(k - fx["particles_in_region"]) <= slack
     x = a["x"]
-    rad = np.array(sorted({t["radius"] for t in fx["templates"]}))
+    # smallest radius a template can give (gaussian: cut at mean - 3 sigma)
+    rad = np.array([t["radius"] - (3 * t["radius2"] if t.get("radius_style") == "gaussian" else 0.0)
+                    for t in fx["templates"]])
     # radii from the masses (rmass = density * 4/3 pi r^3)
     lo, hi = np.array(fx["region_lo"]), np.array(fx["region_hi"])
     xn = x[new]
@@ -266,6 +269,19 @@ def test_insert_pack_places_non_overlapping_particles(kw):
     if fx.get("all_in"):
         gap = np.minimum(xn - lo, hi - xn).min(axis=1)
         assert np.all(gap >= rad.min())
+    r, m = o.radius_mass()
+    rn, mn = r[new], m[new]
+    assert np.allclose(mn, 2500.0 * 4.0 * np.pi / 3.0 * rn ** 3, rtol=1e-14)
+    t0, t1 = fx["templates"]
+    if kw.get("polydisperse"):
+        # uniform template: radii in [1.0, 1.3] mm; gaussian: within 3 sigma of 0.8 mm
+        big, small = rn[rn >= 0.95e-3], rn[rn < 0.95e-3]
+        assert len(big) > 5 and len(small) > 20 and len(np.unique(rn)) > 0.9 * len(rn)
+        assert big.min() >= t0["radius"] and big.max() <= t0["radius2"]
+        assert np.all(np.abs(small - t1["radius"]) <= 3 * t1["radius2"] * (1 + 1e-12))
+        assert abs(small.mean() - t1["radius"]) < 0.3 * t1["radius2"]
+    else:
+        assert set(np.unique(rn)) <= {t0["radius"], t1["radius"]}
 
 
 def test_restart_carries_mesh_history():
