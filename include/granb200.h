@@ -148,7 +148,7 @@ int gb2_add_move_mesh_rotate(gb2_ctx *ctx, int ifix_mesh, const double origin[3]
    skin/2 as for the rotation.  Call before gb2_setup; one mover per mesh. */
 int gb2_add_move_mesh_linear(gb2_ctx *ctx, int ifix_mesh, const double vel[3]);
 /* fix insert/pack (src/fix_insert_pack.cpp with src/fix_insert.cpp) over a
- * region block, fed by fix particledistribution/discrete
+ * region block or cylinder, fed by fix particledistribution/discrete
  * (src/fix_particledistribution_discrete.cpp) of fix particletemplate/sphere
  * templates with constant radius and density (src/fix_template_sphere.cpp).
  * Every insertion step (start, then every insert_every steps; insert_every 0
@@ -194,6 +194,13 @@ typedef struct {
     int tmpl_radius_style[GB2_INSERT_MAX_TEMPLATES];
     double tmpl_radius2[GB2_INSERT_MAX_TEMPLATES];
     int tmpl_seed[GB2_INSERT_MAX_TEMPLATES];
+    /* region style: 0 block (region_lo/hi), 1 cylinder (RegCylinder,
+     * src/region_cylinder.cpp:213-470): axis 0/1/2, centre (c1, c2) in the
+     * other two coordinates in x, y, z order, radius, extent lo..hi along the
+     * axis; region_lo/hi are then ignored */
+    int region_style;
+    int cyl_axis;
+    double cyl_c1, cyl_c2, cyl_radius, cyl_lo, cyl_hi;
 } gb2_insert_pack;
 int gb2_add_insert_pack(gb2_ctx *ctx, const gb2_insert_pack *p);
 /* inserted count and mass so far, and the next insertion step (-1 / 0: none) */

@@ -41,29 +41,61 @@
 
 namespace gb2 {
 
-// region block (interior side) and the bounding box of the near-particle list
+// insertion region (interior side: a block, or a cylinder whose extents are
+// lo/hi) and the bounding box of the near-particle list
 struct InsertRegion {
-    double lo[3], hi[3];     // the block
-    double blo[3], bhi[3];   // FixInsertPack::getBoundingBox: block within the box, widened by 2 maxrad
+    double lo[3], hi[3];     // block, or the cylinder's extents
+    double blo[3], bhi[3];   // FixInsertPack::getBoundingBox: region within the box, widened by 2 maxrad
     double maxrad;
     int all_in;
+    int cyl;                 // 0 block, 1 cylinder
+    int ax, a1, a2;          // cylinder axis and the other two coordinates in x, y, z order
+    double c1, c2, rad, clo, chi;
 
     GB2_HD bool inside(const double *x) const
     {
+        if (cyl) {   // RegCylinder::inside
+            const double del1 = x[a1] - c1, del2 = x[a2] - c2;
+            const double dist = sqrt(del1 * del1 + del2 * del2);
+            return dist <= rad && x[ax] >= clo && x[ax] <= chi;
+        }
         return x[0] >= lo[0] && x[0] <= hi[0] && x[1] >= lo[1] && x[1] <= hi[1] && x[2] >= lo[2] && x[2] <= hi[2];
     }
-    // RegBlock::surface_interior != 0: inside and closer than cut to a face
+    // RegBlock / RegCylinder::surface_interior != 0: inside and closer than cut to a face
     GB2_HD bool surface_interior(const double *x, double cut) const
     {
+        if (cyl) {
+            const double del1 = x[a1] - c1, del2 = x[a2] - c2;
+            const double r = sqrt(del1 * del1 + del2 * del2);
+            if (r > rad || x[ax] < clo || x[ax] > chi) return false;
+            return (rad - r < cut && r > 0.0) || x[ax] - clo < cut || chi - x[ax] < cut;
+        }
         if (x[0] < lo[0] || x[0] > hi[0] || x[1] < lo[1] || x[1] > hi[1] || x[2] < lo[2] || x[2] > hi[2])
             return false;
         for (int d = 0; d < 3; d++)
             if (x[d] - lo[d] < cut || hi[d] - x[d] < cut) return true;
         return false;
     }
-    // RegBlock::surface_exterior != 0: outside (or on the surface) and closer than cut
+    // RegBlock / RegCylinder::surface_exterior != 0: outside (or on the surface) and closer than cut
     GB2_HD bool surface_exterior(const double *x, double cut) const
     {
+        if (cyl) {
+            const double del1 = x[a1] - c1, del2 = x[a2] - c2;
+            const double r = sqrt(del1 * del1 + del2 * del2);
+            if (r >= rad + cut || x[ax] <= clo - cut || x[ax] >= chi + cut) return false;
+            if (r < rad && x[ax] > clo && x[ax] < chi) return false;
+            double p[3];
+            if (r > rad) {
+                p[a1] = c1 + del1 * rad / r;
+                p[a2] = c2 + del2 * rad / r;
+            } else {
+                p[a1] = x[a1];
+                p[a2] = x[a2];
+            }
+            p[ax] = x[ax] < clo ? clo : (x[ax] > chi ? chi : x[ax]);
+            const double dx = x[0] - p[0], dy = x[1] - p[1], dz = x[2] - p[2];
+            return sqrt(dx * dx + dy * dy + dz * dz) < cut;
+        }
         if (x[0] <= lo[0] - cut || x[0] >= hi[0] + cut || x[1] <= lo[1] - cut || x[1] >= hi[1] + cut ||
             x[2] <= lo[2] - cut || x[2] >= hi[2] + cut)
             return false;
@@ -183,8 +215,30 @@ public:
             return "must define exactly one keyword out of 'volumefraction_region', 'particles_in_region', and "
                    "'mass_in_region'";
         if (P.volumefraction_region < 0. || P.volumefraction_region > 1.) return "illegal volumefraction_region";
+        if (P.region_style == 1) {   // cylinder: extents as RegCylinder's bounding box
+            if (P.cyl_axis < 0 || P.cyl_axis > 2 || !(P.cyl_radius > 0.) || !(P.cyl_lo < P.cyl_hi))
+                return "illegal region cylinder";
+            const int ax = P.cyl_axis, a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;
+            P.region_lo[ax] = P.cyl_lo;
+            P.region_hi[ax] = P.cyl_hi;
+            P.region_lo[a1] = P.cyl_c1 - P.cyl_radius;
+            P.region_hi[a1] = P.cyl_c1 + P.cyl_radius;
+            P.region_lo[a2] = P.cyl_c2 - P.cyl_radius;
+            P.region_hi[a2] = P.cyl_c2 + P.cyl_radius;
+            R.cyl = 1;
+            R.ax = ax;
+            R.a1 = a1;
+            R.a2 = a2;
+            R.c1 = P.cyl_c1;
+            R.c2 = P.cyl_c2;
+            R.rad = P.cyl_radius;
+            R.clo = P.cyl_lo;
+            R.chi = P.cyl_hi;
+        } else if (P.region_style != 0) {
+            return "region style must be block or cylinder";
+        }
         for (int d = 0; d < 3; d++)
-            if (!(P.region_lo[d] < P.region_hi[d])) return "empty region block";
+            if (!(P.region_lo[d] < P.region_hi[d])) return "empty region";
         const int nt = P.ntemplates;
         for (int i = 0; i < nt; i++) {
             if (P.tmpl_type[i] < 1 || P.tmpl_type[i] > ntypes) return "template atom type out of range";

@@ -453,14 +453,16 @@ def subset(sc, n):
 
 
 def insert_pour(n_bed=400, seed=77, periodic=True, dt=2e-6, vel_style="uniform", all_in=0, exact_number=1,
-                target=("volumefraction_region", 0.25), insert_every=300, max_atoms=8000, polydisperse=False):
+                target=("volumefraction_region", 0.25), insert_every=300, max_atoms=8000, polydisperse=False,
+                cylinder=False):
     """fix insert/pack above a settled-looking bed: a 20 x 20 x 60 mm box (x/y
     periodic or walled), n_bed spheres of r = 1 mm at the bottom, and a region
     block 2-18 x 2-18 x 30-55 mm refilled every insert_every steps from two
     templates (r = 1.2 mm and 0.8 mm, 2500 kg/m^3, mass fractions 0.5 / 0.5)
     falling at -0.5 m/s (+- 0.1 m/s per component for vel uniform).
     polydisperse: radius uniform in 1.0-1.3 mm and gaussian 0.8 +- 0.05 mm
-    instead of the two constants."""
+    instead of the two constants.  cylinder: a region cylinder z (axis at
+    x = y = 10 mm, radius 8 mm, z 30-55 mm) instead of the block."""
     sc = sphere_pour(n=n_bed, seed=seed, dt=dt, box=(0.02, 0.02, 0.06), spacing=(2.5e-3, 2.5e-3, 2.4e-3), vmax=0.05)
     sc["name"] = "insert_pour"
     sc["periodic"] = [1, 1, 0] if periodic else [0, 0, 0]
@@ -478,6 +480,9 @@ def insert_pour(n_bed=400, seed=77, periodic=True, dt=2e-6, vel_style="uniform",
                       {"type": 1, "radius": 0.8e-3, "density": 2500.0, "weight": 0.5}],
         "max_atoms": max_atoms,
     }
+    if cylinder:
+        del fx["region_lo"], fx["region_hi"]
+        fx["region_cylinder"] = {"axis": 2, "c1": 0.01, "c2": 0.01, "radius": 0.008, "lo": 0.03, "hi": 0.055}
     if polydisperse:
         fx["templates"][0].update(radius=1.0e-3, radius_style="uniform", radius2=1.3e-3, seed=86028121)
         fx["templates"][1].update(radius_style="gaussian", radius2=0.05e-3, seed=49979687)

@@ -100,6 +100,13 @@ class InsertPackParams(ctypes.Structure):
         ("tmpl_radius_style", ctypes.c_int * INSERT_MAX_TEMPLATES),
         ("tmpl_radius2", ctypes.c_double * INSERT_MAX_TEMPLATES),
         ("tmpl_seed", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("region_style", ctypes.c_int),
+        ("cyl_axis", ctypes.c_int),
+        ("cyl_c1", ctypes.c_double),
+        ("cyl_c2", ctypes.c_double),
+        ("cyl_radius", ctypes.c_double),
+        ("cyl_lo", ctypes.c_double),
+        ("cyl_hi", ctypes.c_double),
     ]
 
 
@@ -112,9 +119,14 @@ def insert_pack_params(fx, struct=InsertPackParams):
     reference's keyword defaults where a key is absent)."""
     p = struct()
     p.seed = int(fx["seed"])
+    cyl = fx.get("region_cylinder")
+    if cyl is not None:   # {"axis": 0|1|2, "c1", "c2", "radius", "lo", "hi"}
+        p.region_style, p.cyl_axis = 1, int(cyl["axis"])
+        p.cyl_c1, p.cyl_c2, p.cyl_radius = float(cyl["c1"]), float(cyl["c2"]), float(cyl["radius"])
+        p.cyl_lo, p.cyl_hi = float(cyl["lo"]), float(cyl["hi"])
     for d in range(3):
-        p.region_lo[d] = fx["region_lo"][d]
-        p.region_hi[d] = fx["region_hi"][d]
+        p.region_lo[d] = fx.get("region_lo", (0.0, 0.0, 0.0))[d]
+        p.region_hi[d] = fx.get("region_hi", (0.0, 0.0, 0.0))[d]
         p.vel[d] = fx.get("vel", (0.0, 0.0, 0.0))[d]
         p.vel_fluct[d] = fx.get("vel_fluct", (0.0, 0.0, 0.0))[d]
         p.omega[d] = fx.get("omega", (0.0, 0.0, 0.0))[d]

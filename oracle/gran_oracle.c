@@ -2016,8 +2016,22 @@ static int seed_valid(int seed)
 }
 
 /* RegBlock::inside src/region_block.cpp:147-152 */
+/* RegCylinder: the two coordinates across the axis, in x, y, z order */
+static void cyl_axes(const orc_insert_pack *p, int *a1, int *a2)
+{
+    if (p->cyl_axis == 0) { *a1 = 1; *a2 = 2; }
+    else if (p->cyl_axis == 1) { *a1 = 0; *a2 = 2; }
+    else { *a1 = 0; *a2 = 1; }
+}
+
 static int blk_inside(const orc_insert_pack *p, const double *x)
 {
+    if (p->region_style == 1) {   /* RegCylinder::inside src/region_cylinder.cpp:213-239 */
+        int a1, a2, ax = p->cyl_axis; cyl_axes(p, &a1, &a2);
+        double del1 = x[a1] - p->cyl_c1, del2 = x[a2] - p->cyl_c2;
+        double dist = sqrt(del1*del1 + del2*del2);
+        return dist <= p->cyl_radius && x[ax] >= p->cyl_lo && x[ax] <= p->cyl_hi;
+    }
     return x[0] >= p->region_lo[0] && x[0] <= p->region_hi[0] && x[1] >= p->region_lo[1] && x[1] <= p->region_hi[1]
         && x[2] >= p->region_lo[2] && x[2] <= p->region_hi[2];
 }
@@ -2025,6 +2039,17 @@ static int blk_inside(const orc_insert_pack *p, const double *x)
 /* RegBlock::surface_interior src/region_block.cpp:161-220 (contact count) */
 static int blk_surface_interior(const orc_insert_pack *p, const double *x, double cutoff)
 {
+    if (p->region_style == 1) {   /* RegCylinder::surface_interior src/region_cylinder.cpp:249-330 */
+        int a1, a2, ax = p->cyl_axis; cyl_axes(p, &a1, &a2);
+        double del1 = x[a1] - p->cyl_c1, del2 = x[a2] - p->cyl_c2;
+        double r = sqrt(del1*del1 + del2*del2);
+        if (r > p->cyl_radius || x[ax] < p->cyl_lo || x[ax] > p->cyl_hi) return 0;
+        int n = 0;
+        if (p->cyl_radius - r < cutoff && r > 0.0) n++;
+        if (x[ax] - p->cyl_lo < cutoff) n++;
+        if (p->cyl_hi - x[ax] < cutoff) n++;
+        return n;
+    }
     const double *lo = p->region_lo, *hi = p->region_hi;
     if (x[0] < lo[0] || x[0] > hi[0] || x[1] < lo[1] || x[1] > hi[1] || x[2] < lo[2] || x[2] > hi[2]) return 0;
     int n = 0;
@@ -2038,6 +2063,20 @@ static int blk_surface_interior(const orc_insert_pack *p, const double *x, doubl
 /* RegBlock::surface_exterior src/region_block.cpp:228-259 with Region::add_contact src/region.cpp:248-257 */
 static int blk_surface_exterior(const orc_insert_pack *p, const double *x, double cutoff)
 {
+    if (p->region_style == 1) {   /* RegCylinder::surface_exterior src/region_cylinder.cpp:338-470 */
+        int a1, a2, ax = p->cyl_axis; cyl_axes(p, &a1, &a2);
+        double del1 = x[a1] - p->cyl_c1, del2 = x[a2] - p->cyl_c2;
+        double r = sqrt(del1*del1 + del2*del2);
+        const double R = p->cyl_radius, lo = p->cyl_lo, hi = p->cyl_hi;
+        if (r >= R+cutoff || x[ax] <= lo-cutoff || x[ax] >= hi+cutoff) return 0;
+        if (r < R && x[ax] > lo && x[ax] < hi) return 0;
+        double q[3];
+        if (r > R) { q[a1] = p->cyl_c1 + del1*R/r; q[a2] = p->cyl_c2 + del2*R/r; }
+        else { q[a1] = x[a1]; q[a2] = x[a2]; }
+        if (x[ax] < lo) q[ax] = lo; else if (x[ax] > hi) q[ax] = hi; else q[ax] = x[ax];
+        double delx = x[0] - q[0], dely = x[1] - q[1], delz = x[2] - q[2];
+        return sqrt(delx*delx + dely*dely + delz*delz) < cutoff;
+    }
     const double *lo = p->region_lo, *hi = p->region_hi;
     if (x[0] <= lo[0]-cutoff || x[0] >= hi[0]+cutoff || x[1] <= lo[1]-cutoff || x[1] >= hi[1]+cutoff ||
         x[2] <= lo[2]-cutoff || x[2] >= hi[2]+cutoff) return 0;
@@ -2068,6 +2107,12 @@ int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p)
     if (ndef != 1) { fail(s, "exactly one insertion target"); return -1; }
     struct ins_state *I = calloc(1, sizeof *I);
     I->p = *p;
+    if (p->region_style == 1) {   /* RegCylinder extents (bounding box) src/region_cylinder.cpp:159-183 */
+        int a1, a2, ax = p->cyl_axis; cyl_axes(p, &a1, &a2);
+        I->p.region_lo[ax] = p->cyl_lo; I->p.region_hi[ax] = p->cyl_hi;
+        I->p.region_lo[a1] = p->cyl_c1 - p->cyl_radius; I->p.region_hi[a1] = p->cyl_c1 + p->cyl_radius;
+        I->p.region_lo[a2] = p->cyl_c2 - p->cyl_radius; I->p.region_hi[a2] = p->cyl_c2 + p->cyl_radius;
+    }
     const int nt = p->ntemplates;
     /* FixTemplateSphere: cubic_expectancy(radius)*4.*M_PI/3., density * volume (src/fix_template_sphere.cpp:244-245) */
     for (int i = 0; i < nt; i++) {

@@ -112,6 +112,9 @@ typedef struct {
     int tmpl_radius_style[8];   /* 0 constant, 1 uniform(radius, radius2), 2 gaussian(radius, radius2) */
     double tmpl_radius2[8];
     int tmpl_seed[8];
+    int region_style;             /* 0 block, 1 cylinder */
+    int cyl_axis;
+    double cyl_c1, cyl_c2, cyl_radius, cyl_lo, cyl_hi;
 } orc_insert_pack;
 int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p);
 int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step);

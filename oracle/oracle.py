@@ -119,15 +119,23 @@ class OrcInsertPack(ctypes.Structure):
                 ("tmpl_radius", ctypes.c_double * 8), ("tmpl_density", ctypes.c_double * 8),
                 ("tmpl_weight", ctypes.c_double * 8), ("max_atoms", ctypes.c_int),
                 ("tmpl_radius_style", ctypes.c_int * 8), ("tmpl_radius2", ctypes.c_double * 8),
-                ("tmpl_seed", ctypes.c_int * 8)]
+                ("tmpl_seed", ctypes.c_int * 8), ("region_style", ctypes.c_int), ("cyl_axis", ctypes.c_int),
+                ("cyl_c1", ctypes.c_double), ("cyl_c2", ctypes.c_double), ("cyl_radius", ctypes.c_double),
+                ("cyl_lo", ctypes.c_double), ("cyl_hi", ctypes.c_double)]
 
 
 def make_insert(fx):
     """OrcInsertPack from a scenario fix dict (kind "insert_pack"), keyword defaults as the reference's."""
     p = OrcInsertPack()
     p.seed = int(fx["seed"])
+    cyl = fx.get("region_cylinder")
+    if cyl is not None:
+        p.region_style, p.cyl_axis = 1, int(cyl["axis"])
+        p.cyl_c1, p.cyl_c2, p.cyl_radius = float(cyl["c1"]), float(cyl["c2"]), float(cyl["radius"])
+        p.cyl_lo, p.cyl_hi = float(cyl["lo"]), float(cyl["hi"])
     for d in range(3):
-        p.region_lo[d], p.region_hi[d] = fx["region_lo"][d], fx["region_hi"][d]
+        p.region_lo[d] = fx.get("region_lo", (0.0, 0.0, 0.0))[d]
+        p.region_hi[d] = fx.get("region_hi", (0.0, 0.0, 0.0))[d]
         p.vel[d] = fx.get("vel", (0.0, 0.0, 0.0))[d]
         p.vel_fluct[d] = fx.get("vel_fluct", (0.0, 0.0, 0.0))[d]
         p.omega[d] = fx.get("omega", (0.0, 0.0, 0.0))[d]

@@ -225,7 +225,7 @@ def test_park_miller_minimal_standard():
 
 @pytest.mark.parametrize("kw", [dict(), dict(periodic=False, vel_style="constant", all_in=1),
                                 dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian"),
-                                dict(polydisperse=True, all_in=1)])
+                                dict(polydisperse=True, all_in=1), dict(cylinder=True, all_in=1)])
 def test_insert_pack_places_non_overlapping_particles(kw):
     # fix insert/pack at the first step: the new particles lie in the region
     # (all_in: a radius away from its faces), overlap neither each other nor
@@ -251,8 +251,15 @@ def test_insert_pack_places_non_overlapping_particles(kw):
     rad = np.array([t["radius"] - (3 * t["radius2"] if t.get("radius_style") == "gaussian" else 0.0)
                     for t in fx["templates"]])
     # radii from the masses (rmass = density * 4/3 pi r^3)
-    lo, hi = np.array(fx["region_lo"]), np.array(fx["region_hi"])
     xn = x[new]
+    cyl = fx.get("region_cylinder")
+    if cyl:
+        rr = np.hypot(xn[:, 0] - cyl["c1"], xn[:, 1] - cyl["c2"])
+        assert np.all(rr <= cyl["radius"]) and np.all((xn[:, 2] >= cyl["lo"]) & (xn[:, 2] <= cyl["hi"]))
+        lo = np.array([cyl["c1"] - cyl["radius"], cyl["c2"] - cyl["radius"], cyl["lo"]])
+        hi = np.array([cyl["c1"] + cyl["radius"], cyl["c2"] + cyl["radius"], cyl["hi"]])
+    else:
+        lo, hi = np.array(fx["region_lo"]), np.array(fx["region_hi"])
     assert np.all((xn >= lo) & (xn <= hi))
     vz = a["v"][new][:, 2]
     if kw.get("vel_style", "uniform") == "uniform":
@@ -267,7 +274,8 @@ def test_insert_pack_places_non_overlapping_particles(kw):
     db = np.linalg.norm(xn[:, None, :] - x[~new][None, :, :], axis=2)
     assert db.min() > rad.min() + 1e-3
     if fx.get("all_in"):
-        gap = np.minimum(xn - lo, hi - xn).min(axis=1)
+        gap = np.minimum(xn - lo, hi - xn).min(axis=1) if not cyl else np.minimum(
+            cyl["radius"] - rr, np.minimum(xn[:, 2] - cyl["lo"], cyl["hi"] - xn[:, 2]))
         assert np.all(gap >= rad.min())
     r, m = o.radius_mass()
     rn, mn = r[new], m[new]

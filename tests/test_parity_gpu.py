@@ -292,7 +292,8 @@ def test_mesh_surface_stress():
                                 dict(periodic=False, vel_style="constant", all_in=1),
                                 dict(target=("particles_in_region", 150), exact_number=0, vel_style="gaussian",
                                      insert_every=200),
-                                dict(polydisperse=True, all_in=1, insert_every=250)])
+                                dict(polydisperse=True, all_in=1, insert_every=250),
+                                dict(cylinder=True, target=("mass_in_region", 0.003), insert_every=250)])
 def test_insert_pack(kw):
     """fix insert/pack refilling a region block above a bed (periodic x/y with
     ghosts near the region, or walled; vel uniform / constant / gaussian;
