@@ -28,7 +28,6 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
-#include <unordered_map>
 #include <vector>
 
 #include "../../include/granb200.h"
@@ -524,48 +523,63 @@ public:
     }
 
 private:
-    // cell list over the near particles: a test sees every particle whose
-    // sphere reaches the candidate's (exact, unlike a fixed stencil)
+    // dense cell list over the near-list bounding box (every near particle and
+    // every candidate lies in it): a test sees every particle whose sphere
+    // reaches the candidate's (exact, unlike a fixed stencil); cell indices
+    // are clamped, which keeps the lookup exact because it is monotone
     struct NearGrid {
-        double h, inv;
+        double lo[3], h, inv;
+        int n[3];
         double rmax = 0.;
-        std::unordered_map<long long, std::vector<NearParticle>> cells;
-        NearGrid(const InsertRegion &, double maxrad_)
+        std::vector<int> head, next;
+        std::vector<NearParticle> parts;
+        NearGrid(const InsertRegion &R, double maxrad_)
         {
             h = 4 * maxrad_ > 0 ? 4 * maxrad_ : 1.0;
-            inv = 1.0 / h;
+            for (;;) {
+                inv = 1.0 / h;
+                long cells = 1;
+                for (int d = 0; d < 3; d++) {
+                    lo[d] = R.blo[d];
+                    n[d] = std::max(1, (int)std::ceil((R.bhi[d] - R.blo[d]) * inv) + 1);
+                    cells *= n[d];
+                }
+                if (cells <= (1L << 24)) break;   // at most 16M cells (64 MB of heads)
+                h *= 2;
+            }
+            head.assign((size_t)n[0] * n[1] * n[2], -1);
         }
-        static long long key(long long a, long long b, long long c)
+        int cell(double x, int d) const
         {
-            return ((a & 0x1fffff) << 42) | ((b & 0x1fffff) << 21) | (c & 0x1fffff);
+            const double f = std::floor((x - lo[d]) * inv);
+            return f < 0 ? 0 : (f >= n[d] ? n[d] - 1 : (int)f);
         }
         void add(const NearParticle &q)
         {
             rmax = std::max(rmax, q.r);
-            cells[key((long long)std::floor(q.x[0] * inv), (long long)std::floor(q.x[1] * inv),
-                      (long long)std::floor(q.x[2] * inv))]
-                .push_back(q);
+            const size_t c = ((size_t)cell(q.x[2], 2) * n[1] + cell(q.x[1], 1)) * n[0] + cell(q.x[0], 0);
+            parts.push_back(q);
+            next.push_back(head[c]);
+            head[c] = (int)parts.size() - 1;
         }
         bool overlaps(const double *x, double r) const
         {
             const double reach = r + rmax;
-            long long lo[3], hi[3];
+            int clo[3], chi[3];
             for (int d = 0; d < 3; d++) {
-                lo[d] = (long long)std::floor((x[d] - reach) * inv);
-                hi[d] = (long long)std::floor((x[d] + reach) * inv);
+                clo[d] = cell(x[d] - reach, d);
+                chi[d] = cell(x[d] + reach, d);
             }
-            for (long long a = lo[0]; a <= hi[0]; a++)
-                for (long long b = lo[1]; b <= hi[1]; b++)
-                    for (long long c = lo[2]; c <= hi[2]; c++) {
-                        auto it = cells.find(key(a, b, c));
-                        if (it == cells.end()) continue;
-                        for (const NearParticle &p : it->second) {
+            for (int cz = clo[2]; cz <= chi[2]; cz++)
+                for (int cy = clo[1]; cy <= chi[1]; cy++)
+                    for (int cx = clo[0]; cx <= chi[0]; cx++)
+                        for (int k = head[((size_t)cz * n[1] + cy) * n[0] + cx]; k >= 0; k = next[k]) {
+                            const NearParticle &p = parts[k];
                             double del[3] = {x[0] - p.x[0], x[1] - p.x[1], x[2] - p.x[2]};
                             const double rsq = del[0] * del[0] + del[1] * del[1] + del[2] * del[2];
                             const double radsum = r + p.r;
                             if (rsq <= radsum * radsum) return true;
                         }
-                    }
             return false;
         }
     };
