@@ -273,6 +273,7 @@ constexpr int kMaxNewton = 1000;   // iteration bound on the device (the referen
 
 // calc_contact_point: Newton from the better of `init1` and the sphere
 // solution, golden-section search when a step does not reduce the residual
+template <int MAXIT = kMaxNewton>
 __device__ __noinline__ void newton_solve(const Body &A, const Body &B, double ratio, const double *init1,
                                           bool have_mu, double mu_init, Newton &o)
 {
@@ -313,7 +314,7 @@ __device__ __noinline__ void newton_solve(const Body &A, const Body &B, double r
     double merit1 = merit0, merit2 = merit0, res1 = res0, res2 = res0;
     if (merit0 >= tol1) {
         const double size = fmin(fmin(fmin(A.shape[0], A.shape[1]), A.shape[2]), fmin(fmin(B.shape[0], B.shape[1]), B.shape[2]));
-        for (int iter = 0; iter < kMaxNewton; iter++) {
+        for (int iter = 0; iter < MAXIT; iter++) {
             o.iters++;
             merit2 = merit1;
             res2 = res1;
@@ -412,7 +413,7 @@ __device__ __noinline__ void newton_solve(const Body &A, const Body &B, double r
             }
             merit1 = merit2;
             res1 = res2;
-            if (iter >= kMaxNewton - 1) o.fail = 1;
+            if (iter >= MAXIT - 1) o.fail = 1;
             if (converged || o.fail) break;
         }
     }
@@ -433,6 +434,7 @@ __device__ __noinline__ void newton_solve(const Body &A, const Body &B, double r
 //   mode 1: one solve from `guess` (previous point advanced, or a learned guess
 //           with `guess_mu`).
 // Returns the final stage's solution; iters/solves count all stages.
+template <int MAXIT = kMaxNewton>
 __device__ __forceinline__ void contact_point(const double *ca, const double *qa, const double *sa, double na,
                                               const double *cb, const double *qb, const double *sb, double nb,
                                               int mode, const double *guess, bool have_mu, double guess_mu,
@@ -470,7 +472,7 @@ __device__ __forceinline__ void contact_point(const double *ca, const double *qa
             body_shape(B, xb, 2.0 + (nb - 2.0) * t);
         }
         const double pre[3] = {cp[0], cp[1], cp[2]};
-        newton_solve(A, B, ratio, pre, mode == 1 && have_mu, guess_mu, o);
+        newton_solve<MAXIT>(A, B, ratio, pre, mode == 1 && have_mu, guess_mu, o);
         for (int k = 0; k < 3; k++) cp[k] = o.point[k];
         iters += o.iters;
         solves++;

@@ -224,9 +224,16 @@ __device__ __forceinline__ void mlp_infer(const float *__restrict__ P, const flo
     }
 }
 
+// Newton iterations granted to the solve from the learned guess.  A start
+// the network places well converges in ~10; one that needs more is handed to
+// the homotopy, whose result is the plain method's anyway, so the pairs that
+// defeat both methods no longer pay the full iteration bound twice.
+constexpr int kLearnedNewton = 48;
+
 // Contact point of a pair without a previous point: the learned guess, one
-// Newton solve, and the homotopy as the fallback when that solve does not
-// reach the merit tolerance.  used: 1 learned guess accepted, -1 rejected, 0 off.
+// Newton solve (at most kLearnedNewton iterations), and the homotopy as the
+// fallback when that solve does not reach the merit tolerance.
+// used: 1 learned guess accepted, -1 rejected, 0 off.
 __device__ __forceinline__ void first_contact(const float *mlp, const double *ci, const double *qi, const double *si,
                                               double ni, const double *cj, const double *qj, const double *sj,
                                               double nj, Newton &o, int &iters, int &solves, int &used)
@@ -243,7 +250,8 @@ __device__ __forceinline__ void first_contact(const float *mlp, const double *ci
         matvec(Ri, pl, g);
         for (int k = 0; k < 3; k++) g[k] += ci[k];
         int it1, sv1;
-        contact_point(ci, qi, si, ni, cj, qj, sj, nj, 1, g, true, (double)fabsf(out[3]), o, it1, sv1);
+        contact_point<kLearnedNewton>(ci, qi, si, ni, cj, qj, sj, nj, 1, g, true, (double)fabsf(out[3]), o, it1,
+                                      sv1);
         if (!o.fail && o.merit < 1e-10) {
             iters = it1;
             solves = sv1;
