@@ -1692,6 +1692,7 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
     if (nl + k > c->cap)
         return set_err(c, GB2_ERR_CAPACITY, "fix insert/pack: %d atoms exceed the %d reserved (max_atoms)", nl + k,
                        c->cap);
+    if ((long)c->maxtag + k > 0x7fffffffL) return set_err(c, GB2_ERR_CAPACITY, "atom tags beyond INT_MAX");
     // Atom::tag_extend: tags beyond the largest one, in insertion order
     std::vector<dbl4> hp(k), hv(k), hw(k);
     std::vector<int> ht(k), hg(k);
@@ -1705,7 +1706,6 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
         c->h_radius.push_back(a.radius);
         c->h_type.push_back(a.type);
     }
-    if ((long)c->maxtag + k > 0x7fffffffL) return set_err(c, GB2_ERR_CAPACITY, "atom tags beyond INT_MAX");
     c->maxtag += k;
     if (ensure_nmax(c, nall > nl + k ? nall : nl + k)) return GB2_ERR_CUDA;
     CK(cudaMemcpyAsync(c->pos.p + nl, hp.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
