@@ -496,6 +496,22 @@ static __device__ bool mesh_contact(const Dev &D, const MeshDev &M, int i, int t
             atomicAdd(&M.ftot[c], frc[c]);
             atomicAdd(&M.ftot[3 + c], tq[c]);
         }
+        if (M.wear) {   // Finnie wear (src/mesh_module_stress.cpp:306-352), summed straight into the total
+            const double vr[3] = {v[0] - vwall[0], v[1] - vwall[1], v[2] - vwall[2]};
+            const double vm = sqrt(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+            if (!(delta[0] * vr[0] + delta[1] * vr[1] + delta[2] * vr[2] < 0.) && !(0.0000001 > vm)) {
+                const double *sn = M.tri[t].surfnorm;
+                const double cr[3] = {vr[1] * sn[2] - vr[2] * sn[1], vr[2] * sn[0] - vr[0] * sn[2],
+                                      vr[0] * sn[1] - vr[1] * sn[0]};
+                double sg = fabs(vr[0] * sn[0] + vr[1] * sn[1] + vr[2] * sn[2]) / vm;
+                double cg = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) / vm;
+                cg = cg > 1. ? 1. : cg;
+                sg = sg > 1. ? 1. : sg;
+                double E = (cg < 0.0001 || 3. * sg > cg) ? 0.33333 * cg * cg : 2. * sg * cg - 3. * sg * sg;
+                E *= 2. * M.kfin[itype] * vm * sqrt(frc[0] * frc[0] + frc[1] * frc[1] + frc[2] * frc[2]);
+                atomicAdd(&M.wear[t], E * D.dt / M.tarea[t]);
+            }
+        }
     }
     return true;
 }

@@ -104,6 +104,7 @@ struct MeshFix {
     bool stress = false;
     double pref[3] = {0, 0, 0};
     DBuf<double> trif, ftot;
+    DBuf<double> wear, tarea, kfin;   // Finnie wear
 };
 
 struct HostFix {
@@ -334,6 +335,9 @@ Dev make_dev(gb2_ctx *c)
             m.vnode = M.moving ? M.vnode.p : nullptr;
             m.trif = M.stress ? M.trif.p : nullptr;
             m.ftot = M.stress ? M.ftot.p : nullptr;
+            m.wear = M.stress && M.wear.p ? M.wear.p : nullptr;
+            m.tarea = M.tarea.p;
+            m.kfin = M.kfin.p;
             for (int d = 0; d < 3; d++) m.pref[d] = M.pref[d];
         }
     }
@@ -2181,6 +2185,50 @@ int gb2_add_mesh_stress(gb2_ctx *c, int ifix, const double p_ref[3])
     CK(cudaMemsetAsync(M.ftot.p, 0, sizeof(double) * 6, c->st));
     M.stress = true;
     for (int d = 0; d < 3; d++) M.pref[d] = p_ref[d];
+    return 0;
+}
+
+// mesh/surface/stress ... wear finnie on mesh wall fix ifix (after
+// gb2_add_mesh_stress, before setup): k_finnie is the ntypes x ntypes
+// peratomtypepair property (row-major); the wall's atom type picks the row
+int gb2_add_mesh_wear(gb2_ctx *c, int ifix, const double *k_finnie)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !k_finnie) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "mesh wear is added before setup");
+    MeshFix &M = *c->fix[ifix].mesh;
+    if (!M.stress) return set_err(c, GB2_ERR_STATE, "wear needs mesh/surface/stress on this mesh");
+    const int nt = (int)M.topo.tri.size(), ntypes = c->P.ntypes;
+    const int wt = c->fix[ifix].wtype;
+    if (wt < 1 || wt > ntypes) return set_err(c, GB2_ERR_ARG, "wall atom type out of range");
+    std::vector<double> area(std::max(nt, 1)), kf(kMaxTypes + 1, 0.0);
+    for (int t = 0; t < nt; t++) {   // TriMesh::calcArea of the element as created
+        const TriGeom &T0 = M.topo.tri[t];
+        const double cx = T0.edgevec[0][1] * T0.edgevec[1][2] - T0.edgevec[0][2] * T0.edgevec[1][1];
+        const double cy = T0.edgevec[0][2] * T0.edgevec[1][0] - T0.edgevec[0][0] * T0.edgevec[1][2];
+        const double cz = T0.edgevec[0][0] * T0.edgevec[1][1] - T0.edgevec[0][1] * T0.edgevec[1][0];
+        area[t] = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz) * T0.edgelen[0] * T0.edgelen[1];
+    }
+    for (int j = 1; j <= ntypes; j++) kf[j] = k_finnie[(wt - 1) * ntypes + (j - 1)];
+    CK(M.wear.alloc(std::max(nt, 1)));
+    CK(M.tarea.alloc(std::max(nt, 1)));
+    CK(M.kfin.alloc(kMaxTypes + 1));
+    CK(cudaMemsetAsync(M.wear.p, 0, sizeof(double) * std::max(nt, 1), c->st));
+    CK(cudaMemcpyAsync(M.tarea.p, area.data(), sizeof(double) * area.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(M.kfin.p, kf.data(), sizeof(double) * kf.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// cumulative Finnie wear per element (MeshModuleStress "wear")
+int gb2_download_mesh_wear(gb2_ctx *c, int ifix, int cap, double *wear)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !wear) return GB2_ERR_ARG;
+    MeshFix &M = *c->fix[ifix].mesh;
+    if (!M.wear.p) return set_err(c, GB2_ERR_STATE, "wear not enabled on this mesh");
+    const int nt = (int)M.topo.tri.size();
+    if (cap < nt) return set_err(c, GB2_ERR_ARG, "wear needs %d entries", nt);
+    CK(cudaMemcpyAsync(wear, M.wear.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     return 0;
 }
 

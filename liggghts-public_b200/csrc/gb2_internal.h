@@ -98,6 +98,10 @@ struct MeshDev {
     // about pref of the current step; null when not tracked
     double *trif, *ftot;
     double pref[3];
+    // Finnie wear (null when not tracked): cumulative per element, element
+    // area as created, k_finnie of the wall type against each atom type
+    double *wear;
+    const double *tarea, *kfin;
 };
 
 struct FixDev {

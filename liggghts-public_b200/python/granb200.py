@@ -32,7 +32,7 @@ EXPORTS = (
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
     "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
-    "gb2_upload_mesh_history",
+    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -240,6 +240,8 @@ def lib(path=LIB_PATH):
         L.gb2_upload_wall_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_add_mesh_stress.argtypes = [vp, ctypes.c_int, D]
         L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
+        L.gb2_add_mesh_wear.argtypes = [vp, ctypes.c_int, D]
+        L.gb2_download_mesh_wear.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_download_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, I, I, I, I, I, D]
         L.gb2_upload_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, D]
         L.gb2_add_insert_pack.argtypes = [vp, ctypes.POINTER(InsertPackParams)]
@@ -534,6 +536,17 @@ class Engine:
         h = np.zeros((n, 3))
         self._check(self.L.gb2_download_mesh_contacts(self.h, k, n, ctypes.byref(cnt), _ip(tag), _ip(tri), _dp(h)))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def add_mesh_wear(self, ifix, k_finnie):
+        """Finnie wear on the mesh of scenario fix ifix (after add_mesh_stress, before setup)."""
+        kf = np.ascontiguousarray(k_finnie, dtype=np.float64).reshape(-1)
+        self._check(self.L.gb2_add_mesh_wear(self.h, self.fix_ids[ifix], _dp(kf)))
+
+    def mesh_wear(self, ifix):
+        """Cumulative Finnie wear per triangle."""
+        w = np.zeros(max(self.ntri.get(ifix, 0), 1))
+        self._check(self.L.gb2_download_mesh_wear(self.h, self.fix_ids[ifix], len(w), _dp(w)))
+        return w[:self.ntri.get(ifix, 0)]
 
     def mesh_history(self, ifix):
         """Mesh contact history in the restart layout: {tag, npartner, tri, hist}."""

@@ -89,6 +89,7 @@ typedef struct {
     /* mesh/surface/stress (MeshModuleStress): per-element force, totals */
     int stress; double p_ref[3]; double (*tri_f)[3]; double f_total[3], torque_total[3];
     double (*area_ev)[2][3]; double (*area_el)[2];   /* edge vectors and lengths as created (calcArea) */
+    double *wear, *kfin;   /* Finnie wear per element; k_finnie of the wall type against each atom type */
 } wall_mesh;
 
 typedef struct { int kind; double xacc, yacc, zacc; wall_plane *wp; wall_mesh *wm; int imesh; } fixrec;
@@ -1859,6 +1860,28 @@ static void mesh_post_force(orc_sim *s, wall_mesh *m, int shearupdate)
                     tq[1] = tmp[2]*frc[0] - tmp[0]*frc[2];
                     tq[2] = tmp[0]*frc[1] - tmp[1]*frc[0];
                     for (int c = 0; c < 3; c++) m->torque_total[c] += tq[c];
+                    if (m->wear) {   /* wear finnie src/mesh_module_stress.cpp:306-352 */
+                        double vr[3], cr[3];
+                        const double *sn = m->surfnorm[t];
+                        for (int c = 0; c < 3; c++) vr[c] = s->v[3*ip+c] - vw[c];
+                        double cdot = delta[0]*vr[0] + delta[1]*vr[1] + delta[2]*vr[2];
+                        double vm = sqrt(vr[0]*vr[0] + vr[1]*vr[1] + vr[2]*vr[2]);
+                        if (!(cdot < 0.) && !(0.0000001 > vm)) {
+                            cross3(vr, sn, cr);
+                            double sg = fabs(vr[0]*sn[0] + vr[1]*sn[1] + vr[2]*sn[2]) / vm;
+                            double cg = fabs(sqrt(cr[0]*cr[0] + cr[1]*cr[1] + cr[2]*cr[2])) / vm;
+                            if (cg > 1.) cg = 1.;
+                            if (sg > 1.) sg = 1.;
+                            double E;
+                            if (cg < 0.0001 || 3.*sg > cg) E = 0.33333 * cg * cg;
+                            else E = 2. * sg * cg - 3. * sg * sg;
+                            E *= 2.*m->kfin[s->type[ip]] * vm * sqrt(frc[0]*frc[0] + frc[1]*frc[1] + frc[2]*frc[2]);
+                            double ev[3];
+                            cross3(m->area_ev[t][0], m->area_ev[t][1], ev);
+                            double area = 0.5*sqrt(ev[0]*ev[0] + ev[1]*ev[1] + ev[2]*ev[2]) * m->area_el[t][0] * m->area_el[t][1];
+                            m->wear[t] += E*s->p.dt / area;
+                        }
+                    }
                 }
             }
         }
@@ -2842,6 +2865,25 @@ int orc_get_wall_hist(orc_sim *s, int ifix, double *hist)
     if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wp) return -1;
     memcpy(hist, s->fix[ifix].wp->hist, sizeof(double)*3*s->nlocal);
     return s->nlocal;
+}
+
+/* wear finnie on a mesh with mesh/surface/stress: k_finnie ntypes x ntypes, row of the wall type */
+int orc_add_mesh_wear(orc_sim *s, int ifix, const double *k_finnie)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm || !s->fix[ifix].wm->stress) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    const int nt = s->ntypes;
+    m->wear = calloc(m->ntri > 0 ? m->ntri : 1, sizeof(double));
+    m->kfin = calloc(nt + 1, sizeof(double));
+    for (int j = 1; j <= nt; j++) m->kfin[j] = k_finnie[(m->wtype-1)*nt + (j-1)];
+    return 0;
+}
+
+int orc_get_mesh_wear(orc_sim *s, int ifix, double *wear)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm || !s->fix[ifix].wm->wear) return -1;
+    memcpy(wear, s->fix[ifix].wm->wear, sizeof(double)*s->fix[ifix].wm->ntri);
+    return 0;
 }
 
 /* FixContactHistoryMesh::write_restart (sort_contacts, src/fix_contact_history_mesh.cpp:

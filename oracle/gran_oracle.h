@@ -120,6 +120,8 @@ int orc_add_insert_pack(orc_sim *s, const orc_insert_pack *p);
 int orc_insert_stats(orc_sim *s, long *ninserted, double *massinserted, long *next_step);
 int orc_park_after(int seed, int n);
 void orc_get_radius_mass(orc_sim *s, double *radius, double *rmass);
+int orc_add_mesh_wear(orc_sim *s, int ifix, const double *k_finnie);
+int orc_get_mesh_wear(orc_sim *s, int ifix, double *wear);
 /* mesh contact history in the restart layout (sorts the slots first, as write_restart does) */
 int orc_get_mesh_history(orc_sim *s, int ifix, int cap, int *npartner, int *tri, double *hist);
 int orc_upload_mesh_hist(orc_sim *s, int ifix, int n, const int *npartner, const int *tri, const double *hist);

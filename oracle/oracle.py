@@ -80,6 +80,8 @@ def lib():
         L.orc_get_mesh_sigma.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         L.orc_get_mesh_history.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
         L.orc_upload_mesh_hist.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, I, I, D]
+        L.orc_add_mesh_wear.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
+        L.orc_get_mesh_wear.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
         L.orc_get_radius_mass.argtypes = [ctypes.c_void_p, D, D]
         L.orc_park_after.argtypes = [ctypes.c_int, ctypes.c_int]
         L.orc_add_insert_pack.argtypes = [ctypes.c_void_p, ctypes.POINTER(OrcInsertPack)]
@@ -361,6 +363,18 @@ class Oracle:
         h = np.zeros((n, 3))
         self.L.orc_get_mesh_contacts(self.h, k, n, _ip(tag), _ip(tri), _dp(h))
         return {"tag": tag, "tri": tri, "hist": h}
+
+    def add_mesh_wear(self, ifix, k_finnie):
+        kf = np.ascontiguousarray(k_finnie, dtype=np.float64).reshape(-1)
+        self._keep.append(kf)
+        if self.L.orc_add_mesh_wear(self.h, self.fix_ids[ifix], _dp(kf)) != 0:
+            raise ValueError("orc_add_mesh_wear failed")
+
+    def mesh_wear(self, ifix, ntri):
+        w = np.zeros(ntri)
+        if self.L.orc_get_mesh_wear(self.h, self.fix_ids[ifix], _dp(w)) != 0:
+            raise ValueError("no wear on this mesh")
+        return w
 
     def radius_mass(self):
         """Radius and mass of the owned atoms (current order)."""

@@ -311,3 +311,20 @@ def test_restart_carries_mesh_history():
     o2.upload_mesh_hist(1, mh["npartner"], mh["tri"], mh["hist"])
     o2.setup()
     assert mesh_contact_map(o2.mesh_contacts(1)) == before
+
+
+def test_finnie_wear_linear_in_k():
+    # wear finnie is non-negative, lands on the elements the particles touch,
+    # and doubles bit for bit with k_finnie (only powers of two change)
+    sc = S.silo(n=600, piston_speed=0.5)
+    ntri = len(sc["fixes"][3]["nodes"])
+    out = []
+    for k in (0.5, 1.0):
+        o = oracle.Oracle(sc)
+        o.add_mesh_stress(3, [0.0, 0.0, 0.0])
+        o.add_mesh_wear(3, np.full((sc["ntypes"], sc["ntypes"]), k))
+        o.setup()
+        o.run(1500)
+        out.append(o.mesh_wear(3, ntri))
+    assert np.all(out[0] >= 0) and out[0].max() > 0
+    assert np.array_equal(out[1], 2 * out[0])

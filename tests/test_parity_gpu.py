@@ -267,9 +267,12 @@ def test_mesh_surface_stress():
     1e-12 of the largest value, not bit for bit."""
     sc = S.silo(n=1500, piston_speed=0.5)
     e, o = _pair(sc)
+    kf = np.full((sc["ntypes"], sc["ntypes"]), 0.7)
     for x in (e, o):
         x.add_mesh_stress(3, [0.001, -0.002, 0.01])
+        x.add_mesh_wear(3, kf)
         x.setup()
+    ntri = len(sc["fixes"][3]["nodes"])
     hits = 0
     for _ in range(6):
         e.run(500)
@@ -284,7 +287,11 @@ def test_mesh_surface_stress():
         for k in ("sigma_n", "sigma_t"):
             assert np.abs(a[k] - b[k]).max() <= 1e-10 * max(np.abs(b[k]).max(), 1e-30), k
         hits += int((np.abs(b["tri_f"]).sum(axis=1) > 0).sum())
+        # Finnie wear, cumulative per element (atomics: to 1e-12 of the largest)
+        wa, wb = e.mesh_wear(3), o.mesh_wear(3, ntri)
+        assert np.abs(wa - wb).max() <= 1e-12 * max(wb.max(), 1e-300)
     assert hits > 0, "the piston carried no force"
+    assert wb.max() > 0 and np.all(wb >= 0), "no wear on the piston"
     assert b["f_total"][2] > 0, "particles should push the piston up"
 
 
