@@ -925,9 +925,10 @@ int do_pre_force(gb2_ctx *c)
         } else if (H.kind == FIX_WALL_MESH) {
             MeshFix &M = *H.mesh;
             if (M.moving) {
-                // FixMesh::pre_force on a rebuild step stores the nodes (src/fix_mesh.cpp:567-572)
+                // FixMesh::pre_force on a rebuild step: store the nodes and
+                // recompute the element geometry (src/fix_mesh.cpp:567-572)
                 const int nt = (int)M.topo.tri.size();
-                k_mesh_store_last<<<nblk(nt), kBlock, 0, c->st>>>(M.tri.p, nt, M.node_last.p);
+                k_mesh_refresh<<<nblk(nt), kBlock, 0, c->st>>>(M.tri.p, nt, M.node_last.p, M.tarea.p);
                 CKL();
                 int rc = mesh_bins_device(c, M, true);
                 if (rc) return rc;
@@ -2179,10 +2180,22 @@ int gb2_add_mesh_stress(gb2_ctx *c, int ifix, const double p_ref[3])
     if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !p_ref) return GB2_ERR_ARG;
     if (c->setup_done) return set_err(c, GB2_ERR_STATE, "mesh/surface/stress is added before setup");
     MeshFix &M = *c->fix[ifix].mesh;
+    const int nt = (int)M.topo.tri.size();
+    std::vector<double> area(std::max(nt, 1));
+    for (int t = 0; t < nt; t++) {   // TriMesh::calcArea of the element as created
+        const TriGeom &T0 = M.topo.tri[t];
+        const double cx = T0.edgevec[0][1] * T0.edgevec[1][2] - T0.edgevec[0][2] * T0.edgevec[1][1];
+        const double cy = T0.edgevec[0][2] * T0.edgevec[1][0] - T0.edgevec[0][0] * T0.edgevec[1][2];
+        const double cz = T0.edgevec[0][0] * T0.edgevec[1][1] - T0.edgevec[0][1] * T0.edgevec[1][0];
+        area[t] = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz) * T0.edgelen[0] * T0.edgelen[1];
+    }
     CK(M.trif.alloc((size_t)3 * std::max<size_t>(M.topo.tri.size(), 1)));
     CK(M.ftot.alloc(6));
+    CK(M.tarea.alloc(std::max(nt, 1)));
     CK(cudaMemsetAsync(M.trif.p, 0, sizeof(double) * 3 * M.topo.tri.size(), c->st));
     CK(cudaMemsetAsync(M.ftot.p, 0, sizeof(double) * 6, c->st));
+    CK(cudaMemcpyAsync(M.tarea.p, area.data(), sizeof(double) * area.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
     M.stress = true;
     for (int d = 0; d < 3; d++) M.pref[d] = p_ref[d];
     return 0;
@@ -2200,20 +2213,11 @@ int gb2_add_mesh_wear(gb2_ctx *c, int ifix, const double *k_finnie)
     const int nt = (int)M.topo.tri.size(), ntypes = c->P.ntypes;
     const int wt = c->fix[ifix].wtype;
     if (wt < 1 || wt > ntypes) return set_err(c, GB2_ERR_ARG, "wall atom type out of range");
-    std::vector<double> area(std::max(nt, 1)), kf(kMaxTypes + 1, 0.0);
-    for (int t = 0; t < nt; t++) {   // TriMesh::calcArea of the element as created
-        const TriGeom &T0 = M.topo.tri[t];
-        const double cx = T0.edgevec[0][1] * T0.edgevec[1][2] - T0.edgevec[0][2] * T0.edgevec[1][1];
-        const double cy = T0.edgevec[0][2] * T0.edgevec[1][0] - T0.edgevec[0][0] * T0.edgevec[1][2];
-        const double cz = T0.edgevec[0][0] * T0.edgevec[1][1] - T0.edgevec[0][1] * T0.edgevec[1][0];
-        area[t] = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz) * T0.edgelen[0] * T0.edgelen[1];
-    }
+    std::vector<double> kf(kMaxTypes + 1, 0.0);
     for (int j = 1; j <= ntypes; j++) kf[j] = k_finnie[(wt - 1) * ntypes + (j - 1)];
     CK(M.wear.alloc(std::max(nt, 1)));
-    CK(M.tarea.alloc(std::max(nt, 1)));
     CK(M.kfin.alloc(kMaxTypes + 1));
     CK(cudaMemsetAsync(M.wear.p, 0, sizeof(double) * std::max(nt, 1), c->st));
-    CK(cudaMemcpyAsync(M.tarea.p, area.data(), sizeof(double) * area.size(), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(M.kfin.p, kf.data(), sizeof(double) * kf.size(), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
     return 0;
@@ -2235,8 +2239,9 @@ int gb2_download_mesh_wear(gb2_ctx *c, int ifix, int cap, double *wear)
 // per-element force of the last step (3 per triangle), the element normal and
 // shear stresses of MeshModuleStress::calc_total_force
 // (src/mesh_module_stress.cpp:335-375: |f.n| / area and |f - (f.n) n| / area
-// with the current normal and TriMesh::calcArea's area of the element as
-// created, src/tri_mesh_I.h:305), and f_total, torque_total
+// with the current normal and TriMesh::calcArea's area of the element,
+// src/tri_mesh_I.h:305, as created and, for a moving mesh, as recomputed at
+// its last rebuild), and f_total, torque_total
 int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, double *sigma_n, double *sigma_t,
                              double *tot6)
 {
@@ -2244,10 +2249,11 @@ int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, doubl
     MeshFix &M = *c->fix[ifix].mesh;
     if (!M.stress) return set_err(c, GB2_ERR_STATE, "mesh/surface/stress not enabled on this mesh");
     const int nt = (int)M.topo.tri.size();
-    std::vector<double> f((size_t)3 * nt);
+    std::vector<double> f((size_t)3 * nt), area(std::max(nt, 1));
     std::vector<TriGeom> geo(nt);
     CK(cudaMemcpyAsync(f.data(), M.trif.p, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(geo.data(), M.tri.p, sizeof(TriGeom) * nt, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(area.data(), M.tarea.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->st));
     if (tot6) CK(cudaMemcpyAsync(tot6, M.ftot.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     if (cap < nt) return 0;
@@ -2255,12 +2261,7 @@ int gb2_download_mesh_stress(gb2_ctx *c, int ifix, int cap, double *tri_f, doubl
         const double *fi = &f[3 * (size_t)t];
         if (tri_f)
             for (int k = 0; k < 3; k++) tri_f[3 * t + k] = fi[k];
-        const TriGeom &T0 = M.topo.tri[t];   // as created
-        const double cx = T0.edgevec[0][1] * T0.edgevec[1][2] - T0.edgevec[0][2] * T0.edgevec[1][1];
-        const double cy = T0.edgevec[0][2] * T0.edgevec[1][0] - T0.edgevec[0][0] * T0.edgevec[1][2];
-        const double cz = T0.edgevec[0][0] * T0.edgevec[1][1] - T0.edgevec[0][1] * T0.edgevec[1][0];
-        const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz) * T0.edgelen[0] * T0.edgelen[1];
-        const double invSurfArea = 1. / area;
+        const double invSurfArea = 1. / area[t];
         const double *sn = geo[t].surfnorm;
         double sn_ = fi[0] * sn[0] + fi[1] * sn[1] + fi[2] * sn[2];
         const double tmp[3] = {fi[0] - sn[0] * sn_, fi[1] - sn[1] * sn_, fi[2] - sn[2] * sn_};

@@ -631,13 +631,60 @@ __global__ void k_mesh_translate(TriGeom *tri, int ntri, double *vnode, const do
     if (far) *flag = 1;
 }
 
-// MultiNodeMesh::storeNodePosRebuild (src/multi_node_mesh_I.h:833)
-__global__ void k_mesh_store_last(const TriGeom *tri, int ntri, double *node_last)
+// A moving mesh on a rebuild step (FixMesh::pre_force -> pbcExchangeBorders,
+// src/fix_mesh.cpp:564-574, src/multi_node_mesh_parallel_I.h:652-700):
+// refreshOwned stores the nodes (MultiNodeMesh::storeNodePosRebuild,
+// src/multi_node_mesh_I.h:212-225) and recomputes the element's unit edge
+// vectors and lengths, surface normal, edge normals and obtuse-angle index
+// from its current nodes (SurfaceMesh::recalcLocalSurfProperties,
+// src/surface_mesh_I.h:163-200, with calcEdgeVecLen :361, calcSurfaceNorm
+// :374, calcEdgeNormals :417, calcObtuseAngleIndex :435), in the order and
+// arithmetic the mesh import uses, and with mesh/surface/stress the element
+// area (TriMesh::calcArea, src/tri_mesh_I.h:305).  Centre and bounding radius
+// stay: the reference updates them only for deforming meshes.
+__global__ void k_mesh_refresh(TriGeom *tri, int ntri, double *node_last, double *area)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntri) return;
+    TriGeom &T = tri[t];
     for (int j = 0; j < 3; j++)
-        for (int c = 0; c < 3; c++) node_last[9 * t + 3 * j + c] = tri[t].node[j][c];
+        for (int c = 0; c < 3; c++) node_last[9 * t + 3 * j + c] = T.node[j][c];
+    auto mag = [](const double *v) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); };
+    auto cross = [](const double *a, const double *b, double *r) {
+        r[0] = a[1] * b[2] - a[2] * b[1];
+        r[1] = a[2] * b[0] - a[0] * b[2];
+        r[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto scale_inv = [](double *v, double s) {
+        const double sinv = 1. / s;
+        v[0] = sinv * v[0];
+        v[1] = sinv * v[1];
+        v[2] = sinv * v[2];
+    };
+    for (int k = 0; k < 3; k++) {
+        for (int c = 0; c < 3; c++) T.edgevec[k][c] = T.node[(k + 1) % 3][c] - T.node[k][c];
+        T.edgelen[k] = mag(T.edgevec[k]);
+        scale_inv(T.edgevec[k], T.edgelen[k]);
+    }
+    cross(T.edgevec[0], T.edgevec[1], T.surfnorm);
+    if (mag(T.surfnorm) < 1e-15) cross(T.edgevec[1], T.edgevec[2], T.surfnorm);
+    if (mag(T.surfnorm) < 1e-15) cross(T.edgevec[2], T.edgevec[0], T.surfnorm);
+    scale_inv(T.surfnorm, mag(T.surfnorm));
+    for (int k = 0; k < 3; k++) {
+        cross(T.edgevec[k], T.surfnorm, T.edgenorm[k]);
+        if (mag(T.edgenorm[k]) < 1e-15)
+            for (int c = 0; c < 3; c++) T.edgenorm[k][c] = T.edgevec[(k + 1) % 3][c];
+        else
+            scale_inv(T.edgenorm[k], mag(T.edgenorm[k]));
+    }
+    int ob = -1;
+    for (int k = 0; k < 3; k++) ob = dot3(T.edgevec[k], T.edgevec[(k + 2) % 3]) > 0. ? k : -1;
+    T.obtuse = ob;
+    if (area) {
+        double cr[3];
+        cross(T.edgevec[0], T.edgevec[1], cr);
+        area[t] = 0.5 * mag(cr) * T.edgelen[0] * T.edgelen[1];
+    }
 }
 
 // FixNeighlistMesh with a moving mesh (src/fix_neighlist_mesh.cpp:383-395,

@@ -34,13 +34,15 @@ def _materials(ntypes, E, nu, e, mu, mur=0.0):
 
 def _atoms(pos, radius, density, vel, seed_omega=None):
     n = len(radius)
-    rmass = 4.0 * math.pi / 3.0 * radius ** 3 * density
+    # the reference's read_data mass, in its evaluation order (src/atom_vec_sphere.cpp:1081)
+    rmass = 4.0 * math.pi / 3.0 * radius * radius * radius * density
     return {
         "x": np.ascontiguousarray(pos, dtype=np.float64),
         "v": np.ascontiguousarray(vel, dtype=np.float64),
         "omega": np.zeros((n, 3)) if seed_omega is None else seed_omega,
         "radius": np.ascontiguousarray(radius, dtype=np.float64),
         "rmass": np.ascontiguousarray(rmass, dtype=np.float64),
+        "density": np.ascontiguousarray(np.broadcast_to(np.asarray(density, dtype=np.float64), (n,))),
         "type": np.ones(n, dtype=np.int32),
         "tag": np.arange(1, n + 1, dtype=np.int32),
     }
@@ -476,8 +478,8 @@ def insert_pour(n_bed=400, seed=77, periodic=True, dt=2e-6, vel_style="uniform",
         "region_lo": [0.002, 0.002, 0.03], "region_hi": [0.018, 0.018, 0.055],
         target[0]: target[1], "insert_every": insert_every, "all_in": all_in, "exact_number": exact_number,
         "vel_style": vel_style, "vel": [0.0, 0.0, -0.5], "vel_fluct": [0.1, 0.1, 0.1],
-        "templates": [{"type": 1, "radius": 1.2e-3, "density": 2500.0, "weight": 0.5},
-                      {"type": 1, "radius": 0.8e-3, "density": 2500.0, "weight": 0.5}],
+        "templates": [{"type": 1, "radius": 1.2e-3, "density": 2500.0, "weight": 0.5, "seed": 67867967},
+                      {"type": 1, "radius": 0.8e-3, "density": 2500.0, "weight": 0.5, "seed": 67867979}],
         "max_atoms": max_atoms,
     }
     if cylinder:

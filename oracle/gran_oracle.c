@@ -609,6 +609,26 @@ int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode)
     return m->ntri;
 }
 
+/* per element: centre 3, bounding radius, unit edge vectors 9, edge lengths 3,
+   edge normals 9, surface normal 3, precision -- the layout of the reference
+   harness's element geometry record */
+int orc_get_mesh_geom(orc_sim *s, int ifix, double *geom)
+{
+    if (ifix < 0 || ifix >= s->nfix || !s->fix[ifix].wm) return -1;
+    wall_mesh *m = s->fix[ifix].wm;
+    for (int t = 0; t < m->ntri && geom; t++) {
+        double *g = &geom[29*(size_t)t];
+        for (int c = 0; c < 3; c++) g[c] = m->center[t][c];
+        g[3] = m->rbound[t];
+        for (int a = 0; a < 3; a++)
+            for (int c = 0; c < 3; c++) { g[4+3*a+c] = m->edgevec[t][a][c]; g[16+3*a+c] = m->edgenorm[t][a][c]; }
+        for (int a = 0; a < 3; a++) g[13+a] = m->edgelen[t][a];
+        for (int c = 0; c < 3; c++) g[25+c] = m->surfnorm[t][c];
+        g[28] = m->precision;
+    }
+    return m->ntri;
+}
+
 /* fix move/mesh ... linear vx vy vz (MeshMoverLinear constructor
    src/mesh_mover_linear.cpp:66-77) */
 int orc_add_move_mesh_linear(orc_sim *s, int ifix_mesh, double vx, double vy, double vz)
@@ -703,12 +723,6 @@ static void move_mesh_rotate(orc_sim *s, wall_mesh *m)
         }
 }
 
-/* MultiNodeMesh::storeNodePosRebuild src/multi_node_mesh_I.h:833 */
-static void mesh_store_node_last(wall_mesh *m)
-{
-    if (m->moving) memcpy(m->node_last, m->node, sizeof(double)*9*m->ntri);
-}
-
 /* MultiNodeMesh::decideRebuild src/multi_node_mesh_I.h:791-823 */
 static int mesh_decide_rebuild(orc_sim *s, wall_mesh *m)
 {
@@ -765,6 +779,61 @@ found:
     return 1;
 }
 
+/* Surface properties of one element from its current nodes, as
+   SurfaceMesh::calcSurfPropertiesOfNewElement computes them on import
+   (src/surface_mesh_I.h:282-330) and recalcLocalSurfProperties recomputes
+   them whenever a moving mesh is re-parallelised (:163-200) */
+static void mesh_surf_props(wall_mesh *m, int t)
+{
+    /* calcEdgeVecLen :361 */
+    for (int i = 0; i < 3; i++) {
+        sub3(m->node[t][(i+1)%3], m->node[t][i], m->edgevec[t][i]);
+        m->edgelen[t][i] = mag3(m->edgevec[t][i]);
+        sdiv3(m->edgevec[t][i], m->edgelen[t][i]);
+    }
+    /* calcSurfaceNorm :374 (degenerate fallbacks omitted: duplicates removed) */
+    double *sn = m->surfnorm[t];
+    cross3(m->edgevec[t][0], m->edgevec[t][1], sn);
+    if (mag3(sn) < 1e-15) cross3(m->edgevec[t][1], m->edgevec[t][2], sn);
+    if (mag3(sn) < 1e-15) cross3(m->edgevec[t][2], m->edgevec[t][0], sn);
+    sdiv3(sn, mag3(sn));
+    /* calcEdgeNormals :417 */
+    for (int i = 0; i < 3; i++) {
+        cross3(m->edgevec[t][i], sn, m->edgenorm[t][i]);
+        if (mag3(m->edgenorm[t][i]) < 1e-15) memcpy(m->edgenorm[t][i], m->edgevec[t][(i+1)%3], sizeof(double)*3);
+        else sdiv3(m->edgenorm[t][i], mag3(m->edgenorm[t][i]));
+    }
+    /* calcObtuseAngleIndex :435, called for iNode = 0,1,2 -- each call
+       overwrites the element's index, so the last call decides */
+    m->obtuse[t] = NO_OBTUSE_ANGLE;
+    for (int i = 0; i < 3; i++) {
+        double d = dot3(m->edgevec[t][i], m->edgevec[t][(i+2)%3]);
+        m->obtuse[t] = (d > 0.) ? i : NO_OBTUSE_ANGLE;
+    }
+}
+
+/* FixMesh::pre_force on a re-neighbour step (src/fix_mesh.cpp:564-574):
+   MultiNodeMeshParallel::pbcExchangeBorders (src/multi_node_mesh_parallel_I.h:
+   652-700) returns at once for a static mesh; a moving mesh goes through
+   refreshOwned, i.e. MultiNodeMesh::refreshOwned (storeNodePosRebuild,
+   src/multi_node_mesh_I.h:212-225) and SurfaceMesh::recalcLocalSurfProperties
+   (edge vectors and lengths, normal, edge normals, obtuse index and area from
+   the current nodes, src/surface_mesh_I.h:163-200).  Centres and bounding
+   radii stay (updateCenterRbound runs only for deforming meshes). */
+static void mesh_refresh_owned(wall_mesh *m)
+{
+    if (!m->moving) return;
+    memcpy(m->node_last, m->node, sizeof(double)*9*m->ntri);
+    for (int t = 0; t < m->ntri; t++) {
+        mesh_surf_props(m, t);
+        if (m->area_ev) {   /* TriMesh::calcArea src/tri_mesh_I.h:305 reads edge vectors 0, 1 and lengths */
+            memcpy(m->area_ev[t][0], m->edgevec[t][0], sizeof(double)*3);
+            memcpy(m->area_ev[t][1], m->edgevec[t][1], sizeof(double)*3);
+            m->area_el[t][0] = m->edgelen[t][0]; m->area_el[t][1] = m->edgelen[t][1];
+        }
+    }
+}
+
 static void mesh_build_topology(orc_sim *s, wall_mesh *m)
 {
     const int n = m->ntri;
@@ -775,31 +844,7 @@ static void mesh_build_topology(orc_sim *s, wall_mesh *m)
     m->edge_active = malloc(3*(n?n:1)); m->corner_active = malloc(3*(n?n:1));
     m->nneigh = calloc(n?n:1, sizeof(int)); m->neighfaces = malloc(sizeof(int)*NEIGH_MAX*(n?n:1));
     for (int t = 0; t < n; t++) {
-        /* calcEdgeVecLen :363 */
-        for (int i = 0; i < 3; i++) {
-            sub3(m->node[t][(i+1)%3], m->node[t][i], m->edgevec[t][i]);
-            m->edgelen[t][i] = mag3(m->edgevec[t][i]);
-            sdiv3(m->edgevec[t][i], m->edgelen[t][i]);
-        }
-        /* calcSurfaceNorm :375 (degenerate fallbacks omitted: duplicates removed) */
-        double *sn = m->surfnorm[t];
-        cross3(m->edgevec[t][0], m->edgevec[t][1], sn);
-        if (mag3(sn) < 1e-15) cross3(m->edgevec[t][1], m->edgevec[t][2], sn);
-        if (mag3(sn) < 1e-15) cross3(m->edgevec[t][2], m->edgevec[t][0], sn);
-        sdiv3(sn, mag3(sn));
-        /* calcEdgeNormals :417 */
-        for (int i = 0; i < 3; i++) {
-            cross3(m->edgevec[t][i], sn, m->edgenorm[t][i]);
-            if (mag3(m->edgenorm[t][i]) < 1e-15) memcpy(m->edgenorm[t][i], m->edgevec[t][(i+1)%3], sizeof(double)*3);
-            else sdiv3(m->edgenorm[t][i], mag3(m->edgenorm[t][i]));
-        }
-        /* calcObtuseAngleIndex :433, called for iNode = 0,1,2 -- each call
-           overwrites the element's index, so the last call decides */
-        m->obtuse[t] = NO_OBTUSE_ANGLE;
-        for (int i = 0; i < 3; i++) {
-            double d = dot3(m->edgevec[t][i], m->edgevec[t][(i+2)%3]);
-            m->obtuse[t] = (d > 0.) ? i : NO_OBTUSE_ANGLE;
-        }
+        mesh_surf_props(m, t);
         for (int i = 0; i < 3; i++) { m->edge_active[t][i] = 1; m->corner_active[t][i] = 1; }
         for (int i = 0; i < NEIGH_MAX; i++) m->neighfaces[t][i] = -1;
     }
@@ -1956,7 +2001,7 @@ static void pre_force_all(orc_sim *s, int reneigh)
         fixrec *fr = &s->fix[k];
         if (fr->kind == ORC_FIX_WALL_MESH && fr->wm->moving) {
             /* FixMesh::pre_force src/fix_mesh.cpp:564-588 */
-            if (reneigh) mesh_store_node_last(fr->wm);
+            if (reneigh) mesh_refresh_owned(fr->wm);
             else if (mesh_decide_rebuild(s, fr->wm)) fr->wm->next_reneighbor = s->ntimestep + 1;
         }
         if (fr->kind == ORC_FIX_WALL_PLANE) wall_plane_pre_force(s, fr->wp);

@@ -76,6 +76,9 @@ int orc_add_move_mesh_rotate(orc_sim *s, int ifix_mesh, double ox, double oy, do
 int orc_add_move_mesh_linear(orc_sim *s, int ifix_mesh, double vx, double vy, double vz);
 /* current nodes (ntri x 3 x 3) and node velocities of a mesh fix; returns ntri */
 int orc_get_mesh_nodes(orc_sim *s, int ifix, double *nodes, double *vnode);
+/* element geometry, 29 doubles per triangle (centre, bounding radius, edge
+   vectors, edge lengths, edge normals, surface normal, precision) */
+int orc_get_mesh_geom(orc_sim *s, int ifix, double *geom);
 
 /* Verlet::setup */
 int orc_setup(orc_sim *s);

@@ -72,6 +72,7 @@ def lib():
         L.orc_get_mesh_nneighs.argtypes = [ctypes.c_void_p, ctypes.c_int, I]
         L.orc_add_move_mesh_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 7
         L.orc_get_mesh_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+        L.orc_get_mesh_geom.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
         L.orc_add_move_mesh_linear.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
         L.orc_contact_atom.argtypes = [ctypes.c_void_p, D]
         L.orc_upload_history.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I, D]
@@ -406,6 +407,14 @@ class Oracle:
         vel = np.zeros((n, 3, 3))
         self.L.orc_get_mesh_nodes(self.h, self.fix_ids[ifix], _dp(nodes), _dp(vel))
         return nodes, vel
+
+    def mesh_geom(self, ifix):
+        """Per element: centre, bounding radius, edge vectors, edge lengths,
+        edge normals, surface normal, precision (29 columns)."""
+        n = self.L.orc_get_mesh_geom(self.h, self.fix_ids[ifix], None)
+        g = np.zeros((n, 29))
+        self.L.orc_get_mesh_geom(self.h, self.fix_ids[ifix], _dp(g))
+        return g
 
     def mesh_topology(self, ifix, ntri_max):
         k = self.fix_ids[ifix]
