@@ -2,25 +2,36 @@
 Hertz/history + rolling-friction hopper with a triangulated mesh wall.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload hopper|pour] [--n N] [--settle S]
+                  [--workload hopper|pour|drum|bed|sq] [--particles N]
 
-Own arm: the workload is generated (seeded), uploaded, set up and settled for
-S steps, then W warm-up steps run untimed and K steps are timed with CUDA
-events on the engine's stream, bracketed by a barrier and device syncs.
-``value`` = particles x K / device time (whole job, summed over ranks).
-Multi-GPU: every rank runs an independent replica (different seed) -- the
-domain-decomposed multi-GPU path is not built, see DESIGN.md.
+Own arm: the workload is generated (seeded; the default is the packed
+conical hopper at the start of its discharge), uploaded and set up; W
+warm-up steps run untimed and K steps are timed with CUDA events on the
+engine's stream, bracketed by a barrier and device syncs.  ``value`` =
+particles x K / device time (whole job, summed over ranks).  The headline
+arm computes in FP64 and is bit-exact with the reference; beside it the
+line reports, from the same generated state: the split-precision form
+(FP32 contact math), a longer window in which neighbour rebuilds happen
+(rebuild cost per step, and the kernel timings the roofline uses), the
+end-to-end time through the C ABI with host buffers, and the reference's
+CPU time on one core.  Multi-GPU: every rank runs an independent replica
+(different seed); the spatially decomposed multi-GPU path is not built.
 
-Reference arm (--impl reference): the CPU oracle (a restatement of the
-reference's own CPU algorithm) on rank 0, on the host cores, timed on a
-bounded number of steps of the same workload.
+Reference arm (--impl reference): the reference itself (LIGGGHTS built
+from its own sources as oracle/_ref/lmp_ref) on the same generated state,
+written as a read_data file with its STL mesh and input script; W warm-up
+steps, then K steps timed by the reference's own "Loop time"; one
+single-threaded replica per host core the memory allows (no MPI on the
+box), value = the replicas' summed particle-steps/s.  Rank 0 alone runs it.
 """
 import argparse
 import json
-import math
 import os
+import re
+import shutil
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -30,6 +41,9 @@ sys.path.insert(0, os.path.join(ROOT, "liggghts-public_b200", "python"))
 
 METRIC = "particle-steps/s @1M spheres Hertz/history+mesh, 1 B200 vs plain FP64 GPU & host-CPU ref"
 UNIT = "particle-steps/s"
+# the default workload's state must hold config 2's work when the window starts
+FLOOR_TOUCH_PER_ATOM = 2.0
+FLOOR_MESH_CONTACTS = 10_000
 
 
 def parse():
@@ -39,45 +53,58 @@ def parse():
 def parse_list(argv):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
-    ap.add_argument("--workload", default="hopper", choices=["hopper", "pour", "drum", "sq"])
-    ap.add_argument("--n", type=int, default=0, help="particle count (default: 1M hopper, 20k pour)")
-    ap.add_argument("--settle", type=int, default=200, help="untimed settling steps before warm-up")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
-    ap.add_argument("--precision", default="split", choices=["split", "fp64"],
-                    help="precision of the headline arm (split: FP32 contact math on FP64 state)")
-    ap.add_argument("--fp64-steps", type=int, default=-1,
-                    help="timed steps of the plain FP64 form on the same state (-1: as many as --steps, 0: skip)")
+    ap.add_argument("--workload", default="hopper", choices=["hopper", "pour", "drum", "bed", "sq"])
+    ap.add_argument("--particles", type=int, default=0, help="particle count (default: the configuration's)")
+    ap.add_argument("--settle", type=int, default=0, help="sq arm: untimed settling steps before warm-up")
+    ap.add_argument("--long-steps", type=int, default=2000,
+                    help="steps of the longer window with neighbour rebuilds (0: skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=60.0, help="reference arm: target timed seconds")
+    ap.add_argument("--no-split", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args(argv)
 
 
 def make_workload(args, seed_offset=0):
+    """(scenario, description, config extras) of the selected workload."""
     import gb2_scenarios as S
     if args.workload == "drum":
-        n = args.n or 1_000_000
-        length = 0.85 * (n / 8_000_000)
-        sc = S.drum(n=n, seed=7 + seed_offset, length=max(length, 0.05), n_ax=max(8, int(121 * length / 0.85)))
+        n = args.particles or 8_000_000
+        sc = S.drum_config3(n=n, seed=7 + seed_offset)
         ntri = len(sc["fixes"][1]["nodes"])
-        desc = ("drum-%d: spheres r U(0.8, 1.2) mm, Hertz/history, 0.5 m drum (length scaled to the particle "
-                "count for a 35%% fill of the 8M/0.85 m configuration), %d triangles, fix move/mesh rotate 2 rad/s, "
-                "dt 5e-6" % (n, ntri))
+        desc = ("drum-%d: %d spheres r U(0.8, 1.2) mm, density 2700, E 1e7, nu 0.45, e 0.5, mu 0.4, Hertz/history, "
+                "0.5 m drum (length for a 35%% fill), %d triangles, fix move/mesh rotate 2 rad/s, dt 5e-6"
+                % (n, n, ntri))
+        return sc, desc, {"n_particles": n, "triangles": ntri}
+    if args.workload == "bed":
+        n = args.particles or 20_000_000
+        sc = S.bed_config5(n=n, seed=5 + seed_offset)
+        ntri = len(sc["fixes"][1]["nodes"])
+        desc = ("bed-%d: %d spheres r 0.5 mm in a 0.2 x 0.2 x 0.5 m box, flat floor plus a %d-triangle bumpy plate, "
+                "Hertz/history, dt 2e-6" % (n, n, ntri))
         return sc, desc, {"n_particles": n, "triangles": ntri}
     if args.workload == "hopper":
-        n = args.n or 1_000_000
-        sc = S.hopper(n=n, seed=2024 + seed_offset, gap=0.01, vmax=0.05)
+        n = args.particles or 1_000_000
+        sc = S.hopper_packed(n=n, seed=2024 + seed_offset)
         ntri = len(sc["fixes"][1]["nodes"])
         desc = ("hopper-%d: %d polydisperse spheres (lognormal r, median 1 mm, sigma 0.25, clip 0.5-2 mm), "
-                "Hertz/history + rolling cdt, conical mesh hopper %d triangles (60 deg, 30 mm outlet), "
-                "plane catch floor, dt 5e-6" % (n, n, ntri))
+                "Hertz/history + rolling cdt, conical mesh hopper %d triangles (60 deg, 30 mm outlet), plane catch "
+                "floor, dt 5e-6; packed at the start of its discharge" % (n, n, ntri))
         return sc, desc, {"n_particles": n, "triangles": ntri}
-    n = args.n or 20000
+    n = args.particles or 20000
     sc = S.sphere_pour(n=n, seed=12345 + seed_offset)
     desc = "sphere-pour-%d: monodisperse r=1 mm, Hertz/history, periodic x/y, plane floor, dt 1e-5" % n
     return sc, desc, {"n_particles": n, "triangles": 0}
+
+
+def shared_config(args, desc, extra):
+    """The config both arms print (identical keys and values)."""
+    return dict({"workload": desc, "state": "generated state, %d warm-up steps, then the timed steps" % args.warmup,
+                 "l2": "inputs larger than L2 (per-step working set > 126 MB)"}, **extra)
 
 
 # --------------------------------------------------------------- clocks
@@ -91,9 +118,9 @@ class ClockSampler:
         self.p = None
         self.out = None
         try:
-            self.out = open(os.devnull if False else "/tmp/gb2_clocks_%d.csv" % os.getpid(), "w")
+            self.out = open("/tmp/gb2_clocks_%d.csv" % os.getpid(), "w")
             self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                                       "-i", str(device), "-lms", "250"], stdout=self.out, stderr=subprocess.DEVNULL)
+                                       "-i", str(device), "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
@@ -140,57 +167,93 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(kernel, n, cen, nfix_plane, nfix_mesh, split=False):
-    """Algorithmic HBM bytes per launch (model in DESIGN.md): owned-atom
+def algorithmic_bytes(n, cen, nfix_plane, nfix_mesh, split=False):
+    """Algorithmic HBM bytes per launch of k_pair_step: the owned atoms' own
     records, list indices and shear history that must cross HBM once;
     neighbour-state gathers are served from L2 and not counted."""
     avg = lambda k: 0.5 * (cen[0][k] + cen[1][k])
-    if kernel == "k_pair_step":
-        # own x,v,w,r,m,type 92 + list counts 8 + touch mask 16 + xhold 24 + x,v,w out 72
-        # (+ the 32-byte FP32 kinematics record written in split precision)
-        per_atom = 92 + 8 + 16 + 24 + 72 + (32 if split else 0) + nfix_plane * 1 + nfix_mesh * 4
-        b = n * per_atom + avg("nlist") * 4 + avg("nrev") * 4 + avg("ntouch") * (52 + 25)
-        b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
-        return b
-    if kernel == "k_pair_main":
-        per_atom = 92 + 48 + 4 + 48 + 48 + nfix_plane * 1 + nfix_mesh * 4
-        b = n * per_atom + avg("nlist") * 4 + avg("ntouch") * 52
-        b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
-        return b
-    if kernel == "k_pair_reverse":
-        return n * (92 + 4 + 48) + avg("nrev") * 4 + avg("ntouch") * 24
-    raise ValueError(kernel)
+    # own x,v,w,r,m,type 92 + list counts 8 + touch mask 16 + xhold 24 + x,v,w out 72
+    # (+ the 32-byte FP32 kinematics record written in split precision)
+    per_atom = 92 + 8 + 16 + 24 + 72 + (32 if split else 0) + nfix_plane * 1 + nfix_mesh * 4
+    b = n * per_atom + avg("nlist") * 4 + avg("nrev") * 4 + avg("ntouch") * (52 + 25)
+    b += avg("nwall_touch") * 48 + avg("nmesh_cand") * 4 + avg("nmesh_touch") * 52
+    return b
 
 
 def load_traffic(kernel, workload):
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
             d = json.load(fh)
-        e = d.get(workload, {}).get(kernel)
-        return e
+        return d.get(workload, {}).get(kernel)
     except Exception:
         return None
 
 
-# --------------------------------------------------------------- CPU oracle
+# --------------------------------------------------------------- the reference binary
 
-def run_oracle_sample(sc, target_s, max_steps):
-    """Time the oracle (single thread) on sc: setup + 2 warm-up steps untimed,
-    then steps until ~target_s of CPU time (at most max_steps)."""
+def ref_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    o = oracle.Oracle(sc)
-    o.setup()
-    o.run(2)
-    t0 = time.perf_counter()
-    o.run(1)
-    one = time.perf_counter() - t0
-    k = int(max(1, min(max_steps, target_s / max(one, 1e-6))))
-    t0 = time.perf_counter()
-    o.run(k)
-    dt = time.perf_counter() - t0 + one
-    n = len(sc["atoms"]["tag"])
-    return n * (k + 1) / dt, k + 1
+    import ref
+    return ref
+
+
+LOOP_RE = re.compile(r"Loop time of ([0-9.eE+-]+) on \d+ procs for (\d+) steps with (\d+) atoms")
+
+
+def write_reference_input(sc, warmup, steps, wd):
+    """read_data file, STL meshes and input script of the scenario in the
+    reference's grammar: `run warmup` (setup included) then `run steps`."""
+    ref = ref_module()
+    ref.write_data(os.path.join(wd, "data.txt"), sc)
+    lines = ref.script(sc, wd, [max(warmup, 0), steps], None, thermo=0)
+    path = os.path.join(wd, "in.bench")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    return path
+
+
+def run_reference_replicas(script, wd, nproc):
+    """nproc copies of lmp_ref on the script at once; per replica (atoms,
+    steps, loop seconds) of its last run."""
+    ref = ref_module()
+    procs = []
+    for r in range(nproc):
+        scr = os.path.join(wd, "screen%d.txt" % r)
+        procs.append((subprocess.Popen([ref.LMP, "-in", script, "-log", "none", "-screen", scr],
+                                       stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, cwd=wd), scr))
+    out = []
+    for p, scr in procs:
+        _, err = p.communicate()
+        txt = open(scr).read() if os.path.exists(scr) else ""
+        loops = LOOP_RE.findall(txt)
+        if p.returncode != 0 or len(loops) < 2:
+            raise RuntimeError("lmp_ref failed (rc %d): %s %s" % (p.returncode, err.decode()[-500:], txt[-1500:]))
+        t, k, n = loops[-1]
+        out.append((int(n), int(k), float(t)))
+    return out
+
+
+def reference_steps_cap(n, steps, seconds):
+    """Timed steps of a reference replica: K, capped so a replica's window
+    stays near `seconds` at ~3e6 particle-steps/s per core (the reference's
+    measured rate on the packed 1M hopper, one core)."""
+    est = n / 3.0e6
+    return max(1, min(steps, int(seconds / max(est, 1e-9))))
+
+
+def host_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def avail_bytes():
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 8 << 30
 
 
 # --------------------------------------------------------------- arms
@@ -227,91 +290,52 @@ def allmax(dist, x):
     return float(t.item())
 
 
-def _ref_worker(argv, seconds, barrier, out):
-    """One replica of the reference arm: the oracle port (the reference's
-    algorithm, single-threaded) on the workload, timed for ~`seconds`."""
-    args = parse_list(argv)
-    sc, desc, extra = make_workload(args)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    o = oracle.Oracle(sc)
-    o.setup()
-    o.run(min(args.settle, 200))
-    o.run(min(args.warmup, 3))
-    n = len(sc["atoms"]["tag"])
-    barrier.wait()
-    k, t0 = 0, time.perf_counter()
-    while k < max(args.steps, 1):
-        o.run(1)
-        k += 1
-        if time.perf_counter() - t0 > seconds:
-            break
-    dt = time.perf_counter() - t0
-    out.put((n * k / dt, k, dt))
-
-
 def reference_arm(args):
-    """The reference's CPU path (the oracle port: its algorithm, restated in
-    C, single-threaded like the reference without MPI) on all host cores the
-    process may use: one replica per core on the same workload, timed
-    together; value = the replicas' summed particle-steps/s."""
+    """The reference (lmp_ref) on all host cores the memory allows: one
+    single-threaded replica per core, all on the same generated state, W
+    warm-up steps then the timed steps; value = summed particle-steps/s from
+    each replica's own "Loop time"."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import multiprocessing as mp
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    n_est = args.n or (20_000 if args.workload == "pour" else 1_000_000)
-    try:
-        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-    except (ValueError, OSError):
-        avail = 8 << 30
-    per = 400 + 900 * n_est          # bytes per replica (measured ~0.84 GB at 1M atoms)
-    nproc = max(1, min(cores, int(0.6 * avail // per)))
-    ctx = mp.get_context("spawn")
-    barrier, out = ctx.Barrier(nproc), ctx.Queue()
-    seconds = 20.0
-    procs = [ctx.Process(target=_ref_worker, args=(sys.argv[1:], seconds, barrier, out)) for _ in range(nproc)]
-    for p in procs:
-        p.start()
-    res = [out.get() for _ in range(nproc)]
-    for p in procs:
-        p.join()
-    val = sum(r[0] for r in res)
-    k = min(r[1] for r in res)
-    dt = max(r[2] for r in res)
     sc, desc, extra = make_workload(args)
-    settle, w = min(args.settle, 200), min(args.warmup, 3)
-    sample = ("%s; oracle port, %d single-threaded replicas on %d host cores, each after %d settle + %d warm-up "
-              "steps, ~%.0f s timed together (>= %d steps each)" % (desc, nproc, cores, settle, w, seconds, k))
-    line = {
-        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": k, "warmup": w,
-        "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": dict({"workload": desc, "settle_steps": settle}, **extra),
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "port", "sample": sample},
-        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    n = len(sc["atoms"]["tag"])
+    ref = ref_module()
+    cores = host_cores()
+    k = reference_steps_cap(n, args.steps, args.ref_seconds)
+    W0 = max(args.warmup, 3)
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": ws, "steps": k, "warmup": W0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": shared_config(argparse.Namespace(warmup=W0), desc, extra)}
+    if not ref.available():
+        line.update({"value": None, "unavailable": "reference binary oracle/_ref/lmp_ref not built"})
+        print(json.dumps(line), flush=True)
+        return
+    per = 250e6 + 900.0 * n          # resident bytes per replica (511 MB measured at 1M atoms)
+    nproc = max(1, min(cores, int(0.7 * avail_bytes() // per)))
+    wd = tempfile.mkdtemp(prefix="gb2bench_ref_")
+    try:
+        script = write_reference_input(sc, W0, k, wd)
+        res = run_reference_replicas(script, wd, nproc)
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+    val = sum(na * ka / ta for na, ka, ta in res)
+    tmax = max(t for _, _, t in res)
+    sample = ("%s; LIGGGHTS-PUBLIC 3.8.0 built from its sources (oracle/_ref/lmp_ref, g++ -O2, serial with MPI "
+              "stubs), %d single-threaded replicas on %d host cores at once, each %d warm-up + %d timed steps "
+              "(\"Loop time\")" % (desc, nproc, cores, W0, k))
+    line.update({"value": val, "ms_per_step": 1e3 * tmax / k,
+                 "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": sample},
+                 "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line), flush=True)
 
 
-def state_scenario(sc, a):
-    """Scenario whose x, v, omega are a downloaded engine state (by tag)."""
-    out = dict(sc)
-    order = np.argsort(a["tag"])
-    idx = a["tag"][order] - 1
-    out["atoms"] = dict(sc["atoms"])
-    for k in ("x", "v", "omega"):
-        arr = np.zeros_like(sc["atoms"][k])
-        arr[idx] = a[k][order]
-        out["atoms"][k] = arr
-    return out
+PROFILE_EVERY = 16   # per-kernel CUDA events on every 16th step of a window
 
 
-PROFILE_EVERY = 16   # per-kernel CUDA events on every 16th step of the timed window
-
-
-def timed_window(eng, steps, dist, device, clocks=True):
+def timed_window(eng, steps, dist, device, clocks=True, profile=True):
     """Device-timed window of `steps` steps: CUDA events at its ends give the
     window time; per-kernel CUDA events on every PROFILE_EVERY-th step give
     each kernel's average launch time (the events serialise the pair step
@@ -322,7 +346,8 @@ def timed_window(eng, steps, dist, device, clocks=True):
     sampler = ClockSampler(device) if clocks else None
     barrier(dist)
     eng.sync()
-    eng.set_profiling(True, every=PROFILE_EVERY)
+    if profile:
+        eng.set_profiling(True, every=PROFILE_EVERY)
     eng.timer_start()
     eng.run(steps)
     ms = eng.timer_stop()
@@ -336,7 +361,7 @@ def timed_window(eng, steps, dist, device, clocks=True):
     npm = st1["n_pair_main"] - st0["n_pair_main"]
     return {"ms": allmax(dist, ms), "clocks": clk, "cen": (cen0, cen1), "kt": kt, "npm": npm,
             "kernel_ms_per_step": dict({k: v / max(npm, 1) for k, v in kt.items()},
-                                       note="CUDA events on every %dth step of the timed window (%d steps timed)"
+                                       note="CUDA events on every %dth step of the window (%d steps sampled)"
                                             % (PROFILE_EVERY, npm)),
             "launches": st1["kernel_launches"] - st0["kernel_launches"],
             "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
@@ -344,111 +369,170 @@ def timed_window(eng, steps, dist, device, clocks=True):
             "capacities": {k: st1[k] for k in ("maxneigh", "maxpartner", "maxrev", "maxmesh")}}
 
 
+def long_window(eng, steps, dist, device):
+    """A longer window continuing the run: neighbour rebuilds happen here.
+    Rebuild cost per step = the device time of the sampled rebuild steps'
+    rebuild kernels, scaled to all rebuilds, over the window's steps."""
+    W = timed_window(eng, steps, dist, device, clocks=False)
+    st = eng.stats()
+    out = {"steps": steps, "ms_per_step": W["ms"] / steps, "rebuilds": W["rebuilds"],
+           "kernel_ms_per_step": W["kernel_ms_per_step"], "census_end": W["cen"][1], "launches": W["launches"],
+           "capacity_growth": W["growth"]}
+    # t_rebuild is recorded on sampled steps only; those that rebuilt give the cost of one rebuild
+    out["note"] = ("rebuild kernels timed with CUDA events on the sampled steps; t_rebuild per sampled step "
+                   "averages rebuild and non-rebuild steps alike")
+    out["rebuild_ms_per_step"] = W["kernel_ms_per_step"]["t_rebuild"]
+    return out, W
+
+
+def check_floors(args, n, cen):
+    """The default workload must hold config 2's work at the window start."""
+    if args.workload != "hopper" or n < 1_000_000:
+        return None
+    ok = cen["ntouch"] >= FLOOR_TOUCH_PER_ATOM * n and cen["nmesh_touch"] >= FLOOR_MESH_CONTACTS
+    if not ok:
+        raise SystemExit("bench: the timed state lacks config 2's work: %d touching pairs (need %d), %d mesh "
+                         "contacts (need %d)" % (cen["ntouch"], FLOOR_TOUCH_PER_ATOM * n, cen["nmesh_touch"],
+                                                 FLOOR_MESH_CONTACTS))
+    return {"touching_pairs_per_atom_min": FLOOR_TOUCH_PER_ATOM, "mesh_contacts_min": FLOOR_MESH_CONTACTS,
+            "met": True}
+
+
 def own_arm(args):
     ws, rank, local, dist = dist_init()
     import granb200
-    split = args.precision == "split"
-    prec = granb200.PREC_SPLIT if split else granb200.PREC_FP64
     sc, desc, extra = make_workload(args, seed_offset=rank)
     n = len(sc["atoms"]["tag"])
-    eng = granb200.Engine(sc, precision=prec, device=local)
-    eng.setup()
-    eng.run(args.settle)
-    if args.fp64_steps < 0:
-        args.fp64_steps = args.steps
-    # the settled state the timed window starts from (warm-up aside): the FP64
-    # arm and the end-to-end run start from it too
-    start_state = state_scenario(sc, eng.atoms()) if (args.fp64_steps > 0 and split) or not args.no_e2e else None
-    eng.run(max(args.warmup, 3))
-    W = timed_window(eng, args.steps, dist, local)
-    ms_max = W["ms"]
-    value = n * args.steps * ws / (ms_max * 1e-3)
-
-    # roofline of the dominant kernel
-    nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] == "wall_plane")
+    nfix_plane = sum(1 for f in sc["fixes"] if f["kind"] in ("wall_plane", "wall_cylinder"))
     nfix_mesh = sum(1 for f in sc["fixes"] if f["kind"] == "wall_mesh")
-    dom = "k_pair_step"
-    dom_ms = W["kt"]["t_pair_main"] / max(W["npm"], 1)
-    ab = algorithmic_bytes(dom, n, W["cen"], nfix_plane, nfix_mesh, split)
-    peak, peak_kind = peaks()
-    achieved = ab / (dom_ms * 1e-3) / 1e9
-    traffic = load_traffic(dom + ("_split" if split else ""), args.workload)
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": traffic["bytes_per_launch"] if traffic else None,
-            "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms,
-            "timing": "pair-step launches timed with CUDA events on every %dth step of the timed window"
-                      % PROFILE_EVERY}
+    W0 = max(args.warmup, 3)
 
-    pdesc = ("split (FP32 contact math on FP64-differenced positions and FP64 overlap, Kahan FP32 pair sums; "
-             "FP64 walls, gravity, integration)" if split else "fp64 (bit-exact to the oracle)")
+    # headline: FP64, bit-exact with the reference
+    eng = granb200.Engine(sc, precision=granb200.PREC_FP64, device=local)
+    eng.setup()
+    eng.run(W0)
+    cen_start = eng.census()
+    floors = check_floors(args, n, cen_start)
+    W = timed_window(eng, args.steps, dist, local)
+    value = n * args.steps * ws / (W["ms"] * 1e-3)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 contact / f64 state" if split else "f64", "data": "synthetic",
-        "config": dict({"workload": desc, "settle_steps": args.settle, "precision": pdesc,
-                        "l2": "inputs larger than L2 (per-step working set > 126 MB at 1M particles)",
-                        "parallelism": "replicas x%d" % ws if ws > 1 else "single GPU"}, **extra),
-        "roofline": roof,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": W0,
+        "ms_per_step": W["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": shared_config(argparse.Namespace(warmup=W0), desc, extra),
+        "precision": "fp64: IEEE FP64 throughout, FMA contraction off, bit-exact with the reference",
+        "parallelism": "replicas x%d (no data-path collective)" % ws if ws > 1 else "single GPU",
         "gpu_launches": W["launches"],
         "clocks": W["clocks"],
         "kernel_ms_per_step": W["kernel_ms_per_step"],
-        "census": {k: 0.5 * (W["cen"][0][k] + W["cen"][1][k]) for k in W["cen"][0]},
+        "census_window_start": cen_start,
+        "census_floors": floors,
         "rebuilds": W["rebuilds"],
         "capacity_growth_in_window": W["growth"],
         "capacities": W["capacities"],
     }
 
-    # the plain FP64 form on the same starting state (same settle, warm-up)
-    if start_state is not None and args.fp64_steps > 0 and split:
-        e64 = granb200.Engine(start_state, precision=granb200.PREC_FP64, device=local)
-        e64.setup()
-        e64.run(max(args.warmup, 3))
-        W64 = timed_window(e64, args.fp64_steps, dist, local, clocks=False)
-        v64 = n * args.fp64_steps * ws / (W64["ms"] * 1e-3)
-        line["fp64_gpu"] = {"value": v64, "unit": UNIT, "steps": args.fp64_steps,
-                            "ms_per_step": W64["ms"] / args.fp64_steps,
-                            "kernel_ms_per_step": W64["kernel_ms_per_step"],
-                            "note": "bit-exact FP64 path from the same settled state (same settle and warm-up "
-                                    "steps, %d timed steps; split window %d)" % (args.fp64_steps, args.steps)}
-        line["split_over_fp64"] = value / v64
-        e64.close()
-        del e64
+    # longer FP64 window with rebuilds; its sampled pair-step launches give the roofline
+    dom = "k_pair_step"
+    peak, peak_kind = peaks()
+    if args.long_steps > 0:
+        lw, WL = long_window(eng, args.long_steps, dist, local)
+        line["long_window"] = lw
+        kt_src, npm, cen_src, src = WL["kt"], WL["npm"], WL["cen"], "long FP64 window (%d steps)" % args.long_steps
+    else:
+        kt_src, npm, cen_src, src = W["kt"], W["npm"], W["cen"], "headline window"
+    dom_ms = kt_src["t_pair_main"] / max(npm, 1)
+    ab = algorithmic_bytes(n, cen_src, nfix_plane, nfix_mesh, False)
+    achieved = ab / (dom_ms * 1e-3) / 1e9
+    traffic = load_traffic(dom, args.workload)
+    line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                        "traffic": traffic["bytes_per_launch"] if traffic else None,
+                        "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms, "sampled_launches": npm,
+                        "timing": "pair-step launches timed with CUDA events on every %dth step of the %s"
+                                  % (PROFILE_EVERY, src)}
+    eng.close()
+    del eng
 
-    # end to end through the C ABI: host arrays in, setup, run, host arrays out
+    # split precision from the same generated state (same warm-up)
+    if not args.no_split:
+        e32 = granb200.Engine(sc, precision=granb200.PREC_SPLIT, device=local)
+        e32.setup()
+        e32.run(W0)
+        W32 = timed_window(e32, args.steps, dist, local, clocks=False)
+        v32 = n * args.steps * ws / (W32["ms"] * 1e-3)
+        line["split_gpu"] = {"value": v32, "unit": UNIT, "steps": args.steps, "ms_per_step": W32["ms"] / args.steps,
+                             "kernel_ms_per_step": W32["kernel_ms_per_step"],
+                             "precision": "FP32 contact math on FP64-differenced positions and FP64 overlap, Kahan "
+                                          "FP32 pair sums; FP64 walls, gravity, integration"}
+        line["split_over_fp64"] = v32 / value
+        if args.long_steps > 0:
+            lw32, _ = long_window(e32, args.long_steps, dist, local)
+            line["split_gpu"]["long_window"] = lw32
+            if "long_window" in line:
+                line["split_over_fp64_long"] = line["long_window"]["ms_per_step"] / lw32["ms_per_step"]
+        e32.close()
+        del e32
+
+    # end to end through the C ABI: pinned host arrays in, setup, K steps, host arrays out
     if not args.no_e2e:
-        sc2 = start_state
+        a = sc["atoms"]
+        host = {}
+        for k in ("x", "v", "omega"):
+            host[k] = granb200.pinned_empty((n, 3))
+            host[k][:] = a[k]
+        for k in ("radius", "rmass"):
+            host[k] = granb200.pinned_empty((n,))
+            host[k][:] = a[k]
+        for k in ("type", "tag"):
+            host[k] = granb200.pinned_empty((n,), np.int32)
+            host[k][:] = a[k]
+        out = {k: granb200.pinned_empty((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
+        out["tag"] = granb200.pinned_empty((n,), np.int32)
+        sc2 = dict(sc)
+        sc2["atoms"] = dict(a, **host)
         barrier(dist)
         t0 = time.perf_counter()
-        e2 = granb200.Engine(sc2, precision=prec, device=local)
+        e2 = granb200.Engine(sc2, precision=granb200.PREC_FP64, device=local)
         t1 = time.perf_counter()
         e2.setup()
+        e2.sync()
         t2 = time.perf_counter()
         e2.run(args.steps)
         e2.sync()
         t3 = time.perf_counter()
-        out = e2.atoms()
-        e2.sync()
+        e2.atoms(out)
         t4 = time.perf_counter()
-        dt = t4 - t0
-        dt = allmax(dist, dt)
+        dt = allmax(dist, t4 - t0)
         h2d = n * (3 * 3 * 8 + 2 * 8 + 2 * 4) + sum(f["nodes"].size * 8 for f in sc["fixes"] if f["kind"] == "wall_mesh")
         d2h = n * (5 * 3 * 8 + 4)
         line["e2e"] = {"value": n * args.steps * ws / dt, "unit": UNIT,
                        "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                       "includes": "context create, materials, atom + mesh upload, Verlet setup, %d steps from the "
-                                   "settled state the timed window starts from, download of x/v/omega/f/torque"
-                                   % args.steps,
+                       "includes": "context create, materials, atom + mesh upload from pinned host memory, Verlet "
+                                   "setup, %d FP64 steps from the generated state, download of x/v/omega/f/torque/tag "
+                                   "into pinned host memory" % args.steps,
                        "seconds": {"create_upload": t1 - t0, "setup": t2 - t1, "run": t3 - t2, "download": t4 - t3}}
-        del e2, out
+        e2.close()
+        del e2
 
-    # CPU baseline: the oracle on this rank's state at the start of the window
+    # CPU baseline: the reference itself on one core, same generated state
     if rank == 0 and ws == 1 and not args.no_cpu:
-        sc3 = state_scenario(sc, eng.atoms())
-        cval, ck = run_oracle_sample(sc3, args.cpu_seconds, 200)
-        line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": "oracle port, 1 thread, same %d-particle state as the GPU window end, "
-                                          "setup + 2 untimed steps, %d timed steps" % (n, ck)}
+        ref = ref_module()
+        if ref.available():
+            k = reference_steps_cap(n, args.steps, args.cpu_seconds)
+            wd = tempfile.mkdtemp(prefix="gb2bench_cpu_")
+            try:
+                script = write_reference_input(sc, W0, k, wd)
+                (na, ka, ta), = run_reference_replicas(script, wd, 1)
+            finally:
+                shutil.rmtree(wd, ignore_errors=True)
+            line["cpu_baseline"] = {"value": na * ka / ta, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": "lmp_ref (the reference built from its sources), 1 process, same "
+                                              "generated %d-particle state, %d warm-up + %d timed steps (\"Loop "
+                                              "time\")" % (n, W0, ka)}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": "reference binary not built"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -460,7 +544,8 @@ def sq_arm(args):
     initial guess, same particles, same steps, device-timed."""
     import granb200
     import gb2_scenarios as S
-    n = args.n or 200_000
+    n = args.particles or 200_000
+    settle = args.settle or 100
     t0 = time.perf_counter()
     tr = granb200.MlpTrainer()
     info = tr.make_data(1_000_000, seed=1)
@@ -475,7 +560,7 @@ def sq_arm(args):
     for name, learned in (("plain", None), ("learned", params)):
         e = granb200.SqEngine(sc, learned=learned)
         e.setup()
-        e.run(args.settle)
+        e.run(settle)
         e.run(max(args.warmup, 3))
         c0 = e.counters()
         ms = e.run_timed(args.steps)
@@ -493,14 +578,12 @@ def sq_arm(args):
         "vs_baseline": None, "dtype": "f64 contact solve, bf16 MLP", "data": "synthetic",
         "config": {"workload": "sq-packing-%d: half-axes U(1,2) mm, blockiness U(2,8), random orientations, "
                                "Hertz/history, dt 1e-5, random velocities +-1 m/s" % n,
-                   "settle_steps": args.settle},
+                   "settle_steps": settle},
         "plain": res["plain"], "learned": res["learned"],
         "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
         "first_contact_solve": dict(solve, note="contact-point solve of fresh pairs near contact (a new "
                                                 "contact's first solve), plain homotopy vs learned guess with "
-                                                "homotopy fallback, each launch timed alone; a launch lasts as "
-                                                "long as its slowest pairs (those both methods fail on after "
-                                                "the iteration cap)"),
+                                                "homotopy fallback, each launch timed alone"),
         "training": {"samples": info["valid"], "plain_iters_per_sample": info["plain_iters"],
                      "plain_solves_per_sample": info["plain_solves"], "loss_first": l0, "loss_last": l1,
                      "seconds": train_s, "held_out": ev},

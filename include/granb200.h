@@ -41,6 +41,8 @@
 #ifndef GRANB200_H
 #define GRANB200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -112,7 +114,9 @@ int gb2_set_materials(gb2_ctx *ctx, const double *youngs, const double *poisson,
                       const double *restitution, const double *friction,
                       const double *rollfriction);
 
-/* owned atoms, host arrays: x,v,omega [n][3], radius,rmass [n], type,tag [n] */
+/* owned atoms, host arrays: x,v,omega [n][3], radius,rmass [n], type,tag [n].
+   Arrays in page-locked memory (gb2_host_alloc) are copied to the device
+   directly; others go through the context's pinned staging buffer. */
 int gb2_upload_atoms(gb2_ctx *ctx, int n, const double *x, const double *v,
                      const double *omega, const double *radius, const double *rmass,
                      const int *type, const int *tag);
@@ -215,9 +219,17 @@ int gb2_run(gb2_ctx *ctx, int nsteps);
 /* block until all device work of this context has finished */
 int gb2_sync(gb2_ctx *ctx);
 
-/* downloads (current owned-atom order; any pointer may be NULL) */
+/* downloads (current owned-atom order; any pointer may be NULL); arrays in
+   page-locked memory are written by the device directly */
 int gb2_download_atoms(gb2_ctx *ctx, int cap, int *n, double *x, double *v, double *omega,
                        double *f, double *torque, int *tag);
+/* page-locked host memory for the atom arrays of gb2_upload_atoms and
+   gb2_download_atoms, so their copies run at full bus speed without the
+   staging copy (LAMMPS' own Atom arrays are ordinary heap memory,
+   src/memory.cpp; this has no reference counterpart).  gb2_host_free
+   releases what gb2_host_alloc returned. */
+int gb2_host_alloc(size_t bytes, void **ptr);
+int gb2_host_free(void *ptr);
 /* half-list pairs (tag_i, tag_j, contact flag, shear history[3]); returns
    the pair count in *n, writes at most cap entries */
 int gb2_download_pairs(gb2_ctx *ctx, int cap, int *n, int *tag_i, int *tag_j, int *flag, double *hist);
@@ -320,17 +332,19 @@ int gb2_mesh_topology(gb2_ctx *ctx, int ifix, int cap, int *ntri, unsigned char 
 
 int gb2_get_stats(gb2_ctx *ctx, gb2_stats *st);
 int gb2_census(gb2_ctx *ctx, gb2_contact_census *out);
-/* gb2_census_noalloc: the same census for callers that must not allocate
-   device memory -- code running while a CUDA stream is being captured into a
-   graph (cudaMalloc/cudaFree are illegal or force a device-wide sync there),
-   monitoring hooks of a host framework that owns every allocation, or a
-   process already at its memory cap.  It has no counterpart in the reference
-   (LIGGGHTS allocates freely on the host).  Its scratch is a file-scope device
-   array in libgranb200 of (GB2_NOALLOC_MAX_BLOCKS + 1) x 8 64-bit counters
-   (1 MiB), held by every GPU that loads the library until process exit, so
-   it serves at most GB2_NOALLOC_MAX_ATOMS owned atoms; larger contexts get
-   GB2_ERR_CAPACITY.  No cudaMalloc, cudaFree or allocating library call is
-   made.  The first call on a device looks up the array's device address
+/* gb2_census_noalloc: the same census for callers that cannot allocate
+   device memory -- monitoring hooks inside a host framework whose pool owns
+   every device allocation (a foreign cudaMalloc/cudaFree fragments that pool
+   or makes the whole device wait), and processes already at their device
+   memory cap.  It has no counterpart in the reference (LIGGGHTS allocates
+   freely on the host).  Its scratch is a file-scope device array in
+   libgranb200 of (GB2_NOALLOC_MAX_BLOCKS + 1) x 8 64-bit counters (1 MiB),
+   held by every GPU that loads the library until process exit, so it serves
+   at most GB2_NOALLOC_MAX_ATOMS owned atoms; larger contexts get
+   GB2_ERR_CAPACITY, an empty context gets zeros.  No cudaMalloc, cudaFree or
+   allocating library call is made.  The counts are read back synchronously
+   on the context's stream: the call returns once they are on the host.  The
+   first call on a device looks up the array's device address
    (cudaGetSymbolAddress); make that first call before any stream capture.
    All calls share the one array: two calls whose work overlaps on a GPU
    (different streams or host threads) race and may return wrong counts. */

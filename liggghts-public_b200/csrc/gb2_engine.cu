@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/granb200.h"
@@ -202,8 +203,53 @@ struct gb2_ctx {
     DBuf<uint8_t> insflag;
     DBuf<int> insidx;
     DBuf<dbl4> insrec;
-    ~gb2_ctx() { delete ins; }
+    // atom upload / download: pinned host staging and packed [n][3] planes on the device
+    void *hstage = nullptr;
+    size_t hstage_bytes = 0;
+    DBuf<double> iostage;
+    DBuf<int> iocheck;
+    ~gb2_ctx()
+    {
+        delete ins;
+        if (hstage) cudaFreeHost(hstage);
+    }
 };
+
+namespace {
+
+// host copy of large blocks split over a few threads (a single core copies
+// ~10 GB/s; the staging copies of a 1M-atom state are ~100 MB)
+void host_copy(void *dst, const void *src, size_t bytes)
+{
+    const size_t kChunk = size_t(8) << 20;
+    unsigned nt = std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()));
+    if (bytes < 2 * kChunk || nt < 2) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    nt = (unsigned)std::min<size_t>(nt, bytes / kChunk);
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (unsigned k = 0; k < nt; k++) {
+        const size_t a = k * per, b = std::min(bytes, a + per);
+        if (a >= b) break;
+        th.emplace_back([=] { std::memcpy((char *)dst + a, (const char *)src + a, b - a); });
+    }
+    for (auto &t : th) t.join();
+}
+
+// true when p is page-locked host memory the device can copy to or from directly
+bool host_pinned(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
 
 namespace {
 
@@ -233,6 +279,18 @@ int set_err(gb2_ctx *c, int code, const char *fmt, ...)
             return set_err(c, GB2_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__,       \
                            __LINE__);                                                                             \
     } while (0)
+
+// pinned host staging of at least `bytes` (grown, never shrunk)
+int host_stage(gb2_ctx *c, size_t bytes)
+{
+    if (bytes <= c->hstage_bytes) return 0;
+    if (c->hstage) cudaFreeHost(c->hstage);
+    c->hstage = nullptr;
+    c->hstage_bytes = 0;
+    CK(cudaHostAlloc(&c->hstage, bytes, cudaHostAllocDefault));
+    c->hstage_bytes = bytes;
+    return 0;
+}
 
 Dev make_dev(gb2_ctx *c)
 {
@@ -1267,32 +1325,46 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
 {
     if (!c || n <= 0 || !x || !v || !omega || !radius || !rmass || !type || !tag) return GB2_ERR_ARG;
     if (c->setup_done) return set_err(c, GB2_ERR_STATE, "atoms must be uploaded before setup");
-    for (int i = 0; i < n; i++) {
+    for (int i = 0; i < n; i++)
         if (type[i] < 1 || type[i] > c->P.ntypes) return set_err(c, GB2_ERR_ARG, "atom type out of range");
-        if (!(radius[i] > 0.0)) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
-        if (!(rmass[i] > 0.0)) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
-        for (int d = 0; d < 3; d++)
-            if (!std::isfinite(x[3 * i + d]) || !std::isfinite(v[3 * i + d]) || !std::isfinite(omega[3 * i + d]))
-                return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", i);
-    }
     c->nlocal = n;
     c->cap = (n + 31) / 32 * 32;
     c->nmax = 0;
     c->nghost = 0;
     if (ensure_nmax(c, n + n / 4 + 1024)) return GB2_ERR_CUDA;
-    std::vector<dbl4> hp(n), hv(n), hw(n);
     c->h_radius.assign(radius, radius + n);
     c->h_type.assign(type, type + n);
-    for (int i = 0; i < n; i++) {
-        hp[i] = {x[3 * i], x[3 * i + 1], x[3 * i + 2], radius[i]};
-        hv[i] = {v[3 * i], v[3 * i + 1], v[3 * i + 2], rmass[i]};
-        hw[i] = {omega[3 * i], omega[3 * i + 1], omega[3 * i + 2], 0.0};
+    // x | v | omega | radius | rmass staged as 11 n doubles, one host-to-device
+    // copy per array (straight from the caller's memory when it is pinned),
+    // packed into the 32-byte records and checked on the device
+    const size_t N = (size_t)n;
+    CK(c->iostage.alloc(11 * N));
+    CK(c->iocheck.alloc(2));
+    const double *src[5] = {x, v, omega, radius, rmass};
+    const size_t off[5] = {0, 3 * N, 6 * N, 9 * N, 10 * N}, len[5] = {3 * N, 3 * N, 3 * N, N, N};
+    if (host_stage(c, 11 * N * sizeof(double))) return GB2_ERR_CUDA;
+    for (int k = 0; k < 5; k++) {
+        const size_t bytes = len[k] * sizeof(double);
+        if (host_pinned(src[k])) {
+            CK(cudaMemcpyAsync(c->iostage.p + off[k], src[k], bytes, cudaMemcpyHostToDevice, c->st));
+        } else {
+            double *h = (double *)c->hstage + off[k];
+            host_copy(h, src[k], bytes);
+            CK(cudaMemcpyAsync(c->iostage.p + off[k], h, bytes, cudaMemcpyHostToDevice, c->st));
+        }
     }
-    CK(cudaMemcpyAsync(c->pos.p, hp.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->vel.p, hv.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->omg.p, hw.data(), sizeof(dbl4) * n, cudaMemcpyHostToDevice, c->st));
+    const int init[2] = {INT32_MAX, 0};
+    CK(cudaMemcpyAsync(c->iocheck.p, init, sizeof init, cudaMemcpyHostToDevice, c->st));
+    k_pack_atoms<<<nblk(n), kBlock, 0, c->st>>>(c->iostage.p, n, c->pos.p, c->vel.p, c->omg.p, c->iocheck.p);
+    CKL();
     CK(cudaMemcpyAsync(c->type.p, type, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->tag.p, tag, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+    int bad[2];
+    CK(cudaMemcpyAsync(bad, c->iocheck.p, sizeof bad, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (bad[1] == 2) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
+    if (bad[1] == 3) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
+    if (bad[1] == 1) return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", bad[0]);
     const size_t cap = c->cap;
     CK(c->f.alloc(cap));
     CK(c->tq.alloc(cap));
@@ -1960,6 +2032,10 @@ int gb2_census(gb2_ctx *c, gb2_contact_census *out)
 {
     if (!c || !out) return GB2_ERR_ARG;
     if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "census needs a neighbor list (call gb2_setup)");
+    if (c->nlocal == 0) {   // no atoms: nothing to launch
+        *out = gb2_contact_census{};
+        return 0;
+    }
     DBuf<unsigned long long> cnt;
     CK(cnt.alloc(8));
     CK(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), c->st));
@@ -1983,6 +2059,10 @@ int gb2_census_noalloc(gb2_ctx *c, gb2_contact_census *out)
 {
     if (!c || !out) return GB2_ERR_ARG;
     if (!c->setup_done) return set_err(c, GB2_ERR_STATE, "census needs a neighbor list (call gb2_setup)");
+    if (c->nlocal == 0) {   // no atoms: nothing to launch
+        *out = gb2_contact_census{};
+        return 0;
+    }
     const int nblocks = nblk(c->nlocal, 128);
     if (nblocks > GB2_NOALLOC_MAX_BLOCKS)
         return set_err(c, GB2_ERR_CAPACITY,
@@ -2031,23 +2111,51 @@ int gb2_download_atoms(gb2_ctx *c, int cap, int *n, double *x, double *v, double
     if (n) *n = c->nlocal;
     const int m = std::min(cap, c->nlocal);
     if (m <= 0) return 0;
-    std::vector<dbl4> b(m);
-    auto get4 = [&](const DBuf<dbl4> &src, double *dst) -> int {
-        if (!dst) return 0;
-        CK(cudaMemcpyAsync(b.data(), src.p, sizeof(dbl4) * m, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        for (int i = 0; i < m; i++) {
-            dst[3 * i] = b[i].x;
-            dst[3 * i + 1] = b[i].y;
-            dst[3 * i + 2] = b[i].z;
+    // the five [m][3] planes unpacked on the device into one block, one
+    // device-to-host copy per requested array (straight into the caller's
+    // memory when it is pinned, else through the pinned staging buffer)
+    const size_t M = (size_t)m;
+    CK(c->iostage.alloc(15 * M));
+    k_unpack_atoms<<<nblk(m), kBlock, 0, c->st>>>(c->pos.p, c->vel.p, c->omg.p, c->f.p, c->tq.p, m, c->iostage.p);
+    CKL();
+    double *dst[5] = {x, v, omega, f, torque};
+    if (host_stage(c, 15 * M * sizeof(double) + M * sizeof(int))) return GB2_ERR_CUDA;
+    bool staged[5] = {false, false, false, false, false};
+    for (int k = 0; k < 5; k++) {
+        if (!dst[k]) continue;
+        const size_t bytes = 3 * M * sizeof(double);
+        if (host_pinned(dst[k])) {
+            CK(cudaMemcpyAsync(dst[k], c->iostage.p + 3 * M * k, bytes, cudaMemcpyDeviceToHost, c->st));
+        } else {
+            CK(cudaMemcpyAsync((double *)c->hstage + 3 * M * k, c->iostage.p + 3 * M * k, bytes,
+                               cudaMemcpyDeviceToHost, c->st));
+            staged[k] = true;
         }
-        return 0;
-    };
-    if (get4(c->pos, x) || get4(c->vel, v) || get4(c->omg, omega) || get4(c->f, f) || get4(c->tq, torque))
+    }
+    if (tag) CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < 5; k++)
+        if (staged[k]) host_copy(dst[k], (double *)c->hstage + 3 * M * k, 3 * M * sizeof(double));
+    return 0;
+}
+
+int gb2_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr) return GB2_ERR_ARG;
+    *ptr = nullptr;
+    if (cudaHostAlloc(ptr, std::max<size_t>(bytes, 1), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
         return GB2_ERR_CUDA;
-    if (tag) {
-        CK(cudaMemcpyAsync(tag, c->tag.p, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
+    }
+    return 0;
+}
+
+int gb2_host_free(void *ptr)
+{
+    if (ptr && cudaFreeHost(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return GB2_ERR_CUDA;
     }
     return 0;
 }

@@ -54,6 +54,55 @@ __global__ void k_initial_integrate(Dev D, int check)
     }
 }
 
+// Atom upload: the caller's [n][3] arrays (x, v, omega) and per-atom radius
+// and mass, staged contiguously in `in` (x | v | omega | radius | rmass), packed
+// into the 32-byte records; the values are checked as the host used to
+// (finite state, positive radius and mass), the first bad atom recorded in
+// bad[0] (and its kind in bad[1]: 1 non-finite, 2 radius, 3 mass).
+__global__ void k_pack_atoms(const double *__restrict__ in, int n, dbl4 *pos, dbl4 *vel, dbl4 *omg, int *bad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double *x = in, *v = in + 3 * (size_t)n, *w = in + 6 * (size_t)n, *r = in + 9 * (size_t)n,
+                 *m = in + 10 * (size_t)n;
+    const double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2];
+    const double vi0 = v[3 * i], vi1 = v[3 * i + 1], vi2 = v[3 * i + 2];
+    const double wi0 = w[3 * i], wi1 = w[3 * i + 1], wi2 = w[3 * i + 2];
+    const double ri = r[i], mi = m[i];
+    int kind = 0;
+    if (!(ri > 0.0)) kind = 2;
+    else if (!(mi > 0.0)) kind = 3;
+    else if (!isfinite(xi0) || !isfinite(xi1) || !isfinite(xi2) || !isfinite(vi0) || !isfinite(vi1) ||
+             !isfinite(vi2) || !isfinite(wi0) || !isfinite(wi1) || !isfinite(wi2))
+        kind = 1;
+    if (kind) {
+        atomicMin(&bad[0], i);
+        atomicMax(&bad[1], kind);
+    }
+    pos[i] = dbl4{xi0, xi1, xi2, ri};
+    vel[i] = dbl4{vi0, vi1, vi2, mi};
+    omg[i] = dbl4{wi0, wi1, wi2, 0.0};
+}
+
+// Atom download: x, v, omega, f, torque of atoms [0, n) as five [n][3]
+// planes of `out` (one contiguous block for one device-to-host copy)
+__global__ void k_unpack_atoms(const dbl4 *__restrict__ pos, const dbl4 *__restrict__ vel,
+                               const dbl4 *__restrict__ omg, const dbl4 *__restrict__ f, const dbl4 *__restrict__ tq,
+                               int n, double *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const dbl4 *src[5] = {pos, vel, omg, f, tq};
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const dbl4 a = src[k][i];
+        double *o = out + (size_t)k * 3 * n + 3 * (size_t)i;
+        o[0] = a.x;
+        o[1] = a.y;
+        o[2] = a.z;
+    }
+}
+
 // Comm::forward_comm with AtomVecSphere::pack_comm_vel (src/comm.cpp:773):
 // ghost = owned source + accumulated periodic shift
 __global__ void k_forward_comm(Dev D)

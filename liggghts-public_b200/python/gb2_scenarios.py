@@ -212,6 +212,143 @@ def hopper(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z=32, ha
     return sc
 
 
+def _hex_annulus(a, rho_in, rho_out):
+    """Sites of a triangular lattice of spacing a (centred on the axis) with
+    rho_in <= rho <= rho_out, innermost first (ties in lattice order)."""
+    m = int(rho_out / a * 1.2) + 2
+    i, j = np.meshgrid(np.arange(-m, m + 1), np.arange(-m, m + 1), indexing="ij")
+    x = a * (i + 0.5 * j).ravel()
+    y = a * (0.5 * math.sqrt(3.0) * j).ravel()
+    r2 = x * x + y * y
+    keep = (r2 <= rho_out * rho_out) & (r2 >= rho_in * rho_in)
+    x, y, r2 = x[keep], y[keep], r2[keep]
+    order = np.argsort(r2, kind="stable")
+    return x[order], y[order]
+
+
+def hopper_packed(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z=32, half_angle_deg=60.0,
+                  r_out=0.015, floor_drop=0.08, overlap=1e-4, band=2e-3, wall_overlap=2e-3, sortfreq=1000):
+    """Packed conical hopper at the start of its discharge (config 2's state).
+
+    Radii as ``hopper`` (lognormal, median 1 mm, sigma 0.25, clipped to
+    0.5-2 mm), sorted largest first and stacked bottom-up in horizontal
+    layers.  A layer is filled from the axis outwards in annular patches,
+    each a triangular lattice holding particles of one narrow radius band
+    (at most ``band`` relative) whose spacing is (1 - overlap) x the
+    smallest diameter in the patch, so every in-plane neighbour pair inside
+    a patch touches (overlaps of 1e-4 to ~5e-3 of a diameter); patches are
+    one diameter apart.  Layers are a sum of their largest radii apart, so
+    layers do not overlap.  Every other angular bin
+    of the outermost ring is pushed horizontally outwards until it overlaps
+    the triangulated cone wall by ``wall_overlap`` of its radius (its facet
+    plane), which gives tens of thousands of mesh contacts at 1M particles;
+    a clear ring of one diameter separates those from the lattice.  The 30 mm
+    outlet is open and the particles start at rest, so the bed starts to
+    discharge onto the catch floor ``floor_drop`` below the outlet."""
+    rng = np.random.default_rng(seed)
+    rad = np.exp(rng.normal(math.log(1e-3), 0.25, size=n))
+    rad = np.clip(rad, 0.5e-3, 2e-3)
+    rad = np.sort(rad)[::-1].copy()
+    th = math.radians(half_angle_deg)
+    t = math.tan(th)
+    # facet planes of the triangulated cone (a quad between two generators
+    # is planar and contains the apex): inward unit normal and a point
+    phis = np.linspace(0.0, 2.0 * math.pi, n_theta + 1)
+    p0 = np.stack([r_out * np.cos(phis[:-1]), r_out * np.sin(phis[:-1]), np.zeros(n_theta)], axis=1)
+    p1 = np.stack([r_out * np.cos(phis[1:]), r_out * np.sin(phis[1:]), np.zeros(n_theta)], axis=1)
+    r1 = r_out + 1.0 * t
+    p2 = np.stack([r1 * np.cos(phis[:-1]), r1 * np.sin(phis[:-1]), np.ones(n_theta)], axis=1)
+    nrm = np.cross(p1 - p0, p2 - p0)
+    nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+    nrm *= np.where((nrm[:, 0] * np.cos(phis[:-1]) + nrm[:, 1] * np.sin(phis[:-1])) > 0, -1.0, 1.0)[:, None]
+    pos = np.zeros((n, 3))
+    chunk = max(200, n // 500)
+    placed = 0
+    zbot = 0.5e-3
+    while placed < n:
+        rmax = rad[placed]
+        zc = zbot + rmax
+        R = r_out + zc * t
+        # a sphere of radius r touches the cone at rho = R - r / cos(half angle); keep one diameter clear
+        rho_lim = R - rmax * (1.0 - wall_overlap) / math.cos(th) - 2.1 * rmax
+        if rho_lim <= rmax:
+            zbot += 2.0 * rmax
+            continue
+        # the layer is filled from the axis outwards in annular patches of at
+        # most `chunk` particles, each a lattice whose spacing is the smallest
+        # diameter of its particles (narrow radius band per patch); patches
+        # are one diameter apart
+        rho_in, last = 0.0, None
+        while placed < n:
+            r0 = rad[placed]
+            x, y = _hex_annulus(2.0 * r0, rho_in, rho_lim)
+            if len(x) == 0:
+                break
+            # at most `chunk` particles and a radius band of at most `band` (relative)
+            j = int(np.searchsorted(-rad, -r0 / (1.0 + band), side="right"))
+            take = max(1, min(len(x), chunk, n - placed, j - placed))
+            a = 2.0 * rad[placed + take - 1] * (1.0 - overlap)
+            x, y = _hex_annulus(a, rho_in, rho_lim)
+            take = min(take, len(x))
+            if take == 0:
+                break
+            x, y = x[:take], y[:take]
+            sl = slice(placed, placed + take)
+            pos[sl, 0], pos[sl, 1], pos[sl, 2] = x, y, zc
+            last = (placed, take, a)
+            placed += take
+            rho_in = np.hypot(x, y).max() + 2.0 * r0 + 1e-7
+        if last is not None and last[1] > 7:
+            # outermost band of the outermost patch, in angular order: a
+            # particle is pushed outwards onto the wall when it is at least
+            # 2.05 rmax of arc from the last one pushed (and from the first)
+            p0_, take, a = last
+            idx = np.arange(p0_, p0_ + take)
+            x, y = pos[idx, 0], pos[idx, 1]
+            rho = np.hypot(x, y)
+            phi = np.arctan2(y, x) % (2.0 * math.pi)
+            dphi = 2.05 * rmax / max(R - rmax / math.cos(th), rmax)
+            cand = np.flatnonzero(rho > rho.max() - a)
+            cand = cand[np.argsort(phi[cand], kind="stable")]
+            chosen = []
+            for c in cand:
+                if not chosen or phi[c] - phi[chosen[-1]] >= dphi:
+                    if not chosen or phi[chosen[0]] + 2.0 * math.pi - phi[c] >= dphi:
+                        chosen.append(c)
+            sel = np.array(sorted(chosen), dtype=np.int64)
+            if len(sel):
+                k = np.minimum((phi[sel] / (2.0 * math.pi) * n_theta).astype(int), n_theta - 1)
+                e = np.stack([np.cos(phi[sel]), np.sin(phi[sel]), np.zeros(len(sel))], axis=1)
+                pts = np.stack([x[sel], y[sel], np.full(len(sel), zc)], axis=1)
+                dist = np.einsum("ij,ij->i", pts - p0[k], nrm[k])
+                en = np.einsum("ij,ij->i", e, nrm[k])
+                dh = (dist - rad[idx[sel]] * (1.0 - wall_overlap)) / (-en)
+                pos[idx[sel], 0] = x[sel] + dh * e[:, 0]
+                pos[idx[sel], 1] = y[sel] + dh * e[:, 1]
+        zbot = zc + rmax + 1e-7
+    height = pos[:, 2].max() + 0.01
+    nodes = cone_mesh(n_theta, n_z, r_out, half_angle_deg, height)
+    rtop = r_out + height * t
+    lo = [-(rtop + 0.01), -(rtop + 0.01), -floor_drop - 0.01]
+    hi = [rtop + 0.01, rtop + 0.01, height + 0.02]
+    sc = {
+        "name": "hopper_packed",
+        "dt": dt, "skin": skin,
+        "boxlo": lo, "boxhi": hi, "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": sortfreq, "sortbinsize": 0.0,
+        "rolling_cdt": 1, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2500.0, np.zeros((n, 3))),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_mesh", "nodes": nodes, "wall_type": 1, "curvature": 0.0, "rolling_cdt": 1},
+            {"kind": "wall_plane", "dim": 2, "pos": -floor_drop, "wall_type": 1, "rolling_cdt": 1},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5, 0.1))
+    return sc
+
+
 def plate_mesh(half=0.025, z=0.0, k=8):
     """Square plate at height z, side 2 * half, 2 * k * k triangles (normal +z)."""
     g = np.linspace(-half, half, k + 1)

@@ -32,7 +32,7 @@ EXPORTS = (
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
     "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
-    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear",
+    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_host_alloc", "gb2_host_free",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -265,6 +265,8 @@ def lib(path=LIB_PATH):
         L.gb2_add_wall_cylinder.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_int, ctypes.c_int]
         L.gb2_download_mesh_nodes.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, D, D]
+        L.gb2_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.gb2_host_free.argtypes = [vp]
         _LIB = L
     return _LIB
 
@@ -279,6 +281,23 @@ def _ip(a):
 
 class GB2Error(RuntimeError):
     pass
+
+
+def pinned_empty(shape, dtype=np.float64):
+    """A numpy array in page-locked host memory (gb2_host_alloc): the
+    library's atom upload and download copy it with the device directly.
+    The memory is released (gb2_host_free) when the array is collected."""
+    import weakref
+    L = lib()
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    ptr = ctypes.c_void_p()
+    if L.gb2_host_alloc(max(nbytes, 1), ctypes.byref(ptr)) != 0:
+        raise GB2Error("gb2_host_alloc of %d bytes failed" % nbytes)
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(ptr.value)
+    arr = np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
+    weakref.finalize(buf, L.gb2_host_free, ptr)
+    return arr
 
 
 class Engine:
@@ -426,10 +445,14 @@ class Engine:
         self.n = cnt0.value
         return self.n
 
-    def atoms(self):
+    def atoms(self, out=None):
+        """x, v, omega, f, torque [n][3] and tag [n] of the owned atoms; `out`
+        may hold preallocated arrays (e.g. pinned_empty) of the right shape."""
         n = self.count()
-        out = {k: np.zeros((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
-        tag = np.zeros(n, dtype=np.int32)
+        if out is None or len(out["tag"]) != n:
+            out = {k: np.zeros((n, 3)) for k in ("x", "v", "omega", "f", "torque")}
+            out["tag"] = np.zeros(n, dtype=np.int32)
+        tag = out["tag"]
         cnt = ctypes.c_int()
         self._check(self.L.gb2_download_atoms(self.h, n, ctypes.byref(cnt), _dp(out["x"]), _dp(out["v"]),
                                               _dp(out["omega"]), _dp(out["f"]), _dp(out["torque"]), _ip(tag)))

@@ -51,8 +51,13 @@ def _drum():
     return sc
 
 
+def _hopper_packed():
+    return S.hopper_packed(n=6000, n_theta=48, n_z=12, band=0.02, sortfreq=200)
+
+
 # name -> (scenario builder, run segments); segment 0 is the setup
 SCENES = {
+    "hopper_packed_discharge": (_hopper_packed, [0, 200, 200, 200, 200, 200]),
     "pour3k_rolling": (_pour3k, [0, 150, 150, 150, 150]),
     "two_types_schedule": (_two_types, [0, 300, 300, 300, 300]),
     "hopper_mesh": (_hopper_mesh, [0, 300, 300, 300, 300, 300]),
@@ -73,6 +78,7 @@ SCENES = {
 # reference needs ~110 s); pinned by committed digests and run on the GPU.
 LONG_SCENES = {
     "config1_pour_20k_20000steps": (S.sphere_pour, [0, 20000]),
+    "config2_hopper_1M_100steps": (S.hopper_packed, [0, 100]),
 }
 
 ALL_SCENES = dict(SCENES, **LONG_SCENES)

@@ -43,15 +43,19 @@ def test_allmax_over_two_ranks(tmp_path):
 
 @pytest.mark.timeout(600)
 def test_reference_arm_two_ranks():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.build():
+        pytest.skip("reference not built and its sources are absent")
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--workload", "pour", "--steps", "3", "--warmup", "1",
-           "--settle", "2", "--gpus", "2"]
+           "--impl", "reference", "--workload", "pour", "--particles", "2000", "--steps", "3", "--warmup", "1",
+           "--gpus", "2"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0
-    assert d["cpu_baseline"]["kind"] in ("port", "reference")
+    assert d["cpu_baseline"]["kind"] == "reference" and d["steps"] == 3 and d["warmup"] == 3

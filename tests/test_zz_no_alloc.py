@@ -1,8 +1,10 @@
 """gb2_census_noalloc -- the census entry point for callers that cannot
-allocate device memory (for example code running while a stream is captured
-into a CUDA graph, or a monitoring hook inside a framework that owns all
-allocations).  Its scratch is a static device array inside libgranb200, so
-its counts must equal those of the allocating gb2_census, call after call.
+allocate device memory (a monitoring hook inside a framework whose pool owns
+every device allocation, or a process at its device-memory cap).  Its
+scratch is a static device array inside libgranb200, so its counts must
+equal those of the allocating gb2_census, call after call.  (A context with
+no atoms, answered with zeros before any launch, cannot be built through the
+ABI: gb2_upload_atoms needs at least one atom.)
 
 This file is collected last so that a failure here cannot hide the result of
 any other test in a run that stops at the first failure.
