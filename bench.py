@@ -374,14 +374,14 @@ def long_window(eng, steps, dist, device):
     Rebuild cost per step = the device time of the sampled rebuild steps'
     rebuild kernels, scaled to all rebuilds, over the window's steps."""
     W = timed_window(eng, steps, dist, device, clocks=False)
-    st = eng.stats()
-    out = {"steps": steps, "ms_per_step": W["ms"] / steps, "rebuilds": W["rebuilds"],
-           "kernel_ms_per_step": W["kernel_ms_per_step"], "census_end": W["cen"][1], "launches": W["launches"],
-           "capacity_growth": W["growth"]}
-    # t_rebuild is recorded on sampled steps only; those that rebuilt give the cost of one rebuild
-    out["note"] = ("rebuild kernels timed with CUDA events on the sampled steps; t_rebuild per sampled step "
-                   "averages rebuild and non-rebuild steps alike")
-    out["rebuild_ms_per_step"] = W["kernel_ms_per_step"]["t_rebuild"]
+    nreb = max(W["rebuilds"], 0)
+    out = {"steps": steps, "ms_per_step": W["ms"] / steps, "rebuilds": nreb,
+           "kernel_ms_per_step": W["kernel_ms_per_step"], "census_start": W["cen"][0], "census_end": W["cen"][1],
+           "launches": W["launches"], "capacity_growth": W["growth"],
+           "rebuild_ms_each": W["kt"]["t_rebuild"] / nreb if nreb else None,
+           "rebuild_ms_per_step": W["kt"]["t_rebuild"] / steps,
+           "note": "every rebuild timed with CUDA events (rebuild kernels, device time); the other kernels on "
+                   "every %dth step" % PROFILE_EVERY}
     return out, W
 
 

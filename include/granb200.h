@@ -93,6 +93,7 @@ typedef struct {
     long nsteps_rebuild;         /* steps that rebuilt the neighbour list   */
     int maxrev, maxmesh;         /* reverse-entry and mesh-slot capacities  */
     long ngrow;                  /* capacity growths (device reallocations) */
+    long n_rebuild_timed;        /* rebuilds timed into t_rebuild (all, while profiling) */
 } gb2_stats;
 
 /* contact census of the current state (device reduction): half-list entries,
@@ -214,6 +215,10 @@ int gb2_insert_stats(gb2_ctx *ctx, int ifix, long *ninserted, double *massinsert
 int gb2_download_mesh_nodes(gb2_ctx *ctx, int ifix, int cap, int *ntri, double *nodes, double *vnode);
 
 /* Verlet::setup and Verlet::run(nsteps) */
+/* update->ntimestep at the start of the run (default 0): sets the step the
+   atom-sort schedule counts from (Atom::sort's nextsort, src/atom.cpp:1315);
+   call before gb2_setup */
+int gb2_set_timestep(gb2_ctx *ctx, long ntimestep);
 int gb2_setup(gb2_ctx *ctx);
 int gb2_run(gb2_ctx *ctx, int nsteps);
 /* block until all device work of this context has finished */

@@ -197,6 +197,7 @@ struct gb2_ctx {
     std::vector<EvPair> ev_free, ev_pending;
     double prof_ms[5] = {0, 0, 0, 0, 0};
     long n_pair_main = 0;
+    long n_rebuild_timed = 0;
     // fix insert/pack (at most one)
     InsertPack *ins = nullptr;
     long maxtag = 0;
@@ -427,7 +428,9 @@ enum { PROF_INTEGRATE = 0, PROF_PAIR_TAIL = 1, PROF_PAIR_MAIN = 2, PROF_FORWARD 
 int prof_begin(gb2_ctx *c, int cls, gb2_ctx::EvPair *out)
 {
     out->cls = -1;
-    if (!c->prof || (c->prof_every > 1 && c->ntimestep % c->prof_every != 0)) return 0;
+    // rebuilds are timed whenever profiling is on (they are rare, and no
+    // dependent launch follows them); the other kinds on sampled steps
+    if (!c->prof || (cls != PROF_REBUILD && c->prof_every > 1 && c->ntimestep % c->prof_every != 0)) return 0;
     if (c->ev_free.empty()) {
         gb2_ctx::EvPair e;
         CK(cudaEventCreate(&e.a));
@@ -459,6 +462,7 @@ void prof_resolve(gb2_ctx *c)
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) c->prof_ms[e.cls] += ms;
             if (e.cls == PROF_PAIR_MAIN) c->n_pair_main++;
+            if (e.cls == PROF_REBUILD) c->n_rebuild_timed++;
             c->ev_free.push_back(e);
         } else
             c->ev_pending[keep++] = e;
@@ -1342,7 +1346,9 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     CK(c->iocheck.alloc(2));
     const double *src[5] = {x, v, omega, radius, rmass};
     const size_t off[5] = {0, 3 * N, 6 * N, 9 * N, 10 * N}, len[5] = {3 * N, 3 * N, 3 * N, N, N};
-    if (host_stage(c, 11 * N * sizeof(double))) return GB2_ERR_CUDA;
+    bool pageable = false;
+    for (int k = 0; k < 5; k++) pageable = pageable || !host_pinned(src[k]);
+    if (pageable && host_stage(c, 11 * N * sizeof(double))) return GB2_ERR_CUDA;
     for (int k = 0; k < 5; k++) {
         const size_t bytes = len[k] * sizeof(double);
         if (host_pinned(src[k])) {
@@ -1669,6 +1675,14 @@ int gb2_download_mesh_nodes(gb2_ctx *c, int ifix, int cap, int *ntri, double *no
             std::memset(vnode, 0, sizeof(double) * 9 * n);
         }
     }
+    return 0;
+}
+
+int gb2_set_timestep(gb2_ctx *c, long ntimestep)
+{
+    if (!c || ntimestep < 0) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "the start step is set before setup");
+    c->ntimestep = ntimestep;
     return 0;
 }
 
@@ -2119,7 +2133,9 @@ int gb2_download_atoms(gb2_ctx *c, int cap, int *n, double *x, double *v, double
     k_unpack_atoms<<<nblk(m), kBlock, 0, c->st>>>(c->pos.p, c->vel.p, c->omg.p, c->f.p, c->tq.p, m, c->iostage.p);
     CKL();
     double *dst[5] = {x, v, omega, f, torque};
-    if (host_stage(c, 15 * M * sizeof(double) + M * sizeof(int))) return GB2_ERR_CUDA;
+    bool pageable = false;
+    for (int k = 0; k < 5; k++) pageable = pageable || (dst[k] && !host_pinned(dst[k]));
+    if (pageable && host_stage(c, 15 * M * sizeof(double))) return GB2_ERR_CUDA;
     bool staged[5] = {false, false, false, false, false};
     for (int k = 0; k < 5; k++) {
         if (!dst[k]) continue;
@@ -2647,6 +2663,7 @@ int gb2_get_stats(gb2_ctx *c, gb2_stats *s)
     s->time_neigh = s->t_rebuild;
     s->time_other = s->t_integrate + s->t_forward;
     s->n_pair_main = c->n_pair_main;
+    s->n_rebuild_timed = c->n_rebuild_timed;
     s->nsteps_rebuild = c->nsteps_rebuild;
     s->maxrev = c->maxr;
     for (int k = 0; k < c->nfix; k++)

@@ -32,7 +32,7 @@ EXPORTS = (
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
     "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
-    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_host_alloc", "gb2_host_free",
+    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_host_alloc", "gb2_host_free", "gb2_set_timestep",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -204,6 +204,7 @@ class Stats(ctypes.Structure):
         ("maxrev", ctypes.c_int),
         ("maxmesh", ctypes.c_int),
         ("ngrow", ctypes.c_long),
+        ("n_rebuild_timed", ctypes.c_long),
     ]
 
 
@@ -267,6 +268,7 @@ def lib(path=LIB_PATH):
         L.gb2_download_mesh_nodes.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, D, D]
         L.gb2_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
         L.gb2_host_free.argtypes = [vp]
+        L.gb2_set_timestep.argtypes = [vp, ctypes.c_long]
         _LIB = L
     return _LIB
 

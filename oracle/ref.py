@@ -23,6 +23,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")
 HARNESS = os.path.join(REF_DIR, "ref_harness")
 LMP = os.path.join(REF_DIR, "lmp_ref")
+# the reference with the b200 suffix styles (Makefile.ref target b200)
+HARNESS_B200 = os.path.join(REF_DIR, "ref_harness_b200")
+LMP_B200 = os.path.join(REF_DIR, "lmp_b200")
 REF_SRC = "/root/reference/src"
 
 
@@ -254,19 +257,41 @@ def read_dump(path):
     return out
 
 
-def run(sc, segments, keep=None):
+def available_b200():
+    return os.path.exists(HARNESS_B200) and os.path.exists(LMP_B200)
+
+
+def build_b200(jobs=8):
+    """Build the reference with the b200 suffix styles (needs the built
+    libgranb200.so and the reference sources)."""
+    if available_b200():
+        return True
+    if not os.path.isdir(REF_SRC) or not build(jobs):
+        return False
+    subprocess.run(["make", "-s", "-f", "Makefile.ref", "-j%d" % jobs, "REF=" + REF_SRC, "b200"], cwd=_HERE,
+                   check=True)
+    return available_b200()
+
+
+def run(sc, segments, keep=None, harness=None, extra_args=(), script_lines=None):
     """Run the scenario in the reference: setup + segments[0] steps, then
-    each further segment as a continued run; returns one dump per segment."""
-    if not available():
+    each further segment as a continued run; returns one dump per segment.
+    harness/extra_args select another harness build and LAMMPS command-line
+    arguments (e.g. HARNESS_B200 with "-sf b200"); script_lines replaces the
+    generated input script (its "#@dump s<k>" lines name the dumps)."""
+    harness = harness or HARNESS
+    if not os.path.exists(harness):
         raise RuntimeError("reference harness not built (oracle/Makefile.ref)")
     wd = keep or tempfile.mkdtemp(prefix="gb2ref_")
     os.makedirs(wd, exist_ok=True)
     try:
         write_data(os.path.join(wd, "data.txt"), sc)
         names = ["s%d" % i for i in range(len(segments))]
+        lines = script(sc, wd, segments, names) if script_lines is None else script_lines(wd)
         with open(os.path.join(wd, "in.case"), "w") as f:
-            f.write("\n".join(script(sc, wd, segments, names)) + "\n")
-        r = subprocess.run([HARNESS, os.path.join(wd, "in.case"), wd], capture_output=True, text=True)
+            f.write("\n".join(lines) + "\n")
+        r = subprocess.run([harness, os.path.join(wd, "in.case"), wd] + list(extra_args), capture_output=True,
+                           text=True)
         if r.returncode != 0 or not os.path.exists(os.path.join(wd, names[-1] + ".bin")):
             tail = ""
             for fn in ("screen.txt", "log.lammps"):

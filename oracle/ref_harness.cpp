@@ -5,8 +5,9 @@
  * TEST INFRASTRUCTURE ONLY: the checker that pins the oracle and the engine to
  * the reference itself.  Nothing in the product links or runs it.
  *
- *   ref_harness <script> <outdir>
+ *   ref_harness <script> <outdir> [lammps command-line arguments...]
  *
+ * (e.g. "-sf b200" on the build that includes the b200 suffix styles).
  * Every script line goes to lammps_command (src/library.cpp:129) on an
  * instance made by lammps_open_no_mpi (src/library.cpp:88), except lines
  * "#@dump <name>", which write <outdir>/<name>.bin, and other comments.
@@ -162,7 +163,7 @@ void dump_state(LAMMPS *lmp, const std::string &path)
     int k = 0;
     for (int ifix = 0; ifix < lmp->modify->nfix; ifix++) {
         Fix *fx = lmp->modify->fix[ifix];
-        if (strcmp(fx->style, "wall/gran") != 0) continue;
+        if (strncmp(fx->style, "wall/gran", 9) != 0) continue;   // wall/gran and its suffixed forms
         FixWallGran *fw = dynamic_cast<FixWallGran *>(fx);
         char nm[32];
         if (!fw->is_mesh_wall()) {
@@ -241,8 +242,8 @@ void dump_state(LAMMPS *lmp, const std::string &path)
 
 int main(int argc, char **argv)
 {
-    if (argc != 3) {
-        fprintf(stderr, "usage: ref_harness <script> <outdir>\n");
+    if (argc < 3) {
+        fprintf(stderr, "usage: ref_harness <script> <outdir> [lammps arguments...]\n");
         return 2;
     }
     std::ifstream in(argv[1]);
@@ -252,10 +253,12 @@ int main(int argc, char **argv)
     }
     const std::string out = argv[2];
     const std::string logf = out + "/log.lammps", scr = out + "/screen.txt";
-    char *args[] = {(char *)"ref_harness", (char *)"-log", (char *)logf.c_str(), (char *)"-screen",
-                    (char *)scr.c_str(), (char *)"-echo", (char *)"log", NULL};
+    std::vector<char *> args = {(char *)"ref_harness", (char *)"-log", (char *)logf.c_str(), (char *)"-screen",
+                                (char *)scr.c_str(), (char *)"-echo", (char *)"log"};
+    for (int a = 3; a < argc; a++) args.push_back(argv[a]);
+    args.push_back(NULL);
     void *handle = NULL;
-    lammps_open_no_mpi(7, args, &handle);
+    lammps_open_no_mpi((int)args.size() - 1, args.data(), &handle);
     LAMMPS *lmp = (LAMMPS *)handle;
     std::string line;
     while (std::getline(in, line)) {

@@ -102,14 +102,18 @@ def contact_whitelist(src):
     return "".join(lines)
 
 
-def main(src, out):
+def main(src, out, extra=()):
+    """Style headers for the sources in src plus the style files in the
+    directories `extra` (the b200 suffix styles, as if dropped into src)."""
     os.makedirs(out, exist_ok=True)
     for macro, prefix, name in STYLES:
         files = []
-        for h in sorted(glob.glob(os.path.join(src, prefix + "*.h"))):
-            with open(h, errors="replace") as f:
-                if macro in f.read():
-                    files.append(os.path.basename(h))
+        for d in (src,) + tuple(extra):
+            for h in glob.glob(os.path.join(d, prefix + "*.h")):
+                with open(h, errors="replace") as f:
+                    if macro in f.read():
+                        files.append(os.path.basename(h))
+        files.sort()
         _write(os.path.join(out, "style_%s.h" % name), "".join('#include "%s"\n' % b for b in files))
     with open(os.path.join(src, "version_liggghts.txt")) as f:
         vers = f.read().strip()
@@ -121,4 +125,4 @@ def main(src, out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2])
+    main(sys.argv[1], sys.argv[2], tuple(sys.argv[3:]))
