@@ -292,6 +292,8 @@ void VerletB200::build_context()
         ph.insert(ph.end(), h, h + 3);
       }
     }
+    pt.resize(pt.size() + 1);   // non-null buffers when no atom has a partner
+    ph.resize(ph.size() + 3);
     check(gb2_upload_history(ctx_, n, np.data(), pt.data(), ph.data()), "gb2_upload_history");
   }
   for (size_t k = 0; k < walls_.size(); k++) {
@@ -316,6 +318,8 @@ void VerletB200::build_context()
         const double *h = cm->contacthistory(i, j);
         hist.insert(hist.end(), h, h + 3);
       }
+    tri.resize(tri.size() + 1);
+    hist.resize(hist.size() + 3);
     check(gb2_upload_mesh_history(ctx_, mesh_ifix_[k], n, np.data(), tri.data(), hist.data()),
           "gb2_upload_mesh_history");
   }
