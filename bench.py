@@ -443,10 +443,10 @@ def own_arm(args):
         kt_src, npm, cen_src, src = W["kt"], W["npm"], W["cen"], "headline window"
     dom_ms = kt_src["t_pair_main"] / max(npm, 1)
     ab = algorithmic_bytes(n, cen_src, nfix_plane, nfix_mesh, False)
-    achieved = ab / (dom_ms * 1e-3) / 1e9
+    achieved = ab / (dom_ms * 1e-3) / 1e9 if npm > 0 and dom_ms > 0 else None
     traffic = load_traffic(dom, args.workload)
     line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                        "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                         "traffic": traffic["bytes_per_launch"] if traffic else None,
                         "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms, "sampled_launches": npm,
                         "timing": "pair-step launches timed with CUDA events on every %dth step of the %s"

@@ -11,7 +11,12 @@ configurations name:
 * ``hopper``       -- polydisperse spheres (lognormal radius, median 1 mm,
   sigma 0.25, clipped to 0.5-2 mm) with Hertz/history + rolling friction cdt
   in a procedurally triangulated conical hopper (60 deg half-angle, 30 mm
-  outlet) discharging onto a flat catch floor.
+  outlet) discharging onto a flat catch floor; ``hopper_packed`` is the same
+  hopper packed at the start of its discharge (configuration 2's state).
+* ``drum_config3`` -- configuration 3: 8M spheres packed in the bottom of a
+  0.5 m drum of 32,768 triangles turned by ``fix move/mesh rotate``.
+* ``bed_config5``  -- configuration 5: 20M spheres of r = 0.5 mm in hexagonal
+  close packing over a 65,536-triangle bumpy plate in a walled box.
 
 A scenario is a plain dict (box, materials, atoms, ordered fix list) that the
 engine wrapper and the tests both consume.  Units are SI throughout.
@@ -249,6 +254,7 @@ def hopper_packed(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z
     rad = np.exp(rng.normal(math.log(1e-3), 0.25, size=n))
     rad = np.clip(rad, 0.5e-3, 2e-3)
     rad = np.sort(rad)[::-1].copy()
+    neg_rad = -rad   # ascending, for the band searches
     th = math.radians(half_angle_deg)
     t = math.tan(th)
     # facet planes of the triangulated cone (a quad between two generators
@@ -285,7 +291,7 @@ def hopper_packed(n=1_000_000, seed=2024, dt=5e-6, skin=0.5e-3, n_theta=128, n_z
             if len(x) == 0:
                 break
             # at most `chunk` particles and a radius band of at most `band` (relative)
-            j = int(np.searchsorted(-rad, -r0 / (1.0 + band), side="right"))
+            j = int(np.searchsorted(neg_rad, -r0 / (1.0 + band), side="right"))
             take = max(1, min(len(x), chunk, n - placed, j - placed))
             a = 2.0 * rad[placed + take - 1] * (1.0 - overlap)
             x, y = _hex_annulus(a, rho_in, rho_lim)
@@ -501,6 +507,215 @@ def drum(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length=0.85, n
         ],
     }
     sc.update(_materials(1, 1e7, 0.45, 0.5, 0.4))
+    return sc
+
+
+def _hex_rect(a, x0, x1, y0, y1):
+    """Sites of a triangular lattice of spacing a (rows along x) inside the
+    rectangle [x0, x1] x [y0, y1], ordered by x then y."""
+    h = 0.5 * math.sqrt(3.0) * a
+    j = np.arange(int(math.ceil(y0 / h)) - 1, int(math.floor(y1 / h)) + 2)
+    y = j * h
+    j = j[(y >= y0) & (y <= y1)]
+    off = 0.5 * a * (j % 2)
+    lo = np.ceil((x0 - off) / a).astype(np.int64)
+    hi = np.floor((x1 - off) / a).astype(np.int64)
+    cnt = np.maximum(hi - lo + 1, 0)
+    total = int(cnt.sum())
+    if total == 0:
+        return np.zeros(0), np.zeros(0)
+    start = np.repeat(np.cumsum(cnt) - cnt, cnt)
+    i = np.repeat(lo, cnt) + (np.arange(total) - start)
+    x = i * a + np.repeat(off, cnt)
+    yy = np.repeat(j, cnt) * h
+    order = np.lexsort((yy, x))
+    return x[order], yy[order]
+
+
+def drum_config3(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length=0.85, n_theta=128, n_ax=121,
+                 cap_rings=4, omega=2.0, margin=0.01, clearance=1.5e-3, overlap=1e-4, band=2e-3,
+                 wall_overlap=2e-3, sortfreq=1000):
+    """Rotating drum of configuration 3, packed at the start of the run.
+
+    Radii U(0.8, 1.2) mm sorted largest first, density 2700, E 1e7, nu 0.45,
+    e 0.5, mu 0.4; drum ``diameter`` x ``length`` (0.85 m gives the 35 %% fill
+    for 8M spheres) of 32,768 triangles turning at ``omega`` rad/s about x.
+    Horizontal layers from the bottom of the drum, each filled along x with
+    patches of a triangular lattice holding one narrow radius band (spacing
+    (1 - overlap) x the smallest diameter of the patch, patches one diameter
+    apart), so neighbours inside a patch touch; in every other lattice row
+    the outermost particle of each column is pushed sideways onto the drum's
+    facet plane (overlap ``wall_overlap`` of its radius), giving wall
+    contacts all along the drum."""
+    rng = np.random.default_rng(seed)
+    rad = np.sort(rng.uniform(0.8e-3, 1.2e-3, size=n))[::-1].copy()
+    neg_rad = -rad   # ascending, for the band searches
+    R = 0.5 * diameter
+    pos = np.zeros((n, 3))
+    placed = 0
+    z = -R + clearance
+    xlo, xhi = -0.5 * length + clearance, 0.5 * length - clearance
+    dth = 2.0 * math.pi / n_theta
+    chunk = max(200, n // 4000)
+    while placed < n:
+        rmax = rad[placed]
+        zc = z + rmax
+        if zc + rmax > R - clearance:
+            raise ValueError("drum too small for %d particles" % n)
+        half = math.sqrt(max((R - clearance - rmax) ** 2 - zc ** 2, 0.0)) - 2.1 * rmax
+        if half <= rmax:
+            z += 2.0 * rmax
+            continue
+        x_in = xlo + rmax
+        patches = []
+        while placed < n and x_in < xhi - rmax:
+            r0 = rad[placed]
+            jb = int(np.searchsorted(neg_rad, -r0 / (1.0 + band), side="right"))
+            want = max(1, min(n - placed, jb - placed, chunk))
+            # a window along x long enough for `want` sites (the lattice holds
+            # 2 half / (a h) sites per unit length), not the rest of the layer
+            xw = min(xhi - r0, x_in + 1.5 * want * (2.0 * r0) ** 2 * 0.87 / (2.0 * half) + 8.0 * r0)
+            x, y = _hex_rect(2.0 * r0, x_in, xw, -half, half)
+            if len(x) < want and xw < xhi - r0:
+                xw = xhi - r0
+                x, y = _hex_rect(2.0 * r0, x_in, xw, -half, half)
+            if len(x) == 0:
+                break
+            take = max(1, min(len(x), want))
+            a = 2.0 * rad[placed + take - 1] * (1.0 - overlap)
+            x, y = _hex_rect(a, x_in, xw, -half, half)
+            take = min(take, len(x))
+            if take == 0:
+                break
+            x, y = x[:take], y[:take]
+            sl = slice(placed, placed + take)
+            pos[sl, 0], pos[sl, 1], pos[sl, 2] = x, y, zc
+            patches.append((placed, take, a))
+            placed += take
+            x_in = x.max() + 2.0 * r0 + 1e-7
+        # in even lattice rows (columns one spacing apart) the outermost
+        # particle of every column, at both ends in y, onto the side wall
+        for p0, take, ap in patches:
+            idx = np.arange(p0, p0 + take)
+            row = np.rint(pos[idx, 1] / (0.5 * math.sqrt(3.0) * ap)).astype(np.int64)
+            idx = idx[row % 2 == 0]
+            if len(idx) == 0:
+                continue
+            xs = np.round(pos[idx, 0], 12)
+            for side in (-1.0, 1.0):
+                ys = side * pos[idx, 1]
+                order = np.lexsort((-ys, xs))
+                first = np.ones(len(order), dtype=bool)
+                first[1:] = xs[order][1:] != xs[order][:-1]
+                th = math.atan2(zc, side * R) % (2.0 * math.pi)
+                k = int(th / dth) % n_theta
+                # facet plane through the drum nodes at angles k, k+1 (a chord)
+                c1, s1 = math.cos(k * dth), math.sin(k * dth)
+                c2, s2 = math.cos((k + 1) * dth), math.sin((k + 1) * dth)
+                ny, nz = -(c1 + c2), -(s1 + s2)
+                nn = math.hypot(ny, nz)
+                ny, nz = ny / nn, nz / nn                  # inward unit normal in (y, z)
+                if ny == 0.0:
+                    continue
+                d0 = (R * c1) * ny + (R * s1) * nz         # plane: (y, z).n = d0
+                sel = idx[order[first]]
+                dist = pos[sel, 1] * ny + zc * nz - d0       # distance inside the plane
+                dy = (rad[sel] * (1.0 - wall_overlap) - dist) / ny
+                mv = side * dy > 0
+                pos[sel[mv], 1] += dy[mv]
+        z = zc + rmax + 1e-7
+    nodes = drum_mesh(diameter, length, n_theta, n_ax, cap_rings)
+    lo = [-0.5 * length - margin, -R - margin, -R - margin]
+    hi = [0.5 * length + margin, R + margin, R + margin]
+    sc = {
+        "name": "drum_config3",
+        "dt": dt, "skin": skin,
+        "boxlo": lo, "boxhi": hi, "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": sortfreq, "sortbinsize": 0.0,
+        "rolling_cdt": 0, "tangential_damping": 1,
+        "atoms": _atoms(pos, rad, 2700.0, np.zeros((n, 3))),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_mesh", "nodes": nodes, "wall_type": 1, "curvature": 0.0, "rolling_cdt": 0},
+            {"kind": "move_mesh_rotate", "mesh": 1, "origin": [0.0, 0.0, 0.0], "axis": [1.0, 0.0, 0.0],
+             "period": 2.0 * math.pi / omega},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 1e7, 0.45, 0.5, 0.4))
+    return sc
+
+
+def bumpy_plate_mesh(lx=0.2, ly=0.2, nx=128, ny=256, z0=1.5e-3, amp=1.0e-3, waves=(8, 8)):
+    """Procedural bumpy plate over [0, lx] x [0, ly]: z = z0 + amp sin(2 pi kx x / lx)
+    sin(2 pi ky y / ly) on an nx x ny grid, two triangles per cell
+    (2 nx ny triangles; the defaults give 65,536)."""
+    xs = np.linspace(0.0, lx, nx + 1)
+    ys = np.linspace(0.0, ly, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    Z = z0 + amp * np.sin(2.0 * math.pi * waves[0] * X / lx) * np.sin(2.0 * math.pi * waves[1] * Y / ly)
+    P = np.stack([X, Y, Z], axis=-1)
+    p00, p10, p01, p11 = P[:-1, :-1], P[1:, :-1], P[:-1, 1:], P[1:, 1:]
+    t1 = np.stack([p00, p10, p11], axis=2).reshape(-1, 3, 3)
+    t2 = np.stack([p00, p11, p01], axis=2).reshape(-1, 3, 3)
+    return np.ascontiguousarray(np.stack([t1, t2], axis=1).reshape(-1, 3, 3))
+
+
+def bed_config5(n=20_000_000, seed=5, dt=2e-6, skin=0.5e-3, r=0.5e-3, box=(0.2, 0.2, 0.5), overlap=1e-4,
+                plate_nx=128, plate_ny=256, plate_z0=1.5e-3, plate_amp=1.0e-3, plate_waves=(8, 8), sortfreq=1000):
+    """Large settled bed of configuration 5: n spheres of radius r (density
+    2500, E 5e6, nu 0.45, e 0.3, mu 0.5) in a box walled by planes on all
+    sides but the top, with a procedural bumpy-plate mesh of 65,536 triangles
+    over the floor.  The spheres stand in hexagonal close packing (ABAB
+    stacking, every neighbour at (1 - overlap) x the diameter, so each sphere
+    touches its 12 neighbours), the lowest layer resting on the plate's
+    crests, the sides against the walls."""
+    a = 2.0 * r * (1.0 - overlap)
+    cz = math.sqrt(2.0 / 3.0) * a
+    lx, ly, lz = box
+    m = r * (1.0 - overlap)
+    xa, ya = _hex_rect(a, m, lx - m, m, ly - m)
+    # the lowest layer rests on the plate's crests (overlap up to 2 % of r right above a crest node)
+    z0 = plate_z0 + plate_amp + r * (1.0 - 2e-2)
+    pos = np.zeros((n, 3))
+    placed = 0
+    layer = 0
+    while placed < n:
+        sx = 0.5 * a if layer % 2 else 0.0
+        sy = a / (2.0 * math.sqrt(3.0)) if layer % 2 else 0.0
+        x, y = xa + sx, ya + sy
+        keep = (x <= lx - m) & (y <= ly - m)
+        x, y = x[keep], y[keep]
+        take = min(len(x), n - placed)
+        zl = z0 + layer * cz
+        if zl + r > lz:
+            raise ValueError("box too small for %d spheres" % n)
+        pos[placed:placed + take, 0] = x[:take]
+        pos[placed:placed + take, 1] = y[:take]
+        pos[placed:placed + take, 2] = zl
+        placed += take
+        layer += 1
+    del seed   # the packing is fully determined; kept for the workload interface
+    nodes = bumpy_plate_mesh(lx, ly, plate_nx, plate_ny, plate_z0, plate_amp, plate_waves)
+    sc = {
+        "name": "bed_config5",
+        "dt": dt, "skin": skin,
+        "boxlo": [-0.005, -0.005, -0.005], "boxhi": [lx + 0.005, ly + 0.005, lz], "periodic": [0, 0, 0],
+        "every": 1, "delay": 0, "check": 1, "sortfreq": sortfreq, "sortbinsize": 0.0,
+        "rolling_cdt": 0, "tangential_damping": 1,
+        "atoms": _atoms(pos, np.full(n, r), 2500.0, np.zeros((n, 3))),
+        "fixes": [
+            {"kind": "gravity", "magnitude": 9.81, "vector": [0.0, 0.0, -1.0]},
+            {"kind": "wall_mesh", "nodes": nodes, "wall_type": 1, "curvature": 0.0, "rolling_cdt": 0},
+            {"kind": "wall_plane", "dim": 2, "pos": 0.0, "wall_type": 1},
+            {"kind": "wall_plane", "dim": 0, "pos": 0.0, "wall_type": 1},
+            {"kind": "wall_plane", "dim": 0, "pos": lx, "wall_type": 1},
+            {"kind": "wall_plane", "dim": 1, "pos": 0.0, "wall_type": 1},
+            {"kind": "wall_plane", "dim": 1, "pos": ly, "wall_type": 1},
+            {"kind": "nve_sphere"},
+        ],
+    }
+    sc.update(_materials(1, 5e6, 0.45, 0.3, 0.5))
     return sc
 
 

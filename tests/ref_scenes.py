@@ -55,9 +55,21 @@ def _hopper_packed():
     return S.hopper_packed(n=6000, n_theta=48, n_z=12, band=0.02, sortfreq=200)
 
 
+def _drum_config3():
+    return S.drum_config3(n=6000, diameter=0.06, length=0.05, n_theta=48, n_ax=12, cap_rings=3, band=0.02,
+                          omega=20.0, sortfreq=300)
+
+
+def _bed_config5():
+    return S.bed_config5(n=20000, box=(0.02, 0.02, 0.05), plate_nx=32, plate_ny=32, plate_waves=(2, 2),
+                         sortfreq=300)
+
+
 # name -> (scenario builder, run segments); segment 0 is the setup
 SCENES = {
     "hopper_packed_discharge": (_hopper_packed, [0, 200, 200, 200, 200, 200]),
+    "drum_config3_packed": (_drum_config3, [0, 300, 300, 300, 300]),
+    "bed_config5_packed": (_bed_config5, [0, 300, 300, 300]),
     "pour3k_rolling": (_pour3k, [0, 150, 150, 150, 150]),
     "two_types_schedule": (_two_types, [0, 300, 300, 300, 300]),
     "hopper_mesh": (_hopper_mesh, [0, 300, 300, 300, 300, 300]),
