@@ -37,6 +37,23 @@ constexpr int kBlock = 128;
 
 inline int nblk(long n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
+// Device memory comes from the device's stream-ordered pool (the context
+// creation keeps freed blocks in it for reuse within the process), so a
+// context created after another was destroyed allocates without new page
+// mappings.  Allocation completes before it returns, and a release first
+// waits for the device, as cudaMalloc / cudaFree do.
+inline cudaError_t dev_alloc(void **p, size_t bytes)
+{
+    cudaError_t e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+inline void dev_free(void *p)
+{
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, cudaStreamLegacy);
+}
+
 // device buffer with explicit growth
 template <typename T>
 struct DBuf {
@@ -48,7 +65,7 @@ struct DBuf {
     ~DBuf() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }
@@ -56,15 +73,16 @@ struct DBuf {
     {
         if (m <= n && p) return cudaSuccess;
         release();
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
+        cudaError_t e = dev_alloc(reinterpret_cast<void **>(&p), std::max<size_t>(m, 1) * sizeof(T));
         if (e == cudaSuccess) n = m;
+        else p = nullptr;
         return e;
     }
     cudaError_t grow_keep(size_t m, size_t keep, cudaStream_t s)   // keeps the first `keep` elements
     {
         if (m <= n && p) return cudaSuccess;
         T *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<size_t>(m, 1) * sizeof(T));
+        cudaError_t e = dev_alloc(reinterpret_cast<void **>(&q), std::max<size_t>(m, 1) * sizeof(T));
         if (e != cudaSuccess) return e;
         if (p && keep) cudaMemcpyAsync(q, p, std::min(keep, n) * sizeof(T), cudaMemcpyDeviceToDevice, s);
         cudaStreamSynchronize(s);
@@ -1097,7 +1115,7 @@ void launch_pair(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
         return;
     }
     // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
-    const int mb = c->minb ? c->minb : 6;
+    const int mb = c->minb ? c->minb : 4;
     if (c->P.rolling_cdt) {
         if (mb == 4) launch_pair_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch_pair_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);
@@ -1252,6 +1270,13 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     if (e != cudaSuccess) {
         delete c;
         return GB2_ERR_CUDA;
+    }
+    {   // the device pool keeps freed memory for this process's later contexts
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, p->device) == cudaSuccess) {
+            uint64_t keep_all = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+        }
     }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||

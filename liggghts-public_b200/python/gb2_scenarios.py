@@ -544,9 +544,11 @@ def drum_config3(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length
     patches of a triangular lattice holding one narrow radius band (spacing
     (1 - overlap) x the smallest diameter of the patch, patches one diameter
     apart), so neighbours inside a patch touch; in every other lattice row
-    the outermost particle of each column is pushed sideways onto the drum's
-    facet plane (overlap ``wall_overlap`` of its radius), giving wall
-    contacts all along the drum."""
+    the outermost particle of each column is pushed sideways onto the plane
+    of the drum facet at that height (overlap ``wall_overlap`` of its
+    radius), giving wall contacts all along the drum.  Layers where the wall
+    is closer to horizontal than vertical (more than 60 degrees from the
+    drum's horizontal diameter) are not pushed."""
     rng = np.random.default_rng(seed)
     rad = np.sort(rng.uniform(0.8e-3, 1.2e-3, size=n))[::-1].copy()
     neg_rad = -rad   # ascending, for the band searches
@@ -602,12 +604,15 @@ def drum_config3(n=8_000_000, seed=7, dt=5e-6, skin=0.5e-3, diameter=0.5, length
             if len(idx) == 0:
                 continue
             xs = np.round(pos[idx, 0], 12)
+            yw = math.sqrt(max(R * R - zc * zc, 0.0))   # the drum wall at this height: y = +-yw
+            if yw < 0.5 * R:   # the wall is closer to horizontal than vertical here: no sideways push
+                continue
             for side in (-1.0, 1.0):
                 ys = side * pos[idx, 1]
                 order = np.lexsort((-ys, xs))
                 first = np.ones(len(order), dtype=bool)
                 first[1:] = xs[order][1:] != xs[order][:-1]
-                th = math.atan2(zc, side * R) % (2.0 * math.pi)
+                th = math.atan2(zc, side * yw) % (2.0 * math.pi)
                 k = int(th / dth) % n_theta
                 # facet plane through the drum nodes at angles k, k+1 (a chord)
                 c1, s1 = math.cos(k * dth), math.sin(k * dth)
