@@ -63,6 +63,11 @@ def parse_list(argv):
                     help="steps of the longer window with neighbour rebuilds (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=60.0, help="reference arm: target timed seconds")
+    ap.add_argument("--roofline-steps", type=int, default=32,
+                    help="steps right after the headline window with every pair-step launch timed (roofline)")
+    ap.add_argument("--force-frames", type=int, default=0,
+                    help="FP64 vs split force error on this many frames of the FP64 run (restarts of its state)")
+    ap.add_argument("--frame-every", type=int, default=10, help="steps between force-error frames")
     ap.add_argument("--no-split", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -335,7 +340,56 @@ def reference_arm(args):
 PROFILE_EVERY = 16   # per-kernel CUDA events on every 16th step of a window
 
 
-def timed_window(eng, steps, dist, device, clocks=True, profile=True):
+def force_frames(sc, eng, nframes, every, device, g=9.81):
+    """Force error of the split-precision path on frames of an FP64 run.
+    Every `every` steps the FP64 run's state is downloaded (atoms, pair,
+    wall and mesh contact histories, mesh nodes) and restarted into a fresh
+    FP64 and a fresh split context; each computes the forces at that state
+    (setup, shear history not advanced) and they are compared atom by atom.
+    Per frame: max |df| / max |f|, the RMS ratio, and the 99.9th percentile
+    and maximum of the per-atom error |df_i| / (|f_i| + m_i g) (torques:
+    |dt_i| / (|t_i| + r_i m_i g)), all with max-norm over components."""
+    import granb200
+    frames = []
+    for fr in range(nframes):
+        eng.run(every)
+        snap = eng.snapshot(sc)
+        sc2 = granb200.restart_scenario(sc, snap["atoms"], {i: m["nodes"] for i, m in snap["meshes"].items()})
+        res = {}
+        for prec in (granb200.PREC_FP64, granb200.PREC_SPLIT):
+            e = granb200.Engine(sc2, precision=prec, device=device)
+            e.restore(snap)
+            e.setup()
+            a = e.atoms()
+            order = np.argsort(a["tag"])
+            res[prec] = {k: a[k][order] for k in ("f", "torque", "tag")}
+            e.close()
+            del e
+        f64, f32 = res[granb200.PREC_FP64]["f"], res[granb200.PREC_SPLIT]["f"]
+        t64, t32 = res[granb200.PREC_FP64]["torque"], res[granb200.PREC_SPLIT]["torque"]
+        at = sc2["atoms"]
+        o = np.argsort(at["tag"])
+        mg = np.asarray(at["rmass"])[o] * g
+        rad = np.asarray(at["radius"])[o]
+        df = np.abs(f32 - f64).max(axis=1)
+        dt = np.abs(t32 - t64).max(axis=1)
+        ef = df / (np.abs(f64).max(axis=1) + mg)
+        et = dt / (np.abs(t64).max(axis=1) + rad * mg)
+        frames.append({"frame": fr, "rel_max_force": float(df.max() / max(np.abs(f64).max(), 1e-300)),
+                       "rel_rms_force": float(np.sqrt((df ** 2).mean() / max((np.abs(f64).max(axis=1) ** 2).mean(),
+                                                                             1e-300))),
+                       "atom_p999_force": float(np.percentile(ef, 99.9)), "atom_max_force": float(ef.max()),
+                       "atom_p999_torque": float(np.percentile(et, 99.9)), "atom_max_torque": float(et.max())})
+        print("frame %d: %s" % (fr, frames[-1]), file=sys.stderr, flush=True)
+    keys = [k for k in frames[0] if k != "frame"]
+    return {"frames": len(frames), "steps_between": every,
+            "max_over_frames": {k: max(f[k] for f in frames) for k in keys},
+            "median_over_frames": {k: float(np.median([f[k] for f in frames])) for k in keys},
+            "method": force_frames.__doc__.split("\n\n")[0].replace("\n", " ").strip(),
+            "per_frame": frames}
+
+
+def timed_window(eng, steps, dist, device, clocks=True, profile=True, every=PROFILE_EVERY):
     """Device-timed window of `steps` steps: CUDA events at its ends give the
     window time; per-kernel CUDA events on every PROFILE_EVERY-th step give
     each kernel's average launch time (the events serialise the pair step
@@ -347,7 +401,7 @@ def timed_window(eng, steps, dist, device, clocks=True, profile=True):
     barrier(dist)
     eng.sync()
     if profile:
-        eng.set_profiling(True, every=PROFILE_EVERY)
+        eng.set_profiling(True, every=every)
     eng.timer_start()
     eng.run(steps)
     ms = eng.timer_stop()
@@ -362,7 +416,7 @@ def timed_window(eng, steps, dist, device, clocks=True, profile=True):
     return {"ms": allmax(dist, ms), "clocks": clk, "cen": (cen0, cen1), "kt": kt, "npm": npm,
             "kernel_ms_per_step": dict({k: v / max(npm, 1) for k, v in kt.items()},
                                        note="CUDA events on every %dth step of the window (%d steps sampled)"
-                                            % (PROFILE_EVERY, npm)),
+                                            % (every, npm)),
             "launches": st1["kernel_launches"] - st0["kernel_launches"],
             "rebuilds": st1["nsteps_rebuild"] - st0["nsteps_rebuild"],
             "growth": st1["ngrow"] - st0["ngrow"],
@@ -432,15 +486,16 @@ def own_arm(args):
         "capacities": W["capacities"],
     }
 
-    # longer FP64 window with rebuilds; its sampled pair-step launches give the roofline
+    # roofline: right after the headline window (the same state), every
+    # pair-step launch of a short window timed with CUDA events
     dom = "k_pair_step"
     peak, peak_kind = peaks()
-    if args.long_steps > 0:
-        lw, WL = long_window(eng, args.long_steps, dist, local)
-        line["long_window"] = lw
-        kt_src, npm, cen_src, src = WL["kt"], WL["npm"], WL["cen"], "long FP64 window (%d steps)" % args.long_steps
+    if args.roofline_steps > 0:
+        WR = timed_window(eng, args.roofline_steps, dist, local, clocks=False, every=1)
+        kt_src, npm, cen_src, src = WR["kt"], WR["npm"], WR["cen"], "%d steps right after the headline window" % (
+            args.roofline_steps)
     else:
-        kt_src, npm, cen_src, src = W["kt"], W["npm"], W["cen"], "headline window"
+        kt_src, npm, cen_src, src = W["kt"], W["npm"], W["cen"], "headline window (every %dth step)" % PROFILE_EVERY
     dom_ms = kt_src["t_pair_main"] / max(npm, 1)
     ab = algorithmic_bytes(n, cen_src, nfix_plane, nfix_mesh, False)
     achieved = ab / (dom_ms * 1e-3) / 1e9 if npm > 0 and dom_ms > 0 else None
@@ -448,9 +503,25 @@ def own_arm(args):
     line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                         "traffic": traffic["bytes_per_launch"] if traffic else None,
+                        "traffic_over_algorithmic": traffic["bytes_per_launch"] / ab if traffic and ab else None,
                         "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms, "sampled_launches": npm,
-                        "timing": "pair-step launches timed with CUDA events on every %dth step of the %s"
-                                  % (PROFILE_EVERY, src)}
+                        "timing": "every pair-step launch timed with CUDA events over the %s" % src}
+    if traffic:
+        line["roofline"]["traffic_source"] = traffic.get("capture")
+
+    # longer FP64 window with rebuilds
+    if args.long_steps > 0:
+        lw, WL = long_window(eng, args.long_steps, dist, local)
+        line["long_window"] = lw
+        dl = WL["kt"]["t_pair_main"] / max(WL["npm"], 1)
+        abl = algorithmic_bytes(n, WL["cen"], nfix_plane, nfix_mesh, False)
+        lw["pair_step_roofline"] = {"avg_launch_ms": dl, "algorithmic_bytes_per_launch": abl,
+                                    "achieved_gbs": abl / (dl * 1e-3) / 1e9 if WL["npm"] and dl > 0 else None,
+                                    "frac": abl / (dl * 1e-3) / 1e9 / peak if WL["npm"] and dl > 0 else None}
+
+    # FP64 vs split force error on frames of the FP64 run
+    if args.force_frames > 0:
+        line["force_error_frames"] = force_frames(sc, eng, args.force_frames, args.frame_every, local)
     eng.close()
     del eng
 

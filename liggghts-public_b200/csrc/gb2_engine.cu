@@ -1367,7 +1367,7 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     // copy per array (straight from the caller's memory when it is pinned),
     // packed into the 32-byte records and checked on the device
     const size_t N = (size_t)n;
-    CK(c->iostage.alloc(11 * N));
+    CK(c->iostage.alloc(15 * N));   // also the download's five [n][3] planes
     CK(c->iocheck.alloc(2));
     const double *src[5] = {x, v, omega, radius, rmass};
     const size_t off[5] = {0, 3 * N, 6 * N, 9 * N, 10 * N}, len[5] = {3 * N, 3 * N, 3 * N, N, N};

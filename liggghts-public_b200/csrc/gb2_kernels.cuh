@@ -827,42 +827,44 @@ __global__ void k_tri_bin_fill(Dev D, int ntri, const int *range, const int *off
 }
 
 // contact census (diagnostics and the bench's byte model)
-__global__ void k_census(Dev D, unsigned long long *cnt)
+__global__ void __launch_bounds__(128) k_census(Dev D, unsigned long long *cnt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.nlocal) return;
-    const int cap = D.cap;
-    const dbl4 pi = D.pos[i];
-    const int nn = D.nnum[i];
-    unsigned long long touch = 0;
-    for (int s = 0; s < nn; s++) {
-        const dbl4 pj = D.pos[D.nbr[s * cap + i]];
-        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        const double rs = pi.w + pj.w;
-        if (dx * dx + dy * dy + dz * dz < rs * rs) touch++;
-    }
-    unsigned long long wl = 0, wt = 0, mc = 0, mt = 0;
-    for (int k = 0; k < D.nfix; k++) {
-        const FixDev &F = D.fix[k];
-        if (F.kind == FIX_WALL_PLANE && F.inlist[i]) {
-            wl++;
-            const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
-            const double dist = x > F.pos ? x - F.pos - pi.w : F.pos - x - pi.w;
-            if (dist <= 0) wt++;
-        } else if (F.kind == FIX_WALL_MESH) {
-            const int tc = F.mesh.tcnt[i];
-            mc += tc;
-            for (int q = 0; q < tc; q++)
-                if (F.mesh.spartner[q * cap + i] >= 0) mt++;
+    unsigned long long c[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (i < D.nlocal) {
+        const int cap = D.cap;
+        const dbl4 pi = D.pos[i];
+        const int nn = D.nnum[i];
+        c[0] = nn;
+        for (int s = 0; s < nn; s++) {
+            const dbl4 pj = D.pos[D.nbr[s * cap + i]];
+            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const double rs = pi.w + pj.w;
+            if (dx * dx + dy * dy + dz * dz < rs * rs) c[1]++;
+        }
+        c[2] = D.rnum[i];
+        for (int k = 0; k < D.nfix; k++) {
+            const FixDev &F = D.fix[k];
+            if (F.kind == FIX_WALL_PLANE && F.inlist[i]) {
+                c[3]++;
+                const double x = F.dim == 0 ? pi.x : (F.dim == 1 ? pi.y : pi.z);
+                const double dist = x > F.pos ? x - F.pos - pi.w : F.pos - x - pi.w;
+                if (dist <= 0) c[4]++;
+            } else if (F.kind == FIX_WALL_MESH) {
+                const int tc = F.mesh.tcnt[i];
+                c[5] += tc;
+                for (int q = 0; q < tc; q++)
+                    if (F.mesh.spartner[q * cap + i] >= 0) c[6]++;
+            }
         }
     }
-    atomicAdd(&cnt[0], (unsigned long long)nn);
-    if (touch) atomicAdd(&cnt[1], touch);
-    atomicAdd(&cnt[2], (unsigned long long)D.rnum[i]);
-    if (wl) atomicAdd(&cnt[3], wl);
-    if (wt) atomicAdd(&cnt[4], wt);
-    if (mc) atomicAdd(&cnt[5], mc);
-    if (mt) atomicAdd(&cnt[6], mt);
+    // warp sums, then one atomic per warp and counter (no contention on 7 words)
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        unsigned long long v = c[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[k], v);
+    }
 }
 
 // The tail kernel's atom list, after each neighbour build (count zeroed

@@ -302,6 +302,30 @@ def pinned_empty(shape, dtype=np.float64):
     return arr
 
 
+def restart_scenario(sc, atoms, mesh_nodes=None):
+    """The scenario with its atoms replaced by a run's current state (same
+    tags, the run's atom order), as read_restart would bring them back;
+    `mesh_nodes` maps a scenario fix index to that mesh's current nodes
+    (ntri, 3, 3), for meshes that have moved."""
+    out = dict(sc)
+    a = dict(sc["atoms"])
+    tags = np.asarray(a["tag"])
+    order = np.argsort(tags, kind="stable")
+    idx = order[np.searchsorted(tags, atoms["tag"], sorter=order)]
+    for k in a:
+        a[k] = np.ascontiguousarray(np.asarray(a[k])[idx])
+    for k in ("x", "v", "omega"):
+        a[k] = np.ascontiguousarray(atoms[k])
+    a["tag"] = np.ascontiguousarray(atoms["tag"])
+    out["atoms"] = a
+    if mesh_nodes:
+        fixes = [dict(f) for f in sc["fixes"]]
+        for i, nodes in mesh_nodes.items():
+            fixes[i]["nodes"] = np.ascontiguousarray(np.asarray(nodes, dtype=np.float64).reshape(-1, 9))
+        out["fixes"] = fixes
+    return out
+
+
 class Engine:
     """One device-resident granular simulation (one gb2_ctx)."""
 
@@ -603,6 +627,30 @@ class Engine:
         self._check(self.L.gb2_download_mesh_nodes(self.h, self.fix_ids[ifix], n.value, ctypes.byref(n), _dp(nodes),
                                                    _dp(vel)))
         return nodes, vel
+
+    def snapshot(self, sc):
+        """What a restart of this run needs, downloaded: the atoms, the pair
+        contact history (partner layout), every primitive wall's history and
+        every mesh's contact history (restart layout) and current nodes."""
+        snap = {"atoms": self.atoms(), "history": self.history(), "walls": {}, "meshes": {}}
+        for i, f in enumerate(sc["fixes"]):
+            if f["kind"] in ("wall_plane", "wall_cylinder"):
+                snap["walls"][i] = self.wall_hist(i)
+            elif f["kind"] == "wall_mesh":
+                nodes, _ = self.mesh_nodes(i)
+                snap["meshes"][i] = {"history": self.mesh_history(i), "nodes": nodes}
+        return snap
+
+    def restore(self, snap):
+        """Upload a snapshot's histories (the engine was built from
+        restart_scenario(sc, snap["atoms"], ...)); before setup."""
+        h = snap["history"]
+        self.upload_history(h["npartner"], h["partner_tag"], h["hist"])
+        for i, w in snap["walls"].items():
+            self.upload_wall_hist(i, w)
+        for i, m in snap["meshes"].items():
+            mh = m["history"]
+            self.upload_mesh_hist(i, mh["npartner"], mh["tri"], mh["hist"])
 
     def mesh_topology(self, ifix):
         k = self.fix_ids[ifix]

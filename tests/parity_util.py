@@ -1,6 +1,8 @@
 """Comparison helpers for engine-vs-oracle parity tests."""
 import numpy as np
 
+from granb200 import restart_scenario  # noqa: F401  (restart helper shared with the bench)
+
 
 def by_tag(a):
     order = np.argsort(a["tag"])
@@ -41,22 +43,6 @@ def assert_mesh_equal(eng, orc, ifix):
     assert np.array_equal(p["tag"], q["tag"]) and np.array_equal(p["tri"], q["tri"]), "mesh contact slots differ"
     assert np.array_equal(p["hist"], q["hist"]), "mesh shear history differs"
     return len(p["tag"])
-
-
-def restart_scenario(sc, atoms):
-    """The scenario with its atoms replaced by a run's current state (same
-    tags, the run's atom order), as read_restart would bring them back."""
-    out = dict(sc)
-    a = dict(sc["atoms"])
-    pos_of_tag = {t: k for k, t in enumerate(a["tag"])}
-    idx = np.array([pos_of_tag[t] for t in atoms["tag"]])
-    for k in a:
-        a[k] = np.ascontiguousarray(np.asarray(a[k])[idx])
-    for k in ("x", "v", "omega"):
-        a[k] = np.ascontiguousarray(atoms[k])
-    a["tag"] = np.ascontiguousarray(atoms["tag"])
-    out["atoms"] = a
-    return out
 
 
 def mesh_contact_map(mc):
