@@ -1,6 +1,7 @@
-"""Known-answer tests that pin the CPU oracle (the reference ships no tests,
-golden logs or fixtures, so these analytic cases and symmetry laws stand in
-for them; see DESIGN.md "parity status")."""
+"""Known-answer tests of the CPU oracle: analytic cases and symmetry laws
+(the reference ships no tests, golden logs or fixtures).  They are a second
+pin next to the digests of the reference's own state in
+tests/golden/reference_digests.json."""
 import math
 
 import numpy as np
