@@ -289,11 +289,15 @@ int gb2_download_mesh_stress(gb2_ctx *ctx, int ifix, int cap, double *tri_f, dou
  * add_particle_contribution, src/mesh_module_stress.cpp:306-352, with the
  * element area of TriMesh::calcArea as created): after gb2_add_mesh_stress,
  * before setup.  k_finnie is the peratomtypepair property (ntypes x ntypes,
- * row-major); the row of the wall's atom type applies.  Device atomics: equal
+ * row-major, ntypes * ntypes doubles); the row of the wall's atom type applies.  Device atomics: equal
  * to the reference to rounding.  The download gives the cumulative wear of
  * every element. */
 int gb2_add_mesh_wear(gb2_ctx *ctx, int ifix, const double *k_finnie);
 int gb2_download_mesh_wear(gb2_ctx *ctx, int ifix, int cap, double *wear);
+/* restart of the cumulative wear (MeshModuleStress's restart property "wear",
+ * src/mesh_module_stress.cpp:197): n = the mesh's element count, after
+ * gb2_add_mesh_wear, before setup */
+int gb2_upload_mesh_wear(gb2_ctx *ctx, int ifix, int n, const double *wear);
 /* restart interoperability: the contact history in FixContactHistory's
  * per-atom partner layout (src/fix_contact_history.cpp:588-640 pack_restart /
  * unpack_restart): per atom npartner, then per partner its tag and 3 shear

@@ -1819,10 +1819,9 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
         hw[q] = {a.omega[0], a.omega[1], a.omega[2], 0.0};
         ht[q] = a.type;
         hg[q] = (int)(c->maxtag + 1 + q);
-        c->h_radius.push_back(a.radius);
-        c->h_type.push_back(a.type);
     }
-    c->maxtag += k;
+    // device capacity and copies first; the host mirrors change only once the
+    // device holds the new atoms
     if (ensure_nmax(c, nall > nl + k ? nall : nl + k)) return GB2_ERR_CUDA;
     CK(cudaMemcpyAsync(c->pos.p + nl, hp.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->vel.p + nl, hv.data(), sizeof(dbl4) * k, cudaMemcpyHostToDevice, c->st));
@@ -1847,8 +1846,13 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
             CK(cudaMemsetAsync(H.mesh->snp.p + nl, 0, sizeof(int) * k, c->st));
         }
     }
-    c->nlocal = nl + k;
     CK(cudaStreamSynchronize(c->st));
+    for (int q = 0; q < k; q++) {
+        c->h_radius.push_back(out[q].radius);
+        c->h_type.push_back(out[q].type);
+    }
+    c->maxtag += k;
+    c->nlocal = nl + k;
     return 0;
 }
 
@@ -2381,6 +2385,22 @@ int gb2_download_mesh_wear(gb2_ctx *c, int ifix, int cap, double *wear)
     const int nt = (int)M.topo.tri.size();
     if (cap < nt) return set_err(c, GB2_ERR_ARG, "wear needs %d entries", nt);
     CK(cudaMemcpyAsync(wear, M.wear.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// restart of the cumulative wear (MeshModuleStress registers "wear" as a
+// restart property, src/mesh_module_stress.cpp:197): after gb2_add_mesh_wear,
+// before setup
+int gb2_upload_mesh_wear(gb2_ctx *c, int ifix, int n, const double *wear)
+{
+    if (!c || ifix < 0 || ifix >= c->nfix || c->fix[ifix].kind != FIX_WALL_MESH || !wear) return GB2_ERR_ARG;
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "mesh wear is uploaded before setup");
+    MeshFix &M = *c->fix[ifix].mesh;
+    if (!M.wear.p) return set_err(c, GB2_ERR_STATE, "wear not enabled on this mesh");
+    const int nt = (int)M.topo.tri.size();
+    if (n != nt) return set_err(c, GB2_ERR_ARG, "wear needs %d entries, got %d", nt, n);
+    CK(cudaMemcpyAsync(M.wear.p, wear, sizeof(double) * nt, cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
     return 0;
 }

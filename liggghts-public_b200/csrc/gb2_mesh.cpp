@@ -131,27 +131,50 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
     }
     const int n = (int)T.size();
 
-    // candidate pairs: elements owning nodes in the same or adjacent hash cells
+    // candidate pairs: elements owning a node equal (within `precision`) to
+    // one of the element's nodes.  Node entries are sorted by their hash cell
+    // (side 1000 x precision); equal nodes share a cell unless they sit within
+    // `precision` of a cell face, so a node looks into a neighbouring cell
+    // only along the axes where it is that close to a face.
     const double cell = std::max(1e3 * precision, 1e-9);
-    std::unordered_map<CellKey, std::vector<int>, CellHash> grid;
-    grid.reserve((size_t)n * 3);
-    auto key_of = [&](const double *p) {
-        return CellKey{(int64_t)std::floor(p[0] / cell), (int64_t)std::floor(p[1] / cell),
-                       (int64_t)std::floor(p[2] / cell)};
+    const double near_face = 2.0 * precision / cell;   // in cell units, with a margin for rounding
+    struct NodeEnt {
+        int64_t x, y, z;
+        int t;
+        bool operator<(const NodeEnt &o) const
+        {
+            return x != o.x ? x < o.x : (y != o.y ? y < o.y : (z != o.z ? z < o.z : t < o.t));
+        }
     };
+    std::vector<NodeEnt> ents;
+    ents.reserve((size_t)3 * n);
     for (int t = 0; t < n; t++)
-        for (int k = 0; k < 3; k++) grid[key_of(T[t].node[k])].push_back(t);
+        for (int k = 0; k < 3; k++) {
+            const double *p = T[t].node[k];
+            ents.push_back(NodeEnt{(int64_t)std::floor(p[0] / cell), (int64_t)std::floor(p[1] / cell),
+                                   (int64_t)std::floor(p[2] / cell), t});
+        }
+    std::sort(ents.begin(), ents.end());
     std::vector<std::vector<int>> cand(n);
     for (int t = 0; t < n; t++) {
         for (int k = 0; k < 3; k++) {
-            const CellKey c = key_of(T[t].node[k]);
-            for (int dx = -1; dx <= 1; dx++)
-                for (int dy = -1; dy <= 1; dy++)
-                    for (int dz = -1; dz <= 1; dz++) {
-                        auto it = grid.find(CellKey{c.x + dx, c.y + dy, c.z + dz});
-                        if (it == grid.end()) continue;
-                        for (int u : it->second)
-                            if (u != t) cand[t].push_back(u);
+            const double *p = T[t].node[k];
+            int64_t c[3];
+            int lo[3], hi[3];
+            for (int d = 0; d < 3; d++) {
+                const double q = p[d] / cell;
+                c[d] = (int64_t)std::floor(q);
+                const double fr = q - (double)c[d];
+                lo[d] = fr < near_face ? -1 : 0;
+                hi[d] = 1.0 - fr < near_face ? 1 : 0;
+            }
+            for (int dx = lo[0]; dx <= hi[0]; dx++)
+                for (int dy = lo[1]; dy <= hi[1]; dy++)
+                    for (int dz = lo[2]; dz <= hi[2]; dz++) {
+                        const NodeEnt key{c[0] + dx, c[1] + dy, c[2] + dz, -1};
+                        for (auto it = std::lower_bound(ents.begin(), ents.end(), key);
+                             it != ents.end() && it->x == key.x && it->y == key.y && it->z == key.z; ++it)
+                            if (it->t != t) cand[t].push_back(it->t);
                     }
         }
         std::sort(cand[t].begin(), cand[t].end());
@@ -214,16 +237,22 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
             }
         }
 
-    // corners
-    std::vector<uint8_t> corner_active((size_t)3 * n, 1);
-    std::vector<int> mark(n, -1), queue;
+    // corners.  The walk from corner (t, k) over edge neighbours that hold a
+    // copy of the node reaches the same elements from any of them, so it runs
+    // once per such group and settles every member's corner: active only at
+    // the group's largest element id, when an edge at the node is active and
+    // no two of its edges are colinear.
+    std::vector<uint8_t> corner_active((size_t)3 * n, 1), corner_done((size_t)3 * n, 0);
+    std::vector<int> mark(n, -1), queue, members;
     std::vector<const double *> evec, eend;
     int stamp = 0;
     for (int t = 0; t < n; t++)
         for (int k = 0; k < 3; k++) {
+            if (corner_done[3 * t + k]) continue;
             const double *nc = T[t].node[k];
             stamp++;
             queue.clear();
+            members.clear();
             evec.clear();
             eend.clear();
             queue.push_back(t);
@@ -239,6 +268,7 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
                         break;
                     }
                 if (in < 0) continue;   // visited but holds no copy of the node: not expanded
+                members.push_back(3 * e + in);
                 maxid = std::max(maxid, e);
                 const int prev = (in + 2) % 3;
                 evec.push_back(T[e].edgevec[in]);
@@ -259,7 +289,10 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
                         colinear = true;
                         break;
                     }
-            corner_active[3 * t + k] = (!colinear && any_active && t == maxid) ? 1 : 0;
+            for (int m : members) {
+                corner_active[m] = (!colinear && any_active && m / 3 == maxid) ? 1 : 0;
+                corner_done[m] = 1;
+            }
         }
     for (int t = 0; t < n; t++) {
         int bits = 0;

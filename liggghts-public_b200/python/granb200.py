@@ -32,7 +32,7 @@ EXPORTS = (
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
     "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
-    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_host_alloc", "gb2_host_free", "gb2_set_timestep",
+    "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_upload_mesh_wear", "gb2_host_alloc", "gb2_host_free", "gb2_set_timestep",
 )
 
 NOALLOC_MAX_ATOMS = 16384 * 128   # GB2_NOALLOC_MAX_ATOMS
@@ -243,6 +243,7 @@ def lib(path=LIB_PATH):
         L.gb2_pair_gran_local.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]
         L.gb2_add_mesh_wear.argtypes = [vp, ctypes.c_int, D]
         L.gb2_download_mesh_wear.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
+        L.gb2_upload_mesh_wear.argtypes = [vp, ctypes.c_int, ctypes.c_int, D]
         L.gb2_download_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, I, I, I, I, I, D]
         L.gb2_upload_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, D]
         L.gb2_add_insert_pack.argtypes = [vp, ctypes.POINTER(InsertPackParams)]
@@ -334,6 +335,7 @@ class Engine:
         self.L = L
         p = Params()
         p.ntypes = sc["ntypes"]
+        self.ntypes = int(sc["ntypes"])
         p.dt = sc["dt"]
         p.skin = sc["skin"]
         for d in range(3):
@@ -588,8 +590,17 @@ class Engine:
 
     def add_mesh_wear(self, ifix, k_finnie):
         """Finnie wear on the mesh of scenario fix ifix (after add_mesh_stress, before setup)."""
-        kf = np.ascontiguousarray(k_finnie, dtype=np.float64).reshape(-1)
+        kf = np.ascontiguousarray(k_finnie, dtype=np.float64)
+        nt = self.ntypes
+        if kf.shape != (nt, nt):
+            raise ValueError("k_finnie must be an ntypes x ntypes array (%d x %d), got %s" % (nt, nt, kf.shape))
+        kf = kf.reshape(-1)
         self._check(self.L.gb2_add_mesh_wear(self.h, self.fix_ids[ifix], _dp(kf)))
+
+    def upload_mesh_wear(self, ifix, wear):
+        """Cumulative wear per triangle of a restart (after add_mesh_wear, before setup)."""
+        w = np.ascontiguousarray(wear, dtype=np.float64)
+        self._check(self.L.gb2_upload_mesh_wear(self.h, self.fix_ids[ifix], len(w), _dp(w)))
 
     def mesh_wear(self, ifix):
         """Cumulative Finnie wear per triangle."""

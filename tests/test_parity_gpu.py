@@ -293,6 +293,34 @@ def test_mesh_surface_stress():
     assert hits > 0, "the piston carried no force"
     assert wb.max() > 0 and np.all(wb >= 0), "no wear on the piston"
     assert b["f_total"][2] > 0, "particles should push the piston up"
+    # restart of the wear: two restarts of the same snapshot, one with the
+    # cumulative wear uploaded; after setup they differ by exactly that wear
+    import granb200
+    snap = e.snapshot(sc)
+    sc2 = granb200.restart_scenario(sc, snap["atoms"], {i: m["nodes"] for i, m in snap["meshes"].items()})
+    w = []
+    for up in (True, False):
+        x = granb200.Engine(sc2)
+        x.restore(snap)
+        x.add_mesh_stress(3, [0.001, -0.002, 0.01])
+        x.add_mesh_wear(3, kf)
+        if up:
+            x.upload_mesh_wear(3, wa)
+        x.setup()
+        w.append(x.mesh_wear(3))
+        x.close()
+    assert np.abs((w[0] - w[1]) - wa).max() <= 1e-12 * wa.max()
+
+
+def test_mesh_wear_needs_a_type_matrix():
+    """k_finnie is an ntypes x ntypes matrix; anything else is refused before it reaches the library."""
+    import granb200
+    sc = S.silo(n=200, piston_speed=0.5)
+    e = granb200.Engine(sc)
+    e.add_mesh_stress(3, [0.0, 0.0, 0.0])
+    with pytest.raises(ValueError):
+        e.add_mesh_wear(3, np.full(sc["ntypes"] * sc["ntypes"] - 1, 0.7))
+    e.close()
 
 
 @pytest.mark.parametrize("kw", [dict(insert_every=250),
