@@ -184,6 +184,8 @@ struct gb2_ctx {
     double bboxlo[3], bboxhi[3], bininv[3], binsize[3];
     int nbin[3], mbinlo[3], mbin[3], mbins = 0;
     std::vector<int> h_stencil;
+    std::vector<int2> h_srow;   // stencil runs {first offset, bins}
+    DBuf<int2> srow;
     DBuf<int> stencil, bin_start, bin_atoms, counts, vals, vals2, sel, nsel;
     DBuf<unsigned> keys, keys2;
     DBuf<uint8_t> bflags;
@@ -365,6 +367,8 @@ Dev make_dev(gb2_ctx *c)
     D.mbins = c->mbins;
     D.nstencil = (int)c->h_stencil.size();
     D.stencil = c->stencil.p;
+    D.nsrow = (int)c->h_srow.size();
+    D.srow = c->srow.p;
     D.bin_start = c->bin_start.p;
     D.bin_atoms = c->bin_atoms.p;
     D.mat = c->dmat.p;
@@ -607,6 +611,19 @@ int setup_bins(gb2_ctx *c)
     CK(c->stencil.alloc(c->h_stencil.size()));
     CK(cudaMemcpyAsync(c->stencil.p, c->h_stencil.data(), c->h_stencil.size() * sizeof(int), cudaMemcpyHostToDevice,
                        c->st));
+    // the stencil as runs of consecutive bins (x innermost: one run per (y, z)
+    // offset), in stencil order: a run's atoms are one contiguous range of the
+    // bin-sorted atom array, in the order the per-bin loop visits them
+    c->h_srow.clear();
+    for (size_t q = 0; q < c->h_stencil.size(); q++) {
+        if (!c->h_srow.empty() && c->h_srow.back().x + c->h_srow.back().y == c->h_stencil[q])
+            c->h_srow.back().y++;
+        else
+            c->h_srow.push_back(make_int2(c->h_stencil[q], 1));
+    }
+    CK(c->srow.alloc(std::max<size_t>(c->h_srow.size(), 1)));
+    CK(cudaMemcpyAsync(c->srow.p, c->h_srow.data(), c->h_srow.size() * sizeof(int2), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
     CK(c->bin_start.alloc((size_t)c->mbins + 1));
     CK(c->counts.alloc((size_t)c->mbins + 1));
     for (int k = 0; k < c->nfix; k++)

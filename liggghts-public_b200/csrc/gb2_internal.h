@@ -149,6 +149,8 @@ struct Dev {
     int nbin[3], mbinlo[3], mbin[3], mbins;
     int nstencil;
     const int *stencil;
+    int nsrow;               // the stencil as runs of consecutive bins {first offset, bins}
+    const int2 *srow;
     const int *bin_start;    // [mbins+1]
     const int *bin_atoms;    // atoms sorted by bin, ascending index within a bin
     // materials [(kMaxTypes+1)^2]

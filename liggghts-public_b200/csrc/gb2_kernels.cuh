@@ -334,10 +334,13 @@ __global__ void k_build_list(Dev D)
     const double skin = D.skin;
     const int np = D.pnum[i];
     int n = 0;
-    for (int k = 0; k < D.nstencil; k++) {
-        const int b = ibin + D.stencil[k];
-        if (b < 0 || b >= D.mbins) continue;
-        const int e0 = D.bin_start[b], e1 = D.bin_start[b + 1];
+    // stencil runs: the bins of a run are consecutive, so their atoms are one
+    // range of the bin-sorted array (bins outside the grid are skipped)
+    for (int k = 0; k < D.nsrow; k++) {
+        const int2 run = D.srow[k];
+        const int b0 = max(ibin + run.x, 0), b1 = min(ibin + run.x + run.y, D.mbins);
+        if (b0 >= b1) continue;
+        const int e0 = D.bin_start[b0], e1 = D.bin_start[b1];
         for (int q = e0; q < e1; q++) {
             const int j = D.bin_atoms[q];
             if (j <= i) continue;
