@@ -208,6 +208,43 @@ typedef struct {
     double cyl_c1, cyl_c2, cyl_radius, cyl_lo, cyl_hi;
 } gb2_insert_pack;
 int gb2_add_insert_pack(gb2_ctx *ctx, const gb2_insert_pack *p);
+/* fix insert/stream (src/fix_insert_stream.cpp with src/fix_insert.cpp):
+ * particles appear in the volume swept by a planar insertion face (a fix
+ * mesh/surface, given here as its triangles) extruded against the insertion
+ * velocity's normal component v_n, move with v_n regardless of forces (their
+ * force and torque read as zero) until they reach the face, and are released
+ * there with the insertion velocity and omega.  Insertion steps: start, then
+ * every insert_every steps (or the steps v_n takes to cross extrude_length);
+ * each inserts int(rate * insert_every * dt + uniform) particles until the
+ * total (nparticles or mass; ninsert_inf for no limit) is reached.  The
+ * distribution and template fields mean what they mean for insert/pack.
+ * One insertion fix (pack or stream) per context; before gb2_setup. */
+typedef struct {
+    int seed;
+    int nface;                       /* insertion face triangles */
+    const double *face_nodes;        /* [nface][3][3], planar */
+    double nparticles;               /* total count, or 0 with mass */
+    double mass;                     /* total mass, or 0 with nparticles */
+    int ninsert_inf;                 /* 1: nparticles / mass INF */
+    double particlerate, massrate;   /* exactly one > 0 */
+    int insert_every;                /* -1: from extrude_length */
+    double extrude_length;           /* 0: from insert_every (and duration) */
+    int duration;                    /* 0: insert_every */
+    int start;                       /* first insertion step; 0 = the step after the current one */
+    int maxattempt, overlapcheck, exact_number;
+    int vel_style;                   /* 0 constant, 1 uniform, 2 gaussian */
+    double vel[3], vel_fluct[3], omega[3];
+    int ntry_mc;                     /* insertion-fraction Monte Carlo samples, default 100000 */
+    int dist_seed, dist_mass_based, ntemplates;
+    int tmpl_type[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_radius[GB2_INSERT_MAX_TEMPLATES], tmpl_density[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_weight[GB2_INSERT_MAX_TEMPLATES];
+    int tmpl_radius_style[GB2_INSERT_MAX_TEMPLATES];
+    double tmpl_radius2[GB2_INSERT_MAX_TEMPLATES];
+    int tmpl_seed[GB2_INSERT_MAX_TEMPLATES];
+    int max_atoms;
+} gb2_insert_stream;
+int gb2_add_insert_stream(gb2_ctx *ctx, const gb2_insert_stream *p);
 /* inserted count and mass so far, and the next insertion step (-1 / 0: none) */
 int gb2_insert_stats(gb2_ctx *ctx, int ifix, long *ninserted, double *massinserted, long *next_step);
 /* current mesh nodes [ntri][3][3] and node velocities (zero for a static mesh)

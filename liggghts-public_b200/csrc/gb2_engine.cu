@@ -220,6 +220,11 @@ struct gb2_ctx {
     long n_rebuild_timed = 0;
     // fix insert/pack (at most one)
     InsertPack *ins = nullptr;
+    // fix insert/stream (at most one insertion fix per context): release
+    // data of the owned atoms [4][cap] and the face elements on the device
+    InsertStream *stream = nullptr;
+    DBuf<dbl4> rel, rel_s;
+    DBuf<TriGeom> sface;
     long maxtag = 0;
     DBuf<uint8_t> insflag;
     DBuf<int> insidx;
@@ -232,6 +237,7 @@ struct gb2_ctx {
     ~gb2_ctx()
     {
         delete ins;
+        delete stream;
         if (hstage) cudaFreeHost(hstage);
     }
 };
@@ -271,6 +277,12 @@ bool host_pinned(const void *p)
 }
 
 }  // namespace
+
+// insertion fixes (defined below, in the C-linkage block), called inside a rebuild
+extern "C" {
+static int do_insert(gb2_ctx *c, bool ghosts_prev);
+static int do_insert_stream(gb2_ctx *c, bool ghosts_prev);
+}
 
 namespace {
 
@@ -349,6 +361,7 @@ Dev make_dev(gb2_ctx *c)
     D.rnum = c->rnum.p;
     D.rev = c->rev.p;
     D.revs = c->revs.p;
+    D.rel = c->stream ? c->rel.p : nullptr;
     D.maxp = c->maxp;
     D.pnum = c->pnum.p;
     D.ptag = c->ptag.p;
@@ -534,6 +547,8 @@ void neighbor_init(gb2_ctx *c)
     // future particles of an insertion fix count as dynamic (src/pair_gran.cpp:540-554)
     if (c->ins)
         for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->ins->max_rad(t));
+    if (c->stream)
+        for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->stream->max_rad(t));
     for (int i = 0; i < c->nlocal; i++) maxrad[c->h_type[i]] = std::max(maxrad[c->h_type[i]], c->h_radius[i]);
     c->triggersq = 0.25 * c->P.skin * c->P.skin;
     c->cutneighmax = 0.0;
@@ -889,6 +904,8 @@ int do_atom_sort(gb2_ctx *c)
         if (gather_slots(c->ptag, c->ptag_s, c->maxp, c->pnum.p, 1)) return GB2_ERR_CUDA;
         if (gather_slots(c->phist, c->phist_s, 3 * c->maxp, c->pnum.p, 3)) return GB2_ERR_CUDA;
         if (gather_i(c->pnum, c->pnum_s)) return GB2_ERR_CUDA;
+        if (c->stream)
+            if (gather_slots(c->rel, c->rel_s, 4, nullptr, 1)) return GB2_ERR_CUDA;
         for (int k = 0; k < c->nfix; k++) {
             HostFix &H = c->fix[k];
             if (H.kind == FIX_WALL_PLANE)
@@ -1075,7 +1092,11 @@ int do_pre_force(gb2_ctx *c)
     return 0;
 }
 
-int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
+// insert: an insertion fix adds atoms on this step.  Modify::
+// list_init_pre_exchange (src/modify.cpp:1342-1367) calls the contact-history
+// fixes first, so the pair and mesh histories are packed with the last
+// build's ghost tags before the new atoms take the first ghost slots.
+int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now, bool insert, bool ghosts_prev)
 {
     if (pre_exchange)
         if (do_partners(c)) return GB2_ERR_CUDA;
@@ -1085,6 +1106,11 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now)
             k_mesh_sort_contacts<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, k);
             CKL();
         }
+    if (insert) {
+        const int rci = c->stream ? do_insert_stream(c, ghosts_prev) : do_insert(c, ghosts_prev);
+        if (rci) return rci;
+        D = make_dev(c);
+    }
     if (clear_status(c)) return GB2_ERR_CUDA;
     k_pbc<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, c->P.boxlo[0], c->P.boxlo[1], c->P.boxlo[2], c->P.boxhi[0],
                                                   c->P.boxhi[1], c->P.boxhi[2], c->P.periodic[0], c->P.periodic[1],
@@ -1177,6 +1203,10 @@ int do_force(gb2_ctx *c, int shearupdate, int integrate, int fuse_next, int stor
     launch_tail(c, D, shearupdate, integrate, fuse_next, store_f);
     CKL();
     if (prof_end(c, &e)) return GB2_ERR_CUDA;
+    if (c->stream && integrate && !fuse_next && c->nlocal > 0) {
+        k_stream_positions<<<nblk(c->nlocal), kBlock, 0, c->st>>>(D);
+        CKL();
+    }
     if (shearupdate) c->hist.swap(c->hist2);
     if (integrate) {
         c->vel.swap(c->vel2);
@@ -1664,7 +1694,7 @@ int gb2_add_insert_pack(gb2_ctx *c, const gb2_insert_pack *p)
     if (!c || !p) return GB2_ERR_ARG;
     if (!c->have_atoms) return set_err(c, GB2_ERR_STATE, "upload atoms before adding fixes");
     if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fixes must be added before setup");
-    if (c->ins) return set_err(c, GB2_ERR_UNSUPPORTED, "one fix insert/pack per context");
+    if (c->ins || c->stream) return set_err(c, GB2_ERR_UNSUPPORTED, "one insertion fix per context");
     InsertPack *I = new InsertPack();
     const std::string e = I->init(*p, c->P.boxlo, c->P.boxhi, c->P.ntypes, c->ntimestep);
     if (!e.empty()) {
@@ -1684,9 +1714,50 @@ int gb2_add_insert_pack(gb2_ctx *c, const gb2_insert_pack *p)
     return 0;
 }
 
+int gb2_add_insert_stream(gb2_ctx *c, const gb2_insert_stream *p)
+{
+    if (!c || !p || p->nface <= 0 || !p->face_nodes) return GB2_ERR_ARG;
+    if (!c->have_atoms) return set_err(c, GB2_ERR_STATE, "upload atoms before adding fixes");
+    if (c->setup_done) return set_err(c, GB2_ERR_STATE, "fixes must be added before setup");
+    if (c->ins || c->stream) return set_err(c, GB2_ERR_UNSUPPORTED, "one insertion fix per context");
+    // the insertion face as fix mesh/surface reads it (element geometry only)
+    MeshTopo topo;
+    std::string err;
+    if (!build_mesh_topology(p->face_nodes, p->nface, 0.0, 1e-8, topo, err))
+        return set_err(c, GB2_ERR_ARG, "fix insert/stream face: %s", err.c_str());
+    InsertStream *I = new InsertStream();
+    const std::string e = I->init(*p, topo.tri, c->P.boxlo, c->P.boxhi, c->P.ntypes, c->ntimestep, c->P.dt);
+    if (!e.empty()) {
+        delete I;
+        return set_err(c, GB2_ERR_ARG, "fix insert/stream: %s", e.c_str());
+    }
+    if (p->max_atoms < c->nlocal) {
+        delete I;
+        return set_err(c, GB2_ERR_ARG, "fix insert/stream: max_atoms below the current atom count");
+    }
+    int rc = reserve_cap(c, p->max_atoms);
+    if (!rc && (c->rel.alloc((size_t)4 * c->cap) != cudaSuccess || c->sface.alloc(I->face.size()) != cudaSuccess))
+        rc = GB2_ERR_CUDA;
+    if (rc) {
+        delete I;
+        return rc;
+    }
+    CK(cudaMemsetAsync(c->rel.p, 0, sizeof(dbl4) * 4 * c->cap, c->st));
+    CK(cudaMemcpyAsync(c->sface.p, I->face.data(), sizeof(TriGeom) * I->face.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->stream = I;
+    return 0;
+}
+
 int gb2_insert_stats(gb2_ctx *c, int ifix, long *ninserted, double *massinserted, long *next_step)
 {
-    if (!c || ifix != 0 || !c->ins) return GB2_ERR_ARG;
+    if (!c || ifix != 0 || (!c->ins && !c->stream)) return GB2_ERR_ARG;
+    if (c->stream) {
+        if (ninserted) *ninserted = c->stream->ninserted;
+        if (massinserted) *massinserted = c->stream->massinserted;
+        if (next_step) *next_step = c->stream->next_reneighbor;
+        return 0;
+    }
     if (ninserted) *ninserted = c->ins->ninserted;
     if (massinserted) *massinserted = c->ins->massinserted;
     if (next_step) *next_step = c->ins->next_reneighbor;
@@ -1748,7 +1819,7 @@ int gb2_setup(gb2_ctx *c)
     if (setup_bins(c)) return GB2_ERR_ARG;
     // Verlet::setup: setup_pre_exchange, pbc, exchange, sort (always), borders,
     // neighbor build, setup_pre_force, pair (shearupdate 0), fix setup
-    int rc = do_rebuild(c, c->computeflag, c->P.sort_freq > 0);
+    int rc = do_rebuild(c, c->computeflag, c->P.sort_freq > 0, false, false);
     if (rc) return rc;
     if (do_force(c, 0, 0, 0, 1)) return GB2_ERR_CUDA;
     CK(cudaStreamSynchronize(c->st));
@@ -1756,20 +1827,24 @@ int gb2_setup(gb2_ctx *c)
         const std::string e = c->ins->setup();
         if (!e.empty()) return set_err(c, GB2_ERR_ARG, "fix insert/pack: %s", e.c_str());
     }
+    if (c->stream) {   // FixInsert::setup: FixInsertStream::calc_insertion_properties
+        const std::string e = c->stream->setup();
+        if (!e.empty()) return set_err(c, GB2_ERR_ARG, "fix insert/stream: %s", e.c_str());
+    }
     c->setup_done = true;
     c->computeflag = true;
     return 0;
 }
 
-// fix insert/pack on an insertion step, before the rebuild's history
-// packing (FixInsert::pre_exchange precedes FixContactHistory::pre_exchange,
-// which the pair style adds last): the device selects the owned particles in
-// the region and the particles near it, the host places new particles, and
-// they are appended after the owned ones -- over the first ghost slots, so
-// that, as in the reference, a ghost partner whose slot a new particle took
-// is packed with the new particle's tag.  ghosts_prev: the previous step's
-// ghost positions are in pos2 (the step's integration was fused into the
-// previous pair step and swapped the buffers).
+// fix insert/pack on an insertion step, after the rebuild's history packing
+// (the contact-history fixes run first in Modify::pre_exchange): the device
+// selects the owned particles in the region and the particles near it, the
+// host places new particles, and they are appended after the owned ones, in
+// the first ghost slots.  ghosts_prev: the previous step's ghost positions
+// are in pos2 (the step's integration was fused into the previous pair step
+// and swapped the buffers).
+static int append_inserted(gb2_ctx *c, const std::vector<InsertedParticle> &out, const char *who);
+
 static int do_insert(gb2_ctx *c, bool ghosts_prev)
 {
     InsertPack &I = *c->ins;
@@ -1820,11 +1895,19 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
     std::vector<InsertedParticle> out;
     const std::string e = I.insert(c->ntimestep, rr, rm, std::move(nearp), out);
     if (!e.empty()) return set_err(c, GB2_ERR_STATE, "fix insert/pack: %s", e.c_str());
+    return append_inserted(c, out, "fix insert/pack");
+}
+
+// The accepted particles appended after the owned ones (tags after the
+// largest, Atom::tag_extend), over the first ghost slots as create_atom does;
+// lists, partners and wall histories of the new atoms start empty.
+static int append_inserted(gb2_ctx *c, const std::vector<InsertedParticle> &out, const char *who)
+{
+    const int nl = c->nlocal, nall = c->nlocal + c->nghost;
     const int k = (int)out.size();
     if (k == 0) return 0;
     if (nl + k > c->cap)
-        return set_err(c, GB2_ERR_CAPACITY, "fix insert/pack: %d atoms exceed the %d reserved (max_atoms)", nl + k,
-                       c->cap);
+        return set_err(c, GB2_ERR_CAPACITY, "%s: %d atoms exceed the %d reserved (max_atoms)", who, nl + k, c->cap);
     if ((long)c->maxtag + k > 0x7fffffffL) return set_err(c, GB2_ERR_CAPACITY, "atom tags beyond INT_MAX");
     // Atom::tag_extend: tags beyond the largest one, in insertion order
     std::vector<dbl4> hp(k), hv(k), hw(k);
@@ -1873,6 +1956,82 @@ static int do_insert(gb2_ctx *c, bool ghosts_prev)
     return 0;
 }
 
+// fix insert/stream on an insertion step, at the same place as insert/pack:
+// the near list (FixInsertStream::is_nearby) selected on the device, the
+// placement on the host, the new atoms appended with their release data
+static int do_insert_stream(gb2_ctx *c, bool ghosts_prev)
+{
+    InsertStream &I = *c->stream;
+    const int nl = c->nlocal, nall = c->nlocal + c->nghost;
+    const dbl4 *gpos = ghosts_prev ? c->pos2.p : c->pos.p;
+    std::vector<NearParticle> nearp;
+    if (nall > 0 && I.S.overlapcheck) {
+        CK(c->insflag.alloc((size_t)nall));
+        CK(c->insidx.alloc((size_t)nall + 1));
+        StreamNear SN;
+        for (int d = 0; d < 3; d++) {
+            SN.p_ref[d] = I.p_ref[d];
+            SN.n[d] = I.normalvec[d];
+            SN.bblo[d] = I.bblo[d];
+            SN.bbhi[d] = I.bbhi[d];
+        }
+        SN.maxrad = I.maxrad;
+        SN.extrude_length = I.extrude_length;
+        SN.nface = (int)I.face.size();
+        k_ins_near_stream<<<nblk(nall), kBlock, 0, c->st>>>(c->pos.p, gpos, nl, nall, SN, c->sface.p, c->insflag.p);
+        CKL();
+        thrust::counting_iterator<int> it(0);
+        size_t bytes = 0;
+        cub::DeviceSelect::Flagged(nullptr, bytes, it, c->insflag.p, c->insidx.p, c->insidx.p + nall, nall, c->st);
+        if (cub_tmp(c, bytes)) return GB2_ERR_CUDA;
+        bytes = c->cubtmp.n;
+        CK(cub::DeviceSelect::Flagged(c->cubtmp.p, bytes, it, c->insflag.p, c->insidx.p, c->insidx.p + nall, nall,
+                                      c->st));
+        int cnt = 0;
+        CK(cudaMemcpyAsync(&cnt, c->insidx.p + nall, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (cnt > 0) {
+            CK(c->insrec.alloc(cnt));
+            k_ins_gather<<<nblk(cnt), kBlock, 0, c->st>>>(c->pos.p, c->vel.p, gpos, nl, nullptr, 0, c->insidx.p, cnt,
+                                                          c->insrec.p);
+            CKL();
+            std::vector<dbl4> rec(cnt);
+            CK(cudaMemcpyAsync(rec.data(), c->insrec.p, sizeof(dbl4) * cnt, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            nearp.resize(cnt);
+            for (int k = 0; k < cnt; k++) nearp[k] = NearParticle{{rec[k].x, rec[k].y, rec[k].z}, rec[k].w};
+        }
+    }
+    std::vector<InsertedParticle> out;
+    std::vector<StreamRelease> rel;
+    const std::string e = I.insert(c->ntimestep, std::move(nearp), out, rel);
+    if (!e.empty()) return set_err(c, GB2_ERR_STATE, "fix insert/stream: %s", e.c_str());
+    const int rc = append_inserted(c, out, "fix insert/stream");
+    if (rc) return rc;
+    const int k = (int)rel.size();
+    if (k > 0) {   // release data of the new atoms (release_fix_insert_stream)
+        std::vector<dbl4> h((size_t)4 * k);
+        for (int q = 0; q < k; q++) {
+            const StreamRelease &r = rel[q];
+            h[q] = dbl4{r.x[0], r.x[1], r.x[2], r.istep};
+            h[k + q] = dbl4{r.vint[0], r.vint[1], r.vint[2], r.rstep};
+            h[2 * k + q] = dbl4{r.vrel[0], r.vrel[1], r.vrel[2], 0.0};
+            h[3 * k + q] = dbl4{r.wrel[0], r.wrel[1], r.wrel[2], 0.0};
+        }
+        for (int sl = 0; sl < 4; sl++)
+            CK(cudaMemcpyAsync(c->rel.p + (size_t)sl * c->cap + nl, h.data() + (size_t)sl * k, sizeof(dbl4) * k,
+                               cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return 0;
+}
+
+// an insertion fix inserts on this step
+static bool ins_due(const gb2_ctx *c, long step)
+{
+    return (c->ins && c->ins->due(step)) || (c->stream && c->stream->due(step));
+}
+
 // One Verlet step.  mode 0: the rebuild decision from the device flags
 // (one host synchronisation); mode 1: a rebuild requested by a queued step;
 // mode 2: queued ahead of the decision (no rebuild, no synchronisation).
@@ -1919,7 +2078,7 @@ static int one_step(gb2_ctx *c, bool last, int mode)
         CKL();
     }
     // fix insert/pack: its next_reneighbor forces the rebuild (Neighbor::decide must_check)
-    const bool insert_now = c->ins && c->ins->due(c->ntimestep);
+    const bool insert_now = ins_due(c, c->ntimestep);
     if (insert_now) forced = true;
     bool rebuild = decide && !c->P.neigh_check && mode != 2;
     bool mesh_far = false;
@@ -1937,11 +2096,7 @@ static int one_step(gb2_ctx *c, bool last, int mode)
     if (rebuild) {
         const bool sort_now = c->P.sort_freq > 0 && c->ntimestep >= c->nextsort;
         if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
-        if (insert_now) {
-            const int rci = do_insert(c, ghosts_prev);
-            if (rci) return rci;
-        }
-        int rc = do_rebuild(c, true, sort_now);
+        int rc = do_rebuild(c, true, sort_now, insert_now, ghosts_prev);
         if (rc) return rc;
         if (prof_end(c, &e)) return GB2_ERR_CUDA;
         c->nsteps_rebuild++;
@@ -1992,7 +2147,7 @@ int gb2_run(gb2_ctx *c, int nsteps)
         if (c->fix[k].mesh && c->fix[k].mesh->moving) queueable = false;
     int s = 0;
     while (s < nsteps) {
-        if (!queueable || !c->fused_pending || (c->ins && c->ins->due(c->ntimestep + 1))) {
+        if (!queueable || !c->fused_pending || ins_due(c, c->ntimestep + 1)) {
             int rc = one_step(c, s == nsteps - 1, 0);
             if (rc) return rc;
             s++;
@@ -2013,7 +2168,7 @@ int gb2_run(gb2_ctx *c, int nsteps)
         for (;;) {
             // an insertion step is never queued (it rebuilds unconditionally)
             while (launched < nsteps && launched - head < c->queue_depth &&
-                   !(c->ins && c->ins->due(c->ntimestep + 1))) {
+                   !ins_due(c, c->ntimestep + 1)) {
                 Queued &Q = q[launched % 16];
                 Q.last = launched == nsteps - 1;
                 Q.nev = c->ev_pending.size();

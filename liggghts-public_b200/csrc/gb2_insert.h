@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/granb200.h"
+#include "gb2_internal.h"
 
 #ifdef __CUDACC__
 #define GB2_HD __host__ __device__
@@ -374,6 +375,51 @@ public:
 
     bool due(long step) const { return next_reneighbor == step && most_recent != step; }
 
+    // FixParticledistributionDiscrete::randomize_list (particles per
+    // template, exact or uncorrelated) and FixTemplateSphere::randomize_ptilist
+    // (each particle's radius from its template's generator); the list runs
+    // from large to small templates
+    void randomize(int nlocal_ins, bool exact, std::vector<int> &plist, std::vector<double> &prad)
+    {
+        const int nt = P.ntemplates;
+        int parttogen[GB2_INSERT_MAX_TEMPLATES];
+        if (!exact) {
+            for (int i = 0; i < nt; i++)
+                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i] + rdist.uniform());
+        } else {
+            int ntrunc = 0;
+            double remainder[GB2_INSERT_MAX_TEMPLATES];
+            for (int i = 0; i < nt; i++) {
+                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i]);
+                ntrunc += parttogen[i];
+                remainder[i] = static_cast<double>(nlocal_ins) * distweight[i] - static_cast<double>(parttogen[i]);
+            }
+            const int gap = nlocal_ins - ntrunc;
+            for (int i = 0; i < gap; i++) {
+                const double r = rdist.uniform() * static_cast<double>(gap);
+                int j = 0;
+                double rsum = remainder[0];
+                while (rsum < r && j < nt - 1) {
+                    j++;
+                    rsum += remainder[j];
+                }
+                parttogen[j]++;
+            }
+        }
+        std::vector<double> rad[GB2_INSERT_MAX_TEMPLATES];
+        for (int i = 0; i < nt; i++)
+            for (int j = 0; j < parttogen[i]; j++) rad[i].push_back(draw_radius(i));
+        plist.clear();
+        prad.clear();
+        for (int i = 0; i < nt; i++) {
+            const int t = distorder[i];
+            for (int j = 0; j < parttogen[t]; j++) {
+                plist.push_back(t);
+                prad.push_back(rad[t][j]);
+            }
+        }
+    }
+
     // one insertion (FixInsert::pre_exchange on step `step`): rreg_r / rreg_m
     // are radius and mass of the owned particles inside the region in index
     // order, nearp the particles near it; the accepted particles are appended
@@ -421,46 +467,9 @@ public:
             // the remainder f * n - n is zero: no gap draws
         }
         // FixParticledistributionDiscrete::randomize_list
-        const int nt = P.ntemplates;
-        int parttogen[GB2_INSERT_MAX_TEMPLATES];
-        if (!P.exact_number) {
-            for (int i = 0; i < nt; i++)
-                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i] + rdist.uniform());
-        } else {
-            int ntrunc = 0;
-            double remainder[GB2_INSERT_MAX_TEMPLATES];
-            for (int i = 0; i < nt; i++) {
-                parttogen[i] = static_cast<int>(static_cast<double>(nlocal_ins) * distweight[i]);
-                ntrunc += parttogen[i];
-                remainder[i] = static_cast<double>(nlocal_ins) * distweight[i] - static_cast<double>(parttogen[i]);
-            }
-            const int gap = nlocal_ins - ntrunc;
-            for (int i = 0; i < gap; i++) {
-                const double r = rdist.uniform() * static_cast<double>(gap);
-                int j = 0;
-                double rsum = remainder[0];
-                while (rsum < r && j < nt - 1) {
-                    j++;
-                    rsum += remainder[j];
-                }
-                parttogen[j]++;
-            }
-        }
-        // FixTemplateSphere::randomize_ptilist, template by template: each
-        // particle's radius from the template's own generator
-        std::vector<double> rad[GB2_INSERT_MAX_TEMPLATES];
-        for (int i = 0; i < nt; i++)
-            for (int j = 0; j < parttogen[i]; j++) rad[i].push_back(draw_radius(i));
-        // particles to insert, large to small templates
         std::vector<int> plist;
         std::vector<double> prad;
-        for (int i = 0; i < nt; i++) {
-            const int t = distorder[i];
-            for (int j = 0; j < parttogen[t]; j++) {
-                plist.push_back(t);
-                prad.push_back(rad[t][j]);
-            }
-        }
+        randomize(nlocal_ins, P.exact_number != 0, plist, prad);
         const int ntot = (int)plist.size();
         if (ntot == 0) {
             if (P.insert_every) next_reneighbor += P.insert_every;
@@ -522,7 +531,6 @@ public:
         return "";
     }
 
-private:
     // dense cell list over the near-list bounding box (every near particle and
     // every candidate lies in it): a test sees every particle whose sphere
     // reaches the candidate's (exact, unlike a fixed stencil); cell indices
@@ -617,6 +625,7 @@ private:
         return q;
     }
 
+private:
     // Region::generate_random / generate_random_shrinkby_cut on the block
     // within the single subdomain (the box)
     bool random_position(double *pos, double rbound)
@@ -667,5 +676,480 @@ private:
     }
 };
 
+
+
+// Release data of a particle inserted by fix insert/stream (the reference's
+// per-atom property release_fix_insert_stream): position at insertion and
+// insertion step, integration velocity v_n and release step, velocity and
+// angular velocity given at release.
+struct StreamRelease {
+    double x[3], istep;
+    double vint[3], rstep;
+    double vrel[3], wrel[3];
+};
+
+// fix insert/stream over a planar face (src/fix_insert_stream.cpp with
+// src/fix_insert.cpp), host side: the same particle distribution and
+// templates as insert/pack (an embedded InsertPack holds them), the face's
+// area-weighted random points (its own generator, MultiNodeMesh's fixed seed)
+// extruded against the normal velocity, the Monte-Carlo insertion fraction,
+// and the release data of each inserted particle.
+//   FixInsertStream::calc_insertion_properties   src/fix_insert_stream.cpp:254-373
+//   calc_ins_fraction, is_nearby, getBoundingBox,
+//   generate_random(_global), x_v_omega,
+//   finalize_insertion                          src/fix_insert_stream.cpp:469-836
+//   FixInsert::calc_ninsert_this, pre_exchange,
+//   distribute_ninsert_this                     src/fix_insert.cpp:637-914
+//   SurfaceMesh::randomOwnedGhostElement, searchElementByAreaAcc,
+//   TriMesh::generateRandomOwnedGhost, isInElement, calcArea
+//                                               src/surface_mesh_I.h:167-274, src/tri_mesh_I.h:305-401
+//   Domain::is_in_subdomain, dist_subbox_borders src/domain_I.h:65-143
+class InsertStream {
+public:
+    gb2_insert_stream S{};
+    InsertPack dist;
+    std::vector<TriGeom> face;
+    std::vector<double> area, areaAcc;
+    double area_owned = 0.;
+    double boxlo[3] = {0, 0, 0}, boxhi[3] = {0, 0, 0};
+    double v_insert[3] = {0, 0, 0}, normalvec[3] = {0, 0, 0}, v_normal[3] = {0, 0, 0}, p_ref[3] = {0, 0, 0};
+    double vn_mag = 0.;
+    double extrude_length = 0., extrude_length_min = 0., extrude_length_max = 0.;
+    int insert_every = -1, duration = 0;
+    long ninsert = 0;
+    bool ninsert_exists = true;
+    double massinsert = 0., nflowrate = 0., massflowrate = 0., ninsert_per = 0.;
+    long next_reneighbor = 0, most_recent = -1;
+    long ninserted = 0;
+    double massinserted = 0.;
+    bool exact_number = true;
+    double ins_fraction = 0.;
+    bool frac_done = false, props_done = false;
+    double maxrad = 0., maxrbound = 0.;
+    double bblo[3] = {0, 0, 0}, bbhi[3] = {0, 0, 0};   // getBoundingBox of the near list
+    double dt = 0.;
+    ParkRandom rnd, rmesh;
+
+    // the three commands' constructor checks; face = the element geometry of
+    // the insertion mesh in its element order
+    std::string init(const gb2_insert_stream &p, std::vector<TriGeom> faces, const double lo[3], const double hi[3],
+                     int ntypes, long ntimestep, double dt_)
+    {
+        S = p;
+        dt = dt_;
+        for (int d = 0; d < 3; d++) {
+            boxlo[d] = lo[d];
+            boxhi[d] = hi[d];
+        }
+        if (!insert_seed_ok(S.seed)) return "random seeds must be prime numbers > 10000";
+        // the distribution and templates through insert/pack's checks (its
+        // region and target are placeholders here and never used)
+        gb2_insert_pack q{};
+        q.seed = S.seed;
+        for (int d = 0; d < 3; d++) {
+            q.region_lo[d] = lo[d];
+            q.region_hi[d] = hi[d];
+        }
+        q.particles_in_region = 1;
+        q.maxattempt = S.maxattempt;
+        q.ntry_mc = S.ntry_mc;
+        q.vel_style = 0;
+        q.dist_seed = S.dist_seed;
+        q.dist_mass_based = S.dist_mass_based;
+        q.ntemplates = S.ntemplates;
+        for (int i = 0; i < GB2_INSERT_MAX_TEMPLATES; i++) {
+            q.tmpl_type[i] = S.tmpl_type[i];
+            q.tmpl_radius[i] = S.tmpl_radius[i];
+            q.tmpl_density[i] = S.tmpl_density[i];
+            q.tmpl_weight[i] = S.tmpl_weight[i];
+            q.tmpl_radius_style[i] = S.tmpl_radius_style[i];
+            q.tmpl_radius2[i] = S.tmpl_radius2[i];
+            q.tmpl_seed[i] = S.tmpl_seed[i];
+        }
+        q.max_atoms = S.max_atoms;
+        const std::string e = dist.init(q, lo, hi, ntypes, ntimestep);
+        if (!e.empty()) return e;
+        if (S.maxattempt <= 0 || S.ntry_mc < 1000) return "maxattempt must be > 0 and ntry_mc >= 1000";
+        if (S.vel_style < 0 || S.vel_style > 2) return "vel style must be constant, uniform or gaussian";
+        if (S.insert_every == 0) return "insert_every 0 (once) is not supported with insert/stream";
+        if (S.nparticles > 0. && S.mass > 0.) return "must not define both 'nparticles' and 'mass'";
+        if (S.particlerate > 0. && S.massrate > 0.) return "must not define both 'particlerate' and 'massrate'";
+        if (S.extrude_length < 0.) return "invalid extrude_length";
+        if (S.duration < 0) return "'duration' can not be < 1";
+        if (faces.empty()) return "must define an insertion face";
+        // TriMesh::isPlanar: every element's normal parallel to the first
+        for (const TriGeom &t : faces)
+            if (std::fabs(t.surfnorm[0] * faces[0].surfnorm[0] + t.surfnorm[1] * faces[0].surfnorm[1] +
+                          t.surfnorm[2] * faces[0].surfnorm[2]) < 1. - 1e-10)
+                return "command requires a planar face for insertion";
+        face = std::move(faces);
+        // SurfaceMesh::recalcLocalSurfProperties: area, accumulated area, owned area
+        const int n = (int)face.size();
+        area.resize(n);
+        areaAcc.resize(n);
+        area_owned = 0.;
+        for (int i = 0; i < n; i++) {
+            const TriGeom &t = face[i];
+            const double c[3] = {t.edgevec[0][1] * t.edgevec[1][2] - t.edgevec[0][2] * t.edgevec[1][1],
+                                 t.edgevec[0][2] * t.edgevec[1][0] - t.edgevec[0][0] * t.edgevec[1][2],
+                                 t.edgevec[0][0] * t.edgevec[1][1] - t.edgevec[0][1] * t.edgevec[1][0]};
+            area[i] = 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) * t.edgelen[0] * t.edgelen[1];
+            areaAcc[i] = area[i];
+            if (i > 0) areaAcc[i] += areaAcc[i - 1];
+            area_owned += area[i];
+        }
+        rnd.reset(S.seed);
+        rmesh.reset(179424799);   // MultiNodeMesh's generator
+        for (int d = 0; d < 3; d++) v_insert[d] = S.vel[d];
+        ninsert_exists = !S.ninsert_inf;
+        ninsert = ninsert_exists ? static_cast<long>(S.nparticles) : 0;
+        massinsert = S.mass;
+        nflowrate = S.particlerate;
+        massflowrate = S.massrate;
+        insert_every = S.insert_every;
+        duration = S.duration;
+        extrude_length = S.extrude_length;
+        exact_number = S.exact_number != 0;
+        maxrad = dist.maxrad;
+        maxrbound = dist.maxrbound;
+        const long first = S.start > 0 ? S.start : ntimestep + 1;
+        if (first < ntimestep + 1) return "'start' step can not be before current step";
+        next_reneighbor = first;
+        return "";
+    }
+
+    double max_rad(int type) const { return dist.max_rad(type); }
+
+    // FixInsertStream::calc_insertion_properties (FixInsert::setup, once)
+    std::string setup()
+    {
+        if (props_done) return "";
+        props_done = true;
+        for (int d = 0; d < 3; d++) normalvec[d] = face[0].surfnorm[d];
+        double dot = v_insert[0] * normalvec[0] + v_insert[1] * normalvec[1] + v_insert[2] * normalvec[2];
+        if (dot < 0)
+            for (int d = 0; d < 3; d++) normalvec[d] = normalvec[d] * -1.;
+        dot = v_insert[0] * normalvec[0] + v_insert[1] * normalvec[1] + v_insert[2] * normalvec[2];
+        for (int d = 0; d < 3; d++) v_normal[d] = normalvec[d] * dot;
+        vn_mag = std::sqrt(v_normal[0] * v_normal[0] + v_normal[1] * v_normal[1] + v_normal[2] * v_normal[2]);
+        if (vn_mag < 1.e-3) return "insertion velocity projected on face normal is < 1e-3";
+        for (int d = 0; d < 3; d++) p_ref[d] = face[0].node[0][d];
+        if (std::sqrt(v_insert[0] * v_insert[0] + v_insert[1] * v_insert[1] + v_insert[2] * v_insert[2]) < 1e-5)
+            return "insertion velocity too low";
+        if (insert_every == -1 && extrude_length == 0.) return "must define either 'insert_every' or 'extrude_length'";
+        if (insert_every > -1 && extrude_length > 0.) return "must not provide both 'insert_every' and 'extrude_length'";
+        if (extrude_length > 0. && duration > 0) return "must not provide both 'extrude_length' and 'duration'";
+        if (insert_every == -1) {
+            if (extrude_length < 3. * maxrbound && S.overlapcheck) return "'extrude_length' is too small";
+            insert_every = static_cast<int>((extrude_length + 1e-14) / (dt * vn_mag));
+            if (insert_every == 0) return "insertion velocity too high or extrude_length too low";
+        } else {
+            if (insert_every < 1) return "'insert_every' must be > 0";
+            if (duration == 0) duration = insert_every;
+            else if (duration > insert_every) return "'duration' > 'insert_every' not allowed";
+            extrude_length = static_cast<double>(duration) * dt * vn_mag;
+            if (extrude_length < 2. * maxrbound)
+                return "'insert_every' or 'vel' is too small, or (bounding) radius of inserted particles too large";
+        }
+        const double mass_expect = dist.massexpect;
+        if (ninsert == 0 && ninsert_exists) {
+            if (massinsert / mass_expect > 2.e9) return "attempting to insert more than 2e9 particles";
+            if (massinsert > 0.) ninsert = static_cast<int>((massinsert + 1e-14) / mass_expect);
+            else return "must define either 'nparticles' or 'mass'";
+        }
+        if (nflowrate == 0.) {
+            if (massflowrate == 0.) return "must define either 'massrate' or 'particlerate'";
+            nflowrate = massflowrate / mass_expect;
+        } else {
+            massflowrate = nflowrate * mass_expect;
+        }
+        ninsert_per = nflowrate * (static_cast<double>(insert_every) * dt);
+        if (ninsert_exists) massinsert = static_cast<double>(ninsert) * mass_expect;
+        extrude_length_min = 0.;
+        extrude_length_max = extrude_length;
+        // getBoundingBox: face box extruded by -(extrude_length + 2 cut), shrunk
+        // to the (single) subdomain, widened by 3 maxrad + 2 max bounding radius
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; d++) {
+            lo[d] = face[0].node[0][d];
+            hi[d] = face[0].node[0][d];
+        }
+        for (const TriGeom &t : face)
+            for (int k = 0; k < 3; k++)
+                for (int d = 0; d < 3; d++) {
+                    lo[d] = std::min(lo[d], t.node[k][d]);
+                    hi[d] = std::max(hi[d], t.node[k][d]);
+                }
+        const double cut = 3 * maxrad;
+        const double delta = -(extrude_length + 2 * cut);
+        for (int d = 0; d < 3; d++) {
+            double a = std::min(lo[d], lo[d] + delta * normalvec[d]);
+            double b = std::max(hi[d], hi[d] + delta * normalvec[d]);
+            if (a < boxlo[d]) a = boxlo[d];
+            if (b > boxhi[d]) b = boxhi[d];
+            const double extend = 3 * maxrad + 2. * maxrbound;
+            bblo[d] = a - extend;
+            bbhi[d] = b + extend;
+        }
+        return "";
+    }
+
+    bool due(long step) const { return next_reneighbor == step && most_recent != step; }
+
+    // one insertion (FixInsert::pre_exchange with FixInsertStream's parts);
+    // nearp = the owned and ghost particles FixInsertStream::is_nearby keeps
+    // inside getBoundingBox; accepted particles and their release data are
+    // appended to out / rel
+    std::string insert(long step, std::vector<NearParticle> nearp, std::vector<InsertedParticle> &out,
+                       std::vector<StreamRelease> &rel)
+    {
+        out.clear();
+        rel.clear();
+        most_recent = step;
+        // FixInsert::calc_ninsert_this
+        if (ninsert_per == 0.) return "ninsert_per == 0.";
+        int ninsert_this = static_cast<int>(ninsert_per + rnd.uniform());
+        if (ninsert_exists && ninserted + ninsert_this > ninsert) ninsert_this = static_cast<int>(ninsert - ninserted);
+        if (ninsert_exists && ninserted + ninsert_this >= ninsert) {
+            ninsert_this = static_cast<int>(ninsert - ninserted);
+            if (ninsert_this < 0) ninsert_this = 0;
+            exact_number = true;
+        }
+        // distribute_ninsert_this on one process
+        if (!frac_done) {
+            const std::string e = calc_ins_fraction();
+            if (!e.empty()) return e;
+        }
+        int nlocal_ins;
+        if (!exact_number) {
+            nlocal_ins = static_cast<int>(ins_fraction * static_cast<double>(ninsert_this) + rnd.uniform());
+        } else {
+            double f = ins_fraction;
+            if (f < 0.02) f = 0.;
+            if (f == 0.) return "Internal error distributing particles to processes";
+            f /= f;
+            nlocal_ins = static_cast<int>(f * static_cast<double>(ninsert_this));
+        }
+        std::vector<int> plist;
+        std::vector<double> prad;
+        dist.randomize(nlocal_ins, exact_number, plist, prad);
+        const int ntot = (int)plist.size();
+        if (ntot == 0) {
+            if (insert_every && (!ninsert_exists || ninserted < ninsert)) next_reneighbor += insert_every;
+            else if (0 == insert_every) next_reneighbor = -1;
+            return "";
+        }
+        // x_v_omega: positions in the extruded face, velocity v_n, no omega
+        const int maxtry = ntot * S.maxattempt;
+        int ntry = 0, done = 0;
+        double mass_this = 0.;
+        const double zero3[3] = {0., 0., 0.};
+        if (!S.overlapcheck) {
+            for (int it = 0; it < ntot; it++) {
+                const double rad = prad[done];
+                double pos[3];
+                do {
+                    generate_random(pos, rad);
+                    ntry++;
+                } while (ntry < maxtry && !in_subdomain(pos));
+                if (ntry < maxtry) {
+                    out.push_back(dist.make(plist[done], rad, pos, v_normal));
+                    for (int d = 0; d < 3; d++) out.back().omega[d] = zero3[d];
+                    mass_this += out.back().mass;
+                    done++;
+                }
+            }
+        } else {
+            NearGrid grid(bblo, bbhi, maxrad);
+            for (const NearParticle &q : nearp) grid.add(q);
+            while (ntry < maxtry && done < ntot) {
+                const double rad = prad[done];
+                int nins = 0;
+                while (nins == 0 && ntry < maxtry) {
+                    double pos[3];
+                    do {
+                        generate_random(pos, rad);
+                        ntry++;
+                    } while (ntry < maxtry && (!in_subdomain(pos) || dist_box_borders(pos) < rad));
+                    if (ntry < maxtry && !grid.overlaps(pos, rad)) {
+                        grid.add(NearParticle{{pos[0], pos[1], pos[2]}, rad});
+                        out.push_back(dist.make(plist[done], rad, pos, v_normal));
+                        for (int d = 0; d < 3; d++) out.back().omega[d] = zero3[d];
+                        nins = 1;
+                    }
+                }
+                if (nins > 0) {
+                    mass_this += out.back().mass;
+                    done++;
+                }
+            }
+        }
+        // finalize_insertion: release data, in insertion order
+        for (const InsertedParticle &a : out) {
+            StreamRelease r;
+            const double pos_rel[3] = {p_ref[0] - a.x[0], p_ref[1] - a.x[1], p_ref[2] - a.x[2]};
+            const double dist_normal = pos_rel[0] * normalvec[0] + pos_rel[1] * normalvec[1] + pos_rel[2] * normalvec[2];
+            const int n_steps = static_cast<int>((dist_normal + 1e-14) / (vn_mag * dt));
+            for (int d = 0; d < 3; d++) r.x[d] = a.x[d];
+            r.istep = static_cast<double>(step);
+            r.rstep = static_cast<double>(step + n_steps);
+            for (int d = 0; d < 3; d++) r.vint[d] = v_normal[d];
+            double v[3] = {v_insert[0], v_insert[1], v_insert[2]};
+            random_velocity(v);
+            for (int d = 0; d < 3; d++) {
+                r.vrel[d] = v[d];
+                r.wrel[d] = S.omega[d];
+            }
+            rel.push_back(r);
+        }
+        ninserted += done;
+        massinserted += mass_this;
+        if (insert_every && (!ninsert_exists || ninserted < ninsert)) next_reneighbor += insert_every;
+        else next_reneighbor = 0;
+        return "";
+    }
+
+    // FixInsertStream::is_nearby for a particle at x (the face test of the
+    // near list, SMALL_TRIMESH = 1e-10), with the list's bounding box
+    bool nearby(const double *x) const
+    {
+        if (!(x[0] >= bblo[0] && x[0] <= bbhi[0] && x[1] >= bblo[1] && x[1] <= bbhi[1] && x[2] >= bblo[2] &&
+              x[2] <= bbhi[2]))
+            return false;
+        const double pos_rel[3] = {x[0] - p_ref[0], x[1] - p_ref[1], x[2] - p_ref[2]};
+        const double dist_normal = pos_rel[0] * normalvec[0] + pos_rel[1] * normalvec[1] + pos_rel[2] * normalvec[2];
+        if (dist_normal > maxrad) return false;
+        if (dist_normal < -(extrude_length + 3. * maxrad)) return false;
+        double pp[3];
+        for (int d = 0; d < 3; d++) pp[d] = x[d] + normalvec[d] * dist_normal;
+        for (const TriGeom &t : face)
+            if (in_element(t, pp)) return true;
+        return false;
+    }
+
+private:
+    struct NearGrid : InsertPack::NearGrid {
+        NearGrid(const double *blo, const double *bhi, double maxrad_) : InsertPack::NearGrid(box(blo, bhi), maxrad_) {}
+        static InsertRegion box(const double *blo, const double *bhi)
+        {
+            InsertRegion R{};
+            for (int d = 0; d < 3; d++) {
+                R.blo[d] = blo[d];
+                R.bhi[d] = bhi[d];
+            }
+            return R;
+        }
+    };
+
+    static bool in_element(const TriGeom &t, const double *pos)
+    {
+        double v0[3], v1[3], v2[3];
+        for (int d = 0; d < 3; d++) {
+            v0[d] = t.node[2][d] - t.node[0][d];
+            v1[d] = t.node[1][d] - t.node[0][d];
+            v2[d] = pos[d] - t.node[0][d];
+        }
+        const double dot00 = v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2];
+        const double dot01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
+        const double dot02 = v0[0] * v2[0] + v0[1] * v2[1] + v0[2] * v2[2];
+        const double dot11 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+        const double dot12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+        const double invDenom = 1. / (dot00 * dot11 - dot01 * dot01);
+        const double u = (dot11 * dot02 - dot01 * dot12) * invDenom;
+        const double v = (dot00 * dot12 - dot01 * dot02) * invDenom;
+        return (u > -1e-10) && (v > -1e-10) && (u + v < 1. + 1e-10);
+    }
+
+    // SurfaceMesh::searchElementByAreaAcc (recursive in the reference)
+    int element_by_area(double a, int lo, int hi) const
+    {
+        for (;;) {
+            if ((lo < 1 || a > areaAcc[lo - 1]) && (a <= areaAcc[lo])) return lo;
+            if ((hi < 1 || a > areaAcc[hi - 1]) && (a <= areaAcc[hi])) return hi;
+            const int mid = static_cast<int>((lo + hi) / 2);
+            if (a > areaAcc[mid]) lo = mid;
+            else hi = mid;
+        }
+    }
+
+    // TriMesh::generateRandomOwnedGhost on the face
+    void face_point(double *pos)
+    {
+        const double a = area_owned + 0.;   // areaMeshOwned + areaMeshGhost (no ghosts)
+        const double r = rmesh.uniform() * a;
+        const int chosen = element_by_area(r, 0, (int)face.size() - 1);
+        double u, v;
+        do {
+            u = rmesh.uniform();
+            v = rmesh.uniform();
+        } while (u + v > 1);
+        const double b0 = 1. - u - v, b1 = v, b2 = u;
+        const TriGeom &t = face[chosen];
+        for (int d = 0; d < 3; d++) pos[d] = b0 * t.node[0][d] + b1 * t.node[1][d] + b2 * t.node[2][d];
+    }
+
+    // FixInsertStream::generate_random (all_in no)
+    void generate_random(double *pos, double rad)
+    {
+        face_point(pos);
+        double r;
+        if (S.overlapcheck) r = -1. * (rnd.uniform() * (extrude_length_max) + rad + extrude_length_min);
+        else r = -1. * (rnd.uniform() * (extrude_length_max - 2. * rad) + rad + extrude_length_min);
+        for (int d = 0; d < 3; d++) pos[d] = pos[d] + normalvec[d] * r;
+    }
+
+    // FixInsertStream::calc_ins_fraction (parallel no)
+    std::string calc_ins_fraction()
+    {
+        frac_done = true;
+        int n_in_local = 0;
+        const int n_test = S.ntry_mc;
+        for (int i = 0; i < n_test; i++) {
+            double pos[3];
+            face_point(pos);
+            const double r = -1. * (rnd.uniform() * extrude_length);
+            for (int d = 0; d < 3; d++) pos[d] = pos[d] + normalvec[d] * r;
+            if (in_subdomain(pos)) n_in_local++;
+        }
+        ins_fraction = static_cast<double>(n_in_local) / static_cast<double>(n_test);
+        if (ins_fraction < 0.9 || ins_fraction > 1.1)
+            return "insertion volume could not be distributed properly in parallel. Bad decomposition or insertion "
+                   "face extrusion is too small or outside domain";
+        return "";
+    }
+
+    // Domain::is_in_subdomain on the single subdomain (the box, padded by
+    // SMALL_DMBRDR at the box boundary)
+    bool in_subdomain(const double *pos) const
+    {
+        for (int d = 0; d < 3; d++)
+            if (!(pos[d] >= boxlo[d] - 1.0e-8 && pos[d] < boxhi[d] + 1.0e-8)) return false;
+        return true;
+    }
+
+    double dist_box_borders(const double *pos) const
+    {
+        double dlo = std::fabs(boxlo[0] - pos[0]), dhi = std::fabs(boxhi[0] - pos[0]);
+        for (int d = 1; d < 3; d++) {
+            dlo = std::min(dlo, std::fabs(boxlo[d] - pos[d]));
+            dhi = std::min(dhi, std::fabs(boxhi[d] - pos[d]));
+        }
+        return dlo < dhi ? dlo : dhi;
+    }
+
+    // FixInsert::generate_random_velocity
+    void random_velocity(double *v)
+    {
+        if (S.vel_style == 1) {
+            v[0] = v_insert[0] + S.vel_fluct[0] * 2.0 * (rnd.uniform() - 0.50);
+            v[1] = v_insert[1] + S.vel_fluct[1] * 2.0 * (rnd.uniform() - 0.50);
+            v[2] = v_insert[2] + S.vel_fluct[2] * 2.0 * (rnd.uniform() - 0.50);
+        } else if (S.vel_style == 2) {
+            v[0] = v_insert[0] + S.vel_fluct[0] * rnd.gaussian();
+            v[1] = v_insert[1] + S.vel_fluct[1] * rnd.gaussian();
+            v[2] = v_insert[2] + S.vel_fluct[2] * rnd.gaussian();
+        }
+    }
+};
 
 }  // namespace gb2

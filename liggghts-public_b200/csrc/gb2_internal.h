@@ -166,6 +166,8 @@ struct Dev {
     int *dflag;              // displacement trigger
     int *dstop;              // queued-ahead steps: lowest step whose tail asked for a rebuild (null when not queuing)
     int step;                // step number of this launch (compared with *dstop)
+    const dbl4 *rel;         // fix insert/stream release data [4*cap] (null without a stream):
+                             // {x_ins, i_step} {v_int, r_step} {v_release, -} {omega_release, -}
     int *need;               // [4] capacity demand seen by the last overflowing kernel:
                              // neighbour slots, partners, reverse entries, mesh slots
 };

@@ -926,6 +926,55 @@ __global__ void k_ins_flags(const dbl4 *pos, const dbl4 *gpos, int nlocal, int n
     fnear[i] = R.near(x, p.w) ? 1 : 0;
 }
 
+// fix insert/stream's near list (FixInsertStream::is_nearby with the list's
+// bounding box, src/fix_insert_stream.cpp:573-615): inside the box, within
+// maxrad in front of the face plane and extrude_length + 3 maxrad behind it,
+// and the point x + n d (d = the signed distance to the plane, as the
+// reference forms it) inside one of the face's triangles
+struct StreamNear {
+    double p_ref[3], n[3], bblo[3], bbhi[3];
+    double maxrad, extrude_length;
+    int nface;
+};
+
+__global__ void k_ins_near_stream(const dbl4 *pos, const dbl4 *gpos, int nlocal, int nall, StreamNear S,
+                                  const TriGeom *face, uint8_t *fnear)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nall) return;
+    const dbl4 p = i < nlocal ? pos[i] : gpos[i];
+    const double x[3] = {p.x, p.y, p.z};
+    uint8_t near = 0;
+    if (x[0] >= S.bblo[0] && x[0] <= S.bbhi[0] && x[1] >= S.bblo[1] && x[1] <= S.bbhi[1] && x[2] >= S.bblo[2] &&
+        x[2] <= S.bbhi[2]) {
+        const double rel[3] = {x[0] - S.p_ref[0], x[1] - S.p_ref[1], x[2] - S.p_ref[2]};
+        const double d = rel[0] * S.n[0] + rel[1] * S.n[1] + rel[2] * S.n[2];
+        if (!(d > S.maxrad) && !(d < -(S.extrude_length + 3. * S.maxrad))) {
+            double pp[3];
+            for (int c = 0; c < 3; c++) pp[c] = x[c] + S.n[c] * d;
+            for (int t = 0; t < S.nface && !near; t++) {   // TriMesh::isInElement
+                const TriGeom &T = face[t];
+                double v0[3], v1[3], v2[3];
+                for (int c = 0; c < 3; c++) {
+                    v0[c] = T.node[2][c] - T.node[0][c];
+                    v1[c] = T.node[1][c] - T.node[0][c];
+                    v2[c] = pp[c] - T.node[0][c];
+                }
+                const double dot00 = v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2];
+                const double dot01 = v0[0] * v1[0] + v0[1] * v1[1] + v0[2] * v1[2];
+                const double dot02 = v0[0] * v2[0] + v0[1] * v2[1] + v0[2] * v2[2];
+                const double dot11 = v1[0] * v1[0] + v1[1] * v1[1] + v1[2] * v1[2];
+                const double dot12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+                const double invDenom = 1. / (dot00 * dot11 - dot01 * dot01);
+                const double u = (dot11 * dot02 - dot01 * dot12) * invDenom;
+                const double v = (dot00 * dot12 - dot01 * dot02) * invDenom;
+                if ((u > -1e-10) && (v > -1e-10) && (u + v < 1. + 1e-10)) near = 1;
+            }
+        }
+    }
+    fnear[i] = near;
+}
+
 // records of the selected particles: region ones (radius, mass) first, then
 // near ones (x, y, z, radius)
 __global__ void k_ins_gather(const dbl4 *pos, const dbl4 *vel, const dbl4 *gpos, int nlocal, const int *ireg, int nreg,

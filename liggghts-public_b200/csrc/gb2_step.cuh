@@ -180,11 +180,48 @@ __device__ __forceinline__ void pair_total(const Real *as, const Real *kc, Conta
 
 // store_f / FixNVESphere::final_integrate / the next step's initial_integrate
 // with the displacement test, for one atom whose total force is in acc
+// FixInsertStream::end_of_step (src/fix_insert_stream.cpp:868-935) for atom
+// i: a particle the stream inserted and has not released moves with its
+// integration velocity from its insertion position (x = x_ins + v_int
+// (step - i_step) dt, v = v_int, omega = 0); at its release step it gets the
+// release velocity and omega.  Returns true when it applies; the atom's
+// force and torque then read zero.
+__device__ __forceinline__ bool stream_hold(const Dev &D, int i, dbl4 &x, dbl4 &v, dbl4 &w)
+{
+    const dbl4 r0 = D.rel[i];
+    if (r0.w < 1e-13 && r0.w > -1e-13) return false;   // never inserted by the stream
+    const dbl4 r1 = D.rel[D.cap + i];
+    const int i_step = static_cast<int>(r0.w + 1e-14);
+    const int r_step = static_cast<int>(r1.w + 1e-14);
+    if (D.step > r_step) return false;
+    const double time_elapsed = (D.step - i_step) * D.dt;
+    x.x = r0.x + r1.x * time_elapsed;
+    x.y = r0.y + r1.y * time_elapsed;
+    x.z = r0.z + r1.z * time_elapsed;
+    if (D.step == r_step) {
+        const dbl4 r2 = D.rel[2 * D.cap + i], r3 = D.rel[3 * D.cap + i];
+        v.x = r2.x, v.y = r2.y, v.z = r2.z;
+        w.x = r3.x, w.y = r3.y, w.z = r3.z;
+    } else {
+        v.x = r1.x, v.y = r1.y, v.z = r1.z;
+        w.x = 0.0, w.y = 0.0, w.z = 0.0;
+    }
+    return true;
+}
+
 template <bool SPLIT>
 __device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const dbl4 &pi, dbl4 vi4, dbl4 wi4,
                                                      const dbl4 &hold, int integrate, int fuse_next, int store_f,
-                                                     const ContactOut &acc)
+                                                     const ContactOut &acc_in)
 {
+    // an atom held by fix insert/stream ends the step where end_of_step puts
+    // it, with zero force and torque (the next initial_integrate reads them)
+    ContactOut acc = acc_in;
+    dbl4 pcur = pi;
+    if (D.rel && integrate && stream_hold(D, i, pcur, vi4, wi4)) {
+        for (int c = 0; c < 3; c++) acc.F[c] = acc.T[c] = 0.0;
+        integrate = 2;   // final_integrate's result is replaced
+    }
     if (store_f) {
         dbl4 Fo, To;
         Fo.x = acc.F[0];
@@ -203,13 +240,15 @@ __device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const 
         const double dtf = 0.5 * D.dt * 1.0;
         const double dtfrotate = dtf / 0.4;
         const double dtfm = dtf / (vi4.w * 1.0);
-        vi4.x += dtfm * acc.F[0];
-        vi4.y += dtfm * acc.F[1];
-        vi4.z += dtfm * acc.F[2];
         const double dtirotate = dtfrotate / (pi.w * pi.w * vi4.w);
-        wi4.x += dtirotate * acc.T[0];
-        wi4.y += dtirotate * acc.T[1];
-        wi4.z += dtirotate * acc.T[2];
+        if (integrate == 1) {
+            vi4.x += dtfm * acc.F[0];
+            vi4.y += dtfm * acc.F[1];
+            vi4.z += dtfm * acc.F[2];
+            wi4.x += dtirotate * acc.T[0];
+            wi4.y += dtirotate * acc.T[1];
+            wi4.z += dtirotate * acc.T[2];
+        }
         if (fuse_next) {
             // next step's FixNVESphere::initial_integrate with the same force,
             // then Neighbor::check_distance's displacement test
@@ -217,7 +256,7 @@ __device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const 
             vi4.x += dtfm * acc.F[0];
             vi4.y += dtfm * acc.F[1];
             vi4.z += dtfm * acc.F[2];
-            dbl4 p = pi;
+            dbl4 p = pcur;
             p.x += dtv * vi4.x;
             p.y += dtv * vi4.y;
             p.z += dtv * vi4.z;
@@ -236,6 +275,16 @@ __device__ __forceinline__ void atom_store_integrate(const Dev &D, int i, const 
         D.omg_out[i] = wi4;
         if constexpr (SPLIT) D.kin_out[i] = make_kin(vi4, wi4);
     }
+}
+
+// The last step of a run (no fused initial_integrate): positions of the atoms
+// fix insert/stream holds, set in place once the step's kernels are done.
+static __global__ void k_stream_positions(Dev D)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.nlocal) return;
+    dbl4 x = D.pos[i], v, w;
+    if (stream_hold(D, i, x, v, w)) D.pos[i] = x;
 }
 
 // Shear of own slots that stopped touching this step is carried into the

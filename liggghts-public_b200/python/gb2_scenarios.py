@@ -811,6 +811,40 @@ def subset(sc, n):
     return out
 
 
+def stream_pour(n_bed=400, seed=78, periodic=True, nparticles=300, particlerate=20000.0, insert_every=200,
+                vel=(0.0, 0.0, -2.0), vel_style="uniform", exact_number=1, max_atoms=2000):
+    """fix insert/stream above a bed: the 20 x 20 x 60 mm box of insert_pour
+    (x/y periodic or walled, n_bed spheres of r = 1 mm at the bottom, dt
+    1e-5), an insertion face of two triangles spanning x, y in 2-18 mm at
+    z = 40 mm, the same two templates (r = 1.2 and 0.8 mm, mass fractions
+    0.5 / 0.5), particles inserted every insert_every steps at particlerate
+    per second up to nparticles, moving down at the insertion velocity's
+    normal part until they cross the face, released there with the
+    insertion velocity (+- 0.1 m/s per component for vel uniform)."""
+    sc = sphere_pour(n=n_bed, seed=seed, box=(0.02, 0.02, 0.06), spacing=(2.5e-3, 2.5e-3, 2.4e-3), vmax=0.05)
+    sc["name"] = "stream_pour"
+    sc["periodic"] = [1, 1, 0] if periodic else [0, 0, 0]
+    fixes = [sc["fixes"][0], sc["fixes"][1]]
+    if not periodic:
+        for dim in (0, 1):
+            fixes.append({"kind": "wall_plane", "dim": dim, "pos": 0.0, "wall_type": 1, "rolling_cdt": 0})
+            fixes.append({"kind": "wall_plane", "dim": dim, "pos": 0.02, "wall_type": 1, "rolling_cdt": 0})
+    z = 0.04
+    face = np.array([[0.002, 0.002, z, 0.018, 0.002, z, 0.018, 0.018, z],
+                     [0.002, 0.002, z, 0.018, 0.018, z, 0.002, 0.018, z]])
+    fx = {
+        "kind": "insert_stream", "seed": 32452867, "dist_seed": 15485867, "face_nodes": face,
+        "nparticles": nparticles, "particlerate": particlerate, "insert_every": insert_every,
+        "exact_number": exact_number, "vel_style": vel_style, "vel": list(vel), "vel_fluct": [0.1, 0.1, 0.1],
+        "templates": [{"type": 1, "radius": 1.2e-3, "density": 2500.0, "weight": 0.5, "seed": 67867979},
+                      {"type": 1, "radius": 0.8e-3, "density": 2500.0, "weight": 0.5, "seed": 86028157}],
+        "max_atoms": max_atoms,
+    }
+    fixes += [fx, {"kind": "nve_sphere"}]
+    sc["fixes"] = fixes
+    return sc
+
+
 def insert_pour(n_bed=400, seed=77, periodic=True, dt=2e-6, vel_style="uniform", all_in=0, exact_number=1,
                 target=("volumefraction_region", 0.25), insert_every=300, max_atoms=8000, polydisperse=False,
                 cylinder=False):

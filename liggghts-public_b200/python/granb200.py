@@ -31,7 +31,7 @@ EXPORTS = (
     "gb2_add_move_mesh_linear", "gb2_add_wall_cylinder", "gb2_contact_atom",
     "gb2_upload_history", "gb2_download_history", "gb2_upload_wall_history", "gb2_add_mesh_stress",
     "gb2_download_mesh_stress", "gb2_pair_gran_local",
-    "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_insert_stats", "gb2_download_mesh_history",
+    "gb2_pair_gran_local_keys", "gb2_add_insert_pack", "gb2_add_insert_stream", "gb2_insert_stats", "gb2_download_mesh_history",
     "gb2_upload_mesh_history", "gb2_add_mesh_wear", "gb2_download_mesh_wear", "gb2_upload_mesh_wear", "gb2_host_alloc", "gb2_host_free", "gb2_set_timestep",
 )
 
@@ -110,6 +110,43 @@ class InsertPackParams(ctypes.Structure):
     ]
 
 
+class InsertStreamParams(ctypes.Structure):
+    """gb2_insert_stream: fix insert/stream + particledistribution/discrete + particletemplate/sphere."""
+    _fields_ = [
+        ("seed", ctypes.c_int),
+        ("nface", ctypes.c_int),
+        ("face_nodes", ctypes.POINTER(ctypes.c_double)),
+        ("nparticles", ctypes.c_double),
+        ("mass", ctypes.c_double),
+        ("ninsert_inf", ctypes.c_int),
+        ("particlerate", ctypes.c_double),
+        ("massrate", ctypes.c_double),
+        ("insert_every", ctypes.c_int),
+        ("extrude_length", ctypes.c_double),
+        ("duration", ctypes.c_int),
+        ("start", ctypes.c_int),
+        ("maxattempt", ctypes.c_int),
+        ("overlapcheck", ctypes.c_int),
+        ("exact_number", ctypes.c_int),
+        ("vel_style", ctypes.c_int),
+        ("vel", ctypes.c_double * 3),
+        ("vel_fluct", ctypes.c_double * 3),
+        ("omega", ctypes.c_double * 3),
+        ("ntry_mc", ctypes.c_int),
+        ("dist_seed", ctypes.c_int),
+        ("dist_mass_based", ctypes.c_int),
+        ("ntemplates", ctypes.c_int),
+        ("tmpl_type", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("tmpl_radius", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_density", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_weight", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_radius_style", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("tmpl_radius2", ctypes.c_double * INSERT_MAX_TEMPLATES),
+        ("tmpl_seed", ctypes.c_int * INSERT_MAX_TEMPLATES),
+        ("max_atoms", ctypes.c_int),
+    ]
+
+
 VEL_STYLES = {"constant": 0, "uniform": 1, "gaussian": 2}
 RADIUS_STYLES = {"constant": 0, "uniform": 1, "gaussian": 2}
 
@@ -158,6 +195,51 @@ def insert_pack_params(fx, struct=InsertPackParams):
         p.tmpl_seed[i] = int(t.get("seed", 67867967))
     p.max_atoms = int(fx.get("max_atoms", 0))
     return p
+
+
+def insert_stream_params(fx):
+    """(struct, face node array to keep alive) of a scenario's insert_stream fix."""
+    p = InsertStreamParams()
+    face = np.ascontiguousarray(np.asarray(fx["face_nodes"], dtype=np.float64).reshape(-1, 9))
+    p.seed = int(fx["seed"])
+    p.nface = len(face)
+    p.face_nodes = face.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    p.nparticles = float(fx.get("nparticles", 0))
+    p.mass = float(fx.get("mass", 0.0))
+    p.ninsert_inf = int(fx.get("nparticles") == "INF" or fx.get("mass") == "INF")
+    if p.ninsert_inf:
+        p.nparticles = p.mass = 0.0
+    p.particlerate = float(fx.get("particlerate", 0.0))
+    p.massrate = float(fx.get("massrate", 0.0))
+    p.insert_every = int(fx.get("insert_every", -1))
+    p.extrude_length = float(fx.get("extrude_length", 0.0))
+    p.duration = int(fx.get("duration", 0))
+    p.start = int(fx.get("start", 0))
+    p.maxattempt = int(fx.get("maxattempt", 50))
+    p.overlapcheck = int(fx.get("overlapcheck", 1))
+    p.exact_number = int(fx.get("exact_number", 1))
+    p.vel_style = VEL_STYLES[fx.get("vel_style", "constant")]
+    for d in range(3):
+        p.vel[d] = fx.get("vel", (0.0, 0.0, 0.0))[d]
+        p.vel_fluct[d] = fx.get("vel_fluct", (0.0, 0.0, 0.0))[d]
+        p.omega[d] = fx.get("omega", (0.0, 0.0, 0.0))[d]
+    p.ntry_mc = int(fx.get("ntry_mc", 100000))
+    p.dist_seed = int(fx["dist_seed"])
+    p.dist_mass_based = int(fx.get("dist_mass_based", 1))
+    tm = fx["templates"]
+    if not 1 <= len(tm) <= INSERT_MAX_TEMPLATES:
+        raise ValueError("1 to %d templates" % INSERT_MAX_TEMPLATES)
+    p.ntemplates = len(tm)
+    for i, t in enumerate(tm):
+        p.tmpl_type[i] = int(t["type"])
+        p.tmpl_radius[i] = float(t["radius"])
+        p.tmpl_density[i] = float(t["density"])
+        p.tmpl_weight[i] = float(t["weight"])
+        p.tmpl_radius_style[i] = RADIUS_STYLES[t.get("radius_style", "constant")]
+        p.tmpl_radius2[i] = float(t.get("radius2", 0.0))
+        p.tmpl_seed[i] = int(t.get("seed", 67867967))
+    p.max_atoms = int(fx.get("max_atoms", 0))
+    return p, face
 
 
 class Params(ctypes.Structure):
@@ -247,6 +329,7 @@ def lib(path=LIB_PATH):
         L.gb2_download_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, I, I, I, I, I, D]
         L.gb2_upload_mesh_history.argtypes = [vp, ctypes.c_int, ctypes.c_int, I, I, D]
         L.gb2_add_insert_pack.argtypes = [vp, ctypes.POINTER(InsertPackParams)]
+        L.gb2_add_insert_stream.argtypes = [vp, ctypes.POINTER(InsertStreamParams)]
         L.gb2_insert_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long), D,
                                        ctypes.POINTER(ctypes.c_long)]
         L.gb2_pair_gran_local_keys.argtypes = [vp, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
@@ -401,6 +484,11 @@ class Engine:
                 ip = insert_pack_params(fx)
                 keep.append(ip)
                 self._check(L.gb2_add_insert_pack(self.h, ctypes.byref(ip)))
+                k = 0
+            elif kind == "insert_stream":
+                ip, face = insert_stream_params(fx)
+                keep += [ip, face]
+                self._check(L.gb2_add_insert_stream(self.h, ctypes.byref(ip)))
                 k = 0
             else:
                 raise ValueError("unsupported fix kind " + kind)

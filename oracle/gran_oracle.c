@@ -2355,8 +2355,9 @@ static double ins_dist_borders(orc_sim *s, const double *pos)
 }
 
 /* FixInsert::pre_exchange src/fix_insert.cpp:652-827 for fix insert/pack on
-   one process; appends the new atoms after the owned ones (over the first
-   ghost slots, as Atom::avec->create_atom does) with tags from tag_extend */
+   one process; appends the new atoms after the owned ones (in the first
+   ghost slots, as Atom::avec->create_atom does, after the contact histories
+   were packed) with tags from tag_extend */
 static void ins_pre_exchange(orc_sim *s)
 {
     struct ins_state *I = s->ins;
@@ -2609,9 +2610,12 @@ int orc_run(orc_sim *s, int nsteps)
         int nflag = neighbor_decide(s);
         if (nflag == 0) comm_forward(s);
         else {
-            if (s->ins) { ins_pre_exchange(s); if (s->err[0]) return -1; }   /* fix insert precedes the history fix */
+            /* Modify::list_init_pre_exchange (src/modify.cpp:1342-1367) calls the
+               contact-history fixes first: histories are packed with the ghost
+               tags of the last build, then fix insert appends its atoms */
             history_pre_exchange(s);
             for (int k = 0; k < s->nfix; k++) if (s->fix[k].wm) mesh_sort_contacts(s, s->fix[k].wm);
+            if (s->ins) { ins_pre_exchange(s); if (s->err[0]) return -1; }
             domain_pbc(s);
             if (comm_exchange_check(s)) return -1;
             if (s->p.sortfreq > 0 && s->ntimestep >= s->nextsort) atom_sort(s);

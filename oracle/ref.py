@@ -170,6 +170,8 @@ def script(sc, workdir, segments, dump_names=None, thermo=0):
             lines.append("fix f%d all nve/sphere" % k)
         elif kind == "insert_pack":
             lines += _insert_pack(fx, k)
+        elif kind == "insert_stream":
+            lines += _insert_stream(fx, k, workdir)
         else:
             raise ValueError("no reference input for fix kind %r" % kind)
     lines.append("thermo %d" % thermo)
@@ -229,6 +231,65 @@ def _insert_pack(fx, k):
         if key in fx:
             cmd += " %s %s" % (key, _g(fx[key]) if key != "particles_in_region" else "%d" % int(fx[key]))
     cmd += " region ins%d" % k
+    out.append(cmd)
+    return out
+
+
+def _distribution(fx, k):
+    """fix particletemplate/sphere (one per template) and fix
+    particledistribution/discrete for an insertion fix."""
+    out, names = [], []
+    for t, tp in enumerate(fx["templates"]):
+        if tp.get("radius_style", "constant") != "constant":
+            raise ValueError("the reference's particletemplate/sphere takes only 'radius constant'")
+        nm = "pts%d_%d" % (k, t)
+        names.append(nm)
+        out.append("fix %s all particletemplate/sphere %d atom_type %d density constant %s radius constant %s" % (
+            nm, int(tp.get("seed", 67867967)), int(tp["type"]), _g(tp["density"]), _g(tp["radius"])))
+    style = "particledistribution/discrete" if int(fx.get("dist_mass_based", 1)) else \
+        "particledistribution/discrete/numberbased"
+    out.append("fix pdd%d all %s %d %d %s" % (k, style, int(fx["dist_seed"]), len(names),
+                                              " ".join("%s %s" % (nm, _g(tp["weight"]))
+                                                       for nm, tp in zip(names, fx["templates"]))))
+    return out
+
+
+def _insert_stream(fx, k, workdir):
+    """The insertion face as fix mesh/surface (an STL) and fix insert/stream
+    (src/fix_insert.cpp:118-290 keywords first, then
+    src/fix_insert_stream.cpp:71-150's)."""
+    out = _distribution(fx, k)
+    stl = os.path.join(workdir, "face%d.stl" % k)
+    write_stl(stl, np.asarray(fx["face_nodes"], dtype=np.float64).reshape(-1, 3, 3))
+    out.append("fix face%d all mesh/surface file %s type 1" % (k, stl))
+    vs = fx.get("vel_style", "constant")
+    v = fx.get("vel", (0.0, 0.0, 0.0))
+    vel = "vel constant %s %s %s" % tuple(_g(c) for c in v) if vs == "constant" else \
+        "vel %s %s %s %s %s %s %s" % ((vs,) + tuple(_g(c) for c in v) + tuple(_g(c) for c in fx["vel_fluct"]))
+    w = fx.get("omega", (0.0, 0.0, 0.0))
+    yn = lambda v: "yes" if int(v) else "no"
+    cmd = "fix f%d all insert/stream seed %d distributiontemplate pdd%d" % (k, int(fx["seed"]), k)
+    if fx.get("nparticles") is not None:
+        cmd += " nparticles %s" % ("INF" if fx["nparticles"] == "INF" else "%d" % int(fx["nparticles"]))
+    if fx.get("mass") is not None:
+        cmd += " mass %s" % ("INF" if fx["mass"] == "INF" else _g(fx["mass"]))
+    if fx.get("particlerate"):
+        cmd += " particlerate %s" % _g(fx["particlerate"])
+    if fx.get("massrate"):
+        cmd += " massrate %s" % _g(fx["massrate"])
+    if int(fx.get("insert_every", -1)) > 0:
+        cmd += " insert_every %d" % int(fx["insert_every"])
+    if int(fx.get("start", 0)):
+        cmd += " start %d" % int(fx["start"])
+    cmd += " maxattempt %d overlapcheck %s all_in no random_distribute %s %s omega constant %s %s %s" % (
+        int(fx.get("maxattempt", 50)), yn(fx.get("overlapcheck", 1)),
+        "exact" if int(fx.get("exact_number", 1)) else "uncorrelated", vel, _g(w[0]), _g(w[1]), _g(w[2]))
+    cmd += " insertion_face face%d" % k
+    if float(fx.get("extrude_length", 0.0)) > 0:
+        cmd += " extrude_length %s" % _g(fx["extrude_length"])
+    if int(fx.get("duration", 0)):
+        cmd += " duration %d" % int(fx["duration"])
+    cmd += " ntry_mc %d" % int(fx.get("ntry_mc", 100000))
     out.append(cmd)
     return out
 

@@ -86,6 +86,15 @@ SCENES = {
                                                         insert_every=250), [0, 300, 300, 300, 300]),
 }
 
+# fix insert/stream: the reference (live, CPU) and the engine (GPU) are
+# compared with the digests; the oracle restates insert/pack only
+STREAM_SCENES = {
+    "stream_insert_periodic": (S.stream_pour, [0, 300, 300, 300, 300, 300]),
+    "stream_insert_walled": (lambda: S.stream_pour(periodic=False, vel_style="constant", exact_number=0,
+                                                   particlerate=15000.0, vel=(0.0, 0.0, -1.5)),
+                             [0, 300, 300, 300, 300, 300]),
+}
+
 # Too long for the reference or the oracle inside the CPU test run (the
 # reference needs ~110 s); pinned by committed digests and run on the GPU.
 LONG_SCENES = {
@@ -93,7 +102,7 @@ LONG_SCENES = {
     "config2_hopper_1M_100steps": (S.hopper_packed, [0, 100]),
 }
 
-ALL_SCENES = dict(SCENES, **LONG_SCENES)
+ALL_SCENES = dict(SCENES, **STREAM_SCENES, **LONG_SCENES)
 
 
 def _h(*arrays):

@@ -24,7 +24,7 @@ import pytest
 
 import oracle
 import ref
-from ref_scenes import ALL_SCENES, SCENES, digest_dump, digest_sim, first_difference
+from ref_scenes import ALL_SCENES, SCENES, STREAM_SCENES, digest_dump, digest_sim, first_difference
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_digests.json")
 with open(GOLDEN) as _f:
@@ -70,12 +70,12 @@ def test_golden_covers_every_scene():
     assert last["config1_pour_20k_20000steps"]["ntouch"] > 40000
 
 
-@pytest.mark.parametrize("name", sorted(SCENES))
+@pytest.mark.parametrize("name", sorted(SCENES) + sorted(STREAM_SCENES))
 def test_reference_reproduces_golden(name):
     """The committed digests are the reference's output (live run here)."""
     if not _ref_available():
         pytest.skip("reference not built and its sources are absent")
-    build, segments = SCENES[name]
+    build, segments = ALL_SCENES[name]
     sc = build()
     got = [digest_dump(sc, d) for d in ref.run(sc, segments)]
     _compare(name, got)
