@@ -4,9 +4,10 @@
 //
 // Step sequence as Verlet::run with these styles: initial_integrate,
 // displacement check, neighbour rebuild with contact-history transfer when
-// any particle moved more than skin/2, pair pass (one thread per half-list
-// slot), deterministic per-particle sums (reverse slots in ascending owner
-// order, then own slots), final_integrate.
+// any particle moved more than skin/2, pair pass (screening of every
+// half-list slot, then the contact-point solves in work lists by kind),
+// deterministic per-particle sums (reverse slots in ascending owner order,
+// then own slots), final_integrate.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -236,6 +237,10 @@ struct gb2_sq_ctx {
     Buf<float> mlp;
     bool mlp_on = false;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // work lists of the pair pass: 2 lists of nslots items, then the item
+    // counts and the taken counter
+    Buf<int> work;
+    int nsm = 148;
 };
 
 namespace {
@@ -393,6 +398,7 @@ int sq_build(gb2_sq_ctx *c, bool transfer)
     SQCK(c->pfi.alloc(ns));
     SQCK(c->pti.alloc(ns));
     SQCK(c->ptj.alloc(ns));
+    SQCK(c->work.alloc(2 * ns + 4));
     SQCK(c->rslot.alloc(ns));
     D = sq_dev(c);
     k_sq_neigh<<<nb(n), kB, 0, c->st>>>(D, G, c->cell_start.p, c->cell_atoms.p, nullptr, c->nbr.p, c->own.p, 1);
@@ -429,11 +435,26 @@ int sq_build(gb2_sq_ctx *c, bool transfer)
     return 0;
 }
 
+// the pair pass in work lists (screen, then the solves of the first contacts
+// and the warm starts), then the per-particle sums
 int sq_force(gb2_sq_ctx *c, int shearupdate)
 {
     SqDev D = sq_dev(c);
-    if (c->nslots > 0) k_sq_pair<<<nb(c->nslots), kB, 0, c->st>>>(D, c->own.p, (int)c->nslots, shearupdate);
-    SQCKL();
+    if (c->nslots > 0) {
+        const size_t ns = (size_t)c->nslots;
+        SqWork W;
+        for (int l = 0; l < 2; l++) W.list[l] = c->work.p + l * ns;
+        W.n = c->work.p + 2 * ns;
+        W.next = W.n + 2;
+        SQCK(cudaMemsetAsync(W.n, 0, 4 * sizeof(int), c->st));
+        k_sq_screen<<<nb(c->nslots), kB, 0, c->st>>>(D, c->own.p, (int)c->nslots, W);
+        SQCKL();
+        // the solves: enough resident warps to fill the GPU; each warp takes
+        // the next 32 items (first contacts, then warm starts) until none
+        // are left
+        k_sq_solve<<<2 * c->nsm, kB, 0, c->st>>>(D, W, c->own.p, shearupdate);
+        SQCKL();
+    }
     k_sq_sum<<<nb(c->n), kB, 0, c->st>>>(D);
     SQCKL();
     return 0;
@@ -452,6 +473,8 @@ int gb2_sq_create(const gb2_sq_params *p, gb2_sq_ctx **out)
     if (cudaSetDevice(p->device) != cudaSuccess) return GB2_ERR_CUDA;
     gb2_sq_ctx *c = new gb2_sq_ctx();
     c->P = *p;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, p->device);
+    if (c->nsm <= 0) c->nsm = 1;
     // material constants (src/global_properties.cpp:432-540), one atom type
     const double E = p->youngs, nu = p->poisson;
     c->Yeff = 1. / ((1. - std::pow(nu, 2.)) / E + (1. - std::pow(nu, 2.)) / E);

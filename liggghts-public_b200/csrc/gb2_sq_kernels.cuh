@@ -230,9 +230,29 @@ __device__ __forceinline__ void mlp_infer(const float *__restrict__ P, const flo
 // defeat both methods no longer pay the full iteration bound twice.
 constexpr int kLearnedNewton = 48;
 
-// Contact point of a pair without a previous point: the learned guess, one
-// Newton solve (at most kLearnedNewton iterations), and the homotopy as the
-// fallback when that solve does not reach the merit tolerance.
+// Contact point of a pair without a previous point from the learned guess:
+// the network's point and mu, then one Newton solve of at most
+// kLearnedNewton iterations.  The caller accepts it when it converged to
+// merit < 1e-10 and otherwise runs the homotopy.
+__device__ __forceinline__ void used_learned_guess(const float *mlp, const double *ci, const double *qi,
+                                                   const double *si, double ni, const double *cj, const double *qj,
+                                                   const double *sj, double nj, Newton &o, int &iters, int &solves)
+{
+    double Ri[9];
+    quat_to_mat(qi, Ri);
+    float feat[kMlpIn], out[kMlpOut];
+    const double s = pair_features(ci, qi, si, ni, cj, qj, sj, nj, Ri, feat);
+    mlp_infer(mlp, feat, out);
+    const double pl[3] = {out[0] * s, out[1] * s, out[2] * s};
+    double g[3];
+    matvec(Ri, pl, g);
+    for (int k = 0; k < 3; k++) g[k] += ci[k];
+    contact_point<kLearnedNewton>(ci, qi, si, ni, cj, qj, sj, nj, 1, g, true, (double)fabsf(out[3]), o, iters,
+                                  solves);
+}
+
+// Contact point of a pair without a previous point in one call: the learned
+// guess when a network is given, the homotopy when it is rejected or absent.
 // used: 1 learned guess accepted, -1 rejected, 0 off.
 __device__ __forceinline__ void first_contact(const float *mlp, const double *ci, const double *qi, const double *si,
                                               double ni, const double *cj, const double *qj, const double *sj,
@@ -240,18 +260,8 @@ __device__ __forceinline__ void first_contact(const float *mlp, const double *ci
 {
     used = 0;
     if (mlp) {
-        double Ri[9];
-        quat_to_mat(qi, Ri);
-        float feat[kMlpIn], out[kMlpOut];
-        const double s = pair_features(ci, qi, si, ni, cj, qj, sj, nj, Ri, feat);
-        mlp_infer(mlp, feat, out);
-        const double pl[3] = {out[0] * s, out[1] * s, out[2] * s};
-        double g[3];
-        matvec(Ri, pl, g);
-        for (int k = 0; k < 3; k++) g[k] += ci[k];
         int it1, sv1;
-        contact_point<kLearnedNewton>(ci, qi, si, ni, cj, qj, sj, nj, 1, g, true, (double)fabsf(out[3]), o, it1,
-                                      sv1);
+        used_learned_guess(mlp, ci, qi, si, ni, cj, qj, sj, nj, o, it1, sv1);
         if (!o.fail && o.merit < 1e-10) {
             iters = it1;
             solves = sv1;
@@ -269,145 +279,217 @@ __device__ __forceinline__ void first_contact(const float *mlp, const double *ci
 }
 
 // ------------------------------------------------------------------
-// pair pass: one thread per half-list slot (PairGran::compute with the
-// superquadric surface model, src/pair_gran_base.h:255-430,
-// src/surface_model_superquadric.h:108-205, non-spherical Hertz/history)
-__global__ void k_sq_pair(SqDev D, const int *__restrict__ own, int nslots, int shearupdate)
+// pair pass (PairGran::compute with the superquadric surface model,
+// src/pair_gran_base.h:255-430, src/surface_model_superquadric.h:108-205,
+// non-spherical Hertz/history) in two kernels: k_sq_screen tests every
+// half-list slot (bounding spheres, oriented boxes) and gathers the slots
+// that need a contact-point solve in two lists, first contacts and warm
+// starts (a previous point exists); k_sq_solve runs the solves, each warp
+// taking the next 32 items, first contacts first.  A step holds few solves
+// (a few per cent of the slots), and its time is set by the longest solve
+// chains -- first contacts through the homotopy or the learned guess -- so
+// these start at once, on dense warps, and the short warm starts fill the
+// GPU around them.  Every slot's result is the one-pass result (the solves
+// are deterministic and independent).
+
+// lists of one pair pass: 0 first contacts, 1 warm starts
+struct SqWork {
+    int *list[2];
+    int *n;      // item counts, [2]
+    int *next;   // items taken (over both lists)
+};
+
+__device__ __forceinline__ void work_push(const SqWork &W, int l, int item, bool take)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&W.n[l], __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) W.list[l][base + __popc(m & ((1u << lane) - 1u))] = item;
+}
+
+// the slot's contact point, state and forces from a finished solve
+__device__ __forceinline__ void sq_finish(const SqDev &D, int sl, int i, int j, int shearupdate, const Newton &o)
+{
+    D.cp[sl] = dbl4{o.point[0], o.point[1], o.point[2], 0.0};
+    if (!(fmax(o.fi, o.fj) < 0.0)) {
+        D.state[sl] = CLOSE;
+        return;
+    }
+    const dbl4 xi4 = D.x[i], xj4 = D.x[j], qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
+    const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
+    const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
+    const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
+    double en[3] = {o.gB[0] - o.gA[0], o.gB[1] - o.gA[1], o.gB[2] - o.gA[2]};
+    const double nrm = sqrt(en[0] * en[0] + en[1] * en[1] + en[2] * en[2]);
+    const double inv = nrm == 0. ? 0. : 1. / nrm;
+    for (int k = 0; k < 3; k++) en[k] *= inv;
+    Body A, B;
+    body_set(A, ci, qi, si, si4.w);
+    body_set(B, cj, qj, sj, sj4.w);
+    double2 al = D.alpha[sl];
+    const double ne[3] = {-en[0], -en[1], -en[2]};
+    double cpa[3], cpb[3];
+    al.x = line_intersection(A, o.point, ne, al.x, cpa);
+    al.y = line_intersection(B, o.point, en, al.y, cpb);
+    D.alpha[sl] = al;
+    const double deltan = fabs(al.x) + fabs(al.y);
+    // forces: non-spherical kinematics, Hertz, tangential history
+    const dbl4 vi4 = D.v[i], vj4 = D.v[j], wi4 = D.w[i], wj4 = D.w[j], ii4 = D.inert[i], ij4 = D.inert[j];
+    const double wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
+    double xci[3], xcj[3], vri[3], vrj[3], vrel[3];
+    for (int k = 0; k < 3; k++) {
+        xci[k] = o.point[k] - ci[k];
+        xcj[k] = o.point[k] - cj[k];
+    }
+    cross3(wi, xci, vri);
+    cross3(wj, xcj, vrj);
+    const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
+    for (int k = 0; k < 3; k++) vrel[k] = vi[k] - vj[k] + (vri[k] - vrj[k]);
+    const double vn = dot3(vrel, en);
+    const double vtr[3] = {vrel[0] - vn * en[0], vrel[1] - vn * en[1], vrel[2] - vn * en[2]};
+    const double radi = ii4.w, radj = ij4.w, mi = vi4.w, mj = vj4.w, meff = mi * mj / (mi + mj);
+    const double reff = radi * radj / (radi + radj);
+    const double sqrtval = sqrt(reff * deltan);
+    const double Sn = 2. * D.Yeff * sqrtval, St = 8. * D.Geff * sqrtval;
+    const double kn = 4. / 3. * D.Yeff * sqrtval, kt = St;
+    const double c56 = 0.91287092917527685576161630466800355658790782499663875;
+    const double gamman = -2. * c56 * D.betaeff * sqrt(Sn * meff);
+    const double gammat = -2. * c56 * D.betaeff * sqrt(St * meff);
+    const double Fn = -gamman * vn + kn * deltan;
+    const double Fi[3] = {Fn * en[0], Fn * en[1], Fn * en[2]}, Fnj[3] = {-Fi[0], -Fi[1], -Fi[2]};
+    double Ti[3], Tj[3];
+    cross3(xci, Fi, Ti);
+    cross3(xcj, Fnj, Tj);
+    dbl4 sh4 = D.shear[sl];
+    double sh[3] = {sh4.x, sh4.y, sh4.z};
+    if (shearupdate) {
+        for (int k = 0; k < 3; k++) sh[k] += vtr[k] * D.dt;
+        const double rsht = dot3(sh, en);
+        for (int k = 0; k < 3; k++) sh[k] -= rsht * en[k];
+    }
+    const double shrmag = sqrt(dot3(sh, sh));
+    double Ft[3] = {-(kt * sh[0]), -(kt * sh[1]), -(kt * sh[2])};
+    const double Ft_shear = kt * shrmag, Ft_friction = D.mu * fabs(Fn);
+    if (Ft_shear > Ft_friction) {
+        if (shrmag != 0.0) {
+            const double ratio = Ft_friction / Ft_shear;
+            for (int k = 0; k < 3; k++) Ft[k] *= ratio;
+            if (shearupdate)
+                for (int k = 0; k < 3; k++) sh[k] = -Ft[k] / kt;
+        } else {
+            Ft[0] = Ft[1] = Ft[2] = 0.0;
+        }
+    } else {
+        for (int k = 0; k < 3; k++) Ft[k] -= gammat * vtr[k];
+    }
+    D.shear[sl] = dbl4{sh[0], sh[1], sh[2], 0.0};
+    double tti[3], ttj[3];
+    const double Ftj[3] = {-Ft[0], -Ft[1], -Ft[2]};
+    cross3(xci, Ft, tti);
+    cross3(xcj, Ftj, ttj);
+    D.pfi[sl] = dbl4{Fi[0] + Ft[0], Fi[1] + Ft[1], Fi[2] + Ft[2], 1.0};
+    D.pti[sl] = dbl4{Ti[0] + tti[0], Ti[1] + tti[1], Ti[2] + tti[2], 0.0};
+    D.ptj[sl] = dbl4{Tj[0] + ttj[0], Tj[1] + ttj[1], Tj[2] + ttj[2], 0.0};
+    D.flag[sl] |= 5;
+    D.state[sl] = INTERSECT;
+}
+
+// every slot: no force unless a solve below finds a contact; the bounding
+// spheres and (for a pair not yet intersecting) the oriented boxes decide
+// whether the slot needs a solve and which kind
+__global__ void k_sq_screen(SqDev D, const int *__restrict__ own, int nslots, SqWork W)
 {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sl >= nslots) return;
-    const int i = own[sl], j = D.nbr[sl];
-    const dbl4 xi4 = D.x[i], xj4 = D.x[j];
-    dbl4 fo{0, 0, 0, 0}, ti{0, 0, 0, 0}, tj{0, 0, 0, 0};
-    const double dx = xi4.x - xj4.x, dy = xi4.y - xj4.y, dz = xi4.z - xj4.z;
-    const double rsq = dx * dx + dy * dy + dz * dz, radsum = xi4.w + xj4.w;
-    if (rsq < radsum * radsum) {
-        const dbl4 qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
-        const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
-        const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
-        const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
-        int state = D.state[sl];
-        double Ri[9], Rj[9];
-        quat_to_mat(qi, Ri);
-        quat_to_mat(qj, Rj);
-        const bool obb = state == INTERSECT ? true : obb_intersect(ci, Ri, si, cj, Rj, sj);
-        bool contact = false;
-        if (obb) {
-            Newton o;
-            int it = 0, sv = 0, used = 0;
-            if (state == FAR) {
-                first_contact(D.mlp, ci, qi, si, si4.w, cj, qj, sj, sj4.w, o, it, sv, used);
-            } else {
-                // previous point advanced with the mass-weighted contact-point velocity
-                const dbl4 cp4 = D.cp[sl], wi4 = D.w[i], wj4 = D.w[j], vi4 = D.v[i], vj4 = D.v[j];
-                const double cp[3] = {cp4.x, cp4.y, cp4.z}, wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
-                double xci[3], xcj[3], vri[3], vrj[3], est[3];
-                for (int k = 0; k < 3; k++) {
-                    xci[k] = cp[k] - ci[k];
-                    xcj[k] = cp[k] - cj[k];
-                }
-                cross3(wi, xci, vri);
-                cross3(wj, xcj, vrj);
-                const double mi = vi4.w, mj = vj4.w;
-                const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
-                for (int k = 0; k < 3; k++) {
-                    const double a = vi[k] + vri[k], b = vj[k] + vrj[k];
-                    est[k] = cp[k] + (a * mi + b * mj) / (mi + mj) * D.dt;
-                }
-                contact_point(ci, qi, si, si4.w, cj, qj, sj, sj4.w, 1, est, false, 0.0, o, it, sv);
+    int kind = -1;
+    if (sl < nslots) {
+        const int i = own[sl], j = D.nbr[sl];
+        const dbl4 xi4 = D.x[i], xj4 = D.x[j];
+        D.pfi[sl] = dbl4{0, 0, 0, 0};
+        D.pti[sl] = dbl4{0, 0, 0, 0};
+        D.ptj[sl] = dbl4{0, 0, 0, 0};
+        const double dx = xi4.x - xj4.x, dy = xi4.y - xj4.y, dz = xi4.z - xj4.z;
+        const double rsq = dx * dx + dy * dy + dz * dz, radsum = xi4.w + xj4.w;
+        if (rsq < radsum * radsum) {
+            const int state = D.state[sl];
+            bool obb = true;
+            if (state != INTERSECT) {
+                const dbl4 qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
+                const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
+                const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
+                const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
+                double Ri[9], Rj[9];
+                quat_to_mat(qi, Ri);
+                quat_to_mat(qj, Rj);
+                obb = obb_intersect(ci, Ri, si, cj, Rj, sj);
             }
-            atomicAdd(&D.cnt[0], (unsigned long long)it);
-            atomicAdd(&D.cnt[1], (unsigned long long)sv);
-            atomicAdd(&D.cnt[2], 1ull);
-            if (used == 1) atomicAdd(&D.cnt[3], 1ull);
-            if (used == -1) atomicAdd(&D.cnt[4], 1ull);
-            D.cp[sl] = dbl4{o.point[0], o.point[1], o.point[2], 0.0};
-            contact = fmax(o.fi, o.fj) < 0.0;
-            if (contact) {
-                double en[3] = {o.gB[0] - o.gA[0], o.gB[1] - o.gA[1], o.gB[2] - o.gA[2]};
-                const double nrm = sqrt(en[0] * en[0] + en[1] * en[1] + en[2] * en[2]);
-                const double inv = nrm == 0. ? 0. : 1. / nrm;
-                for (int k = 0; k < 3; k++) en[k] *= inv;
-                Body A, B;
-                body_set(A, ci, qi, si, si4.w);
-                body_set(B, cj, qj, sj, sj4.w);
-                double2 al = D.alpha[sl];
-                const double ne[3] = {-en[0], -en[1], -en[2]};
-                double cpa[3], cpb[3];
-                al.x = line_intersection(A, o.point, ne, al.x, cpa);
-                al.y = line_intersection(B, o.point, en, al.y, cpb);
-                D.alpha[sl] = al;
-                const double deltan = fabs(al.x) + fabs(al.y);
-                state = INTERSECT;
-                // forces: non-spherical kinematics, Hertz, tangential history
-                const dbl4 vi4 = D.v[i], vj4 = D.v[j], wi4 = D.w[i], wj4 = D.w[j], ii4 = D.inert[i], ij4 = D.inert[j];
-                const double wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
-                double xci[3], xcj[3], vri[3], vrj[3], vrel[3];
-                for (int k = 0; k < 3; k++) {
-                    xci[k] = o.point[k] - ci[k];
-                    xcj[k] = o.point[k] - cj[k];
-                }
-                cross3(wi, xci, vri);
-                cross3(wj, xcj, vrj);
-                const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
-                for (int k = 0; k < 3; k++) vrel[k] = vi[k] - vj[k] + (vri[k] - vrj[k]);
-                const double vn = dot3(vrel, en);
-                const double vtr[3] = {vrel[0] - vn * en[0], vrel[1] - vn * en[1], vrel[2] - vn * en[2]};
-                const double radi = ii4.w, radj = ij4.w, mi = vi4.w, mj = vj4.w, meff = mi * mj / (mi + mj);
-                const double reff = radi * radj / (radi + radj);
-                const double sqrtval = sqrt(reff * deltan);
-                const double Sn = 2. * D.Yeff * sqrtval, St = 8. * D.Geff * sqrtval;
-                const double kn = 4. / 3. * D.Yeff * sqrtval, kt = St;
-                const double c56 = 0.91287092917527685576161630466800355658790782499663875;
-                const double gamman = -2. * c56 * D.betaeff * sqrt(Sn * meff);
-                const double gammat = -2. * c56 * D.betaeff * sqrt(St * meff);
-                const double Fn = -gamman * vn + kn * deltan;
-                const double Fi[3] = {Fn * en[0], Fn * en[1], Fn * en[2]}, Fnj[3] = {-Fi[0], -Fi[1], -Fi[2]};
-                double Ti[3], Tj[3];
-                cross3(xci, Fi, Ti);
-                cross3(xcj, Fnj, Tj);
-                dbl4 sh4 = D.shear[sl];
-                double sh[3] = {sh4.x, sh4.y, sh4.z};
-                if (shearupdate) {
-                    for (int k = 0; k < 3; k++) sh[k] += vtr[k] * D.dt;
-                    const double rsht = dot3(sh, en);
-                    for (int k = 0; k < 3; k++) sh[k] -= rsht * en[k];
-                }
-                const double shrmag = sqrt(dot3(sh, sh));
-                double Ft[3] = {-(kt * sh[0]), -(kt * sh[1]), -(kt * sh[2])};
-                const double Ft_shear = kt * shrmag, Ft_friction = D.mu * fabs(Fn);
-                if (Ft_shear > Ft_friction) {
-                    if (shrmag != 0.0) {
-                        const double ratio = Ft_friction / Ft_shear;
-                        for (int k = 0; k < 3; k++) Ft[k] *= ratio;
-                        if (shearupdate)
-                            for (int k = 0; k < 3; k++) sh[k] = -Ft[k] / kt;
-                    } else {
-                        Ft[0] = Ft[1] = Ft[2] = 0.0;
-                    }
-                } else {
-                    for (int k = 0; k < 3; k++) Ft[k] -= gammat * vtr[k];
-                }
-                D.shear[sl] = dbl4{sh[0], sh[1], sh[2], 0.0};
-                double tti[3], ttj[3];
-                const double Ftj[3] = {-Ft[0], -Ft[1], -Ft[2]};
-                cross3(xci, Ft, tti);
-                cross3(xcj, Ftj, ttj);
-                fo = dbl4{Fi[0] + Ft[0], Fi[1] + Ft[1], Fi[2] + Ft[2], 1.0};
-                ti = dbl4{Ti[0] + tti[0], Ti[1] + tti[1], Ti[2] + tti[2], 0.0};
-                tj = dbl4{Tj[0] + ttj[0], Tj[1] + ttj[1], Tj[2] + ttj[2], 0.0};
-                D.flag[sl] |= 5;
-            } else {
-                state = CLOSE;
-            }
-        } else {
-            state = FAR;
+            if (!obb) D.state[sl] = FAR;
+            else kind = state == FAR ? 0 : 1;
         }
-        D.state[sl] = state;
     }
-    D.pfi[sl] = fo;
-    D.pti[sl] = ti;
-    D.ptj[sl] = tj;
+    work_push(W, 0, sl, kind == 0);
+    work_push(W, 1, sl, kind == 1);
+}
+
+// the solve of one listed slot: a first contact (learned guess with the
+// homotopy as fallback, or the homotopy) or a warm start (the previous point
+// advanced with the mass-weighted contact-point velocity)
+__device__ __forceinline__ void sq_solve_item(const SqDev &D, int sl, bool first, const int *own, int shearupdate)
+{
+    const int i = own[sl], j = D.nbr[sl];
+    const dbl4 xi4 = D.x[i], xj4 = D.x[j], qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
+    const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
+    const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
+    const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
+    Newton o;
+    int it = 0, sv = 0, used = 0;
+    if (first) {
+        first_contact(D.mlp, ci, qi, si, si4.w, cj, qj, sj, sj4.w, o, it, sv, used);
+    } else {
+        const dbl4 cp4 = D.cp[sl], wi4 = D.w[i], wj4 = D.w[j], vi4 = D.v[i], vj4 = D.v[j];
+        const double cp[3] = {cp4.x, cp4.y, cp4.z}, wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
+        double xci[3], xcj[3], vri[3], vrj[3], est[3];
+        for (int k = 0; k < 3; k++) {
+            xci[k] = cp[k] - ci[k];
+            xcj[k] = cp[k] - cj[k];
+        }
+        cross3(wi, xci, vri);
+        cross3(wj, xcj, vrj);
+        const double mi = vi4.w, mj = vj4.w;
+        const double vi[3] = {vi4.x, vi4.y, vi4.z}, vj[3] = {vj4.x, vj4.y, vj4.z};
+        for (int k = 0; k < 3; k++) {
+            const double a = vi[k] + vri[k], b = vj[k] + vrj[k];
+            est[k] = cp[k] + (a * mi + b * mj) / (mi + mj) * D.dt;
+        }
+        contact_point(ci, qi, si, si4.w, cj, qj, sj, sj4.w, 1, est, false, 0.0, o, it, sv);
+    }
+    atomicAdd(&D.cnt[0], (unsigned long long)it);
+    atomicAdd(&D.cnt[1], (unsigned long long)sv);
+    atomicAdd(&D.cnt[2], 1ull);
+    if (used == 1) atomicAdd(&D.cnt[3], 1ull);
+    if (used == -1) atomicAdd(&D.cnt[4], 1ull);
+    sq_finish(D, sl, i, j, shearupdate, o);
+}
+
+// the listed solves; each warp takes the next 32 items (the lists are
+// complete when the kernel starts)
+__global__ void __launch_bounds__(128) k_sq_solve(SqDev D, SqWork W, const int *__restrict__ own, int shearupdate)
+{
+    const int lane = threadIdx.x & 31;
+    const int nfirst = W.n[0], total = nfirst + W.n[1];
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(W.next, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int q = base + lane;
+        if (q < total) {
+            const bool first = q < nfirst;
+            sq_solve_item(D, first ? W.list[0][q] : W.list[1][q - nfirst], first, own, shearupdate);
+        }
+    }
 }
 
 // per-atom sums in the reference's order: slots where the atom is the j
