@@ -7,13 +7,14 @@
 // gb2_sq_kernels.cuh (normalisation statistics first).  Training keeps an
 // FP32 master copy of the weights; every forward pass uses them rounded to
 // BF16, activations are rounded to BF16 between layers, products accumulate
-// in FP32 -- the same rounding points as mlp_infer() in the contact kernel.
+// in FP32 -- the contact pass infers with these same layers (mlp_infer_warp).
 // Loss: mean squared error of the normalised outputs (point in particle i's
 // frame / (ri + rj), mu).
 #pragma once
 
 #include <cuda_bf16.h>
 
+#include "gb2_mma.cuh"
 #include "gb2_sq_kernels.cuh"
 
 namespace gb2 {
@@ -120,17 +121,23 @@ __global__ void k_mlp_make(unsigned long long seed, long n, float *out)
 // Learned guess against the plain method on fresh samples: per sample the
 // plain cost, the learned cost (guess solve + fallback), whether the learned
 // guess was accepted, and the distance between the two converged points.
-__global__ void k_mlp_eval(unsigned long long seed, long n, const float *__restrict__ P, long long *stats,
-                           double *maxdiff_bits)
+__global__ void __launch_bounds__(128) k_mlp_eval(unsigned long long seed, long n, const float *__restrict__ P,
+                                                  long long *stats, double *maxdiff_bits)
 {
+    __shared__ __align__(16) MlpInfer M;
+    mlp_stage(M, P);
+    __syncthreads();
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
     PairSample S;
-    if (!sample_pair(seed, k, S)) return;
+    const bool valid = k < n && sample_pair(seed, k, S);
+    float feat[kMlpIn], out[kMlpOut];
+    if (valid) pair_features_of(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, feat);
+    mlp_infer_warp(M, valid, feat, out);
+    if (!valid) return;
     Newton plain, learned;
     int it0, sv0, it1, sv1, used;
     contact_point(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, 0, nullptr, false, 0.0, plain, it0, sv0);
-    first_contact(P, S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, learned, it1, sv1, used);
+    first_contact(out, S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, learned, it1, sv1, used);
     atomicAdd((unsigned long long *)&stats[0], 1ull);
     atomicAdd((unsigned long long *)&stats[1], (unsigned long long)it0);
     atomicAdd((unsigned long long *)&stats[2], (unsigned long long)sv0);
@@ -152,10 +159,13 @@ __global__ void k_mlp_eval(unsigned long long seed, long n, const float *__restr
 }
 
 // Timed comparison of the two first-contact solves on the same stored pairs:
-// k_mlp_store_pairs keeps the valid samples, k_mlp_solve runs one method per
-// pair (the plain homotopy from spheres, or the learned guess with the
-// homotopy as fallback) and keeps its point and iteration count, so each
-// launch can be timed alone with CUDA events.
+// k_mlp_store_pairs keeps the valid samples; the plain method is one launch
+// of the homotopy from spheres (one thread per pair); the learned method is a
+// launch of the learned attempts (guesses on the tensor cores, one warp per
+// 32 pairs) that gathers the rejected pairs in a list, then the homotopy over
+// that list (k_mlp_solve_rejected), so the few pairs the guess does not
+// settle no longer hold warps of settled ones.  Points and iteration counts
+// are those of one call of first_contact() per pair.
 __global__ void k_mlp_store_pairs(unsigned long long seed, long n, PairSample *out, int *nvalid)
 {
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -166,18 +176,62 @@ __global__ void k_mlp_store_pairs(unsigned long long seed, long n, PairSample *o
 }
 
 template <bool LEARNED>
-__global__ void k_mlp_solve(const PairSample *pairs, const int *nvalid, const float *__restrict__ P, double *point,
-                            long long *iters)
+__global__ void __launch_bounds__(128) k_mlp_solve(const PairSample *pairs, const int *nvalid,
+                                                   const float *__restrict__ P, double *point, long long *iters,
+                                                   int *rejected, int *nrejected)
 {
+    __shared__ __align__(16) MlpInfer M;
+    if constexpr (LEARNED) {
+        mlp_stage(M, P);
+        __syncthreads();
+    }
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= *nvalid) return;
+    const bool valid = k < *nvalid;
+    bool reject = false;
+    PairSample S;
+    if (valid) S = pairs[k];
+    float out[kMlpOut];
+    if constexpr (LEARNED) {
+        float feat[kMlpIn];
+        if (valid) pair_features_of(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, feat);
+        mlp_infer_warp(M, valid, feat, out);
+    }
+    if (valid) {
+        Newton o;
+        int it, sv;
+        if constexpr (LEARNED) {
+            used_learned_guess(out, S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, o, it, sv);
+            reject = o.fail || !(o.merit < 1e-10);
+        } else {
+            contact_point(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, 0, nullptr, false, 0.0, o, it, sv);
+        }
+        if (!reject)
+            for (int c = 0; c < 3; c++) point[3 * k + c] = o.point[c];
+        atomicAdd((unsigned long long *)iters, (unsigned long long)it);
+    }
+    if constexpr (LEARNED) {   // warp-aggregated append of the rejected pairs
+        const unsigned m = __ballot_sync(0xffffffffu, reject);
+        if (m) {
+            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(nrejected, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (reject) rejected[base + __popc(m & ((1u << lane) - 1u))] = k;
+        }
+    }
+}
+
+// the homotopy for the pairs whose learned guess was rejected
+__global__ void k_mlp_solve_rejected(const PairSample *pairs, const int *rejected, const int *nrejected, double *point,
+                                     long long *iters)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= *nrejected) return;
+    const int k = rejected[q];
     const PairSample S = pairs[k];
     Newton o;
-    int it, sv, used;
-    if constexpr (LEARNED)
-        first_contact(P, S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, o, it, sv, used);
-    else
-        contact_point(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, 0, nullptr, false, 0.0, o, it, sv);
+    int it, sv;
+    contact_point(S.ci, S.qi, S.si, S.ni, S.cj, S.qj, S.sj, S.nj, 0, nullptr, false, 0.0, o, it, sv);
     for (int c = 0; c < 3; c++) point[3 * k + c] = o.point[c];
     atomicAdd((unsigned long long *)iters, (unsigned long long)it);
 }
@@ -201,74 +255,6 @@ struct MlpSmem {
     __nv_bfloat16 E[kWarps][kTile][kMlpH];   // delta of the layer below
     __nv_bfloat16 DY[kWarps][kTile][16];     // output delta, columns 4..15 zero
 };
-
-__device__ __forceinline__ unsigned pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi)
-{
-    return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
-}
-
-// D(16x8, f32) += A(16x16, bf16, row) * B(16x8, bf16, col)
-__device__ __forceinline__ void mma16816(float *d, const unsigned *a, const unsigned *b)
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// A fragment of a 16x16 tile at (row0, col0) of a row-major bf16 matrix with
-// leading dimension ld, optionally transposed (element (r, c) read at [c][r])
-template <bool TRANS>
-__device__ __forceinline__ void load_a(const __nv_bfloat16 *M, int ld, int row0, int col0, unsigned *a)
-{
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    auto at = [&](int r, int c) { return TRANS ? M[(col0 + c) * ld + row0 + r] : M[(row0 + r) * ld + col0 + c]; };
-    a[0] = pack_bf16(at(g, 2 * t), at(g, 2 * t + 1));
-    a[1] = pack_bf16(at(g + 8, 2 * t), at(g + 8, 2 * t + 1));
-    a[2] = pack_bf16(at(g, 2 * t + 8), at(g, 2 * t + 9));
-    a[3] = pack_bf16(at(g + 8, 2 * t + 8), at(g + 8, 2 * t + 9));
-}
-// B fragment of a 16x8 tile (k0, n0) where element (k, n) is read at
-// M[n][k] (NK: weights [out][in] used as B = W^T) or M[k][n] (KN)
-template <bool NK>
-__device__ __forceinline__ void load_b(const __nv_bfloat16 *M, int ld, int k0, int n0, unsigned *b)
-{
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    auto at = [&](int k, int n) { return NK ? M[(n0 + n) * ld + k0 + k] : M[(k0 + k) * ld + n0 + n]; };
-    b[0] = pack_bf16(at(2 * t, g), at(2 * t + 1, g));
-    b[1] = pack_bf16(at(2 * t + 8, g), at(2 * t + 9, g));
-}
-
-// Y(16 x N) = X(16 x K) W^T with W [N][K] in shared memory; epilogue
-// bias + ReLU, result rounded to bf16 into H (row-major 16 x N)
-template <int K, int N>
-__device__ __forceinline__ void layer_fwd(const __nv_bfloat16 *X, const __nv_bfloat16 *W, const float *b,
-                                          __nv_bfloat16 *H, bool relu)
-{
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    for (int n0 = 0; n0 < N; n0 += 8) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int k0 = 0; k0 < K; k0 += 16) {
-            unsigned a[4], bb[2];
-            load_a<false>(X, K, 0, k0, a);
-            load_b<true>(W, K, k0, n0, bb);
-            mma16816(acc, a, bb);
-        }
-        const int c = n0 + 2 * t;
-        float v0 = acc[0] + b[c], v1 = acc[1] + b[c + 1], v2 = acc[2] + b[c], v3 = acc[3] + b[c + 1];
-        if (relu) {
-            v0 = fmaxf(v0, 0.f);
-            v1 = fmaxf(v1, 0.f);
-            v2 = fmaxf(v2, 0.f);
-            v3 = fmaxf(v3, 0.f);
-        }
-        H[g * N + c] = __float2bfloat16_rn(v0);
-        H[g * N + c + 1] = __float2bfloat16_rn(v1);
-        H[(g + 8) * N + c] = __float2bfloat16_rn(v2);
-        H[(g + 8) * N + c + 1] = __float2bfloat16_rn(v3);
-    }
-}
 
 // E(16 x K) = D(16 x N) W (W [N][K]); masked by the ReLU of Hin (> 0)
 template <int N, int K>

@@ -42,12 +42,17 @@ struct Buf {
         p = nullptr;
         n = 0;
     }
+    // grows with 50% headroom: the neighbour lists are rebuilt every few
+    // steps with slightly different sizes and swap roles with the previous
+    // list, and a cudaFree/cudaMalloc pair at each of those would stall the
+    // device for longer than the rebuild's kernels take
     cudaError_t alloc(size_t m)
     {
         if (m <= n && p) return cudaSuccess;
         release();
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
-        if (e == cudaSuccess) n = m;
+        const size_t want = std::max<size_t>(m + m / 2, 1);
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) n = want;
         return e;
     }
     void swap(Buf &o)
@@ -990,37 +995,40 @@ int gb2_mlp_time_solves(gb2_mlp_ctx *c, long n, unsigned long long seed, double 
     if (!c || n <= 0 || n > (1L << 24) || !ms_plain || !ms_learned || !counts) return GB2_ERR_ARG;
     Buf<PairSample> pairs;
     Buf<double> pt;
-    Buf<int> nv;
+    Buf<int> nv, rej;
     Buf<long long> it;
     MLCK(pairs.alloc(n));
     MLCK(pt.alloc(3 * n));
-    MLCK(nv.alloc(1));
+    MLCK(nv.alloc(2));
+    MLCK(rej.alloc(n));
     MLCK(it.alloc(2));
-    MLCK(cudaMemsetAsync(nv.p, 0, sizeof(int), c->st));
+    MLCK(cudaMemsetAsync(nv.p, 0, 2 * sizeof(int), c->st));
     MLCK(cudaMemsetAsync(it.p, 0, 2 * sizeof(long long), c->st));
     k_mlp_store_pairs<<<nb(n), kB, 0, c->st>>>(seed, n, pairs.p, nv.p);
     MLCK(cudaGetLastError());
     cudaEvent_t e[3];
     for (auto &x : e) MLCK(cudaEventCreate(&x));
-    // one untimed pass of each (code and data warm), then the timed ones
-    k_mlp_solve<false><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p);
-    k_mlp_solve<true><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p + 1);
-    MLCK(cudaMemsetAsync(it.p, 0, 2 * sizeof(long long), c->st));
-    MLCK(cudaEventRecord(e[0], c->st));
-    k_mlp_solve<false><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p);
-    MLCK(cudaEventRecord(e[1], c->st));
-    k_mlp_solve<true><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p + 1);
-    MLCK(cudaEventRecord(e[2], c->st));
+    // one untimed round of each method (code and data warm), then the timed one
+    for (int round = 0; round < 2; round++) {
+        MLCK(cudaMemsetAsync(it.p, 0, 2 * sizeof(long long), c->st));
+        MLCK(cudaEventRecord(e[0], c->st));
+        k_mlp_solve<false><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p, nullptr, nullptr);
+        MLCK(cudaEventRecord(e[1], c->st));
+        MLCK(cudaMemsetAsync(nv.p + 1, 0, sizeof(int), c->st));
+        k_mlp_solve<true><<<nb(n), kB, 0, c->st>>>(pairs.p, nv.p, c->P.p, pt.p, it.p + 1, rej.p, nv.p + 1);
+        k_mlp_solve_rejected<<<nb(n), kB, 0, c->st>>>(pairs.p, rej.p, nv.p + 1, pt.p, it.p + 1);
+        MLCK(cudaEventRecord(e[2], c->st));
+    }
     MLCK(cudaGetLastError());
-    int hv = 0;
-    MLCK(cudaMemcpyAsync(&hv, nv.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    int hv[2] = {0, 0};
+    MLCK(cudaMemcpyAsync(hv, nv.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
     MLCK(cudaMemcpyAsync(counts + 1, it.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, c->st));
     MLCK(cudaStreamSynchronize(c->st));
     float a = 0.f, b = 0.f;
     MLCK(cudaEventElapsedTime(&a, e[0], e[1]));
     MLCK(cudaEventElapsedTime(&b, e[1], e[2]));
     for (auto &x : e) cudaEventDestroy(x);
-    counts[0] = hv;
+    counts[0] = hv[0];
     *ms_plain = a;
     *ms_learned = b;
     return 0;

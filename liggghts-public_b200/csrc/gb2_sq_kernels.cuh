@@ -14,6 +14,7 @@
 
 #include "gb2_sq.cuh"
 #include "gb2_internal.h"
+#include "gb2_mma.cuh"
 
 namespace gb2 {
 namespace sq {
@@ -196,32 +197,81 @@ __device__ __forceinline__ double pair_features(const double *ci, const double *
     return s;
 }
 
-// forward pass of one sample (the same BF16 rounding points as the training
-// kernels): out = de-normalised (point in i's frame / s, mu)
-__device__ __forceinline__ void mlp_infer(const float *__restrict__ P, const float *feat, float *out)
+// Inference on the tensor cores.  The parameters are staged once per block
+// (weights rounded to BF16 and zero-padded exactly as the training kernel
+// does), and each warp runs the forward pass of its 32 lanes' pairs as two
+// 16-row tiles through the training kernel's own layers (mma.sync m16n8k16,
+// FP32 accumulation, bias + ReLU, BF16 activations), so a guess is computed
+// with the arithmetic the network was trained with.
+struct MlpInfer {
+    __nv_bfloat16 W1[kMlpH][16], W2[kMlpH][kMlpH], W3[kMlpH][kMlpH], W4[8][kMlpH];
+    float b1[kMlpH], b2[kMlpH], b3[kMlpH], b4[8];
+    float stat[2 * kMlpIn + 2 * kMlpOut];   // in_mean, in_std, out_mean, out_std
+    __nv_bfloat16 X[4][32][16];             // per warp: normalised features
+    __nv_bfloat16 H[4][2][16][kMlpH];       // per warp: activations of one tile
+    float Y[4][32][kMlpOut];                // per warp: outputs
+};
+
+// all threads of the block; the caller synchronises the block afterwards
+__device__ __forceinline__ void mlp_stage(MlpInfer &S, const float *__restrict__ P)
 {
-    float x[kMlpH], h[kMlpH];
-    for (int c = 0; c < kMlpIn; c++) x[c] = bf16_round((feat[c] - __ldg(&P[c])) / __ldg(&P[kMlpIn + c]));
-    for (int o = 0; o < kMlpH; o++) {
-        float acc = 0.f;
-        for (int c = 0; c < kMlpIn; c++) acc += __ldg(&P[kMlpOffW1 + o * kMlpIn + c]) * x[c];
-        h[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB1 + o]), 0.f));
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < kMlpH * 16; e += nt) {
+        const int o = e / 16, c = e % 16;
+        S.W1[o][c] = __float2bfloat16_rn(c < kMlpIn ? P[kMlpOffW1 + o * kMlpIn + c] : 0.f);
     }
-    for (int o = 0; o < kMlpH; o++) {
-        float acc = 0.f;
-        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW2 + o * kMlpH + c]) * h[c];
-        x[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB2 + o]), 0.f));
+    for (int e = tid; e < kMlpH * kMlpH; e += nt) {
+        S.W2[e / kMlpH][e % kMlpH] = __float2bfloat16_rn(P[kMlpOffW2 + e]);
+        S.W3[e / kMlpH][e % kMlpH] = __float2bfloat16_rn(P[kMlpOffW3 + e]);
     }
-    for (int o = 0; o < kMlpH; o++) {
-        float acc = 0.f;
-        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW3 + o * kMlpH + c]) * x[c];
-        h[o] = bf16_round(fmaxf(acc + __ldg(&P[kMlpOffB3 + o]), 0.f));
+    for (int e = tid; e < 8 * kMlpH; e += nt) {
+        const int o = e / kMlpH;
+        S.W4[o][e % kMlpH] = __float2bfloat16_rn(o < kMlpOut ? P[kMlpOffW4 + e] : 0.f);
     }
-    for (int o = 0; o < kMlpOut; o++) {
-        float acc = 0.f;
-        for (int c = 0; c < kMlpH; c++) acc += __ldg(&P[kMlpOffW4 + o * kMlpH + c]) * h[c];
-        out[o] = (acc + __ldg(&P[kMlpOffB4 + o])) * __ldg(&P[2 * kMlpIn + kMlpOut + o]) + __ldg(&P[2 * kMlpIn + o]);
+    for (int e = tid; e < kMlpH; e += nt) {
+        S.b1[e] = P[kMlpOffB1 + e];
+        S.b2[e] = P[kMlpOffB2 + e];
+        S.b3[e] = P[kMlpOffB3 + e];
     }
+    if (tid < 8) S.b4[tid] = tid < kMlpOut ? P[kMlpOffB4 + tid] : 0.f;
+    for (int e = tid; e < 2 * kMlpIn + 2 * kMlpOut; e += nt) S.stat[e] = P[e];
+}
+
+// The forward pass of the warp's 32 lanes (called by the whole warp of a
+// 128-thread block; lanes with active false contribute zero rows): out =
+// de-normalised (point in i's frame / s, mu) of the lane's pair.
+__device__ __forceinline__ void mlp_infer_warp(MlpInfer &S, bool active, const float *feat, float *out)
+{
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 3;
+    for (int c = 0; c < 16; c++) {
+        const float v = (active && c < kMlpIn) ? (feat[c] - S.stat[c]) / S.stat[kMlpIn + c] : 0.f;
+        S.X[w][lane][c] = __float2bfloat16_rn(v);
+    }
+    __syncwarp();
+    const int g = lane >> 2, t = lane & 3;
+    for (int tile = 0; tile < 2; tile++) {
+        layer_fwd<16, kMlpH>(&S.X[w][16 * tile][0], &S.W1[0][0], S.b1, &S.H[w][0][0][0], true);
+        __syncwarp();
+        layer_fwd<kMlpH, kMlpH>(&S.H[w][0][0][0], &S.W2[0][0], S.b2, &S.H[w][1][0][0], true);
+        __syncwarp();
+        layer_fwd<kMlpH, kMlpH>(&S.H[w][1][0][0], &S.W3[0][0], S.b3, &S.H[w][0][0][0], true);
+        __syncwarp();
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int k0 = 0; k0 < kMlpH; k0 += 16) {
+            unsigned a[4], bb[2];
+            load_a<false>(&S.H[w][0][0][0], kMlpH, 0, k0, a);
+            load_b<true>(&S.W4[0][0], kMlpH, k0, 0, bb);
+            mma16816(acc, a, bb);
+        }
+        for (int q = 0; q < 4; q++) {
+            const int r = g + (q >> 1) * 8, c = 2 * t + (q & 1);
+            if (c < kMlpOut) S.Y[w][16 * tile + r][c] = acc[q] + S.b4[c];
+        }
+        __syncwarp();
+    }
+    for (int c = 0; c < kMlpOut; c++)
+        out[c] = S.Y[w][lane][c] * S.stat[2 * kMlpIn + kMlpOut + c] + S.stat[2 * kMlpIn + c];
+    __syncwarp();
 }
 
 // Newton iterations granted to the solve from the learned guess.  A start
@@ -230,19 +280,17 @@ __device__ __forceinline__ void mlp_infer(const float *__restrict__ P, const flo
 // defeat both methods no longer pay the full iteration bound twice.
 constexpr int kLearnedNewton = 48;
 
-// Contact point of a pair without a previous point from the learned guess:
-// the network's point and mu, then one Newton solve of at most
+// Contact point of a pair without a previous point from the network's
+// output `out` (point in i's frame / s, mu): one Newton solve of at most
 // kLearnedNewton iterations.  The caller accepts it when it converged to
 // merit < 1e-10 and otherwise runs the homotopy.
-__device__ __forceinline__ void used_learned_guess(const float *mlp, const double *ci, const double *qi,
+__device__ __forceinline__ void used_learned_guess(const float *out, const double *ci, const double *qi,
                                                    const double *si, double ni, const double *cj, const double *qj,
                                                    const double *sj, double nj, Newton &o, int &iters, int &solves)
 {
     double Ri[9];
     quat_to_mat(qi, Ri);
-    float feat[kMlpIn], out[kMlpOut];
-    const double s = pair_features(ci, qi, si, ni, cj, qj, sj, nj, Ri, feat);
-    mlp_infer(mlp, feat, out);
+    const double s = cbrt(si[0] * si[1] * si[2]) + cbrt(sj[0] * sj[1] * sj[2]);
     const double pl[3] = {out[0] * s, out[1] * s, out[2] * s};
     double g[3];
     matvec(Ri, pl, g);
@@ -251,17 +299,27 @@ __device__ __forceinline__ void used_learned_guess(const float *mlp, const doubl
                                   solves);
 }
 
+// The network's features of a pair (i's body frame)
+__device__ __forceinline__ void pair_features_of(const double *ci, const double *qi, const double *si, double ni,
+                                                 const double *cj, const double *qj, const double *sj, double nj,
+                                                 float *feat)
+{
+    double Ri[9];
+    quat_to_mat(qi, Ri);
+    pair_features(ci, qi, si, ni, cj, qj, sj, nj, Ri, feat);
+}
+
 // Contact point of a pair without a previous point in one call: the learned
-// guess when a network is given, the homotopy when it is rejected or absent.
-// used: 1 learned guess accepted, -1 rejected, 0 off.
-__device__ __forceinline__ void first_contact(const float *mlp, const double *ci, const double *qi, const double *si,
+// guess when the network's output is given, the homotopy when it is
+// rejected or absent.  used: 1 learned guess accepted, -1 rejected, 0 off.
+__device__ __forceinline__ void first_contact(const float *out, const double *ci, const double *qi, const double *si,
                                               double ni, const double *cj, const double *qj, const double *sj,
                                               double nj, Newton &o, int &iters, int &solves, int &used)
 {
     used = 0;
-    if (mlp) {
+    if (out) {
         int it1, sv1;
-        used_learned_guess(mlp, ci, qi, si, ni, cj, qj, sj, nj, o, it1, sv1);
+        used_learned_guess(out, ci, qi, si, ni, cj, qj, sj, nj, o, it1, sv1);
         if (!o.fail && o.merit < 1e-10) {
             iters = it1;
             solves = sv1;
@@ -436,7 +494,8 @@ __global__ void k_sq_screen(SqDev D, const int *__restrict__ own, int nslots, Sq
 // the solve of one listed slot: a first contact (learned guess with the
 // homotopy as fallback, or the homotopy) or a warm start (the previous point
 // advanced with the mass-weighted contact-point velocity)
-__device__ __forceinline__ void sq_solve_item(const SqDev &D, int sl, bool first, const int *own, int shearupdate)
+__device__ __forceinline__ void sq_solve_item(const SqDev &D, int sl, bool first, const int *own, int shearupdate,
+                                              const float *guess)
 {
     const int i = own[sl], j = D.nbr[sl];
     const dbl4 xi4 = D.x[i], xj4 = D.x[j], qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i], sj4 = D.shape[j];
@@ -446,7 +505,7 @@ __device__ __forceinline__ void sq_solve_item(const SqDev &D, int sl, bool first
     Newton o;
     int it = 0, sv = 0, used = 0;
     if (first) {
-        first_contact(D.mlp, ci, qi, si, si4.w, cj, qj, sj, sj4.w, o, it, sv, used);
+        first_contact(guess, ci, qi, si, si4.w, cj, qj, sj, sj4.w, o, it, sv, used);
     } else {
         const dbl4 cp4 = D.cp[sl], wi4 = D.w[i], wj4 = D.w[j], vi4 = D.v[i], vj4 = D.v[j];
         const double cp[3] = {cp4.x, cp4.y, cp4.z}, wi[3] = {wi4.x, wi4.y, wi4.z}, wj[3] = {wj4.x, wj4.y, wj4.z};
@@ -474,9 +533,15 @@ __device__ __forceinline__ void sq_solve_item(const SqDev &D, int sl, bool first
 }
 
 // the listed solves; each warp takes the next 32 items (the lists are
-// complete when the kernel starts)
+// complete when the kernel starts).  With a network, a warp holding first
+// contacts computes their learned guesses together on the tensor cores.
 __global__ void __launch_bounds__(128) k_sq_solve(SqDev D, SqWork W, const int *__restrict__ own, int shearupdate)
 {
+    __shared__ __align__(16) MlpInfer S;
+    if (D.mlp) {
+        mlp_stage(S, D.mlp);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const int nfirst = W.n[0], total = nfirst + W.n[1];
     for (;;) {
@@ -485,10 +550,24 @@ __global__ void __launch_bounds__(128) k_sq_solve(SqDev D, SqWork W, const int *
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= total) break;
         const int q = base + lane;
-        if (q < total) {
-            const bool first = q < nfirst;
-            sq_solve_item(D, first ? W.list[0][q] : W.list[1][q - nfirst], first, own, shearupdate);
+        const bool has = q < total, first = has && q < nfirst;
+        const int sl = has ? (first ? W.list[0][q] : W.list[1][q - nfirst]) : 0;
+        float out[kMlpOut] = {0.f, 0.f, 0.f, 0.f};
+        const bool learned = D.mlp != nullptr && __any_sync(0xffffffffu, first);
+        if (learned) {
+            float feat[kMlpIn];
+            if (first) {
+                const int i = own[sl], j = D.nbr[sl];
+                const dbl4 xi4 = D.x[i], xj4 = D.x[j], qi4 = D.q[i], qj4 = D.q[j], si4 = D.shape[i],
+                           sj4 = D.shape[j];
+                const double ci[3] = {xi4.x, xi4.y, xi4.z}, cj[3] = {xj4.x, xj4.y, xj4.z};
+                const double qi[4] = {qi4.x, qi4.y, qi4.z, qi4.w}, qj[4] = {qj4.x, qj4.y, qj4.z, qj4.w};
+                const double si[3] = {si4.x, si4.y, si4.z}, sj[3] = {sj4.x, sj4.y, sj4.z};
+                pair_features_of(ci, qi, si, si4.w, cj, qj, sj, sj4.w, feat);
+            }
+            mlp_infer_warp(S, first, feat, out);
         }
+        if (has) sq_solve_item(D, sl, first, own, shearupdate, learned ? out : nullptr);
     }
 }
 

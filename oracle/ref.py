@@ -351,14 +351,16 @@ def run(sc, segments, keep=None, harness=None, extra_args=(), script_lines=None)
         lines = script(sc, wd, segments, names) if script_lines is None else script_lines(wd)
         with open(os.path.join(wd, "in.case"), "w") as f:
             f.write("\n".join(lines) + "\n")
+        # the reference's messages may hold stray non-UTF-8 bytes (an error
+        # line printing an unterminated keyword buffer): decode leniently
         r = subprocess.run([harness, os.path.join(wd, "in.case"), wd] + list(extra_args), capture_output=True,
-                           text=True)
+                           text=True, errors="replace")
         if r.returncode != 0 or not os.path.exists(os.path.join(wd, names[-1] + ".bin")):
             tail = ""
             for fn in ("screen.txt", "log.lammps"):
                 p = os.path.join(wd, fn)
                 if os.path.exists(p):
-                    with open(p) as f:
+                    with open(p, errors="replace") as f:
                         tail += f.read()[-3000:]
             raise RuntimeError("reference run failed (rc %d): %s %s" % (r.returncode, r.stderr[-2000:], tail))
         return [read_dump(os.path.join(wd, n + ".bin")) for n in names]

@@ -105,10 +105,10 @@ def test_learned_guess_in_simulation(trained):
 
 def test_learned_guess_solve_time(trained):
     """The first-contact solve itself on the same fresh pairs both ways: the
-    learned guess needs about half the Newton iterations.  The kernel times
-    are reported, not asserted: each launch lasts as long as its slowest
-    pairs, those the plain solver also fails on after the iteration cap, and
-    for them the learned attempt comes on top of the homotopy."""
+    learned guess needs about half the Newton iterations.  The times are
+    reported, not asserted (the learned method is its attempts, then the
+    homotopy over the pairs it rejected; both launches depend on their
+    slowest pairs, which the plain solver may also fail on)."""
     t, info, l0, l1 = trained
     ts = t.time_solves(100_000, seed=7)
     print(ts)
