@@ -386,12 +386,15 @@ def pinned_empty(shape, dtype=np.float64):
     return arr
 
 
-def restart_scenario(sc, atoms, mesh_nodes=None):
+def restart_scenario(sc, atoms, mesh_nodes=None, ntimestep=None):
     """The scenario with its atoms replaced by a run's current state (same
     tags, the run's atom order), as read_restart would bring them back;
     `mesh_nodes` maps a scenario fix index to that mesh's current nodes
-    (ntri, 3, 3), for meshes that have moved."""
+    (ntri, 3, 3), for meshes that have moved; `ntimestep` is the step the
+    restarted run starts from (the restart file's timestep)."""
     out = dict(sc)
+    if ntimestep is not None:
+        out["ntimestep"] = int(ntimestep)
     a = dict(sc["atoms"])
     tags = np.asarray(a["tag"])
     order = np.argsort(tags, kind="stable")
@@ -496,6 +499,8 @@ class Engine:
                 self._check(k)
             self.fix_ids.append(k)
         self.n = n
+        if int(sc.get("ntimestep", 0)):   # a restarted run keeps its step count (atom-sort schedule)
+            self._check(L.gb2_set_timestep(self.h, int(sc["ntimestep"])))
 
     def _err(self):
         buf = ctypes.create_string_buffer(512)
@@ -728,10 +733,12 @@ class Engine:
         return nodes, vel
 
     def snapshot(self, sc):
-        """What a restart of this run needs, downloaded: the atoms, the pair
-        contact history (partner layout), every primitive wall's history and
-        every mesh's contact history (restart layout) and current nodes."""
-        snap = {"atoms": self.atoms(), "history": self.history(), "walls": {}, "meshes": {}}
+        """What a restart of this run needs, downloaded: the timestep, the
+        atoms, the pair contact history (partner layout), every primitive
+        wall's history and every mesh's contact history (restart layout) and
+        current nodes."""
+        snap = {"atoms": self.atoms(), "history": self.history(), "walls": {}, "meshes": {},
+                "ntimestep": int(self.stats()["ntimestep"])}
         for i, f in enumerate(sc["fixes"]):
             if f["kind"] in ("wall_plane", "wall_cylinder"):
                 snap["walls"][i] = self.wall_hist(i)

@@ -334,6 +334,37 @@ def build_b200(jobs=8):
     return available_b200()
 
 
+def restart_script(sc, workdir, n_before, segments):
+    """A run of n_before steps that ends in write_restart, then clear and
+    read_restart (src/write_restart.cpp, src/read_restart.cpp) and the given
+    segments with a dump after each.  The restart file carries the box, the
+    atoms with their per-atom fix data (pair contact history, primitive-wall
+    history, mesh contact slots), the pair settings and the global fix state
+    (mesh nodes, the mover's time); neighbour and communication settings,
+    materials, the timestep, newton pair and every fix are given again,
+    under the same fix ids, so their restart data is applied to them."""
+    first = script(sc, workdir, [n_before])
+    path = os.path.join(workdir, "phase1.restart")
+    out = first + ["write_restart %s" % path, "clear"]
+    second = script(sc, workdir, segments, ["s%d" % i for i in range(len(segments))])
+    skip = ("atom_style", "boundary", "newton", "units", "communicate")
+    for line in second:
+        if line.startswith(skip):
+            continue
+        if line.startswith("read_data"):
+            # newton pair follows the script, not the file (src/read_restart.cpp)
+            out += ["read_restart %s" % path, "newton off", "communicate single vel yes"]
+            continue
+        out.append(line)
+    return out
+
+
+def run_restart(sc, n_before, segments, keep=None):
+    """The scenario through a real restart file: one dump per segment after
+    the restart (see restart_script)."""
+    return run(sc, segments, keep=keep, script_lines=lambda wd: restart_script(sc, wd, n_before, segments))
+
+
 def run(sc, segments, keep=None, harness=None, extra_args=(), script_lines=None):
     """Run the scenario in the reference: setup + segments[0] steps, then
     each further segment as a continued run; returns one dump per segment.

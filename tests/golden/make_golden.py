@@ -1,6 +1,7 @@
 """Regenerate reference_digests.json from the reference itself.
 
-Runs every scene of tests/ref_scenes.py through the reference harness
+Runs every scene of tests/ref_scenes.py (the restart scenes through a real
+restart file) through the reference harness
 (oracle/_ref/ref_harness, built from the reference's sources by
 oracle/Makefile.ref) and writes, per checkpoint, SHA-256 digests of the raw
 state: atoms (tag, x, v, omega, f, torque in local order), the pair list
@@ -34,12 +35,19 @@ def main(names):
     if os.path.exists(OUT):
         with open(OUT) as f:
             data = json.load(f)
-    for name in names or list(ref_scenes.ALL_SCENES):
-        build, segments = ref_scenes.ALL_SCENES[name]
-        sc = build()
+    for name in names or list(ref_scenes.ALL_SCENES) + list(ref_scenes.RESTART_SCENES):
         t = time.time()
-        dumps = ref.run(sc, segments)
-        data[name] = {"segments": segments, "checkpoints": [ref_scenes.digest_dump(sc, d) for d in dumps]}
+        if name in ref_scenes.RESTART_SCENES:
+            build, n_before, segments = ref_scenes.RESTART_SCENES[name]
+            sc = build()
+            dumps = ref.run_restart(sc, n_before, segments)
+            data[name] = {"restart_after": n_before, "segments": segments,
+                          "checkpoints": [ref_scenes.digest_dump(sc, d) for d in dumps]}
+        else:
+            build, segments = ref_scenes.ALL_SCENES[name]
+            sc = build()
+            dumps = ref.run(sc, segments)
+            data[name] = {"segments": segments, "checkpoints": [ref_scenes.digest_dump(sc, d) for d in dumps]}
         print("%-32s %6.1f s  last: %s" % (name, time.time() - t, {k: v for k, v in data[name]["checkpoints"][-1].items()
                                                                      if not isinstance(v, str)}))
     data = {k: data[k] for k in sorted(data)}

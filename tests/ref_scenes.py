@@ -104,6 +104,17 @@ LONG_SCENES = {
 
 ALL_SCENES = dict(SCENES, **STREAM_SCENES, **LONG_SCENES)
 
+# Restart through a real restart file: the reference runs n_before steps,
+# write_restart, clear, read_restart, then the segments (setup first); the
+# engine restarts from its own download of the same state (atoms, pair,
+# primitive-wall and mesh contact histories, current mesh nodes).
+# name -> (scenario builder, n_before, segments after the restart)
+RESTART_SCENES = {
+    "drum_rotating_restart": (_drum, 2500, [0, 500, 500]),
+    "silo_cylinder_piston_restart": (lambda: S.silo(n=1500, piston_speed=0.5), 1500, [0, 500, 500]),
+    "pour3k_rolling_restart": (_pour3k, 300, [0, 150, 150]),
+}
+
 
 def _h(*arrays):
     h = hashlib.sha256()

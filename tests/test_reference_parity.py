@@ -24,7 +24,7 @@ import pytest
 
 import oracle
 import ref
-from ref_scenes import ALL_SCENES, SCENES, STREAM_SCENES, digest_dump, digest_sim, first_difference
+from ref_scenes import ALL_SCENES, RESTART_SCENES, SCENES, STREAM_SCENES, digest_dump, digest_sim, first_difference
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_digests.json")
 with open(GOLDEN) as _f:
@@ -38,8 +38,8 @@ def _ref_available():
         return False
 
 
-def _run_checkpoints(sim, sc, segments, nbuilds):
-    out, t = [], 0
+def _run_checkpoints(sim, sc, segments, nbuilds, t0=0):
+    out, t = [], t0
     sim.setup()
     for s in segments:
         if s:
@@ -68,6 +68,26 @@ def test_golden_covers_every_scene():
     assert last["silo_cylinder_piston"]["nmesh3"] > 0
     assert last["insert_pack_periodic"]["nlocal"] > 400
     assert last["config1_pour_20k_20000steps"]["ntouch"] > 40000
+
+
+def test_golden_covers_every_restart_scene():
+    for name, (_, n_before, segments) in RESTART_SCENES.items():
+        assert DIGESTS[name]["restart_after"] == n_before and DIGESTS[name]["segments"] == segments
+        first = DIGESTS[name]["checkpoints"][0]
+        assert first["ntimestep"] == n_before and first["ntouch"] > 0
+    assert DIGESTS["drum_rotating_restart"]["checkpoints"][0]["nmesh1"] > 0
+    assert DIGESTS["silo_cylinder_piston_restart"]["checkpoints"][0]["nmesh3"] > 0
+
+
+@pytest.mark.parametrize("name", sorted(RESTART_SCENES))
+def test_reference_restart_reproduces_golden(name):
+    """The restart digests are the reference's output through a real
+    restart file (write_restart, clear, read_restart; live run here)."""
+    if not _ref_available():
+        pytest.skip("reference not built and its sources are absent")
+    build, n_before, segments = RESTART_SCENES[name]
+    sc = build()
+    _compare(name, [digest_dump(sc, d) for d in ref.run_restart(sc, n_before, segments)])
 
 
 @pytest.mark.parametrize("name", sorted(SCENES) + sorted(STREAM_SCENES))
@@ -124,6 +144,33 @@ def test_engine_matches_reference(name):
     sc = build()
     e = granb200.Engine(sc)
     _compare(name, _run_checkpoints(e, sc, segments, lambda s: s.stats()["nbuilds"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(RESTART_SCENES))
+def test_engine_restart_matches_reference(name):
+    """A restart: the engine runs n_before steps, its state is downloaded
+    in the restart layout (atoms in local order, pair contact history as
+    partner tags and shear, primitive-wall histories, mesh contact slots,
+    current mesh nodes), and a new engine built from that download equals,
+    bit for bit at every checkpoint, the reference continued from its own
+    restart file (the restarted setup re-sorts the atoms and computes forces
+    without a shear update, as every setup does, and the atom-sort schedule
+    counts from the restart's timestep)."""
+    import granb200
+    build, n_before, segments = RESTART_SCENES[name]
+    sc = build()
+    e = granb200.Engine(sc)
+    e.setup()
+    e.run(n_before)
+    snap = e.snapshot(sc)
+    e.close()
+    assert snap["ntimestep"] == n_before
+    sc2 = granb200.restart_scenario(sc, snap["atoms"], {i: m["nodes"] for i, m in snap["meshes"].items()},
+                                    ntimestep=snap["ntimestep"])
+    e2 = granb200.Engine(sc2)
+    e2.restore(snap)
+    _compare(name, _run_checkpoints(e2, sc2, segments, lambda s: s.stats()["nbuilds"], t0=n_before))
 
 
 @pytest.mark.gpu
