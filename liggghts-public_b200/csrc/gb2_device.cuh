@@ -333,6 +333,68 @@ __device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn,
     }
 }
 
+// Screening that also lists the warp's touching entries in shared memory,
+// so the contact rounds read each item's partner and slot there instead of
+// gathering the list index again: lrev holds the j-side entries, lown the
+// own entries, each as {other atom, owner lane | slot << 8} in the order the
+// owner's sum takes them (every atom's rev entries by r, then its own entries
+// by s; the rev list is evaluated first).  Entries are appended per loop
+// step with ballots; the loop runs to the warp's longest list so every lane
+// takes part.  Inactive lanes (invalid or serial atoms) pass nr = nn = 0.
+// Returns false when a list outgrew kItemCap (the bitmasks are complete
+// either way, and the caller falls back to enumerating them).
+constexpr int kItemCap = 160;
+
+__device__ __forceinline__ void list_append(int2 *list, int &n, bool take, int other, int code)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int pos = n + __popc(m & ((1u << lane) - 1u));
+    if (take && pos < kItemCap) list[pos] = make_int2(other, code);
+    n += __popc(m);
+}
+
+__device__ __forceinline__ bool screen_list(const Dev &D, int k, int nr, int nn, const dbl4 &pk,
+                                            unsigned long long &mrev, unsigned long long &mown, int2 *lrev,
+                                            int2 *lown, int &nlrev, int &nlown)
+{
+    const int cap = D.cap, lane = threadIdx.x & 31;
+    const int nw = __reduce_max_sync(0xffffffffu, max(nr, nn));
+    nlrev = nlown = 0;
+    int a0 = (0 < nr) ? ld_stream(&D.rev[k]) : 0;
+    int a1 = (1 < nr) ? ld_stream(&D.rev[cap + k]) : 0;
+    int s0 = (0 < nr) ? (int)D.revs[k] : 0;
+    int s1 = (1 < nr) ? (int)D.revs[cap + k] : 0;
+    int b0 = (0 < nn) ? ld_stream(&D.nbr[k]) : 0;
+    int b1 = (1 < nn) ? ld_stream(&D.nbr[cap + k]) : 0;
+    for (int t = 0; t < nw; t += 2) {
+        const dbl4 qa0 = ldg4(&D.pos[a0]);
+        const dbl4 qa1 = ldg4(&D.pos[a1]);
+        const dbl4 qb0 = ldg4(&D.pos[b0]);
+        const dbl4 qb1 = ldg4(&D.pos[b1]);
+        const int ca0 = a0, ca1 = a1, cs0 = s0, cs1 = s1, cb0 = b0, cb1 = b1;
+        const int u = t + 2;
+        a0 = (u < nr) ? ld_stream(&D.rev[u * cap + k]) : 0;
+        a1 = (u + 1 < nr) ? ld_stream(&D.rev[(u + 1) * cap + k]) : 0;
+        s0 = (u < nr) ? (int)D.revs[u * cap + k] : 0;
+        s1 = (u + 1 < nr) ? (int)D.revs[(u + 1) * cap + k] : 0;
+        b0 = (u < nn) ? ld_stream(&D.nbr[u * cap + k]) : 0;
+        b1 = (u + 1 < nn) ? ld_stream(&D.nbr[(u + 1) * cap + k]) : 0;
+        const bool ta0 = t < nr && touching(pk, qa0), ta1 = t + 1 < nr && touching(pk, qa1);
+        const bool tb0 = t < nn && touching(pk, qb0), tb1 = t + 1 < nn && touching(pk, qb1);
+        if (ta0) mrev |= 1ull << t;
+        if (ta1) mrev |= 1ull << (t + 1);
+        if (tb0) mown |= 1ull << t;
+        if (tb1) mown |= 1ull << (t + 1);
+        list_append(lrev, nlrev, ta0, ca0, lane | (cs0 << 8));
+        list_append(lrev, nlrev, ta1, ca1, lane | (cs1 << 8));
+        list_append(lown, nlown, tb0, cb0, lane | (t << 8));
+        list_append(lown, nlown, tb1, cb1, lane | ((t + 1) << 8));
+    }
+    return nlrev <= kItemCap && nlown <= kItemCap;
+}
+
 __device__ __forceinline__ WarpItems warp_items_cnt(int cnt)
 {
     const unsigned FULL = 0xffffffffu;

@@ -1157,8 +1157,10 @@ void launch_pair(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int f
         launch_pair_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f);
         return;
     }
-    // MINB: minimum resident 128-thread blocks per SM asked of the register allocator
-    const int mb = c->minb ? c->minb : 4;
+    // MINB: minimum resident 128-thread blocks per SM asked of the register
+    // allocator; 5 (96 registers, a small spill) measured fastest on the
+    // packed 1M hopper, ahead of 4 (128) and 6 (80)
+    const int mb = c->minb ? c->minb : 5;
     if (c->P.rolling_cdt) {
         if (mb == 4) launch_pair_kernel<true, 4>(c, D, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch_pair_kernel<true, 5>(c, D, shearupdate, integrate, fuse_next, store_f);

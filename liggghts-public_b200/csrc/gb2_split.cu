@@ -21,7 +21,7 @@ static void launch(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, 
 void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
                        int fuse_next, int store_f)
 {
-    const int mb = minb ? minb : 7;
+    const int mb = minb ? minb : 5;   // 5 (96 registers, no spill) measured fastest on the packed 1M hopper
     if (D.rolling) {
         if (mb == 4) launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
         else if (mb == 5) launch<true, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);

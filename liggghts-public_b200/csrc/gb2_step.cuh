@@ -357,6 +357,10 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     // velocity, position at the last rebuild) wait here, not in registers,
     // while the screening and the contact rounds run
     __shared__ __align__(16) dbl4 stail[3][128];
+    // per warp: the touching entries listed by the screening (rev, own) and
+    // each round's owner-lane masks, tagged with the round
+    __shared__ int2 slist[4][2][kItemCap];
+    __shared__ unsigned long long sgrp[4][32];
     grid_dep_launch();   // the tail kernel may be scheduled once every block of this grid runs
     if (step_cancelled(D)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -382,18 +386,55 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
         tk = D.type[k];
         serial = nr > 64 || nn > 64;
         tail = tail_atom(D, k, nr, nn);
-        if (!serial) {
-            if (upd) prevm = D.prevmask[k];
-            screen_both(D, k, nr, nn, pk, mrev, mown);
-        }
+        if (!serial && upd) prevm = D.prevmask[k];
     }
+    // screening of every non-serial atom of the warp, listing its touching
+    // entries (all lanes take part in the list ballots)
+    int nlrev = 0, nlown = 0;
+    const bool listed = screen_list(D, k, (valid && !serial) ? nr : 0, (valid && !serial) ? nn : 0, pk, mrev, mown,
+                                    slist[wid][0], slist[wid][1], nlrev, nlown);
     // FP64 path: plain in-order sums (bit-exact).  Split path: FP32 sums of
     // the FP32 pair contributions with Kahan compensation kc.
     Real as[6], kc[6];
 #pragma unroll
     for (int c = 0; c < 6; c++) as[c] = kc[c] = Real(0);
-    const int crev = __popcll(mrev);
-    {
+    if (listed) {
+        // rounds over the listed items, rev list first: lane t evaluates item
+        // base + t; the lanes holding one owner's items find each other with
+        // a match, the first of them publishes the group to the owner, and
+        // the owner adds its items in list order
+        sgrp[wid][lane] = ~0ull;
+        __syncwarp();
+        int round = 0;
+        for (int li = 0; li < 2; li++) {
+            const int tot = li ? nlown : nlrev;
+            for (int base = 0; base < tot; base += 32, round++) {
+                const int w = base + lane;
+                int L = -1 - lane;   // lanes without an item match nobody
+                if (w < tot) {
+                    const int2 item = slist[wid][li][w];
+                    L = item.y & 31;
+                    Real res[6];
+                    eval_item<ROLLING, SPLIT>(D, wbase + L, item.x, item.y >> 8, li == 1, upd, res);
+#pragma unroll
+                    for (int c = 0; c < 6; c++) sres[wid][lane][c] = res[c];
+                }
+                const unsigned grp = __match_any_sync(0xffffffffu, L);
+                if (w < tot && (grp & ((1u << lane) - 1u)) == 0u)
+                    sgrp[wid][L] = ((unsigned long long)(unsigned)round << 32) | grp;
+                __syncwarp();
+                const unsigned long long g = sgrp[wid][lane];
+                unsigned mine = (unsigned)(g >> 32) == (unsigned)round ? (unsigned)g : 0u;
+                while (mine) {
+                    const int q = __ffs(mine) - 1;
+                    mine &= mine - 1u;
+                    sum_item<SPLIT>(as, kc, &sres[wid][q][0]);
+                }
+                __syncwarp();
+            }
+        }
+    } else {   // a list outgrew its capacity: enumerate the bitmasks
+        const int crev = __popcll(mrev);
         const WarpItems it = warp_items_cnt(crev + __popcll(mown));
         for (int base = 0; base < it.total; base += 32) {
             const int w = base + lane;
