@@ -500,14 +500,23 @@ def own_arm(args):
     ab = algorithmic_bytes(n, cen_src, nfix_plane, nfix_mesh, False)
     achieved = ab / (dom_ms * 1e-3) / 1e9 if npm > 0 and dom_ms > 0 else None
     traffic = load_traffic(dom, args.workload)
+    # the capture's DRAM bytes belong to its own state (census at capture):
+    # the ratio to the algorithmic bytes is taken there, and the per-launch
+    # traffic of this window is that ratio times this window's algorithmic bytes
+    t_ratio = None
+    if traffic and traffic.get("algorithmic_bytes_at_capture"):
+        t_ratio = traffic["bytes_per_launch"] / traffic["algorithmic_bytes_at_capture"]
     line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                        "traffic": traffic["bytes_per_launch"] if traffic else None,
-                        "traffic_over_algorithmic": traffic["bytes_per_launch"] / ab if traffic and ab else None,
+                        "traffic": t_ratio * ab if t_ratio and ab else None,
+                        "traffic_over_algorithmic": t_ratio,
                         "algorithmic_bytes_per_launch": ab, "avg_launch_ms": dom_ms, "sampled_launches": npm,
                         "timing": "every pair-step launch timed with CUDA events over the %s" % src}
     if traffic:
-        line["roofline"]["traffic_source"] = traffic.get("capture")
+        line["roofline"]["traffic_source"] = (traffic.get("capture", "") + "; measured %d bytes at a state of %d "
+                                              "algorithmic bytes, scaled to this window by its algorithmic bytes"
+                                              % (traffic["bytes_per_launch"],
+                                                 traffic.get("algorithmic_bytes_at_capture", 0)))
 
     # longer FP64 window with rebuilds
     if args.long_steps > 0:
