@@ -341,8 +341,8 @@ __device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn,
 // by s; the rev list is evaluated first).  Entries are appended per loop
 // step with ballots; the loop runs to the warp's longest list so every lane
 // takes part.  Inactive lanes (invalid or serial atoms) pass nr = nn = 0.
-// Returns false when a list outgrew kItemCap (the bitmasks are complete
-// either way, and the caller falls back to enumerating them).
+// Returns false when a list outgrew D.item_cap (<= kItemCap; the bitmasks
+// are complete either way, and the caller falls back to enumerating them).
 constexpr int kItemCap = 160;
 
 __device__ __forceinline__ void list_append(int2 *list, int &n, bool take, int other, int code)
@@ -392,7 +392,7 @@ __device__ __forceinline__ bool screen_list(const Dev &D, int k, int nr, int nn,
         list_append(lown, nlown, tb0, cb0, lane | (t << 8));
         list_append(lown, nlown, tb1, cb1, lane | ((t + 1) << 8));
     }
-    return nlrev <= kItemCap && nlown <= kItemCap;
+    return nlrev <= D.item_cap && nlown <= D.item_cap;
 }
 
 __device__ __forceinline__ WarpItems warp_items_cnt(int cnt)

@@ -163,6 +163,7 @@ struct gb2_ctx {
     int minb = 0;                 // register-allocation target of the pair step kernel (blocks/SM; 0: default)
     int nsm = 148;                // SMs of the device
     int tail_per_sm = 8;          // blocks of the tail kernel per SM (kTailAtoms atoms per warp)
+    int item_cap = kItemCap;      // listed-round capacity per warp; GB2_ITEM_CAP lowers it (0: masks only)
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
     // steps queued ahead of the rebuild decision (see gb2_run)
     bool queue_ok = true;         // GB2_QUEUE_DEPTH=0 turns it off
@@ -351,6 +352,7 @@ Dev make_dev(gb2_ctx *c)
     D.tailcnt = c->dtailcnt.p;
     D.xhold = c->xhold.p;
     D.maxn = c->maxn;
+    D.item_cap = c->item_cap;
     D.nnum = c->nnum.p;
     D.nbr = c->nbr.p;
     D.flag = c->flag.p;
@@ -1311,6 +1313,7 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
     if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
     if (const char *tb = std::getenv("GB2_TAIL_BLOCKS")) c->tail_per_sm = std::max(1, std::atoi(tb));
+    if (const char *ic = std::getenv("GB2_ITEM_CAP")) c->item_cap = std::min(std::max(std::atoi(ic), 0), kItemCap);
     if (const char *qd = std::getenv("GB2_QUEUE_DEPTH")) {
         c->queue_depth = std::min(std::max(std::atoi(qd), 0), 15);
         c->queue_ok = c->queue_depth > 0;

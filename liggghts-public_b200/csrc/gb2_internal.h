@@ -129,6 +129,7 @@ struct Dev {
     int *tail, *tailcnt;   // tail-kernel atom list and its length
     // half list
     int maxn;
+    int item_cap;          // per-warp list capacity of the pair step's listed rounds (<= kItemCap)
     int *nnum, *nbr, *flag;
     double *hist;          // shear read buffer (current values)
     double *hist_out;      // shear write buffer of the pair step

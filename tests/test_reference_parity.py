@@ -147,6 +147,22 @@ def test_engine_matches_reference(name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["hopper_packed_discharge", "bidisperse_long_lists", "insert_pack_periodic"])
+def test_engine_mask_rounds_match_reference(name, monkeypatch):
+    """The pair step's other enumeration: with the per-warp item lists
+    disabled (GB2_ITEM_CAP=0, as a warp whose lists outgrow their capacity
+    runs) every warp evaluates its pairs from the screening bitmasks; the
+    results are the same digests, bit for bit."""
+    import granb200
+    monkeypatch.setenv("GB2_ITEM_CAP", "0")
+    build, segments = ALL_SCENES[name]
+    sc = build()
+    e = granb200.Engine(sc)
+    _compare(name, _run_checkpoints(e, sc, segments, lambda s: s.stats()["nbuilds"]))
+    e.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(RESTART_SCENES))
 def test_engine_restart_matches_reference(name):
     """A restart: the engine runs n_before steps, its state is downloaded
