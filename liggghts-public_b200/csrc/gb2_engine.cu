@@ -895,8 +895,7 @@ int do_atom_sort(gb2_ctx *c)
         auto gather_slots = [&](auto &a, auto &sh, int nslot, const int *cnt_old, int div) -> int {
             if (nslot <= 0) return 0;
             CK(sh.alloc((size_t)nslot * c->cap));
-            dim3 g(nblk(n), nslot);
-            k_gather_slots_cnt<<<g, kBlock, 0, c->st>>>(a.p, sh.p, perm, n, c->cap, nslot, cnt_old, div);
+            if (n > 0) k_gather_slots_cnt<<<nblk(n), kBlock, 0, c->st>>>(a.p, sh.p, perm, n, c->cap, nslot, cnt_old, div);
             CKL();
             a.swap(sh);
             return 0;

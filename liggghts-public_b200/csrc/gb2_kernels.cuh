@@ -227,28 +227,19 @@ __global__ void k_gather(const T *__restrict__ src, T *__restrict__ dst, const i
     if (i < n) dst[i] = src[perm[i]];
 }
 
-// slot-major gather: dst[s*cap + i] = src[s*cap + perm[i]] for s < nslot
-template <typename T>
-__global__ void k_gather_slots(const T *__restrict__ src, T *__restrict__ dst, const int *__restrict__ perm, int n,
-                               int cap, int nslot)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = blockIdx.y;
-    if (i < n && s < nslot) dst[(size_t)s * cap + i] = src[(size_t)s * cap + perm[i]];
-}
-
 // slot-major gather of the slots an atom uses: dst[s*cap+i] = src[s*cap+perm[i]]
 // for s / div < cnt_old[perm[i]] (all slots when cnt_old is null)
+// (one thread per atom: it reads its source index and count once and copies
+// only the occupied slots, so empty histories cost one thread per atom)
 template <typename T>
 __global__ void k_gather_slots_cnt(const T *__restrict__ src, T *__restrict__ dst, const int *__restrict__ perm, int n,
                                    int cap, int nslot, const int *__restrict__ cnt_old, int div)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = blockIdx.y;
-    if (i >= n || s >= nslot) return;
+    if (i >= n) return;
     const int o = perm[i];
-    if (cnt_old && s / div >= cnt_old[o]) return;
-    dst[(size_t)s * cap + i] = src[(size_t)s * cap + o];
+    const int m = cnt_old ? min(nslot, cnt_old[o] * div) : nslot;
+    for (int s = 0; s < m; s++) dst[(size_t)s * cap + i] = src[(size_t)s * cap + o];
 }
 
 // Comm::borders swap selection (src/comm.cpp:1028, Comm::decide src/comm_I.h:66)
