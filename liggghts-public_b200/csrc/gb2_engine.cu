@@ -1405,15 +1405,12 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
 {
     if (!c || n <= 0 || !x || !v || !omega || !radius || !rmass || !type || !tag) return GB2_ERR_ARG;
     if (c->setup_done) return set_err(c, GB2_ERR_STATE, "atoms must be uploaded before setup");
-    for (int i = 0; i < n; i++)
-        if (type[i] < 1 || type[i] > c->P.ntypes) return set_err(c, GB2_ERR_ARG, "atom type out of range");
+    c->have_atoms = false;   // until this upload has passed every check
     c->nlocal = n;
     c->cap = (n + 31) / 32 * 32;
     c->nmax = 0;
     c->nghost = 0;
     if (ensure_nmax(c, n + n / 4 + 1024)) return GB2_ERR_CUDA;
-    c->h_radius.assign(radius, radius + n);
-    c->h_type.assign(type, type + n);
     // x | v | omega | radius | rmass staged as 11 n doubles, one host-to-device
     // copy per array (straight from the caller's memory when it is pinned),
     // packed into the 32-byte records and checked on the device
@@ -1443,7 +1440,16 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     CK(cudaMemcpyAsync(c->tag.p, tag, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
     int bad[2];
     CK(cudaMemcpyAsync(bad, c->iocheck.p, sizeof bad, cudaMemcpyDeviceToHost, c->st));
+    // host-side checks and mirrors while the copies are in flight
+    int bad_type = -1;
+    for (int i = 0; i < n && bad_type < 0; i++)
+        if (type[i] < 1 || type[i] > c->P.ntypes) bad_type = i;
+    if (bad_type < 0) {
+        c->h_radius.assign(radius, radius + n);
+        c->h_type.assign(type, type + n);
+    }
     CK(cudaStreamSynchronize(c->st));
+    if (bad_type >= 0) return set_err(c, GB2_ERR_ARG, "atom type out of range");
     if (bad[1] == 2) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
     if (bad[1] == 3) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
     if (bad[1] == 1) return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", bad[0]);

@@ -312,6 +312,24 @@ def test_mesh_surface_stress():
     assert np.abs((w[0] - w[1]) - wa).max() <= 1e-12 * wa.max()
 
 
+def test_upload_rejects_bad_atoms():
+    """An atom type outside 1..ntypes, a zero radius or a non-finite
+    position is refused by the upload with its reason (the checks run while
+    the copies are in flight), and a context whose upload failed has no atoms."""
+    import granb200
+    cases = [("type", 0, "atom type out of range"), ("radius", 0.0, "extended particles"),
+             ("x", np.nan, "non-finite atom state")]
+    for key, value, msg in cases:
+        sc = S.sphere_pour(n=200, seed=3)
+        a = dict(sc["atoms"])
+        arr = np.array(a[key], copy=True)
+        arr[7] = value
+        a[key] = arr
+        sc["atoms"] = a
+        with pytest.raises(granb200.GB2Error, match=msg):
+            granb200.Engine(sc)
+
+
 def test_mesh_wear_needs_a_type_matrix():
     """k_finnie is an ntypes x ntypes matrix; anything else is refused before it reaches the library."""
     import granb200
