@@ -341,17 +341,18 @@ __device__ __forceinline__ void screen_both(const Dev &D, int k, int nr, int nn,
 // by s; the rev list is evaluated first).  Entries are appended per loop
 // step with ballots; the loop runs to the warp's longest list so every lane
 // takes part.  Inactive lanes (invalid or serial atoms) pass nr = nn = 0.
-// Returns false when a list outgrew D.item_cap (<= kItemCap; the bitmasks
-// are complete either way, and the caller falls back to enumerating them).
-constexpr int kItemCap = 160;
+// Returns false when a list outgrew D.item_cap (the lists' size in the
+// kernel's dynamic shared memory, at most kItemCap; the bitmasks are
+// complete either way, and the caller falls back to enumerating them).
+constexpr int kItemCap = 256;
 
-__device__ __forceinline__ void list_append(int2 *list, int &n, bool take, int other, int code)
+__device__ __forceinline__ void list_append(int2 *list, int cap, int &n, bool take, int other, int code)
 {
     const unsigned m = __ballot_sync(0xffffffffu, take);
     if (!m) return;
     const int lane = threadIdx.x & 31;
     const int pos = n + __popc(m & ((1u << lane) - 1u));
-    if (take && pos < kItemCap) list[pos] = make_int2(other, code);
+    if (take && pos < cap) list[pos] = make_int2(other, code);
     n += __popc(m);
 }
 
@@ -387,10 +388,10 @@ __device__ __forceinline__ bool screen_list(const Dev &D, int k, int nr, int nn,
         if (ta1) mrev |= 1ull << (t + 1);
         if (tb0) mown |= 1ull << t;
         if (tb1) mown |= 1ull << (t + 1);
-        list_append(lrev, nlrev, ta0, ca0, lane | (cs0 << 8));
-        list_append(lrev, nlrev, ta1, ca1, lane | (cs1 << 8));
-        list_append(lown, nlown, tb0, cb0, lane | (t << 8));
-        list_append(lown, nlown, tb1, cb1, lane | ((t + 1) << 8));
+        list_append(lrev, D.item_cap, nlrev, ta0, ca0, lane | (cs0 << 8));
+        list_append(lrev, D.item_cap, nlrev, ta1, ca1, lane | (cs1 << 8));
+        list_append(lown, D.item_cap, nlown, tb0, cb0, lane | (t << 8));
+        list_append(lown, D.item_cap, nlown, tb1, cb1, lane | ((t + 1) << 8));
     }
     return nlrev <= D.item_cap && nlown <= D.item_cap;
 }

@@ -163,7 +163,9 @@ struct gb2_ctx {
     int minb = 0;                 // register-allocation target of the pair step kernel (blocks/SM; 0: default)
     int nsm = 148;                // SMs of the device
     int tail_per_sm = 8;          // blocks of the tail kernel per SM (kTailAtoms atoms per warp)
-    int item_cap = kItemCap;      // listed-round capacity per warp; GB2_ITEM_CAP lowers it (0: masks only)
+    int item_cap = 160;           // listed-round capacity per warp and side (grown on demand up to kItemCap)
+    bool item_cap_fixed = false;  // GB2_ITEM_CAP sets it and stops the growth (0: masks only)
+    int item_cap_grown = 0;
     bool fused_pending = false;   // the previous pass B already ran this step's initial_integrate
     // steps queued ahead of the rebuild decision (see gb2_run)
     bool queue_ok = true;         // GB2_QUEUE_DEPTH=0 turns it off
@@ -193,7 +195,7 @@ struct gb2_ctx {
     DBuf<char> cubtmp;
     DBuf<int> dstatus, ddflag, dneed, dtailcnt;
     long ngrow = 0;
-    int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel
+    int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel, [6] short item lists
     // neighbor
     double cutneighmax = 0, triggersq = 0;
     int ago = 0, nbuilds = 0;
@@ -1144,10 +1146,33 @@ int do_rebuild(gb2_ctx *c, bool pre_exchange, bool sort_now, bool insert, bool g
     return 0;
 }
 
+// Dynamic shared memory of the pair step: each of its 4 warps lists up to
+// item_cap touching entries on each side (8 bytes each).
+size_t pair_list_smem(const gb2_ctx *c) { return (size_t)4 * 2 * c->item_cap * sizeof(int2); }
+
+// The pair step counts warps whose touching entries outgrew their lists
+// (they take the slower mask enumeration); at setup and at each rebuild the
+// lists grow by half, up to kItemCap, while any warp did.  Short lists keep
+// shared memory, and with it L1 for the neighbour gathers, on beds with few
+// contacts per atom.
+int adapt_item_cap(gb2_ctx *c)
+{
+    if (c->item_cap_fixed || c->item_cap >= kItemCap) return 0;
+    CK(cudaMemcpyAsync(&c->h_pinned[6], c->dneed.p + 4, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_pinned[6] > 0) {
+        c->item_cap = std::min(kItemCap, (c->item_cap * 3 / 2 + 31) / 32 * 32);
+        c->item_cap_grown++;
+    }
+    CK(cudaMemsetAsync(c->dneed.p + 4, 0, sizeof(int), c->st));
+    return 0;
+}
+
 template <bool R, int MINB>
 void launch_pair_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
-    k_pair_step<R, MINB, false><<<nblk(c->nlocal), kBlock, 0, c->st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    k_pair_step<R, MINB, false><<<nblk(c->nlocal), kBlock, pair_list_smem(c), c->st>>>(D, shearupdate, integrate,
+                                                                                     fuse_next, store_f);
 }
 
 // The pair step kernel of one time step (every atom's pair sums; the
@@ -1155,7 +1180,8 @@ void launch_pair_kernel(gb2_ctx *c, const Dev &D, int shearupdate, int integrate
 void launch_pair(gb2_ctx *c, const Dev &D, int shearupdate, int integrate, int fuse_next, int store_f)
 {
     if (c->split) {
-        launch_pair_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f);
+        launch_pair_split(D, nblk(c->nlocal), c->st, c->minb, shearupdate, integrate, fuse_next, store_f,
+                          pair_list_smem(c));
         return;
     }
     // MINB: minimum resident 128-thread blocks per SM asked of the register
@@ -1312,7 +1338,10 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     if (c->P.neigh_every <= 0) c->P.neigh_every = 1;
     if (const char *mb = std::getenv("GB2_PAIR_MINB")) c->minb = std::atoi(mb);
     if (const char *tb = std::getenv("GB2_TAIL_BLOCKS")) c->tail_per_sm = std::max(1, std::atoi(tb));
-    if (const char *ic = std::getenv("GB2_ITEM_CAP")) c->item_cap = std::min(std::max(std::atoi(ic), 0), kItemCap);
+    if (const char *ic = std::getenv("GB2_ITEM_CAP")) {
+        c->item_cap = std::min(std::max(std::atoi(ic), 0), kItemCap);
+        c->item_cap_fixed = true;
+    }
     if (const char *qd = std::getenv("GB2_QUEUE_DEPTH")) {
         c->queue_depth = std::min(std::max(std::atoi(qd), 0), 15);
         c->queue_ok = c->queue_depth > 0;
@@ -1331,9 +1360,9 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
     }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
-        c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(4) != cudaSuccess || c->dstop.alloc(1) != cudaSuccess ||
+        c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(5) != cudaSuccess || c->dstop.alloc(1) != cudaSuccess ||
         c->dtailcnt.alloc(1) != cudaSuccess || cudaMallocHost(&c->h_stop, 16 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->dneed.p, 0, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->dneed.p, 0, 5 * sizeof(int)) != cudaSuccess ||
         cudaMemset(c->dtailcnt.p, 0, sizeof(int)) != cudaSuccess ||
         cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess ||
@@ -1833,6 +1862,7 @@ int gb2_setup(gb2_ctx *c)
     if (rc) return rc;
     if (do_force(c, 0, 0, 0, 1)) return GB2_ERR_CUDA;
     CK(cudaStreamSynchronize(c->st));
+    if (adapt_item_cap(c)) return GB2_ERR_CUDA;
     if (c->ins) {   // FixInsert::setup: region volume by Monte Carlo
         const std::string e = c->ins->setup();
         if (!e.empty()) return set_err(c, GB2_ERR_ARG, "fix insert/pack: %s", e.c_str());
@@ -2108,6 +2138,7 @@ static int one_step(gb2_ctx *c, bool last, int mode)
         if (prof_begin(c, PROF_REBUILD, &e)) return GB2_ERR_CUDA;
         int rc = do_rebuild(c, true, sort_now, insert_now, ghosts_prev);
         if (rc) return rc;
+        if (adapt_item_cap(c)) return GB2_ERR_CUDA;
         if (prof_end(c, &e)) return GB2_ERR_CUDA;
         c->nsteps_rebuild++;
     } else if (c->nghost > 0) {

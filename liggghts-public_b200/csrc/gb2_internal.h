@@ -169,8 +169,9 @@ struct Dev {
     int step;                // step number of this launch (compared with *dstop)
     const dbl4 *rel;         // fix insert/stream release data [4*cap] (null without a stream):
                              // {x_ins, i_step} {v_int, r_step} {v_release, -} {omega_release, -}
-    int *need;               // [4] capacity demand seen by the last overflowing kernel:
-                             // neighbour slots, partners, reverse entries, mesh slots
+    int *need;               // [5] capacity demand seen by the last overflowing kernel:
+                             // neighbour slots, partners, reverse entries, mesh slots;
+                             // [4] pair-step warps whose item lists were too short
 };
 
 // host-side mesh topology (gb2_mesh.cpp)
@@ -183,7 +184,7 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
                          std::string &err);
 // split-precision pair step (gb2_split.cu)
 void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
-                       int fuse_next, int store_f);
+                       int fuse_next, int store_f, size_t smem);
 void launch_tail_split(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
                        int store_f);
 bool tri_neighbuild_host(const TriGeom &T, double rSphere, const double *c, double treshold);

@@ -13,27 +13,27 @@ namespace gb2 {
 
 template <bool R, int MINB>
 static void launch(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
-                   int store_f)
+                   int store_f, size_t smem)
 {
-    k_pair_step<R, MINB, true><<<nblocks, 128, 0, st>>>(D, shearupdate, integrate, fuse_next, store_f);
+    k_pair_step<R, MINB, true><<<nblocks, 128, smem, st>>>(D, shearupdate, integrate, fuse_next, store_f);
 }
 
 void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int shearupdate, int integrate,
-                       int fuse_next, int store_f)
+                       int fuse_next, int store_f, size_t smem)
 {
     const int mb = minb ? minb : 5;   // 5 (96 registers, no spill) measured fastest on the packed 1M hopper
     if (D.rolling) {
-        if (mb == 4) launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 5) launch<true, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 6) launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 7) launch<true, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<true, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch<true, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 5) launch<true, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 6) launch<true, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 7) launch<true, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else launch<true, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
     } else {
-        if (mb == 4) launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 5) launch<false, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 6) launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else if (mb == 7) launch<false, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
-        else launch<false, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f);
+        if (mb == 4) launch<false, 4>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 5) launch<false, 5>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 6) launch<false, 6>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else if (mb == 7) launch<false, 7>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
+        else launch<false, 8>(D, nblocks, st, shearupdate, integrate, fuse_next, store_f, smem);
     }
 }
 

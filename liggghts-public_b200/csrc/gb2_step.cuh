@@ -357,9 +357,10 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     // velocity, position at the last rebuild) wait here, not in registers,
     // while the screening and the contact rounds run
     __shared__ __align__(16) dbl4 stail[3][128];
-    // per warp: the touching entries listed by the screening (rev, own) and
+    // per warp: the touching entries listed by the screening (rev, own; the
+    // launch gives 4 x 2 x D.item_cap of them in dynamic shared memory) and
     // each round's owner-lane masks, tagged with the round
-    __shared__ int2 slist[4][2][kItemCap];
+    extern __shared__ __align__(16) unsigned char pair_dyn[];
     __shared__ unsigned long long sgrp[4][32];
     grid_dep_launch();   // the tail kernel may be scheduled once every block of this grid runs
     if (step_cancelled(D)) return;
@@ -391,8 +392,10 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
     // screening of every non-serial atom of the warp, listing its touching
     // entries (all lanes take part in the list ballots)
     int nlrev = 0, nlown = 0;
+    int2 *lrev = reinterpret_cast<int2 *>(pair_dyn) + (size_t)wid * 2 * D.item_cap, *lown = lrev + D.item_cap;
     const bool listed = screen_list(D, k, (valid && !serial) ? nr : 0, (valid && !serial) ? nn : 0, pk, mrev, mown,
-                                    slist[wid][0], slist[wid][1], nlrev, nlown);
+                                    lrev, lown, nlrev, nlown);
+    if (!listed && lane == 0 && D.item_cap > 0) atomicAdd(&D.need[4], 1);   // lists too short: counted for the host
     // FP64 path: plain in-order sums (bit-exact).  Split path: FP32 sums of
     // the FP32 pair contributions with Kahan compensation kc.
     Real as[6], kc[6];
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(128, MINB) k_pair_step(Dev D, int shearupdate,
                 const int w = base + lane;
                 int L = -1 - lane;   // lanes without an item match nobody
                 if (w < tot) {
-                    const int2 item = slist[wid][li][w];
+                    const int2 item = (li ? lown : lrev)[w];
                     L = item.y & 31;
                     Real res[6];
                     eval_item<ROLLING, SPLIT>(D, wbase + L, item.x, item.y >> 8, li == 1, upd, res);
