@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -154,8 +155,9 @@ struct gb2_ctx {
     DBuf<MatPair> dmat;
 
     int nlocal = 0, nghost = 0, nmax = 0, cap = 0;
-    std::vector<double> h_radius;
-    std::vector<int> h_type;
+    // per type, the largest radius of the atoms uploaded or inserted (the
+    // neighbour cutoff at setup)
+    double h_maxrad[kMaxTypes + 1] = {};
     DBuf<dbl4> pos, vel, omg, pos2, vel2, omg2, f, tq, tailf, tailt, xhold;
     bool split = false;           // GB2_PREC_SPLIT
     DBuf<flt8> kin, kin2;         // split precision: FP32 kinematics records (double-buffered like vel)
@@ -195,7 +197,7 @@ struct gb2_ctx {
     DBuf<char> cubtmp;
     DBuf<int> dstatus, ddflag, dneed, dtailcnt;
     long ngrow = 0;
-    int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel, [6] short item lists
+    int *h_pinned = nullptr;   // [0] status, [1] dflag, [2] nsel, [6] short item lists, [8..9] upload checks
     // neighbor
     double cutneighmax = 0, triggersq = 0;
     int ago = 0, nbuilds = 0;
@@ -280,6 +282,41 @@ bool host_pinned(const void *p)
 }
 
 }  // namespace
+
+// The pinned-slot arena: 64 KiB page-locked blocks (portable, so contexts on
+// every device can copy through them) cut into kPinnedSlot-byte slots, handed
+// out and taken back under a mutex; blocks are never unlocked.
+namespace {
+std::mutex g_pinned_mu;
+std::vector<int *> g_pinned_free;
+constexpr size_t kPinnedBlock = 64 * 1024;
+}  // namespace
+
+int gb2::pinned_slot_get(int **slot)
+{
+    *slot = nullptr;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        char *blk = nullptr;
+        if (cudaHostAlloc((void **)&blk, kPinnedBlock, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return GB2_ERR_CUDA;
+        }
+        for (size_t o = kPinnedBlock; o >= kPinnedSlot; o -= kPinnedSlot)
+            g_pinned_free.push_back(reinterpret_cast<int *>(blk + o - kPinnedSlot));
+    }
+    *slot = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    std::memset(*slot, 0, kPinnedSlot);
+    return 0;
+}
+
+void gb2::pinned_slot_put(int *slot)
+{
+    if (!slot) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(slot);
+}
 
 // insertion fixes (defined below, in the C-linkage block), called inside a rebuild
 extern "C" {
@@ -553,7 +590,7 @@ void neighbor_init(gb2_ctx *c)
         for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->ins->max_rad(t));
     if (c->stream)
         for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->stream->max_rad(t));
-    for (int i = 0; i < c->nlocal; i++) maxrad[c->h_type[i]] = std::max(maxrad[c->h_type[i]], c->h_radius[i]);
+    for (int t = 1; t <= nt; t++) maxrad[t] = std::max(maxrad[t], c->h_maxrad[t]);
     c->triggersq = 0.25 * c->P.skin * c->P.skin;
     c->cutneighmax = 0.0;
     for (int i = 1; i <= nt; i++)
@@ -1358,18 +1395,22 @@ int gb2_create(const gb2_params *p, gb2_ctx **out)
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
         }
     }
+    // one arena slot holds h_pinned (ints 0..31) and the stop-word ring h_stop (ints 32..47)
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&c->h_pinned, 8 * sizeof(int)) != cudaSuccess || c->dstatus.alloc(1) != cudaSuccess ||
+        pinned_slot_get(&c->h_pinned) != 0 || c->dstatus.alloc(1) != cudaSuccess ||
         c->ddflag.alloc(2) != cudaSuccess || c->dneed.alloc(5) != cudaSuccess || c->dstop.alloc(1) != cudaSuccess ||
-        c->dtailcnt.alloc(1) != cudaSuccess || cudaMallocHost(&c->h_stop, 16 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->dneed.p, 0, 5 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->dtailcnt.p, 0, sizeof(int)) != cudaSuccess ||
+        c->dtailcnt.alloc(1) != cudaSuccess ||
+        cudaMemsetAsync(c->dneed.p, 0, 5 * sizeof(int), c->st) != cudaSuccess ||
+        cudaMemsetAsync(c->dtailcnt.p, 0, sizeof(int), c->st) != cudaSuccess ||
         cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess ||
         cudaEventCreate(&c->ev1) != cudaSuccess) {
+        pinned_slot_put(c->h_pinned);
+        if (c->st) cudaStreamDestroy(c->st);
         delete c;
         return GB2_ERR_CUDA;
     }
+    c->h_stop = c->h_pinned + 32;
     *out = c;
     return 0;
 }
@@ -1387,8 +1428,7 @@ int gb2_destroy(gb2_ctx *c)
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);
     }
-    if (c->h_pinned) cudaFreeHost(c->h_pinned);
-    if (c->h_stop) cudaFreeHost(c->h_stop);
+    pinned_slot_put(c->h_pinned);   // h_stop lies in the same slot
     for (auto &e : c->qev)
         if (e) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1461,27 +1501,15 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
             CK(cudaMemcpyAsync(c->iostage.p + off[k], h, bytes, cudaMemcpyHostToDevice, c->st));
         }
     }
-    const int init[2] = {INT32_MAX, 0};
-    CK(cudaMemcpyAsync(c->iocheck.p, init, sizeof init, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->iocheck.p, 0x7f, sizeof(int), c->st));   // first bad atom: none (> any index)
+    CK(cudaMemsetAsync(c->iocheck.p + 1, 0, sizeof(int), c->st));
     k_pack_atoms<<<nblk(n), kBlock, 0, c->st>>>(c->iostage.p, n, c->pos.p, c->vel.p, c->omg.p, c->iocheck.p);
     CKL();
     CK(cudaMemcpyAsync(c->type.p, type, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->tag.p, tag, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
-    int bad[2];
-    CK(cudaMemcpyAsync(bad, c->iocheck.p, sizeof bad, cudaMemcpyDeviceToHost, c->st));
-    // host-side checks and mirrors while the copies are in flight
-    int bad_type = -1;
-    for (int i = 0; i < n && bad_type < 0; i++)
-        if (type[i] < 1 || type[i] > c->P.ntypes) bad_type = i;
-    if (bad_type < 0) {
-        c->h_radius.assign(radius, radius + n);
-        c->h_type.assign(type, type + n);
-    }
-    CK(cudaStreamSynchronize(c->st));
-    if (bad_type >= 0) return set_err(c, GB2_ERR_ARG, "atom type out of range");
-    if (bad[1] == 2) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
-    if (bad[1] == 3) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
-    if (bad[1] == 1) return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", bad[0]);
+    // the device check's verdict lands in pinned memory, so this readback
+    // stays asynchronous and the host work below overlaps the copies
+    CK(cudaMemcpyAsync(&c->h_pinned[8], c->iocheck.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
     const size_t cap = c->cap;
     CK(c->f.alloc(cap));
     CK(c->tq.alloc(cap));
@@ -1506,9 +1534,30 @@ int gb2_upload_atoms(gb2_ctx *c, int n, const double *x, const double *v, const 
     CK(cudaMemsetAsync(c->nnum.p, 0, sizeof(int) * cap, c->st));
     CK(cudaMemsetAsync(c->rnum.p, 0, sizeof(int) * cap, c->st));
     CK(cudaMemsetAsync(c->pnum.p, 0, sizeof(int) * cap, c->st));
+    // host checks while the copies are in flight, in one pass over the
+    // caller's arrays: type range, per type the largest radius (the
+    // neighbour cutoff at setup), the largest tag (Atom::tag_extend)
+    const int nt = c->P.ntypes;
+    int bad_type = -1;
+    double maxrad[kMaxTypes + 1] = {};
+    long maxtag = 0;
+    for (int i = 0; i < n; i++) {
+        const int t = type[i];
+        if (t < 1 || t > nt) {
+            bad_type = i;
+            break;
+        }
+        if (radius[i] > maxrad[t]) maxrad[t] = radius[i];
+        if (tag[i] > maxtag) maxtag = tag[i];
+    }
     CK(cudaStreamSynchronize(c->st));
-    c->maxtag = 0;
-    for (int i = 0; i < n; i++) c->maxtag = std::max<long>(c->maxtag, tag[i]);
+    const int bad0 = c->h_pinned[8], bad1 = c->h_pinned[9];
+    if (bad_type >= 0) return set_err(c, GB2_ERR_ARG, "atom type out of range");
+    if (bad1 == 2) return set_err(c, GB2_ERR_ARG, "Fix nve/sphere requires extended particles");
+    if (bad1 == 3) return set_err(c, GB2_ERR_ARG, "atom mass must be positive");
+    if (bad1 == 1) return set_err(c, GB2_ERR_ARG, "non-finite atom state (atom %d)", bad0);
+    std::memcpy(c->h_maxrad, maxrad, sizeof maxrad);
+    c->maxtag = maxtag;
     c->have_atoms = true;
     return 0;
 }
@@ -1987,10 +2036,7 @@ static int append_inserted(gb2_ctx *c, const std::vector<InsertedParticle> &out,
         }
     }
     CK(cudaStreamSynchronize(c->st));
-    for (int q = 0; q < k; q++) {
-        c->h_radius.push_back(out[q].radius);
-        c->h_type.push_back(out[q].type);
-    }
+    for (int q = 0; q < k; q++) c->h_maxrad[out[q].type] = std::max(c->h_maxrad[out[q].type], out[q].radius);
     c->maxtag += k;
     c->nlocal = nl + k;
     return 0;

@@ -188,5 +188,12 @@ void launch_pair_split(const Dev &D, int nblocks, cudaStream_t st, int minb, int
 void launch_tail_split(const Dev &D, int nblocks, cudaStream_t st, int shearupdate, int integrate, int fuse_next,
                        int store_f);
 bool tri_neighbuild_host(const TriGeom &T, double rSphere, const double *c, double treshold);
+// Small page-locked host words (flags and counts read back from the device)
+// in 256-byte slots of a process-wide arena: locking host pages costs
+// milliseconds per allocation, so contexts take a slot instead of locking
+// their own pages.  The arena's pages stay locked until the process exits.
+constexpr size_t kPinnedSlot = 256;
+int pinned_slot_get(int **slot);
+void pinned_slot_put(int *slot);
 
 }  // namespace gb2

@@ -488,9 +488,12 @@ int gb2_sq_create(const gb2_sq_params *p, gb2_sq_ctx **out)
     c->betaeff = lg / std::sqrt(std::pow(lg, 2.) + std::pow(M_PI, 2.));
     c->mu = p->friction;
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&c->h_pin, 4 * sizeof(int)) != cudaSuccess || c->counters.alloc(8) != cudaSuccess ||
-        c->dflag.alloc(1) != cudaSuccess || cudaMemset(c->counters.p, 0, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        pinned_slot_get(&c->h_pin) != 0 || c->counters.alloc(8) != cudaSuccess ||
+        c->dflag.alloc(1) != cudaSuccess ||
+        cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->st) != cudaSuccess ||
         cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess) {
+        pinned_slot_put(c->h_pin);
+        if (c->st) cudaStreamDestroy(c->st);
         delete c;
         return GB2_ERR_CUDA;
     }
@@ -502,7 +505,7 @@ int gb2_sq_destroy(gb2_sq_ctx *c)
 {
     if (!c) return 0;
     cudaStreamSynchronize(c->st);
-    if (c->h_pin) cudaFreeHost(c->h_pin);
+    pinned_slot_put(c->h_pin);
     if (c->e0) cudaEventDestroy(c->e0);
     if (c->e1) cudaEventDestroy(c->e1);
     cudaStream_t st = c->st;
