@@ -178,9 +178,9 @@ def test_split_pour_statistics():
     fraction and overlap distribution (cumulative histogram over 8 bins)
     agree within 1%.  Trajectories are chaotic, so only statistics compare;
     the spread between two FP64 realisations (another seed) is printed for
-    reference.  The FP64 arm reproduces the reference bit for bit (the
-    golden digests of the reference's own config-1 pour), so its statistics
-    are the reference's."""
+    reference.  The FP64 arm is the bit-exact path, pinned to the
+    reference's own state digests on config 1's 20k pour and the other
+    golden scenes, so its statistics stand for the reference's."""
     box = (0.08, 0.08, 0.2)
     res = []
     for split, seed in ((False, 12345), (True, 12345), (False, 777)):
