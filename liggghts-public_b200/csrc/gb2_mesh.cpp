@@ -362,62 +362,61 @@ bool build_mesh_topology(const double *nodes, int ntri_in, double curvature, dou
         }
 
     // corners.  The walk from corner (t, k) over edge neighbours that hold a
-    // copy of the node reaches the same elements from any of them, so it runs
-    // once per such group and settles every member's corner: active only at
-    // the group's largest element id, when an edge at the node is active and
-    // no two of its edges are colinear.
-    std::vector<uint8_t> corner_active((size_t)3 * n, 1), corner_done((size_t)3 * n, 0);
-    std::vector<int> mark(n, -1), queue, members;
-    std::vector<const double *> evec, eend;
-    int stamp = 0;
-    for (int t = 0; t < n; t++)
-        for (int k = 0; k < 3; k++) {
-            if (corner_done[3 * t + k]) continue;
-            const double *nc = T[t].node[k];
-            stamp++;
-            queue.clear();
-            members.clear();
-            evec.clear();
-            eend.clear();
-            queue.push_back(t);
-            mark[t] = stamp;
-            bool any_active = false;
-            int maxid = -1;
-            for (size_t qi = 0; qi < queue.size(); qi++) {
-                const int e = queue[qi];
-                int in = -1;
-                for (int q = 0; q < 3; q++)
-                    if (nodes_equal(T[e].node[q], nc, precision)) {
-                        in = q;
-                        break;
-                    }
-                if (in < 0) continue;   // visited but holds no copy of the node: not expanded
-                members.push_back(3 * e + in);
-                maxid = std::max(maxid, e);
-                const int prev = (in + 2) % 3;
-                evec.push_back(T[e].edgevec[in]);
-                eend.push_back(T[e].node[(in + 1) % 3]);
-                evec.push_back(T[e].edgevec[prev]);
-                eend.push_back(T[e].node[prev]);
-                if (edge_active[3 * e + in] || edge_active[3 * e + prev]) any_active = true;
-                for (int nb : out.edge_neigh[e])
-                    if (mark[nb] != stamp) {
-                        mark[nb] = stamp;
-                        queue.push_back(nb);
-                    }
+    // copy of the node reaches the same group of corners from any of its
+    // members (the connected holders of the node), so every corner walks its
+    // own group, in parallel, and settles only itself: active only at the
+    // group's largest element id, when an edge at the node is active and no
+    // two of the group's edges are colinear.
+    std::vector<uint8_t> corner_active((size_t)3 * n, 1);
+#pragma omp parallel if (n > 2048)
+    {
+        std::vector<int> mark(n, -1), queue;
+        std::vector<const double *> evec, eend;
+        int stamp = 0;
+#pragma omp for schedule(dynamic, 64)
+        for (int t = 0; t < n; t++)
+            for (int k = 0; k < 3; k++) {
+                const double *nc = T[t].node[k];
+                stamp++;
+                queue.clear();
+                evec.clear();
+                eend.clear();
+                queue.push_back(t);
+                mark[t] = stamp;
+                bool any_active = false;
+                int maxid = -1;
+                for (size_t qi = 0; qi < queue.size(); qi++) {
+                    const int e = queue[qi];
+                    int in = -1;
+                    for (int q = 0; q < 3; q++)
+                        if (nodes_equal(T[e].node[q], nc, precision)) {
+                            in = q;
+                            break;
+                        }
+                    if (in < 0) continue;   // visited but holds no copy of the node: not expanded
+                    maxid = std::max(maxid, e);
+                    const int prev = (in + 2) % 3;
+                    evec.push_back(T[e].edgevec[in]);
+                    eend.push_back(T[e].node[(in + 1) % 3]);
+                    evec.push_back(T[e].edgevec[prev]);
+                    eend.push_back(T[e].node[prev]);
+                    if (edge_active[3 * e + in] || edge_active[3 * e + prev]) any_active = true;
+                    for (int nb : out.edge_neigh[e])
+                        if (mark[nb] != stamp) {
+                            mark[nb] = stamp;
+                            queue.push_back(nb);
+                        }
+                }
+                bool colinear = false;
+                for (size_t a = 0; a < evec.size() && !colinear; a++)
+                    for (size_t b = a + 1; b < evec.size(); b++)
+                        if (std::fabs(dotv(evec[a], evec[b])) > curvature && !nodes_equal(eend[a], eend[b], precision)) {
+                            colinear = true;
+                            break;
+                        }
+                corner_active[3 * t + k] = (!colinear && any_active && t == maxid) ? 1 : 0;
             }
-            bool colinear = false;
-            for (size_t a = 0; a < evec.size() && !colinear; a++)
-                for (size_t b = a + 1; b < evec.size(); b++)
-                    if (std::fabs(dotv(evec[a], evec[b])) > curvature && !nodes_equal(eend[a], eend[b], precision)) {
-                        colinear = true;
-                        break;
-                    }
-            for (int m : members) {
-                corner_active[m] = (!colinear && any_active && m / 3 == maxid) ? 1 : 0;
-                corner_done[m] = 1;
-            }
-        }
+    }
     for (int t = 0; t < n; t++) {
         int bits = 0;
         for (int k = 0; k < 3; k++) {
