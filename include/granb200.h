@@ -103,7 +103,11 @@ typedef struct {
     long nlist, ntouch, nrev, nwall_list, nwall_touch, nmesh_cand, nmesh_touch;
 } gb2_contact_census;
 
-/* context lifecycle */
+/* context lifecycle.  A context's small page-locked host words (flags and
+   counts it reads back from the device) are a 256-byte slot of a pinned
+   arena the library shares between contexts: the first context of a process
+   locks a 64 KiB block (256 slots; more blocks as more contexts are live at
+   once), and those pages stay locked until the process exits. */
 int gb2_create(const gb2_params *p, gb2_ctx **out);
 int gb2_destroy(gb2_ctx *ctx);
 
