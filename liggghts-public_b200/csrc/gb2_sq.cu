@@ -9,6 +9,7 @@
 // deterministic per-particle sums (reverse slots in ascending owner order,
 // then own slots), final_integrate.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -245,6 +246,7 @@ struct gb2_sq_ctx {
     // work lists of the pair pass: 2 lists of nslots items, then the item
     // counts and the taken counter
     Buf<int> work;
+    Buf<signed char> kind;   // per slot: the work list the screen puts it on
     int nsm = 148;
 };
 
@@ -404,6 +406,7 @@ int sq_build(gb2_sq_ctx *c, bool transfer)
     SQCK(c->pti.alloc(ns));
     SQCK(c->ptj.alloc(ns));
     SQCK(c->work.alloc(2 * ns + 4));
+    SQCK(c->kind.alloc(ns));
     SQCK(c->rslot.alloc(ns));
     D = sq_dev(c);
     k_sq_neigh<<<nb(n), kB, 0, c->st>>>(D, G, c->cell_start.p, c->cell_atoms.p, nullptr, c->nbr.p, c->own.p, 1);
@@ -452,8 +455,19 @@ int sq_force(gb2_sq_ctx *c, int shearupdate)
         W.n = c->work.p + 2 * ns;
         W.next = W.n + 2;
         SQCK(cudaMemsetAsync(W.n, 0, 4 * sizeof(int), c->st));
-        k_sq_screen<<<nb(c->nslots), kB, 0, c->st>>>(D, c->own.p, (int)c->nslots, W);
+        k_sq_screen<<<nb(c->nslots), kB, 0, c->st>>>(D, c->own.p, (int)c->nslots, c->kind.p);
         SQCKL();
+        // the two work lists in slot order (stable selections; the counts
+        // stay on the device for the solve kernel)
+        thrust::counting_iterator<int> slots(0);
+        size_t bytes = 0;
+        cub::DeviceSelect::If(nullptr, bytes, slots, W.list[0], W.n, (int)ns, SlotKindIs{c->kind.p, 0}, c->st);
+        SQCK(c->tmp.alloc(bytes));
+        for (int l = 0; l < 2; l++) {
+            bytes = c->tmp.n;
+            SQCK(cub::DeviceSelect::If(c->tmp.p, bytes, slots, W.list[l], W.n + l, (int)ns,
+                                       SlotKindIs{c->kind.p, (signed char)l}, c->st));
+        }
         // the solves: enough resident warps to fill the GPU; each warp takes
         // the next 32 items (first contacts, then warm starts) until none
         // are left

@@ -340,9 +340,10 @@ __device__ __forceinline__ void first_contact(const float *out, const double *ci
 // pair pass (PairGran::compute with the superquadric surface model,
 // src/pair_gran_base.h:255-430, src/surface_model_superquadric.h:108-205,
 // non-spherical Hertz/history) in two kernels: k_sq_screen tests every
-// half-list slot (bounding spheres, oriented boxes) and gathers the slots
-// that need a contact-point solve in two lists, first contacts and warm
-// starts (a previous point exists); k_sq_solve runs the solves, each warp
+// half-list slot (bounding spheres, oriented boxes) and marks the slots
+// that need a contact-point solve for one of two lists, first contacts and
+// warm starts (a previous point exists), which stable selections gather in
+// slot order; k_sq_solve runs the solves, each warp
 // taking the next 32 items, first contacts first.  A step holds few solves
 // (a few per cent of the slots), and its time is set by the longest solve
 // chains -- first contacts through the homotopy or the learned guess -- so
@@ -357,16 +358,12 @@ struct SqWork {
     int *next;   // items taken (over both lists)
 };
 
-__device__ __forceinline__ void work_push(const SqWork &W, int l, int item, bool take)
-{
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    if (!m) return;
-    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&W.n[l], __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (take) W.list[l][base + __popc(m & ((1u << lane) - 1u))] = item;
-}
+// the work list a screened slot joins: 0 first contact, 1 warm start, -1 none
+struct SlotKindIs {
+    const signed char *kind;
+    signed char want;
+    __host__ __device__ bool operator()(int sl) const { return kind[sl] == want; }
+};
 
 // the slot's contact point, state and forces from a finished solve
 __device__ __forceinline__ void sq_finish(const SqDev &D, int sl, int i, int j, int shearupdate, const Newton &o)
@@ -457,8 +454,9 @@ __device__ __forceinline__ void sq_finish(const SqDev &D, int sl, int i, int j, 
 
 // every slot: no force unless a solve below finds a contact; the bounding
 // spheres and (for a pair not yet intersecting) the oriented boxes decide
-// whether the slot needs a solve and which kind
-__global__ void k_sq_screen(SqDev D, const int *__restrict__ own, int nslots, SqWork W)
+// whether the slot needs a solve and which kind (kind[sl]; the host gathers
+// the work lists from it in slot order, so they are the same in every run)
+__global__ void k_sq_screen(SqDev D, const int *__restrict__ own, int nslots, signed char *kind_out)
 {
     const int sl = blockIdx.x * blockDim.x + threadIdx.x;
     int kind = -1;
@@ -487,8 +485,7 @@ __global__ void k_sq_screen(SqDev D, const int *__restrict__ own, int nslots, Sq
             else kind = state == FAR ? 0 : 1;
         }
     }
-    work_push(W, 0, sl, kind == 0);
-    work_push(W, 1, sl, kind == 1);
+    if (sl < nslots) kind_out[sl] = (signed char)kind;
 }
 
 // the solve of one listed slot: a first contact (learned guess with the
