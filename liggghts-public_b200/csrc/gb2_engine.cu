@@ -852,13 +852,17 @@ int mesh_bins_device(gb2_ctx *c, MeshFix &M, bool moving)
     CK(cudaMemsetAsync(M.bincnt.p, 0, sizeof(int) * ((size_t)c->mbins + 1), c->st));
     int endbit = 1;
     if (moving) {
-        k_tri_bin_fill<<<nblk(n), kBlock, 0, c->st>>>(D, n, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p, M.bincnt.p);
+        if (npairs > 0)
+            k_tri_bin_fill<<<nblk(npairs), kBlock, 0, c->st>>>(D, n, npairs, M.trange.p, M.toff.p, M.pkeys.p,
+                                                                M.pvals.p, M.bincnt.p);
         while ((1l << endbit) < (long)c->mbins + 1) endbit++;
     } else {
         const double dx = c->binsize[0] / 2.0, dy = c->binsize[1] / 2.0, dz = c->binsize[2] / 2.0;
         const double maxdiag = std::sqrt(dx * dx + dy * dy + dz * dz);
-        k_tri_bin_fill_cull<<<nblk(n), kBlock, 0, c->st>>>(D, M.tri.p, n, M.trange.p, M.toff.p, M.pkeys.p,
-                                                             M.pvals.p, M.bincnt.p, maxdiag, M.distmax + M.nl_skin);
+        if (npairs > 0)
+            k_tri_bin_fill_cull<<<nblk(npairs), kBlock, 0, c->st>>>(D, M.tri.p, n, npairs, M.trange.p, M.toff.p,
+                                                                     M.pkeys.p, M.pvals.p, M.bincnt.p, maxdiag,
+                                                                     M.distmax + M.nl_skin);
         endbit = 32;   // dropped pairs carry key 0xffffffff
     }
     CKL();

@@ -768,56 +768,71 @@ __global__ void k_tri_bin_range(Dev D, const TriGeom *tri, int ntri, double dist
     count[t] = (int)n;
 }
 
+// One (triangle, bin) pair of the bin lists per thread: the pair's slot p
+// lies in its triangle's range [off[t], off[t+1]) of the exclusive scan of
+// the per-triangle bin counts, found by binary search (a triangle without
+// bins repeats its successor's offset), and its bin is the (p - off[t])-th of
+// the triangle's bin box.  A large triangle spans hundreds of bins, so one
+// thread per pair keeps the whole GPU busy where one thread per triangle
+// left most SMs idle.  Which slot of its triangle's range a bin takes does
+// not matter: the stable sort by bin that follows orders each bin's
+// triangles by slot, and so by triangle.
+__device__ __forceinline__ int tri_of_pair(const int *off, int ntri, int p)
+{
+    int lo = 0, hi = ntri;   // off[lo] <= p < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int pair_bin(const Dev &D, const int *r, int q, int &ix, int &iy, int &iz)
+{
+    const int nz = r[5] - r[2] + 1, ny = r[4] - r[1] + 1;
+    iz = r[2] + q % nz;
+    iy = r[1] + (q / nz) % ny;
+    ix = r[0] + q / (nz * ny);
+    return iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
+}
+
 // Static mesh (FixNeighlistMesh::generate_bin_list, src/fix_neighlist_mesh.cpp:456-490):
 // the same pairs, but a bin is kept only when a sphere of the bin's half
 // diagonal at the bin centre passes the neighbour-build test against the
 // triangle with threshold distmax + skin; dropped pairs get key 0xffffffff
 // and sort to the end.
-__global__ void k_tri_bin_fill_cull(Dev D, const TriGeom *tri, int ntri, const int *range, const int *off,
-                                    unsigned *keys, int *vals, int *bincnt, double maxdiag, double thresh)
+__global__ void k_tri_bin_fill_cull(Dev D, const TriGeom *tri, int ntri, int npairs, const int *range,
+                                    const int *off, unsigned *keys, int *vals, int *bincnt, double maxdiag,
+                                    double thresh)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntri) return;
-    int p = off[t];
-    const int end = off[t + 1];
-    if (p == end) return;
-    const int *r = range + 6 * t;
-    const TriGeom &T = tri[t];
-    for (int ix = r[0]; ix <= r[3]; ix++)
-        for (int iy = r[1]; iy <= r[4]; iy++)
-            for (int iz = r[2]; iz <= r[5]; iz++) {
-                const int b = iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
-                double center[3];
-                center[0] = (D.mbinlo[0] + ix + 0.5) * D.binsize[0] + D.bboxlo[0];
-                center[1] = (D.mbinlo[1] + iy + 0.5) * D.binsize[1] + D.bboxlo[1];
-                center[2] = (D.mbinlo[2] + iz + 0.5) * D.binsize[2] + D.bboxlo[2];
-                const bool keep = tri_neighbuild(T, maxdiag, center, thresh);
-                keys[p] = keep ? (unsigned)b : 0xffffffffu;
-                vals[p] = t;
-                if (keep) atomicAdd(&bincnt[b], 1);
-                p++;
-            }
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int t = tri_of_pair(off, ntri, p);
+    int ix, iy, iz;
+    const int b = pair_bin(D, range + 6 * t, p - off[t], ix, iy, iz);
+    double center[3];
+    center[0] = (D.mbinlo[0] + ix + 0.5) * D.binsize[0] + D.bboxlo[0];
+    center[1] = (D.mbinlo[1] + iy + 0.5) * D.binsize[1] + D.bboxlo[1];
+    center[2] = (D.mbinlo[2] + iz + 0.5) * D.binsize[2] + D.bboxlo[2];
+    const bool keep = tri_neighbuild(tri[t], maxdiag, center, thresh);
+    keys[p] = keep ? (unsigned)b : 0xffffffffu;
+    vals[p] = t;
+    if (keep) atomicAdd(&bincnt[b], 1);
 }
 
-// Pass 2: (bin, triangle) pairs in triangle order, and per-bin counts
-__global__ void k_tri_bin_fill(Dev D, int ntri, const int *range, const int *off, unsigned *keys, int *vals,
-                               int *bincnt)
+// Moving mesh, at every rebuild: (bin, triangle) pairs and per-bin counts
+__global__ void k_tri_bin_fill(Dev D, int ntri, int npairs, const int *range, const int *off, unsigned *keys,
+                               int *vals, int *bincnt)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntri) return;
-    int p = off[t];
-    const int end = off[t + 1];
-    if (p == end) return;
-    const int *r = range + 6 * t;
-    for (int iz = r[2]; iz <= r[5]; iz++)
-        for (int iy = r[1]; iy <= r[4]; iy++)
-            for (int ix = r[0]; ix <= r[3]; ix++) {
-                const int b = iz * D.mbin[1] * D.mbin[0] + iy * D.mbin[0] + ix;
-                keys[p] = (unsigned)b;
-                vals[p] = t;
-                atomicAdd(&bincnt[b], 1);
-                p++;
-            }
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int t = tri_of_pair(off, ntri, p);
+    int ix, iy, iz;
+    const int b = pair_bin(D, range + 6 * t, p - off[t], ix, iy, iz);
+    keys[p] = (unsigned)b;
+    vals[p] = t;
+    atomicAdd(&bincnt[b], 1);
 }
 
 // contact census (diagnostics and the bench's byte model)
