@@ -853,16 +853,14 @@ int mesh_bins_device(gb2_ctx *c, MeshFix &M, bool moving)
     int endbit = 1;
     if (moving) {
         if (npairs > 0)
-            k_tri_bin_fill<<<nblk(npairs), kBlock, 0, c->st>>>(D, n, npairs, M.trange.p, M.toff.p, M.pkeys.p,
-                                                                M.pvals.p, M.bincnt.p);
+            k_tri_bin_fill<<<n, kBlock, 0, c->st>>>(D, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p, M.bincnt.p);
         while ((1l << endbit) < (long)c->mbins + 1) endbit++;
     } else {
         const double dx = c->binsize[0] / 2.0, dy = c->binsize[1] / 2.0, dz = c->binsize[2] / 2.0;
         const double maxdiag = std::sqrt(dx * dx + dy * dy + dz * dz);
         if (npairs > 0)
-            k_tri_bin_fill_cull<<<nblk(npairs), kBlock, 0, c->st>>>(D, M.tri.p, n, npairs, M.trange.p, M.toff.p,
-                                                                     M.pkeys.p, M.pvals.p, M.bincnt.p, maxdiag,
-                                                                     M.distmax + M.nl_skin);
+            k_tri_bin_fill_cull<<<n, kBlock, 0, c->st>>>(D, M.tri.p, M.trange.p, M.toff.p, M.pkeys.p, M.pvals.p,
+                                                          M.bincnt.p, maxdiag, M.distmax + M.nl_skin);
         endbit = 32;   // dropped pairs carry key 0xffffffff
     }
     CKL();

@@ -768,26 +768,14 @@ __global__ void k_tri_bin_range(Dev D, const TriGeom *tri, int ntri, double dist
     count[t] = (int)n;
 }
 
-// One (triangle, bin) pair of the bin lists per thread: the pair's slot p
-// lies in its triangle's range [off[t], off[t+1]) of the exclusive scan of
-// the per-triangle bin counts, found by binary search (a triangle without
-// bins repeats its successor's offset), and its bin is the (p - off[t])-th of
-// the triangle's bin box.  A large triangle spans hundreds of bins, so one
-// thread per pair keeps the whole GPU busy where one thread per triangle
-// left most SMs idle.  Which slot of its triangle's range a bin takes does
-// not matter: the stable sort by bin that follows orders each bin's
-// triangles by slot, and so by triangle.
-__device__ __forceinline__ int tri_of_pair(const int *off, int ntri, int p)
-{
-    int lo = 0, hi = ntri;   // off[lo] <= p < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (off[mid] <= p) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
+// The bin lists' (triangle, bin) pairs: one block per triangle, its threads
+// striding over the triangle's bin box (the q-th bin takes slot off[t] + q
+// of the triangle's range in the exclusive scan of the per-triangle bin
+// counts).  A large triangle spans hundreds of bins, so a block per triangle
+// keeps the whole GPU busy where one thread per triangle left most SMs idle.
+// Which slot of its triangle's range a bin takes does not matter: the stable
+// sort by bin that follows orders each bin's triangles by slot, and so by
+// triangle.
 __device__ __forceinline__ int pair_bin(const Dev &D, const int *r, int q, int &ix, int &iy, int &iz)
 {
     const int nz = r[5] - r[2] + 1, ny = r[4] - r[1] + 1;
@@ -802,37 +790,39 @@ __device__ __forceinline__ int pair_bin(const Dev &D, const int *r, int q, int &
 // diagonal at the bin centre passes the neighbour-build test against the
 // triangle with threshold distmax + skin; dropped pairs get key 0xffffffff
 // and sort to the end.
-__global__ void k_tri_bin_fill_cull(Dev D, const TriGeom *tri, int ntri, int npairs, const int *range,
-                                    const int *off, unsigned *keys, int *vals, int *bincnt, double maxdiag,
-                                    double thresh)
+__global__ void k_tri_bin_fill_cull(Dev D, const TriGeom *tri, const int *range, const int *off, unsigned *keys,
+                                    int *vals, int *bincnt, double maxdiag, double thresh)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npairs) return;
-    const int t = tri_of_pair(off, ntri, p);
-    int ix, iy, iz;
-    const int b = pair_bin(D, range + 6 * t, p - off[t], ix, iy, iz);
-    double center[3];
-    center[0] = (D.mbinlo[0] + ix + 0.5) * D.binsize[0] + D.bboxlo[0];
-    center[1] = (D.mbinlo[1] + iy + 0.5) * D.binsize[1] + D.bboxlo[1];
-    center[2] = (D.mbinlo[2] + iz + 0.5) * D.binsize[2] + D.bboxlo[2];
-    const bool keep = tri_neighbuild(tri[t], maxdiag, center, thresh);
-    keys[p] = keep ? (unsigned)b : 0xffffffffu;
-    vals[p] = t;
-    if (keep) atomicAdd(&bincnt[b], 1);
+    const int t = blockIdx.x;
+    const int p0 = off[t], cnt = off[t + 1] - p0;
+    const int *r = range + 6 * t;
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+        int ix, iy, iz;
+        const int b = pair_bin(D, r, q, ix, iy, iz);
+        double center[3];
+        center[0] = (D.mbinlo[0] + ix + 0.5) * D.binsize[0] + D.bboxlo[0];
+        center[1] = (D.mbinlo[1] + iy + 0.5) * D.binsize[1] + D.bboxlo[1];
+        center[2] = (D.mbinlo[2] + iz + 0.5) * D.binsize[2] + D.bboxlo[2];
+        const bool keep = tri_neighbuild(tri[t], maxdiag, center, thresh);
+        keys[p0 + q] = keep ? (unsigned)b : 0xffffffffu;
+        vals[p0 + q] = t;
+        if (keep) atomicAdd(&bincnt[b], 1);
+    }
 }
 
 // Moving mesh, at every rebuild: (bin, triangle) pairs and per-bin counts
-__global__ void k_tri_bin_fill(Dev D, int ntri, int npairs, const int *range, const int *off, unsigned *keys,
-                               int *vals, int *bincnt)
+__global__ void k_tri_bin_fill(Dev D, const int *range, const int *off, unsigned *keys, int *vals, int *bincnt)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npairs) return;
-    const int t = tri_of_pair(off, ntri, p);
-    int ix, iy, iz;
-    const int b = pair_bin(D, range + 6 * t, p - off[t], ix, iy, iz);
-    keys[p] = (unsigned)b;
-    vals[p] = t;
-    atomicAdd(&bincnt[b], 1);
+    const int t = blockIdx.x;
+    const int p0 = off[t], cnt = off[t + 1] - p0;
+    const int *r = range + 6 * t;
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+        int ix, iy, iz;
+        const int b = pair_bin(D, r, q, ix, iy, iz);
+        keys[p0 + q] = (unsigned)b;
+        vals[p0 + q] = t;
+        atomicAdd(&bincnt[b], 1);
+    }
 }
 
 // contact census (diagnostics and the bench's byte model)
